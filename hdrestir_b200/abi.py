@@ -1,0 +1,149 @@
+"""ctypes binding of the C ABI declared in ``include/hdrestir.h``.
+
+The library is the in-tree ``libhdrestir_b200.so``; there is no other
+implementation to fall back to, so a missing library or a missing GPU fails
+loudly here.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libhdrestir_b200.so"
+
+HDR_OK, HDR_EINVAL, HDR_ENOMEM, HDR_ECANCELLED, HDR_ETIMEOUT, HDR_ECUDA, HDR_ENOSCENE, HDR_EDEVICE = range(8)
+STATUS_NAMES = {0: "HDR_OK", 1: "HDR_EINVAL", 2: "HDR_ENOMEM", 3: "HDR_ECANCELLED", 4: "HDR_ETIMEOUT",
+                5: "HDR_ECUDA", 6: "HDR_ENOSCENE", 7: "HDR_EDEVICE"}
+LIGHT_DISTANT, LIGHT_DOME, LIGHT_RECT, LIGHT_POINT = 0, 1, 2, 3
+AOV_DEPTH, AOV_ALBEDO, AOV_NORMAL = 1, 2, 4
+ACCUM_PARITY, ACCUM_SHADER = 0, 1
+
+_f = C.c_float
+_i = C.c_int32
+_pf = C.POINTER(C.c_float)
+_pi = C.POINTER(C.c_int32)
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("points", _pf), ("num_points", _i), ("indices", _pi), ("num_triangles", _i),
+                ("uvs", _pf), ("num_uvs", _i), ("normals", _pf), ("num_normals", _i),
+                ("colors", _pf), ("num_colors", _i), ("material_indices", _pi), ("num_material_indices", _i)]
+
+
+class InstanceDesc(C.Structure):
+    _fields_ = [("mesh", _i), ("material", _i), ("light", _i), ("reserved", _i), ("transform", _f * 16)]
+
+
+class MaterialDesc(C.Structure):
+    _fields_ = [("diffuse_color", _f * 3), ("metallic", _f), ("roughness", _f), ("specular_color", _f * 3),
+                ("specular", _f), ("opacity", _f), ("ior", _f), ("transmission", _f),
+                ("transmission_color", _f * 3), ("transmission_depth", _f), ("transmission_scatter", _f * 3),
+                ("emission_color", _f * 3), ("emission", _f), ("coat", _f), ("coat_color", _f * 3),
+                ("coat_roughness", _f), ("coat_ior", _f), ("sheen", _f), ("sheen_color", _f * 3),
+                ("sheen_roughness", _f), ("subsurface", _f), ("subsurface_color", _f * 3),
+                ("subsurface_radius", _f * 3), ("subsurface_scale", _f), ("subsurface_anisotropy", _f),
+                ("thin_walled", _i), ("diffuse_roughness", _f)]
+
+
+class LightDesc(C.Structure):
+    _fields_ = [("type", _i), ("color", _f * 3), ("intensity", _f), ("exposure", _f),
+                ("transform", C.c_double * 16), ("width", _f), ("height", _f), ("shaping_cone_angle", _f),
+                ("shaping_cone_softness", _f), ("texture", _pf), ("tex_width", _i), ("tex_height", _i)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("meshes", C.POINTER(MeshDesc)), ("num_meshes", _i),
+                ("instances", C.POINTER(InstanceDesc)), ("num_instances", _i),
+                ("materials", C.POINTER(MaterialDesc)), ("num_materials", _i),
+                ("lights", C.POINTER(LightDesc)), ("num_lights", _i)]
+
+
+class CameraDesc(C.Structure):
+    _fields_ = [("view", C.c_double * 16), ("proj", C.c_double * 16), ("width", _i), ("height", _i),
+                ("has_params", _i), ("enable_dof", _i), ("enable_exposure", _i), ("focal_length", _f),
+                ("f_stop", _f), ("focus_distance", _f), ("bokeh_blades", _i), ("lens_distortion", _f),
+                ("iso", _f), ("shutter_speed", _f)]
+
+
+class PathSettings(C.Structure):
+    _fields_ = [("max_depth", _i), ("enable_subsurface", _i), ("max_reflection_bounces", _i),
+                ("max_refraction_bounces", _i), ("render_ibl_background", _i), ("roulette_aggressiveness", _f)]
+
+
+class RisParams(C.Structure):
+    _fields_ = [("path", PathSettings), ("candidate_count", _i), ("use_reservoir", _i), ("skip_visibility", _i),
+                ("m_cap", _i), ("spatial_neighbors", _i), ("spatial_radius", _f), ("reserved", _i * 2)]
+
+
+class CtxDesc(C.Structure):
+    _fields_ = [("device", _i), ("flags", C.c_uint32), ("hbm_budget_bytes", C.c_size_t)]
+
+
+GBUFFER_DTYPE = np.dtype([("position", "<f4", 3), ("depth", "<f4"), ("normal", "<f4", 3), ("prim_id", "<i4"),
+                          ("smooth_normal", "<f4", 3), ("tri_id", "<i4"), ("albedo", "<f4", 3), ("hit", "<i4"),
+                          ("uv", "<f4", 2), ("dpdu", "<f4", 3), ("dpdv", "<f4", 3)])
+assert GBUFFER_DTYPE.itemsize == 96
+
+# "__ris_reservoir": five float4 planes per pixel
+RESERVOIR_PLANES = ("dir_dist", "color_pdf", "normal_phat", "throughput", "wsum_w_m_meta")
+RES_HAS_SAMPLE, RES_HAS_CANDIDATE, RES_VIS_TESTED, RES_PDF_SOLID = 1, 2, 4, 8
+
+
+class HdrError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads the in-tree library (built by hdrestir_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m hdrestir_b200.build` (needs nvcc)")
+        L = C.CDLL(str(LIB_PATH))
+        vp, i32, sz = C.c_void_p, C.c_int32, C.c_size_t
+        sig = {
+            "hdr_abi_version": (C.c_int, []),
+            "hdr_last_error": (C.c_char_p, []),
+            "hdr_ctx_create": (C.c_int, [C.POINTER(vp), C.POINTER(CtxDesc)]),
+            "hdr_ctx_destroy": (None, [vp]),
+            "hdr_scene_upload": (C.c_int, [vp, C.POINTER(SceneDesc)]),
+            "hdr_raycast": (C.c_int, [vp, C.POINTER(CameraDesc), i32, C.c_uint32]),
+            "hdr_ris_path_trace": (C.c_int, [vp, C.POINTER(CameraDesc), i32, C.POINTER(RisParams)]),
+            "hdr_path_trace": (C.c_int, [vp, C.POINTER(CameraDesc), i32, C.POINTER(PathSettings)]),
+            "hdr_accumulate": (C.c_int, [vp, i32, i32, i32]),
+            "hdr_clear_persistent": (C.c_int, [vp]),
+            "hdr_download": (C.c_int, [vp, C.c_char_p, vp, sz]),
+            "hdr_upload": (C.c_int, [vp, C.c_char_p, vp, sz]),
+            "hdr_buffer_size": (C.c_int, [vp, C.c_char_p, C.POINTER(sz)]),
+            "hdr_synchronize": (C.c_int, [vp]),
+            "hdr_set_cancel": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+            "hdr_trace_rays": (C.c_int, [vp, vp, vp, i32, i32, vp]),
+            "hdr_rng_floats": (C.c_int, [vp, vp, i32, i32, vp]),
+            "hdr_pass_times": (C.c_int, [vp, C.POINTER(C.c_float), i32]),
+            "hdr_launch_count": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != HDR_OK:
+        raise HdrError(status, lib().hdr_last_error().decode(errors="replace"))
+
+
+def exported_symbols() -> list[str]:
+    """Names declared in include/hdrestir.h (used by the export test)."""
+    import re
+    hdr = (Path(__file__).resolve().parent.parent / "include" / "hdrestir.h").read_text()
+    return sorted(set(re.findall(r"^\s*(?:hdr_status|void|int|const char \*)\s*\*?\s*(hdr_\w+)\s*\(", hdr, re.M)))

@@ -1,0 +1,149 @@
+"""Python handle on one ``hdr_ctx``: resident scene, named device frame
+buffers and the pass entry points of include/hdrestir.h."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .scene import Camera, Scene
+
+BUFFER_LAYOUT = {  # name -> (dtype, trailing shape)
+    "Color": (np.float32, (4,)),
+    "__accum_color": (np.float32, (4,)),
+    "Depth": (np.float32, ()),
+    "Albedo": (np.float32, (3,)),
+    "Normal": (np.float32, (3,)),
+}
+
+
+def path_settings(max_depth=32, enable_subsurface=True, max_reflection_bounces=8, max_refraction_bounces=8,
+                  render_ibl_background=True, roulette_aggressiveness=1.0) -> abi.PathSettings:
+    """PathTracePassSettings (integrators/path_integrator.h:12-19) + maxDepth, with the reference defaults."""
+    return abi.PathSettings(int(max_depth), int(enable_subsurface), int(max_reflection_bounces),
+                            int(max_refraction_bounces), int(render_ibl_background), float(roulette_aggressiveness))
+
+
+class Context:
+    def __init__(self, device: int = 0, timings: bool = True, hbm_budget: int = 0):
+        self._lib = abi.lib()
+        self._h = C.c_void_p()
+        desc = abi.CtxDesc(int(device), 1 if timings else 0, int(hbm_budget))
+        abi.check(self._lib.hdr_ctx_create(C.byref(self._h), C.byref(desc)))
+        self.width = self.height = 0
+        self._cancel = None
+
+    # ------------------------------------------------------------ lifetime
+    def close(self) -> None:
+        if self._h:
+            self._lib.hdr_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ scene
+    def upload_scene(self, scene: Scene) -> None:
+        desc = scene.c_desc()
+        abi.check(self._lib.hdr_scene_upload(self._h, C.byref(desc)))
+
+    # ------------------------------------------------------------ passes
+    def raycast(self, cam: Camera, frame_index: int = 0, aovs=()) -> None:
+        mask = 0
+        for a in aovs:
+            mask |= {"Depth": abi.AOV_DEPTH, "Albedo": abi.AOV_ALBEDO, "Normal": abi.AOV_NORMAL}[a]
+        abi.check(self._lib.hdr_raycast(self._h, C.byref(cam.c_desc()), int(frame_index), mask))
+        self.width, self.height = cam.width, cam.height
+
+    def ris_path_trace(self, cam: Camera, frame_index: int, candidate_count=16, use_reservoir=True,
+                       skip_visibility=False, m_cap=0, **settings) -> None:
+        p = abi.RisParams()
+        p.path = path_settings(**settings)
+        p.candidate_count, p.use_reservoir, p.skip_visibility = int(candidate_count), int(use_reservoir), int(
+            skip_visibility)
+        p.m_cap = int(m_cap)
+        abi.check(self._lib.hdr_ris_path_trace(self._h, C.byref(cam.c_desc()), int(frame_index), C.byref(p)))
+
+    def path_trace(self, cam: Camera, frame_index: int, **settings) -> None:
+        p = path_settings(**settings)
+        abi.check(self._lib.hdr_path_trace(self._h, C.byref(cam.c_desc()), int(frame_index), C.byref(p)))
+
+    def accumulate(self, frame_index: int, firefly: bool = True, mode: str = "parity") -> None:
+        m = {"parity": abi.ACCUM_PARITY, "shader": abi.ACCUM_SHADER}[mode]
+        abi.check(self._lib.hdr_accumulate(self._h, int(frame_index), int(firefly), m))
+
+    def clear_persistent(self) -> None:
+        abi.check(self._lib.hdr_clear_persistent(self._h))
+
+    def synchronize(self) -> None:
+        abi.check(self._lib.hdr_synchronize(self._h))
+
+    def set_cancel(self, flag: C.c_int32 | None) -> None:
+        self._cancel = flag
+        abi.check(self._lib.hdr_set_cancel(self._h, C.byref(flag) if flag is not None else None))
+
+    # ------------------------------------------------------------ buffers
+    def buffer_size(self, name: str) -> int:
+        n = C.c_size_t()
+        abi.check(self._lib.hdr_buffer_size(self._h, name.encode(), C.byref(n)))
+        return n.value
+
+    def download(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        nbytes = self.buffer_size(name)
+        if name == "GBuffer":
+            arr = out if out is not None else np.empty(nbytes // 96, abi.GBUFFER_DTYPE)
+        elif name == "__ris_reservoir":
+            arr = out if out is not None else np.empty((5, nbytes // 80, 4), np.float32)
+        elif name in BUFFER_LAYOUT:
+            dt, tail = BUFFER_LAYOUT[name]
+            per = int(np.prod(tail)) if tail else 1
+            arr = out if out is not None else np.empty((nbytes // (4 * per),) + tail, dt)
+        else:
+            arr = out if out is not None else np.empty(nbytes, np.uint8)
+        if arr.nbytes != nbytes or not arr.flags.c_contiguous:
+            raise ValueError(f"{name}: need a contiguous array of {nbytes} bytes")
+        abi.check(self._lib.hdr_download(self._h, name.encode(), arr.ctypes.data_as(C.c_void_p), nbytes))
+        return arr
+
+    def upload(self, name: str, arr: np.ndarray) -> None:
+        arr = np.ascontiguousarray(arr)
+        abi.check(self._lib.hdr_upload(self._h, name.encode(), arr.ctypes.data_as(C.c_void_p), arr.nbytes))
+
+    # ------------------------------------------------------------ queries
+    def trace_rays(self, rays: np.ndarray, tmax: np.ndarray | None = None, any_hit: bool = False) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        out = np.empty(len(rays), abi.GBUFFER_DTYPE)
+        tp = None
+        if tmax is not None:
+            tmax = np.ascontiguousarray(tmax, np.float32)
+            tp = tmax.ctypes.data_as(C.c_void_p)
+        abi.check(self._lib.hdr_trace_rays(self._h, rays.ctypes.data_as(C.c_void_p), tp, len(rays), int(any_hit),
+                                           out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def rng_floats(self, seeds, count: int) -> np.ndarray:
+        seeds = np.ascontiguousarray(seeds, np.uint32)
+        out = np.empty((len(seeds), count), np.float32)
+        abi.check(self._lib.hdr_rng_floats(self._h, seeds.ctypes.data_as(C.c_void_p), len(seeds), int(count),
+                                           out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def pass_times(self) -> tuple[float, float, float]:
+        ms = (C.c_float * 3)()
+        abi.check(self._lib.hdr_pass_times(self._h, ms, 3))
+        return tuple(ms)
+
+    def launch_count(self) -> int:
+        n = C.c_uint64()
+        abi.check(self._lib.hdr_launch_count(self._h, C.byref(n)))
+        return int(n.value)

@@ -1,0 +1,96 @@
+// Device frame-buffer views shared by the pass kernels and their launchers.
+// Every per-pixel buffer is a structure of float4 planes so a warp's loads and
+// stores are 16-byte vectors over consecutive pixels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "camera.cuh"
+#include "traverse.cuh"
+
+namespace hdr {
+
+// "GBuffer" (std::optional<HitRecord> per pixel, raycast_pass.cpp:60-61)
+struct GBufferView {
+    float4 *pos_depth;    // position.xyz, depth
+    float4 *normal_prim;  // normal.xyz, prim id bits (-1 = no hit)
+    float4 *smooth_tri;   // smooth normal.xyz, triangle id bits
+    float4 *albedo_uv;    // albedo.xyz, uv.x
+    float4 *aux0;         // uv.y, dpdu.xyz
+    float4 *aux1;         // dpdv.xyz, 0
+};
+
+struct AovView {       // optional RaycastPass AOVs
+    float *depth;      // f32 x P   (miss = 1)
+    float *albedo;     // f32x3 x P (miss = 0)
+    float *normal;     // f32x3 x P (miss = 0)
+};
+
+// Persistent "__ris_reservoir": WeightedReservoir<RISLightCandidate> per pixel
+// (restir/reservoir.h:69-161, ris_direct_light_integrator.h:26-43).
+struct ReservoirView {
+    float4 *dir_dist;       // Ls.Dir.xyz, Ls.Dist
+    float4 *color_pdf;      // Ls.Color.xyz, Ls.Pdf.value
+    float4 *normal_phat;    // Ls.LightNormal.xyz, targetFunction
+    float4 *throughput;     // Throughput (4 wavelengths)
+    float4 *wsum_w_m_meta;  // WSum, W, CandidateCount bits, meta bits
+};
+// meta bits
+constexpr unsigned kResHasSample = 1u << 0;     // ChosenSample engaged
+constexpr unsigned kResHasCandidate = 1u << 1;  // ChosenSample->Candidate engaged
+constexpr unsigned kResVisTested = 1u << 2;     // VisibilityTested
+constexpr unsigned kResPdfSolidAngle = 1u << 3; // Ls.Pdf.space == SolidAngle
+constexpr unsigned kResOriginShift = 4;         // CandidateOrigin (2 bits)
+constexpr unsigned kResLightShift = 8;          // light index (24 bits)
+
+struct RisParamsD {
+    int candidate_count;
+    int use_reservoir;
+    int skip_visibility;
+    int max_depth;
+    int enable_subsurface;
+    int max_refl, max_refr;
+    int render_ibl_background;
+    float roulette;
+    int m_cap;
+    int spatial_neighbors;
+    float spatial_radius;
+};
+
+struct PathParamsD {
+    int max_depth;
+    int enable_subsurface;
+    int max_refl, max_refr;
+    int render_ibl_background;
+    float roulette;
+};
+
+void launch_raycast(const DeviceScene &s, const CameraD &cam, int frame_index, GBufferView gb, AovView aov,
+                    unsigned *err, cudaStream_t st);
+void launch_trace_rays(const DeviceScene &s, const float *rays, const float *tmax, int n, int any_hit,
+                       float4 *out /* 6 float4 per ray: hdr_gbuffer_texel */, unsigned *err, cudaStream_t st);
+void launch_rng_floats(const uint32_t *seeds, int n, int count, float *out, cudaStream_t st);
+void launch_ris_path_trace(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                           GBufferView gb, ReservoirView res, float4 *color, unsigned *err, cudaStream_t st);
+void launch_path_trace(const DeviceScene &s, const CameraD &cam, int frame_index, const PathParamsD &p,
+                       GBufferView gb, float4 *color, unsigned *err, cudaStream_t st);
+// Returns the number of kernels launched.
+int launch_accumulate(float4 *color, float4 *accum, float4 *scratch, int *flag_dev, int width, int height,
+                      int frame_index, int firefly, int mode, cudaStream_t st);
+
+// Pixel of thread t in a 16x16 tile: each warp covers an 8x4 sub-tile so the
+// rays it traces start close together.
+__device__ __forceinline__ bool tile_pixel(int width, int height, int &x, int &y) {
+    const int tiles_x = (width + 15) >> 4;
+    const int tile = blockIdx.x;
+    const int tx = tile % tiles_x, ty = tile / tiles_x;
+    const int t = threadIdx.x;
+    const int w = t >> 5, lane = t & 31;
+    x = (tx << 4) + ((w & 1) << 3) + (lane & 7);
+    y = (ty << 4) + ((w >> 1) << 2) + (lane >> 3);
+    return x < width && y < height;
+}
+inline int tile_blocks(int width, int height) { return ((width + 15) >> 4) * ((height + 15) >> 4); }
+
+}  // namespace hdr

@@ -1,0 +1,697 @@
+// Integrators on the device.
+//   PathIntegrator::Li / _li                 integrators/path_integrator.cpp:48-209
+//   SampleBounceWithConnection              integrators/direct_light_integrator_interface.h:18-40
+//   MisDirectLightIntegrator                integrators/mis_direct_light_integrator.cpp:37-271
+//   RisDirectLightIntegrator (RIS, ReSTIR)  restir/ris_direct_light_integrator.cpp:84-634
+//   WeightedReservoir                       restir/reservoir.h:69-161
+//   RIS::RandomIndexFromWeights             restir/random_index.h:27-63
+//
+// One thread integrates one pixel. Candidate generation keeps only the running
+// reservoir (no per-candidate arrays): the reference draws all candidate
+// samples first and the reservoir-update numbers after them, so the kernel
+// first replays the sampling decisions alone (no rays) to find where the
+// update numbers start, then generates the candidates for real while a second
+// cursor on the same stream supplies the update numbers. Both cursors must end
+// where the reference's single stream would; a mismatch raises kErrRngDesync.
+#pragma once
+
+#include "frame.cuh"
+#include "lights.cuh"
+#include "material.cuh"
+
+namespace hdr {
+
+constexpr unsigned kErrRngDesync = 4u;
+constexpr unsigned kErrRisCapacity = 8u;
+constexpr int kMaxPlainRisCandidates = 64;
+
+struct Surface {  // RayIntersection with its ShadingPoint
+    V3 ray_o, ray_d;
+    Hit hit;
+    Closure c;
+    V3 sn;  // shading normal
+    bool inside;
+};
+
+struct Connection {  // BsdfBounceConnection
+    Bounce b;
+    bool has_hit;
+    Hit hit;
+};
+
+// Scene::IntersectScene -> optional<HitRecord>
+__device__ __forceinline__ bool intersect(const DeviceScene &s, V3 o, V3 d, Hit &h, unsigned &err) {
+    HitId id;
+    if (!trace_ray<false>(s, o, d, 0.0f, id, err)) return false;
+    h = make_hit(s, o, d, id);
+    return true;
+}
+// "shadowHit && shadowHit->Depth < limit"
+__device__ __forceinline__ bool occluded(const DeviceScene &s, V3 o, V3 d, float limit, unsigned &err) {
+    HitId id;
+    return trace_ray<true>(s, o, d, limit, id, err) && id.t < limit;
+}
+
+__device__ __forceinline__ Surface make_surface(const DeviceScene &s, V3 ro, V3 rd, const Hit &h, const Closure &c,
+                                                bool inside) {
+    Surface sf;
+    sf.ray_o = ro;
+    sf.ray_d = rd;
+    sf.hit = h;
+    sf.c = c;
+    sf.inside = inside;
+    sf.sn = inside ? -c.normal : c.normal;
+    return sf;
+}
+
+// Detail::SampleBounceWithConnection
+__device__ __forceinline__ Connection sample_bounce_with_connection(const DeviceScene &s, const Surface &sf,
+                                                                    int max_refl, int max_refr, BounceState &st,
+                                                                    const SpectralCtx &sc, MtStream &rng,
+                                                                    unsigned &err) {
+    Connection cn;
+    cn.b = sample_bounce(sf.c, sf.sn, sf.inside, sf.hit.position, sf.ray_d, max_refl, max_refr, st, sc, rng);
+    cn.has_hit = false;
+    if (cn.b.ok) cn.has_hit = intersect(s, cn.b.origin, cn.b.dir, cn.hit, err);
+    return cn;
+}
+
+// ============================================================================
+// MisDirectLightIntegrator (PathTracePass)
+// ============================================================================
+struct MisNee {
+    Spec radiance;
+    float p_nee, p_bsdf;
+    bool delta;
+};
+
+// _evaluateNEE (mis_direct_light_integrator.cpp:70-120)
+__device__ inline MisNee mis_evaluate_nee(const DeviceScene &s, const Surface &sf, int li, const LightSampleD &ls,
+                                   const SpectralCtx &sc, unsigned &err) {
+    MisNee r{spec(0.0f), 0.0f, 0.0f, false};
+    const float n_l = dot(sf.sn, ls.dir);
+    if (n_l <= 0.0f) return r;
+    const bool delta = light_is_delta(s, li);
+    const float dist2 = ls.dist * ls.dist;
+    const float cos_y = smaxf(0.0f, dot(-ls.dir, ls.normal));
+    if (cos_y <= 0.0f && !delta) return r;
+    const float p_nee = pdf_to_solid_angle(ls.pdf, ls.pdf_solid_angle, dist2, smaxf(cos_y, 1e-6f));
+    if (p_nee <= 0.0f) return r;
+    if (occluded(s, sf.hit.position + sf.sn * 1e-4f, ls.dir, ls.dist - 1e-3f, err)) return r;
+    const V3 wo = -sf.ray_d;
+    const float bpdf = ggx_pdf(sf.c, sf.sn, wo, ls.dir);
+    const V3 bval = ggx_eval(sf.c, sf.sn, wo, ls.dir);
+    r.radiance = rgb_to_spectrum(bval, sc.up) * rgb_to_spectrum(ls.color, sc.up) * (n_l / p_nee);
+    r.p_nee = p_nee;
+    r.p_bsdf = bpdf;
+    r.delta = delta;
+    return r;
+}
+
+// MisDirectLightIntegrator::Li (per-bounce form, :250-269) = _integrateNEE + _integrateBSDFConnection
+__device__ inline Spec mis_direct_li(const DeviceScene &s, const Surface &sf, bool has_conn, const Connection &cn,
+                              const SpectralCtx &sc, MtStream &rng, unsigned &err) {
+    Spec total = spec(0.0f);
+    // _integrateNEE (:122-178); the environment, when present, is a scene light
+    // and so part of the sampler (no separate sky technique)
+    int li;
+    LightSampleD ls;
+    if (propose_candidate(s, sf.hit.position, rng, li, ls)) {
+        const MisNee nee = mis_evaluate_nee(s, sf, li, ls, sc, err);
+        if (nee.p_nee > 0.0f) {
+            const float w = (nee.delta || !has_conn) ? 1.0f : power_heuristic2(nee.p_nee, nee.p_bsdf);
+            total = total + nee.radiance * w;
+        }
+    }
+    if (!has_conn) return total;
+    // _integrateBSDFConnection (:180-248)
+    const Bounce &b = cn.b;
+    if (b.impossible_nee || b.pdf <= 0.0f) {
+        if (!cn.has_hit) return total + rgb_to_spectrum(env_radiance(s, b.dir), sc.up) * b.tmul;
+        const Closure hc = get_closure(s, cn.hit);
+        return total + rgb_to_spectrum(hc.emission, sc.up) * b.tmul;
+    }
+    float p_sampler = 0.0f, p_env = 0.0f;
+    Spec radiance;
+    if (!cn.has_hit) {
+        if (s.env_light < 0) return total;
+        radiance = rgb_to_spectrum(env_radiance(s, b.dir), sc.up);
+        const float sel = light_select_pdf(s);
+        const float epdf = env_pdf(s, b.dir);
+        p_sampler = sel * epdf;
+        p_env = sel <= 0.0f ? epdf : 0.0f;
+    } else {
+        const Closure hc = get_closure(s, cn.hit);
+        radiance = rgb_to_spectrum(hc.emission, sc.up);
+        if (cn.hit.light >= 0) {
+            const float sel = light_select_pdf(s);
+            if (sel > 0.0f) {
+                const V3 off = cn.hit.position - b.origin;
+                const float dist2 = dot(off, off);
+                const float cos_y = smaxf(0.0f, dot(-b.dir, cn.hit.normal));
+                if (cos_y > 0.0f) {
+                    float av;
+                    bool solid;
+                    light_eval_pdf(s, cn.hit.light, b.dir, av, solid);
+                    p_sampler = sel * pdf_to_solid_angle(av, solid, dist2, cos_y);
+                }
+            }
+        }
+    }
+    if (p_sampler + p_env <= 0.0f) return total + radiance * b.tmul;
+    const float w = power_heuristic3(b.pdf, 1, p_sampler, 1, p_env, 1);
+    return total + radiance * w * b.tmul;
+}
+
+// ============================================================================
+// RisDirectLightIntegrator
+// ============================================================================
+struct Cand {  // optional<RISLightCandidate>
+    bool valid;
+    bool has_lc;  // Candidate (LightCandidate) engaged
+    int light;
+    LightSampleD ls;
+    int origin;   // CandidateOrigin: 0 NEE, 1 SkyNEE, 2 BSDF
+    Spec tp;      // Throughput
+    double ris_weight;
+    float target; // targetFunction (always a float value)
+    bool vis_tested;
+};
+
+__device__ __forceinline__ Cand cand_none() {
+    Cand c;
+    c.valid = false;
+    c.has_lc = false;
+    c.light = -1;
+    c.ls = LightSampleD{v3s(0.0f), v3s(0.0f), v3s(0.0f), 1e30f, 0.0f, false};
+    c.origin = 0;
+    c.tp = spec(0.0f);
+    c.ris_weight = 0.0;
+    c.target = 0.0f;
+    c.vis_tested = true;
+    return c;
+}
+
+struct RisStrategy {  // SamplingStrategy
+    int n_nee, n_sky, n_bsdf;
+    bool skip_vis;
+};
+
+struct RisContrib {  // RisDirectLightIntegrator::MISContrib
+    Spec emission, tmul;
+    float p_nee, p_bsdf;
+    bool use_mis;
+    bool vis_tested;
+};
+
+// _evaluateLightSample (:628-673)
+__device__ inline RisContrib ris_evaluate_light_sample(const DeviceScene &s, const Surface &sf, int li,
+                                                const LightSampleD &ls, bool skip_vis, const SpectralCtx &sc,
+                                                unsigned &err) {
+    const V3 wo = -sf.ray_d;
+    const float n_l = dot(sf.sn, ls.dir);
+    const float dist2 = ls.dist * ls.dist;
+    const float cos_y = smaxf(0.0f, dot(-ls.dir, ls.normal));
+    const float p_nee = pdf_to_solid_angle(ls.pdf, ls.pdf_solid_angle, dist2, smaxf(cos_y, 1e-6f));
+    const float p_bsdf = ggx_pdf(sf.c, sf.sn, wo, ls.dir);
+    const V3 bval = ggx_eval(sf.c, sf.sn, wo, ls.dir);
+    const bool delta = light_is_delta(s, li);
+    RisContrib r{spec(0.0f), spec(0.0f), p_nee, p_bsdf, !delta, true};
+    if (n_l <= 0.0f || p_nee <= 0.0f || (cos_y <= 0.0f && !delta)) return r;
+    r.tmul = rgb_to_spectrum(bval * n_l, sc.up);
+    if (skip_vis) {
+        r.emission = rgb_to_spectrum(ls.color, sc.up);
+        r.vis_tested = false;
+        return r;
+    }
+    if (occluded(s, sf.hit.position + sf.sn * 1e-4f, ls.dir, ls.dist - 1e-3f, err)) return r;
+    r.emission = rgb_to_spectrum(ls.color, sc.up);
+    return r;
+}
+
+// _reEvaluateForTemporalReuse (:675-691)
+__device__ inline Spec ris_reevaluate(const DeviceScene &s, const Surface &sf, int li, const LightSampleD &ls,
+                               const SpectralCtx &sc) {
+    const V3 wo = -sf.ray_d;
+    const float n_l = dot(sf.sn, ls.dir);
+    const float dist2 = ls.dist * ls.dist;
+    const float cos_y = smaxf(0.0f, dot(-ls.dir, ls.normal));
+    const float p_nee = pdf_to_solid_angle(ls.pdf, ls.pdf_solid_angle, dist2, smaxf(cos_y, 1e-6f));
+    if (n_l <= 0.0f || p_nee <= 0.0f || (cos_y <= 0.0f && !light_is_delta(s, li))) return spec(0.0f);
+    const V3 bval = ggx_eval(sf.c, sf.sn, wo, ls.dir);
+    return rgb_to_spectrum(ls.color, sc.up) * rgb_to_spectrum(bval * n_l, sc.up);
+}
+
+// _evaluateBSDFConnection (:693-780)
+__device__ inline RisContrib ris_evaluate_bsdf_connection(const DeviceScene &s, const Surface &sf, const Connection &cn,
+                                                   const RisStrategy &strat, const SpectralCtx &sc) {
+    const Bounce &b = cn.b;
+    RisContrib r{spec(0.0f), b.integrand, 0.0f, b.pdf, false, true};
+    if (b.impossible_nee || b.pdf <= 0.0f) {
+        if (!cn.has_hit) {
+            if (s.env_light >= 0) r.emission = rgb_to_spectrum(env_radiance(s, b.dir), sc.up);
+            return r;
+        }
+        r.emission = rgb_to_spectrum(get_closure(s, cn.hit).emission, sc.up);
+        return r;
+    }
+    if (!cn.has_hit) {
+        if (s.env_light < 0) return r;
+        const float sel = light_select_pdf(s);
+        const float epdf = env_pdf(s, b.dir);
+        const float p_nee = sel > 0.0f ? sel * epdf : (strat.n_sky > 0 ? epdf : 0.0f);
+        r.emission = rgb_to_spectrum(env_radiance(s, b.dir), sc.up);
+        r.p_nee = p_nee;
+        r.use_mis = p_nee > 0.0f;
+        return r;
+    }
+    float p_nee = 0.f;
+    r.emission = rgb_to_spectrum(get_closure(s, cn.hit).emission, sc.up);
+    if (cn.hit.light >= 0) {
+        const float sel = light_select_pdf(s);
+        const V3 off = cn.hit.position - b.origin;
+        const float dist2 = dot(off, off);
+        const float cos_y = smaxf(0.0f, dot(-b.dir, cn.hit.normal));
+        if (cos_y > 0.0f && sel > 0.0f) {
+            float av;
+            bool solid;
+            light_eval_pdf(s, cn.hit.light, b.dir, av, solid);
+            p_nee = sel * pdf_to_solid_angle(av, solid, dist2, cos_y);
+        }
+    }
+    r.p_nee = p_nee;
+    r.use_mis = p_nee > 0.0f;
+    return r;
+}
+
+struct RisCtx {
+    const DeviceScene *s;
+    const Surface *sf;
+    const SpectralCtx *sc;
+    RisStrategy strat;
+    bool has_conn;
+    const Connection *conn;
+    bool conn_cand;  // the caller's connection becomes candidate #0 (its pdf > 0)
+    int n_total;     // allCandidates.size()
+    int max_refl, max_refr;
+};
+
+// Candidate j of allCandidates: NEE (sampler), then sky NEE, then BSDF.
+// kFull = false only advances the stream exactly like the full generation.
+template <bool kFull>
+__device__ Cand ris_candidate(const RisCtx &x, int j, MtStream &rng, unsigned &err) {
+    const DeviceScene &s = *x.s;
+    const Surface &sf = *x.sf;
+    const SpectralCtx &sc = *x.sc;
+    Cand c = cand_none();
+    if (j < x.strat.n_nee) {
+        // _generateNEECandidates (:553-589)
+        if (!kFull) {
+            skip_propose_candidate(s, rng);
+            return c;
+        }
+        int li;
+        LightSampleD ls;
+        if (!propose_candidate(s, sf.hit.position, rng, li, ls)) return c;
+        const RisContrib nee = ris_evaluate_light_sample(s, sf, li, ls, x.strat.skip_vis, sc, err);
+        const Spec contribution = nee.emission * nee.tmul;
+        const float target = spectrum_luminance(contribution, sc.cie);
+        const float mis = nee.use_mis ? power_heuristic3(nee.p_nee, x.strat.n_nee, 0.0f, x.strat.n_sky, nee.p_bsdf,
+                                                         x.strat.n_bsdf)
+                                      : 1.0f;
+        c.valid = true;
+        c.has_lc = true;
+        c.light = li;
+        c.ls = ls;
+        c.origin = 0;
+        c.tp = contribution;
+        c.ris_weight = (double)(mis * target) / ((double)nee.p_nee + 1e-9);
+        c.target = target;
+        c.vis_tested = nee.vis_tested;
+        return c;
+    }
+    j -= x.strat.n_nee;
+    if (j < x.strat.n_sky) {
+        // sky NEE needs an environment outside the light sampler; every supported
+        // environment is a scene light, so this technique never has candidates.
+        return c;
+    }
+    j -= x.strat.n_sky;
+    // _generateBSDFSamplingCandidates (:396-551)
+    if (x.conn_cand && j == 0) {
+        if (!kFull) return c;
+        const RisContrib bc = ris_evaluate_bsdf_connection(s, sf, *x.conn, x.strat, sc);
+        const Spec contribution = bc.emission * bc.tmul;
+        const double target = (double)spectrum_luminance(contribution, sc.cie);
+        float p_sampler = bc.p_nee, p_sky = 0.0f;
+        if (!x.conn->has_hit && (s.env_light < 0 || light_select_pdf(s) <= 0.0f)) {
+            p_sampler = 0.0f;
+            p_sky = bc.p_nee;
+        }
+        const double mis =
+            (double)power_heuristic3(bc.p_bsdf, x.strat.n_bsdf, p_sampler, x.strat.n_nee, p_sky, x.strat.n_sky);
+        c.valid = true;
+        c.has_lc = false;
+        c.origin = 0;
+        c.tp = contribution;
+        c.ris_weight = mis * target / ((double)bc.p_bsdf + 1e-9);
+        c.target = (float)target;
+        c.vis_tested = true;
+        return c;
+    }
+    BounceState st{0, 0};
+    if (!kFull) {
+        (void)sample_bounce(sf.c, sf.sn, sf.inside, sf.hit.position, sf.ray_d, 1, 1, st, sc, rng);
+        return c;
+    }
+    const Connection cn = sample_bounce_with_connection(s, sf, 1, 1, st, sc, rng, err);
+    if (!cn.b.ok) return c;
+    if (!cn.has_hit) {
+        if (s.env_light < 0) return c;
+        const Spec env_tp = cn.b.integrand;
+        const V3 wi = cn.b.dir;
+        const V3 env_rgb = env_radiance(s, wi);
+        const Spec env_em = rgb_to_spectrum(env_rgb, sc.up);
+        const float p_bsdf = cn.b.pdf;
+        const float sel = light_select_pdf(s);
+        const float epdf = env_pdf(s, wi);
+        const float p_sampler = sel * epdf;
+        const float p_sky = (sel <= 0.0f && x.strat.n_sky > 0) ? epdf : 0.0f;
+        const float p_nee = p_sampler + p_sky;
+        const double target = (double)spectrum_luminance(env_em * env_tp, sc.cie);
+        const double mis =
+            (double)power_heuristic3(p_bsdf, x.strat.n_bsdf, p_sampler, x.strat.n_nee, p_sky, x.strat.n_sky);
+        c.valid = true;
+        c.has_lc = p_nee > 0.0f;
+        c.light = s.env_light;
+        c.ls = LightSampleD{wi, env_rgb, -wi, 1e30f, p_nee, true};
+        c.origin = 2;
+        c.tp = env_em * env_tp;
+        c.ris_weight = mis * target / ((double)p_bsdf + 1e-9);
+        c.target = (float)target;
+        c.vis_tested = true;
+        return c;
+    }
+    if (cn.hit.light < 0) return c;  // GetLightAtHit == nullptr
+    const RisContrib bc = ris_evaluate_bsdf_connection(s, sf, cn, x.strat, sc);
+    const Spec contribution = bc.emission * bc.tmul;
+    const double target = (double)spectrum_luminance(contribution, sc.cie);
+    const double mis =
+        (double)power_heuristic3(bc.p_bsdf, x.strat.n_bsdf, bc.p_nee, x.strat.n_nee, 0.0f, x.strat.n_sky);
+    const V3 wi = cn.b.dir;
+    float av;
+    bool solid;
+    light_eval_pdf(s, cn.hit.light, wi, av, solid);
+    av *= light_select_pdf(s);
+    c.valid = true;
+    c.has_lc = true;
+    c.light = cn.hit.light;
+    c.ls = LightSampleD{wi, get_closure(s, cn.hit).emission, cn.hit.normal, cn.hit.depth, av, solid};
+    c.origin = 2;
+    c.tp = contribution;
+    c.ris_weight = mis * target / ((double)bc.p_bsdf + 1e-9);
+    c.target = (float)target;
+    c.vis_tested = true;
+    return c;
+}
+
+struct Reservoir {  // WeightedReservoir<RISLightCandidate>
+    Cand chosen;    // chosen.valid == ChosenSample engaged
+    float wsum;
+    int m;
+    float w;
+};
+
+__device__ __forceinline__ void reservoir_update(Reservoir &r, const Cand &c, float weight, MtStream &rng) {
+    ++r.m;
+    if (weight <= 0.0f) return;
+    r.wsum += weight;
+    if (rng.next_float() <= weight / r.wsum) r.chosen = c;
+}
+
+__device__ __forceinline__ void reservoir_finalize(Reservoir &r, int cpf) {
+    if (!r.chosen.valid || r.m <= 0) {
+        r.w = 0.0f;
+        return;
+    }
+    const float phat = r.chosen.target;
+    if (phat <= 0.0f) {
+        r.w = 0.0f;
+        return;
+    }
+    const int frames = smaxi(1, r.m / smaxi(1, cpf));
+    r.w = r.wsum / ((float)frames * phat);
+    if (!isfinite(r.w)) r.w = 0.0f;
+}
+
+__device__ __forceinline__ void reservoir_load(const ReservoirView &v, size_t i, Reservoir &r) {
+    const float4 a = v.dir_dist[i], b = v.color_pdf[i], c = v.normal_phat[i], d = v.throughput[i];
+    const float4 e = v.wsum_w_m_meta[i];
+    const unsigned meta = (unsigned)fbits(e.w);
+    r.wsum = e.x;
+    r.w = e.y;
+    r.m = fbits(e.z);
+    Cand &k = r.chosen;
+    k.valid = (meta & kResHasSample) != 0;
+    k.has_lc = (meta & kResHasCandidate) != 0;
+    k.vis_tested = (meta & kResVisTested) != 0;
+    k.origin = (int)((meta >> kResOriginShift) & 3u);
+    k.light = (int)(meta >> kResLightShift) - 1;
+    k.ls = LightSampleD{V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, V3{c.x, c.y, c.z}, a.w, b.w,
+                        (meta & kResPdfSolidAngle) != 0};
+    k.tp = Spec{{d.x, d.y, d.z, d.w}};
+    k.target = c.w;
+    k.ris_weight = 0.0;
+}
+
+__device__ __forceinline__ void reservoir_store(const ReservoirView &v, size_t i, const Reservoir &r) {
+    const Cand &k = r.chosen;
+    unsigned meta = 0;
+    if (k.valid) meta |= kResHasSample;
+    if (k.has_lc) meta |= kResHasCandidate;
+    if (k.vis_tested) meta |= kResVisTested;
+    if (k.ls.pdf_solid_angle) meta |= kResPdfSolidAngle;
+    meta |= ((unsigned)k.origin & 3u) << kResOriginShift;
+    meta |= ((unsigned)(k.light + 1) & 0xFFFFFFu) << kResLightShift;
+    v.dir_dist[i] = make_float4(k.ls.dir.x, k.ls.dir.y, k.ls.dir.z, k.ls.dist);
+    v.color_pdf[i] = make_float4(k.ls.color.x, k.ls.color.y, k.ls.color.z, k.ls.pdf);
+    v.normal_phat[i] = make_float4(k.ls.normal.x, k.ls.normal.y, k.ls.normal.z, k.target);
+    v.throughput[i] = make_float4(k.tp.v[0], k.tp.v[1], k.tp.v[2], k.tp.v[3]);
+    v.wsum_w_m_meta[i] = make_float4(r.wsum, r.w, __int_as_float(r.m), __int_as_float((int)meta));
+}
+
+struct RisRun {
+    int candidate_count;
+    bool use_reservoir;
+    bool skip_vis;
+    int m_cap;  // extension: 0 = unbounded (reference)
+};
+
+// RisDirectLightIntegrator::Li, per-bounce form (:230-361). primary == (callId.id < callId.stride).
+__device__ inline Spec ris_direct_li(const DeviceScene &s, const Surface &sf, bool has_conn, const Connection &cn,
+                              const SpectralCtx &sc, MtStream &rng, bool primary, const RisRun &run,
+                              const ReservoirView &rv, size_t pixel, unsigned &err) {
+    // technique split (:239-246); every supported environment is a scene light,
+    // so the sampler covers it and there is no separate sky technique
+    const int N = run.candidate_count;
+    const int n_tech = 2;
+    RisCtx x;
+    x.s = &s;
+    x.sf = &sf;
+    x.sc = &sc;
+    x.strat.n_nee = smaxi(1, N / n_tech);
+    x.strat.n_sky = 0;
+    x.strat.n_bsdf = smaxi(0, N - x.strat.n_nee - x.strat.n_sky);
+    x.strat.skip_vis = run.skip_vis;
+    x.has_conn = has_conn;
+    x.conn = &cn;
+    x.conn_cand = has_conn && cn.b.pdf > 0.0f;
+    const int n_fresh = x.strat.n_bsdf - (x.conn_cand ? 1 : 0);
+    x.n_total = x.strat.n_nee + x.strat.n_sky + (x.conn_cand ? 1 : 0) + smaxi(0, n_fresh);
+
+    if (run.use_reservoir && primary) {
+        // ---- reservoir branch (:267-331)
+        MtStream upd = rng;  // replay the sampling draws to find the first update draw
+        for (int j = 0; j < x.n_total; ++j) (void)ris_candidate<false>(x, j, upd, err);
+        const uint32_t gen_end = upd.k;
+        Reservoir r;
+        r.chosen = cand_none();
+        r.wsum = 0.0f;
+        r.m = 0;
+        r.w = 0.0f;
+        for (int j = 0; j < x.n_total; ++j) {
+            const Cand c = ris_candidate<true>(x, j, rng, err);
+            if (c.valid)
+                reservoir_update(r, c, (float)c.ris_weight, upd);
+            else
+                ++r.m;  // CountMiss
+        }
+        if (rng.k != gen_end) err |= kErrRngDesync;
+        rng = upd;
+        // temporal reuse (:284-305)
+        Reservoir prev;
+        reservoir_load(rv, pixel, prev);
+        if (prev.chosen.valid && prev.chosen.has_lc) {
+            const Spec reeval = ris_reevaluate(s, sf, prev.chosen.light, prev.chosen.ls, sc);
+            const float phat_curr = spectrum_luminance(reeval, sc.cie);
+            const float phat_gen = prev.chosen.target;
+            if (phat_gen > 0.0f) {
+                prev.chosen.target = phat_curr;
+                prev.chosen.tp = reeval;
+                if (run.m_cap > 0) {  // extension: bound the history (M-cap)
+                    const int cap = run.m_cap * x.n_total;
+                    if (prev.m > cap) {
+                        prev.wsum *= (float)cap / (float)prev.m;
+                        prev.m = cap;
+                    }
+                }
+                const float mw = prev.wsum * (phat_curr / phat_gen);
+                // Merge (:157-166)
+                r.m += prev.m;
+                if (mw > 0.0f) {
+                    r.wsum += mw;
+                    if (rng.next_float() <= mw / r.wsum) r.chosen = prev.chosen;
+                }
+            }
+        }
+        reservoir_finalize(r, x.n_total);
+        // winner visibility (:309-321)
+        if (r.chosen.valid && !r.chosen.vis_tested && r.chosen.has_lc) {
+            const RisContrib nee = ris_evaluate_light_sample(s, sf, r.chosen.light, r.chosen.ls, false, sc, err);
+            r.chosen.tp = nee.emission * nee.tmul;
+            r.chosen.vis_tested = true;
+        }
+        reservoir_store(rv, pixel, r);
+        if (!r.chosen.valid || r.w <= 0.0f) return spec(0.0f);
+        return r.chosen.tp * r.w;
+    }
+
+    // ---- standard RIS (:333-361): RandomIndexFromWeights over stored weights
+    if (x.n_total > kMaxPlainRisCandidates) {
+        err |= kErrRisCapacity;
+        return spec(0.0f);
+    }
+    const MtStream start = rng;
+    double weights[kMaxPlainRisCandidates];
+    double wsum = 0.0;
+    for (int j = 0; j < x.n_total; ++j) {
+        const Cand c = ris_candidate<true>(x, j, rng, err);
+        const double w = c.valid ? c.ris_weight : 0.0;
+        weights[j] = w;
+        if (w > 0.0) wsum += w;
+    }
+    if (wsum <= 0.0) return spec(0.0f);
+    double remaining = (double)rng.next_float() * wsum;
+    int chosen = -1;
+    for (int j = 0; j < x.n_total; ++j) {
+        const double w = weights[j];
+        if (w <= 0.0) continue;
+        remaining -= w;
+        if (remaining <= 0.0) {
+            chosen = j;
+            break;
+        }
+    }
+    if (chosen < 0) return spec(0.0f);
+    // rebuild the winner from its own draws (a second pass over the same stream)
+    MtStream replay = start;
+    for (int j = 0; j < chosen; ++j) (void)ris_candidate<false>(x, j, replay, err);
+    const Cand c = ris_candidate<true>(x, chosen, replay, err);
+    if (!c.valid) return spec(0.0f);
+    const float W = (float)(wsum / (double)c.target);
+    Spec tp = c.tp;
+    if (!c.vis_tested && c.has_lc) {
+        const RisContrib nee = ris_evaluate_light_sample(s, sf, c.light, c.ls, false, sc, err);
+        tp = nee.emission * nee.tmul;
+    }
+    return tp * W;
+}
+
+// ============================================================================
+// PathIntegrator (integrators/path_integrator.cpp:48-209)
+// ============================================================================
+struct PathRun {
+    int max_depth;
+    bool enable_subsurface;
+    int max_refl, max_refr;
+    bool render_ibl_background;
+    float roulette;
+};
+
+template <bool kRis>
+__device__ __forceinline__ Spec direct_li(const DeviceScene &s, const Surface &sf, bool has_conn,
+                                          const Connection &cn, const SpectralCtx &sc, MtStream &rng, bool primary,
+                                          const RisRun &ris, const ReservoirView &rv, size_t pixel, unsigned &err) {
+    if (kRis) return ris_direct_li(s, sf, has_conn, cn, sc, rng, primary, ris, rv, pixel, err);
+    return mis_direct_li(s, sf, has_conn, cn, sc, rng, err);
+}
+
+// _li (:92-209)
+template <bool kRis>
+__device__ Spec path_li_shaded(const DeviceScene &s, const Surface &sf0, const SpectralCtx &sc, MtStream &rng,
+                               const PathRun &pr, const RisRun &ris, const ReservoirView &rv, size_t pixel,
+                               unsigned &err) {
+    Spec total = rgb_to_spectrum(sf0.c.emission, sc.up);
+    Spec tp = spec(1.0f);
+    BounceState st{0, 0};
+    const Connection first = sample_bounce_with_connection(s, sf0, pr.max_refl, pr.max_refr, st, sc, rng, err);
+    total = total + direct_li<kRis>(s, sf0, first.b.ok, first, sc, rng, true, ris, rv, pixel, err);
+    if (!first.b.ok) return total;
+    tp = tp * first.b.tmul;
+    V3 ro = first.b.origin, rd = first.b.dir;
+    bool has_next = first.has_hit;
+    Hit next = first.hit;
+    for (int bounce = 1; bounce < pr.max_depth; ++bounce) {
+        if (!has_next) break;
+        const Hit bh = next;
+        Closure c = get_closure(s, bh);
+        if (!pr.enable_subsurface) c.subsurface = 0.0f;
+        if (c.opacity < 0.999f && rng.next_float() > c.opacity) {
+            ro = bh.position + rd * 1e-4f;
+            has_next = intersect(s, ro, rd, next, err);
+            --bounce;
+            continue;
+        }
+        const bool inside = dot(c.normal, rd) > 0.0f;
+        beer_absorption(tp, c, bh.depth, inside, sc);
+        const Surface sf = make_surface(s, ro, rd, bh, c, inside);
+        const Connection cn = sample_bounce_with_connection(s, sf, pr.max_refl, pr.max_refr, st, sc, rng, err);
+        total = total + tp * direct_li<kRis>(s, sf, cn.b.ok, cn, sc, rng, false, ris, rv, pixel, err);
+        if (!cn.b.ok) break;
+        tp = tp * cn.b.tmul;
+        ro = cn.b.origin;
+        rd = cn.b.dir;
+        has_next = cn.has_hit;
+        next = cn.hit;
+        if (cn.b.skip_roulette) continue;
+        if (bounce > 3) {
+            const float p = sclampf(spec_max(tp) * pr.roulette, 0.0f, 1.0f);
+            if (rng.next_float() > p) break;
+            tp = tp * (1.0f / p);
+        }
+    }
+    return total;
+}
+
+// PathIntegrator::Li (:48-90): opacity skip at the GBuffer hit, Beer, then _li.
+template <bool kRis>
+__device__ Spec path_li(const DeviceScene &s, V3 ray_o, V3 ray_d, bool has_hit, Hit hit, const SpectralCtx &sc,
+                        MtStream &rng, const PathRun &pr, const RisRun &ris, const ReservoirView &rv, size_t pixel,
+                        unsigned &err) {
+    Spec tp = spec(1.0f);
+    while (has_hit) {
+        Closure c = get_closure(s, hit);
+        if (!pr.enable_subsurface) c.subsurface = 0.0f;
+        if (c.opacity >= 0.999f || rng.next_float() <= c.opacity) {
+            const bool inside = dot(c.normal, ray_d) > 0.0f;
+            beer_absorption(tp, c, hit.depth, inside, sc);
+            const Surface sf = make_surface(s, ray_o, ray_d, hit, c, inside);
+            return tp * path_li_shaded<kRis>(s, sf, sc, rng, pr, ris, rv, pixel, err);
+        }
+        has_hit = intersect(s, hit.position + ray_d * 1e-4f, ray_d, hit, err);
+    }
+    if (s.env_light >= 0 && pr.render_ibl_background) return rgb_to_spectrum(env_radiance(s, ray_d), sc.up);
+    return spec(0.0f);
+}
+
+}  // namespace hdr

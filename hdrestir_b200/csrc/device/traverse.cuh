@@ -1,0 +1,287 @@
+// Scene query on the device: Scene::IntersectScene (scene/scene.cpp:409-535)
+// over the reference's own two-level tree (TLAS of instances, one midpoint-split
+// BLAS per mesh subset), replayed in the reference's visiting order so the
+// closest hit and its tie-breaks are bit-identical:
+//  * TLAS: explicit stack, right child pushed before left, nodes rejected when
+//    the slab entry distance exceeds the current closest t (scene.cpp:414-510);
+//  * BLAS: depth-first, left before right, leaf triangles in array order,
+//    closest hit replaced only on strictly smaller t (bvh.cpp:243-305);
+//  * slab and Moller-Trumbore tests with the reference's thresholds: the BLAS
+//    slab compares |d| < 1e-8 in double (bvh.cpp:43), the TLAS slab in float
+//    (scene.cpp:25), the triangle determinant in double (bvh.cpp:16).
+// Shadow rays only need "is the closest hit nearer than L": running the same
+// traversal and stopping as soon as the running closest t drops below L gives
+// exactly that answer, because the running t only decreases.
+#pragma once
+
+#include "gf.cuh"
+
+namespace hdr {
+
+constexpr int kBlasStack = 64;
+constexpr int kTlasStack = 64;
+
+// error bits reported back to the host
+constexpr unsigned kErrBlasStack = 1u;
+constexpr unsigned kErrTlasStack = 2u;
+
+struct DeviceScene {
+    const float4 *blas_nodes;  // 2 per node
+    const float4 *tri_geo;     // 3 per triangle
+    const float4 *tri_attr;    // 9 per triangle
+    const float4 *instances;   // 8 per instance
+    const float4 *tlas_nodes;  // 2 per node
+    const int *tlas_inst;
+    const float4 *materials;   // 12 per material
+    const float4 *lights;      // 12 per light
+    const float *dome_pixels;
+    const float *dome_row_cdf;
+    const float *dome_col_cdf;
+    int num_instances;
+    int num_materials;
+    int num_lights;
+    int env_light;
+    int dome_width, dome_height;
+    float dome_total_lum;
+    int has_tlas;
+};
+
+__device__ __forceinline__ int fbits(float f) { return __float_as_int(f); }
+
+struct SlabRay {
+    V3 o;
+    V3 inv;
+    bool small[3];
+};
+
+// IntersectAABB of scene.cpp:16-47 (float thresholds) or bvh.cpp:32-64 (double ones).
+template <bool kDoubleThresholds>
+__device__ __forceinline__ SlabRay make_slab_ray(V3 o, V3 d) {
+    SlabRay r;
+    r.o = o;
+    const float dd[3] = {d.x, d.y, d.z};
+    float inv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float a = fabsf(dd[i]);
+        // |d| < 1e-8 in double  <=>  |d| <= 9.99999993922529e-09f (the float nearest below 1e-8)
+        r.small[i] = kDoubleThresholds ? (a <= 9.99999993922529e-09f) : (a < 1e-8f);
+        inv[i] = 1.0f / dd[i];
+    }
+    r.inv = V3{inv[0], inv[1], inv[2]};
+    return r;
+}
+
+__device__ __forceinline__ bool slab_test(const SlabRay &r, float4 lo, float4 hi, float &t_entry) {
+    if (lo.x > hi.x || lo.y > hi.y || lo.z > hi.z) return false;  // GfRange3f::IsEmpty
+    float tmin = -1e30f, tmax = 1e30f;
+    const float o[3] = {r.o.x, r.o.y, r.o.z};
+    const float iv[3] = {r.inv.x, r.inv.y, r.inv.z};
+    const float mn[3] = {lo.x, lo.y, lo.z};
+    const float mx[3] = {hi.x, hi.y, hi.z};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (r.small[i]) {
+            if (o[i] < mn[i] || o[i] > mx[i]) return false;
+        } else {
+            float t1 = (mn[i] - o[i]) * iv[i];
+            float t2 = (mx[i] - o[i]) * iv[i];
+            if (t1 > t2) {
+                const float tt = t1;
+                t1 = t2;
+                t2 = tt;
+            }
+            tmin = smaxf(tmin, t1);
+            tmax = sminf(tmax, t2);
+            if (tmin > tmax) return false;
+        }
+    }
+    t_entry = tmin;
+    return tmax > 0.0f && tmax > 1e-4f;
+}
+
+// IntersectTriangle (bvh.cpp:8-30)
+__device__ __forceinline__ bool tri_test(V3 o, V3 d, const float4 *g, float &t, float &u, float &v) {
+    const float4 g0 = __ldg(g), g1 = __ldg(g + 1), g2 = __ldg(g + 2);
+    const V3 v0{g0.x, g0.y, g0.z};
+    const V3 e1{g0.w, g1.x, g1.y};
+    const V3 e2{g1.z, g1.w, g2.x};
+    const V3 pvec = cross(d, e2);
+    const float det = dot(e1, pvec);
+    if (fabsf(det) <= 9.99999993922529e-09f) return false;  // std::abs(det) < 1e-8 (double)
+    const float inv_det = 1.0f / det;
+    const V3 tvec = o - v0;
+    u = dot(tvec, pvec) * inv_det;
+    if (u < 0.0f || u > 1.0f) return false;
+    const V3 qvec = cross(tvec, e1);
+    v = dot(d, qvec) * inv_det;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    t = dot(e2, qvec) * inv_det;
+    return t > 1e-4f;
+}
+
+struct HitId {
+    float t;
+    int inst;  // -1: miss
+    int tri;   // triangle index local to the instance's mesh
+    float u, v;
+};
+
+// Closest hit (kAnyHit = false), or "closest t < t_limit" test (kAnyHit = true).
+// err receives kErr* bits if a stack would overflow (the host rejects scenes
+// deeper than the stacks, so this is a guard, not a path).
+template <bool kAnyHit>
+__device__ bool trace_ray(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId &hit, unsigned &err) {
+    hit.t = 1e30f;
+    hit.inst = -1;
+    hit.tri = -1;
+    hit.u = hit.v = 0.0f;
+    if (!s.has_tlas) return false;
+    const SlabRay wr = make_slab_ray<false>(o, d);
+    int tstack[kTlasStack];
+    int tsp = 0;
+    tstack[tsp++] = 0;
+    bool was_hit = false;
+    while (tsp > 0) {
+        const int ni = tstack[--tsp];
+        const float4 lo = __ldg(&s.tlas_nodes[2 * ni]);
+        const float4 hi = __ldg(&s.tlas_nodes[2 * ni + 1]);
+        float t_aabb = 0.0f;
+        if (!slab_test(wr, lo, hi, t_aabb) || t_aabb > hit.t) continue;
+        const int left = fbits(lo.w);
+        if (left < 0) {
+            const int start = -left - 1;
+            const int count = fbits(hi.w);
+            for (int k = 0; k < count; ++k) {
+                const int ii = __ldg(&s.tlas_inst[start + k]);
+                const float4 *ip = s.instances + 8 * ii;
+                const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2), m3 = __ldg(ip + 3);
+                const float4 r7 = __ldg(ip + 7);
+                if (fbits(r7.y) == 0) continue;  // mesh without triangles: empty BVH
+                const float inv[16] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w,
+                                       m2.x, m2.y, m2.z, m2.w, m3.x, m3.y, m3.z, m3.w};
+                const V3 oo = m4f_transform(inv, o);
+                const V3 od = m4f_transform_dir(inv, d);
+                const int node_base = fbits(__ldg(&ip[4].w));
+                const int tri_base = fbits(__ldg(&ip[5].w));
+                const SlabRay br = make_slab_ray<true>(oo, od);
+                float bt = hit.t;
+                int btri = -1;
+                float bu = 0.0f, bv = 0.0f;
+                int bstack[kBlasStack];
+                int bsp = 0;
+                bstack[bsp++] = 0;
+                bool done = false;
+                while (bsp > 0 && !done) {
+                    const int bn = bstack[--bsp];
+                    const float4 nlo = __ldg(&s.blas_nodes[2 * (node_base + bn)]);
+                    const float4 nhi = __ldg(&s.blas_nodes[2 * (node_base + bn) + 1]);
+                    float ta;
+                    if (!slab_test(br, nlo, nhi, ta)) continue;
+                    if (ta > bt) continue;
+                    const int bl = fbits(nlo.w);
+                    if (bl < 0) {
+                        const int st = -bl - 1;
+                        const int cnt = fbits(nhi.w);
+                        for (int q = 0; q < cnt; ++q) {
+                            float tt, uu, vv;
+                            if (tri_test(oo, od, s.tri_geo + 3 * (size_t)(tri_base + st + q), tt, uu, vv)) {
+                                if (tt < bt) {
+                                    bt = tt;
+                                    btri = st + q;
+                                    bu = uu;
+                                    bv = vv;
+                                    if (kAnyHit && bt < t_limit) {
+                                        done = true;
+                                        break;
+                                    }
+                                }
+                            }
+                        }
+                    } else {
+                        if (bsp + 2 > kBlasStack) {
+                            err |= kErrBlasStack;
+                            done = true;
+                            break;
+                        }
+                        bstack[bsp++] = bl + 1;
+                        bstack[bsp++] = bl;
+                    }
+                }
+                if (btri < 0) continue;
+                if (bt >= hit.t) continue;
+                hit.t = bt;
+                hit.inst = ii;
+                hit.tri = btri;
+                hit.u = bu;
+                hit.v = bv;
+                was_hit = true;
+                if (kAnyHit && hit.t < t_limit) return true;
+            }
+        } else {
+            if (tsp + 2 > kTlasStack) {
+                err |= kErrTlasStack;
+                break;
+            }
+            tstack[tsp++] = left + 1;
+            tstack[tsp++] = left;
+        }
+    }
+    return was_hit;
+}
+
+// HitRecord (core/hit_record.h:15-27) of IntersectScene (scene.cpp:437-535)
+struct Hit {
+    V3 position;
+    V3 normal;
+    V3 smooth_normal;
+    V3 dpdu, dpdv;
+    V2 uv;
+    V3 albedo;
+    float depth;
+    int prim;      // PrimId == MatId == instance index
+    int tri;
+    int material;  // PreviewSurface params index, -1 = DefaultMaterial
+    int light;     // GetLightAtHit result, -1 = none
+};
+
+__device__ __forceinline__ V3 ld3(float4 a) { return V3{a.x, a.y, a.z}; }
+
+__device__ inline Hit make_hit(const DeviceScene &s, V3 o, V3 d, const HitId &h) {
+    Hit r;
+    const float4 *ip = s.instances + 8 * h.inst;
+    const float4 t0 = __ldg(ip + 4), t1 = __ldg(ip + 5), t2 = __ldg(ip + 6), r7 = __ldg(ip + 7);
+    const float T[16] = {t0.x, t0.y, t0.z, 0.0f, t1.x, t1.y, t1.z, 0.0f, t2.x, t2.y, t2.z, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f};
+    const int tri_base = fbits(t1.w);
+    const float4 *a = s.tri_attr + 9 * (size_t)(tri_base + h.tri);
+    const float4 a0 = __ldg(a), a1 = __ldg(a + 1), a2 = __ldg(a + 2), a3 = __ldg(a + 3), a4 = __ldg(a + 4);
+    const float4 a5 = __ldg(a + 5), a6 = __ldg(a + 6), a7 = __ldg(a + 7), a8 = __ldg(a + 8);
+    const float w = 1.0f - h.u - h.v;
+    const V3 ng = ld3(a0);
+    // bvh.cpp:276-292
+    const V2 uv = (V2{a1.w, a2.w} * w + V2{a3.w, a4.w} * h.u) + V2{a5.w, a6.w} * h.v;
+    V3 sn = ng;
+    if (a0.w != 0.0f) sn = normalized((ld3(a1) * w + ld3(a2) * h.u) + ld3(a3) * h.v);
+    const V3 color = (ld3(a4) * w + ld3(a5) * h.u) + ld3(a6) * h.v;
+    // scene.cpp:467-474
+    r.normal = normalized(m4f_transform_dir(T, ng));
+    r.smooth_normal = normalized(m4f_transform_dir(T, sn));
+    r.dpdu = normalized(m4f_transform_dir(T, ld3(a7)));
+    r.dpdv = normalized(m4f_transform_dir(T, ld3(a8)));
+    r.uv = uv;
+    r.material = fbits(t2.w);
+    r.light = fbits(r7.x);
+    if (r.material >= 0) {
+        const float4 m0 = __ldg(&s.materials[12 * r.material]);
+        r.albedo = ld3(m0);  // PreviewSurfaceParams::DiffuseColor (scene.cpp:476-478)
+    } else {
+        r.albedo = color;
+    }
+    r.position = o + h.t * d;
+    r.depth = h.t;
+    r.prim = h.inst;
+    r.tri = h.tri;
+    return r;
+}
+
+}  // namespace hdr

@@ -1,0 +1,617 @@
+// C ABI of the device passes (declared in include/hdrestir.h).
+//
+// One hdr_ctx owns a CUDA stream, the resident device scene and the named
+// device frame buffers. The reference moves its named host buffers in and out
+// of a FrameBuffersMap per pipeline run (core/frame_buffer_map.cpp:76-101);
+// here the same names stay resident on the GPU and only cross to the host on
+// hdr_download / hdr_upload.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/hdrestir.h"
+#include "device/frame.cuh"
+#include "host/scene_build.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+hdr_status fail(hdr_status st, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+#define HDR_CUDA(call)                                                                                 \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return fail(HDR_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));       \
+    } while (0)
+
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct hdr_ctx {
+    int device = 0;
+    uint32_t flags = 0;
+    size_t budget = 0;
+    size_t allocated = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+
+    // resident scene
+    std::vector<DevBuf> scene_bufs;
+    hdr::DeviceScene scene{};
+    bool has_scene = false;
+
+    // named frame buffers
+    std::map<std::string, DevBuf> buffers;
+    int width = 0, height = 0;
+
+    unsigned *d_err = nullptr;
+    int *d_flag = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    float pass_ms[3] = {0, 0, 0};
+    const volatile int32_t *cancel = nullptr;
+    uint64_t launches = 0;
+};
+
+namespace {
+
+hdr_status dev_alloc(hdr_ctx *c, DevBuf &b, size_t bytes) {
+    if (c->budget && c->allocated + bytes > c->budget)
+        return fail(HDR_ENOMEM, "allocation of %zu bytes exceeds the HBM budget (%zu of %zu in use)", bytes,
+                    c->allocated, c->budget);
+    void *p = nullptr;
+    if (bytes) {
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) return fail(HDR_ENOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+    b.ptr = p;
+    b.bytes = bytes;
+    c->allocated += bytes;
+    return HDR_OK;
+}
+
+void dev_free(hdr_ctx *c, DevBuf &b) {
+    if (b.ptr) cudaFree(b.ptr);
+    c->allocated -= b.bytes;
+    b = DevBuf{};
+}
+
+// FrameBuffersMap::Add / AddOrGetPersistent: create (zeroed) or resize keeping
+// the prefix; a same-size request returns the existing buffer untouched.
+hdr_status ensure_buffer(hdr_ctx *c, const char *name, size_t bytes, void **out) {
+    auto it = c->buffers.find(name);
+    if (it != c->buffers.end() && it->second.bytes == bytes) {
+        *out = it->second.ptr;
+        return HDR_OK;
+    }
+    DevBuf nb;
+    hdr_status st = dev_alloc(c, nb, bytes);
+    if (st != HDR_OK) return st;
+    if (bytes) HDR_CUDA(cudaMemsetAsync(nb.ptr, 0, bytes, c->stream));
+    if (it != c->buffers.end()) {
+        const size_t keep = std::min(bytes, it->second.bytes);
+        if (keep) HDR_CUDA(cudaMemcpyAsync(nb.ptr, it->second.ptr, keep, cudaMemcpyDeviceToDevice, c->stream));
+        HDR_CUDA(cudaStreamSynchronize(c->stream));
+        dev_free(c, it->second);
+        it->second = nb;
+    } else {
+        c->buffers[name] = nb;
+    }
+    *out = nb.ptr;
+    return HDR_OK;
+}
+
+void *find_buffer(hdr_ctx *c, const char *name, size_t *bytes) {
+    auto it = c->buffers.find(name);
+    if (it == c->buffers.end()) return nullptr;
+    if (bytes) *bytes = it->second.bytes;
+    return it->second.ptr;
+}
+
+hdr_status check_cancel(hdr_ctx *c) {
+    if (c->cancel && *c->cancel) return fail(HDR_ECANCELLED, "render job cancelled");
+    return HDR_OK;
+}
+
+hdr_status check_camera(const hdr_camera *cam) {
+    if (!cam) return fail(HDR_EINVAL, "camera is NULL");
+    if (cam->width <= 0 || cam->height <= 0 || (int64_t)cam->width * cam->height > (int64_t)1 << 28)
+        return fail(HDR_EINVAL, "bad frame size %dx%d", cam->width, cam->height);
+    return HDR_OK;
+}
+
+// RenderContext camera -> device: inverses as the passes compute them
+// (raycast_pass.cpp:86-87), exposure as GetExposureMultiplier (camera_params.h:22-31).
+hdr::CameraD make_camera(const hdr_camera *cam) {
+    hdr::CameraD d{};
+    hdr::gf_inverse4d(cam->view, d.inv_view);
+    hdr::gf_inverse4d(cam->proj, d.inv_proj);
+    d.width = cam->width;
+    d.height = cam->height;
+    d.p.has_params = cam->has_params;
+    d.p.enable_dof = cam->enable_dof;
+    d.p.enable_exposure = cam->enable_exposure;
+    d.p.focal_length = cam->focal_length;
+    d.p.f_stop = cam->f_stop;
+    d.p.focus_distance = cam->focus_distance;
+    d.p.bokeh_blades = cam->bokeh_blades;
+    d.p.lens_distortion = cam->lens_distortion;
+    d.p.iso = cam->iso;
+    d.p.shutter_speed = cam->shutter_speed;
+    float mult = 1.0f;
+    if (cam->has_params && cam->enable_exposure) {
+        const float safe = std::max(cam->f_stop, 0.1f);
+        mult = (cam->iso / 100.0f) * cam->shutter_speed / (safe * safe) * 100.0f;
+    }
+    d.p.exposure_mult = mult;
+    return d;
+}
+
+constexpr size_t kGbPlanes = 6;
+constexpr size_t kResPlanes = 5;
+
+hdr_status gbuffer_view(hdr_ctx *c, size_t count, bool create, hdr::GBufferView &gb) {
+    void *p = nullptr;
+    if (create) {
+        hdr_status st = ensure_buffer(c, "GBuffer", count * kGbPlanes * sizeof(float4), &p);
+        if (st != HDR_OK) return st;
+    } else {
+        size_t bytes = 0;
+        p = find_buffer(c, "GBuffer", &bytes);
+        if (!p || bytes != count * kGbPlanes * sizeof(float4))
+            return fail(HDR_EINVAL, "GBuffer must be present (produced by RaycastPass) for %zu pixels", count);
+    }
+    float4 *b = (float4 *)p;
+    gb = hdr::GBufferView{b, b + count, b + 2 * count, b + 3 * count, b + 4 * count, b + 5 * count};
+    return HDR_OK;
+}
+
+hdr_status begin_pass(hdr_ctx *c) {
+    if (c->flags & 1u) HDR_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    return HDR_OK;
+}
+hdr_status end_pass(hdr_ctx *c, int slot) {
+    HDR_CUDA(cudaGetLastError());
+    if (c->flags & 1u) {
+        HDR_CUDA(cudaEventRecord(c->ev[1], c->stream));
+        HDR_CUDA(cudaEventSynchronize(c->ev[1]));
+        float ms = 0.0f;
+        HDR_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+        c->pass_ms[slot] = ms;
+    }
+    return HDR_OK;
+}
+
+hdr_status read_device_error(hdr_ctx *c) {
+    unsigned e = 0;
+    HDR_CUDA(cudaMemcpyAsync(&e, c->d_err, sizeof(e), cudaMemcpyDeviceToHost, c->stream));
+    HDR_CUDA(cudaStreamSynchronize(c->stream));
+    if (e) {
+        HDR_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), c->stream));
+        return fail(HDR_EDEVICE, "device traversal stack limit reached (error bits 0x%x)", e);
+    }
+    return HDR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hdr_abi_version(void) { return HDR_ABI_VERSION; }
+
+const char *hdr_last_error(void) { return g_last_error.c_str(); }
+
+hdr_status hdr_ctx_create(hdr_ctx **out, const hdr_ctx_desc *desc) {
+    if (!out) return fail(HDR_EINVAL, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    HDR_CUDA(cudaGetDeviceCount(&ndev));
+    const int dev = desc ? desc->device : 0;
+    if (dev < 0 || dev >= ndev) return fail(HDR_EINVAL, "device %d not present (%d devices)", dev, ndev);
+    HDR_CUDA(cudaSetDevice(dev));
+    hdr_ctx *c = new hdr_ctx();
+    c->device = dev;
+    c->flags = desc ? desc->flags : 0;
+    c->budget = desc ? desc->hbm_budget_bytes : 0;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_err, 64);
+    if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, 64);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev[1]);
+    if (e != cudaSuccess) {
+        hdr_ctx_destroy(c);
+        return fail(HDR_ECUDA, "context setup: %s", cudaGetErrorString(e));
+    }
+    c->d_flag = (int *)((char *)c->d_err + 32);
+    *out = c;
+    return HDR_OK;
+}
+
+void hdr_ctx_destroy(hdr_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &b : c->scene_bufs) dev_free(c, b);
+    for (auto &kv : c->buffers) dev_free(c, kv.second);
+    if (c->d_err) cudaFree(c->d_err);
+    for (auto &e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
+    if (!c || !desc) return fail(HDR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaSetDevice(c->device));
+    hdr::FlatScene f;
+    std::string err;
+    if (!hdr::build_flat_scene(*desc, f, err)) return fail(HDR_EINVAL, "%s", err.c_str());
+    if (f.max_blas_depth >= hdr::kBlasStack - 1 || f.max_tlas_depth >= hdr::kTlasStack - 1)
+        return fail(HDR_EINVAL, "BVH depth %d / TLAS depth %d exceeds the device traversal stack (%d)",
+                    f.max_blas_depth, f.max_tlas_depth, hdr::kBlasStack);
+    HDR_CUDA(cudaStreamSynchronize(c->stream));
+    for (auto &b : c->scene_bufs) dev_free(c, b);
+    c->scene_bufs.clear();
+    c->has_scene = false;
+
+    auto upload = [&](const void *src, size_t bytes, const void **dst) -> hdr_status {
+        DevBuf b;
+        hdr_status st = dev_alloc(c, b, std::max<size_t>(bytes, 16));
+        if (st != HDR_OK) return st;
+        if (bytes) HDR_CUDA(cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, c->stream));
+        c->scene_bufs.push_back(b);
+        *dst = b.ptr;
+        return HDR_OK;
+    };
+    hdr::DeviceScene s{};
+    hdr_status st;
+#define UP(vec, field)                                                                              \
+    st = upload(vec.data(), vec.size() * sizeof(vec[0]), (const void **)&s.field);                   \
+    if (st != HDR_OK) return st;
+    UP(f.blas_nodes, blas_nodes);
+    UP(f.tri_geo, tri_geo);
+    UP(f.tri_attr, tri_attr);
+    UP(f.instances, instances);
+    UP(f.tlas_nodes, tlas_nodes);
+    UP(f.tlas_inst, tlas_inst);
+    UP(f.materials, materials);
+    UP(f.lights, lights);
+    UP(f.dome_pixels, dome_pixels);
+    UP(f.dome_row_cdf, dome_row_cdf);
+    UP(f.dome_col_cdf, dome_col_cdf);
+#undef UP
+    s.num_instances = f.num_instances;
+    s.num_materials = f.num_materials;
+    s.num_lights = f.num_lights;
+    s.env_light = f.env_light;
+    s.dome_width = f.dome_width;
+    s.dome_height = f.dome_height;
+    s.dome_total_lum = f.dome_total_lum;
+    s.has_tlas = f.num_instances > 0 ? 1 : 0;
+    HDR_CUDA(cudaStreamSynchronize(c->stream));
+    c->scene = s;
+    c->has_scene = true;
+    return HDR_OK;
+}
+
+hdr_status hdr_raycast(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, uint32_t aov_mask) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    hdr_status st = check_camera(cam);
+    if (st != HDR_OK) return st;
+    if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_raycast before hdr_scene_upload");
+    if ((st = check_cancel(c)) != HDR_OK) return st;
+    HDR_CUDA(cudaSetDevice(c->device));
+    const size_t count = (size_t)cam->width * cam->height;
+    hdr::GBufferView gb;
+    if ((st = gbuffer_view(c, count, true, gb)) != HDR_OK) return st;
+    hdr::AovView aov{nullptr, nullptr, nullptr};
+    void *p;
+    if (aov_mask & HDR_AOV_DEPTH) {
+        if ((st = ensure_buffer(c, "Depth", count * 4, &p)) != HDR_OK) return st;
+        aov.depth = (float *)p;
+    }
+    if (aov_mask & HDR_AOV_ALBEDO) {
+        if ((st = ensure_buffer(c, "Albedo", count * 12, &p)) != HDR_OK) return st;
+        aov.albedo = (float *)p;
+    }
+    if (aov_mask & HDR_AOV_NORMAL) {
+        if ((st = ensure_buffer(c, "Normal", count * 12, &p)) != HDR_OK) return st;
+        aov.normal = (float *)p;
+    }
+    c->width = cam->width;
+    c->height = cam->height;
+    const hdr::CameraD d = make_camera(cam);
+    if ((st = begin_pass(c)) != HDR_OK) return st;
+    hdr::launch_raycast(c->scene, d, frame_index, gb, aov, c->d_err, c->stream);
+    c->launches += 1;
+    return end_pass(c, 0);
+}
+
+hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, const hdr_ris_params *p) {
+    if (!c || !p) return fail(HDR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    hdr_status st = check_camera(cam);
+    if (st != HDR_OK) return st;
+    if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_ris_path_trace before hdr_scene_upload");
+    if (p->candidate_count < 1 || p->candidate_count > 4096)
+        return fail(HDR_EINVAL, "candidate_count %d out of range [1, 4096]", p->candidate_count);
+    if (p->path.max_depth < 1) return fail(HDR_EINVAL, "max_depth must be >= 1");
+    if ((st = check_cancel(c)) != HDR_OK) return st;
+    HDR_CUDA(cudaSetDevice(c->device));
+    const size_t count = (size_t)cam->width * cam->height;
+    hdr::GBufferView gb;
+    if ((st = gbuffer_view(c, count, false, gb)) != HDR_OK) return st;
+    void *color = nullptr, *res = nullptr;
+    if ((st = ensure_buffer(c, "Color", count * 16, &color)) != HDR_OK) return st;
+    hdr::ReservoirView rv{};
+    if (p->use_reservoir) {
+        // GetOrCreatePersistent("__ris_reservoir") (ris_direct_light_integrator.cpp:56-67)
+        if ((st = ensure_buffer(c, "__ris_reservoir", count * kResPlanes * sizeof(float4), &res)) != HDR_OK) return st;
+        float4 *r = (float4 *)res;
+        rv = hdr::ReservoirView{r, r + count, r + 2 * count, r + 3 * count, r + 4 * count};
+    }
+    hdr::RisParamsD d{};
+    d.candidate_count = p->candidate_count;
+    d.use_reservoir = p->use_reservoir;
+    d.skip_visibility = p->skip_visibility;
+    d.max_depth = p->path.max_depth;
+    d.enable_subsurface = p->path.enable_subsurface;
+    d.max_refl = p->path.max_reflection_bounces;
+    d.max_refr = p->path.max_refraction_bounces;
+    d.render_ibl_background = p->path.render_ibl_background;
+    d.roulette = p->path.roulette_aggressiveness;
+    d.m_cap = p->m_cap;
+    d.spatial_neighbors = p->spatial_neighbors;
+    d.spatial_radius = p->spatial_radius;
+    const hdr::CameraD cd = make_camera(cam);
+    if ((st = begin_pass(c)) != HDR_OK) return st;
+    hdr::launch_ris_path_trace(c->scene, cd, frame_index, d, gb, rv, (float4 *)color, c->d_err, c->stream);
+    c->launches += 1;
+    return end_pass(c, 1);
+}
+
+hdr_status hdr_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, const hdr_path_settings *p) {
+    if (!c || !p) return fail(HDR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    hdr_status st = check_camera(cam);
+    if (st != HDR_OK) return st;
+    if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_path_trace before hdr_scene_upload");
+    if (p->max_depth < 1) return fail(HDR_EINVAL, "max_depth must be >= 1");
+    if ((st = check_cancel(c)) != HDR_OK) return st;
+    HDR_CUDA(cudaSetDevice(c->device));
+    const size_t count = (size_t)cam->width * cam->height;
+    hdr::GBufferView gb;
+    if ((st = gbuffer_view(c, count, false, gb)) != HDR_OK) return st;
+    void *color = nullptr;
+    if ((st = ensure_buffer(c, "Color", count * 16, &color)) != HDR_OK) return st;
+    hdr::PathParamsD d{};
+    d.max_depth = p->max_depth;
+    d.enable_subsurface = p->enable_subsurface;
+    d.max_refl = p->max_reflection_bounces;
+    d.max_refr = p->max_refraction_bounces;
+    d.render_ibl_background = p->render_ibl_background;
+    d.roulette = p->roulette_aggressiveness;
+    const hdr::CameraD cd = make_camera(cam);
+    if ((st = begin_pass(c)) != HDR_OK) return st;
+    hdr::launch_path_trace(c->scene, cd, frame_index, d, gb, (float4 *)color, c->d_err, c->stream);
+    c->launches += 1;
+    return end_pass(c, 1);
+}
+
+hdr_status hdr_accumulate(hdr_ctx *c, int32_t frame_index, int32_t firefly, int32_t mode) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (mode != HDR_ACCUM_PARITY && mode != HDR_ACCUM_SHADER) return fail(HDR_EINVAL, "unknown accumulation mode");
+    if (frame_index < 0) return fail(HDR_EINVAL, "frame_index must be >= 0");
+    hdr_status st;
+    if ((st = check_cancel(c)) != HDR_OK) return st;
+    HDR_CUDA(cudaSetDevice(c->device));
+    size_t bytes = 0;
+    void *color = find_buffer(c, "Color", &bytes);
+    if (!color || c->width <= 0 || bytes != (size_t)c->width * c->height * 16)
+        return fail(HDR_EINVAL, "Color must be present (produced by PathTracePass) at the current frame size");
+    const size_t count = (size_t)c->width * c->height;
+    void *accum = nullptr, *scratch = nullptr;
+    if ((st = ensure_buffer(c, "__accum_color", count * 16, &accum)) != HDR_OK) return st;
+    if (firefly)
+        if ((st = ensure_buffer(c, "__firefly_scratch", count * 32, &scratch)) != HDR_OK) return st;
+    if ((st = begin_pass(c)) != HDR_OK) return st;
+    const int n = hdr::launch_accumulate((float4 *)color, (float4 *)accum, (float4 *)scratch, c->d_flag, c->width,
+                                         c->height, frame_index, firefly, mode, c->stream);
+    if (n < 0) return fail(HDR_ECUDA, "accumulation launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    c->launches += (uint64_t)n;
+    return end_pass(c, 2);
+}
+
+hdr_status hdr_clear_persistent(hdr_ctx *c) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaSetDevice(c->device));
+    for (const char *name : {"__accum_color", "__ris_reservoir"}) {
+        auto it = c->buffers.find(name);
+        if (it != c->buffers.end()) dev_free(c, it->second), c->buffers.erase(it);
+    }
+    return HDR_OK;
+}
+
+hdr_status hdr_buffer_size(hdr_ctx *c, const char *name, size_t *bytes) {
+    if (!c || !name || !bytes) return fail(HDR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (!find_buffer(c, name, bytes)) return fail(HDR_EINVAL, "no buffer named '%s'", name);
+    return HDR_OK;
+}
+
+hdr_status hdr_download(hdr_ctx *c, const char *name, void *dst, size_t bytes) {
+    if (!c || !name || (!dst && bytes)) return fail(HDR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaSetDevice(c->device));
+    size_t have = 0;
+    void *src = find_buffer(c, name, &have);
+    if (!src) return fail(HDR_EINVAL, "no buffer named '%s'", name);
+    if (have != bytes) return fail(HDR_EINVAL, "buffer '%s' holds %zu bytes, %zu requested", name, have, bytes);
+    if (std::strcmp(name, "GBuffer") == 0) {
+        // planar float4 planes -> hdr_gbuffer_texel records
+        const size_t count = have / (kGbPlanes * sizeof(float4));
+        std::vector<float4> planes(count * kGbPlanes);
+        HDR_CUDA(cudaMemcpyAsync(planes.data(), src, have, cudaMemcpyDeviceToHost, c->stream));
+        HDR_CUDA(cudaStreamSynchronize(c->stream));
+        hdr_gbuffer_texel *t = (hdr_gbuffer_texel *)dst;
+        if (have != count * sizeof(hdr_gbuffer_texel))
+            return fail(HDR_EINVAL, "GBuffer texel size mismatch");
+        for (size_t i = 0; i < count; ++i) {
+            const float4 a = planes[i], b = planes[count + i], s = planes[2 * count + i], al = planes[3 * count + i];
+            const float4 x0 = planes[4 * count + i], x1 = planes[5 * count + i];
+            hdr_gbuffer_texel &o = t[i];
+            int prim, tri;
+            std::memcpy(&prim, &b.w, 4);
+            std::memcpy(&tri, &s.w, 4);
+            o.position[0] = a.x, o.position[1] = a.y, o.position[2] = a.z, o.depth = a.w;
+            o.normal[0] = b.x, o.normal[1] = b.y, o.normal[2] = b.z, o.prim_id = prim;
+            o.smooth_normal[0] = s.x, o.smooth_normal[1] = s.y, o.smooth_normal[2] = s.z, o.tri_id = tri;
+            o.albedo[0] = al.x, o.albedo[1] = al.y, o.albedo[2] = al.z, o.hit = prim >= 0 ? 1 : 0;
+            o.uv[0] = al.w, o.uv[1] = x0.x;
+            o.dpdu[0] = x0.y, o.dpdu[1] = x0.z, o.dpdu[2] = x0.w;
+            o.dpdv[0] = x1.x, o.dpdv[1] = x1.y, o.dpdv[2] = x1.z;
+        }
+        return read_device_error(c);
+    }
+    HDR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+    HDR_CUDA(cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
+
+hdr_status hdr_upload(hdr_ctx *c, const char *name, const void *src, size_t bytes) {
+    if (!c || !name || (!src && bytes)) return fail(HDR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaSetDevice(c->device));
+    if (std::strcmp(name, "GBuffer") == 0) return fail(HDR_EINVAL, "GBuffer is produced on the device only");
+    void *dst = nullptr;
+    hdr_status st = ensure_buffer(c, name, bytes, &dst);
+    if (st != HDR_OK) return st;
+    if (bytes) HDR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    return HDR_OK;
+}
+
+hdr_status hdr_synchronize(hdr_ctx *c) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaSetDevice(c->device));
+    HDR_CUDA(cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
+
+hdr_status hdr_set_cancel(hdr_ctx *c, const volatile int32_t *flag) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->cancel = flag;
+    return HDR_OK;
+}
+
+hdr_status hdr_trace_rays(hdr_ctx *c, const float *rays, const float *tmax, int32_t n, int32_t any_hit,
+                          hdr_gbuffer_texel *out) {
+    if (!c || (n > 0 && (!rays || !out)) || n < 0) return fail(HDR_EINVAL, "bad argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_trace_rays before hdr_scene_upload");
+    if (n == 0) return HDR_OK;
+    HDR_CUDA(cudaSetDevice(c->device));
+    static_assert(sizeof(hdr_gbuffer_texel) == 96, "texel layout");
+    DevBuf dr, dt, dout;
+    hdr_status st;
+    if ((st = dev_alloc(c, dr, (size_t)n * 24)) != HDR_OK) return st;
+    if ((st = dev_alloc(c, dt, tmax ? (size_t)n * 4 : 0)) != HDR_OK) return dev_free(c, dr), st;
+    if ((st = dev_alloc(c, dout, (size_t)n * 96)) != HDR_OK) return dev_free(c, dr), dev_free(c, dt), st;
+    cudaError_t e = cudaMemcpyAsync(dr.ptr, rays, (size_t)n * 24, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && tmax) e = cudaMemcpyAsync(dt.ptr, tmax, (size_t)n * 4, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        hdr::launch_trace_rays(c->scene, (const float *)dr.ptr, tmax ? (const float *)dt.ptr : nullptr, n, any_hit,
+                               (float4 *)dout.ptr, c->d_err, c->stream);
+        c->launches += 1;
+        e = cudaGetLastError();
+    }
+    std::vector<float4> raw;
+    if (e == cudaSuccess) {
+        raw.resize((size_t)n * 6);
+        e = cudaMemcpyAsync(raw.data(), dout.ptr, (size_t)n * 96, cudaMemcpyDeviceToHost, c->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dev_free(c, dr);
+    dev_free(c, dt);
+    dev_free(c, dout);
+    if (e != cudaSuccess) return fail(HDR_ECUDA, "hdr_trace_rays: %s", cudaGetErrorString(e));
+    for (int32_t k = 0; k < n; ++k) {
+        const float4 *r = &raw[(size_t)k * 6];
+        hdr_gbuffer_texel &o = out[k];
+        int prim, tri, hit;
+        std::memcpy(&prim, &r[1].w, 4);
+        std::memcpy(&tri, &r[2].w, 4);
+        std::memcpy(&hit, &r[3].w, 4);
+        o.position[0] = r[0].x, o.position[1] = r[0].y, o.position[2] = r[0].z, o.depth = r[0].w;
+        o.normal[0] = r[1].x, o.normal[1] = r[1].y, o.normal[2] = r[1].z, o.prim_id = prim;
+        o.smooth_normal[0] = r[2].x, o.smooth_normal[1] = r[2].y, o.smooth_normal[2] = r[2].z, o.tri_id = tri;
+        o.albedo[0] = r[3].x, o.albedo[1] = r[3].y, o.albedo[2] = r[3].z, o.hit = hit;
+        o.uv[0] = r[4].x, o.uv[1] = r[4].y;
+        o.dpdu[0] = r[4].z, o.dpdu[1] = r[4].w, o.dpdu[2] = r[5].x;
+        o.dpdv[0] = r[5].y, o.dpdv[1] = r[5].z, o.dpdv[2] = r[5].w;
+    }
+    return read_device_error(c);
+}
+
+hdr_status hdr_rng_floats(hdr_ctx *c, const uint32_t *seeds, int32_t n_seeds, int32_t count, float *out) {
+    if (!c || n_seeds < 0 || count < 0 || (n_seeds > 0 && (!seeds || !out))) return fail(HDR_EINVAL, "bad argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (n_seeds == 0 || count == 0) return HDR_OK;
+    HDR_CUDA(cudaSetDevice(c->device));
+    DevBuf ds, dout;
+    hdr_status st;
+    if ((st = dev_alloc(c, ds, (size_t)n_seeds * 4)) != HDR_OK) return st;
+    if ((st = dev_alloc(c, dout, (size_t)n_seeds * count * 4)) != HDR_OK) return dev_free(c, ds), st;
+    cudaError_t e = cudaMemcpyAsync(ds.ptr, seeds, (size_t)n_seeds * 4, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        hdr::launch_rng_floats((const uint32_t *)ds.ptr, n_seeds, count, (float *)dout.ptr, c->stream);
+        c->launches += 1;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, dout.ptr, (size_t)n_seeds * count * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dev_free(c, ds);
+    dev_free(c, dout);
+    if (e != cudaSuccess) return fail(HDR_ECUDA, "hdr_rng_floats: %s", cudaGetErrorString(e));
+    return HDR_OK;
+}
+
+hdr_status hdr_pass_times(hdr_ctx *c, float *ms, int32_t n) {
+    if (!c || (!ms && n > 0)) return fail(HDR_EINVAL, "bad argument");
+    for (int i = 0; i < n && i < 3; ++i) ms[i] = c->pass_ms[i];
+    return HDR_OK;
+}
+
+hdr_status hdr_launch_count(hdr_ctx *c, uint64_t *count) {
+    if (!c || !count) return fail(HDR_EINVAL, "bad argument");
+    *count = c->launches;
+    return HDR_OK;
+}
+
+}  // extern "C"

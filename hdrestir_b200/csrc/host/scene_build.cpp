@@ -1,0 +1,445 @@
+// Host-side scene preparation (see scene_build.h for the reference map).
+// Compiled with -ffp-contract=off: the values computed here (centroids,
+// bounds, tangent frames, light frames) must round exactly like the
+// reference's host code.
+#include "scene_build.h"
+
+#include <cmath>
+#include <cstring>
+#include <utility>
+
+namespace hdr {
+
+namespace {
+
+inline float as_float(int i) {
+    float f;
+    std::memcpy(&f, &i, 4);
+    return f;
+}
+
+// Tangent frame and per-triangle data of BVH::Build (bvh.cpp:81-179).
+bool make_triangle(const hdr_mesh_desc &m, int i, BlasTriangle &tri) {
+    const int ntri = m.num_triangles;
+    const int i0 = m.indices[3 * i + 0], i1 = m.indices[3 * i + 1], i2 = m.indices[3 * i + 2];
+    const int np = m.num_points;
+    if (i0 < 0 || i0 >= np || i1 < 0 || i1 >= np || i2 < 0 || i2 >= np) return false;
+    auto P = [&](int k) { return V3{m.points[3 * k], m.points[3 * k + 1], m.points[3 * k + 2]}; };
+    tri.v0 = P(i0);
+    tri.v1 = P(i1);
+    tri.v2 = P(i2);
+
+    if (m.num_uvs > 0) {
+        auto UV = [&](int k) { return V2{m.uvs[2 * k], m.uvs[2 * k + 1]}; };
+        if (m.num_uvs == ntri * 3) {
+            tri.uv0 = UV(i * 3 + 0);
+            tri.uv1 = UV(i * 3 + 1);
+            tri.uv2 = UV(i * 3 + 2);
+        } else {
+            tri.uv0 = (i0 < m.num_uvs) ? UV(i0) : V2{0.0f, 0.0f};
+            tri.uv1 = (i1 < m.num_uvs) ? UV(i1) : V2{0.0f, 0.0f};
+            tri.uv2 = (i2 < m.num_uvs) ? UV(i2) : V2{0.0f, 0.0f};
+        }
+    } else {
+        tri.uv0 = tri.uv1 = tri.uv2 = V2{0.0f, 0.0f};
+    }
+
+    auto N = [&](const float *a, int k) { return V3{a[3 * k], a[3 * k + 1], a[3 * k + 2]}; };
+    if (m.num_normals > 0) {
+        if (m.num_normals == ntri * 3) {
+            tri.n0 = N(m.normals, i * 3 + 0);
+            tri.n1 = N(m.normals, i * 3 + 1);
+            tri.n2 = N(m.normals, i * 3 + 2);
+        } else {
+            const V3 up{0.0f, 1.0f, 0.0f};
+            tri.n0 = (i0 < m.num_normals) ? N(m.normals, i0) : up;
+            tri.n1 = (i1 < m.num_normals) ? N(m.normals, i1) : up;
+            tri.n2 = (i2 < m.num_normals) ? N(m.normals, i2) : up;
+        }
+    } else {
+        tri.n0 = tri.n1 = tri.n2 = V3{0.0f, 0.0f, 0.0f};
+    }
+
+    if (m.num_colors > 0) {
+        if (m.num_colors == ntri * 3) {
+            tri.c0 = N(m.colors, i * 3 + 0);
+            tri.c1 = N(m.colors, i * 3 + 1);
+            tri.c2 = N(m.colors, i * 3 + 2);
+        } else {
+            const V3 one{1.0f, 1.0f, 1.0f};
+            tri.c0 = (i0 < m.num_colors) ? N(m.colors, i0) : one;
+            tri.c1 = (i1 < m.num_colors) ? N(m.colors, i1) : one;
+            tri.c2 = (i2 < m.num_colors) ? N(m.colors, i2) : one;
+        }
+    } else {
+        tri.c0 = tri.c1 = tri.c2 = V3{1.0f, 1.0f, 1.0f};
+    }
+
+    const V3 edge1 = tri.v1 - tri.v0;
+    const V3 edge2 = tri.v2 - tri.v0;
+    const V2 duv1{tri.uv1.x - tri.uv0.x, tri.uv1.y - tri.uv0.y};
+    const V2 duv2{tri.uv2.x - tri.uv0.x, tri.uv2.y - tri.uv0.y};
+    float f = duv1.x * duv2.y - duv2.x * duv1.y;
+    if (std::abs(f) > 1e-8f) {
+        f = 1.0f / f;
+        tri.dpdu = (edge1 * duv2.y - edge2 * duv1.y) * f;
+        tri.dpdv = (edge2 * duv1.x - edge1 * duv2.x) * f;
+        tri.dpdu = normalized(tri.dpdu);
+        tri.dpdv = normalized(tri.dpdv);
+    } else {
+        const V3 n = normalized(cross(edge1, edge2));
+        const V3 up = std::abs(n.y) < 0.999f ? V3{0, 1, 0} : V3{1, 0, 0};
+        tri.dpdu = normalized(cross(up, n));
+        tri.dpdv = normalized(cross(n, tri.dpdu));
+    }
+    tri.material = (i < m.num_material_indices && m.material_indices) ? m.material_indices[i] : -1;
+    tri.centroid = div_d(tri.v0 + tri.v1 + tri.v2, 3.0);
+    return true;
+}
+
+struct BlasBuilder {
+    Blas &b;
+    void subdivide(int node_idx, int start, int end, int depth) {
+        if (depth > b.max_depth) b.max_depth = depth;
+        BlasNode &node = b.nodes[node_idx];
+        node.bounds.set_empty();
+        for (int i = start; i < end; ++i) {
+            node.bounds.extend(b.tris[i].v0);
+            node.bounds.extend(b.tris[i].v1);
+            node.bounds.extend(b.tris[i].v2);
+        }
+        const int count = end - start;
+        if (count <= 4) {
+            node.left = -start - 1;
+            node.count = count;
+            return;
+        }
+        const V3 size = node.bounds.size();
+        int axis = 0;
+        if (size.y > size.x) axis = 1;
+        if (comp(size, 2) > comp(size, axis)) axis = 2;
+        const float split = comp(node.bounds.mn, axis) + comp(size, axis) * 0.5f;
+        int i = start, j = end - 1;
+        while (i <= j) {
+            if (comp(b.tris[i].centroid, axis) < split) {
+                i++;
+            } else {
+                std::swap(b.tris[i], b.tris[j]);
+                j--;
+            }
+        }
+        const int left_count = i - start;
+        if (left_count == 0 || left_count == count) i = start + count / 2;
+        const int left_idx = (int)b.nodes.size();
+        b.nodes.push_back(BlasNode());
+        b.nodes.push_back(BlasNode());
+        b.nodes[node_idx].left = left_idx;
+        b.nodes[node_idx].count = 0;
+        subdivide(left_idx, start, i, depth + 1);
+        subdivide(left_idx + 1, i, end, depth + 1);
+    }
+};
+
+struct TlasBuilder {
+    std::vector<TlasNode> &nodes;
+    std::vector<int> &idx;
+    const std::vector<HostInstance> &inst;
+    int max_depth = 0;
+    void subdivide(int node_idx, int start, int end, int depth) {
+        if (depth > max_depth) max_depth = depth;
+        const int left_idx = (int)nodes.size();
+        nodes.push_back(TlasNode{});
+        nodes.push_back(TlasNode{});
+        nodes[node_idx].left = left_idx;
+        nodes[node_idx].count = 0;
+        nodes[node_idx].bounds.set_empty();
+        for (int i = start; i < end; ++i) {
+            const Range3 &bb = inst[idx[i]].bounds;
+            nodes[node_idx].bounds.extend(bb.mn);
+            nodes[node_idx].bounds.extend(bb.mx);
+        }
+        const int count = end - start;
+        if (count <= 2) {
+            nodes[node_idx].left = -start - 1;
+            nodes[node_idx].count = count;
+            return;
+        }
+        const V3 size = nodes[node_idx].bounds.size();
+        int axis = 0;
+        if (size.y > size.x) axis = 1;
+        if (comp(size, 2) > comp(size, axis)) axis = 2;
+        const float split = comp(nodes[node_idx].bounds.mn, axis) + comp(size, axis) * 0.5f;
+        int i = start, j = end - 1;
+        while (i <= j) {
+            if (comp(inst[idx[i]].centroid, axis) < split) {
+                ++i;
+            } else {
+                std::swap(idx[i], idx[j]);
+                --j;
+            }
+        }
+        if (i == start || i == end) i = start + count / 2;
+        subdivide(left_idx, start, i, depth + 1);
+        subdivide(left_idx + 1, i, end, depth + 1);
+    }
+};
+
+// Scene::_TransformBounds (scene.cpp:101-116)
+Range3 transform_bounds(const Range3 &b, const float *m) {
+    if (b.empty()) return b;
+    const V3 mn = b.mn, mx = b.mx;
+    const V3 corners[8] = {{mn.x, mn.y, mn.z}, {mx.x, mn.y, mn.z}, {mn.x, mx.y, mn.z}, {mx.x, mx.y, mn.z},
+                           {mn.x, mn.y, mx.z}, {mx.x, mn.y, mx.z}, {mn.x, mx.y, mx.z}, {mx.x, mx.y, mx.z}};
+    Range3 r;
+    for (const V3 &c : corners) r.extend(m4f_transform(m, c));
+    return r;
+}
+
+void put_node(std::vector<float> &dst, const Range3 &r, int left, int count) {
+    const float rec[8] = {r.mn.x, r.mn.y, r.mn.z, as_float(left), r.mx.x, r.mx.y, r.mx.z, as_float(count)};
+    dst.insert(dst.end(), rec, rec + 8);
+}
+
+}  // namespace
+
+void gf_inverse4d(const double *m, double *out) {
+    const double s0 = m[0] * m[5] - m[4] * m[1];
+    const double s1 = m[0] * m[6] - m[4] * m[2];
+    const double s2 = m[0] * m[7] - m[4] * m[3];
+    const double s3 = m[1] * m[6] - m[5] * m[2];
+    const double s4 = m[1] * m[7] - m[5] * m[3];
+    const double s5 = m[2] * m[7] - m[6] * m[3];
+    const double c5 = m[10] * m[15] - m[14] * m[11];
+    const double c4 = m[9] * m[15] - m[13] * m[11];
+    const double c3 = m[9] * m[14] - m[13] * m[10];
+    const double c2 = m[8] * m[15] - m[12] * m[11];
+    const double c1 = m[8] * m[14] - m[12] * m[10];
+    const double c0 = m[8] * m[13] - m[12] * m[9];
+    const double det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+    if (!(std::fabs(det) > 0.0)) {
+        for (int i = 0; i < 16; ++i) out[i] = 0.0;
+        out[0] = out[5] = out[10] = 3.402823466e+38;
+        out[15] = 1.0;
+        return;
+    }
+    const double r = 1.0 / det;
+    out[0] = (m[5] * c5 - m[6] * c4 + m[7] * c3) * r;
+    out[1] = (-m[1] * c5 + m[2] * c4 - m[3] * c3) * r;
+    out[2] = (m[13] * s5 - m[14] * s4 + m[15] * s3) * r;
+    out[3] = (-m[9] * s5 + m[10] * s4 - m[11] * s3) * r;
+    out[4] = (-m[4] * c5 + m[6] * c2 - m[7] * c1) * r;
+    out[5] = (m[0] * c5 - m[2] * c2 + m[3] * c1) * r;
+    out[6] = (-m[12] * s5 + m[14] * s2 - m[15] * s1) * r;
+    out[7] = (m[8] * s5 - m[10] * s2 + m[11] * s1) * r;
+    out[8] = (m[4] * c4 - m[5] * c2 + m[7] * c0) * r;
+    out[9] = (-m[0] * c4 + m[1] * c2 - m[3] * c0) * r;
+    out[10] = (m[12] * s4 - m[13] * s2 + m[15] * s0) * r;
+    out[11] = (-m[8] * s4 + m[9] * s2 - m[11] * s0) * r;
+    out[12] = (-m[4] * c3 + m[5] * c1 - m[6] * c0) * r;
+    out[13] = (m[0] * c3 - m[1] * c1 + m[2] * c0) * r;
+    out[14] = (-m[12] * s3 + m[13] * s1 - m[14] * s0) * r;
+    out[15] = (m[8] * s3 - m[9] * s1 + m[10] * s0) * r;
+}
+
+void gf_inverse4f(const float *m, float *out) {
+    double md[16], od[16];
+    for (int i = 0; i < 16; ++i) md[i] = (double)m[i];
+    gf_inverse4d(md, od);
+    for (int i = 0; i < 16; ++i) out[i] = (float)od[i];
+}
+
+Blas build_blas(const hdr_mesh_desc &m) {
+    Blas b;
+    // MeshSubset::range over the referenced points (hd_restir_mesh.cpp:523-529)
+    for (int i = 0; i < m.num_triangles; ++i) {
+        for (int k = 0; k < 3; ++k) {
+            const int p = m.indices[3 * i + k];
+            if (p >= 0 && p < m.num_points) b.range.extend(V3{m.points[3 * p], m.points[3 * p + 1], m.points[3 * p + 2]});
+        }
+    }
+    if (m.num_triangles <= 0 || m.num_points <= 0) return b;
+    b.tris.reserve((size_t)m.num_triangles);
+    for (int i = 0; i < m.num_triangles; ++i) {
+        BlasTriangle t;
+        if (make_triangle(m, i, t)) b.tris.push_back(t);
+    }
+    if (b.tris.empty()) return b;
+    b.nodes.reserve((size_t)m.num_triangles * 2);
+    b.nodes.push_back(BlasNode());
+    BlasBuilder bb{b};
+    bb.subdivide(0, 0, (int)b.tris.size(), 1);
+    return b;
+}
+
+bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &err) {
+    out = FlatScene{};
+    if (desc.num_meshes < 0 || desc.num_instances < 0 || desc.num_materials < 0 || desc.num_lights < 0) {
+        err = "negative count in hdr_scene_desc";
+        return false;
+    }
+    // ---- BLAS per mesh
+    std::vector<int> node_base(desc.num_meshes), tri_base(desc.num_meshes), blas_ok(desc.num_meshes);
+    std::vector<Range3> ranges(desc.num_meshes);
+    for (int mi = 0; mi < desc.num_meshes; ++mi) {
+        const hdr_mesh_desc &m = desc.meshes[mi];
+        if ((m.num_points > 0 && !m.points) || (m.num_triangles > 0 && !m.indices) || (m.num_uvs > 0 && !m.uvs) ||
+            (m.num_normals > 0 && !m.normals) || (m.num_colors > 0 && !m.colors)) {
+            err = "mesh " + std::to_string(mi) + ": NULL array with non-zero count";
+            return false;
+        }
+        Blas b = build_blas(m);
+        ranges[mi] = b.range;
+        node_base[mi] = (int)out.num_blas_nodes;
+        tri_base[mi] = (int)out.num_triangles;
+        blas_ok[mi] = b.nodes.empty() ? 0 : 1;
+        if (b.max_depth > out.max_blas_depth) out.max_blas_depth = b.max_depth;
+        for (const BlasNode &n : b.nodes) put_node(out.blas_nodes, n.bounds, n.left, n.count);
+        for (const BlasTriangle &t : b.tris) {
+            const V3 e1 = t.v1 - t.v0, e2 = t.v2 - t.v0;
+            const float g[12] = {t.v0.x, t.v0.y, t.v0.z, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z, 0.0f, 0.0f, 0.0f};
+            out.tri_geo.insert(out.tri_geo.end(), g, g + 12);
+            // geometric normal of bvh.cpp:277 and the smooth-normal switch of bvh.cpp:281
+            const V3 ng = normalized(cross(t.v1 - t.v0, t.v2 - t.v0));
+            const float smooth = (length_sq(t.n0) > 1e-6f) ? 1.0f : 0.0f;
+            const float a[36] = {ng.x,     ng.y,     ng.z,     smooth,   t.n0.x,  t.n0.y,  t.n0.z,  t.uv0.x,  t.n1.x,
+                                 t.n1.y,   t.n1.z,   t.uv0.y,  t.n2.x,   t.n2.y,  t.n2.z,  t.uv1.x, t.c0.x,   t.c0.y,
+                                 t.c0.z,   t.uv1.y,  t.c1.x,   t.c1.y,   t.c1.z,  t.uv2.x, t.c2.x,  t.c2.y,   t.c2.z,
+                                 t.uv2.y,  t.dpdu.x, t.dpdu.y, t.dpdu.z, as_float(t.material), t.dpdv.x, t.dpdv.y,
+                                 t.dpdv.z, 0.0f};
+            out.tri_attr.insert(out.tri_attr.end(), a, a + 36);
+        }
+        out.num_blas_nodes += b.nodes.size();
+        out.num_triangles += b.tris.size();
+    }
+    // ---- instances (appendMeshInstance, scene.cpp:187-222)
+    std::vector<HostInstance> inst((size_t)desc.num_instances);
+    for (int ii = 0; ii < desc.num_instances; ++ii) {
+        const hdr_instance_desc &d = desc.instances[ii];
+        if (d.mesh < 0 || d.mesh >= desc.num_meshes) {
+            err = "instance " + std::to_string(ii) + ": mesh index out of range";
+            return false;
+        }
+        if (d.material < -1 || d.material >= desc.num_materials || d.light < -1 || d.light >= desc.num_lights) {
+            err = "instance " + std::to_string(ii) + ": material/light index out of range";
+            return false;
+        }
+        HostInstance &h = inst[ii];
+        h.mesh = d.mesh;
+        h.material = d.material;
+        h.light = d.light;
+        std::memcpy(h.xf, d.transform, sizeof(h.xf));
+        gf_inverse4f(h.xf, h.inv);
+        h.bounds = transform_bounds(ranges[d.mesh], h.xf);
+        h.centroid = (h.bounds.mn + h.bounds.mx) * 0.5f;
+        float rec[32];
+        std::memcpy(rec, h.inv, sizeof(h.inv));
+        const float *T = h.xf;
+        const float r4[16] = {T[0], T[1], T[2], as_float(node_base[d.mesh]), T[4], T[5], T[6], as_float(tri_base[d.mesh]),
+                              T[8], T[9], T[10], as_float(d.material), as_float(d.light), as_float(blas_ok[d.mesh]),
+                              0.0f, 0.0f};
+        std::memcpy(rec + 16, r4, sizeof(r4));
+        out.instances.insert(out.instances.end(), rec, rec + 32);
+    }
+    out.num_instances = desc.num_instances;
+    // ---- TLAS (scene.cpp:333-407)
+    if (desc.num_instances > 0) {
+        std::vector<TlasNode> nodes;
+        std::vector<int> idx((size_t)desc.num_instances);
+        for (int i = 0; i < desc.num_instances; ++i) idx[i] = i;
+        nodes.reserve((size_t)desc.num_instances * 2);
+        nodes.push_back(TlasNode{});
+        TlasBuilder tb{nodes, idx, inst};
+        tb.subdivide(0, 0, desc.num_instances, 1);
+        out.max_tlas_depth = tb.max_depth;
+        for (const TlasNode &n : nodes) put_node(out.tlas_nodes, n.bounds, n.left, n.count);
+        out.tlas_inst = idx;
+    }
+    // ---- materials: PreviewSurfaceMaterial::GetClosure inputs (preview_surface.cpp:61-127)
+    out.num_materials = desc.num_materials;
+    out.materials.assign((size_t)desc.num_materials * kMaterialFloats, 0.0f);
+    for (int i = 0; i < desc.num_materials; ++i) {
+        const hdr_material_desc &p = desc.materials[i];
+        float *r = &out.materials[(size_t)i * kMaterialFloats];
+        const V3 emission = V3{p.emission_color[0], p.emission_color[1], p.emission_color[2]} * p.emission;
+        const float v[40] = {p.diffuse_color[0], p.diffuse_color[1], p.diffuse_color[2], p.metallic,
+                             p.specular_color[0], p.specular_color[1], p.specular_color[2], p.specular,
+                             emission.x, emission.y, emission.z, std::max(0.001f, p.roughness),
+                             p.transmission_color[0], p.transmission_color[1], p.transmission_color[2], p.transmission,
+                             p.coat_color[0], p.coat_color[1], p.coat_color[2], p.coat,
+                             p.sheen_color[0], p.sheen_color[1], p.sheen_color[2], p.sheen,
+                             p.subsurface_color[0], p.subsurface_color[1], p.subsurface_color[2], p.subsurface,
+                             p.ior, p.opacity, p.transmission_depth, as_float(p.thin_walled),
+                             p.coat_roughness, p.coat_ior, p.sheen_roughness, p.roughness,
+                             0.0f, 0.0f, 0.0f, 0.0f};
+        std::memcpy(r, v, sizeof(v));
+    }
+    // ---- lights (rect_light.cpp, point_light.cpp, distant_light.cpp, dome_light.cpp)
+    out.num_lights = desc.num_lights;
+    out.lights.assign((size_t)desc.num_lights * kLightFloats, 0.0f);
+    for (int i = 0; i < desc.num_lights; ++i) {
+        const hdr_light_desc &L = desc.lights[i];
+        if (L.type < HDR_LIGHT_DISTANT || L.type > HDR_LIGHT_POINT) {
+            err = "light " + std::to_string(i) + ": unknown type";
+            return false;
+        }
+        float *r = &out.lights[(size_t)i * kLightFloats];
+        float M[16];
+        for (int k = 0; k < 16; ++k) M[k] = (float)L.transform[k];  // GfMatrix4f(GfMatrix4d)
+        const float eff = L.intensity * std::exp2(L.exposure);       // LightParams::EffectiveIntensity
+        const V3 color = V3{L.color[0], L.color[1], L.color[2]} * eff;
+        const V3 lnormal = normalized(m4f_transform_dir(M, V3{0.0f, 0.0f, -1.0f}));
+        const float area = L.width * L.height;
+        const float cone_rad = L.shaping_cone_angle * (float)(3.14159265358979323846 / 180.0);
+        const float cos_cone = std::cos(cone_rad);
+        const float cos_inner = std::cos(cone_rad * (1.0f - L.shaping_cone_softness));
+        const int is_delta = (L.type == HDR_LIGHT_POINT || L.type == HDR_LIGHT_DISTANT) ? 1 : 0;
+        const float head[16] = {as_float(L.type), as_float(is_delta), L.width, L.height,
+                                color.x, color.y, color.z, area,
+                                lnormal.x, lnormal.y, lnormal.z, L.shaping_cone_angle,
+                                cos_cone, cos_inner, L.shaping_cone_softness, 0.0f};
+        std::memcpy(r, head, sizeof(head));
+        std::memcpy(r + 16, M, sizeof(M));
+        // light params color & intensity kept separately for the dome's CompMult
+        r[32] = L.color[0];
+        r[33] = L.color[1];
+        r[34] = L.color[2];
+        r[35] = eff;
+        if (L.type == HDR_LIGHT_DOME) {
+            if (out.env_light < 0) out.env_light = i;
+            if (L.texture && L.tex_width > 0 && L.tex_height > 0 && out.dome_width == 0) {
+                // DomeLight::Prepare (dome_light.cpp:21-83)
+                const int W = L.tex_width, H = L.tex_height;
+                out.dome_width = W;
+                out.dome_height = H;
+                out.dome_pixels.assign(L.texture, L.texture + (size_t)W * H * 3);
+                std::vector<float> &row = out.dome_row_cdf;
+                std::vector<float> &col = out.dome_col_cdf;
+                row.assign((size_t)H + 1, 0.0f);
+                col.assign((size_t)H * (W + 1), 0.0f);
+                const float *px = out.dome_pixels.data();
+                float total = 0.0f;
+                for (int y = 0; y < H; ++y) {
+                    float row_lum = 0.0f;
+                    const float sin_theta = std::sin(3.14159265358979323846 * (float)(y + 0.5f) / (float)H);
+                    for (int x = 0; x < W; ++x) {
+                        const size_t idx = (size_t)(y * W + x) * 3;
+                        float lum = 0.2126f * px[idx] + 0.7152f * px[idx + 1] + 0.0722f * px[idx + 2];
+                        lum *= sin_theta;
+                        row_lum += lum;
+                        col[(size_t)y * (W + 1) + x + 1] = col[(size_t)y * (W + 1) + x] + lum;
+                    }
+                    if (row_lum > 0)
+                        for (int x = 0; x <= W; ++x) col[(size_t)y * (W + 1) + x] /= row_lum;
+                    total += row_lum;
+                    row[y + 1] = row[y] + row_lum;
+                }
+                if (total > 0)
+                    for (int y = 0; y <= H; ++y) row[y] /= total;
+                out.dome_total_lum = total;
+            }
+        }
+    }
+    return true;
+}
+
+}  // namespace hdr

@@ -1,0 +1,288 @@
+/*
+ * hdrestir.h — C ABI of the B200 (sm_100a) light-transport passes.
+ *
+ * The reference renderer (hdRestir) runs its per-pixel light transport as CPU
+ * RenderPasses behind `RenderPass::Execute/_execute` (source/passes/render_pass.h:13-42).
+ * Its only GPU boundary is pass-granular too (GpuAccumulationPass,
+ * source/gpu_passes/gpu_accumulation_pass.h). This header is the same boundary
+ * for every pass on the hot path: plain C, plain pointers and sizes, no C++ or
+ * torch types, integer status codes and a thread-local error string. A pass
+ * wrapper on the host (C++ RenderPass subclass, ctypes, cgo, …) forwards its
+ * `_execute(RenderContext&)` to one call here; device buffers keep the
+ * reference's frame-buffer names ("GBuffer", "Color", "__accum_color",
+ * "__ris_reservoir", …; source/passes/output_names.h:10-40,
+ * source/restir/output_names.h:10) and stay resident on the GPU between frames.
+ *
+ * Threading: one hdr_ctx per pipeline instance; calls on one ctx are
+ * serialised by an internal mutex and run on the ctx's own CUDA stream.
+ * Errors never throw across the ABI.
+ */
+#ifndef HDRESTIR_B200_H
+#define HDRESTIR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HDR_ABI_VERSION 1
+
+/* Status codes. The reference reports failures with exceptions
+ * (gpu_accumulation_kernel.cpp:63-109) and DBG_ASSERT/Expects; across this ABI
+ * they become integers plus hdr_last_error(). */
+typedef enum hdr_status {
+    HDR_OK = 0,
+    HDR_EINVAL = 1,      /* bad argument, size or name */
+    HDR_ENOMEM = 2,      /* device or host allocation failed, or HBM budget exceeded */
+    HDR_ECANCELLED = 3,  /* the cancel word was set (IRenderJob::IsCancelled, render_job.h:9-37) */
+    HDR_ETIMEOUT = 4,    /* a bounded device wait gave up */
+    HDR_ECUDA = 5,       /* a CUDA runtime call failed */
+    HDR_ENOSCENE = 6,    /* pass called before hdr_scene_upload */
+    HDR_EDEVICE = 7      /* a kernel reported an internal limit (e.g. traversal stack) */
+} hdr_status;
+
+typedef struct hdr_ctx hdr_ctx;
+
+/* ---------------------------------------------------------------------------
+ * Scene description (host memory, copied at upload).
+ * Mirrors what Scene::BuildRenderState consumes (scene/scene.cpp:118-271):
+ * mesh subsets (one BLAS each, BVH::Build inputs, renderContext/bvh.h:44-45),
+ * instances (appendMeshInstance, scene.cpp:187-222), PreviewSurface params
+ * (materials/preview_surface_params.h:12-52) and lights
+ * (sceneInterface/scene_interface.h:24-29, light_params.h).
+ * ------------------------------------------------------------------------- */
+typedef struct hdr_mesh_desc {
+    const float *points;          /* xyz per point */
+    int32_t num_points;
+    const int32_t *indices;       /* 3 point indices per triangle */
+    int32_t num_triangles;
+    const float *uvs;             /* 2 per entry; per corner when num_uvs == 3*num_triangles, else per point */
+    int32_t num_uvs;
+    const float *normals;         /* 3 per entry; same per-corner/per-point rule */
+    int32_t num_normals;
+    const float *colors;          /* 3 per entry; same rule */
+    int32_t num_colors;
+    const int32_t *material_indices; /* per triangle (BVHTriangle::materialIndex), may be NULL */
+    int32_t num_material_indices;
+} hdr_mesh_desc;
+
+typedef struct hdr_instance_desc {
+    int32_t mesh;        /* index into hdr_scene_desc.meshes */
+    int32_t material;    /* index into materials, -1 = DefaultMaterial (default_material.cpp:55-64) */
+    int32_t light;       /* light whose geometry this instance is (Scene::GetLightAtHit), -1 = none */
+    int32_t reserved;
+    float transform[16]; /* GfMatrix4f, row-major, row-vector convention (translation in row 3) */
+} hdr_instance_desc;
+
+typedef struct hdr_material_desc { /* PreviewSurfaceParams field for field */
+    float diffuse_color[3];
+    float metallic;
+    float roughness;
+    float specular_color[3];
+    float specular;
+    float opacity;
+    float ior;
+    float transmission;
+    float transmission_color[3];
+    float transmission_depth;
+    float transmission_scatter[3];
+    float emission_color[3];
+    float emission;
+    float coat;
+    float coat_color[3];
+    float coat_roughness;
+    float coat_ior;
+    float sheen;
+    float sheen_color[3];
+    float sheen_roughness;
+    float subsurface;
+    float subsurface_color[3];
+    float subsurface_radius[3];
+    float subsurface_scale;
+    float subsurface_anisotropy;
+    int32_t thin_walled;
+    float diffuse_roughness;
+} hdr_material_desc;
+
+/* LightType order of scene/light_factory.h */
+enum { HDR_LIGHT_DISTANT = 0, HDR_LIGHT_DOME = 1, HDR_LIGHT_RECT = 2, HDR_LIGHT_POINT = 3 };
+
+typedef struct hdr_light_desc {
+    int32_t type;
+    float color[3];
+    float intensity;
+    float exposure;
+    double transform[16];        /* GfMatrix4d row-major */
+    float width, height;
+    float shaping_cone_angle;    /* degrees, 180 = no cone */
+    float shaping_cone_softness;
+    const float *texture;        /* dome: RGB f32, tex_width*tex_height*3 (the decoded TextureFile) */
+    int32_t tex_width, tex_height;
+} hdr_light_desc;
+
+typedef struct hdr_scene_desc {
+    const hdr_mesh_desc *meshes;
+    int32_t num_meshes;
+    const hdr_instance_desc *instances;
+    int32_t num_instances;
+    const hdr_material_desc *materials;
+    int32_t num_materials;
+    const hdr_light_desc *lights;
+    int32_t num_lights;
+} hdr_scene_desc;
+
+/* ---------------------------------------------------------------------------
+ * Per-frame inputs
+ * ------------------------------------------------------------------------- */
+typedef struct hdr_camera {
+    double view[16];             /* RenderContext::viewMatrix (GfMatrix4d row-major) */
+    double proj[16];             /* RenderContext::projMatrix */
+    int32_t width, height;       /* CameraFrame::RenderedWidth/Height */
+    int32_t has_params;          /* RenderContext::cameraParams engaged (else pinhole) */
+    int32_t enable_dof;          /* CameraParams (scene/camera_params.h:8-20) */
+    int32_t enable_exposure;
+    float focal_length;
+    float f_stop;
+    float focus_distance;
+    int32_t bokeh_blades;
+    float lens_distortion;
+    float iso;
+    float shutter_speed;
+} hdr_camera;
+
+/* PathTracePassSettings (integrators/path_integrator.h:12-19) + maxDepth */
+typedef struct hdr_path_settings {
+    int32_t max_depth;
+    int32_t enable_subsurface;
+    int32_t max_reflection_bounces;
+    int32_t max_refraction_bounces;
+    int32_t render_ibl_background;
+    float roulette_aggressiveness;
+} hdr_path_settings;
+
+/* RisDirectLightIntegrator::MakeFactory(candidateCount, useReservoir, skipVisibility)
+ * (restir/ris_direct_light_integrator.h:73-74). The fields after skip_visibility
+ * are extensions with no reference counterpart; zero keeps reference behaviour. */
+typedef struct hdr_ris_params {
+    hdr_path_settings path;
+    int32_t candidate_count;
+    int32_t use_reservoir;
+    int32_t skip_visibility;
+    int32_t m_cap;               /* 0 = unbounded CandidateCount (reservoir.h:147-155) */
+    int32_t spatial_neighbors;   /* 0 = temporal-only, same-pixel reuse */
+    float spatial_radius;
+    int32_t reserved[2];
+} hdr_ris_params;
+
+/* AOV selection for hdr_raycast (RaycastPass requestedOutputs, raycast_pass.cpp:39-55) */
+enum { HDR_AOV_DEPTH = 1, HDR_AOV_ALBEDO = 2, HDR_AOV_NORMAL = 4 };
+
+/* Accumulation firefly semantics. PARITY reproduces AccumulationPass's in-place
+ * row-major clamp (accumulation_pass.cpp:22-60); SHADER reproduces
+ * accumulation.slang:55-81, which clamps against the unclamped input. */
+enum { HDR_ACCUM_PARITY = 0, HDR_ACCUM_SHADER = 1 };
+
+/* Device GBuffer texel returned by hdr_download("GBuffer"): the fields of
+ * std::optional<HitRecord> (core/hit_record.h:15-27) plus the triangle index. */
+typedef struct hdr_gbuffer_texel {
+    float position[3];
+    float depth;
+    float normal[3];
+    int32_t prim_id;             /* == MatId == instance index (scene.cpp:531-533) */
+    float smooth_normal[3];
+    int32_t tri_id;              /* BLAS triangle index (new field, -1 on miss) */
+    float albedo[3];
+    int32_t hit;                 /* optional engaged */
+    float uv[2];
+    float dpdu[3];
+    float dpdv[3];
+} hdr_gbuffer_texel;
+
+/* ---------------------------------------------------------------------------
+ * Context
+ * ------------------------------------------------------------------------- */
+typedef struct hdr_ctx_desc {
+    int32_t device;              /* CUDA ordinal */
+    uint32_t flags;              /* bit 0: record per-pass CUDA-event timings */
+    size_t hbm_budget_bytes;     /* 0 = unlimited; allocations past it fail with HDR_ENOMEM */
+} hdr_ctx_desc;
+
+/* Replaces the LightRHI device/kernel setup of Gpu::AccumulationKernel
+ * (gpu_functions/gpu_accumulation_kernel.cpp:63-192) for all passes. */
+hdr_status hdr_ctx_create(hdr_ctx **out, const hdr_ctx_desc *desc);
+void hdr_ctx_destroy(hdr_ctx *ctx);
+int hdr_abi_version(void);
+/* Thread-local text of the last failure on this thread ("" if none). */
+const char *hdr_last_error(void);
+
+/* Uploads and builds the device scene: BLAS per mesh (BVH::Build,
+ * renderContext/bvh.cpp:66-241), instances and TLAS (Scene::_BuildTLAS,
+ * scene/scene.cpp:333-407), materials, lights, dome CDF (DomeLight::Prepare,
+ * scene/dome_light.cpp:21-83). Replaces the per-frame Scene::BuildRenderState:
+ * the scene stays resident until the next upload. */
+hdr_status hdr_scene_upload(hdr_ctx *ctx, const hdr_scene_desc *scene);
+
+/* RaycastPass::_execute (passes/raycast_pass.cpp:57-162): GBuffer (+AOVs). */
+hdr_status hdr_raycast(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_index, uint32_t aov_mask);
+
+/* RISPathTracePass (restir_passes/ris_path_trace_pass.h:12-28) = IntegrationPass::_execute
+ * (passes/integration_pass.cpp:157-252) with PathIntegrator + RisDirectLightIntegrator:
+ * reads GBuffer and "__ris_reservoir", writes "Color" and the reservoirs. */
+hdr_status hdr_ris_path_trace(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_index,
+                              const hdr_ris_params *params);
+
+/* PathTracePass (passes/path_trace_pass.h:12-39) with MisDirectLightIntegrator. */
+hdr_status hdr_path_trace(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_index,
+                          const hdr_path_settings *settings);
+
+/* AccumulationPass::_execute (passes/accumulation_pass.cpp:64-139) and
+ * GpuAccumulationPass (accumulation.slang:39-97): optional firefly clamp,
+ * "__accum_color" += "Color", "Color" = accum / (frame_index+1). */
+hdr_status hdr_accumulate(hdr_ctx *ctx, int32_t frame_index, int32_t firefly, int32_t mode);
+
+/* RenderPipeline::ClearPersistentBuffers (pipeline/render_pipeline.cpp:42-45):
+ * zeroes "__accum_color" and "__ris_reservoir". */
+hdr_status hdr_clear_persistent(hdr_ctx *ctx);
+
+/* Copies a named device buffer to host memory (bytes must equal the buffer size,
+ * query it with hdr_buffer_size). Names: "GBuffer" (hdr_gbuffer_texel),
+ * "Color" (RGBA f32), "Depth" (f32), "Albedo"/"Normal" (RGB f32),
+ * "__accum_color" (RGBA f32), "__ris_reservoir" (see DESIGN.md layout). */
+hdr_status hdr_download(hdr_ctx *ctx, const char *name, void *dst, size_t bytes);
+hdr_status hdr_upload(hdr_ctx *ctx, const char *name, const void *src, size_t bytes);
+hdr_status hdr_buffer_size(hdr_ctx *ctx, const char *name, size_t *bytes);
+
+/* Waits for all work queued on the ctx stream. */
+hdr_status hdr_synchronize(hdr_ctx *ctx);
+
+/* Host-visible cancel word polled between launches and by long device loops
+ * (the IRenderJob::IsCancelled poll of scene.cpp:422-423). NULL detaches. */
+hdr_status hdr_set_cancel(hdr_ctx *ctx, const volatile int32_t *flag);
+
+/* Scene::IntersectScene (scene.cpp:515-535) on caller rays: rays = n x
+ * (ox,oy,oz,dx,dy,dz) f32 host array; out = n x hdr_gbuffer_texel.
+ * any_hit != 0: only depth/hit are meaningful and traversal stops at the first
+ * hit closer than the per-ray limit tmax (NULL = +inf). */
+hdr_status hdr_trace_rays(hdr_ctx *ctx, const float *rays, const float *tmax, int32_t n,
+                          int32_t any_hit, hdr_gbuffer_texel *out);
+
+/* Restir::Rng (core/rng.h:10-56) on the device: for each seed, the first
+ * `count` NextFloat() values of std::mt19937_64(seed) mapped through
+ * uniform_real_distribution<float>. out = n_seeds x count floats. */
+hdr_status hdr_rng_floats(hdr_ctx *ctx, const uint32_t *seeds, int32_t n_seeds, int32_t count,
+                          float *out);
+
+/* Per-pass device times (ms) of the last call of each pass, measured with CUDA
+ * events on the ctx stream when flag bit 0 is set:
+ * [0] raycast, [1] integrate, [2] accumulate. */
+hdr_status hdr_pass_times(hdr_ctx *ctx, float *ms, int32_t n);
+
+/* Number of this library's kernels launched on the ctx so far. */
+hdr_status hdr_launch_count(hdr_ctx *ctx, uint64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HDRESTIR_B200_H */

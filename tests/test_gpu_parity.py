@@ -1,0 +1,134 @@
+"""Parity of the CUDA passes (through the C ABI) with the CPU oracle.
+
+Integer / index / hit results must be bit-identical (closest-hit instance and
+triangle, hit distance bits, RNG streams, reservoir candidate counts M).
+Radiance goes through expf/powf/sinf/cosf, which CUDA and glibc round
+differently by a few ulp, so colours are compared with a relative tolerance
+on the pixels, plus a bound on the fraction of pixels allowed to differ more
+(a ulp-level direction change can move a secondary ray across an edge).
+"""
+import numpy as np
+import pytest
+
+from hdrestir_b200 import configs
+from oracle.oracle import Oracle, rng_floats
+
+pytestmark = pytest.mark.gpu
+
+SMALL = {
+    0: dict(width=64, height=48),
+    1: dict(width=64, height=48, n_lights=128),
+    2: dict(width=64, height=48, grid=96, n_spheres=60, n_lights=300),
+}
+RTOL = 1e-4          # per-pixel relative tolerance on RGB (north-star: 1e-4 relative)
+ATOL = 1e-6
+MAX_OUTLIERS = 0.01  # fraction of pixels allowed outside the tolerance
+
+
+def _scene(cfg):
+    kw = dict(SMALL[cfg])
+    return configs.small_variant(cfg, **kw)
+
+
+def _color_outliers(a, b):
+    a = a[:, :3].astype(np.float64)
+    b = b[:, :3].astype(np.float64)
+    bad = np.abs(a - b) > (ATOL + RTOL * np.maximum(np.abs(a), np.abs(b)))
+    return bad.any(1).mean()
+
+
+def test_rng_streams_bit_exact(gpu_ctx):
+    seeds = np.array([0, 1, 7, 1234 ^ 56, 0xFFFFFFFF, 0xC0FFEE00] + list(range(100, 160)), np.uint32)
+    dev = gpu_ctx.rng_floats(seeds, 700)  # crosses the 156 / 311 / 312 cursor boundaries
+    ref = rng_floats(seeds, 700)
+    assert np.array_equal(dev.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.parametrize("cfg", [0, 1, 2])
+def test_raycast_gbuffer_bit_exact(gpu_ctx, cfg):
+    sc, cam = _scene(cfg)
+    gpu_ctx.upload_scene(sc)
+    gpu_ctx.raycast(cam, 0, aovs=("Depth", "Albedo", "Normal"))
+    g = gpu_ctx.download("GBuffer")
+    o = Oracle(sc).raycast(cam, 0)
+    assert g["hit"].sum() > 0
+    assert np.array_equal(g["prim_id"], o["prim_id"])
+    assert np.array_equal(g["tri_id"], o["tri_id"])
+    for f in ("position", "depth", "normal", "smooth_normal", "albedo", "uv", "dpdu", "dpdv"):
+        hit = o["hit"] == 1
+        assert np.array_equal(g[f][hit].view(np.uint32), o[f][hit].view(np.uint32)), f
+    depth = gpu_ctx.download("Depth")
+    assert np.array_equal(depth[o["hit"] == 0], np.ones((o["hit"] == 0).sum(), np.float32))
+
+
+@pytest.mark.parametrize("cfg", [1, 2])
+def test_trace_rays_closest_and_any_hit(gpu_ctx, cfg):
+    sc, cam = _scene(cfg)
+    gpu_ctx.upload_scene(sc)
+    rng = np.random.default_rng(5)
+    n = 4096
+    o = rng.uniform(-6, 6, (n, 3)) + np.array([0, 3.0, 0])
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.concatenate([o, d], 1).astype(np.float32)
+    orc = Oracle(sc)
+    a = gpu_ctx.trace_rays(rays)
+    b = orc.trace_rays(rays)
+    assert np.array_equal(a["prim_id"], b["prim_id"]) and np.array_equal(a["tri_id"], b["tri_id"])
+    assert np.array_equal(a["depth"].view(np.uint32), b["depth"].view(np.uint32))
+    tmax = rng.uniform(0.0, 10.0, n).astype(np.float32)
+    a = gpu_ctx.trace_rays(rays, tmax, any_hit=True)
+    b = orc.trace_rays(rays, tmax, any_hit=True)
+    assert np.array_equal(a["hit"], b["hit"])
+
+
+def test_path_trace_matches_oracle(gpu_ctx):
+    sc, cam = _scene(0)
+    gpu_ctx.upload_scene(sc)
+    orc = Oracle(sc)
+    gpu_ctx.clear_persistent()
+    for frame in range(2):
+        gpu_ctx.raycast(cam, frame)
+        gpu_ctx.path_trace(cam, frame, max_depth=4)
+        gpu = gpu_ctx.download("Color")
+        orc.raycast(cam, frame)
+        ref, _ = orc.integrate(cam, frame, ris=False, max_depth=4)
+        frac = _color_outliers(gpu, ref)
+        print(f"PT frame {frame}: outlier fraction {frac:.4f}")
+        assert frac <= MAX_OUTLIERS
+        gpu_ctx.accumulate(frame, firefly=True)
+        orc.accumulate(cam, frame, firefly=True)
+
+
+def test_ris_plain_matches_oracle(gpu_ctx):
+    sc, cam = _scene(1)
+    gpu_ctx.upload_scene(sc)
+    orc = Oracle(sc)
+    gpu_ctx.raycast(cam, 0)
+    gpu_ctx.ris_path_trace(cam, 0, candidate_count=16, use_reservoir=False, skip_visibility=True, max_depth=1)
+    gpu = gpu_ctx.download("Color")
+    orc.raycast(cam, 0)
+    ref, _ = orc.integrate(cam, 0, ris=True, candidate_count=16, use_reservoir=False, skip_visibility=True,
+                           max_depth=1)
+    frac = _color_outliers(gpu, ref)
+    print(f"RIS: outlier fraction {frac:.4f}, mean {gpu[:, :3].mean():.5f} vs {ref[:, :3].mean():.5f}")
+    assert frac <= MAX_OUTLIERS
+
+
+def test_restir_temporal_matches_oracle(gpu_ctx):
+    sc, cam = _scene(2)
+    gpu_ctx.upload_scene(sc)
+    gpu_ctx.clear_persistent()
+    orc = Oracle(sc)
+    for frame in range(3):
+        gpu_ctx.raycast(cam, frame)
+        gpu_ctx.ris_path_trace(cam, frame, candidate_count=32, use_reservoir=True, max_depth=1)
+        gpu = gpu_ctx.download("Color")
+        res = gpu_ctx.download("__ris_reservoir")
+        orc.raycast(cam, frame)
+        ref, _ = orc.integrate(cam, frame, ris=True, candidate_count=32, use_reservoir=True, max_depth=1)
+        m_gpu = res[4, :, 2].view(np.int32)
+        assert np.array_equal(m_gpu, orc.res["m"]), "reservoir CandidateCount (M) must be bit-exact"
+        frac = _color_outliers(gpu, ref)
+        print(f"ReSTIR frame {frame}: outlier fraction {frac:.4f}")
+        assert frac <= MAX_OUTLIERS
