@@ -126,8 +126,11 @@ def lib() -> C.CDLL:
             "hdr_set_cancel": (C.c_int, [vp, C.POINTER(C.c_int32)]),
             "hdr_trace_rays": (C.c_int, [vp, vp, vp, i32, i32, vp]),
             "hdr_rng_floats": (C.c_int, [vp, vp, i32, i32, vp]),
-            "hdr_pass_times": (C.c_int, [vp, C.POINTER(C.c_float), i32]),
+            "hdr_pass_times": (C.c_int, [vp, C.POINTER(C.c_float), C.POINTER(C.c_int32), i32, i32]),
             "hdr_launch_count": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
+            "hdr_region_begin": (C.c_int, [vp, i32]),
+            "hdr_region_end": (C.c_int, [vp, i32]),
+            "hdr_region_elapsed": (C.c_int, [vp, i32, C.POINTER(C.c_float)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

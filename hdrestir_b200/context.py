@@ -138,10 +138,23 @@ class Context:
                                            out.ctypes.data_as(C.c_void_p)))
         return out
 
-    def pass_times(self) -> tuple[float, float, float]:
+    def pass_times(self, reset: bool = False) -> tuple[tuple[float, float, float], tuple[int, int, int]]:
+        """(average ms, call count) of raycast / integrate / accumulate since the last reset."""
         ms = (C.c_float * 3)()
-        abi.check(self._lib.hdr_pass_times(self._h, ms, 3))
-        return tuple(ms)
+        n = (C.c_int32 * 3)()
+        abi.check(self._lib.hdr_pass_times(self._h, ms, n, 3, int(reset)))
+        return tuple(ms), tuple(n)
+
+    def region_begin(self, slot: int = 0) -> None:
+        abi.check(self._lib.hdr_region_begin(self._h, int(slot)))
+
+    def region_end(self, slot: int = 0) -> None:
+        abi.check(self._lib.hdr_region_end(self._h, int(slot)))
+
+    def region_elapsed(self, slot: int = 0) -> float:
+        ms = C.c_float()
+        abi.check(self._lib.hdr_region_elapsed(self._h, int(slot), C.byref(ms)))
+        return float(ms.value)
 
     def launch_count(self) -> int:
         n = C.c_uint64()

@@ -67,8 +67,15 @@ struct hdr_ctx {
 
     unsigned *d_err = nullptr;
     int *d_flag = nullptr;
-    cudaEvent_t ev[2] = {nullptr, nullptr};
-    float pass_ms[3] = {0, 0, 0};
+    // per pass slot (raycast, integrate, accumulate): one start/stop event pair;
+    // the previous pair is folded into the running sums when the slot is reused
+    cudaEvent_t ev_start[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev_stop[3] = {nullptr, nullptr, nullptr};
+    bool ev_pending[3] = {false, false, false};
+    double pass_sum_ms[3] = {0, 0, 0};
+    int pass_count[3] = {0, 0, 0};
+    float pass_last_ms[3] = {0, 0, 0};
+    cudaEvent_t region_ev[4][2] = {};
     const volatile int32_t *cancel = nullptr;
     uint64_t launches = 0;
 };
@@ -186,18 +193,30 @@ hdr_status gbuffer_view(hdr_ctx *c, size_t count, bool create, hdr::GBufferView 
     return HDR_OK;
 }
 
-hdr_status begin_pass(hdr_ctx *c) {
-    if (c->flags & 1u) HDR_CUDA(cudaEventRecord(c->ev[0], c->stream));
+hdr_status fold_pass_time(hdr_ctx *c, int slot) {
+    if (!c->ev_pending[slot]) return HDR_OK;
+    HDR_CUDA(cudaEventSynchronize(c->ev_stop[slot]));
+    float ms = 0.0f;
+    HDR_CUDA(cudaEventElapsedTime(&ms, c->ev_start[slot], c->ev_stop[slot]));
+    c->pass_last_ms[slot] = ms;
+    c->pass_sum_ms[slot] += ms;
+    c->pass_count[slot] += 1;
+    c->ev_pending[slot] = false;
+    return HDR_OK;
+}
+hdr_status begin_pass(hdr_ctx *c, int slot) {
+    if (c->flags & 1u) {
+        hdr_status st = fold_pass_time(c, slot);
+        if (st != HDR_OK) return st;
+        HDR_CUDA(cudaEventRecord(c->ev_start[slot], c->stream));
+    }
     return HDR_OK;
 }
 hdr_status end_pass(hdr_ctx *c, int slot) {
     HDR_CUDA(cudaGetLastError());
     if (c->flags & 1u) {
-        HDR_CUDA(cudaEventRecord(c->ev[1], c->stream));
-        HDR_CUDA(cudaEventSynchronize(c->ev[1]));
-        float ms = 0.0f;
-        HDR_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
-        c->pass_ms[slot] = ms;
+        HDR_CUDA(cudaEventRecord(c->ev_stop[slot], c->stream));
+        c->ev_pending[slot] = true;
     }
     return HDR_OK;
 }
@@ -236,8 +255,14 @@ hdr_status hdr_ctx_create(hdr_ctx **out, const hdr_ctx_desc *desc) {
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_err, 64);
     if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, 64);
-    if (e == cudaSuccess) e = cudaEventCreate(&c->ev[0]);
-    if (e == cudaSuccess) e = cudaEventCreate(&c->ev[1]);
+    for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+        e = cudaEventCreate(&c->ev_start[k]);
+        if (e == cudaSuccess) e = cudaEventCreate(&c->ev_stop[k]);
+    }
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
+        e = cudaEventCreate(&c->region_ev[k][0]);
+        if (e == cudaSuccess) e = cudaEventCreate(&c->region_ev[k][1]);
+    }
     if (e != cudaSuccess) {
         hdr_ctx_destroy(c);
         return fail(HDR_ECUDA, "context setup: %s", cudaGetErrorString(e));
@@ -254,8 +279,13 @@ void hdr_ctx_destroy(hdr_ctx *c) {
     for (auto &b : c->scene_bufs) dev_free(c, b);
     for (auto &kv : c->buffers) dev_free(c, kv.second);
     if (c->d_err) cudaFree(c->d_err);
-    for (auto &e : c->ev)
-        if (e) cudaEventDestroy(e);
+    for (int k = 0; k < 3; ++k) {
+        if (c->ev_start[k]) cudaEventDestroy(c->ev_start[k]);
+        if (c->ev_stop[k]) cudaEventDestroy(c->ev_stop[k]);
+    }
+    for (auto &pair : c->region_ev)
+        for (auto &e : pair)
+            if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -343,7 +373,7 @@ hdr_status hdr_raycast(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, u
     c->width = cam->width;
     c->height = cam->height;
     const hdr::CameraD d = make_camera(cam);
-    if ((st = begin_pass(c)) != HDR_OK) return st;
+    if ((st = begin_pass(c, 0)) != HDR_OK) return st;
     hdr::launch_raycast(c->scene, d, frame_index, gb, aov, c->d_err, c->stream);
     c->launches += 1;
     return end_pass(c, 0);
@@ -386,7 +416,7 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
     d.spatial_neighbors = p->spatial_neighbors;
     d.spatial_radius = p->spatial_radius;
     const hdr::CameraD cd = make_camera(cam);
-    if ((st = begin_pass(c)) != HDR_OK) return st;
+    if ((st = begin_pass(c, 1)) != HDR_OK) return st;
     hdr::launch_ris_path_trace(c->scene, cd, frame_index, d, gb, rv, (float4 *)color, c->d_err, c->stream);
     c->launches += 1;
     return end_pass(c, 1);
@@ -414,7 +444,7 @@ hdr_status hdr_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index
     d.render_ibl_background = p->render_ibl_background;
     d.roulette = p->roulette_aggressiveness;
     const hdr::CameraD cd = make_camera(cam);
-    if ((st = begin_pass(c)) != HDR_OK) return st;
+    if ((st = begin_pass(c, 1)) != HDR_OK) return st;
     hdr::launch_path_trace(c->scene, cd, frame_index, d, gb, (float4 *)color, c->d_err, c->stream);
     c->launches += 1;
     return end_pass(c, 1);
@@ -437,7 +467,7 @@ hdr_status hdr_accumulate(hdr_ctx *c, int32_t frame_index, int32_t firefly, int3
     if ((st = ensure_buffer(c, "__accum_color", count * 16, &accum)) != HDR_OK) return st;
     if (firefly)
         if ((st = ensure_buffer(c, "__firefly_scratch", count * 32, &scratch)) != HDR_OK) return st;
-    if ((st = begin_pass(c)) != HDR_OK) return st;
+    if ((st = begin_pass(c, 2)) != HDR_OK) return st;
     const int n = hdr::launch_accumulate((float4 *)color, (float4 *)accum, (float4 *)scratch, c->d_flag, c->width,
                                          c->height, frame_index, firefly, mode, c->stream);
     if (n < 0) return fail(HDR_ECUDA, "accumulation launch failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -602,9 +632,41 @@ hdr_status hdr_rng_floats(hdr_ctx *c, const uint32_t *seeds, int32_t n_seeds, in
     return HDR_OK;
 }
 
-hdr_status hdr_pass_times(hdr_ctx *c, float *ms, int32_t n) {
-    if (!c || (!ms && n > 0)) return fail(HDR_EINVAL, "bad argument");
-    for (int i = 0; i < n && i < 3; ++i) ms[i] = c->pass_ms[i];
+hdr_status hdr_pass_times(hdr_ctx *c, float *avg_ms, int32_t *counts, int32_t n, int32_t reset) {
+    if (!c || (n > 0 && (!avg_ms || !counts))) return fail(HDR_EINVAL, "bad argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    for (int k = 0; k < 3; ++k) {
+        hdr_status st = fold_pass_time(c, k);
+        if (st != HDR_OK) return st;
+    }
+    for (int i = 0; i < n && i < 3; ++i) {
+        avg_ms[i] = c->pass_count[i] ? (float)(c->pass_sum_ms[i] / c->pass_count[i]) : 0.0f;
+        counts[i] = c->pass_count[i];
+    }
+    if (reset)
+        for (int k = 0; k < 3; ++k) c->pass_sum_ms[k] = 0.0, c->pass_count[k] = 0;
+    return HDR_OK;
+}
+
+hdr_status hdr_region_begin(hdr_ctx *c, int32_t slot) {
+    if (!c || slot < 0 || slot >= 4) return fail(HDR_EINVAL, "bad region slot");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaEventRecord(c->region_ev[slot][0], c->stream));
+    return HDR_OK;
+}
+
+hdr_status hdr_region_end(hdr_ctx *c, int32_t slot) {
+    if (!c || slot < 0 || slot >= 4) return fail(HDR_EINVAL, "bad region slot");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaEventRecord(c->region_ev[slot][1], c->stream));
+    return HDR_OK;
+}
+
+hdr_status hdr_region_elapsed(hdr_ctx *c, int32_t slot, float *ms) {
+    if (!c || !ms || slot < 0 || slot >= 4) return fail(HDR_EINVAL, "bad argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaEventSynchronize(c->region_ev[slot][1]));
+    HDR_CUDA(cudaEventElapsedTime(ms, c->region_ev[slot][0], c->region_ev[slot][1]));
     return HDR_OK;
 }
 

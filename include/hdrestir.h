@@ -274,10 +274,19 @@ hdr_status hdr_trace_rays(hdr_ctx *ctx, const float *rays, const float *tmax, in
 hdr_status hdr_rng_floats(hdr_ctx *ctx, const uint32_t *seeds, int32_t n_seeds, int32_t count,
                           float *out);
 
-/* Per-pass device times (ms) of the last call of each pass, measured with CUDA
- * events on the ctx stream when flag bit 0 is set:
- * [0] raycast, [1] integrate, [2] accumulate. */
-hdr_status hdr_pass_times(hdr_ctx *ctx, float *ms, int32_t n);
+/* Average device time (ms) and number of calls of each pass since the last
+ * reset, measured with CUDA events on the ctx stream when flag bit 0 is set
+ * (the replacement for the reference's METRICS_ENABLED pass timers,
+ * core/metrics_on_buffers.h): [0] raycast, [1] integrate, [2] accumulate.
+ * reset != 0 clears the sums after reading them. */
+hdr_status hdr_pass_times(hdr_ctx *ctx, float *avg_ms, int32_t *counts, int32_t n, int32_t reset);
+
+/* Device-time regions on the ctx stream (4 slots): begin records a start event,
+ * end records a stop event; hdr_region_elapsed waits for the stop event and
+ * returns the milliseconds between them. */
+hdr_status hdr_region_begin(hdr_ctx *ctx, int32_t slot);
+hdr_status hdr_region_end(hdr_ctx *ctx, int32_t slot);
+hdr_status hdr_region_elapsed(hdr_ctx *ctx, int32_t slot, float *ms);
 
 /* Number of this library's kernels launched on the ctx so far. */
 hdr_status hdr_launch_count(hdr_ctx *ctx, uint64_t *count);

@@ -71,6 +71,9 @@ def lib() -> C.CDLL:
         L.orc_raycast.argtypes = [vp, C.POINTER(abi.CameraDesc), C.c_int, vp, C.c_int]
         L.orc_integrate.argtypes = [vp, C.POINTER(abi.CameraDesc), C.c_int, C.POINTER(FrameParams), vp, vp, vp,
                                     vp, C.c_int]
+        L.orc_raycast_band.argtypes = [vp, C.POINTER(abi.CameraDesc), C.c_int, vp, C.c_int, C.c_int, C.c_int]
+        L.orc_integrate_band.argtypes = [vp, C.POINTER(abi.CameraDesc), C.c_int, C.POINTER(FrameParams), vp, vp,
+                                         vp, vp, C.c_int, C.c_int, C.c_int]
         L.orc_accumulate.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_rng_floats.argtypes = [vp, C.c_int, C.c_int, vp]
         L.orc_trace_rays.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp]
@@ -136,6 +139,18 @@ class Oracle:
         self._lib.orc_integrate(self._s, C.byref(cam.c_desc()), int(frame), C.byref(fp), _p(self.gbuf),
                                 _p(self.color), _p(self.res), _p(tr), self.threads)
         return self.color, tr
+
+    def frame_band(self, cam, frame, y0, y1, ris=True, candidate_count=32, use_reservoir=True,
+                   skip_visibility=False, max_depth=1):
+        """Raycast + integration of image rows [y0, y1) (a bounded CPU sample of one frame)."""
+        n = cam.width * cam.height
+        self._ensure(n)
+        cd = cam.c_desc()
+        fp = FrameParams(int(ris), PathParams(max_depth, 1, 8, 8, 1, 1.0),
+                         RisParams(candidate_count, int(use_reservoir), int(skip_visibility), 0))
+        self._lib.orc_raycast_band(self._s, C.byref(cd), int(frame), _p(self.gbuf), int(y0), int(y1), self.threads)
+        self._lib.orc_integrate_band(self._s, C.byref(cd), int(frame), C.byref(fp), _p(self.gbuf), _p(self.color),
+                                     _p(self.res), None, int(y0), int(y1), self.threads)
 
     def accumulate(self, cam, frame, firefly=True):
         self._lib.orc_accumulate(_p(self.color), _p(self.accum), cam.width, cam.height, int(frame), int(firefly))

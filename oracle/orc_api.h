@@ -53,6 +53,12 @@ void orc_camera_ray(const hdr_camera *cam, const double *inv_view, const double 
 void orc_raycast(const orc_scene *s, const hdr_camera *cam, int frame, hdr_gbuffer_texel *gbuf, int threads);
 void orc_integrate(const orc_scene *s, const hdr_camera *cam, int frame, const orc_frame_params *fp,
                    hdr_gbuffer_texel *gbuf, float *color, orc_reservoir *res, orc_pixel_trace *trace, int threads);
+/* the same passes restricted to image rows [y0, y1) (bounded CPU-baseline samples) */
+void orc_raycast_band(const orc_scene *s, const hdr_camera *cam, int frame, hdr_gbuffer_texel *gbuf, int y0,
+                      int y1, int threads);
+void orc_integrate_band(const orc_scene *s, const hdr_camera *cam, int frame, const orc_frame_params *fp,
+                        hdr_gbuffer_texel *gbuf, float *color, orc_reservoir *res, orc_pixel_trace *trace, int y0,
+                        int y1, int threads);
 void orc_accumulate(float *color, float *accum, int width, int height, int frame, int firefly);
 void orc_rng_floats(const uint32_t *seeds, int n, int count, float *out);
 void orc_trace_rays(const orc_scene *s, const float *rays, const float *tmax, int n, int any_hit,

@@ -1239,27 +1239,45 @@ static void *run_rows(void *arg) {
     return NULL;
 }
 
-static void run_pass(job *base, int threads) {
-    int H = base->cam->height;
-    if (threads < 1) threads = 1;
-    if (threads > H) threads = H;
-    pthread_t th[256];
-    job js[256];
-    if (threads > 256) threads = 256;
-    for (int t = 0; t < threads; ++t) {
-        js[t] = *base;
-        js[t].y0 = (int)((long)H * t / threads);
-        js[t].y1 = (int)((long)H * (t + 1) / threads);
-        if (threads == 1)
-            run_rows(&js[t]);
-        else
-            pthread_create(&th[t], NULL, run_rows, &js[t]);
+/* rows [base->y0, base->y1) split over threads in interleaved strips of 4 rows */
+static void *run_strips(void *arg);
+typedef struct {
+    job base;
+    int t, threads;
+} strip_job;
+static void *run_strips(void *arg) {
+    strip_job *sj = (strip_job *)arg;
+    for (int y = sj->base.y0 + 4 * sj->t; y < sj->base.y1; y += 4 * sj->threads) {
+        job j = sj->base;
+        j.y0 = y;
+        j.y1 = y + 4 < sj->base.y1 ? y + 4 : sj->base.y1;
+        run_rows(&j);
     }
-    if (threads > 1)
-        for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+    return NULL;
 }
 
-void orc_raycast(const orc_scene *s, const hdr_camera *cam, int frame, hdr_gbuffer_texel *gbuf, int threads) {
+static void run_pass(job *base, int threads) {
+    int H = base->y1 - base->y0;
+    if (H <= 0) return;
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    if (threads > 1) {
+        pthread_t th[256];
+        strip_job sj[256];
+        for (int t = 0; t < threads; ++t) {
+            sj[t].base = *base;
+            sj[t].t = t;
+            sj[t].threads = threads;
+            pthread_create(&th[t], NULL, run_strips, &sj[t]);
+        }
+        for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+        return;
+    }
+    run_rows(base);
+}
+
+void orc_raycast_band(const orc_scene *s, const hdr_camera *cam, int frame, hdr_gbuffer_texel *gbuf, int y0,
+                      int y1, int threads) {
     job j;
     memset(&j, 0, sizeof(j));
     j.s = s;
@@ -1269,11 +1287,18 @@ void orc_raycast(const orc_scene *s, const hdr_camera *cam, int frame, hdr_gbuff
     j.frame = frame;
     j.gbuf = gbuf;
     j.pass = 0;
+    j.y0 = y0;
+    j.y1 = y1;
     run_pass(&j, threads);
 }
 
-void orc_integrate(const orc_scene *s, const hdr_camera *cam, int frame, const orc_frame_params *fp,
-                   hdr_gbuffer_texel *gbuf, float *color, orc_reservoir *res, orc_pixel_trace *trace, int threads) {
+void orc_raycast(const orc_scene *s, const hdr_camera *cam, int frame, hdr_gbuffer_texel *gbuf, int threads) {
+    orc_raycast_band(s, cam, frame, gbuf, 0, cam->height, threads);
+}
+
+void orc_integrate_band(const orc_scene *s, const hdr_camera *cam, int frame, const orc_frame_params *fp,
+                        hdr_gbuffer_texel *gbuf, float *color, orc_reservoir *res, orc_pixel_trace *trace, int y0,
+                        int y1, int threads) {
     job j;
     memset(&j, 0, sizeof(j));
     j.s = s;
@@ -1287,7 +1312,14 @@ void orc_integrate(const orc_scene *s, const hdr_camera *cam, int frame, const o
     j.res = res;
     j.trace = trace;
     j.pass = 1;
+    j.y0 = y0;
+    j.y1 = y1;
     run_pass(&j, threads);
+}
+
+void orc_integrate(const orc_scene *s, const hdr_camera *cam, int frame, const orc_frame_params *fp,
+                   hdr_gbuffer_texel *gbuf, float *color, orc_reservoir *res, orc_pixel_trace *trace, int threads) {
+    orc_integrate_band(s, cam, frame, fp, gbuf, color, res, trace, 0, cam->height, threads);
 }
 
 /* AccumulationPass::_execute (passes/accumulation_pass.cpp:22-139): firefly
