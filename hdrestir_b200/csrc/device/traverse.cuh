@@ -18,9 +18,6 @@
 
 namespace hdr {
 
-constexpr int kBlasStack = 64;
-constexpr int kTlasStack = 64;
-
 // error bits reported back to the host
 constexpr unsigned kErrBlasStack = 1u;
 constexpr unsigned kErrTlasStack = 2u;
@@ -128,8 +125,20 @@ struct HitId {
 };
 
 // Closest hit (kAnyHit = false), or "closest t < t_limit" test (kAnyHit = true).
-// err receives kErr* bits if a stack would overflow (the host rejects scenes
-// deeper than the stacks, so this is a guard, not a path).
+//
+// One loop over one stack holds TLAS nodes, instance slots and BLAS nodes
+// (tag in the low 2 bits), so the threads of a warp step through the two
+// levels together instead of diverging in nested loops. The visiting order is
+// the reference's: a TLAS leaf pushes its instances so they pop in leaf order;
+// an instance pushes its BLAS root, whose nodes all pop before the next
+// instance; BLAS children pop left first. A single running closest t replaces
+// the reference's per-instance copy (instT starts at hit.t and hit.t is only
+// written from it), which gives the same comparisons.
+// err receives kErr* bits if the stack would overflow (the host rejects scenes
+// deeper than the stack, so this is a guard, not a path).
+constexpr int kTraceStack = 96;
+constexpr int kTagTlas = 0, kTagInst = 1, kTagBlas = 2;
+
 template <bool kAnyHit>
 __device__ bool trace_ray(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId &hit, unsigned &err) {
     hit.t = 1e30f;
@@ -138,96 +147,79 @@ __device__ bool trace_ray(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId
     hit.u = hit.v = 0.0f;
     if (!s.has_tlas) return false;
     const SlabRay wr = make_slab_ray<false>(o, d);
-    int tstack[kTlasStack];
-    int tsp = 0;
-    tstack[tsp++] = 0;
-    bool was_hit = false;
-    while (tsp > 0) {
-        const int ni = tstack[--tsp];
-        const float4 lo = __ldg(&s.tlas_nodes[2 * ni]);
-        const float4 hi = __ldg(&s.tlas_nodes[2 * ni + 1]);
-        float t_aabb = 0.0f;
-        if (!slab_test(wr, lo, hi, t_aabb) || t_aabb > hit.t) continue;
-        const int left = fbits(lo.w);
-        if (left < 0) {
-            const int start = -left - 1;
-            const int count = fbits(hi.w);
-            for (int k = 0; k < count; ++k) {
-                const int ii = __ldg(&s.tlas_inst[start + k]);
-                const float4 *ip = s.instances + 8 * ii;
-                const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2), m3 = __ldg(ip + 3);
-                const float4 r7 = __ldg(ip + 7);
-                if (fbits(r7.y) == 0) continue;  // mesh without triangles: empty BVH
-                const float inv[16] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w,
-                                       m2.x, m2.y, m2.z, m2.w, m3.x, m3.y, m3.z, m3.w};
-                const V3 oo = m4f_transform(inv, o);
-                const V3 od = m4f_transform_dir(inv, d);
-                const int node_base = fbits(__ldg(&ip[4].w));
-                const int tri_base = fbits(__ldg(&ip[5].w));
-                const SlabRay br = make_slab_ray<true>(oo, od);
-                float bt = hit.t;
-                int btri = -1;
-                float bu = 0.0f, bv = 0.0f;
-                int bstack[kBlasStack];
-                int bsp = 0;
-                bstack[bsp++] = 0;
-                bool done = false;
-                while (bsp > 0 && !done) {
-                    const int bn = bstack[--bsp];
-                    const float4 nlo = __ldg(&s.blas_nodes[2 * (node_base + bn)]);
-                    const float4 nhi = __ldg(&s.blas_nodes[2 * (node_base + bn) + 1]);
-                    float ta;
-                    if (!slab_test(br, nlo, nhi, ta)) continue;
-                    if (ta > bt) continue;
-                    const int bl = fbits(nlo.w);
-                    if (bl < 0) {
-                        const int st = -bl - 1;
-                        const int cnt = fbits(nhi.w);
-                        for (int q = 0; q < cnt; ++q) {
-                            float tt, uu, vv;
-                            if (tri_test(oo, od, s.tri_geo + 3 * (size_t)(tri_base + st + q), tt, uu, vv)) {
-                                if (tt < bt) {
-                                    bt = tt;
-                                    btri = st + q;
-                                    bu = uu;
-                                    bv = vv;
-                                    if (kAnyHit && bt < t_limit) {
-                                        done = true;
-                                        break;
-                                    }
-                                }
-                            }
-                        }
-                    } else {
-                        if (bsp + 2 > kBlasStack) {
-                            err |= kErrBlasStack;
-                            done = true;
-                            break;
-                        }
-                        bstack[bsp++] = bl + 1;
-                        bstack[bsp++] = bl;
+    SlabRay br = wr;
+    V3 oo = o, od = d;
+    int cur_inst = -1, node_base = 0, tri_base = 0;
+    int stack[kTraceStack];
+    int sp = 0;
+    stack[sp++] = (0 << 2) | kTagTlas;
+    while (sp > 0) {
+        const int e = stack[--sp];
+        const int tag = e & 3, idx = e >> 2;
+        if (tag == kTagBlas) {
+            const float4 nlo = __ldg(&s.blas_nodes[2 * (node_base + idx)]);
+            const float4 nhi = __ldg(&s.blas_nodes[2 * (node_base + idx) + 1]);
+            float ta;
+            if (!slab_test(br, nlo, nhi, ta) || ta > hit.t) continue;
+            const int bl = fbits(nlo.w);
+            if (bl < 0) {
+                const int st = -bl - 1;
+                const int cnt = fbits(nhi.w);
+                for (int q = 0; q < cnt; ++q) {
+                    float tt, uu, vv;
+                    if (tri_test(oo, od, s.tri_geo + 3 * (size_t)(tri_base + st + q), tt, uu, vv) && tt < hit.t) {
+                        hit.t = tt;
+                        hit.inst = cur_inst;
+                        hit.tri = st + q;
+                        hit.u = uu;
+                        hit.v = vv;
                     }
                 }
-                if (btri < 0) continue;
-                if (bt >= hit.t) continue;
-                hit.t = bt;
-                hit.inst = ii;
-                hit.tri = btri;
-                hit.u = bu;
-                hit.v = bv;
-                was_hit = true;
-                if (kAnyHit && hit.t < t_limit) return true;
+                if (kAnyHit && hit.inst >= 0 && hit.t < t_limit) return true;
+            } else {
+                if (sp + 2 > kTraceStack) {
+                    err |= kErrBlasStack;
+                    break;
+                }
+                stack[sp++] = ((bl + 1) << 2) | kTagBlas;
+                stack[sp++] = (bl << 2) | kTagBlas;
             }
-        } else {
-            if (tsp + 2 > kTlasStack) {
+        } else if (tag == kTagTlas) {
+            const float4 lo = __ldg(&s.tlas_nodes[2 * idx]);
+            const float4 hi = __ldg(&s.tlas_nodes[2 * idx + 1]);
+            float t_aabb = 0.0f;
+            if (!slab_test(wr, lo, hi, t_aabb) || t_aabb > hit.t) continue;
+            const int left = fbits(lo.w);
+            if (sp + 2 > kTraceStack) {
                 err |= kErrTlasStack;
                 break;
             }
-            tstack[tsp++] = left + 1;
-            tstack[tsp++] = left;
+            if (left < 0) {
+                const int start = -left - 1;
+                const int count = fbits(hi.w);
+                for (int k = count - 1; k >= 0; --k) stack[sp++] = ((start + k) << 2) | kTagInst;
+            } else {
+                stack[sp++] = ((left + 1) << 2) | kTagTlas;
+                stack[sp++] = (left << 2) | kTagTlas;
+            }
+        } else {  // instance slot of a TLAS leaf: enter its BLAS in object space
+            const int ii = __ldg(&s.tlas_inst[idx]);
+            const float4 *ip = s.instances + 8 * ii;
+            const float4 r7 = __ldg(ip + 7);
+            if (fbits(r7.y) == 0) continue;  // mesh without triangles: empty BVH
+            const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2), m3 = __ldg(ip + 3);
+            const float inv[16] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w,
+                                   m2.x, m2.y, m2.z, m2.w, m3.x, m3.y, m3.z, m3.w};
+            oo = m4f_transform(inv, o);
+            od = m4f_transform_dir(inv, d);
+            br = make_slab_ray<true>(oo, od);
+            node_base = fbits(__ldg(&ip[4].w));
+            tri_base = fbits(__ldg(&ip[5].w));
+            cur_inst = ii;
+            stack[sp++] = (0 << 2) | kTagBlas;
         }
     }
-    return was_hit;
+    return hit.inst >= 0;
 }
 
 // HitRecord (core/hit_record.h:15-27) of IntersectScene (scene.cpp:437-535)

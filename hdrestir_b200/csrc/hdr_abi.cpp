@@ -297,9 +297,10 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     hdr::FlatScene f;
     std::string err;
     if (!hdr::build_flat_scene(*desc, f, err)) return fail(HDR_EINVAL, "%s", err.c_str());
-    if (f.max_blas_depth >= hdr::kBlasStack - 1 || f.max_tlas_depth >= hdr::kTlasStack - 1)
-        return fail(HDR_EINVAL, "BVH depth %d / TLAS depth %d exceeds the device traversal stack (%d)",
-                    f.max_blas_depth, f.max_tlas_depth, hdr::kBlasStack);
+    // one pending sibling per level of each tree, plus the two instance slots of a TLAS leaf
+    if (f.max_blas_depth + f.max_tlas_depth + 4 > hdr::kTraceStack)
+        return fail(HDR_EINVAL, "BVH depth %d + TLAS depth %d exceeds the device traversal stack (%d)",
+                    f.max_blas_depth, f.max_tlas_depth, hdr::kTraceStack);
     HDR_CUDA(cudaStreamSynchronize(c->stream));
     for (auto &b : c->scene_bufs) dev_free(c, b);
     c->scene_bufs.clear();

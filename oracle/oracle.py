@@ -76,6 +76,8 @@ def lib() -> C.CDLL:
                                          vp, vp, C.c_int, C.c_int, C.c_int]
         L.orc_accumulate.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_rng_floats.argtypes = [vp, C.c_int, C.c_int, vp]
+        L.orc_reservoir_known_answer.restype = C.c_float
+        L.orc_reservoir_known_answer.argtypes = [C.c_float, C.c_float, C.c_int]
         L.orc_trace_rays.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp]
         _lib = L
     return _lib

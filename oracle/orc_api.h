@@ -61,6 +61,7 @@ void orc_integrate_band(const orc_scene *s, const hdr_camera *cam, int frame, co
                         int y1, int threads);
 void orc_accumulate(float *color, float *accum, int width, int height, int frame, int firefly);
 void orc_rng_floats(const uint32_t *seeds, int n, int count, float *out);
+float orc_reservoir_known_answer(float weight, float phat, int candidates_per_frame);
 void orc_trace_rays(const orc_scene *s, const float *rays, const float *tmax, int n, int any_hit,
                     hdr_gbuffer_texel *out);
 

@@ -1355,6 +1355,31 @@ void orc_accumulate(float *color, float *accum, int width, int height, int frame
     }
 }
 
+/* WeightedReservoir::Update + Finalize (restir/reservoir.h:76-125) for one
+ * candidate with the given weight and target function; returns W. The draw
+ * comes from Rng{777} as in tests/test_reservoir.cpp:67-76. */
+float orc_reservoir_known_answer(float weight, float phat, int candidates_per_frame) {
+    orc_rng r;
+    orc_rng_seed(&r, 777u);
+    int m = 0, chosen = 0;
+    float wsum = 0.0f, chosen_phat = 0.0f;
+    ++m;
+    if (weight > 0.0f) {
+        wsum += weight;
+        if (orc_rng_float(&r) <= weight / wsum) {
+            chosen = 1;
+            chosen_phat = phat;
+        }
+    }
+    if (!chosen || m <= 0) return 0.0f;
+    if (chosen_phat <= 0.0f) return 0.0f;
+    int cpf = candidates_per_frame > 1 ? candidates_per_frame : 1;
+    int frames = m / cpf;
+    if (frames < 1) frames = 1;
+    float w = wsum / ((float)frames * chosen_phat);
+    return isfinite(w) ? w : 0.0f;
+}
+
 void orc_rng_floats(const uint32_t *seeds, int n, int count, float *out) {
     for (int k = 0; k < n; ++k) {
         orc_rng r;

@@ -1,0 +1,369 @@
+// Harness around the reference's own hot-path sources, compiled in place
+// against the shim headers (oracle/shim) — TEST INFRASTRUCTURE.
+//
+// Builds a Restir::Scene from an hdr_scene_desc the way the Hydra adapter
+// feeds it (one mesh subset per instance, PreviewSurface params per material,
+// LightFactoryInput per light), runs the reference passes RaycastPass ->
+// PathTracePass | RISPathTracePass -> AccumulationPass with the persistent
+// buffer store of RenderPipeline::Execute (pipeline/render_pipeline.cpp:24-40),
+// and exports GBuffer, Color and "__ris_reservoir" through a C interface for
+// the parity tests and the CPU baseline. Nothing here is part of the product.
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../include/hdrestir.h"
+#include "accumulation_pass.h"
+#include "path_trace_pass.h"
+#include "pxr/imaging/hio/image.h"
+#include "raycast_pass.h"
+#include "render_context.h"
+#include "reservoir.h"
+#include "restir/output_names.h"
+#include "ris_direct_light_integrator.h"
+#include "ris_path_trace_pass.h"
+#include "rng.h"
+#include "scene.h"
+
+using namespace Restir;
+
+// Texture loading is out of scope (no benchmark scene uses textures); the
+// factory's loader is the only ImageTextureSamplerFactory symbol referenced.
+const detail::Texture *ImageTextureSamplerFactory::_getOrLoad(std::string_view, bool) const { return nullptr; }
+
+namespace {
+
+class RefMesh final : public IMesh {
+  public:
+    VtVec3fArray points, colors, normals;
+    VtVec2fArray uvs;
+    std::vector<MeshSubset> subsets;
+    GfMatrix4f transform{1.0f};
+    SdfPath id, instancer;
+    const VtVec3fArray &GetPoints() const override { return points; }
+    const GfMatrix4f &GetTransform() const override { return transform; }
+    bool IsVisible() const override { return true; }
+    const VtVec3fArray &GetColors() const override { return colors; }
+    const VtVec2fArray &GetUVs() const override { return uvs; }
+    const VtVec3fArray &GetNormals() const override { return normals; }
+    const std::vector<MeshSubset> &GetSubsets() const override { return subsets; }
+    const SdfPath &GetInstancerId() const override { return instancer; }
+    const SdfPath &GetId() const override { return id; }
+};
+
+std::string path_of(const char *prefix, int i) {
+    char b[64];
+    std::snprintf(b, sizeof(b), "/%s%08d", prefix, i);
+    return b;
+}
+
+}  // namespace
+
+struct ref_params {
+    int32_t pipeline;  // 0 PathTracer, 1 RIS
+    int32_t candidate_count, use_reservoir, skip_visibility;
+    int32_t max_depth, enable_subsurface, max_refl, max_refr, render_ibl_background;
+    float roulette;
+    int32_t firefly, accumulate;
+    int32_t resolution_level;
+};
+
+struct ref_reservoir {  // same layout as the C oracle's orc_reservoir
+    int32_t has_sample, has_lc, light, origin, vis_tested, pdf_solid, m;
+    float dir[3], color[3], normal[3];
+    float dist, pdf, target, wsum, w;
+    float tp[4];
+};
+
+struct RefScene {
+    Scene scene;
+    std::vector<std::unique_ptr<RefMesh>> meshes;
+    FrameBuffersMap store;
+    std::unordered_map<const ILight *, int> light_index;
+    std::string error;
+};
+
+extern "C" {
+
+RefScene *ref_create(const hdr_scene_desc *d) {
+    auto *rs = new RefScene();
+    try {
+        // one reference BVH per desc mesh, copied into every instance subset
+        std::vector<MeshSubset> protos((size_t)d->num_meshes);
+        std::vector<VtVec3fArray> proto_points((size_t)d->num_meshes);
+        for (int mi = 0; mi < d->num_meshes; ++mi) {
+            const hdr_mesh_desc &m = d->meshes[mi];
+            VtVec3fArray pts((size_t)m.num_points);
+            for (int i = 0; i < m.num_points; ++i) pts[i] = GfVec3f(m.points[3 * i], m.points[3 * i + 1], m.points[3 * i + 2]);
+            VtVec3iArray idx((size_t)m.num_triangles);
+            for (int i = 0; i < m.num_triangles; ++i) idx[i] = GfVec3i(m.indices[3 * i], m.indices[3 * i + 1], m.indices[3 * i + 2]);
+            VtVec2fArray uvs((size_t)m.num_uvs);
+            for (int i = 0; i < m.num_uvs; ++i) uvs[i] = GfVec2f(m.uvs[2 * i], m.uvs[2 * i + 1]);
+            VtVec3fArray nrm((size_t)m.num_normals), col((size_t)m.num_colors);
+            for (int i = 0; i < m.num_normals; ++i) nrm[i] = GfVec3f(m.normals[3 * i], m.normals[3 * i + 1], m.normals[3 * i + 2]);
+            for (int i = 0; i < m.num_colors; ++i) col[i] = GfVec3f(m.colors[3 * i], m.colors[3 * i + 1], m.colors[3 * i + 2]);
+            MeshSubset &s = protos[mi];
+            s.indices = idx;
+            // HdRestirMesh::_rebuildSubsetsIfNeeded (hydra/hd_restir_mesh.cpp:516-531)
+            if (!idx.empty() && !pts.empty()) {
+                s.bvh.Build(pts, idx, uvs, nrm, col, std::vector<int>());
+                s.range.SetEmpty();
+                for (const auto &t : idx) {
+                    s.range.ExtendBy(pts[t[0]]);
+                    s.range.ExtendBy(pts[t[1]]);
+                    s.range.ExtendBy(pts[t[2]]);
+                }
+            }
+            proto_points[mi] = pts;
+        }
+        for (int k = 0; k < d->num_materials; ++k) {
+            const hdr_material_desc &p = d->materials[k];
+            PreviewSurfaceParams q;
+            q.DiffuseColor = GfVec3f(p.diffuse_color[0], p.diffuse_color[1], p.diffuse_color[2]);
+            q.Metallic = p.metallic;
+            q.Roughness = p.roughness;
+            q.SpecularColor = GfVec3f(p.specular_color[0], p.specular_color[1], p.specular_color[2]);
+            q.Specular = p.specular;
+            q.Opacity = p.opacity;
+            q.Ior = p.ior;
+            q.Transmission = p.transmission;
+            q.TransmissionColor = GfVec3f(p.transmission_color[0], p.transmission_color[1], p.transmission_color[2]);
+            q.TransmissionDepth = p.transmission_depth;
+            q.TransmissionScatter = GfVec3f(p.transmission_scatter[0], p.transmission_scatter[1], p.transmission_scatter[2]);
+            q.EmissionColor = GfVec3f(p.emission_color[0], p.emission_color[1], p.emission_color[2]);
+            q.Emission = p.emission;
+            q.Coat = p.coat;
+            q.CoatColor = GfVec3f(p.coat_color[0], p.coat_color[1], p.coat_color[2]);
+            q.CoatRoughness = p.coat_roughness;
+            q.CoatIor = p.coat_ior;
+            q.Sheen = p.sheen;
+            q.SheenColor = GfVec3f(p.sheen_color[0], p.sheen_color[1], p.sheen_color[2]);
+            q.SheenRoughness = p.sheen_roughness;
+            q.Subsurface = p.subsurface;
+            q.SubsurfaceColor = GfVec3f(p.subsurface_color[0], p.subsurface_color[1], p.subsurface_color[2]);
+            q.ThinWalled = p.thin_walled != 0;
+            rs->scene.SetMaterialParams(SdfPath(path_of("mat", k)), q);
+        }
+        for (int i = 0; i < d->num_instances; ++i) {
+            const hdr_instance_desc &in = d->instances[i];
+            if (in.light >= 0) {
+                rs->error = "light-linked geometry is not supported by the reference harness";
+                delete rs;
+                return nullptr;
+            }
+            auto m = std::make_unique<RefMesh>();
+            m->id = SdfPath(path_of("mesh", i));
+            for (int r = 0; r < 4; ++r)
+                for (int c = 0; c < 4; ++c) m->transform[r][c] = in.transform[4 * r + c];
+            m->points = proto_points[in.mesh];
+            MeshSubset s = protos[in.mesh];
+            s.materialId = in.material >= 0 ? SdfPath(path_of("mat", in.material)) : SdfPath();
+            m->subsets.push_back(std::move(s));
+            rs->scene.AddMesh(m->id, m.get());
+            rs->meshes.push_back(std::move(m));
+        }
+        for (int k = 0; k < d->num_lights; ++k) {
+            const hdr_light_desc &L = d->lights[k];
+            LightFactoryInput li;
+            li.Id = SdfPath(path_of("light", k));
+            li.Type = (LightType)L.type;
+            li.Params.Color = GfVec3f(L.color[0], L.color[1], L.color[2]);
+            li.Params.Intensity = L.intensity;
+            li.Params.Exposure = L.exposure;
+            for (int r = 0; r < 4; ++r)
+                for (int c = 0; c < 4; ++c) li.Params.Transform[r][c] = L.transform[4 * r + c];
+            li.Params.Width = L.width;
+            li.Params.Height = L.height;
+            li.Params.ShapingConeAngle = L.shaping_cone_angle;
+            li.Params.ShapingConeSoftness = L.shaping_cone_softness;
+            if (L.texture && L.tex_width > 0 && L.tex_height > 0) {
+                const std::string tex = "mem://" + li.Id.GetString();
+                HioImage::Register(tex, L.tex_width, L.tex_height, L.texture);
+                li.Params.TextureFile = SdfAssetPath(tex);
+            }
+            rs->scene.SetLightFactoryInput(li.Id, li);
+        }
+        rs->scene.BuildRenderState(SceneBuildRenderStateConfig{}, GetMainThreadRenderJob());
+        const auto lights = rs->scene.GetLights();
+        for (size_t k = 0; k < lights.size(); ++k) rs->light_index[lights[k]] = (int)k;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_create: %s\n", e.what());
+        delete rs;
+        return nullptr;
+    }
+    return rs;
+}
+
+void ref_destroy(RefScene *rs) { delete rs; }
+
+void ref_clear_persistent(RefScene *rs) { rs->store.Clear(); }
+
+static void texel_from_hit(hdr_gbuffer_texel &t, const std::optional<HitRecord> &h) {
+    std::memset(&t, 0, sizeof(t));
+    t.tri_id = -1;
+    if (!h) {
+        t.depth = 3.402823466e+38f;
+        t.prim_id = -1;
+        return;
+    }
+    for (int i = 0; i < 3; ++i) {
+        t.position[i] = h->Position[i];
+        t.normal[i] = h->Normal[i];
+        t.smooth_normal[i] = h->SmoothNormal[i];
+        t.albedo[i] = h->Albedo[i];
+        t.dpdu[i] = h->Dpdu[i];
+        t.dpdv[i] = h->Dpdv[i];
+    }
+    t.depth = h->Depth;
+    t.prim_id = h->PrimId;
+    t.hit = 1;
+    t.uv[0] = h->Uv[0];
+    t.uv[1] = h->Uv[1];
+}
+
+// One frame through the reference passes. Outputs may be NULL; sizes are
+// RenderedWidth x RenderedHeight of the chosen resolution level.
+int ref_render_frame(RefScene *rs, const hdr_camera *cam, int frame_index, const ref_params *p,
+                     hdr_gbuffer_texel *gbuf_out, float *color_out, ref_reservoir *res_out) {
+    try {
+        GfMatrix4d view, proj;
+        for (int r = 0; r < 4; ++r)
+            for (int c = 0; c < 4; ++c) view[r][c] = cam->view[4 * r + c], proj[r][c] = cam->proj[4 * r + c];
+        std::optional<CameraParams> cp;
+        if (cam->has_params) {
+            CameraParams q;
+            q.enableDoF = cam->enable_dof != 0;
+            q.enableExposure = cam->enable_exposure != 0;
+            q.focalLength = cam->focal_length;
+            q.fStop = cam->f_stop;
+            q.focusDistance = cam->focus_distance;
+            q.bokehBlades = cam->bokeh_blades;
+            q.lensDistortion = cam->lens_distortion;
+            q.iso = cam->iso;
+            q.shutterSpeed = cam->shutter_speed;
+            cp = q;
+        }
+        Rng rng{static_cast<std::uint32_t>(frame_index)};
+        RenderContext ctx{
+            .scene = &rs->scene,
+            .viewMatrix = view,
+            .projMatrix = proj,
+            .frame = CameraFrame{.windowWidth = cam->width, .windowHeight = cam->height,
+                                 .resolutionLevel = p->resolution_level, .visibleMinX = 0, .visibleMinY = 0,
+                                 .visibleMaxX = cam->width, .visibleMaxY = cam->height},
+            .frameIndex = frame_index,
+            .rng = rng,
+            .buffers = FrameBuffersMap{},
+            .OutputNames = {"Color"},
+            .cameraParams = cp,
+        };
+        PathTracePassSettings settings;
+        settings.EnableSubsurface = p->enable_subsurface != 0;
+        settings.MaxReflectionBounces = p->max_refl;
+        settings.MaxRefractionBounces = p->max_refr;
+        settings.RenderIblBackground = p->render_ibl_background != 0;
+        settings.RouletteAggressiveness = p->roulette;
+        RaycastPass raycast{};
+        std::unique_ptr<RenderPass> integ;
+        if (p->pipeline == 1)
+            integ = std::make_unique<RISPathTracePass>(p->candidate_count, p->use_reservoir != 0,
+                                                       p->skip_visibility != 0, settings, p->max_depth);
+        else
+            integ = std::make_unique<PathTracePass>(settings, p->max_depth);
+        AccumulationPass accum{p->firefly != 0};
+        // RenderPipeline::Execute (pipeline/render_pipeline.cpp:24-40)
+        ctx.buffers.InjectFrom(rs->store);
+        raycast.Execute(ctx);
+        integ->Execute(ctx);
+        if (p->accumulate) accum.Execute(ctx);
+        ctx.buffers.ExtractPersistentTo(rs->store);
+
+        const size_t n = ctx.frame.PixelCount();
+        if (gbuf_out) {
+            auto g = ctx.buffers.Get<std::optional<HitRecord>>("GBuffer");
+            for (size_t i = 0; i < n; ++i) texel_from_hit(gbuf_out[i], g[i]);
+        }
+        if (color_out) {
+            auto c = ctx.buffers.Get<GfVec4f>("Color");
+            for (size_t i = 0; i < n; ++i)
+                for (int k = 0; k < 4; ++k) color_out[4 * i + k] = c[i][k];
+        }
+        if (res_out && rs->store.Has(kReservoirBufferName)) {
+            using ResT = WeightedReservoir<RisDirectLightIntegrator::Candidate>;
+            auto rb = rs->store.GetFrameBuffer(kReservoirBufferName).As<ResT>();
+            for (size_t i = 0; i < n; ++i) {
+                const ResT &r = rb[i];
+                ref_reservoir &o = res_out[i];
+                std::memset(&o, 0, sizeof(o));
+                o.light = -1;
+                o.m = r.CandidateCount;
+                o.wsum = r.WSum;
+                o.w = r.W;
+                if (!r.ChosenSample) continue;
+                const auto &cs = *r.ChosenSample;
+                o.has_sample = 1;
+                o.origin = (int)cs.Origin;
+                o.vis_tested = cs.VisibilityTested ? 1 : 0;
+                o.target = (float)cs.targetFunction;
+                for (int k = 0; k < 4; ++k) o.tp[k] = cs.Throughput[k];
+                if (cs.Candidate) {
+                    const LightCandidate &lc = *cs.Candidate;
+                    o.has_lc = 1;
+                    auto it = rs->light_index.find(lc.Light.get());
+                    o.light = it == rs->light_index.end() ? -2 : it->second;
+                    for (int k = 0; k < 3; ++k) {
+                        o.dir[k] = lc.Ls.Dir[k];
+                        o.color[k] = lc.Ls.Color[k];
+                        o.normal[k] = lc.Ls.LightNormal[k];
+                    }
+                    o.dist = lc.Ls.Dist;
+                    o.pdf = lc.Ls.Pdf.value;
+                    o.pdf_solid = lc.Ls.Pdf.space == PdfSpace::SolidAngle ? 1 : 0;
+                }
+            }
+        }
+        return (int)n;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_render_frame: %s\n", e.what());
+        return -1;
+    }
+}
+
+int ref_trace_rays(RefScene *rs, const float *rays, int n, hdr_gbuffer_texel *out) {
+    for (int k = 0; k < n; ++k) {
+        const GfVec3f o(rays[6 * k], rays[6 * k + 1], rays[6 * k + 2]);
+        const GfVec3f d(rays[6 * k + 3], rays[6 * k + 4], rays[6 * k + 5]);
+        texel_from_hit(out[k], rs->scene.IntersectScene(o, d));
+    }
+    return n;
+}
+
+void ref_rng_floats(const uint32_t *seeds, int n, int count, float *out) {
+    for (int k = 0; k < n; ++k) {
+        Rng r{seeds[k]};
+        for (int j = 0; j < count; ++j) out[(size_t)k * count + j] = r.NextFloat();
+    }
+}
+
+// WeightedReservoir known answers of tests/test_reservoir.cpp, run on the
+// reference type itself: returns W of (weight 6, p-hat 3, one candidate).
+float ref_reservoir_known_answer(float weight, float phat, int candidates_per_frame) {
+    struct S {
+        int id;
+        float targetFunction;
+    };
+    WeightedReservoir<S> r{};
+    Rng rng{777u};
+    r.Update(S{0, phat}, weight, rng);
+    r.Finalize(candidates_per_frame);
+    return r.W;
+}
+
+const char *ref_version(void) { return "hdRestir reference sources compiled in place with the oracle shim"; }
+
+}  // extern "C"

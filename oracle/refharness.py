@@ -1,0 +1,155 @@
+"""ctypes wrapper of the reference's own hot-path sources compiled in place
+(oracle/_ref/libhdr_ref.so, built by ``make -C oracle ref`` where the reference
+tree is present) — TEST INFRASTRUCTURE.
+
+Used to pin the C oracle (tests/test_oracle_pin.py), to generate the golden
+fixtures, and as bench.py's CPU baseline when the library is available.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_ref" / "libhdr_ref.so"
+REFERENCE_TREE = Path(os.environ.get("HDR_REFERENCE_TREE", "/root/reference"))
+
+import sys  # noqa: E402
+
+sys.path.insert(0, str(HERE.parent))
+from hdrestir_b200 import abi  # noqa: E402
+from oracle.oracle import RESERVOIR_DTYPE  # noqa: E402
+
+
+class RefParams(C.Structure):
+    _fields_ = [("pipeline", C.c_int32), ("candidate_count", C.c_int32), ("use_reservoir", C.c_int32),
+                ("skip_visibility", C.c_int32), ("max_depth", C.c_int32), ("enable_subsurface", C.c_int32),
+                ("max_refl", C.c_int32), ("max_refr", C.c_int32), ("render_ibl_background", C.c_int32),
+                ("roulette", C.c_float), ("firefly", C.c_int32), ("accumulate", C.c_int32),
+                ("resolution_level", C.c_int32)]
+
+
+def available() -> bool:
+    return LIB.exists()
+
+
+def build() -> bool:
+    """Builds the in-place reference library when the reference tree is present."""
+    if not (REFERENCE_TREE / "source" / "restir").exists():
+        return LIB.exists()
+    subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REFERENCE_TREE}", "ref", f"-j{os.cpu_count() or 4}"],
+                   check=True)
+    return LIB.exists()
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            raise RuntimeError(f"{LIB} is not built (needs the reference tree: make -C oracle ref)")
+        L = C.CDLL(str(LIB))
+        vp = C.c_void_p
+        L.ref_create.restype = vp
+        L.ref_create.argtypes = [C.POINTER(abi.SceneDesc)]
+        L.ref_destroy.argtypes = [vp]
+        L.ref_clear_persistent.argtypes = [vp]
+        L.ref_render_frame.restype = C.c_int
+        L.ref_render_frame.argtypes = [vp, C.POINTER(abi.CameraDesc), C.c_int, C.POINTER(RefParams), vp, vp, vp]
+        L.ref_trace_rays.argtypes = [vp, vp, C.c_int, vp]
+        L.ref_rng_floats.argtypes = [vp, C.c_int, C.c_int, vp]
+        L.ref_reservoir_known_answer.restype = C.c_float
+        L.ref_reservoir_known_answer.argtypes = [C.c_float, C.c_float, C.c_int]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Reference:
+    """The reference's Scene + passes for one scene description."""
+
+    def __init__(self, scene):
+        self._lib = lib()
+        self._desc = scene.c_desc()
+        self._s = self._lib.ref_create(C.byref(self._desc))
+        if not self._s:
+            raise RuntimeError("reference harness rejected the scene")
+
+    def close(self):
+        if self._s:
+            self._lib.ref_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def clear_persistent(self):
+        self._lib.ref_clear_persistent(self._s)
+
+    def render(self, cam, frame, ris=False, candidate_count=16, use_reservoir=True, skip_visibility=False,
+               max_depth=32, firefly=True, accumulate=True, resolution_level=0, enable_subsurface=True,
+               max_reflection_bounces=8, max_refraction_bounces=8, render_ibl_background=True,
+               roulette_aggressiveness=1.0, outputs=("gbuf", "color", "res")):
+        div = 1 << max(0, min(4, resolution_level))
+        w, h = max(1, (cam.width + div - 1) // div), max(1, (cam.height + div - 1) // div)
+        n = w * h
+        g = np.zeros(n, abi.GBUFFER_DTYPE) if "gbuf" in outputs else None
+        c = np.zeros((n, 4), np.float32) if "color" in outputs else None
+        r = np.zeros(n, RESERVOIR_DTYPE) if "res" in outputs else None
+        p = RefParams(1 if ris else 0, candidate_count, int(use_reservoir), int(skip_visibility), max_depth,
+                      int(enable_subsurface), max_reflection_bounces, max_refraction_bounces,
+                      int(render_ibl_background), roulette_aggressiveness, int(firefly), int(accumulate),
+                      resolution_level)
+        got = self._lib.ref_render_frame(self._s, C.byref(cam.c_desc()), int(frame), C.byref(p), _p(g), _p(c), _p(r))
+        if got != n:
+            raise RuntimeError(f"reference render failed ({got})")
+        return g, c, r
+
+    def trace_rays(self, rays):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        out = np.zeros(len(rays), abi.GBUFFER_DTYPE)
+        self._lib.ref_trace_rays(self._s, _p(rays), len(rays), _p(out))
+        return out
+
+
+def rng_floats(seeds, count) -> np.ndarray:
+    seeds = np.ascontiguousarray(seeds, np.uint32)
+    out = np.empty((len(seeds), count), np.float32)
+    lib().ref_rng_floats(_p(seeds), len(seeds), int(count), _p(out))
+    return out
+
+
+def cpu_sample(scene, cam, budget_s: float, threads: int, frame: int = 0):
+    """Times the reference pipeline (Raycast -> RISPathTrace(32, reservoir) ->
+    Accumulation) on the host cores at the coarsest resolution level whose
+    frame fits the budget; returns (seconds per full-resolution frame, rows)."""
+    os.environ["HDR_REF_THREADS"] = str(threads)
+    ref = Reference(scene)
+    level, sec = 4, None
+    while True:
+        div = 1 << level
+        rows = (cam.height + div - 1) // div
+        t0 = time.perf_counter()
+        ref.render(cam, frame, ris=True, candidate_count=32, use_reservoir=True, max_depth=1,
+                   resolution_level=level, outputs=())
+        dt = time.perf_counter() - t0
+        px = ((cam.width + div - 1) // div) * rows
+        sec = dt * (cam.width * cam.height) / px
+        if level == 0 or dt * 4 > budget_s:
+            break
+        level -= 1
+    ref.close()
+    return sec, rows

@@ -1,0 +1,2 @@
+#pragma once
+#include "pxr/base/gf/gf_shim.h"

@@ -1,0 +1,70 @@
+"""Live pin of the C oracle against the reference's own sources compiled in
+place (oracle/_ref). Skipped where that library has not been built (it needs
+the reference tree)."""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from hdrestir_b200 import configs
+from oracle import oracle as orc
+from oracle import refharness
+
+pytestmark = pytest.mark.skipif(not refharness.available(), reason="oracle/_ref not built (needs the reference tree)")
+REF_DIR = Path(refharness.__file__).resolve().parent / "_ref"
+
+
+def bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint32) if a.dtype == np.float32 else a
+
+
+@pytest.mark.parametrize("name", ["test_reservoir", "test_rng", "test_camera"])
+def test_reference_unit_tests_pass_on_the_shim(name):
+    """The reference's own unit tests, built against the same shim the oracle build uses."""
+    exe = REF_DIR / name
+    if not exe.exists():
+        pytest.skip(f"{name} not built")
+    assert subprocess.run([str(exe)], timeout=120).returncode == 0
+
+
+def test_rng_matches_reference_for_pixel_seeds():
+    seeds = (np.arange(4096, dtype=np.uint64) ^ np.uint64((7 * 12345) & 0xFFFFFFFF)).astype(np.uint32)
+    assert np.array_equal(bits(orc.rng_floats(seeds, 160)), bits(refharness.rng_floats(seeds, 160)))
+
+
+@pytest.mark.parametrize("cfg,kw", [
+    (0, dict(ris=False, max_depth=6)),
+    (1, dict(ris=True, candidate_count=8, use_reservoir=True, skip_visibility=True, max_depth=1)),
+    (2, dict(ris=True, candidate_count=4, use_reservoir=True, skip_visibility=False, max_depth=2)),
+    (2, dict(ris=False, max_depth=3)),
+])
+def test_oracle_equals_reference(cfg, kw):
+    extra = {1: dict(n_lights=64), 2: dict(grid=64, n_spheres=40, n_lights=100)}.get(cfg, {})
+    sc, cam = configs.small_variant(cfg, 40, 30, **extra)
+    ref = refharness.Reference(sc)
+    o = orc.Oracle(sc, threads=4)
+    for f in range(2):
+        g, c, r = ref.render(cam, f, accumulate=True, firefly=True, **kw)
+        assert np.array_equal(o.raycast(cam, f)["prim_id"], g["prim_id"])
+        o.integrate(cam, f, **kw)
+        o.accumulate(cam, f, firefly=True)
+        assert np.array_equal(bits(o.color), bits(c))
+        assert np.array_equal(o.res["m"], r["m"])
+
+
+def test_trace_rays_match_reference():
+    sc, cam = configs.small_variant(2, 16, 16, grid=64, n_spheres=40, n_lights=50)
+    rng = np.random.default_rng(3)
+    o = rng.uniform(-15, 15, (2000, 3)) + np.array([0, 4.0, 0])
+    d = rng.normal(size=(2000, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.concatenate([o, d], 1).astype(np.float32)
+    a = orc.Oracle(sc).trace_rays(rays)
+    b = refharness.Reference(sc).trace_rays(rays)
+    assert np.array_equal(a["prim_id"], b["prim_id"])
+    hit = b["hit"] == 1
+    assert hit.sum() > 100
+    for field in ("position", "depth", "normal", "smooth_normal", "albedo"):
+        assert np.array_equal(bits(a[field][hit]), bits(b[field][hit])), field
