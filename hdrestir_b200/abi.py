@@ -74,7 +74,11 @@ class PathSettings(C.Structure):
 
 class RisParams(C.Structure):
     _fields_ = [("path", PathSettings), ("candidate_count", _i), ("use_reservoir", _i), ("skip_visibility", _i),
-                ("m_cap", _i), ("spatial_neighbors", _i), ("spatial_radius", _f), ("reserved", _i * 2)]
+                ("m_cap", _i), ("spatial_neighbors", _i), ("spatial_radius", _f), ("flags", C.c_uint32),
+                ("reserved", _i)]
+
+
+RIS_TRACE_ALL_RAYS, RIS_ONE_KERNEL = 1, 2
 
 
 class CtxDesc(C.Structure):

@@ -66,12 +66,13 @@ class Context:
         self.width, self.height = cam.width, cam.height
 
     def ris_path_trace(self, cam: Camera, frame_index: int, candidate_count=16, use_reservoir=True,
-                       skip_visibility=False, m_cap=0, **settings) -> None:
+                       skip_visibility=False, m_cap=0, trace_all_rays=False, one_kernel=False, **settings) -> None:
         p = abi.RisParams()
         p.path = path_settings(**settings)
         p.candidate_count, p.use_reservoir, p.skip_visibility = int(candidate_count), int(use_reservoir), int(
             skip_visibility)
         p.m_cap = int(m_cap)
+        p.flags = (abi.RIS_TRACE_ALL_RAYS if trace_all_rays else 0) | (abi.RIS_ONE_KERNEL if one_kernel else 0)
         abi.check(self._lib.hdr_ris_path_trace(self._h, C.byref(cam.c_desc()), int(frame_index), C.byref(p)))
 
     def path_trace(self, cam: Camera, frame_index: int, **settings) -> None:

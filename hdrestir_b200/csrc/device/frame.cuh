@@ -66,6 +66,25 @@ struct PathParamsD {
     float roulette;
 };
 
+// Scratch of the wavefront RISPathTracePass (per frame, not persistent).
+struct WaveBuffers {
+    float4 *q_closest;    // 2 per entry: origin.xyz + slot bits | direction.xyz
+    float4 *q_shadow;     // 2 per entry: origin.xyz + slot bits | direction.xyz + distance limit
+    int *counts;          // [0] closest-hit queue length, [1] shadow queue length
+    float4 *hits;         // pixels * n_closest: t, instance bits, triangle bits, u
+    float *hit_v;         // pixels * n_closest
+    unsigned char *occ;   // pixels * n_shadow
+    uint4 *rng_state;     // 3 planes of pixels: stream state at the end of candidate generation
+    unsigned char *done;  // pixels: 1 = no GBuffer hit, colour already written
+    size_t pixels;
+    int n_closest, n_shadow;
+};
+
+// Returns the number of kernels launched, or -1 on a launch error.
+int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                         GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
+                         unsigned *err, cudaStream_t st);
+
 void launch_raycast(const DeviceScene &s, const CameraD &cam, int frame_index, GBufferView gb, AovView aov,
                     unsigned *err, cudaStream_t st);
 void launch_trace_rays(const DeviceScene &s, const float *rays, const float *tmax, int n, int any_hit,

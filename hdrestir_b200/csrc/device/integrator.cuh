@@ -52,6 +52,45 @@ __device__ __forceinline__ bool occluded(const DeviceScene &s, V3 o, V3 d, float
     return trace_ray<true>(s, o, d, limit, id, err) && id.t < limit;
 }
 
+// Where the integrators get ray results from. Every ray a pixel casts has a
+// slot: closest-hit slot 0 is the path's bounce ray, closest-hit slot 1 + k
+// the k-th generated BSDF candidate, shadow slot j the j-th NEE candidate.
+// TraceNow traverses at the call (one thread per pixel); TracedResults reads
+// what the wavefront trace kernels wrote for the pixel's slots.
+struct TraceNow {
+    const DeviceScene *s;
+    __device__ __forceinline__ bool shadow(int, V3 o, V3 d, float limit, unsigned &err) const {
+        return occluded(*s, o, d, limit, err);
+    }
+    __device__ __forceinline__ bool closest(int, V3 o, V3 d, Hit &h, unsigned &err) const {
+        return intersect(*s, o, d, h, err);
+    }
+    __device__ __forceinline__ bool winner_shadow(V3 o, V3 d, float limit, unsigned &err) const {
+        return occluded(*s, o, d, limit, err);
+    }
+};
+
+struct TracedResults {
+    const DeviceScene *s;
+    const float4 *hits;        // this pixel's closest-hit slots: t, instance bits, triangle bits, u
+    const float *hit_v;        // and v
+    const unsigned char *occ;  // this pixel's shadow slots
+    bool bsdf_traced;          // false: BSDF-candidate slots were not cast (their result cannot matter)
+    __device__ __forceinline__ bool shadow(int slot, V3, V3, float, unsigned &) const { return occ[slot] != 0; }
+    __device__ __forceinline__ bool closest(int slot, V3 o, V3 d, Hit &h, unsigned &) const {
+        if (slot > 0 && !bsdf_traced) return false;
+        const float4 r = hits[slot];
+        const HitId id{r.x, fbits(r.y), fbits(r.z), r.w, hit_v[slot]};
+        if (id.inst < 0) return false;
+        h = make_hit(*s, o, d, id);
+        return true;
+    }
+    // the winner's visibility test of a skipVisibility selection is cast on the spot
+    __device__ __forceinline__ bool winner_shadow(V3 o, V3 d, float limit, unsigned &err) const {
+        return occluded(*s, o, d, limit, err);
+    }
+};
+
 __device__ __forceinline__ Surface make_surface(const DeviceScene &s, V3 ro, V3 rd, const Hit &h, const Closure &c,
                                                 bool inside) {
     Surface sf;
@@ -64,15 +103,36 @@ __device__ __forceinline__ Surface make_surface(const DeviceScene &s, V3 ro, V3 
     return sf;
 }
 
+// GBuffer texel -> HitRecord (the "GBuffer" input of IntegrationPass, integration_pass.cpp:184)
+__device__ inline bool load_gbuffer_hit(const DeviceScene &s, const GBufferView &gb, size_t i, Hit &h) {
+    const float4 a = gb.pos_depth[i], b = gb.normal_prim[i], c = gb.smooth_tri[i], d = gb.albedo_uv[i];
+    h.prim = fbits(b.w);
+    if (h.prim < 0) return false;
+    h.position = V3{a.x, a.y, a.z};
+    h.depth = a.w;
+    h.normal = V3{b.x, b.y, b.z};
+    h.smooth_normal = V3{c.x, c.y, c.z};
+    h.tri = fbits(c.w);
+    h.albedo = V3{d.x, d.y, d.z};
+    h.uv = V2{d.w, 0.0f};
+    h.dpdu = h.dpdv = v3s(0.0f);
+    const float4 r = __ldg(&s.instances[8 * h.prim + 6]);
+    const float4 r7 = __ldg(&s.instances[8 * h.prim + 7]);
+    h.material = fbits(r.w);
+    h.light = fbits(r7.x);
+    return true;
+}
+
 // Detail::SampleBounceWithConnection
-__device__ __forceinline__ Connection sample_bounce_with_connection(const DeviceScene &s, const Surface &sf,
+template <class RP>
+__device__ __forceinline__ Connection sample_bounce_with_connection(const RP &rp, int slot, const Surface &sf,
                                                                     int max_refl, int max_refr, BounceState &st,
                                                                     const SpectralCtx &sc, MtStream &rng,
                                                                     unsigned &err) {
     Connection cn;
     cn.b = sample_bounce(sf.c, sf.sn, sf.inside, sf.hit.position, sf.ray_d, max_refl, max_refr, st, sc, rng);
     cn.has_hit = false;
-    if (cn.b.ok) cn.has_hit = intersect(s, cn.b.origin, cn.b.dir, cn.hit, err);
+    if (cn.b.ok) cn.has_hit = rp.closest(slot, cn.b.origin, cn.b.dir, cn.hit, err);
     return cn;
 }
 
@@ -204,10 +264,11 @@ struct RisContrib {  // RisDirectLightIntegrator::MISContrib
     bool vis_tested;
 };
 
-// _evaluateLightSample (:628-673)
-__device__ inline RisContrib ris_evaluate_light_sample(const DeviceScene &s, const Surface &sf, int li,
-                                                const LightSampleD &ls, bool skip_vis, const SpectralCtx &sc,
-                                                unsigned &err) {
+// _evaluateLightSample (:628-673). shadow_slot < 0: the winner's own test.
+template <class RP>
+__device__ inline RisContrib ris_evaluate_light_sample(const DeviceScene &s, const RP &rp, int shadow_slot,
+                                                       const Surface &sf, int li, const LightSampleD &ls,
+                                                       bool skip_vis, const SpectralCtx &sc, unsigned &err) {
     const V3 wo = -sf.ray_d;
     const float n_l = dot(sf.sn, ls.dir);
     const float dist2 = ls.dist * ls.dist;
@@ -224,9 +285,29 @@ __device__ inline RisContrib ris_evaluate_light_sample(const DeviceScene &s, con
         r.vis_tested = false;
         return r;
     }
-    if (occluded(s, sf.hit.position + sf.sn * 1e-4f, ls.dir, ls.dist - 1e-3f, err)) return r;
+    const V3 so = sf.hit.position + sf.sn * 1e-4f;
+    const float lim = ls.dist - 1e-3f;
+    const bool occ = shadow_slot >= 0 ? rp.shadow(shadow_slot, so, ls.dir, lim, err) : rp.winner_shadow(so, ls.dir, lim, err);
+    if (occ) return r;
     r.emission = rgb_to_spectrum(ls.color, sc.up);
     return r;
+}
+
+// The shadow ray _evaluateLightSample would cast for a fresh NEE sample, or
+// false when its early-outs (or skipVisibility) mean none is cast.
+__device__ __forceinline__ bool ris_nee_shadow_ray(const DeviceScene &s, const Surface &sf, int li,
+                                                   const LightSampleD &ls, bool skip_vis, V3 &o, V3 &d,
+                                                   float &limit) {
+    const float n_l = dot(sf.sn, ls.dir);
+    const float dist2 = ls.dist * ls.dist;
+    const float cos_y = smaxf(0.0f, dot(-ls.dir, ls.normal));
+    const float p_nee = pdf_to_solid_angle(ls.pdf, ls.pdf_solid_angle, dist2, smaxf(cos_y, 1e-6f));
+    const bool delta = light_is_delta(s, li);
+    if (n_l <= 0.0f || p_nee <= 0.0f || (cos_y <= 0.0f && !delta) || skip_vis) return false;
+    o = sf.hit.position + sf.sn * 1e-4f;
+    d = ls.dir;
+    limit = ls.dist - 1e-3f;
+    return true;
 }
 
 // _reEvaluateForTemporalReuse (:675-691)
@@ -284,8 +365,10 @@ __device__ inline RisContrib ris_evaluate_bsdf_connection(const DeviceScene &s, 
     return r;
 }
 
+template <class RP>
 struct RisCtx {
     const DeviceScene *s;
+    const RP *rp;
     const Surface *sf;
     const SpectralCtx *sc;
     RisStrategy strat;
@@ -298,8 +381,8 @@ struct RisCtx {
 
 // Candidate j of allCandidates: NEE (sampler), then sky NEE, then BSDF.
 // kFull = false only advances the stream exactly like the full generation.
-template <bool kFull>
-__device__ Cand ris_candidate(const RisCtx &x, int j, MtStream &rng, unsigned &err) {
+template <bool kFull, class RP>
+__device__ Cand ris_candidate(const RisCtx<RP> &x, int j, MtStream &rng, unsigned &err) {
     const DeviceScene &s = *x.s;
     const Surface &sf = *x.sf;
     const SpectralCtx &sc = *x.sc;
@@ -313,7 +396,7 @@ __device__ Cand ris_candidate(const RisCtx &x, int j, MtStream &rng, unsigned &e
         int li;
         LightSampleD ls;
         if (!propose_candidate(s, sf.hit.position, rng, li, ls)) return c;
-        const RisContrib nee = ris_evaluate_light_sample(s, sf, li, ls, x.strat.skip_vis, sc, err);
+        const RisContrib nee = ris_evaluate_light_sample(s, *x.rp, j, sf, li, ls, x.strat.skip_vis, sc, err);
         const Spec contribution = nee.emission * nee.tmul;
         const float target = spectrum_luminance(contribution, sc.cie);
         const float mis = nee.use_mis ? power_heuristic3(nee.p_nee, x.strat.n_nee, 0.0f, x.strat.n_sky, nee.p_bsdf,
@@ -364,7 +447,8 @@ __device__ Cand ris_candidate(const RisCtx &x, int j, MtStream &rng, unsigned &e
         (void)sample_bounce(sf.c, sf.sn, sf.inside, sf.hit.position, sf.ray_d, 1, 1, st, sc, rng);
         return c;
     }
-    const Connection cn = sample_bounce_with_connection(s, sf, 1, 1, st, sc, rng, err);
+    const int fresh = j - (x.conn_cand ? 1 : 0);  // index among the generated BSDF candidates
+    const Connection cn = sample_bounce_with_connection(*x.rp, 1 + fresh, sf, 1, 1, st, sc, rng, err);
     if (!cn.b.ok) return c;
     if (!cn.has_hit) {
         if (s.env_light < 0) return c;
@@ -488,15 +572,21 @@ struct RisRun {
 };
 
 // RisDirectLightIntegrator::Li, per-bounce form (:230-361). primary == (callId.id < callId.stride).
-__device__ inline Spec ris_direct_li(const DeviceScene &s, const Surface &sf, bool has_conn, const Connection &cn,
-                              const SpectralCtx &sc, MtStream &rng, bool primary, const RisRun &run,
-                              const ReservoirView &rv, size_t pixel, unsigned &err) {
+// gen_end: the stream state right after candidate generation when the caller
+// already knows it (the wavefront generate kernel saved it); NULL replays the
+// sampling decisions to find it.
+template <class RP>
+__device__ inline Spec ris_direct_li(const DeviceScene &s, const RP &rp, const Surface &sf, bool has_conn,
+                                     const Connection &cn, const SpectralCtx &sc, MtStream &rng, bool primary,
+                                     const RisRun &run, const ReservoirView &rv, size_t pixel,
+                                     const MtStream *gen_end_state, unsigned &err) {
     // technique split (:239-246); every supported environment is a scene light,
     // so the sampler covers it and there is no separate sky technique
     const int N = run.candidate_count;
     const int n_tech = 2;
-    RisCtx x;
+    RisCtx<RP> x;
     x.s = &s;
+    x.rp = &rp;
     x.sf = &sf;
     x.sc = &sc;
     x.strat.n_nee = smaxi(1, N / n_tech);
@@ -511,8 +601,13 @@ __device__ inline Spec ris_direct_li(const DeviceScene &s, const Surface &sf, bo
 
     if (run.use_reservoir && primary) {
         // ---- reservoir branch (:267-331)
-        MtStream upd = rng;  // replay the sampling draws to find the first update draw
-        for (int j = 0; j < x.n_total; ++j) (void)ris_candidate<false>(x, j, upd, err);
+        MtStream upd = rng;
+        if (gen_end_state) {
+            upd = *gen_end_state;
+            upd.spill = rng.spill;
+        } else {  // replay the sampling draws to find the first update draw
+            for (int j = 0; j < x.n_total; ++j) (void)ris_candidate<false>(x, j, upd, err);
+        }
         const uint32_t gen_end = upd.k;
         Reservoir r;
         r.chosen = cand_none();
@@ -557,7 +652,8 @@ __device__ inline Spec ris_direct_li(const DeviceScene &s, const Surface &sf, bo
         reservoir_finalize(r, x.n_total);
         // winner visibility (:309-321)
         if (r.chosen.valid && !r.chosen.vis_tested && r.chosen.has_lc) {
-            const RisContrib nee = ris_evaluate_light_sample(s, sf, r.chosen.light, r.chosen.ls, false, sc, err);
+            const RisContrib nee =
+                ris_evaluate_light_sample(s, rp, -1, sf, r.chosen.light, r.chosen.ls, false, sc, err);
             r.chosen.tp = nee.emission * nee.tmul;
             r.chosen.vis_tested = true;
         }
@@ -601,7 +697,7 @@ __device__ inline Spec ris_direct_li(const DeviceScene &s, const Surface &sf, bo
     const float W = (float)(wsum / (double)c.target);
     Spec tp = c.tp;
     if (!c.vis_tested && c.has_lc) {
-        const RisContrib nee = ris_evaluate_light_sample(s, sf, c.light, c.ls, false, sc, err);
+        const RisContrib nee = ris_evaluate_light_sample(s, rp, -1, sf, c.light, c.ls, false, sc, err);
         tp = nee.emission * nee.tmul;
     }
     return tp * W;
@@ -618,29 +714,32 @@ struct PathRun {
     float roulette;
 };
 
-template <bool kRis>
-__device__ __forceinline__ Spec direct_li(const DeviceScene &s, const Surface &sf, bool has_conn,
+template <bool kRis, class RP>
+__device__ __forceinline__ Spec direct_li(const DeviceScene &s, const RP &rp, const Surface &sf, bool has_conn,
                                           const Connection &cn, const SpectralCtx &sc, MtStream &rng, bool primary,
-                                          const RisRun &ris, const ReservoirView &rv, size_t pixel, unsigned &err) {
-    if (kRis) return ris_direct_li(s, sf, has_conn, cn, sc, rng, primary, ris, rv, pixel, err);
+                                          const RisRun &ris, const ReservoirView &rv, size_t pixel,
+                                          const MtStream *gen_end_state, unsigned &err) {
+    if (kRis) return ris_direct_li(s, rp, sf, has_conn, cn, sc, rng, primary, ris, rv, pixel, gen_end_state, err);
     return mis_direct_li(s, sf, has_conn, cn, sc, rng, err);
 }
 
-// _li (:92-209)
-template <bool kRis>
-__device__ Spec path_li_shaded(const DeviceScene &s, const Surface &sf0, const SpectralCtx &sc, MtStream &rng,
-                               const PathRun &pr, const RisRun &ris, const ReservoirView &rv, size_t pixel,
-                               unsigned &err) {
+// _li (:92-209). Later bounces query the scene directly (they only run in the
+// one-thread-per-pixel form).
+template <bool kRis, class RP>
+__device__ Spec path_li_shaded(const DeviceScene &s, const RP &rp, const Surface &sf0, const SpectralCtx &sc,
+                               MtStream &rng, const PathRun &pr, const RisRun &ris, const ReservoirView &rv,
+                               size_t pixel, const MtStream *gen_end_state, unsigned &err) {
     Spec total = rgb_to_spectrum(sf0.c.emission, sc.up);
     Spec tp = spec(1.0f);
     BounceState st{0, 0};
-    const Connection first = sample_bounce_with_connection(s, sf0, pr.max_refl, pr.max_refr, st, sc, rng, err);
-    total = total + direct_li<kRis>(s, sf0, first.b.ok, first, sc, rng, true, ris, rv, pixel, err);
+    const Connection first = sample_bounce_with_connection(rp, 0, sf0, pr.max_refl, pr.max_refr, st, sc, rng, err);
+    total = total + direct_li<kRis>(s, rp, sf0, first.b.ok, first, sc, rng, true, ris, rv, pixel, gen_end_state, err);
     if (!first.b.ok) return total;
     tp = tp * first.b.tmul;
     V3 ro = first.b.origin, rd = first.b.dir;
     bool has_next = first.has_hit;
     Hit next = first.hit;
+    const TraceNow now{&s};
     for (int bounce = 1; bounce < pr.max_depth; ++bounce) {
         if (!has_next) break;
         const Hit bh = next;
@@ -655,8 +754,8 @@ __device__ Spec path_li_shaded(const DeviceScene &s, const Surface &sf0, const S
         const bool inside = dot(c.normal, rd) > 0.0f;
         beer_absorption(tp, c, bh.depth, inside, sc);
         const Surface sf = make_surface(s, ro, rd, bh, c, inside);
-        const Connection cn = sample_bounce_with_connection(s, sf, pr.max_refl, pr.max_refr, st, sc, rng, err);
-        total = total + tp * direct_li<kRis>(s, sf, cn.b.ok, cn, sc, rng, false, ris, rv, pixel, err);
+        const Connection cn = sample_bounce_with_connection(now, 0, sf, pr.max_refl, pr.max_refr, st, sc, rng, err);
+        total = total + tp * direct_li<kRis>(s, now, sf, cn.b.ok, cn, sc, rng, false, ris, rv, pixel, nullptr, err);
         if (!cn.b.ok) break;
         tp = tp * cn.b.tmul;
         ro = cn.b.origin;
@@ -674,10 +773,10 @@ __device__ Spec path_li_shaded(const DeviceScene &s, const Surface &sf0, const S
 }
 
 // PathIntegrator::Li (:48-90): opacity skip at the GBuffer hit, Beer, then _li.
-template <bool kRis>
-__device__ Spec path_li(const DeviceScene &s, V3 ray_o, V3 ray_d, bool has_hit, Hit hit, const SpectralCtx &sc,
-                        MtStream &rng, const PathRun &pr, const RisRun &ris, const ReservoirView &rv, size_t pixel,
-                        unsigned &err) {
+template <bool kRis, class RP>
+__device__ Spec path_li(const DeviceScene &s, const RP &rp, V3 ray_o, V3 ray_d, bool has_hit, Hit hit,
+                        const SpectralCtx &sc, MtStream &rng, const PathRun &pr, const RisRun &ris,
+                        const ReservoirView &rv, size_t pixel, const MtStream *gen_end_state, unsigned &err) {
     Spec tp = spec(1.0f);
     while (has_hit) {
         Closure c = get_closure(s, hit);
@@ -686,7 +785,7 @@ __device__ Spec path_li(const DeviceScene &s, V3 ray_o, V3 ray_d, bool has_hit, 
             const bool inside = dot(c.normal, ray_d) > 0.0f;
             beer_absorption(tp, c, hit.depth, inside, sc);
             const Surface sf = make_surface(s, ray_o, ray_d, hit, c, inside);
-            return tp * path_li_shaded<kRis>(s, sf, sc, rng, pr, ris, rv, pixel, err);
+            return tp * path_li_shaded<kRis>(s, rp, sf, sc, rng, pr, ris, rv, pixel, gen_end_state, err);
         }
         has_hit = intersect(s, hit.position + ray_d * 1e-4f, ray_d, hit, err);
     }

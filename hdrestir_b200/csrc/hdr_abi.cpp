@@ -60,6 +60,8 @@ struct hdr_ctx {
     std::vector<DevBuf> scene_bufs;
     hdr::DeviceScene scene{};
     bool has_scene = false;
+    bool scene_opaque = true;          // every material has opacity >= 0.999 (no stochastic pass-through)
+    bool scene_light_geometry = false; // some instance is a light's geometry (GetLightAtHit can succeed)
 
     // named frame buffers
     std::map<std::string, DevBuf> buffers;
@@ -343,6 +345,12 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     HDR_CUDA(cudaStreamSynchronize(c->stream));
     c->scene = s;
     c->has_scene = true;
+    c->scene_opaque = true;
+    for (int i = 0; i < desc->num_materials; ++i)
+        if (!(desc->materials[i].opacity >= 0.999f)) c->scene_opaque = false;
+    c->scene_light_geometry = false;
+    for (int i = 0; i < desc->num_instances; ++i)
+        if (desc->instances[i].light >= 0) c->scene_light_geometry = true;
     return HDR_OK;
 }
 
@@ -417,6 +425,41 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
     d.spatial_neighbors = p->spatial_neighbors;
     d.spatial_radius = p->spatial_radius;
     const hdr::CameraD cd = make_camera(cam);
+    // wavefront form: direct light only (no later bounces) and no stochastic opacity
+    const bool wave = p->path.max_depth == 1 && c->scene_opaque && !(p->flags & HDR_RIS_ONE_KERNEL);
+    if (wave) {
+        const int n_nee = std::max(1, p->candidate_count / 2);
+        const int n_bsdf = std::max(0, p->candidate_count - n_nee);
+        hdr::WaveBuffers wb{};
+        wb.pixels = count;
+        wb.n_closest = 1 + n_bsdf;
+        wb.n_shadow = n_nee;
+        void *q;
+        if ((st = ensure_buffer(c, "__wave_q_closest", count * wb.n_closest * 32, &q)) != HDR_OK) return st;
+        wb.q_closest = (float4 *)q;
+        if ((st = ensure_buffer(c, "__wave_q_shadow", count * wb.n_shadow * 32, &q)) != HDR_OK) return st;
+        wb.q_shadow = (float4 *)q;
+        if ((st = ensure_buffer(c, "__wave_counts", 16, &q)) != HDR_OK) return st;
+        wb.counts = (int *)q;
+        if ((st = ensure_buffer(c, "__wave_hits", count * wb.n_closest * 16, &q)) != HDR_OK) return st;
+        wb.hits = (float4 *)q;
+        if ((st = ensure_buffer(c, "__wave_hit_v", count * wb.n_closest * 4, &q)) != HDR_OK) return st;
+        wb.hit_v = (float *)q;
+        if ((st = ensure_buffer(c, "__wave_occ", count * wb.n_shadow, &q)) != HDR_OK) return st;
+        wb.occ = (unsigned char *)q;
+        if ((st = ensure_buffer(c, "__wave_rng", count * 48, &q)) != HDR_OK) return st;
+        wb.rng_state = (uint4 *)q;
+        if ((st = ensure_buffer(c, "__wave_done", count, &q)) != HDR_OK) return st;
+        wb.done = (unsigned char *)q;
+        const int trace_bsdf =
+            ((p->flags & HDR_RIS_TRACE_ALL_RAYS) || c->scene_light_geometry || c->scene.env_light >= 0) ? 1 : 0;
+        if ((st = begin_pass(c, 1)) != HDR_OK) return st;
+        const int n = hdr::launch_ris_wavefront(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color,
+                                                trace_bsdf, c->d_err, c->stream);
+        if (n < 0) return fail(HDR_ECUDA, "wavefront launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        c->launches += (uint64_t)n;
+        return end_pass(c, 1);
+    }
     if ((st = begin_pass(c, 1)) != HDR_OK) return st;
     hdr::launch_ris_path_trace(c->scene, cd, frame_index, d, gb, rv, (float4 *)color, c->d_err, c->stream);
     c->launches += 1;

@@ -10,25 +10,6 @@
 
 namespace hdr {
 
-__device__ __forceinline__ bool load_gbuffer_hit(const DeviceScene &s, const GBufferView &gb, size_t i, Hit &h) {
-    const float4 a = gb.pos_depth[i], b = gb.normal_prim[i], c = gb.smooth_tri[i], d = gb.albedo_uv[i];
-    h.prim = fbits(b.w);
-    if (h.prim < 0) return false;
-    h.position = V3{a.x, a.y, a.z};
-    h.depth = a.w;
-    h.normal = V3{b.x, b.y, b.z};
-    h.smooth_normal = V3{c.x, c.y, c.z};
-    h.tri = fbits(c.w);
-    h.albedo = V3{d.x, d.y, d.z};
-    h.uv = V2{d.w, 0.0f};
-    h.dpdu = h.dpdv = v3s(0.0f);
-    const float4 r = __ldg(&s.instances[8 * h.prim + 6]);
-    const float4 r7 = __ldg(&s.instances[8 * h.prim + 7]);
-    h.material = fbits(r.w);
-    h.light = fbits(r7.x);
-    return true;
-}
-
 template <bool kRis>
 __global__ void __launch_bounds__(256) integrate_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
                                                         RisRun ris, GBufferView gb, ReservoirView rv, float4 *color,
@@ -46,7 +27,8 @@ __global__ void __launch_bounds__(256) integrate_kernel(DeviceScene s, CameraD c
     unsigned e = 0;
     Hit h;
     const bool has = load_gbuffer_hit(s, gb, i, h);
-    const Spec L = path_li<kRis>(s, ray.o, ray.d, has, h, sc, rng, pr, ris, rv, i, e);
+    const TraceNow now{&s};
+    const Spec L = path_li<kRis>(s, now, ray.o, ray.d, has, h, sc, rng, pr, ris, rv, i, nullptr, e);
     V3 rgb = spectrum_to_rgb(L, sc.cie);
     if (cam.p.has_params && cam.p.enable_exposure) rgb = rgb * cam.p.exposure_mult;
     color[i] = make_float4(rgb.x, rgb.y, rgb.z, 1.0f);

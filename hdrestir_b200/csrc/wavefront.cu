@@ -1,0 +1,225 @@
+// RISPathTracePass as a wavefront (maxDepth 1, opaque materials): the same
+// per-pixel integrator as the one-thread-per-pixel kernel, with its rays cast
+// by dedicated traversal kernels instead of inside the shading code.
+//
+//   generate : per pixel, draws exactly the numbers IntegrationPass::_execute
+//              and RisDirectLightIntegrator draw while building the candidate
+//              list (integration_pass.cpp:210-226, ris_direct_light_integrator.cpp:
+//              230-262), and appends the rays those draws define to two
+//              compacted queues: closest-hit (the bounce ray, BSDF candidates)
+//              and shadow (one per NEE candidate that passes the early-outs of
+//              _evaluateLightSample, :628-658). It saves the stream state at the
+//              end of generation: the reservoir-update numbers start there.
+//   trace    : one thread per queued ray; closest hit or "occluded before the
+//              light" for the ray's slot.
+//   shade    : per pixel, repeats the same draws, reads the slot results instead
+//              of tracing, and runs the reference's resampling, temporal merge and
+//              colour write-back with the saved stream state supplying the
+//              update numbers.
+// The shade kernel checks that its own stream ends where generate's did.
+//
+// Rays whose result cannot reach the image are not queued unless the caller
+// asks for them: a generated BSDF candidate contributes only when its ray hits
+// light geometry or escapes to an environment, so a scene with neither makes
+// every such candidate an empty one whatever the ray hits.
+#include "device/integrator.cuh"
+
+namespace hdr {
+
+__device__ __forceinline__ int queue_append(int *counter, bool want) {
+    const unsigned active = __activemask();
+    const unsigned mask = __ballot_sync(active, want);
+    if (!want) return -1;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void store_stream(uint4 *st, size_t i, size_t n, const MtStream &r) {
+    st[i] = make_uint4((unsigned)r.a, (unsigned)(r.a >> 32), (unsigned)r.b, (unsigned)(r.b >> 32));
+    st[n + i] = make_uint4((unsigned)r.c, (unsigned)(r.c >> 32), (unsigned)r.d, (unsigned)(r.d >> 32));
+    st[2 * n + i] = make_uint4((unsigned)r.new0, (unsigned)(r.new0 >> 32), r.k, r.seed);
+}
+__device__ __forceinline__ MtStream load_stream(const uint4 *st, size_t i, size_t n) {
+    const uint4 p = st[i], q = st[n + i], w = st[2 * n + i];
+    MtStream r;
+    r.a = (uint64_t)p.x | ((uint64_t)p.y << 32);
+    r.b = (uint64_t)p.z | ((uint64_t)p.w << 32);
+    r.c = (uint64_t)q.x | ((uint64_t)q.y << 32);
+    r.d = (uint64_t)q.z | ((uint64_t)q.w << 32);
+    r.new0 = (uint64_t)w.x | ((uint64_t)w.y << 32);
+    r.k = w.z;
+    r.seed = w.w;
+    r.spill = nullptr;
+    return r;
+}
+
+// Per-pixel prologue shared by generate and shade: stream, jittered camera
+// ray, wavelengths, GBuffer hit (integration_pass.cpp:210-233).
+struct PixelStart {
+    size_t i;
+    RayF ray;
+    SpectralCtx sc;
+    Hit hit;
+    bool has_hit;
+};
+
+__device__ __forceinline__ bool pixel_start(const DeviceScene &s, const CameraD &cam, int frame_index,
+                                            const GBufferView &gb, MtStream &rng, uint64_t *spill, PixelStart &ps) {
+    int x, y;
+    if (!tile_pixel(cam.width, cam.height, x, y)) return false;
+    ps.i = (size_t)y * (size_t)cam.width + (size_t)x;
+    rng.init((uint32_t)ps.i ^ (uint32_t)((unsigned long long)frame_index * 12345ULL), spill);
+    const float px = (float)x + rng.next_float();
+    const float py = (float)y + rng.next_float();
+    ps.ray = camera_ray(cam, px, py, rng);
+    ps.sc = make_spectral_ctx(rng.next_float());
+    ps.has_hit = load_gbuffer_hit(s, gb, ps.i, ps.hit);
+    return true;
+}
+
+__global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
+                                                           RisRun ris, GBufferView gb, WaveBuffers wb, float4 *color,
+                                                           int trace_bsdf, unsigned *err) {
+    uint64_t spill[312];
+    MtStream rng;
+    PixelStart ps;
+    if (!pixel_start(s, cam, frame_index, gb, rng, spill, ps)) return;
+    const size_t i = ps.i;
+    if (!ps.has_hit) {  // PathIntegrator::Li without a hit: background only, no reservoir access
+        V3 rgb = v3s(0.0f);
+        if (s.env_light >= 0 && pr.render_ibl_background)
+            rgb = spectrum_to_rgb(rgb_to_spectrum(env_radiance(s, ps.ray.d), ps.sc.up), ps.sc.cie);
+        if (cam.p.has_params && cam.p.enable_exposure) rgb = rgb * cam.p.exposure_mult;
+        color[i] = make_float4(rgb.x, rgb.y, rgb.z, 1.0f);
+        wb.done[i] = 1;
+        return;
+    }
+    wb.done[i] = 0;
+    Closure c = get_closure(s, ps.hit);
+    if (!pr.enable_subsurface) c.subsurface = 0.0f;
+    const bool inside = dot(c.normal, ps.ray.d) > 0.0f;
+    const Surface sf = make_surface(s, ps.ray.o, ps.ray.d, ps.hit, c, inside);
+    const size_t cbase = i * (size_t)wb.n_closest, sbase = i * (size_t)wb.n_shadow;
+    // the path's bounce ray (_li, path_integrator.cpp:104-111)
+    BounceState st{0, 0};
+    const Bounce fb = sample_bounce(c, sf.sn, inside, ps.hit.position, ps.ray.d, pr.max_refl, pr.max_refr, st, ps.sc,
+                                    rng);
+    {
+        const int q = queue_append(&wb.counts[0], fb.ok);
+        if (q >= 0) {
+            wb.q_closest[2 * (size_t)q] = make_float4(fb.origin.x, fb.origin.y, fb.origin.z, __int_as_float((int)cbase));
+            wb.q_closest[2 * (size_t)q + 1] = make_float4(fb.dir.x, fb.dir.y, fb.dir.z, 0.0f);
+        }
+    }
+    // technique split and NEE candidates (:239-246, :553-589)
+    const int N = ris.candidate_count;
+    const int n_nee = smaxi(1, N / 2), n_bsdf = smaxi(0, N - n_nee);
+    for (int j = 0; j < n_nee; ++j) {
+        int li;
+        LightSampleD ls;
+        V3 o, d;
+        float lim = 0.0f;
+        const bool want = propose_candidate(s, ps.hit.position, rng, li, ls) &&
+                          ris_nee_shadow_ray(s, sf, li, ls, ris.skip_vis, o, d, lim);
+        const int q = queue_append(&wb.counts[1], want);
+        if (q >= 0) {
+            wb.q_shadow[2 * (size_t)q] = make_float4(o.x, o.y, o.z, __int_as_float((int)(sbase + j)));
+            wb.q_shadow[2 * (size_t)q + 1] = make_float4(d.x, d.y, d.z, lim);
+        }
+    }
+    // generated BSDF candidates (:442-450)
+    const int n_fresh = n_bsdf - ((fb.ok && fb.pdf > 0.0f) ? 1 : 0);
+    for (int k = 0; k < n_fresh; ++k) {
+        BounceState st2{0, 0};
+        const Bounce b = sample_bounce(c, sf.sn, inside, ps.hit.position, ps.ray.d, 1, 1, st2, ps.sc, rng);
+        const int q = queue_append(&wb.counts[0], b.ok && trace_bsdf);
+        if (q >= 0) {
+            wb.q_closest[2 * (size_t)q] = make_float4(b.origin.x, b.origin.y, b.origin.z,
+                                                      __int_as_float((int)(cbase + 1 + k)));
+            wb.q_closest[2 * (size_t)q + 1] = make_float4(b.dir.x, b.dir.y, b.dir.z, 0.0f);
+        }
+    }
+    store_stream(wb.rng_state, i, wb.pixels, rng);
+}
+
+__global__ void __launch_bounds__(128) trace_closest_kernel(DeviceScene s, const float4 *__restrict__ q,
+                                                            const int *counts, float4 *hits, float *hit_v,
+                                                            unsigned *err) {
+    const int n = counts[0];
+    unsigned e = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
+        HitId h;
+        trace_ray<false>(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, 0.0f, h, e);
+        const int slot = __float_as_int(a.w);
+        hits[slot] = make_float4(h.t, __int_as_float(h.inst), __int_as_float(h.tri), h.u);
+        hit_v[slot] = h.v;
+    }
+    if (e) atomicOr(err, e);
+}
+
+__global__ void __launch_bounds__(128) trace_shadow_kernel(DeviceScene s, const float4 *__restrict__ q,
+                                                           const int *counts, unsigned char *occ, unsigned *err) {
+    const int n = counts[1];
+    unsigned e = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
+        HitId h;
+        const bool hit = trace_ray<true>(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, b.w, h, e) && h.t < b.w;
+        occ[__float_as_int(a.w)] = hit ? 1 : 0;
+    }
+    if (e) atomicOr(err, e);
+}
+
+__global__ void __launch_bounds__(256) ris_shade_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
+                                                        RisRun ris, GBufferView gb, ReservoirView rv, WaveBuffers wb,
+                                                        float4 *color, int trace_bsdf, unsigned *err) {
+    uint64_t spill[312];
+    MtStream rng;
+    PixelStart ps;
+    if (!pixel_start(s, cam, frame_index, gb, rng, spill, ps)) return;
+    const size_t i = ps.i;
+    if (wb.done[i]) return;
+    unsigned e = 0;
+    const TracedResults tr{&s, wb.hits + i * (size_t)wb.n_closest, wb.hit_v + i * (size_t)wb.n_closest,
+                           wb.occ + i * (size_t)wb.n_shadow, trace_bsdf != 0};
+    const MtStream gen_end = load_stream(wb.rng_state, i, wb.pixels);
+    // past 311 draws the state lives in local memory only: replay instead
+    const MtStream *gen_end_ptr = gen_end.k < 312 ? &gen_end : nullptr;
+    const Spec L = path_li<true>(s, tr, ps.ray.o, ps.ray.d, true, ps.hit, ps.sc, rng, pr, ris, rv, i, gen_end_ptr, e);
+    V3 rgb = spectrum_to_rgb(L, ps.sc.cie);
+    if (cam.p.has_params && cam.p.enable_exposure) rgb = rgb * cam.p.exposure_mult;
+    color[i] = make_float4(rgb.x, rgb.y, rgb.z, 1.0f);
+    if (e) atomicOr(err, e);
+}
+
+int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                         GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
+                         unsigned *err, cudaStream_t st) {
+    PathRun pr;
+    pr.max_depth = p.max_depth;
+    pr.enable_subsurface = p.enable_subsurface != 0;
+    pr.max_refl = p.max_refl;
+    pr.max_refr = p.max_refr;
+    pr.render_ibl_background = p.render_ibl_background != 0;
+    pr.roulette = p.roulette;
+    RisRun ris;
+    ris.candidate_count = p.candidate_count;
+    ris.use_reservoir = p.use_reservoir != 0;
+    ris.skip_vis = p.skip_visibility != 0;
+    ris.m_cap = p.m_cap;
+    if (cudaMemsetAsync(wb.counts, 0, 2 * sizeof(int), st) != cudaSuccess) return -1;
+    const int blocks = tile_blocks(cam.width, cam.height);
+    ris_generate_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, wb, color, trace_bsdf, err);
+    const int tgrid = 148 * 16;
+    trace_closest_kernel<<<tgrid, 128, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, err);
+    trace_shadow_kernel<<<tgrid, 128, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ, err);
+    ris_shade_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_bsdf, err);
+    return cudaGetLastError() == cudaSuccess ? 4 : -1;
+}
+
+}  // namespace hdr

@@ -173,8 +173,16 @@ typedef struct hdr_ris_params {
     int32_t m_cap;               /* 0 = unbounded CandidateCount (reservoir.h:147-155) */
     int32_t spatial_neighbors;   /* 0 = temporal-only, same-pixel reuse */
     float spatial_radius;
-    int32_t reserved[2];
+    uint32_t flags;              /* HDR_RIS_* execution options; 0 = defaults */
+    int32_t reserved;
 } hdr_ris_params;
+
+/* hdr_ris_params.flags. Neither changes the image.
+ * TRACE_ALL_RAYS: also cast the rays of generated BSDF candidates in scenes
+ *   without light geometry or environment, where their result cannot matter.
+ * ONE_KERNEL: integrate each pixel in one thread that casts its own rays,
+ *   instead of the generate / trace / shade wavefront. */
+enum { HDR_RIS_TRACE_ALL_RAYS = 1, HDR_RIS_ONE_KERNEL = 2 };
 
 /* AOV selection for hdr_raycast (RaycastPass requestedOutputs, raycast_pass.cpp:39-55) */
 enum { HDR_AOV_DEPTH = 1, HDR_AOV_ALBEDO = 2, HDR_AOV_NORMAL = 4 };

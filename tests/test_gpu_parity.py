@@ -100,12 +100,17 @@ def test_path_trace_matches_oracle(gpu_ctx):
         orc.accumulate(cam, frame, firefly=True)
 
 
-def test_ris_plain_matches_oracle(gpu_ctx):
+MODES = {"wavefront": {}, "one_kernel": dict(one_kernel=True), "all_rays": dict(trace_all_rays=True)}
+
+
+@pytest.mark.parametrize("mode", list(MODES))
+def test_ris_plain_matches_oracle(gpu_ctx, mode):
     sc, cam = _scene(1)
     gpu_ctx.upload_scene(sc)
     orc = Oracle(sc)
     gpu_ctx.raycast(cam, 0)
-    gpu_ctx.ris_path_trace(cam, 0, candidate_count=16, use_reservoir=False, skip_visibility=True, max_depth=1)
+    gpu_ctx.ris_path_trace(cam, 0, candidate_count=16, use_reservoir=False, skip_visibility=True, max_depth=1,
+                           **MODES[mode])
     gpu = gpu_ctx.download("Color")
     orc.raycast(cam, 0)
     ref, _ = orc.integrate(cam, 0, ris=True, candidate_count=16, use_reservoir=False, skip_visibility=True,
@@ -115,14 +120,15 @@ def test_ris_plain_matches_oracle(gpu_ctx):
     assert frac <= MAX_OUTLIERS
 
 
-def test_restir_temporal_matches_oracle(gpu_ctx):
+@pytest.mark.parametrize("mode", list(MODES))
+def test_restir_temporal_matches_oracle(gpu_ctx, mode):
     sc, cam = _scene(2)
     gpu_ctx.upload_scene(sc)
     gpu_ctx.clear_persistent()
     orc = Oracle(sc)
     for frame in range(3):
         gpu_ctx.raycast(cam, frame)
-        gpu_ctx.ris_path_trace(cam, frame, candidate_count=32, use_reservoir=True, max_depth=1)
+        gpu_ctx.ris_path_trace(cam, frame, candidate_count=32, use_reservoir=True, max_depth=1, **MODES[mode])
         gpu = gpu_ctx.download("Color")
         res = gpu_ctx.download("__ris_reservoir")
         orc.raycast(cam, frame)
@@ -132,3 +138,37 @@ def test_restir_temporal_matches_oracle(gpu_ctx):
         frac = _color_outliers(gpu, ref)
         print(f"ReSTIR frame {frame}: outlier fraction {frac:.4f}")
         assert frac <= MAX_OUTLIERS
+
+
+def test_restir_multibounce_one_kernel_matches_oracle(gpu_ctx):
+    """maxDepth 2 runs in the one-thread-per-pixel form (the bounce loop casts its own rays)."""
+    sc, cam = _scene(2)
+    gpu_ctx.upload_scene(sc)
+    gpu_ctx.clear_persistent()
+    orc = Oracle(sc)
+    for frame in range(2):
+        gpu_ctx.raycast(cam, frame)
+        gpu_ctx.ris_path_trace(cam, frame, candidate_count=8, use_reservoir=True, max_depth=2)
+        gpu = gpu_ctx.download("Color")
+        orc.raycast(cam, frame)
+        ref, _ = orc.integrate(cam, frame, ris=True, candidate_count=8, use_reservoir=True, max_depth=2)
+        frac = _color_outliers(gpu, ref)
+        print(f"ReSTIR depth 2 frame {frame}: outlier fraction {frac:.4f}")
+        assert frac <= MAX_OUTLIERS
+
+
+def test_wavefront_modes_identical(gpu_ctx):
+    """Skipping rays whose result cannot matter and the one-kernel form give bit-identical images."""
+    sc, cam = _scene(2)
+    gpu_ctx.upload_scene(sc)
+    outs = []
+    for mode in MODES.values():
+        gpu_ctx.clear_persistent()
+        frames = []
+        for frame in range(2):
+            gpu_ctx.raycast(cam, frame)
+            gpu_ctx.ris_path_trace(cam, frame, candidate_count=32, use_reservoir=True, max_depth=1, **mode)
+            frames.append(gpu_ctx.download("Color").copy())
+        outs.append(np.stack(frames))
+    for o in outs[1:]:
+        assert np.array_equal(o.view(np.uint32), outs[0].view(np.uint32))
