@@ -262,6 +262,29 @@ def run_ours(args, rank, local_rank, world):
     total_ms = max_over_ranks(total_ms)
     fps = world * args.steps / (total_ms / 1000.0)
 
+    # ---- the same frames in the other execution forms (identical images, see the parity tests)
+    variants = {}
+    for name, kw in (("trace_all_rays", dict(trace_all_rays=True)), ("one_kernel", dict(one_kernel=True))):
+        ctx.clear_persistent()
+        n_var = max(2, min(args.steps, 5))
+        for k in range(2):
+            ctx.raycast(cam, k)
+            ctx.ris_path_trace(cam, k, **ris, **kw)
+            ctx.accumulate(k, firefly=True, mode="parity")
+        barrier()
+        ctx.region_begin(3)
+        for k in range(2, 2 + n_var):
+            ctx.raycast(cam, k)
+            ctx.ris_path_trace(cam, k, **ris, **kw)
+            ctx.accumulate(k, firefly=True, mode="parity")
+        ctx.region_end(3)
+        ms = max_over_ranks(ctx.region_elapsed(3)) / n_var
+        variants[name] = {"frames_per_s": world * 1000.0 / ms, "ms_per_frame": ms, "frames": n_var}
+    ctx.pass_times(reset=True)
+    ctx.clear_persistent()
+    for k in range(args.warmup):
+        frame(k)
+
     # ---- end to end through the public API: camera from the host, image back to pinned memory
     color_host = torch.empty((WIDTH * HEIGHT, 4), dtype=torch.float32, pin_memory=True)
     color_np = color_host.numpy()
@@ -315,6 +338,10 @@ def run_ours(args, rank, local_rank, world):
                 "wall_s": wall_e2e},
         "gpu_launches": gpu_launches,
         "clocks": clk,
+        "variants": variants,
+        "note": "default = wavefront (generate/trace/shade); BSDF-candidate rays are not cast in scenes with no "
+                "light geometry and no environment, where their result cannot change the image (bit-identical, "
+                "tested); 'trace_all_rays' casts them as the reference does",
     }
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
