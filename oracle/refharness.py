@@ -42,7 +42,10 @@ def build() -> bool:
     """Builds the in-place reference library when the reference tree is present."""
     if not (REFERENCE_TREE / "source" / "restir").exists():
         return LIB.exists()
-    subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REFERENCE_TREE}", "ref", f"-j{os.cpu_count() or 4}"],
+    targets = ["ref"]
+    if (HERE.parent / "hdrestir_b200" / "libhdrestir_b200.so").exists():
+        targets.append("ref-gpu")  # the reference pipeline with the GPU passes dropped in
+    subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REFERENCE_TREE}", *targets, f"-j{os.cpu_count() or 4}"],
                    check=True)
     return LIB.exists()
 
@@ -123,6 +126,36 @@ class Reference:
         out = np.zeros(len(rays), abi.GBUFFER_DTYPE)
         self._lib.ref_trace_rays(self._s, _p(rays), len(rays), _p(out))
         return out
+
+
+GPU_LIB = HERE / "_ref" / "libhdr_ref_gpu.so"
+
+
+class RefGpuParams(C.Structure):
+    _fields_ = [("pipeline", C.c_int32), ("candidate_count", C.c_int32), ("use_reservoir", C.c_int32),
+                ("skip_visibility", C.c_int32), ("max_depth", C.c_int32), ("firefly", C.c_int32)]
+
+
+def gpu_pipeline_available() -> bool:
+    return GPU_LIB.exists()
+
+
+def gpu_pipeline_render(scene, cam, frames, ris=True, candidate_count=16, use_reservoir=True, skip_visibility=False,
+                        max_depth=1, firefly=True) -> np.ndarray:
+    """The reference's RenderPipeline with the GPU passes of
+    hdrestir_b200/integration/gpu_passes.h; returns "Color" after `frames` frames."""
+    L = C.CDLL(str(GPU_LIB))
+    L.refgpu_render.restype = C.c_int
+    L.refgpu_render.argtypes = [C.POINTER(abi.SceneDesc), C.POINTER(abi.CameraDesc), C.c_int,
+                                C.POINTER(RefGpuParams), C.c_void_p]
+    desc = scene.c_desc()
+    out = np.zeros((cam.width * cam.height, 4), np.float32)
+    p = RefGpuParams(1 if ris else 0, candidate_count, int(use_reservoir), int(skip_visibility), max_depth,
+                     int(firefly))
+    n = L.refgpu_render(C.byref(desc), C.byref(cam.c_desc()), int(frames), C.byref(p), _p(out))
+    if n != len(out):
+        raise RuntimeError("GPU pipeline render failed")
+    return out
 
 
 def rng_floats(seeds, count) -> np.ndarray:

@@ -1,0 +1,31 @@
+"""Drop-in check: the reference's own RenderPipeline driving the GPU passes of
+hdrestir_b200/integration/gpu_passes.h (as INTEGRATION.md wires them) renders
+what the same pipeline renders with the reference's CPU passes."""
+import numpy as np
+import pytest
+
+from hdrestir_b200 import configs
+from oracle import refharness
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (refharness.available() and refharness.gpu_pipeline_available()),
+                                 reason="reference build with the GPU passes not present")]
+
+
+@pytest.mark.parametrize("cfg,kw", [
+    (2, dict(ris=True, candidate_count=32, use_reservoir=True, max_depth=1)),
+    (1, dict(ris=True, candidate_count=16, use_reservoir=False, skip_visibility=True, max_depth=1)),
+    (0, dict(ris=False, max_depth=4)),
+])
+def test_reference_pipeline_with_gpu_passes(cfg, kw):
+    extra = {1: dict(n_lights=128), 2: dict(grid=96, n_spheres=60, n_lights=300)}.get(cfg, {})
+    sc, cam = configs.small_variant(cfg, 48, 32, **extra)
+    frames = 3
+    gpu = refharness.gpu_pipeline_render(sc, cam, frames, **kw)
+    ref = refharness.Reference(sc)
+    for f in range(frames):
+        _, cpu, _ = ref.render(cam, f, accumulate=True, firefly=True, **kw)
+    a, b = gpu[:, :3].astype(np.float64), cpu[:, :3].astype(np.float64)
+    bad = (np.abs(a - b) > 1e-6 + 1e-4 * np.maximum(np.abs(a), np.abs(b))).any(1).mean()
+    print(f"cfg{cfg}: GPU-pass pipeline vs CPU pipeline, outlier fraction {bad:.4f}")
+    assert bad <= 0.01
