@@ -122,6 +122,7 @@ def lib() -> C.CDLL:
             "hdr_ris_path_trace": (C.c_int, [vp, C.POINTER(CameraDesc), i32, C.POINTER(RisParams)]),
             "hdr_path_trace": (C.c_int, [vp, C.POINTER(CameraDesc), i32, C.POINTER(PathSettings)]),
             "hdr_accumulate": (C.c_int, [vp, i32, i32, i32]),
+            "hdr_accumulate_noalloc": (C.c_int, [vp, vp, i32, i32, i32, i32, i32, vp]),
             "hdr_clear_persistent": (C.c_int, [vp]),
             "hdr_download": (C.c_int, [vp, C.c_char_p, vp, sz]),
             "hdr_upload": (C.c_int, [vp, C.c_char_p, vp, sz]),

@@ -48,6 +48,19 @@ struct DevBuf {
 
 }  // namespace
 
+namespace hdr {
+// Sets hdr_last_error() for entry points defined in other translation units.
+hdr_status set_last_error(hdr_status st, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+}  // namespace hdr
+
 struct hdr_ctx {
     int device = 0;
     uint32_t flags = 0;

@@ -250,6 +250,17 @@ hdr_status hdr_path_trace(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_ind
  * "__accum_color" += "Color", "Color" = accum / (frame_index+1). */
 hdr_status hdr_accumulate(hdr_ctx *ctx, int32_t frame_index, int32_t firefly, int32_t mode);
 
+/* No reference counterpart. hdr_accumulate on caller-owned device planes
+ * (color, accum: width*height RGBA f32, 16-byte aligned, on the current
+ * device) that allocates nothing: the firefly scratch is a fixed static device
+ * array, so frames above 2,097,152 pixels with firefly != 0 are rejected
+ * (HDR_EINVAL). For callers that may not allocate device memory while they
+ * accumulate. The first call on a device loads the scratch (make it before any
+ * stream capture); accum must be zero before frame 0; calls that overlap on one
+ * device race on the shared scratch. stream: a cudaStream_t (NULL = default). */
+hdr_status hdr_accumulate_noalloc(float *color, float *accum, int32_t width, int32_t height, int32_t frame_index,
+                                  int32_t firefly, int32_t mode, void *stream);
+
 /* RenderPipeline::ClearPersistentBuffers (pipeline/render_pipeline.cpp:42-45):
  * zeroes "__accum_color" and "__ris_reservoir". */
 hdr_status hdr_clear_persistent(hdr_ctx *ctx);
