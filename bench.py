@@ -45,6 +45,10 @@ INTEGRATE_BYTES_PER_PX = 80 + 80 + 64 + 16
 # accumulation: colour in 16 + accum in 16 + accum out 16 + colour out 16, plus the firefly
 # clamp and its check (colour in 16 + clamped out 16; clamped in 16 + colour in 16)
 ACCUM_BYTES_PER_PX = 64 + 32 + 32
+# trace_shadow_kernel, the dominant kernel: per shadow ray it must read its queue record
+# (origin, slot, direction, limit: 32 B) and write one occlusion byte; the BVH and the
+# triangles it reads are the scene's, shared by all rays of the launch
+SHADOW_BYTES_PER_RAY = 32 + 1
 
 
 def parse():
@@ -60,9 +64,8 @@ def parse():
     return ap.parse_args()
 
 
-def dist_env():
-    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(
-        os.environ.get("WORLD_SIZE", "1"))
+from hdrestir_b200.replicas import barrier as replica_barrier  # noqa: E402
+from hdrestir_b200.replicas import dist_env, max_over_ranks, whole_job_rate  # noqa: E402
 
 
 def measured_peaks():
@@ -199,6 +202,7 @@ def config_block():
 
 
 def run_ours(args, rank, local_rank, world):
+    import numpy as np
     import torch
     from hdrestir_b200 import configs
     from hdrestir_b200.context import Context
@@ -220,19 +224,7 @@ def run_ours(args, rank, local_rank, world):
         ctx.accumulate(k, firefly=True, mode="parity")
 
     def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        replica_barrier(world)
 
     # ---- warm-up (frame indices continue through the timed region: reservoirs persist)
     ctx.clear_persistent()
@@ -258,9 +250,12 @@ def run_ours(args, rank, local_rank, world):
     barrier()
     clk = clocks.stop()
     gpu_launches = ctx.launch_count() - launches0
-    (t_ray, t_int, t_acc), counts = ctx.pass_times(reset=True)
-    total_ms = max_over_ranks(total_ms)
-    fps = world * args.steps / (total_ms / 1000.0)
+    (t_ray, t_int, t_acc, t_gen, t_closest, t_shadow, t_shade), counts = ctx.pass_times(reset=True, slots=7)
+    wave_counts = ctx.download("__wave_counts").view(np.int32)  # [0] closest rays, [1] shadow rays (last frame)
+    n_shadow = int(wave_counts[1])
+    n_closest = int(wave_counts[0])
+    total_ms = max_over_ranks(total_ms, world)
+    fps = whole_job_rate(args.steps, world, total_ms)
 
     # ---- the same frames in the other execution forms (identical images, see the parity tests)
     variants = {}
@@ -278,7 +273,7 @@ def run_ours(args, rank, local_rank, world):
             ctx.ris_path_trace(cam, k, **ris, **kw)
             ctx.accumulate(k, firefly=True, mode="parity")
         ctx.region_end(3)
-        ms = max_over_ranks(ctx.region_elapsed(3)) / n_var
+        ms = max_over_ranks(ctx.region_elapsed(3), world) / n_var
         variants[name] = {"frames_per_s": world * 1000.0 / ms, "ms_per_frame": ms, "frames": n_var}
     ctx.pass_times(reset=True)
     ctx.clear_persistent()
@@ -298,8 +293,8 @@ def run_ours(args, rank, local_rank, world):
     e2e_ms = ctx.region_elapsed(2)
     wall_e2e = time.perf_counter() - t0
     barrier()
-    e2e_ms = max_over_ranks(e2e_ms)
-    e2e_fps = world * args.steps / (e2e_ms / 1000.0)
+    e2e_ms = max_over_ranks(e2e_ms, world)
+    e2e_fps = whole_job_rate(args.steps, world, e2e_ms)
     h2d = 2 * len(bytes(cam.c_desc())) + 64  # camera block per camera-taking pass + pass parameters
     d2h = WIDTH * HEIGHT * 16
 
@@ -312,8 +307,8 @@ def run_ours(args, rank, local_rank, world):
 
     peak, peak_kind = measured_peaks()
     px = WIDTH * HEIGHT
-    achieved = INTEGRATE_BYTES_PER_PX * px / (t_int / 1000.0) / 1e9
-    traffic, traffic_src = ncu_traffic("ris_integrate")
+    achieved = SHADOW_BYTES_PER_RAY * n_shadow / (t_shadow / 1000.0) / 1e9
+    traffic, traffic_src = ncu_traffic("trace_shadow")
     rays = 33 * px  # 1 primary (raycast) + 1 first bounce + 15 BSDF candidates + 16 shadow rays
     out = {
         "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
@@ -324,13 +319,17 @@ def run_ours(args, rank, local_rank, world):
         "latency_ms": {"p50": statistics.median(frame_ms), "p99": sorted(frame_ms)[
             min(len(frame_ms) - 1, int(round(0.99 * (len(frame_ms) - 1))))], "max": max(frame_ms)},
         "pass_ms": {"raycast": t_ray, "ris_integrate": t_int, "accumulate": t_acc},
+        "kernel_ms": {"ris_generate": t_gen, "trace_closest": t_closest, "trace_shadow": t_shadow,
+                      "ris_shade": t_shade},
+        "rays_per_frame": {"primary": px, "closest": n_closest, "shadow": n_shadow},
         "rays_per_s": rays / (total_ms / args.steps / 1000.0),
-        "roofline": {"kernel": "ris_integrate (RISPathTracePass megakernel)", "bound": "hbm",
+        "roofline": {"kernel": "trace_shadow_kernel (NEE shadow rays, any-hit)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind,
-                     "traffic": traffic, "traffic_source": traffic_src,
-                     "note": "software BVH traversal (33 rays/px) makes this kernel latency/issue bound; "
-                             "algorithmic bytes = reservoir r/w + GBuffer read + colour write per pixel"},
+                     "peak_kind": peak_kind, "traffic": traffic, "traffic_source": traffic_src,
+                     "algorithmic_bytes": SHADOW_BYTES_PER_RAY * n_shadow, "launch_ms": t_shadow,
+                     "shadow_rays_per_s": n_shadow / (t_shadow / 1000.0),
+                     "note": "algorithmic bytes = 33 B per shadow ray (queue record + occlusion byte); the "
+                             "kernel is issue/divergence bound (software BVH traversal), not HBM bound"},
         "roofline_accumulate": {"bound": "hbm", "achieved": ACCUM_BYTES_PER_PX * px / (t_acc / 1000.0) / 1e9,
                                 "peak": peak, "unit": "GB/s",
                                 "frac": ACCUM_BYTES_PER_PX * px / (t_acc / 1000.0) / 1e9 / peak},

@@ -139,11 +139,13 @@ class Context:
                                            out.ctypes.data_as(C.c_void_p)))
         return out
 
-    def pass_times(self, reset: bool = False) -> tuple[tuple[float, float, float], tuple[int, int, int]]:
-        """(average ms, call count) of raycast / integrate / accumulate since the last reset."""
-        ms = (C.c_float * 3)()
-        n = (C.c_int32 * 3)()
-        abi.check(self._lib.hdr_pass_times(self._h, ms, n, 3, int(reset)))
+    def pass_times(self, reset: bool = False, slots: int = 3) -> tuple[tuple[float, ...], tuple[int, ...]]:
+        """(average ms, call count) since the last reset of raycast / integrate /
+        accumulate, and with slots=7 also of the wavefront kernels generate /
+        trace closest / trace shadow / shade."""
+        ms = (C.c_float * slots)()
+        n = (C.c_int32 * slots)()
+        abi.check(self._lib.hdr_pass_times(self._h, ms, n, slots, int(reset)))
         return tuple(ms), tuple(n)
 
     def region_begin(self, slot: int = 0) -> None:

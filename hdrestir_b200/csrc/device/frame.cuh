@@ -81,9 +81,12 @@ struct WaveBuffers {
 };
 
 // Returns the number of kernels launched, or -1 on a launch error.
+// ev_begin / ev_end (4 events each, or null): recorded around the generate,
+// trace-closest, trace-shadow and shade launches for per-kernel device times.
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                          GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
-                         unsigned *err, cudaStream_t st);
+                         unsigned *err, cudaStream_t st, cudaEvent_t *ev_begin = nullptr,
+                         cudaEvent_t *ev_end = nullptr);
 
 void launch_raycast(const DeviceScene &s, const CameraD &cam, int frame_index, GBufferView gb, AovView aov,
                     unsigned *err, cudaStream_t st);

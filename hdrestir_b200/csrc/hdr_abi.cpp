@@ -61,6 +61,11 @@ hdr_status set_last_error(hdr_status st, const char *fmt, ...) {
 }
 }  // namespace hdr
 
+// timing slots: 0 raycast, 1 integrate, 2 accumulate, then the wavefront
+// kernels 3 ris_generate, 4 trace_closest, 5 trace_shadow, 6 ris_shade
+constexpr int kTimeSlots = 7;
+constexpr int kSlotWaveFirst = 3;
+
 struct hdr_ctx {
     int device = 0;
     uint32_t flags = 0;
@@ -82,14 +87,15 @@ struct hdr_ctx {
 
     unsigned *d_err = nullptr;
     int *d_flag = nullptr;
-    // per pass slot (raycast, integrate, accumulate): one start/stop event pair;
-    // the previous pair is folded into the running sums when the slot is reused
-    cudaEvent_t ev_start[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t ev_stop[3] = {nullptr, nullptr, nullptr};
-    bool ev_pending[3] = {false, false, false};
-    double pass_sum_ms[3] = {0, 0, 0};
-    int pass_count[3] = {0, 0, 0};
-    float pass_last_ms[3] = {0, 0, 0};
+    // per timing slot (raycast, integrate, accumulate, then the four wavefront
+    // kernels): one start/stop event pair; the previous pair is folded into the
+    // running sums when the slot is reused
+    cudaEvent_t ev_start[kTimeSlots] = {};
+    cudaEvent_t ev_stop[kTimeSlots] = {};
+    bool ev_pending[kTimeSlots] = {};
+    double pass_sum_ms[kTimeSlots] = {};
+    int pass_count[kTimeSlots] = {};
+    float pass_last_ms[kTimeSlots] = {};
     cudaEvent_t region_ev[4][2] = {};
     const volatile int32_t *cancel = nullptr;
     uint64_t launches = 0;
@@ -270,7 +276,7 @@ hdr_status hdr_ctx_create(hdr_ctx **out, const hdr_ctx_desc *desc) {
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_err, 64);
     if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, 64);
-    for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+    for (int k = 0; k < kTimeSlots && e == cudaSuccess; ++k) {
         e = cudaEventCreate(&c->ev_start[k]);
         if (e == cudaSuccess) e = cudaEventCreate(&c->ev_stop[k]);
     }
@@ -294,7 +300,7 @@ void hdr_ctx_destroy(hdr_ctx *c) {
     for (auto &b : c->scene_bufs) dev_free(c, b);
     for (auto &kv : c->buffers) dev_free(c, kv.second);
     if (c->d_err) cudaFree(c->d_err);
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < kTimeSlots; ++k) {
         if (c->ev_start[k]) cudaEventDestroy(c->ev_start[k]);
         if (c->ev_stop[k]) cudaEventDestroy(c->ev_stop[k]);
     }
@@ -467,9 +473,17 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
         const int trace_bsdf =
             ((p->flags & HDR_RIS_TRACE_ALL_RAYS) || c->scene_light_geometry || c->scene.env_light >= 0) ? 1 : 0;
         if ((st = begin_pass(c, 1)) != HDR_OK) return st;
+        const bool timed = (c->flags & 1u) != 0;
+        if (timed)
+            for (int k = kSlotWaveFirst; k < kSlotWaveFirst + 4; ++k)
+                if ((st = fold_pass_time(c, k)) != HDR_OK) return st;
         const int n = hdr::launch_ris_wavefront(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color,
-                                                trace_bsdf, c->d_err, c->stream);
+                                                trace_bsdf, c->d_err, c->stream,
+                                                timed ? c->ev_start + kSlotWaveFirst : nullptr,
+                                                timed ? c->ev_stop + kSlotWaveFirst : nullptr);
         if (n < 0) return fail(HDR_ECUDA, "wavefront launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        if (timed)
+            for (int k = kSlotWaveFirst; k < kSlotWaveFirst + 4; ++k) c->ev_pending[k] = true;
         c->launches += (uint64_t)n;
         return end_pass(c, 1);
     }
@@ -692,16 +706,16 @@ hdr_status hdr_rng_floats(hdr_ctx *c, const uint32_t *seeds, int32_t n_seeds, in
 hdr_status hdr_pass_times(hdr_ctx *c, float *avg_ms, int32_t *counts, int32_t n, int32_t reset) {
     if (!c || (n > 0 && (!avg_ms || !counts))) return fail(HDR_EINVAL, "bad argument");
     std::lock_guard<std::mutex> lock(c->mu);
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < kTimeSlots; ++k) {
         hdr_status st = fold_pass_time(c, k);
         if (st != HDR_OK) return st;
     }
-    for (int i = 0; i < n && i < 3; ++i) {
+    for (int i = 0; i < n && i < kTimeSlots; ++i) {
         avg_ms[i] = c->pass_count[i] ? (float)(c->pass_sum_ms[i] / c->pass_count[i]) : 0.0f;
         counts[i] = c->pass_count[i];
     }
     if (reset)
-        for (int k = 0; k < 3; ++k) c->pass_sum_ms[k] = 0.0, c->pass_count[k] = 0;
+        for (int k = 0; k < kTimeSlots; ++k) c->pass_sum_ms[k] = 0.0, c->pass_count[k] = 0;
     return HDR_OK;
 }
 

@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(256) ris_shade_kernel(DeviceScene s, CameraD c
 
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                          GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
-                         unsigned *err, cudaStream_t st) {
+                         unsigned *err, cudaStream_t st, cudaEvent_t *ev_begin, cudaEvent_t *ev_end) {
     PathRun pr;
     pr.max_depth = p.max_depth;
     pr.enable_subsurface = p.enable_subsurface != 0;
@@ -214,11 +214,17 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
     ris.m_cap = p.m_cap;
     if (cudaMemsetAsync(wb.counts, 0, 2 * sizeof(int), st) != cudaSuccess) return -1;
     const int blocks = tile_blocks(cam.width, cam.height);
-    ris_generate_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, wb, color, trace_bsdf, err);
+    auto mark = [&](cudaEvent_t *ev, int k) { return !ev || cudaEventRecord(ev[k], st) == cudaSuccess; };
     const int tgrid = 148 * 16;
+    if (!mark(ev_begin, 0)) return -1;
+    ris_generate_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, wb, color, trace_bsdf, err);
+    if (!mark(ev_end, 0) || !mark(ev_begin, 1)) return -1;
     trace_closest_kernel<<<tgrid, 128, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, err);
+    if (!mark(ev_end, 1) || !mark(ev_begin, 2)) return -1;
     trace_shadow_kernel<<<tgrid, 128, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ, err);
+    if (!mark(ev_end, 2) || !mark(ev_begin, 3)) return -1;
     ris_shade_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_bsdf, err);
+    if (!mark(ev_end, 3)) return -1;
     return cudaGetLastError() == cudaSuccess ? 4 : -1;
 }
 

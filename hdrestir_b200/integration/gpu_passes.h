@@ -1,6 +1,6 @@
 // GPU passes for the reference renderer's RenderPipeline, on the hdrestir
 // C ABI (include/hdrestir.h). Header-only; compiled inside the reference tree
-// next to passes/raycast_pass.h etc..
+// next to passes/raycast_pass.h etc., with -I for include/ and this directory.
 //
 // They implement the reference's pass interface (passes/render_pass.h:13-48,
 // HasStaticPassIo) with the same names, inputs and outputs as the CPU passes

@@ -268,7 +268,9 @@ hdr_status hdr_clear_persistent(hdr_ctx *ctx);
 /* Copies a named device buffer to host memory (bytes must equal the buffer size,
  * query it with hdr_buffer_size). Names: "GBuffer" (hdr_gbuffer_texel),
  * "Color" (RGBA f32), "Depth" (f32), "Albedo"/"Normal" (RGB f32),
- * "__accum_color" (RGBA f32), "__ris_reservoir" (see DESIGN.md layout). */
+ * "__accum_color" (RGBA f32), "__ris_reservoir" (5 planes of width*height
+ * float4: light dir + dist, light colour + pdf, light normal + target
+ * function, throughput, then WSum, W, candidate count and flag bits). */
 hdr_status hdr_download(hdr_ctx *ctx, const char *name, void *dst, size_t bytes);
 hdr_status hdr_upload(hdr_ctx *ctx, const char *name, const void *src, size_t bytes);
 hdr_status hdr_buffer_size(hdr_ctx *ctx, const char *name, size_t *bytes);
@@ -296,7 +298,9 @@ hdr_status hdr_rng_floats(hdr_ctx *ctx, const uint32_t *seeds, int32_t n_seeds, 
 /* Average device time (ms) and number of calls of each pass since the last
  * reset, measured with CUDA events on the ctx stream when flag bit 0 is set
  * (the replacement for the reference's METRICS_ENABLED pass timers,
- * core/metrics_on_buffers.h): [0] raycast, [1] integrate, [2] accumulate.
+ * core/metrics_on_buffers.h): [0] raycast, [1] integrate, [2] accumulate,
+ * and for the wavefront form of hdr_ris_path_trace its kernels [3] generate,
+ * [4] trace closest, [5] trace shadow, [6] shade (n <= 7).
  * reset != 0 clears the sums after reading them. */
 hdr_status hdr_pass_times(hdr_ctx *ctx, float *avg_ms, int32_t *counts, int32_t n, int32_t reset);
 

@@ -1,7 +1,7 @@
 // Drop-in check — TEST INFRASTRUCTURE. Runs the reference's own RenderPipeline
 // (pipeline/render_pipeline.cpp) with the GPU passes of
 // hdrestir_b200/integration/gpu_passes.h in place of the CPU passes, exactly
-// as a maintainer would wire them in (INTEGRATION.md), and returns the final
+// as a maintainer would wire them in, and returns the final
 // "Color" the renderer would resolve. Built with the reference sources in place
 // (oracle/Makefile, target ref-gpu) and linked against libhdrestir_b200.so.
 #include <cstdio>

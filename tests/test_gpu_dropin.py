@@ -1,5 +1,5 @@
 """Drop-in check: the reference's own RenderPipeline driving the GPU passes of
-hdrestir_b200/integration/gpu_passes.h (as INTEGRATION.md wires them) renders
+hdrestir_b200/integration/gpu_passes.h renders
 what the same pipeline renders with the reference's CPU passes."""
 import numpy as np
 import pytest
