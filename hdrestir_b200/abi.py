@@ -19,6 +19,7 @@ STATUS_NAMES = {0: "HDR_OK", 1: "HDR_EINVAL", 2: "HDR_ENOMEM", 3: "HDR_ECANCELLE
 LIGHT_DISTANT, LIGHT_DOME, LIGHT_RECT, LIGHT_POINT = 0, 1, 2, 3
 AOV_DEPTH, AOV_ALBEDO, AOV_NORMAL = 1, 2, 4
 ACCUM_PARITY, ACCUM_SHADER = 0, 1
+CTX_TIMINGS, CTX_BINARY_BVH, CTX_LANE_PER_RAY = 1, 2, 8
 
 _f = C.c_float
 _i = C.c_int32
@@ -130,6 +131,7 @@ def lib() -> C.CDLL:
             "hdr_synchronize": (C.c_int, [vp]),
             "hdr_set_cancel": (C.c_int, [vp, C.POINTER(C.c_int32)]),
             "hdr_trace_rays": (C.c_int, [vp, vp, vp, i32, i32, vp]),
+            "hdr_trace_stats": (C.c_int, [vp, vp, vp, i32, i32, vp]),
             "hdr_rng_floats": (C.c_int, [vp, vp, i32, i32, vp]),
             "hdr_pass_times": (C.c_int, [vp, C.POINTER(C.c_float), C.POINTER(C.c_int32), i32, i32]),
             "hdr_launch_count": (C.c_int, [vp, C.POINTER(C.c_uint64)]),

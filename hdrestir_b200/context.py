@@ -26,10 +26,13 @@ def path_settings(max_depth=32, enable_subsurface=True, max_reflection_bounces=8
 
 
 class Context:
-    def __init__(self, device: int = 0, timings: bool = True, hbm_budget: int = 0):
+    def __init__(self, device: int = 0, timings: bool = True, hbm_budget: int = 0, binary_bvh: bool = False,
+                 lane_per_ray: bool = False):
         self._lib = abi.lib()
         self._h = C.c_void_p()
-        desc = abi.CtxDesc(int(device), 1 if timings else 0, int(hbm_budget))
+        flags = ((abi.CTX_TIMINGS if timings else 0) | (abi.CTX_BINARY_BVH if binary_bvh else 0)
+                 | (abi.CTX_LANE_PER_RAY if lane_per_ray else 0))
+        desc = abi.CtxDesc(int(device), flags, int(hbm_budget))
         abi.check(self._lib.hdr_ctx_create(C.byref(self._h), C.byref(desc)))
         self.width = self.height = 0
         self._cancel = None
@@ -121,6 +124,19 @@ class Context:
         abi.check(self._lib.hdr_upload(self._h, name.encode(), arr.ctypes.data_as(C.c_void_p), arr.nbytes))
 
     # ------------------------------------------------------------ queries
+    def trace_stats(self, rays: np.ndarray, walk: int, tmax: np.ndarray | None = None) -> np.ndarray:
+        """Per-ray (nodes popped, leaves, triangles tested, answer) of one traversal form
+        (0 closest binary, 1 closest wide, 2 shadow binary, 3 shadow wide)."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        out = np.empty((len(rays), 4), np.int32)
+        tp = None
+        if tmax is not None:
+            tmax = np.ascontiguousarray(tmax, np.float32)
+            tp = tmax.ctypes.data_as(C.c_void_p)
+        abi.check(self._lib.hdr_trace_stats(self._h, rays.ctypes.data_as(C.c_void_p), tp, len(rays), int(walk),
+                                            out.ctypes.data_as(C.c_void_p)))
+        return out
+
     def trace_rays(self, rays: np.ndarray, tmax: np.ndarray | None = None, any_hit: bool = False) -> np.ndarray:
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
         out = np.empty(len(rays), abi.GBUFFER_DTYPE)

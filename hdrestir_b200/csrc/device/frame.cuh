@@ -81,17 +81,22 @@ struct WaveBuffers {
 };
 
 // Returns the number of kernels launched, or -1 on a launch error.
+// trace_mode: kTraceLanePerRay keeps each lane on one ray until it is done
+// (default: lanes take the next queued ray as soon as theirs is finished).
 // ev_begin / ev_end (4 events each, or null): recorded around the generate,
 // trace-closest, trace-shadow and shade launches for per-kernel device times.
+constexpr int kTraceLanePerRay = 1;
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                          GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
-                         unsigned *err, cudaStream_t st, cudaEvent_t *ev_begin = nullptr,
+                         unsigned *err, cudaStream_t st, int trace_mode = 0, cudaEvent_t *ev_begin = nullptr,
                          cudaEvent_t *ev_end = nullptr);
 
 void launch_raycast(const DeviceScene &s, const CameraD &cam, int frame_index, GBufferView gb, AovView aov,
                     unsigned *err, cudaStream_t st);
 void launch_trace_rays(const DeviceScene &s, const float *rays, const float *tmax, int n, int any_hit,
                        float4 *out /* 6 float4 per ray: hdr_gbuffer_texel */, unsigned *err, cudaStream_t st);
+void launch_trace_stats(const DeviceScene &s, const float *rays, const float *tmax, int n, int mode, int4 *out,
+                        unsigned *err, cudaStream_t st);
 void launch_rng_floats(const uint32_t *seeds, int n, int count, float *out, cudaStream_t st);
 void launch_ris_path_trace(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                            GBufferView gb, ReservoirView res, float4 *color, unsigned *err, cudaStream_t st);

@@ -48,8 +48,7 @@ __device__ __forceinline__ bool intersect(const DeviceScene &s, V3 o, V3 d, Hit 
 }
 // "shadowHit && shadowHit->Depth < limit"
 __device__ __forceinline__ bool occluded(const DeviceScene &s, V3 o, V3 d, float limit, unsigned &err) {
-    HitId id;
-    return trace_ray<true>(s, o, d, limit, id, err) && id.t < limit;
+    return shadow_ray(s, o, d, limit, err);
 }
 
 // Where the integrators get ray results from. Every ray a pixel casts has a

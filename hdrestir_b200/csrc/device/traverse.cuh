@@ -14,6 +14,7 @@
 // exactly that answer, because the running t only decreases.
 #pragma once
 
+#include "bvh_layout.h"
 #include "gf.cuh"
 
 namespace hdr {
@@ -41,6 +42,12 @@ struct DeviceScene {
     int dome_width, dome_height;
     float dome_total_lum;
     int has_tlas;
+    // 4-wide collapse of the same trees (bvh_layout.h)
+    const float4 *blas4;       // 8 per wide node
+    const float4 *blas_roots;  // 2 per mesh: root min.xyz + root code, root max.xyz
+    const float4 *tlas4;       // 8 per wide node
+    float4 tlas_root_lo, tlas_root_hi;
+    int wide;                  // 1: walk the wide trees, 0: the binary ones (same results)
 };
 
 __device__ __forceinline__ int fbits(float f) { return __float_as_int(f); }
@@ -69,32 +76,31 @@ __device__ __forceinline__ SlabRay make_slab_ray(V3 o, V3 d) {
     return r;
 }
 
+// IntersectAABB without branches. The reference returns false as soon as the
+// running entry distance passes the running exit distance; the entry only
+// grows and the exit only shrinks, so testing once after all three axes gives
+// the same answer. Each axis' (t1, t2) pair is ordered with min/max instead of
+// a swap (no NaN can occur on an axis with |d| above the threshold, where
+// 1/d is finite); an axis below the threshold only checks the origin. The
+// entry distance is the reference's value (up to the sign of a zero, which no
+// comparison sees).
 __device__ __forceinline__ bool slab_test(const SlabRay &r, float4 lo, float4 hi, float &t_entry) {
-    if (lo.x > hi.x || lo.y > hi.y || lo.z > hi.z) return false;  // GfRange3f::IsEmpty
-    float tmin = -1e30f, tmax = 1e30f;
     const float o[3] = {r.o.x, r.o.y, r.o.z};
     const float iv[3] = {r.inv.x, r.inv.y, r.inv.z};
     const float mn[3] = {lo.x, lo.y, lo.z};
     const float mx[3] = {hi.x, hi.y, hi.z};
+    bool fail = (lo.x > hi.x) | (lo.y > hi.y) | (lo.z > hi.z);  // GfRange3f::IsEmpty
+    float tmin = -1e30f, tmax = 1e30f;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        if (r.small[i]) {
-            if (o[i] < mn[i] || o[i] > mx[i]) return false;
-        } else {
-            float t1 = (mn[i] - o[i]) * iv[i];
-            float t2 = (mx[i] - o[i]) * iv[i];
-            if (t1 > t2) {
-                const float tt = t1;
-                t1 = t2;
-                t2 = tt;
-            }
-            tmin = smaxf(tmin, t1);
-            tmax = sminf(tmax, t2);
-            if (tmin > tmax) return false;
-        }
+        const float t1 = (mn[i] - o[i]) * iv[i];
+        const float t2 = (mx[i] - o[i]) * iv[i];
+        fail |= r.small[i] & ((o[i] < mn[i]) | (o[i] > mx[i]));
+        tmin = r.small[i] ? tmin : fmaxf(tmin, fminf(t1, t2));
+        tmax = r.small[i] ? tmax : fminf(tmax, fmaxf(t1, t2));
     }
     t_entry = tmin;
-    return tmax > 0.0f && tmax > 1e-4f;
+    return !fail & !(tmin > tmax) & (tmax > 1e-4f);
 }
 
 // IntersectTriangle (bvh.cpp:8-30)
@@ -116,6 +122,19 @@ __device__ __forceinline__ bool tri_test(V3 o, V3 d, const float4 *g, float &t, 
     t = dot(e2, qvec) * inv_det;
     return t > 1e-4f;
 }
+
+// Traversal counters for the statistics entry point; NoStats compiles away.
+struct NoStats {
+    __device__ __forceinline__ void pop() {}
+    __device__ __forceinline__ void leaf() {}
+    __device__ __forceinline__ void tri() {}
+};
+struct CountStats {
+    int pops = 0, leaves = 0, tris = 0;
+    __device__ __forceinline__ void pop() { ++pops; }
+    __device__ __forceinline__ void leaf() { ++leaves; }
+    __device__ __forceinline__ void tri() { ++tris; }
+};
 
 struct HitId {
     float t;
@@ -139,74 +158,96 @@ struct HitId {
 constexpr int kTraceStack = 96;
 constexpr int kTagTlas = 0, kTagInst = 1, kTagBlas = 2;
 
+// The binary walk as a resumable state machine: start() takes a ray, each
+// step() pops one stack entry. A persistent kernel can then give a lane whose
+// ray is finished the next queued ray while the other lanes keep walking.
 template <bool kAnyHit>
-__device__ bool trace_ray(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId &hit, unsigned &err) {
-    hit.t = 1e30f;
-    hit.inst = -1;
-    hit.tri = -1;
-    hit.u = hit.v = 0.0f;
-    if (!s.has_tlas) return false;
-    const SlabRay wr = make_slab_ray<false>(o, d);
-    SlabRay br = wr;
-    V3 oo = o, od = d;
-    int cur_inst = -1, node_base = 0, tri_base = 0;
+struct BinaryWalk {
+    V3 o, d, oo, od;
+    SlabRay wr, br;
+    int cur_inst, node_base, tri_base, sp;
+    float t_limit;
+    HitId hit;
     int stack[kTraceStack];
-    int sp = 0;
-    stack[sp++] = (0 << 2) | kTagTlas;
-    while (sp > 0) {
+
+    __device__ __forceinline__ void start(const DeviceScene &s, V3 ro, V3 rd, float limit) {
+        o = ro;
+        d = rd;
+        t_limit = limit;
+        hit.t = 1e30f;
+        hit.inst = -1;
+        hit.tri = -1;
+        hit.u = hit.v = 0.0f;
+        wr = make_slab_ray<false>(o, d);
+        br = wr;
+        oo = o;
+        od = d;
+        cur_inst = -1;
+        node_base = tri_base = 0;
+        sp = 0;
+        if (s.has_tlas) stack[sp++] = (0 << 2) | kTagTlas;
+    }
+    // "closest hit nearer than t_limit" (kAnyHit) once the walk is over
+    __device__ __forceinline__ bool shadow_answer() const { return hit.inst >= 0 && hit.t < t_limit; }
+
+    // Pops one entry; false once the walk is over (stack empty, an any-hit
+    // answer found, or a stack limit reached, which sets err).
+    template <class St>
+    __device__ __forceinline__ bool step(const DeviceScene &s, unsigned &err, St &st) {
+        if (sp <= 0) return false;
         const int e = stack[--sp];
+        st.pop();
         const int tag = e & 3, idx = e >> 2;
-        if (tag == kTagBlas) {
-            const float4 nlo = __ldg(&s.blas_nodes[2 * (node_base + idx)]);
-            const float4 nhi = __ldg(&s.blas_nodes[2 * (node_base + idx) + 1]);
+        if (tag != kTagInst) {  // a TLAS or BLAS node: one code path for both levels
+            const bool blas = tag == kTagBlas;
+            const float4 *np = blas ? s.blas_nodes + 2 * (size_t)(node_base + idx) : s.tlas_nodes + 2 * (size_t)idx;
+            const float4 lo = __ldg(np), hi = __ldg(np + 1);
             float ta;
-            if (!slab_test(br, nlo, nhi, ta) || ta > hit.t) continue;
-            const int bl = fbits(nlo.w);
-            if (bl < 0) {
-                const int st = -bl - 1;
-                const int cnt = fbits(nhi.w);
+            if (!slab_test(blas ? br : wr, lo, hi, ta) || ta > hit.t) return sp > 0;
+            const int left = fbits(lo.w);
+            if (left >= 0) {
+                if (sp + 2 > kTraceStack) {
+                    err |= blas ? kErrBlasStack : kErrTlasStack;
+                    sp = 0;
+                    return false;
+                }
+                stack[sp++] = ((left + 1) << 2) | tag;
+                stack[sp++] = (left << 2) | tag;
+            } else if (blas) {
+                const int first = -left - 1;
+                const int cnt = fbits(hi.w);
+                st.leaf();
                 for (int q = 0; q < cnt; ++q) {
                     float tt, uu, vv;
-                    if (tri_test(oo, od, s.tri_geo + 3 * (size_t)(tri_base + st + q), tt, uu, vv) && tt < hit.t) {
+                    st.tri();
+                    if (tri_test(oo, od, s.tri_geo + 3 * (size_t)(tri_base + first + q), tt, uu, vv) &&
+                        tt < hit.t) {
                         hit.t = tt;
                         hit.inst = cur_inst;
-                        hit.tri = st + q;
+                        hit.tri = first + q;
                         hit.u = uu;
                         hit.v = vv;
                     }
                 }
-                if (kAnyHit && hit.inst >= 0 && hit.t < t_limit) return true;
+                if (kAnyHit && hit.inst >= 0 && hit.t < t_limit) {
+                    sp = 0;
+                    return false;
+                }
             } else {
                 if (sp + 2 > kTraceStack) {
-                    err |= kErrBlasStack;
-                    break;
+                    err |= kErrTlasStack;
+                    sp = 0;
+                    return false;
                 }
-                stack[sp++] = ((bl + 1) << 2) | kTagBlas;
-                stack[sp++] = (bl << 2) | kTagBlas;
-            }
-        } else if (tag == kTagTlas) {
-            const float4 lo = __ldg(&s.tlas_nodes[2 * idx]);
-            const float4 hi = __ldg(&s.tlas_nodes[2 * idx + 1]);
-            float t_aabb = 0.0f;
-            if (!slab_test(wr, lo, hi, t_aabb) || t_aabb > hit.t) continue;
-            const int left = fbits(lo.w);
-            if (sp + 2 > kTraceStack) {
-                err |= kErrTlasStack;
-                break;
-            }
-            if (left < 0) {
-                const int start = -left - 1;
+                const int first = -left - 1;
                 const int count = fbits(hi.w);
-                for (int k = count - 1; k >= 0; --k) stack[sp++] = ((start + k) << 2) | kTagInst;
-            } else {
-                stack[sp++] = ((left + 1) << 2) | kTagTlas;
-                stack[sp++] = (left << 2) | kTagTlas;
+                for (int k = count - 1; k >= 0; --k) stack[sp++] = ((first + k) << 2) | kTagInst;
             }
         } else {  // instance slot of a TLAS leaf: enter its BLAS in object space
             const int ii = __ldg(&s.tlas_inst[idx]);
             const float4 *ip = s.instances + 8 * ii;
             const float4 r7 = __ldg(ip + 7);
-            if (fbits(r7.y) == 0) continue;  // mesh without triangles: empty BVH
+            if (fbits(r7.y) == 0) return sp > 0;  // mesh without triangles: empty BVH
             const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2), m3 = __ldg(ip + 3);
             const float inv[16] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w,
                                    m2.x, m2.y, m2.z, m2.w, m3.x, m3.y, m3.z, m3.w};
@@ -218,8 +259,183 @@ __device__ bool trace_ray(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId
             cur_inst = ii;
             stack[sp++] = (0 << 2) | kTagBlas;
         }
+        return sp > 0;
     }
+};
+
+template <bool kAnyHit, class St = NoStats>
+__device__ bool trace_ray_binary(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId &hit, unsigned &err,
+                                 St &&st = St()) {
+    BinaryWalk<kAnyHit> w;
+    w.start(s, o, d, t_limit);
+    while (w.step(s, err, st)) {
+    }
+    hit = w.hit;
     return hit.inst >= 0;
+}
+
+// The same query over the 4-wide collapse of the same trees. A wide node holds
+// the boxes of a binary node's grandchildren (or of a child that is a leaf);
+// the skipped middle boxes contain their children's, and the slab test is
+// monotone under inclusion, so dropping them changes neither which leaves are
+// reached nor the order or running t with which their triangles are tested:
+// the result, ties included, is the binary walk's. Slab tests run when the
+// parent is visited; the entry distance travels on the stack and the
+// reference's "tAabb > closest t" cull is applied when the entry pops, with
+// the closest t of that moment, as in the binary walk.
+constexpr int kWideStack = 96;
+
+__device__ __forceinline__ int wide_children(const SlabRay &r, const float4 *n, int codes_out[4], float ta_out[4]) {
+    const float4 lx = __ldg(n), ly = __ldg(n + 1), lz = __ldg(n + 2);
+    const float4 hx = __ldg(n + 3), hy = __ldg(n + 4), hz = __ldg(n + 5);
+    const float4 cd = __ldg(n + 6);
+    const float lxs[4] = {lx.x, lx.y, lx.z, lx.w}, lys[4] = {ly.x, ly.y, ly.z, ly.w}, lzs[4] = {lz.x, lz.y, lz.z, lz.w};
+    const float hxs[4] = {hx.x, hx.y, hx.z, hx.w}, hys[4] = {hy.x, hy.y, hy.z, hy.w}, hzs[4] = {hz.x, hz.y, hz.z, hz.w};
+    const int cs[4] = {fbits(cd.x), fbits(cd.y), fbits(cd.z), fbits(cd.w)};
+    int m = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        float ta = 0.0f;
+        const bool pass = cs[k] >= 0 && slab_test(r, make_float4(lxs[k], lys[k], lzs[k], 0.0f),
+                                                  make_float4(hxs[k], hys[k], hzs[k], 0.0f), ta);
+        codes_out[k] = pass ? cs[k] : -1;
+        ta_out[k] = ta;
+        m += pass ? 1 : 0;
+    }
+    return m;
+}
+
+template <bool kAnyHit>
+struct WideWalk {
+    V3 o, d, oo, od;
+    SlabRay wr, br;
+    int cur_inst, wide_base, tri_base, sp;
+    float t_limit;
+    HitId hit;
+    int2 stack[kWideStack];
+
+    __device__ __forceinline__ void start(const DeviceScene &s, V3 ro, V3 rd, float limit) {
+        o = ro;
+        d = rd;
+        t_limit = limit;
+        hit.t = 1e30f;
+        hit.inst = -1;
+        hit.tri = -1;
+        hit.u = hit.v = 0.0f;
+        wr = make_slab_ray<false>(o, d);
+        br = wr;
+        oo = o;
+        od = d;
+        cur_inst = -1;
+        wide_base = tri_base = 0;
+        sp = 0;
+        if (!s.has_tlas) return;
+        float ta = 0.0f;
+        const int code = fbits(s.tlas_root_lo.w);
+        if (code >= 0 && slab_test(wr, s.tlas_root_lo, s.tlas_root_hi, ta)) stack[sp++] = make_int2(code, fbits(ta));
+    }
+    __device__ __forceinline__ bool shadow_answer() const { return hit.inst >= 0 && hit.t < t_limit; }
+
+    template <class St>
+    __device__ __forceinline__ bool step(const DeviceScene &s, unsigned &err, St &st) {
+        if (sp <= 0) return false;
+        const int2 e = stack[--sp];
+        st.pop();
+        if (__int_as_float(e.y) > hit.t) return sp > 0;  // entry beyond the closest hit so far
+        const int tag = e.x & ((1 << kWideTagBits) - 1), pay = e.x >> kWideTagBits;
+        if (tag == kWTagBlasNode || tag == kWTagTlasNode) {
+            if (sp + 4 > kWideStack) {
+                err |= (tag == kWTagBlasNode) ? kErrBlasStack : kErrTlasStack;
+                sp = 0;
+                return false;
+            }
+            const bool blas = tag == kWTagBlasNode;
+            const float4 *n = blas ? s.blas4 + 8 * (size_t)(wide_base + pay) : s.tlas4 + 8 * (size_t)pay;
+            int cs[4];
+            float ts[4];
+            wide_children(blas ? br : wr, n, cs, ts);
+#pragma unroll
+            for (int k = 3; k >= 0; --k)
+                if (cs[k] >= 0) stack[sp++] = make_int2(cs[k], fbits(ts[k]));
+        } else if (tag == kWTagBlasLeaf) {
+            const int first = pay >> kBlasLeafCountBits;
+            const int cnt = (pay & ((1 << kBlasLeafCountBits) - 1)) + 1;
+            st.leaf();
+            for (int q = 0; q < cnt; ++q) {
+                float tt, uu, vv;
+                st.tri();
+                if (tri_test(oo, od, s.tri_geo + 3 * (size_t)(tri_base + first + q), tt, uu, vv) && tt < hit.t) {
+                    hit.t = tt;
+                    hit.inst = cur_inst;
+                    hit.tri = first + q;
+                    hit.u = uu;
+                    hit.v = vv;
+                }
+            }
+            if (kAnyHit && hit.inst >= 0 && hit.t < t_limit) {
+                sp = 0;
+                return false;
+            }
+        } else if (tag == kWTagTlasLeaf) {
+            if (sp + 2 > kWideStack) {
+                err |= kErrTlasStack;
+                sp = 0;
+                return false;
+            }
+            const int first = pay >> kTlasLeafCountBits;
+            const int cnt = (pay & ((1 << kTlasLeafCountBits) - 1)) + 1;
+            // instances pop in leaf order; no entry-distance cull at this level
+            for (int k = cnt - 1; k >= 0; --k)
+                stack[sp++] = make_int2(((first + k) << kWideTagBits) | kWTagInst, fbits(-3.402823466e+38f));
+        } else {  // instance of a TLAS leaf: enter its BLAS in object space
+            const int ii = __ldg(&s.tlas_inst[pay]);
+            const float4 *ip = s.instances + 8 * ii;
+            const float4 r7 = __ldg(ip + 7);
+            if (fbits(r7.y) == 0) return sp > 0;  // mesh without triangles: empty BVH
+            const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2), m3 = __ldg(ip + 3);
+            const float inv[16] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w,
+                                   m2.x, m2.y, m2.z, m2.w, m3.x, m3.y, m3.z, m3.w};
+            oo = m4f_transform(inv, o);
+            od = m4f_transform_dir(inv, d);
+            br = make_slab_ray<true>(oo, od);
+            wide_base = fbits(r7.z);
+            tri_base = fbits(__ldg(&ip[5].w));
+            cur_inst = ii;
+            const int mesh = fbits(r7.w);
+            const float4 rlo = __ldg(&s.blas_roots[2 * mesh]), rhi = __ldg(&s.blas_roots[2 * mesh + 1]);
+            float ta = 0.0f;
+            const int code = fbits(rlo.w);
+            if (code >= 0 && slab_test(br, rlo, rhi, ta)) stack[sp++] = make_int2(code, fbits(ta));
+        }
+        return sp > 0;
+    }
+};
+
+template <bool kAnyHit, class St = NoStats>
+__device__ bool trace_ray_wide(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId &hit, unsigned &err,
+                               St &&st = St()) {
+    WideWalk<kAnyHit> w;
+    w.start(s, o, d, t_limit);
+    while (w.step(s, err, st)) {
+    }
+    hit = w.hit;
+    return hit.inst >= 0;
+}
+
+template <bool kAnyHit>
+__device__ __forceinline__ bool trace_ray(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId &hit,
+                                          unsigned &err) {
+    return s.wide ? trace_ray_wide<kAnyHit>(s, o, d, t_limit, hit, err)
+                  : trace_ray_binary<kAnyHit>(s, o, d, t_limit, hit, err);
+}
+
+// Shadow query of the reference, "IntersectScene(o, d) && Depth < limit"
+// (ris_direct_light_integrator.cpp:513-515): the closest-hit walk, stopped as
+// soon as its running closest t drops below limit (the running t only
+// decreases, so the answer is the full walk's).
+__device__ __forceinline__ bool shadow_ray(const DeviceScene &s, V3 o, V3 d, float limit, unsigned &err) {
+    HitId h;
+    return trace_ray<true>(s, o, d, limit, h, err) && h.t < limit;
 }
 
 // HitRecord (core/hit_record.h:15-27) of IntersectScene (scene.cpp:437-535)

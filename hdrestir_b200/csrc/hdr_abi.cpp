@@ -318,10 +318,14 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     hdr::FlatScene f;
     std::string err;
     if (!hdr::build_flat_scene(*desc, f, err)) return fail(HDR_EINVAL, "%s", err.c_str());
-    // one pending sibling per level of each tree, plus the two instance slots of a TLAS leaf
+    // binary walk: one pending sibling per level of each tree, plus the two instance slots of a TLAS leaf
     if (f.max_blas_depth + f.max_tlas_depth + 4 > hdr::kTraceStack)
         return fail(HDR_EINVAL, "BVH depth %d + TLAS depth %d exceeds the device traversal stack (%d)",
                     f.max_blas_depth, f.max_tlas_depth, hdr::kTraceStack);
+    // wide walk: at most three pending siblings per wide level, the root entry and a TLAS leaf's second instance
+    if (3 * (f.max_blas4_depth + f.max_tlas4_depth) + 6 > hdr::kWideStack)
+        return fail(HDR_EINVAL, "wide BVH depth %d + wide TLAS depth %d exceeds the device traversal stack (%d)",
+                    f.max_blas4_depth, f.max_tlas4_depth, hdr::kWideStack);
     HDR_CUDA(cudaStreamSynchronize(c->stream));
     for (auto &b : c->scene_bufs) dev_free(c, b);
     c->scene_bufs.clear();
@@ -352,7 +356,13 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     UP(f.dome_pixels, dome_pixels);
     UP(f.dome_row_cdf, dome_row_cdf);
     UP(f.dome_col_cdf, dome_col_cdf);
+    UP(f.blas4, blas4);
+    UP(f.blas_roots, blas_roots);
+    UP(f.tlas4, tlas4);
 #undef UP
+    std::memcpy(&s.tlas_root_lo, f.tlas_root, sizeof(float4));
+    std::memcpy(&s.tlas_root_hi, f.tlas_root + 4, sizeof(float4));
+    s.wide = (c->flags & HDR_CTX_BINARY_BVH) ? 0 : 1;
     s.num_instances = f.num_instances;
     s.num_materials = f.num_materials;
     s.num_lights = f.num_lights;
@@ -479,6 +489,7 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
                 if ((st = fold_pass_time(c, k)) != HDR_OK) return st;
         const int n = hdr::launch_ris_wavefront(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color,
                                                 trace_bsdf, c->d_err, c->stream,
+                                                (c->flags & HDR_CTX_LANE_PER_RAY) ? hdr::kTraceLanePerRay : 0,
                                                 timed ? c->ev_start + kSlotWaveFirst : nullptr,
                                                 timed ? c->ev_stop + kSlotWaveFirst : nullptr);
         if (n < 0) return fail(HDR_ECUDA, "wavefront launch failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -676,6 +687,35 @@ hdr_status hdr_trace_rays(hdr_ctx *c, const float *rays, const float *tmax, int3
         o.dpdu[0] = r[4].z, o.dpdu[1] = r[4].w, o.dpdu[2] = r[5].x;
         o.dpdv[0] = r[5].y, o.dpdv[1] = r[5].z, o.dpdv[2] = r[5].w;
     }
+    return read_device_error(c);
+}
+
+hdr_status hdr_trace_stats(hdr_ctx *c, const float *rays, const float *tmax, int32_t n, int32_t walk,
+                           int32_t *out) {
+    if (!c || (n > 0 && (!rays || !out)) || n < 0 || walk < 0 || walk > 3) return fail(HDR_EINVAL, "bad argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_trace_stats before hdr_scene_upload");
+    if (n == 0) return HDR_OK;
+    HDR_CUDA(cudaSetDevice(c->device));
+    DevBuf dr, dt, dout;
+    hdr_status st;
+    if ((st = dev_alloc(c, dr, (size_t)n * 24)) != HDR_OK) return st;
+    if ((st = dev_alloc(c, dt, tmax ? (size_t)n * 4 : 0)) != HDR_OK) return dev_free(c, dr), st;
+    if ((st = dev_alloc(c, dout, (size_t)n * 16)) != HDR_OK) return dev_free(c, dr), dev_free(c, dt), st;
+    cudaError_t e = cudaMemcpyAsync(dr.ptr, rays, (size_t)n * 24, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && tmax) e = cudaMemcpyAsync(dt.ptr, tmax, (size_t)n * 4, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        hdr::launch_trace_stats(c->scene, (const float *)dr.ptr, tmax ? (const float *)dt.ptr : nullptr, n, walk,
+                                (int4 *)dout.ptr, c->d_err, c->stream);
+        c->launches += 1;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout.ptr, (size_t)n * 16, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dev_free(c, dr);
+    dev_free(c, dt);
+    dev_free(c, dout);
+    if (e != cudaSuccess) return fail(HDR_ECUDA, "hdr_trace_stats: %s", cudaGetErrorString(e));
     return read_device_error(c);
 }
 

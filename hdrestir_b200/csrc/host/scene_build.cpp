@@ -200,6 +200,88 @@ void put_node(std::vector<float> &dst, const Range3 &r, int left, int count) {
     dst.insert(dst.end(), rec, rec + 8);
 }
 
+// Collapse of a binary tree (children of an inner node at left and left+1, a
+// leaf when left < 0) into 4-wide nodes over the SAME boxes: the slots of the
+// wide node made for binary node n are n's grandchildren, or n's child itself
+// when that child is a leaf, in left-to-right order. Only the boxes of the
+// odd-depth nodes are dropped. Every tree here is built bottom-up as the union
+// of its children's boxes, and the slab test is monotone under box inclusion
+// (the rounded products (bound - o) * inv are monotone in bound), so a child's
+// box passes only if its parent's passes and enters no earlier. The dropped
+// test therefore never rejects a ray its children would keep, nor culls one by
+// entry distance that its children would not, and a depth-first walk of the
+// wide tree tests the same leaves in the same order with the same running
+// closest t as the binary walk.
+template <class Node>
+struct WideBuilder {
+    const std::vector<Node> &nodes;
+    int leaf_tag, inner_tag, count_bits;
+    std::vector<float> out;
+    int max_depth = 0;
+    bool overflow = false;
+
+    int leaf_code(const Node &n) const {
+        const long long start = -(long long)n.left - 1;
+        const long long payload = (start << count_bits) | (long long)(n.count - 1);
+        const int count = n.count, max_count = 1 << count_bits;
+        if (count < 1 || count > max_count || payload >= (1ll << 28)) return -2;
+        return (int)(payload << kWideTagBits) | leaf_tag;
+    }
+    int code_of(int idx, int depth) {
+        const Node &n = nodes[(size_t)idx];
+        if (n.left < 0) return leaf_code(n);
+        const int w = emit(idx, depth);
+        if (w >= (1 << 28)) return -2;
+        return (w << kWideTagBits) | inner_tag;
+    }
+    // returns the wide-node index of inner binary node idx
+    int emit(int idx, int depth) {
+        if (depth > max_depth) max_depth = depth;
+        const int w = (int)(out.size() / kWideNodeFloats);
+        out.resize(out.size() + kWideNodeFloats, 0.0f);
+        int slot_node[4];
+        int ns = 0;
+        const Node &n = nodes[(size_t)idx];
+        for (int c = 0; c < 2; ++c) {
+            const int ci = n.left + c;
+            const Node &ch = nodes[(size_t)ci];
+            if (ch.left < 0) {
+                slot_node[ns++] = ci;
+            } else {
+                slot_node[ns++] = ch.left;
+                slot_node[ns++] = ch.left + 1;
+            }
+        }
+        int codes[4] = {-1, -1, -1, -1};
+        for (int k = 0; k < ns; ++k) {
+            codes[k] = code_of(slot_node[k], depth + 1);
+            if (codes[k] == -2) overflow = true;
+        }
+        float *r = &out[(size_t)w * kWideNodeFloats];
+        for (int k = 0; k < 4; ++k) {
+            Range3 b;  // empty slot: min > max, never passes the slab test
+            if (k < ns) b = nodes[(size_t)slot_node[k]].bounds;
+            r[0 + k] = b.mn.x;
+            r[4 + k] = b.mn.y;
+            r[8 + k] = b.mn.z;
+            r[12 + k] = b.mx.x;
+            r[16 + k] = b.mx.y;
+            r[20 + k] = b.mx.z;
+            r[24 + k] = as_float(codes[k]);
+        }
+        return w;
+    }
+    // root entry: {min.xyz, code, max.xyz, 0}
+    void root(float rec[8]) {
+        const Node &n = nodes[0];
+        const int code = code_of(0, 1);
+        if (code == -2) overflow = true;
+        const float r[8] = {n.bounds.mn.x, n.bounds.mn.y, n.bounds.mn.z, as_float(code),
+                            n.bounds.mx.x, n.bounds.mx.y, n.bounds.mx.z, 0.0f};
+        std::memcpy(rec, r, sizeof(r));
+    }
+};
+
 }  // namespace
 
 void gf_inverse4d(const double *m, double *out) {
@@ -279,6 +361,7 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
     }
     // ---- BLAS per mesh
     std::vector<int> node_base(desc.num_meshes), tri_base(desc.num_meshes), blas_ok(desc.num_meshes);
+    std::vector<int> wide_base(desc.num_meshes);
     std::vector<Range3> ranges(desc.num_meshes);
     for (int mi = 0; mi < desc.num_meshes; ++mi) {
         const hdr_mesh_desc &m = desc.meshes[mi];
@@ -294,6 +377,19 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
         blas_ok[mi] = b.nodes.empty() ? 0 : 1;
         if (b.max_depth > out.max_blas_depth) out.max_blas_depth = b.max_depth;
         for (const BlasNode &n : b.nodes) put_node(out.blas_nodes, n.bounds, n.left, n.count);
+        wide_base[mi] = (int)(out.blas4.size() / kWideNodeFloats);
+        float root[8] = {0.0f, 0.0f, 0.0f, as_float(-1), 0.0f, 0.0f, 0.0f, 0.0f};
+        if (!b.nodes.empty()) {
+            WideBuilder<BlasNode> wb{b.nodes, kWTagBlasLeaf, kWTagBlasNode, kBlasLeafCountBits, {}};
+            wb.root(root);
+            if (wb.overflow) {
+                err = "mesh " + std::to_string(mi) + ": too many triangles for the wide BVH encoding";
+                return false;
+            }
+            if (wb.max_depth > out.max_blas4_depth) out.max_blas4_depth = wb.max_depth;
+            out.blas4.insert(out.blas4.end(), wb.out.begin(), wb.out.end());
+        }
+        out.blas_roots.insert(out.blas_roots.end(), root, root + 8);
         for (const BlasTriangle &t : b.tris) {
             const V3 e1 = t.v1 - t.v0, e2 = t.v2 - t.v0;
             const float g[12] = {t.v0.x, t.v0.y, t.v0.z, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z, 0.0f, 0.0f, 0.0f};
@@ -336,7 +432,7 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
         const float *T = h.xf;
         const float r4[16] = {T[0], T[1], T[2], as_float(node_base[d.mesh]), T[4], T[5], T[6], as_float(tri_base[d.mesh]),
                               T[8], T[9], T[10], as_float(d.material), as_float(d.light), as_float(blas_ok[d.mesh]),
-                              0.0f, 0.0f};
+                              as_float(wide_base[d.mesh]), as_float(d.mesh)};
         std::memcpy(rec + 16, r4, sizeof(r4));
         out.instances.insert(out.instances.end(), rec, rec + 32);
     }
@@ -353,6 +449,14 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
         out.max_tlas_depth = tb.max_depth;
         for (const TlasNode &n : nodes) put_node(out.tlas_nodes, n.bounds, n.left, n.count);
         out.tlas_inst = idx;
+        WideBuilder<TlasNode> wt{nodes, kWTagTlasLeaf, kWTagTlasNode, kTlasLeafCountBits, {}};
+        wt.root(out.tlas_root);
+        if (wt.overflow) {
+            err = "too many instances for the wide TLAS encoding";
+            return false;
+        }
+        out.max_tlas4_depth = wt.max_depth;
+        out.tlas4 = std::move(wt.out);
     }
     // ---- materials: PreviewSurfaceMaterial::GetClosure inputs (preview_surface.cpp:61-127)
     out.num_materials = desc.num_materials;

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../../include/hdrestir.h"
+#include "../device/bvh_layout.h"
 #include "../device/gf.cuh"
 
 namespace hdr {
@@ -75,6 +76,11 @@ struct HostInstance {
 // Flattened device-ready arrays (all float4-sized records, little-endian
 // int fields stored bitwise in float slots).
 struct FlatScene {
+    std::vector<float> blas4;       // wide BLAS nodes, all meshes (node indices relative to the mesh base)
+    std::vector<float> blas_roots;  // 8 floats per mesh: root min.xyz, root code | root max.xyz, 0
+    std::vector<float> tlas4;       // wide TLAS nodes
+    float tlas_root[8] = {};        // root min.xyz, root code | root max.xyz, 0
+    int max_blas4_depth = 0, max_tlas4_depth = 0;
     std::vector<float> blas_nodes;  // 8 floats per node: min.xyz,left | max.xyz,count
     std::vector<float> tri_geo;     // 12 floats per tri: v0.xyz,e1.x | e1.yz,e2.xy | e2.z,0,0,0
     std::vector<float> tri_attr;    // 36 floats per tri (see scene_build.cpp)

@@ -63,10 +63,10 @@ __global__ void trace_rays_kernel(DeviceScene s, const float *rays, const float 
     float4 *t = out + 6 * (size_t)k;
     if (any_hit) {
         const float lim = tmax ? tmax[k] : 3.402823466e+38f;
-        const bool occ = trace_ray<true>(s, o, d, lim, hid, e) && hid.t < lim;
-        t[0] = make_float4(0.0f, 0.0f, 0.0f, occ ? hid.t : 3.402823466e+38f);
-        t[1] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(occ ? hid.inst : -1));
-        t[2] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(occ ? hid.tri : -1));
+        const bool occ = shadow_ray(s, o, d, lim, e);
+        t[0] = make_float4(0.0f, 0.0f, 0.0f, 3.402823466e+38f);
+        t[1] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+        t[2] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
         t[3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(occ ? 1 : 0));
         t[4] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         t[5] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -104,6 +104,34 @@ __global__ void rng_floats_kernel(const uint32_t *seeds, int n, int count, float
 void launch_raycast(const DeviceScene &s, const CameraD &cam, int frame_index, GBufferView gb, AovView aov,
                     unsigned *err, cudaStream_t st) {
     raycast_kernel<<<tile_blocks(cam.width, cam.height), 256, 0, st>>>(s, cam, frame_index, gb, aov, err);
+}
+
+// Per-ray traversal work of one walk (hdr_trace_stats): nodes popped, leaves
+// entered, triangles tested, and the answer.
+__global__ void trace_stats_kernel(DeviceScene s, const float *rays, const float *tmax, int n, int mode, int4 *out,
+                                   unsigned *err) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const V3 o{rays[6 * k], rays[6 * k + 1], rays[6 * k + 2]};
+    const V3 d{rays[6 * k + 3], rays[6 * k + 4], rays[6 * k + 5]};
+    const float lim = tmax ? tmax[k] : 3.402823466e+38f;
+    unsigned e = 0;
+    CountStats st;
+    HitId h;
+    bool r = false;
+    switch (mode) {
+        case 0: r = trace_ray_binary<false>(s, o, d, 0.0f, h, e, st); break;
+        case 1: r = trace_ray_wide<false>(s, o, d, 0.0f, h, e, st); break;
+        case 2: r = trace_ray_binary<true>(s, o, d, lim, h, e, st) && h.t < lim; break;
+        default: r = trace_ray_wide<true>(s, o, d, lim, h, e, st) && h.t < lim; break;
+    }
+    out[k] = make_int4(st.pops, st.leaves, st.tris, r ? 1 : 0);
+    if (e) atomicOr(err, e);
+}
+
+void launch_trace_stats(const DeviceScene &s, const float *rays, const float *tmax, int n, int mode, int4 *out,
+                        unsigned *err, cudaStream_t st) {
+    trace_stats_kernel<<<(n + 127) / 128, 128, 0, st>>>(s, rays, tmax, n, mode, out, err);
 }
 
 void launch_trace_rays(const DeviceScene &s, const float *rays, const float *tmax, int n, int any_hit, float4 *out,

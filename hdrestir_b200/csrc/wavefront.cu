@@ -146,31 +146,97 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
     store_stream(wb.rng_state, i, wb.pixels, rng);
 }
 
-__global__ void __launch_bounds__(128) trace_closest_kernel(DeviceScene s, const float4 *__restrict__ q,
-                                                            const int *counts, float4 *hits, float *hit_v,
-                                                            unsigned *err) {
+// Trace kernels. Rays of a warp take very different numbers of steps (shadow
+// rays towards random lights: 43 % of lane-steps did work when each lane
+// traced a fixed ray), so the default form is persistent: a lane whose ray is
+// finished takes the next queued ray (one atomic per warp for all its idle
+// lanes) and every lane steps its own walk, one stack entry per iteration,
+// until the queue is drained. fetch_at counts the rays handed out.
+constexpr unsigned kFullMask = 0xffffffffu;
+
+__device__ __forceinline__ int fetch_ray(int *fetch_at, int n, bool need, bool &drained) {
+    const unsigned want = __ballot_sync(kFullMask, need);
+    if (!want || drained) return -1;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(want) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(fetch_at, __popc(want));
+    base = __shfl_sync(kFullMask, base, leader);
+    if (base + __popc(want) >= n) drained = true;  // warp-uniform
+    const int k = base + __popc(want & ((1u << lane) - 1));
+    return (need && k < n) ? k : -1;
+}
+
+template <template <bool> class Walk, bool kRefill>
+__global__ void __launch_bounds__(128) trace_closest_kernel(DeviceScene s, const float4 *__restrict__ q, int *counts,
+                                                            float4 *hits, float *hit_v, unsigned *err) {
     const int n = counts[0];
     unsigned e = 0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
-        HitId h;
-        trace_ray<false>(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, 0.0f, h, e);
-        const int slot = __float_as_int(a.w);
-        hits[slot] = make_float4(h.t, __int_as_float(h.inst), __int_as_float(h.tri), h.u);
-        hit_v[slot] = h.v;
+    Walk<false> w;
+    NoStats ns;
+    auto put = [&](int slot) {
+        hits[slot] = make_float4(w.hit.t, __int_as_float(w.hit.inst), __int_as_float(w.hit.tri), w.hit.u);
+        hit_v[slot] = w.hit.v;
+    };
+    if (!kRefill) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+            const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
+            w.start(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, 0.0f);
+            while (w.step(s, e, ns)) {
+            }
+            put(__float_as_int(a.w));
+        }
+    } else {
+        int slot = -1;
+        bool drained = false;
+        for (;;) {
+            const int k = fetch_ray(&counts[3], n, slot < 0, drained);
+            if (k >= 0) {
+                const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
+                w.start(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, 0.0f);
+                slot = __float_as_int(a.w);
+            }
+            if (!__any_sync(kFullMask, slot >= 0)) break;
+            if (slot >= 0 && !w.step(s, e, ns)) {
+                put(slot);
+                slot = -1;
+            }
+        }
     }
     if (e) atomicOr(err, e);
 }
 
-__global__ void __launch_bounds__(128) trace_shadow_kernel(DeviceScene s, const float4 *__restrict__ q,
-                                                           const int *counts, unsigned char *occ, unsigned *err) {
+template <template <bool> class Walk, bool kRefill>
+__global__ void __launch_bounds__(128) trace_shadow_kernel(DeviceScene s, const float4 *__restrict__ q, int *counts,
+                                                           unsigned char *occ, unsigned *err) {
     const int n = counts[1];
     unsigned e = 0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
-        HitId h;
-        const bool hit = trace_ray<true>(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, b.w, h, e) && h.t < b.w;
-        occ[__float_as_int(a.w)] = hit ? 1 : 0;
+    Walk<true> w;
+    NoStats ns;
+    if (!kRefill) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+            const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
+            w.start(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, b.w);
+            while (w.step(s, e, ns)) {
+            }
+            occ[__float_as_int(a.w)] = w.shadow_answer() ? 1 : 0;
+        }
+    } else {
+        int slot = -1;
+        bool drained = false;
+        for (;;) {
+            const int k = fetch_ray(&counts[2], n, slot < 0, drained);
+            if (k >= 0) {
+                const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
+                w.start(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, b.w);
+                slot = __float_as_int(a.w);
+            }
+            if (!__any_sync(kFullMask, slot >= 0)) break;
+            if (slot >= 0 && !w.step(s, e, ns)) {
+                occ[slot] = w.shadow_answer() ? 1 : 0;
+                slot = -1;
+            }
+        }
     }
     if (e) atomicOr(err, e);
 }
@@ -199,7 +265,8 @@ __global__ void __launch_bounds__(256) ris_shade_kernel(DeviceScene s, CameraD c
 
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                          GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
-                         unsigned *err, cudaStream_t st, cudaEvent_t *ev_begin, cudaEvent_t *ev_end) {
+                         unsigned *err, cudaStream_t st, int trace_mode, cudaEvent_t *ev_begin,
+                         cudaEvent_t *ev_end) {
     PathRun pr;
     pr.max_depth = p.max_depth;
     pr.enable_subsurface = p.enable_subsurface != 0;
@@ -212,16 +279,30 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
     ris.use_reservoir = p.use_reservoir != 0;
     ris.skip_vis = p.skip_visibility != 0;
     ris.m_cap = p.m_cap;
-    if (cudaMemsetAsync(wb.counts, 0, 2 * sizeof(int), st) != cudaSuccess) return -1;
+    // [0] closest rays queued, [1] shadow rays queued, [2] / [3] shadow / closest rays handed out
+    if (cudaMemsetAsync(wb.counts, 0, 4 * sizeof(int), st) != cudaSuccess) return -1;
     const int blocks = tile_blocks(cam.width, cam.height);
     auto mark = [&](cudaEvent_t *ev, int k) { return !ev || cudaEventRecord(ev[k], st) == cudaSuccess; };
     const int tgrid = 148 * 16;
     if (!mark(ev_begin, 0)) return -1;
     ris_generate_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, wb, color, trace_bsdf, err);
     if (!mark(ev_end, 0) || !mark(ev_begin, 1)) return -1;
-    trace_closest_kernel<<<tgrid, 128, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, err);
+    const bool refill = (trace_mode & kTraceLanePerRay) == 0;
+    if (s.wide)
+        (refill ? trace_closest_kernel<WideWalk, true> : trace_closest_kernel<WideWalk, false>)<<<tgrid, 128, 0, st>>>(
+            s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, err);
+    else
+        (refill ? trace_closest_kernel<BinaryWalk, true>
+                : trace_closest_kernel<BinaryWalk, false>)<<<tgrid, 128, 0, st>>>(s, wb.q_closest, wb.counts,
+                                                                                   wb.hits, wb.hit_v, err);
     if (!mark(ev_end, 1) || !mark(ev_begin, 2)) return -1;
-    trace_shadow_kernel<<<tgrid, 128, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ, err);
+    if (s.wide)
+        (refill ? trace_shadow_kernel<WideWalk, true> : trace_shadow_kernel<WideWalk, false>)<<<tgrid, 128, 0, st>>>(
+            s, wb.q_shadow, wb.counts, wb.occ, err);
+    else
+        (refill ? trace_shadow_kernel<BinaryWalk, true> : trace_shadow_kernel<BinaryWalk, false>)<<<tgrid, 128, 0,
+                                                                                                     st>>>(
+            s, wb.q_shadow, wb.counts, wb.occ, err);
     if (!mark(ev_end, 2) || !mark(ev_begin, 3)) return -1;
     ris_shade_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_bsdf, err);
     if (!mark(ev_end, 3)) return -1;

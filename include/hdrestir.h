@@ -211,9 +211,16 @@ typedef struct hdr_gbuffer_texel {
 /* ---------------------------------------------------------------------------
  * Context
  * ------------------------------------------------------------------------- */
+/* hdr_ctx_desc.flags */
+#define HDR_CTX_TIMINGS 1u        /* record per-pass CUDA-event timings (hdr_pass_times) */
+#define HDR_CTX_BINARY_BVH 2u    /* walk the reference's binary trees node by node instead of their
+                                    4-wide collapse (identical results; for A/B timing) */
+#define HDR_CTX_LANE_PER_RAY 8u  /* wavefront trace kernels keep each lane on one ray until it is
+                                    done instead of refilling idle lanes (for A/B timing) */
+
 typedef struct hdr_ctx_desc {
     int32_t device;              /* CUDA ordinal */
-    uint32_t flags;              /* bit 0: record per-pass CUDA-event timings */
+    uint32_t flags;              /* HDR_CTX_* bits */
     size_t hbm_budget_bytes;     /* 0 = unlimited; allocations past it fail with HDR_ENOMEM */
 } hdr_ctx_desc;
 
@@ -284,10 +291,18 @@ hdr_status hdr_set_cancel(hdr_ctx *ctx, const volatile int32_t *flag);
 
 /* Scene::IntersectScene (scene.cpp:515-535) on caller rays: rays = n x
  * (ox,oy,oz,dx,dy,dz) f32 host array; out = n x hdr_gbuffer_texel.
- * any_hit != 0: only depth/hit are meaningful and traversal stops at the first
- * hit closer than the per-ray limit tmax (NULL = +inf). */
+ * any_hit != 0: the shadow query "closest hit nearer than tmax" (per-ray
+ * limit, NULL = +inf) as the passes cast it; only `hit` is meaningful. */
 hdr_status hdr_trace_rays(hdr_ctx *ctx, const float *rays, const float *tmax, int32_t n,
                           int32_t any_hit, hdr_gbuffer_texel *out);
+
+/* Diagnostic, no reference counterpart: the work one traversal form does per
+ * ray. walk: 0 closest hit on the binary trees, 1 closest hit on their 4-wide
+ * collapse, 2 shadow query on the binary trees, 3 shadow query on the 4-wide
+ * collapse. out = n x int32[4]: nodes popped, leaves entered, triangles
+ * tested, answer (hit / occluded). */
+hdr_status hdr_trace_stats(hdr_ctx *ctx, const float *rays, const float *tmax, int32_t n, int32_t walk,
+                           int32_t *out);
 
 /* Restir::Rng (core/rng.h:10-56) on the device: for each seed, the first
  * `count` NextFloat() values of std::mt19937_64(seed) mapped through

@@ -82,6 +82,34 @@ def test_trace_rays_closest_and_any_hit(gpu_ctx, cfg):
     assert np.array_equal(a["hit"], b["hit"])
 
 
+@pytest.mark.parametrize("cfg", [0, 1, 2])
+def test_traversal_forms_identical(cfg):
+    """The binary walk and its 4-wide collapse give the same closest hits
+    (instance, triangle, t, u, v bits) and the same shadow answers."""
+    from hdrestir_b200.context import Context
+    sc, cam = _scene(cfg)
+    rng = np.random.default_rng(11 + cfg)
+    n = 1 << 15
+    o = rng.uniform(-8, 8, (n, 3)) + np.array([0, 2.0, 0])
+    d = rng.uniform(-1.5, 1.5, (n, 3)) - o  # mostly towards the middle of the scene
+    d[: n // 8, 1] = 0.0  # rays parallel to the ground plane and to slab faces
+    d[n // 8: n // 4, 0] = 0.0
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.concatenate([o, d], 1).astype(np.float32)
+    tmax = rng.uniform(0.0, 12.0, n).astype(np.float32)
+    out = []
+    for kw in ({}, dict(binary_bvh=True)):
+        with Context(device=0, **kw) as ctx:
+            ctx.upload_scene(sc)
+            out.append((ctx.trace_rays(rays), ctx.trace_rays(rays, tmax, any_hit=True)))
+    (ba, bh) = out[0]
+    for wa, wh in out[1:]:
+        assert np.array_equal(wa.view(np.uint8), ba.view(np.uint8))
+        assert np.array_equal(wh["hit"], bh["hit"])
+    assert ba["hit"].sum() > n // 50
+    assert 0 < bh["hit"].sum() < n
+
+
 def test_path_trace_matches_oracle(gpu_ctx):
     sc, cam = _scene(0)
     gpu_ctx.upload_scene(sc)
@@ -170,5 +198,26 @@ def test_wavefront_modes_identical(gpu_ctx):
             gpu_ctx.ris_path_trace(cam, frame, candidate_count=32, use_reservoir=True, max_depth=1, **mode)
             frames.append(gpu_ctx.download("Color").copy())
         outs.append(np.stack(frames))
+    for o in outs[1:]:
+        assert np.array_equal(o.view(np.uint32), outs[0].view(np.uint32))
+
+
+def test_trace_kernel_forms_give_identical_images():
+    """ReSTIR frames of the config-2 scene family are bit-identical whichever
+    walk (binary or 4-wide) and lane schedule (refill or one ray per lane) the
+    wavefront trace kernels use."""
+    from hdrestir_b200.context import Context
+    sc, cam = configs.small_variant(2, 160, 96, grid=128, n_spheres=200, n_lights=2000)
+    outs = []
+    for kw in ({}, dict(lane_per_ray=True), dict(binary_bvh=True), dict(binary_bvh=True, lane_per_ray=True)):
+        with Context(device=0, **kw) as ctx:
+            ctx.upload_scene(sc)
+            frames = []
+            for frame in range(2):
+                ctx.raycast(cam, frame)
+                ctx.ris_path_trace(cam, frame, candidate_count=32, use_reservoir=True, max_depth=1)
+                ctx.accumulate(frame, firefly=True)
+                frames.append(ctx.download("Color").copy())
+            outs.append(np.stack(frames))
     for o in outs[1:]:
         assert np.array_equal(o.view(np.uint32), outs[0].view(np.uint32))
