@@ -158,17 +158,41 @@ struct HitId {
 constexpr int kTraceStack = 96;
 constexpr int kTagTlas = 0, kTagInst = 1, kTagBlas = 2;
 
+// Traversal stacks. A walk holds only scalars and a stack object, so its
+// state stays in registers; the entries live where the stack object says.
+template <class T>
+struct LocalStack {  // all entries in per-thread local memory
+    T *e;
+    __device__ __forceinline__ T get(int k) const { return e[k]; }
+    __device__ __forceinline__ void set(int k, T v) { e[k] = v; }
+};
+// Entries below kDepth in this thread's column of a shared-memory array
+// (entry k at col[k * kThreads]), deeper ones in a per-thread local array:
+// depth-first walks rarely go deep, so the hot entries stay on chip.
+template <class T, int kDepth, int kThreads>
+struct SplitStack {
+    T *col;
+    T *deep;
+    __device__ __forceinline__ T get(int k) const { return k < kDepth ? col[k * kThreads] : deep[k - kDepth]; }
+    __device__ __forceinline__ void set(int k, T v) {
+        if (k < kDepth)
+            col[k * kThreads] = v;
+        else
+            deep[k - kDepth] = v;
+    }
+};
+
 // The binary walk as a resumable state machine: start() takes a ray, each
 // step() pops one stack entry. A persistent kernel can then give a lane whose
 // ray is finished the next queued ray while the other lanes keep walking.
-template <bool kAnyHit>
+template <bool kAnyHit, class Stk = LocalStack<int>>
 struct BinaryWalk {
     V3 o, d, oo, od;
     SlabRay wr, br;
     int cur_inst, node_base, tri_base, sp;
     float t_limit;
     HitId hit;
-    int stack[kTraceStack];
+    Stk stack;
 
     __device__ __forceinline__ void start(const DeviceScene &s, V3 ro, V3 rd, float limit) {
         o = ro;
@@ -185,7 +209,7 @@ struct BinaryWalk {
         cur_inst = -1;
         node_base = tri_base = 0;
         sp = 0;
-        if (s.has_tlas) stack[sp++] = (0 << 2) | kTagTlas;
+        if (s.has_tlas) stack.set(sp++, (0 << 2) | kTagTlas);
     }
     // "closest hit nearer than t_limit" (kAnyHit) once the walk is over
     __device__ __forceinline__ bool shadow_answer() const { return hit.inst >= 0 && hit.t < t_limit; }
@@ -195,7 +219,7 @@ struct BinaryWalk {
     template <class St>
     __device__ __forceinline__ bool step(const DeviceScene &s, unsigned &err, St &st) {
         if (sp <= 0) return false;
-        const int e = stack[--sp];
+        const int e = stack.get(--sp);
         st.pop();
         const int tag = e & 3, idx = e >> 2;
         if (tag != kTagInst) {  // a TLAS or BLAS node: one code path for both levels
@@ -211,8 +235,8 @@ struct BinaryWalk {
                     sp = 0;
                     return false;
                 }
-                stack[sp++] = ((left + 1) << 2) | tag;
-                stack[sp++] = (left << 2) | tag;
+                stack.set(sp++, ((left + 1) << 2) | tag);
+                stack.set(sp++, (left << 2) | tag);
             } else if (blas) {
                 const int first = -left - 1;
                 const int cnt = fbits(hi.w);
@@ -241,7 +265,7 @@ struct BinaryWalk {
                 }
                 const int first = -left - 1;
                 const int count = fbits(hi.w);
-                for (int k = count - 1; k >= 0; --k) stack[sp++] = ((first + k) << 2) | kTagInst;
+                for (int k = count - 1; k >= 0; --k) stack.set(sp++, ((first + k) << 2) | kTagInst);
             }
         } else {  // instance slot of a TLAS leaf: enter its BLAS in object space
             const int ii = __ldg(&s.tlas_inst[idx]);
@@ -257,7 +281,7 @@ struct BinaryWalk {
             node_base = fbits(__ldg(&ip[4].w));
             tri_base = fbits(__ldg(&ip[5].w));
             cur_inst = ii;
-            stack[sp++] = (0 << 2) | kTagBlas;
+            stack.set(sp++, (0 << 2) | kTagBlas);
         }
         return sp > 0;
     }
@@ -266,7 +290,9 @@ struct BinaryWalk {
 template <bool kAnyHit, class St = NoStats>
 __device__ bool trace_ray_binary(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId &hit, unsigned &err,
                                  St &&st = St()) {
+    int mem[kTraceStack];
     BinaryWalk<kAnyHit> w;
+    w.stack.e = mem;
     w.start(s, o, d, t_limit);
     while (w.step(s, err, st)) {
     }
@@ -305,14 +331,14 @@ __device__ __forceinline__ int wide_children(const SlabRay &r, const float4 *n, 
     return m;
 }
 
-template <bool kAnyHit>
+template <bool kAnyHit, class Stk = LocalStack<int2>>
 struct WideWalk {
     V3 o, d, oo, od;
     SlabRay wr, br;
     int cur_inst, wide_base, tri_base, sp;
     float t_limit;
     HitId hit;
-    int2 stack[kWideStack];
+    Stk stack;
 
     __device__ __forceinline__ void start(const DeviceScene &s, V3 ro, V3 rd, float limit) {
         o = ro;
@@ -332,14 +358,14 @@ struct WideWalk {
         if (!s.has_tlas) return;
         float ta = 0.0f;
         const int code = fbits(s.tlas_root_lo.w);
-        if (code >= 0 && slab_test(wr, s.tlas_root_lo, s.tlas_root_hi, ta)) stack[sp++] = make_int2(code, fbits(ta));
+        if (code >= 0 && slab_test(wr, s.tlas_root_lo, s.tlas_root_hi, ta)) stack.set(sp++, make_int2(code, fbits(ta)));
     }
     __device__ __forceinline__ bool shadow_answer() const { return hit.inst >= 0 && hit.t < t_limit; }
 
     template <class St>
     __device__ __forceinline__ bool step(const DeviceScene &s, unsigned &err, St &st) {
         if (sp <= 0) return false;
-        const int2 e = stack[--sp];
+        const int2 e = stack.get(--sp);
         st.pop();
         if (__int_as_float(e.y) > hit.t) return sp > 0;  // entry beyond the closest hit so far
         const int tag = e.x & ((1 << kWideTagBits) - 1), pay = e.x >> kWideTagBits;
@@ -356,7 +382,7 @@ struct WideWalk {
             wide_children(blas ? br : wr, n, cs, ts);
 #pragma unroll
             for (int k = 3; k >= 0; --k)
-                if (cs[k] >= 0) stack[sp++] = make_int2(cs[k], fbits(ts[k]));
+                if (cs[k] >= 0) stack.set(sp++, make_int2(cs[k], fbits(ts[k])));
         } else if (tag == kWTagBlasLeaf) {
             const int first = pay >> kBlasLeafCountBits;
             const int cnt = (pay & ((1 << kBlasLeafCountBits) - 1)) + 1;
@@ -386,7 +412,7 @@ struct WideWalk {
             const int cnt = (pay & ((1 << kTlasLeafCountBits) - 1)) + 1;
             // instances pop in leaf order; no entry-distance cull at this level
             for (int k = cnt - 1; k >= 0; --k)
-                stack[sp++] = make_int2(((first + k) << kWideTagBits) | kWTagInst, fbits(-3.402823466e+38f));
+                stack.set(sp++, make_int2(((first + k) << kWideTagBits) | kWTagInst, fbits(-3.402823466e+38f)));
         } else {  // instance of a TLAS leaf: enter its BLAS in object space
             const int ii = __ldg(&s.tlas_inst[pay]);
             const float4 *ip = s.instances + 8 * ii;
@@ -405,7 +431,7 @@ struct WideWalk {
             const float4 rlo = __ldg(&s.blas_roots[2 * mesh]), rhi = __ldg(&s.blas_roots[2 * mesh + 1]);
             float ta = 0.0f;
             const int code = fbits(rlo.w);
-            if (code >= 0 && slab_test(br, rlo, rhi, ta)) stack[sp++] = make_int2(code, fbits(ta));
+            if (code >= 0 && slab_test(br, rlo, rhi, ta)) stack.set(sp++, make_int2(code, fbits(ta)));
         }
         return sp > 0;
     }
@@ -414,7 +440,9 @@ struct WideWalk {
 template <bool kAnyHit, class St = NoStats>
 __device__ bool trace_ray_wide(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId &hit, unsigned &err,
                                St &&st = St()) {
+    int2 mem[kWideStack];
     WideWalk<kAnyHit> w;
+    w.stack.e = mem;
     w.start(s, o, d, t_limit);
     while (w.step(s, err, st)) {
     }

@@ -362,7 +362,7 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
 #undef UP
     std::memcpy(&s.tlas_root_lo, f.tlas_root, sizeof(float4));
     std::memcpy(&s.tlas_root_hi, f.tlas_root + 4, sizeof(float4));
-    s.wide = (c->flags & HDR_CTX_BINARY_BVH) ? 0 : 1;
+    s.wide = (c->flags & HDR_CTX_WIDE_BVH) ? 1 : 0;
     s.num_instances = f.num_instances;
     s.num_materials = f.num_materials;
     s.num_lights = f.num_lights;

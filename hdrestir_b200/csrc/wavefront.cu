@@ -167,24 +167,41 @@ __device__ __forceinline__ int fetch_ray(int *fetch_at, int n, bool need, bool &
     return (need && k < n) ? k : -1;
 }
 
-template <template <bool> class Walk, bool kRefill>
-__global__ void __launch_bounds__(128) trace_closest_kernel(DeviceScene s, const float4 *__restrict__ q, int *counts,
-                                                            float4 *hits, float *hit_v, unsigned *err) {
+// Stack entries below kSharedDepth live in the block's shared memory (one
+// column per thread), deeper ones in local memory.
+constexpr int kTraceThreads = 128;
+constexpr int kSharedDepth = 24;
+static_assert(kTraceStack == kWideStack, "one spill size for both walks");
+
+template <bool kWide, bool kAnyHit>
+struct TraceWalk {
+    using Entry = typename std::conditional<kWide, int2, int>::type;
+    using Stack = SplitStack<Entry, kSharedDepth, kTraceThreads>;
+    using type = typename std::conditional<kWide, WideWalk<kAnyHit, Stack>, BinaryWalk<kAnyHit, Stack>>::type;
+};
+
+template <bool kWide, bool kRefill>
+__global__ void __launch_bounds__(kTraceThreads) trace_closest_kernel(DeviceScene s, const float4 *__restrict__ q,
+                                                                      int *counts, float4 *hits, float *hit_v,
+                                                                      unsigned *err) {
+    using TW = TraceWalk<kWide, false>;
+    __shared__ typename TW::Entry col[kSharedDepth * kTraceThreads];
+    typename TW::Entry deep[kTraceStack - kSharedDepth];
+    typename TW::type w;
+    w.stack.col = col + threadIdx.x;
+    w.stack.deep = deep;
     const int n = counts[0];
     unsigned e = 0;
-    Walk<false> w;
     NoStats ns;
-    auto put = [&](int slot) {
-        hits[slot] = make_float4(w.hit.t, __int_as_float(w.hit.inst), __int_as_float(w.hit.tri), w.hit.u);
-        hit_v[slot] = w.hit.v;
-    };
     if (!kRefill) {
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
             const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
             w.start(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, 0.0f);
             while (w.step(s, e, ns)) {
             }
-            put(__float_as_int(a.w));
+            const int slot = __float_as_int(a.w);
+            hits[slot] = make_float4(w.hit.t, __int_as_float(w.hit.inst), __int_as_float(w.hit.tri), w.hit.u);
+            hit_v[slot] = w.hit.v;
         }
     } else {
         int slot = -1;
@@ -198,7 +215,8 @@ __global__ void __launch_bounds__(128) trace_closest_kernel(DeviceScene s, const
             }
             if (!__any_sync(kFullMask, slot >= 0)) break;
             if (slot >= 0 && !w.step(s, e, ns)) {
-                put(slot);
+                hits[slot] = make_float4(w.hit.t, __int_as_float(w.hit.inst), __int_as_float(w.hit.tri), w.hit.u);
+                hit_v[slot] = w.hit.v;
                 slot = -1;
             }
         }
@@ -206,12 +224,17 @@ __global__ void __launch_bounds__(128) trace_closest_kernel(DeviceScene s, const
     if (e) atomicOr(err, e);
 }
 
-template <template <bool> class Walk, bool kRefill>
-__global__ void __launch_bounds__(128) trace_shadow_kernel(DeviceScene s, const float4 *__restrict__ q, int *counts,
-                                                           unsigned char *occ, unsigned *err) {
+template <bool kWide, bool kRefill>
+__global__ void __launch_bounds__(kTraceThreads) trace_shadow_kernel(DeviceScene s, const float4 *__restrict__ q,
+                                                                     int *counts, unsigned char *occ, unsigned *err) {
+    using TW = TraceWalk<kWide, true>;
+    __shared__ typename TW::Entry col[kSharedDepth * kTraceThreads];
+    typename TW::Entry deep[kTraceStack - kSharedDepth];
+    typename TW::type w;
+    w.stack.col = col + threadIdx.x;
+    w.stack.deep = deep;
     const int n = counts[1];
     unsigned e = 0;
-    Walk<true> w;
     NoStats ns;
     if (!kRefill) {
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -288,21 +311,13 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
     ris_generate_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, wb, color, trace_bsdf, err);
     if (!mark(ev_end, 0) || !mark(ev_begin, 1)) return -1;
     const bool refill = (trace_mode & kTraceLanePerRay) == 0;
-    if (s.wide)
-        (refill ? trace_closest_kernel<WideWalk, true> : trace_closest_kernel<WideWalk, false>)<<<tgrid, 128, 0, st>>>(
-            s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, err);
-    else
-        (refill ? trace_closest_kernel<BinaryWalk, true>
-                : trace_closest_kernel<BinaryWalk, false>)<<<tgrid, 128, 0, st>>>(s, wb.q_closest, wb.counts,
-                                                                                   wb.hits, wb.hit_v, err);
+    auto closest = s.wide ? (refill ? trace_closest_kernel<true, true> : trace_closest_kernel<true, false>)
+                          : (refill ? trace_closest_kernel<false, true> : trace_closest_kernel<false, false>);
+    closest<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, err);
     if (!mark(ev_end, 1) || !mark(ev_begin, 2)) return -1;
-    if (s.wide)
-        (refill ? trace_shadow_kernel<WideWalk, true> : trace_shadow_kernel<WideWalk, false>)<<<tgrid, 128, 0, st>>>(
-            s, wb.q_shadow, wb.counts, wb.occ, err);
-    else
-        (refill ? trace_shadow_kernel<BinaryWalk, true> : trace_shadow_kernel<BinaryWalk, false>)<<<tgrid, 128, 0,
-                                                                                                     st>>>(
-            s, wb.q_shadow, wb.counts, wb.occ, err);
+    auto shadow = s.wide ? (refill ? trace_shadow_kernel<true, true> : trace_shadow_kernel<true, false>)
+                         : (refill ? trace_shadow_kernel<false, true> : trace_shadow_kernel<false, false>);
+    shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ, err);
     if (!mark(ev_end, 2) || !mark(ev_begin, 3)) return -1;
     ris_shade_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_bsdf, err);
     if (!mark(ev_end, 3)) return -1;

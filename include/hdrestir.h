@@ -213,8 +213,9 @@ typedef struct hdr_gbuffer_texel {
  * ------------------------------------------------------------------------- */
 /* hdr_ctx_desc.flags */
 #define HDR_CTX_TIMINGS 1u        /* record per-pass CUDA-event timings (hdr_pass_times) */
-#define HDR_CTX_BINARY_BVH 2u    /* walk the reference's binary trees node by node instead of their
-                                    4-wide collapse (identical results; for A/B timing) */
+#define HDR_CTX_WIDE_BVH 2u      /* walk the 4-wide collapse of the reference's binary trees
+                                    instead of the trees node by node (identical results; for
+                                    A/B timing) */
 #define HDR_CTX_LANE_PER_RAY 8u  /* wavefront trace kernels keep each lane on one ray until it is
                                     done instead of refilling idle lanes (for A/B timing) */
 

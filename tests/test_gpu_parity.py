@@ -98,7 +98,7 @@ def test_traversal_forms_identical(cfg):
     rays = np.concatenate([o, d], 1).astype(np.float32)
     tmax = rng.uniform(0.0, 12.0, n).astype(np.float32)
     out = []
-    for kw in ({}, dict(binary_bvh=True)):
+    for kw in ({}, dict(wide_bvh=True)):
         with Context(device=0, **kw) as ctx:
             ctx.upload_scene(sc)
             out.append((ctx.trace_rays(rays), ctx.trace_rays(rays, tmax, any_hit=True)))
@@ -209,7 +209,7 @@ def test_trace_kernel_forms_give_identical_images():
     from hdrestir_b200.context import Context
     sc, cam = configs.small_variant(2, 160, 96, grid=128, n_spheres=200, n_lights=2000)
     outs = []
-    for kw in ({}, dict(lane_per_ray=True), dict(binary_bvh=True), dict(binary_bvh=True, lane_per_ray=True)):
+    for kw in ({}, dict(lane_per_ray=True), dict(wide_bvh=True), dict(wide_bvh=True, lane_per_ray=True)):
         with Context(device=0, **kw) as ctx:
             ctx.upload_scene(sc)
             frames = []
