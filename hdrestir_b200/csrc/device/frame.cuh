@@ -82,10 +82,12 @@ struct WaveBuffers {
 
 // Returns the number of kernels launched, or -1 on a launch error.
 // trace_mode: kTraceLanePerRay keeps each lane on one ray until it is done
-// (default: lanes take the next queued ray as soon as theirs is finished).
+// (default: lanes take the next queued ray as soon as theirs is finished);
+// kTraceUnphased steps every lane's whole walk each iteration instead of
+// serving leaves, instance entries and ray starts in separate phases.
 // ev_begin / ev_end (4 events each, or null): recorded around the generate,
 // trace-closest, trace-shadow and shade launches for per-kernel device times.
-constexpr int kTraceLanePerRay = 1;
+constexpr int kTraceLanePerRay = 1, kTraceUnphased = 2;
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                          GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
                          unsigned *err, cudaStream_t st, int trace_mode = 0, cudaEvent_t *ev_begin = nullptr,

@@ -287,6 +287,127 @@ struct BinaryWalk {
     }
 };
 
+// The binary walk split into phases for warps that trace many rays. A lane's
+// node steps are cheap and frequent; its leaves (triangle tests), instance
+// entries (ray transform) and ray starts are costly and rare, and when every
+// step may take any of them the warp pays for all of them on most steps. So a
+// lane that pops a leaf or an instance entry, or finishes its walk, parks it
+// (mode) and stops stepping; the warp keeps stepping the other lanes' nodes
+// and serves the parked work of all lanes together afterwards. Each lane
+// still handles its own entries in its own order, with the same running t at
+// every test, so the results are BinaryWalk's.
+enum : int { kModeNode = 0, kModeLeaf = 1, kModeInst = 2, kModeDone = 3, kModeIdle = 4 };
+
+template <bool kAnyHit, class Stk>
+struct PhasedWalk {
+    V3 o, d, oo, od;
+    SlabRay wr, br;
+    int cur_inst, node_base, tri_base, sp;
+    float t_limit;
+    HitId hit;
+    int mode;
+    int pend;  // kModeLeaf: (first triangle << 3) | count; kModeInst: TLAS instance slot
+    Stk stack;
+
+    __device__ __forceinline__ void start(const DeviceScene &s, V3 ro, V3 rd, float limit) {
+        o = ro;
+        d = rd;
+        t_limit = limit;
+        hit.t = 1e30f;
+        hit.inst = -1;
+        hit.tri = -1;
+        hit.u = hit.v = 0.0f;
+        wr = make_slab_ray<false>(o, d);
+        br = wr;
+        oo = o;
+        od = d;
+        cur_inst = -1;
+        node_base = tri_base = 0;
+        sp = 0;
+        if (s.has_tlas) stack.set(sp++, (0 << 2) | kTagTlas);
+        mode = sp > 0 ? kModeNode : kModeDone;
+    }
+    __device__ __forceinline__ bool shadow_answer() const { return hit.inst >= 0 && hit.t < t_limit; }
+
+    // one stack entry of a lane in kModeNode
+    template <class St>
+    __device__ __forceinline__ void node_step(const DeviceScene &s, unsigned &err, St &st) {
+        if (sp <= 0) {
+            mode = kModeDone;
+            return;
+        }
+        const int e = stack.get(--sp);
+        st.pop();
+        const int tag = e & 3, idx = e >> 2;
+        if (tag == kTagInst) {
+            pend = idx;
+            mode = kModeInst;
+            return;
+        }
+        const bool blas = tag == kTagBlas;
+        const float4 *np = blas ? s.blas_nodes + 2 * (size_t)(node_base + idx) : s.tlas_nodes + 2 * (size_t)idx;
+        const float4 lo = __ldg(np), hi = __ldg(np + 1);
+        float ta;
+        if (!slab_test(blas ? br : wr, lo, hi, ta) || ta > hit.t) return;
+        const int left = fbits(lo.w);
+        if (left >= 0 || !blas) {
+            if (sp + 2 > kTraceStack) {
+                err |= blas ? kErrBlasStack : kErrTlasStack;
+                sp = 0;
+                mode = kModeDone;
+                return;
+            }
+            if (left >= 0) {
+                stack.set(sp++, ((left + 1) << 2) | tag);
+                stack.set(sp++, (left << 2) | tag);
+            } else {  // TLAS leaf: its instances pop in leaf order
+                const int first = -left - 1;
+                const int count = fbits(hi.w);
+                for (int k = count - 1; k >= 0; --k) stack.set(sp++, ((first + k) << 2) | kTagInst);
+            }
+        } else {
+            pend = ((-left - 1) << 3) | fbits(hi.w);
+            mode = kModeLeaf;
+        }
+    }
+    template <class St>
+    __device__ __forceinline__ void leaf(const DeviceScene &s, St &st) {
+        const int first = pend >> 3, cnt = pend & 7;
+        st.leaf();
+        for (int q = 0; q < cnt; ++q) {
+            float tt, uu, vv;
+            st.tri();
+            if (tri_test(oo, od, s.tri_geo + 3 * (size_t)(tri_base + first + q), tt, uu, vv) && tt < hit.t) {
+                hit.t = tt;
+                hit.inst = cur_inst;
+                hit.tri = first + q;
+                hit.u = uu;
+                hit.v = vv;
+            }
+        }
+        if (kAnyHit && hit.inst >= 0 && hit.t < t_limit) sp = 0;
+        mode = sp > 0 ? kModeNode : kModeDone;
+    }
+    __device__ __forceinline__ void inst(const DeviceScene &s) {
+        const int ii = __ldg(&s.tlas_inst[pend]);
+        const float4 *ip = s.instances + 8 * ii;
+        const float4 r7 = __ldg(ip + 7);
+        if (fbits(r7.y) != 0) {  // a mesh without triangles has an empty BVH
+            const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2), m3 = __ldg(ip + 3);
+            const float inv[16] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w,
+                                   m2.x, m2.y, m2.z, m2.w, m3.x, m3.y, m3.z, m3.w};
+            oo = m4f_transform(inv, o);
+            od = m4f_transform_dir(inv, d);
+            br = make_slab_ray<true>(oo, od);
+            node_base = fbits(__ldg(&ip[4].w));
+            tri_base = fbits(__ldg(&ip[5].w));
+            cur_inst = ii;
+            stack.set(sp++, (0 << 2) | kTagBlas);
+        }
+        mode = sp > 0 ? kModeNode : kModeDone;
+    }
+};
+
 template <bool kAnyHit, class St = NoStats>
 __device__ bool trace_ray_binary(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId &hit, unsigned &err,
                                  St &&st = St()) {

@@ -489,7 +489,8 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
                 if ((st = fold_pass_time(c, k)) != HDR_OK) return st;
         const int n = hdr::launch_ris_wavefront(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color,
                                                 trace_bsdf, c->d_err, c->stream,
-                                                (c->flags & HDR_CTX_LANE_PER_RAY) ? hdr::kTraceLanePerRay : 0,
+                                                ((c->flags & HDR_CTX_LANE_PER_RAY) ? hdr::kTraceLanePerRay : 0) |
+                                                    ((c->flags & HDR_CTX_UNPHASED) ? hdr::kTraceUnphased : 0),
                                                 timed ? c->ev_start + kSlotWaveFirst : nullptr,
                                                 timed ? c->ev_stop + kSlotWaveFirst : nullptr);
         if (n < 0) return fail(HDR_ECUDA, "wavefront launch failed: %s", cudaGetErrorString(cudaGetLastError()));

@@ -180,6 +180,72 @@ struct TraceWalk {
     using type = typename std::conditional<kWide, WideWalk<kAnyHit, Stack>, BinaryWalk<kAnyHit, Stack>>::type;
 };
 
+// Phased schedule (PhasedWalk): node steps run while at least kNodeQuorum
+// lanes of the warp are stepping nodes; then the parked leaves, instance
+// entries and finished rays of all lanes are served, and finished lanes take
+// the next queued rays.
+constexpr int kNodeQuorum = 16;
+
+template <bool kAnyHit, class Put>
+__device__ __forceinline__ void phased_trace(const DeviceScene &s, const float4 *__restrict__ q, int n,
+                                             int *fetch_at, Put put, unsigned &e) {
+    __shared__ int col[kSharedDepth * kTraceThreads];
+    int deep[kTraceStack - kSharedDepth];
+    PhasedWalk<kAnyHit, SplitStack<int, kSharedDepth, kTraceThreads>> w;
+    w.stack.col = col + threadIdx.x;
+    w.stack.deep = deep;
+    w.mode = kModeDone;
+    NoStats ns;
+    int slot = -1;
+    bool drained = false;
+    for (;;) {
+        const bool done = w.mode == kModeDone;
+        if (done && slot >= 0) {
+            put(slot, w);
+            slot = -1;
+        }
+        const int k = fetch_ray(fetch_at, n, done, drained);
+        if (done) {
+            if (k >= 0) {
+                const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
+                w.start(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, kAnyHit ? b.w : 0.0f);
+                slot = __float_as_int(a.w);
+            } else {
+                w.mode = kModeIdle;
+            }
+        }
+        if (!__any_sync(kFullMask, w.mode != kModeIdle)) break;
+        do {
+            if (w.mode == kModeNode) w.node_step(s, e, ns);
+        } while (__popc(__ballot_sync(kFullMask, w.mode == kModeNode)) >= kNodeQuorum);
+        if (w.mode == kModeLeaf) w.leaf(s, ns);
+        if (w.mode == kModeInst) w.inst(s);
+    }
+}
+
+__global__ void __launch_bounds__(kTraceThreads) trace_closest_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
+                                                                             int *counts, float4 *hits, float *hit_v,
+                                                                             unsigned *err) {
+    unsigned e = 0;
+    phased_trace<false>(
+        s, q, counts[0], &counts[3],
+        [&](int slot, const auto &w) {
+            hits[slot] = make_float4(w.hit.t, __int_as_float(w.hit.inst), __int_as_float(w.hit.tri), w.hit.u);
+            hit_v[slot] = w.hit.v;
+        },
+        e);
+    if (e) atomicOr(err, e);
+}
+
+__global__ void __launch_bounds__(kTraceThreads) trace_shadow_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
+                                                                            int *counts, unsigned char *occ,
+                                                                            unsigned *err) {
+    unsigned e = 0;
+    phased_trace<true>(
+        s, q, counts[1], &counts[2], [&](int slot, const auto &w) { occ[slot] = w.shadow_answer() ? 1 : 0; }, e);
+    if (e) atomicOr(err, e);
+}
+
 template <bool kWide, bool kRefill>
 __global__ void __launch_bounds__(kTraceThreads) trace_closest_kernel(DeviceScene s, const float4 *__restrict__ q,
                                                                       int *counts, float4 *hits, float *hit_v,
@@ -311,12 +377,15 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
     ris_generate_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, wb, color, trace_bsdf, err);
     if (!mark(ev_end, 0) || !mark(ev_begin, 1)) return -1;
     const bool refill = (trace_mode & kTraceLanePerRay) == 0;
-    auto closest = s.wide ? (refill ? trace_closest_kernel<true, true> : trace_closest_kernel<true, false>)
-                          : (refill ? trace_closest_kernel<false, true> : trace_closest_kernel<false, false>);
+    const bool phased = !s.wide && refill && (trace_mode & kTraceUnphased) == 0;
+    auto closest = phased   ? trace_closest_phased_kernel
+                   : s.wide ? (refill ? trace_closest_kernel<true, true> : trace_closest_kernel<true, false>)
+                            : (refill ? trace_closest_kernel<false, true> : trace_closest_kernel<false, false>);
     closest<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, err);
     if (!mark(ev_end, 1) || !mark(ev_begin, 2)) return -1;
-    auto shadow = s.wide ? (refill ? trace_shadow_kernel<true, true> : trace_shadow_kernel<true, false>)
-                         : (refill ? trace_shadow_kernel<false, true> : trace_shadow_kernel<false, false>);
+    auto shadow = phased   ? trace_shadow_phased_kernel
+                  : s.wide ? (refill ? trace_shadow_kernel<true, true> : trace_shadow_kernel<true, false>)
+                           : (refill ? trace_shadow_kernel<false, true> : trace_shadow_kernel<false, false>);
     shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ, err);
     if (!mark(ev_end, 2) || !mark(ev_begin, 3)) return -1;
     ris_shade_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_bsdf, err);

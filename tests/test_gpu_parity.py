@@ -209,7 +209,8 @@ def test_trace_kernel_forms_give_identical_images():
     from hdrestir_b200.context import Context
     sc, cam = configs.small_variant(2, 160, 96, grid=128, n_spheres=200, n_lights=2000)
     outs = []
-    for kw in ({}, dict(lane_per_ray=True), dict(wide_bvh=True), dict(wide_bvh=True, lane_per_ray=True)):
+    for kw in ({}, dict(unphased=True), dict(lane_per_ray=True), dict(wide_bvh=True),
+               dict(wide_bvh=True, lane_per_ray=True)):
         with Context(device=0, **kw) as ctx:
             ctx.upload_scene(sc)
             frames = []
