@@ -82,6 +82,10 @@ class RisParams(C.Structure):
 RIS_TRACE_ALL_RAYS, RIS_ONE_KERNEL = 1, 2
 
 
+class TraceTuning(C.Structure):
+    _fields_ = [("node_quorum", _i), ("blocks_per_sm", _i), ("trace_ms", _f)]
+
+
 class CtxDesc(C.Structure):
     _fields_ = [("device", _i), ("flags", C.c_uint32), ("hbm_budget_bytes", C.c_size_t)]
 
@@ -132,6 +136,9 @@ def lib() -> C.CDLL:
             "hdr_set_cancel": (C.c_int, [vp, C.POINTER(C.c_int32)]),
             "hdr_trace_rays": (C.c_int, [vp, vp, vp, i32, i32, vp]),
             "hdr_trace_stats": (C.c_int, [vp, vp, vp, i32, i32, vp]),
+            "hdr_get_trace_tuning": (C.c_int, [vp, C.POINTER(TraceTuning)]),
+            "hdr_set_trace_tuning": (C.c_int, [vp, C.POINTER(TraceTuning)]),
+            "hdr_autotune_trace": (C.c_int, [vp, C.POINTER(TraceTuning)]),
             "hdr_rng_floats": (C.c_int, [vp, vp, i32, i32, vp]),
             "hdr_pass_times": (C.c_int, [vp, C.POINTER(C.c_float), C.POINTER(C.c_int32), i32, i32]),
             "hdr_launch_count": (C.c_int, [vp, C.POINTER(C.c_uint64)]),

@@ -124,6 +124,21 @@ class Context:
         abi.check(self._lib.hdr_upload(self._h, name.encode(), arr.ctypes.data_as(C.c_void_p), arr.nbytes))
 
     # ------------------------------------------------------------ queries
+    def trace_tuning(self) -> dict:
+        t = abi.TraceTuning()
+        abi.check(self._lib.hdr_get_trace_tuning(self._h, C.byref(t)))
+        return {"node_quorum": t.node_quorum, "blocks_per_sm": t.blocks_per_sm}
+
+    def set_trace_tuning(self, node_quorum: int, blocks_per_sm: int) -> None:
+        t = abi.TraceTuning(int(node_quorum), int(blocks_per_sm), 0.0)
+        abi.check(self._lib.hdr_set_trace_tuning(self._h, C.byref(t)))
+
+    def autotune_trace(self) -> dict:
+        """Picks the fastest trace schedule on the last wavefront frame's ray queues."""
+        t = abi.TraceTuning()
+        abi.check(self._lib.hdr_autotune_trace(self._h, C.byref(t)))
+        return {"node_quorum": t.node_quorum, "blocks_per_sm": t.blocks_per_sm, "trace_ms": t.trace_ms}
+
     def trace_stats(self, rays: np.ndarray, walk: int, tmax: np.ndarray | None = None) -> np.ndarray:
         """Per-ray (nodes popped, leaves, triangles tested, answer) of one traversal form
         (0 closest binary, 1 closest wide, 2 shadow binary, 3 shadow wide)."""

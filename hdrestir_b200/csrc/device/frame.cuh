@@ -81,16 +81,29 @@ struct WaveBuffers {
 };
 
 // Returns the number of kernels launched, or -1 on a launch error.
-// trace_mode: kTraceLanePerRay keeps each lane on one ray until it is done
-// (default: lanes take the next queued ray as soon as theirs is finished);
-// kTraceUnphased steps every lane's whole walk each iteration instead of
-// serving leaves, instance entries and ray starts in separate phases.
+// How the wavefront trace kernels run. mode: kTraceLanePerRay keeps each lane
+// on one ray until it is done (default: lanes take the next queued ray as soon
+// as theirs is finished); kTraceUnphased steps every lane's whole walk each
+// iteration instead of serving leaves, instance entries and ray starts in
+// separate phases. node_quorum: the phased kernels keep stepping nodes while
+// this many lanes of a warp do. Grid: sm_count x blocks_per_sm persistent blocks.
+constexpr int kTraceLanePerRay = 1, kTraceUnphased = 2;
+struct TraceTuning {
+    int mode = 0;
+    int node_quorum = 16;
+    int blocks_per_sm = 16;
+    int sm_count = 148;
+};
+// The two trace kernels over the queues of the last ris_generate (they read
+// the queue counts and reset nothing but their own fetch counters' use, so the
+// caller zeroes counts[2..3] before a rerun); returns the launches, -1 on error.
+int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &tune, unsigned *err, cudaStream_t st,
+                      cudaEvent_t *ev_begin = nullptr, cudaEvent_t *ev_end = nullptr);
 // ev_begin / ev_end (4 events each, or null): recorded around the generate,
 // trace-closest, trace-shadow and shade launches for per-kernel device times.
-constexpr int kTraceLanePerRay = 1, kTraceUnphased = 2;
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                          GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
-                         unsigned *err, cudaStream_t st, int trace_mode = 0, cudaEvent_t *ev_begin = nullptr,
+                         unsigned *err, cudaStream_t st, const TraceTuning &tune, cudaEvent_t *ev_begin = nullptr,
                          cudaEvent_t *ev_end = nullptr);
 
 void launch_raycast(const DeviceScene &s, const CameraD &cam, int frame_index, GBufferView gb, AovView aov,

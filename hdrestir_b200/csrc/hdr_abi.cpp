@@ -99,6 +99,10 @@ struct hdr_ctx {
     cudaEvent_t region_ev[4][2] = {};
     const volatile int32_t *cancel = nullptr;
     uint64_t launches = 0;
+    // wavefront trace schedule, and the queues of the last wavefront frame (for hdr_autotune_trace)
+    hdr::TraceTuning tune;
+    hdr::WaveBuffers last_wave{};
+    bool have_wave = false;
 };
 
 namespace {
@@ -289,6 +293,11 @@ hdr_status hdr_ctx_create(hdr_ctx **out, const hdr_ctx_desc *desc) {
         return fail(HDR_ECUDA, "context setup: %s", cudaGetErrorString(e));
     }
     c->d_flag = (int *)((char *)c->d_err + 32);
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
+        c->tune.sm_count = sms;
+    c->tune.mode = ((c->flags & HDR_CTX_LANE_PER_RAY) ? hdr::kTraceLanePerRay : 0) |
+                   ((c->flags & HDR_CTX_UNPHASED) ? hdr::kTraceUnphased : 0);
     *out = c;
     return HDR_OK;
 }
@@ -374,6 +383,7 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     HDR_CUDA(cudaStreamSynchronize(c->stream));
     c->scene = s;
     c->has_scene = true;
+    c->have_wave = false;
     c->scene_opaque = true;
     for (int i = 0; i < desc->num_materials; ++i)
         if (!(desc->materials[i].opacity >= 0.999f)) c->scene_opaque = false;
@@ -488,15 +498,15 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
             for (int k = kSlotWaveFirst; k < kSlotWaveFirst + 4; ++k)
                 if ((st = fold_pass_time(c, k)) != HDR_OK) return st;
         const int n = hdr::launch_ris_wavefront(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color,
-                                                trace_bsdf, c->d_err, c->stream,
-                                                ((c->flags & HDR_CTX_LANE_PER_RAY) ? hdr::kTraceLanePerRay : 0) |
-                                                    ((c->flags & HDR_CTX_UNPHASED) ? hdr::kTraceUnphased : 0),
+                                                trace_bsdf, c->d_err, c->stream, c->tune,
                                                 timed ? c->ev_start + kSlotWaveFirst : nullptr,
                                                 timed ? c->ev_stop + kSlotWaveFirst : nullptr);
         if (n < 0) return fail(HDR_ECUDA, "wavefront launch failed: %s", cudaGetErrorString(cudaGetLastError()));
         if (timed)
             for (int k = kSlotWaveFirst; k < kSlotWaveFirst + 4; ++k) c->ev_pending[k] = true;
         c->launches += (uint64_t)n;
+        c->last_wave = wb;
+        c->have_wave = true;
         return end_pass(c, 1);
     }
     if ((st = begin_pass(c, 1)) != HDR_OK) return st;
@@ -717,6 +727,69 @@ hdr_status hdr_trace_stats(hdr_ctx *c, const float *rays, const float *tmax, int
     dev_free(c, dt);
     dev_free(c, dout);
     if (e != cudaSuccess) return fail(HDR_ECUDA, "hdr_trace_stats: %s", cudaGetErrorString(e));
+    return read_device_error(c);
+}
+
+hdr_status hdr_get_trace_tuning(hdr_ctx *c, hdr_trace_tuning *out) {
+    if (!c || !out) return fail(HDR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    out->node_quorum = c->tune.node_quorum;
+    out->blocks_per_sm = c->tune.blocks_per_sm;
+    out->trace_ms = 0.0f;
+    return HDR_OK;
+}
+
+hdr_status hdr_set_trace_tuning(hdr_ctx *c, const hdr_trace_tuning *t) {
+    if (!c || !t) return fail(HDR_EINVAL, "NULL argument");
+    if (t->node_quorum < 1 || t->node_quorum > 32 || t->blocks_per_sm < 1 || t->blocks_per_sm > 64)
+        return fail(HDR_EINVAL, "node_quorum must be 1..32 and blocks_per_sm 1..64");
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->tune.node_quorum = t->node_quorum;
+    c->tune.blocks_per_sm = t->blocks_per_sm;
+    return HDR_OK;
+}
+
+hdr_status hdr_autotune_trace(hdr_ctx *c, hdr_trace_tuning *best) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (!c->have_wave || !c->has_scene)
+        return fail(HDR_EINVAL, "hdr_autotune_trace needs a previous wavefront hdr_ris_path_trace on this ctx");
+    HDR_CUDA(cudaSetDevice(c->device));
+    static const int kQuorum[] = {8, 12, 16, 20, 24, 28};
+    static const int kBlocks[] = {4, 6, 8, 16};
+    hdr::TraceTuning t = c->tune;
+    hdr::TraceTuning pick = c->tune;
+    float pick_ms = 3.4e38f;
+    cudaEvent_t ev[2] = {c->region_ev[3][0], c->region_ev[3][1]};
+    for (int qi = 0; qi < (int)(sizeof(kQuorum) / sizeof(int)); ++qi) {
+        for (int bi = 0; bi < (int)(sizeof(kBlocks) / sizeof(int)); ++bi) {
+            t.node_quorum = kQuorum[qi];
+            t.blocks_per_sm = kBlocks[bi];
+            float ms_min = 3.4e38f;
+            for (int rep = 0; rep < 2; ++rep) {
+                // the trace kernels only read the queues and rewrite the same results; rerunning them
+                // needs nothing but their fetch counters back at zero
+                HDR_CUDA(cudaMemsetAsync(c->last_wave.counts + 2, 0, 2 * sizeof(int), c->stream));
+                HDR_CUDA(cudaEventRecord(ev[0], c->stream));
+                if (hdr::launch_wave_trace(c->scene, c->last_wave, t, c->d_err, c->stream) < 0)
+                    return fail(HDR_ECUDA, "trace launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+                c->launches += 2;
+                HDR_CUDA(cudaEventRecord(ev[1], c->stream));
+                HDR_CUDA(cudaEventSynchronize(ev[1]));
+                float ms = 0.0f;
+                HDR_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+                ms_min = std::min(ms_min, ms);
+            }
+            if (ms_min < pick_ms) pick_ms = ms_min, pick = t;
+        }
+    }
+    c->tune.node_quorum = pick.node_quorum;
+    c->tune.blocks_per_sm = pick.blocks_per_sm;
+    if (best) {
+        best->node_quorum = pick.node_quorum;
+        best->blocks_per_sm = pick.blocks_per_sm;
+        best->trace_ms = pick_ms;
+    }
     return read_device_error(c);
 }
 

@@ -180,15 +180,13 @@ struct TraceWalk {
     using type = typename std::conditional<kWide, WideWalk<kAnyHit, Stack>, BinaryWalk<kAnyHit, Stack>>::type;
 };
 
-// Phased schedule (PhasedWalk): node steps run while at least kNodeQuorum
-// lanes of the warp are stepping nodes; then the parked leaves, instance
-// entries and finished rays of all lanes are served, and finished lanes take
-// the next queued rays.
-constexpr int kNodeQuorum = 16;
-
+// Phased schedule (PhasedWalk): node steps run while at least `quorum` lanes
+// of the warp are stepping nodes; then the parked leaves, instance entries and
+// finished rays of all lanes are served, and finished lanes take the next
+// queued rays.
 template <bool kAnyHit, class Put>
 __device__ __forceinline__ void phased_trace(const DeviceScene &s, const float4 *__restrict__ q, int n,
-                                             int *fetch_at, Put put, unsigned &e) {
+                                             int *fetch_at, int quorum, Put put, unsigned &e) {
     __shared__ int col[kSharedDepth * kTraceThreads];
     int deep[kTraceStack - kSharedDepth];
     PhasedWalk<kAnyHit, SplitStack<int, kSharedDepth, kTraceThreads>> w;
@@ -217,7 +215,7 @@ __device__ __forceinline__ void phased_trace(const DeviceScene &s, const float4 
         if (!__any_sync(kFullMask, w.mode != kModeIdle)) break;
         do {
             if (w.mode == kModeNode) w.node_step(s, e, ns);
-        } while (__popc(__ballot_sync(kFullMask, w.mode == kModeNode)) >= kNodeQuorum);
+        } while (__popc(__ballot_sync(kFullMask, w.mode == kModeNode)) >= quorum);
         if (w.mode == kModeLeaf) w.leaf(s, ns);
         if (w.mode == kModeInst) w.inst(s);
     }
@@ -225,10 +223,10 @@ __device__ __forceinline__ void phased_trace(const DeviceScene &s, const float4 
 
 __global__ void __launch_bounds__(kTraceThreads) trace_closest_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
                                                                              int *counts, float4 *hits, float *hit_v,
-                                                                             unsigned *err) {
+                                                                             int quorum, unsigned *err) {
     unsigned e = 0;
     phased_trace<false>(
-        s, q, counts[0], &counts[3],
+        s, q, counts[0], &counts[3], quorum,
         [&](int slot, const auto &w) {
             hits[slot] = make_float4(w.hit.t, __int_as_float(w.hit.inst), __int_as_float(w.hit.tri), w.hit.u);
             hit_v[slot] = w.hit.v;
@@ -238,11 +236,12 @@ __global__ void __launch_bounds__(kTraceThreads) trace_closest_phased_kernel(Dev
 }
 
 __global__ void __launch_bounds__(kTraceThreads) trace_shadow_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
-                                                                            int *counts, unsigned char *occ,
+                                                                            int *counts, unsigned char *occ, int quorum,
                                                                             unsigned *err) {
     unsigned e = 0;
     phased_trace<true>(
-        s, q, counts[1], &counts[2], [&](int slot, const auto &w) { occ[slot] = w.shadow_answer() ? 1 : 0; }, e);
+        s, q, counts[1], &counts[2], quorum,
+        [&](int slot, const auto &w) { occ[slot] = w.shadow_answer() ? 1 : 0; }, e);
     if (e) atomicOr(err, e);
 }
 
@@ -352,9 +351,37 @@ __global__ void __launch_bounds__(256) ris_shade_kernel(DeviceScene s, CameraD c
     if (e) atomicOr(err, e);
 }
 
+int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &tune, unsigned *err, cudaStream_t st,
+                      cudaEvent_t *ev_begin, cudaEvent_t *ev_end) {
+    auto mark = [&](cudaEvent_t *ev, int k) { return !ev || cudaEventRecord(ev[k], st) == cudaSuccess; };
+    const int tgrid = tune.sm_count * tune.blocks_per_sm;
+    const bool refill = (tune.mode & kTraceLanePerRay) == 0;
+    const bool phased = !s.wide && refill && (tune.mode & kTraceUnphased) == 0;
+    if (!mark(ev_begin, 0)) return -1;
+    if (phased) {
+        trace_closest_phased_kernel<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v,
+                                                                      tune.node_quorum, err);
+    } else {
+        auto closest = s.wide ? (refill ? trace_closest_kernel<true, true> : trace_closest_kernel<true, false>)
+                              : (refill ? trace_closest_kernel<false, true> : trace_closest_kernel<false, false>);
+        closest<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, err);
+    }
+    if (!mark(ev_end, 0) || !mark(ev_begin, 1)) return -1;
+    if (phased) {
+        trace_shadow_phased_kernel<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ,
+                                                                     tune.node_quorum, err);
+    } else {
+        auto shadow = s.wide ? (refill ? trace_shadow_kernel<true, true> : trace_shadow_kernel<true, false>)
+                             : (refill ? trace_shadow_kernel<false, true> : trace_shadow_kernel<false, false>);
+        shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ, err);
+    }
+    if (!mark(ev_end, 1)) return -1;
+    return cudaGetLastError() == cudaSuccess ? 2 : -1;
+}
+
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                          GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
-                         unsigned *err, cudaStream_t st, int trace_mode, cudaEvent_t *ev_begin,
+                         unsigned *err, cudaStream_t st, const TraceTuning &tune, cudaEvent_t *ev_begin,
                          cudaEvent_t *ev_end) {
     PathRun pr;
     pr.max_depth = p.max_depth;
@@ -372,22 +399,12 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
     if (cudaMemsetAsync(wb.counts, 0, 4 * sizeof(int), st) != cudaSuccess) return -1;
     const int blocks = tile_blocks(cam.width, cam.height);
     auto mark = [&](cudaEvent_t *ev, int k) { return !ev || cudaEventRecord(ev[k], st) == cudaSuccess; };
-    const int tgrid = 148 * 16;
     if (!mark(ev_begin, 0)) return -1;
     ris_generate_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, wb, color, trace_bsdf, err);
-    if (!mark(ev_end, 0) || !mark(ev_begin, 1)) return -1;
-    const bool refill = (trace_mode & kTraceLanePerRay) == 0;
-    const bool phased = !s.wide && refill && (trace_mode & kTraceUnphased) == 0;
-    auto closest = phased   ? trace_closest_phased_kernel
-                   : s.wide ? (refill ? trace_closest_kernel<true, true> : trace_closest_kernel<true, false>)
-                            : (refill ? trace_closest_kernel<false, true> : trace_closest_kernel<false, false>);
-    closest<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, err);
-    if (!mark(ev_end, 1) || !mark(ev_begin, 2)) return -1;
-    auto shadow = phased   ? trace_shadow_phased_kernel
-                  : s.wide ? (refill ? trace_shadow_kernel<true, true> : trace_shadow_kernel<true, false>)
-                           : (refill ? trace_shadow_kernel<false, true> : trace_shadow_kernel<false, false>);
-    shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ, err);
-    if (!mark(ev_end, 2) || !mark(ev_begin, 3)) return -1;
+    if (!mark(ev_end, 0)) return -1;
+    if (launch_wave_trace(s, wb, tune, err, st, ev_begin ? ev_begin + 1 : nullptr, ev_end ? ev_end + 1 : nullptr) < 0)
+        return -1;
+    if (!mark(ev_begin, 3)) return -1;
     ris_shade_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_bsdf, err);
     if (!mark(ev_end, 3)) return -1;
     return cudaGetLastError() == cudaSuccess ? 4 : -1;

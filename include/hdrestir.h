@@ -300,6 +300,22 @@ hdr_status hdr_set_cancel(hdr_ctx *ctx, const volatile int32_t *flag);
 hdr_status hdr_trace_rays(hdr_ctx *ctx, const float *rays, const float *tmax, int32_t n,
                           int32_t any_hit, hdr_gbuffer_texel *out);
 
+/* Schedule of the wavefront trace kernels (no reference counterpart; no effect
+ * on results). node_quorum: node steps continue while this many lanes of a
+ * warp step nodes (1..32); blocks_per_sm: persistent blocks per SM (1..64).
+ * trace_ms: device time of the two trace kernels (autotune output). */
+typedef struct hdr_trace_tuning {
+    int32_t node_quorum;
+    int32_t blocks_per_sm;
+    float trace_ms;
+} hdr_trace_tuning;
+hdr_status hdr_get_trace_tuning(hdr_ctx *ctx, hdr_trace_tuning *out);
+hdr_status hdr_set_trace_tuning(hdr_ctx *ctx, const hdr_trace_tuning *tuning);
+/* Autotuner: reruns the trace kernels of the last wavefront hdr_ris_path_trace
+ * (they only read its ray queues and rewrite the same hit / occlusion slots)
+ * over a grid of schedules, keeps the fastest in the ctx and returns it. */
+hdr_status hdr_autotune_trace(hdr_ctx *ctx, hdr_trace_tuning *best);
+
 /* Diagnostic, no reference counterpart: the work one traversal form does per
  * ray. walk: 0 closest hit on the binary trees, 1 closest hit on their 4-wide
  * collapse, 2 shadow query on the binary trees, 3 shadow query on the 4-wide

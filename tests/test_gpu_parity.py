@@ -10,7 +10,7 @@ on the pixels, plus a bound on the fraction of pixels allowed to differ more
 import numpy as np
 import pytest
 
-from hdrestir_b200 import configs
+from hdrestir_b200 import abi, configs
 from oracle.oracle import Oracle, rng_floats
 
 pytestmark = pytest.mark.gpu
@@ -210,9 +210,12 @@ def test_trace_kernel_forms_give_identical_images():
     sc, cam = configs.small_variant(2, 160, 96, grid=128, n_spheres=200, n_lights=2000)
     outs = []
     for kw in ({}, dict(unphased=True), dict(lane_per_ray=True), dict(wide_bvh=True),
-               dict(wide_bvh=True, lane_per_ray=True)):
+               dict(wide_bvh=True, lane_per_ray=True), dict(tuning=(3, 2))):
+        tuning = kw.pop("tuning", None)
         with Context(device=0, **kw) as ctx:
             ctx.upload_scene(sc)
+            if tuning:
+                ctx.set_trace_tuning(*tuning)
             frames = []
             for frame in range(2):
                 ctx.raycast(cam, frame)
@@ -222,3 +225,23 @@ def test_trace_kernel_forms_give_identical_images():
             outs.append(np.stack(frames))
     for o in outs[1:]:
         assert np.array_equal(o.view(np.uint32), outs[0].view(np.uint32))
+
+
+def test_autotune_trace_keeps_results():
+    """The trace-schedule autotuner picks a schedule from its grid, and frames
+    rendered with it are those rendered before tuning."""
+    from hdrestir_b200.context import Context
+    sc, cam = configs.small_variant(2, 96, 64, grid=96, n_spheres=60, n_lights=300)
+    with Context(device=0) as ctx:
+        ctx.upload_scene(sc)
+        with pytest.raises(abi.HdrError):
+            ctx.autotune_trace()  # no wavefront frame yet
+        ris = dict(candidate_count=32, use_reservoir=False, max_depth=1)
+        ctx.raycast(cam, 0)
+        ctx.ris_path_trace(cam, 0, **ris)
+        before = ctx.download("Color").copy()
+        best = ctx.autotune_trace()
+        assert best["node_quorum"] in (8, 12, 16, 20, 24, 28) and best["blocks_per_sm"] in (4, 6, 8, 16)
+        assert best["trace_ms"] > 0.0 and ctx.trace_tuning()["node_quorum"] == best["node_quorum"]
+        ctx.ris_path_trace(cam, 0, **ris)
+        assert np.array_equal(ctx.download("Color").view(np.uint32), before.view(np.uint32))
