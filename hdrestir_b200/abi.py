@@ -83,7 +83,7 @@ RIS_TRACE_ALL_RAYS, RIS_ONE_KERNEL = 1, 2
 
 
 class TraceTuning(C.Structure):
-    _fields_ = [("node_quorum", _i), ("blocks_per_sm", _i), ("trace_ms", _f)]
+    _fields_ = [("node_quorum", _i), ("blocks_per_sm", _i), ("trace_ms", _f), ("shade_shape", _i)]
 
 
 class CtxDesc(C.Structure):

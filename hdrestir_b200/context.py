@@ -127,10 +127,10 @@ class Context:
     def trace_tuning(self) -> dict:
         t = abi.TraceTuning()
         abi.check(self._lib.hdr_get_trace_tuning(self._h, C.byref(t)))
-        return {"node_quorum": t.node_quorum, "blocks_per_sm": t.blocks_per_sm}
+        return {"node_quorum": t.node_quorum, "blocks_per_sm": t.blocks_per_sm, "shade_shape": t.shade_shape}
 
-    def set_trace_tuning(self, node_quorum: int, blocks_per_sm: int) -> None:
-        t = abi.TraceTuning(int(node_quorum), int(blocks_per_sm), 0.0)
+    def set_trace_tuning(self, node_quorum: int, blocks_per_sm: int, shade_shape: int = 0) -> None:
+        t = abi.TraceTuning(int(node_quorum), int(blocks_per_sm), 0.0, int(shade_shape))
         abi.check(self._lib.hdr_set_trace_tuning(self._h, C.byref(t)))
 
     def autotune_trace(self) -> dict:

@@ -93,7 +93,11 @@ struct TraceTuning {
     int node_quorum = 16;
     int blocks_per_sm = 16;
     int sm_count = 148;
+    int shade_shape = 1;  // ris_shade launch shape, 0 .. kShadeShapes - 1
 };
+// ris_shade launch shapes: (threads per block, minimum resident blocks per SM)
+// = (256, 1), (256, 2), (128, 3), (128, 4)
+constexpr int kShadeShapes = 4;
 // The two trace kernels over the queues of the last ris_generate (they read
 // the queue counts and reset nothing but their own fetch counters' use, so the
 // caller zeroes counts[2..3] before a rerun); returns the launches, -1 on error.
@@ -123,16 +127,22 @@ int launch_accumulate(float4 *color, float4 *accum, float4 *scratch, int *flag_d
 
 // Pixel of thread t in a 16x16 tile: each warp covers an 8x4 sub-tile so the
 // rays it traces start close together.
+template <int kThreads = 256>
 __device__ __forceinline__ bool tile_pixel(int width, int height, int &x, int &y) {
+    constexpr int kTileH = kThreads / 16;  // tiles 16 pixels wide, one 8x4 patch per warp
     const int tiles_x = (width + 15) >> 4;
     const int tile = blockIdx.x;
     const int tx = tile % tiles_x, ty = tile / tiles_x;
     const int t = threadIdx.x;
     const int w = t >> 5, lane = t & 31;
     x = (tx << 4) + ((w & 1) << 3) + (lane & 7);
-    y = (ty << 4) + ((w >> 1) << 2) + (lane >> 3);
+    y = ty * kTileH + ((w >> 1) << 2) + (lane >> 3);
     return x < width && y < height;
 }
-inline int tile_blocks(int width, int height) { return ((width + 15) >> 4) * ((height + 15) >> 4); }
+template <int kThreads = 256>
+inline int tile_blocks(int width, int height) {
+    constexpr int kTileH = kThreads / 16;
+    return ((width + 15) >> 4) * ((height + kTileH - 1) / kTileH);
+}
 
 }  // namespace hdr

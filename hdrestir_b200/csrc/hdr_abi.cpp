@@ -736,16 +736,20 @@ hdr_status hdr_get_trace_tuning(hdr_ctx *c, hdr_trace_tuning *out) {
     out->node_quorum = c->tune.node_quorum;
     out->blocks_per_sm = c->tune.blocks_per_sm;
     out->trace_ms = 0.0f;
+    out->shade_shape = c->tune.shade_shape;
     return HDR_OK;
 }
 
 hdr_status hdr_set_trace_tuning(hdr_ctx *c, const hdr_trace_tuning *t) {
     if (!c || !t) return fail(HDR_EINVAL, "NULL argument");
-    if (t->node_quorum < 1 || t->node_quorum > 32 || t->blocks_per_sm < 1 || t->blocks_per_sm > 64)
-        return fail(HDR_EINVAL, "node_quorum must be 1..32 and blocks_per_sm 1..64");
+    if (t->node_quorum < 1 || t->node_quorum > 32 || t->blocks_per_sm < 1 || t->blocks_per_sm > 64 ||
+        t->shade_shape < 0 || t->shade_shape >= hdr::kShadeShapes)
+        return fail(HDR_EINVAL, "node_quorum must be 1..32, blocks_per_sm 1..64, shade_shape 0..%d",
+                    hdr::kShadeShapes - 1);
     std::lock_guard<std::mutex> lock(c->mu);
     c->tune.node_quorum = t->node_quorum;
     c->tune.blocks_per_sm = t->blocks_per_sm;
+    c->tune.shade_shape = t->shade_shape;
     return HDR_OK;
 }
 
@@ -789,6 +793,7 @@ hdr_status hdr_autotune_trace(hdr_ctx *c, hdr_trace_tuning *best) {
         best->node_quorum = pick.node_quorum;
         best->blocks_per_sm = pick.blocks_per_sm;
         best->trace_ms = pick_ms;
+        best->shade_shape = c->tune.shade_shape;
     }
     return read_device_error(c);
 }

@@ -67,10 +67,11 @@ struct PixelStart {
     bool has_hit;
 };
 
+template <int kThreads = 256>
 __device__ __forceinline__ bool pixel_start(const DeviceScene &s, const CameraD &cam, int frame_index,
                                             const GBufferView &gb, MtStream &rng, uint64_t *spill, PixelStart &ps) {
     int x, y;
-    if (!tile_pixel(cam.width, cam.height, x, y)) return false;
+    if (!tile_pixel<kThreads>(cam.width, cam.height, x, y)) return false;
     ps.i = (size_t)y * (size_t)cam.width + (size_t)x;
     rng.init((uint32_t)ps.i ^ (uint32_t)((unsigned long long)frame_index * 12345ULL), spill);
     const float px = (float)x + rng.next_float();
@@ -329,13 +330,15 @@ __global__ void __launch_bounds__(kTraceThreads) trace_shadow_kernel(DeviceScene
     if (e) atomicOr(err, e);
 }
 
-__global__ void __launch_bounds__(256) ris_shade_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
-                                                        RisRun ris, GBufferView gb, ReservoirView rv, WaveBuffers wb,
-                                                        float4 *color, int trace_bsdf, unsigned *err) {
+template <int kThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) ris_shade_kernel(DeviceScene s, CameraD cam, int frame_index,
+                                                                         PathRun pr, RisRun ris, GBufferView gb,
+                                                                         ReservoirView rv, WaveBuffers wb, float4 *color,
+                                                                         int trace_bsdf, unsigned *err) {
     uint64_t spill[312];
     MtStream rng;
     PixelStart ps;
-    if (!pixel_start(s, cam, frame_index, gb, rng, spill, ps)) return;
+    if (!pixel_start<kThreads>(s, cam, frame_index, gb, rng, spill, ps)) return;
     const size_t i = ps.i;
     if (wb.done[i]) return;
     unsigned e = 0;
@@ -405,7 +408,23 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
     if (launch_wave_trace(s, wb, tune, err, st, ev_begin ? ev_begin + 1 : nullptr, ev_end ? ev_end + 1 : nullptr) < 0)
         return -1;
     if (!mark(ev_begin, 3)) return -1;
-    ris_shade_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_bsdf, err);
+    switch (tune.shade_shape) {
+        case 1:
+            ris_shade_kernel<256, 2><<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color,
+                                                             trace_bsdf, err);
+            break;
+        case 2:
+            ris_shade_kernel<128, 3><<<tile_blocks<128>(cam.width, cam.height), 128, 0, st>>>(
+                s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_bsdf, err);
+            break;
+        case 3:
+            ris_shade_kernel<128, 4><<<tile_blocks<128>(cam.width, cam.height), 128, 0, st>>>(
+                s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_bsdf, err);
+            break;
+        default:
+            ris_shade_kernel<256, 1><<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color,
+                                                             trace_bsdf, err);
+    }
     if (!mark(ev_end, 3)) return -1;
     return cudaGetLastError() == cudaSuccess ? 4 : -1;
 }
