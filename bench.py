@@ -169,10 +169,13 @@ def run_reference(args, rank, world):
     use_ref = _ref_available()
     per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
     fps = []
+    ref = None
+    if use_ref:
+        from oracle import refharness
+        ref = refharness.Reference(scene)  # scene build, untimed like the GPU arm's upload
     for k in range(args.warmup + args.steps):
         if use_ref:
-            from oracle import refharness
-            sec, rows = refharness.cpu_sample(scene, cam, per_step, threads, frame=k)
+            sec, rows = refharness.cpu_sample(scene, cam, per_step, threads, frame=k, ref=ref)
         else:
             sec, rows = cpu_sample(scene, cam, per_step, threads, frame=0)
         if k >= args.warmup:

@@ -84,6 +84,7 @@ struct RefScene {
     Scene scene;
     std::vector<std::unique_ptr<RefMesh>> meshes;
     FrameBuffersMap store;
+    size_t store_pixels = 0;  // frame size the persistent buffers in `store` were made for
     std::unordered_map<const ILight *, int> light_index;
     std::string error;
 };
@@ -201,7 +202,10 @@ RefScene *ref_create(const hdr_scene_desc *d) {
 
 void ref_destroy(RefScene *rs) { delete rs; }
 
-void ref_clear_persistent(RefScene *rs) { rs->store.Clear(); }
+void ref_clear_persistent(RefScene *rs) {
+    rs->store.Clear();
+    rs->store_pixels = 0;
+}
 
 static void texel_from_hit(hdr_gbuffer_texel &t, const std::optional<HitRecord> &h) {
     std::memset(&t, 0, sizeof(t));
@@ -276,6 +280,12 @@ int ref_render_frame(RefScene *rs, const hdr_camera *cam, int frame_index, const
         else
             integ = std::make_unique<PathTracePass>(settings, p->max_depth);
         AccumulationPass accum{p->firefly != 0};
+        // A new frame size makes the renderer mark its integrand dirty and clear the
+        // persistent buffers (renderer.cpp:401-406); the passes index them by pixel.
+        if (rs->store_pixels != ctx.frame.PixelCount()) {
+            rs->store.Clear();
+            rs->store_pixels = ctx.frame.PixelCount();
+        }
         // RenderPipeline::Execute (pipeline/render_pipeline.cpp:24-40)
         ctx.buffers.InjectFrom(rs->store);
         raycast.Execute(ctx);

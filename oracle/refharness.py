@@ -165,12 +165,15 @@ def rng_floats(seeds, count) -> np.ndarray:
     return out
 
 
-def cpu_sample(scene, cam, budget_s: float, threads: int, frame: int = 0):
+def cpu_sample(scene, cam, budget_s: float, threads: int, frame: int = 0, ref: "Reference | None" = None):
     """Times the reference pipeline (Raycast -> RISPathTrace(32, reservoir) ->
-    Accumulation) on the host cores at the coarsest resolution level whose
-    frame fits the budget; returns (seconds per full-resolution frame, rows)."""
+    Accumulation) on the host cores at the finest resolution level whose frame
+    fits the budget; returns (seconds per full-resolution frame, rows). `ref`
+    reuses an already built reference scene (its build is not timed)."""
     os.environ["HDR_REF_THREADS"] = str(threads)
-    ref = Reference(scene)
+    own = ref is None
+    if own:
+        ref = Reference(scene)
     level, sec = 4, None
     while True:
         div = 1 << level
@@ -184,5 +187,6 @@ def cpu_sample(scene, cam, budget_s: float, threads: int, frame: int = 0):
         if level == 0 or dt * 4 > budget_s:
             break
         level -= 1
-    ref.close()
+    if own:
+        ref.close()
     return sec, rows

@@ -68,3 +68,16 @@ def test_trace_rays_match_reference():
     assert hit.sum() > 100
     for field in ("position", "depth", "normal", "smooth_normal", "albedo"):
         assert np.array_equal(bits(a[field][hit]), bits(b[field][hit])), field
+
+
+def test_reference_harness_survives_frame_size_changes():
+    """A new frame size clears the persistent buffers before the passes index
+    them (the reference renderer does the same), so the CPU baseline can sample
+    several resolution levels with one scene."""
+    sc, cam = configs.small_variant(2, 64, 48, grid=48, n_spheres=20, n_lights=100)
+    ref = refharness.Reference(sc)
+    for level in (2, 1, 0, 1):
+        _, c, _ = ref.render(cam, 0, ris=True, candidate_count=8, use_reservoir=True, max_depth=1,
+                             resolution_level=level, outputs=("color",))
+        assert np.isfinite(c).all()
+    ref.close()
