@@ -18,6 +18,30 @@ BUFFER_LAYOUT = {  # name -> (dtype, trailing shape)
 }
 
 
+def ris_params(candidate_count=16, use_reservoir=True, skip_visibility=False, m_cap=0, trace_all_rays=False,
+               one_kernel=False, **settings) -> abi.RisParams:
+    p = abi.RisParams()
+    p.path = path_settings(**settings)
+    p.candidate_count, p.use_reservoir, p.skip_visibility = int(candidate_count), int(use_reservoir), int(
+        skip_visibility)
+    p.m_cap = int(m_cap)
+    p.flags = (abi.RIS_TRACE_ALL_RAYS if trace_all_rays else 0) | (abi.RIS_ONE_KERNEL if one_kernel else 0)
+    return p
+
+
+def ris_path_trace_batch(contexts, cameras, frame_indices, **ris) -> None:
+    """One wavefront RIS frame for several images (one Context each, all sharing
+    one scene via Context.share_scene); each image gets what ris_path_trace gives it."""
+    n = len(contexts)
+    ctxs = (C.c_void_p * n)(*[c._h for c in contexts])
+    cams = (abi.CameraDesc * n)(*[cam.c_desc() for cam in cameras])
+    frames = (C.c_int32 * n)(*[int(f) for f in frame_indices])
+    p = ris_params(**ris)
+    params = (abi.RisParams * n)(*([p] * n))
+    lib = abi.lib()
+    abi.check(lib.hdr_ris_path_trace_batch(ctxs, n, cams, frames, params))
+
+
 def path_settings(max_depth=32, enable_subsurface=True, max_reflection_bounces=8, max_refraction_bounces=8,
                   render_ibl_background=True, roulette_aggressiveness=1.0) -> abi.PathSettings:
     """PathTracePassSettings (integrators/path_integrator.h:12-19) + maxDepth, with the reference defaults."""
@@ -60,6 +84,10 @@ class Context:
         desc = scene.c_desc()
         abi.check(self._lib.hdr_scene_upload(self._h, C.byref(desc)))
 
+    def share_scene(self, other: "Context") -> None:
+        """Render `other`'s resident scene (no second copy in HBM)."""
+        abi.check(self._lib.hdr_scene_share(self._h, other._h))
+
     # ------------------------------------------------------------ passes
     def raycast(self, cam: Camera, frame_index: int = 0, aovs=()) -> None:
         mask = 0
@@ -68,14 +96,8 @@ class Context:
         abi.check(self._lib.hdr_raycast(self._h, C.byref(cam.c_desc()), int(frame_index), mask))
         self.width, self.height = cam.width, cam.height
 
-    def ris_path_trace(self, cam: Camera, frame_index: int, candidate_count=16, use_reservoir=True,
-                       skip_visibility=False, m_cap=0, trace_all_rays=False, one_kernel=False, **settings) -> None:
-        p = abi.RisParams()
-        p.path = path_settings(**settings)
-        p.candidate_count, p.use_reservoir, p.skip_visibility = int(candidate_count), int(use_reservoir), int(
-            skip_visibility)
-        p.m_cap = int(m_cap)
-        p.flags = (abi.RIS_TRACE_ALL_RAYS if trace_all_rays else 0) | (abi.RIS_ONE_KERNEL if one_kernel else 0)
+    def ris_path_trace(self, cam: Camera, frame_index: int, **ris) -> None:
+        p = ris_params(**ris)
         abi.check(self._lib.hdr_ris_path_trace(self._h, C.byref(cam.c_desc()), int(frame_index), C.byref(p)))
 
     def path_trace(self, cam: Camera, frame_index: int, **settings) -> None:

@@ -78,6 +78,10 @@ struct WaveBuffers {
     unsigned char *done;  // pixels: 1 = no GBuffer hit, colour already written
     size_t pixels;
     int n_closest, n_shadow;
+    // added to the result slots the generate kernel writes into the queues: a
+    // batch of images shares one queue and one result array (0 for one image,
+    // whose hits / hit_v / occ then start at its own slot 0)
+    int slot_base_closest, slot_base_shadow;
 };
 
 // Returns the number of kernels launched, or -1 on a launch error.
@@ -103,6 +107,15 @@ constexpr int kShadeShapes = 4;
 // caller zeroes counts[2..3] before a rerun); returns the launches, -1 on error.
 int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &tune, unsigned *err, cudaStream_t st,
                       cudaEvent_t *ev_begin = nullptr, cudaEvent_t *ev_end = nullptr);
+// The three stages of the wavefront RIS pass on their own (a batch of images
+// runs every image's generate, one trace over their shared queues, then every
+// image's shade). Return the launches, -1 on a launch error.
+int launch_ris_generate(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                        GBufferView gb, WaveBuffers wb, float4 *color, int trace_bsdf, unsigned *err,
+                        cudaStream_t st);
+int launch_ris_shade(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                     GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf, unsigned *err,
+                     cudaStream_t st, const TraceTuning &tune);
 // ev_begin / ev_end (4 events each, or null): recorded around the generate,
 // trace-closest, trace-shadow and shade launches for per-kernel device times.
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -61,6 +62,23 @@ hdr_status set_last_error(hdr_status st, const char *fmt, ...) {
 }
 }  // namespace hdr
 
+// The device memory of one uploaded scene. Contexts hold it by shared_ptr so
+// several can render the same resident scene (hdr_scene_share); the memory is
+// freed when the last holder lets go, after that holder's stream is idle.
+struct SceneStore {
+    int device = 0;
+    std::vector<void *> ptrs;
+    size_t bytes = 0;
+    ~SceneStore() {
+        if (ptrs.empty()) return;
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        for (void *p : ptrs) cudaFree(p);
+        cudaSetDevice(prev);
+    }
+};
+
 // timing slots: 0 raycast, 1 integrate, 2 accumulate, then the wavefront
 // kernels 3 ris_generate, 4 trace_closest, 5 trace_shadow, 6 ris_shade
 constexpr int kTimeSlots = 7;
@@ -74,8 +92,9 @@ struct hdr_ctx {
     cudaStream_t stream = nullptr;
     std::mutex mu;
 
-    // resident scene
-    std::vector<DevBuf> scene_bufs;
+    // resident scene (scene_store owns the memory; the fields below describe it)
+    std::shared_ptr<SceneStore> scene_store;
+    size_t scene_bytes_accounted = 0;  // part of `allocated` this ctx uploaded for its scene
     hdr::DeviceScene scene{};
     bool has_scene = false;
     bool scene_opaque = true;          // every material has opacity >= 0.999 (no stochastic pass-through)
@@ -103,6 +122,7 @@ struct hdr_ctx {
     hdr::TraceTuning tune;
     hdr::WaveBuffers last_wave{};
     bool have_wave = false;
+    cudaEvent_t sync_ev = nullptr;  // orders this ctx's stream against a batch's lead stream
 };
 
 namespace {
@@ -288,6 +308,7 @@ hdr_status hdr_ctx_create(hdr_ctx **out, const hdr_ctx_desc *desc) {
         e = cudaEventCreate(&c->region_ev[k][0]);
         if (e == cudaSuccess) e = cudaEventCreate(&c->region_ev[k][1]);
     }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->sync_ev, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         hdr_ctx_destroy(c);
         return fail(HDR_ECUDA, "context setup: %s", cudaGetErrorString(e));
@@ -306,7 +327,7 @@ void hdr_ctx_destroy(hdr_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (auto &b : c->scene_bufs) dev_free(c, b);
+    c->scene_store.reset();
     for (auto &kv : c->buffers) dev_free(c, kv.second);
     if (c->d_err) cudaFree(c->d_err);
     for (int k = 0; k < kTimeSlots; ++k) {
@@ -316,6 +337,7 @@ void hdr_ctx_destroy(hdr_ctx *c) {
     for (auto &pair : c->region_ev)
         for (auto &e : pair)
             if (e) cudaEventDestroy(e);
+    if (c->sync_ev) cudaEventDestroy(c->sync_ev);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -336,16 +358,22 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
         return fail(HDR_EINVAL, "wide BVH depth %d + wide TLAS depth %d exceeds the device traversal stack (%d)",
                     f.max_blas4_depth, f.max_tlas4_depth, hdr::kWideStack);
     HDR_CUDA(cudaStreamSynchronize(c->stream));
-    for (auto &b : c->scene_bufs) dev_free(c, b);
-    c->scene_bufs.clear();
+    // this ctx lets go of its scene (another ctx sharing it keeps the memory alive)
+    c->scene_store.reset();
+    c->allocated -= c->scene_bytes_accounted;
+    c->scene_bytes_accounted = 0;
     c->has_scene = false;
+    c->have_wave = false;
 
+    auto store = std::make_shared<SceneStore>();
+    store->device = c->device;
     auto upload = [&](const void *src, size_t bytes, const void **dst) -> hdr_status {
         DevBuf b;
         hdr_status st = dev_alloc(c, b, std::max<size_t>(bytes, 16));
         if (st != HDR_OK) return st;
+        store->ptrs.push_back(b.ptr);
+        store->bytes += b.bytes;
         if (bytes) HDR_CUDA(cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, c->stream));
-        c->scene_bufs.push_back(b);
         *dst = b.ptr;
         return HDR_OK;
     };
@@ -353,7 +381,11 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     hdr_status st;
 #define UP(vec, field)                                                                              \
     st = upload(vec.data(), vec.size() * sizeof(vec[0]), (const void **)&s.field);                   \
-    if (st != HDR_OK) return st;
+    if (st != HDR_OK) {                                                                             \
+        cudaStreamSynchronize(c->stream);                                                           \
+        c->allocated -= store->bytes;                                                               \
+        return st;                                                                                  \
+    }
     UP(f.blas_nodes, blas_nodes);
     UP(f.tri_geo, tri_geo);
     UP(f.tri_attr, tri_attr);
@@ -380,7 +412,10 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     s.dome_height = f.dome_height;
     s.dome_total_lum = f.dome_total_lum;
     s.has_tlas = f.num_instances > 0 ? 1 : 0;
-    HDR_CUDA(cudaStreamSynchronize(c->stream));
+    const cudaError_t sync_err = cudaStreamSynchronize(c->stream);
+    c->scene_store = store;  // owns the buffers from here on, also on the error path below
+    c->scene_bytes_accounted = store->bytes;
+    if (sync_err != cudaSuccess) return fail(HDR_ECUDA, "scene upload: %s", cudaGetErrorString(sync_err));
     c->scene = s;
     c->has_scene = true;
     c->have_wave = false;
@@ -513,6 +548,201 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
     hdr::launch_ris_path_trace(c->scene, cd, frame_index, d, gb, rv, (float4 *)color, c->d_err, c->stream);
     c->launches += 1;
     return end_pass(c, 1);
+}
+
+hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src) {
+    if (!dst || !src || dst == src) return fail(HDR_EINVAL, "need two distinct contexts");
+    if (dst->device != src->device) return fail(HDR_EINVAL, "contexts are on different devices");
+    std::lock(dst->mu, src->mu);
+    std::lock_guard<std::mutex> l1(dst->mu, std::adopt_lock), l2(src->mu, std::adopt_lock);
+    if (!src->has_scene) return fail(HDR_ENOSCENE, "the source context has no scene");
+    HDR_CUDA(cudaSetDevice(dst->device));
+    HDR_CUDA(cudaStreamSynchronize(dst->stream));  // dst's old scene may still be in use on its stream
+    dst->scene_store = src->scene_store;
+    dst->allocated -= dst->scene_bytes_accounted;
+    dst->scene_bytes_accounted = 0;
+    dst->scene = src->scene;
+    dst->scene.wide = (dst->flags & HDR_CTX_WIDE_BVH) ? 1 : 0;
+    dst->scene_opaque = src->scene_opaque;
+    dst->scene_light_geometry = src->scene_light_geometry;
+    dst->has_scene = true;
+    dst->have_wave = false;
+    return HDR_OK;
+}
+
+namespace {
+
+// Everything one image of a wavefront RIS frame needs, prepared on its own ctx.
+struct RisJob {
+    hdr_ctx *c;
+    hdr::CameraD cd;
+    hdr::RisParamsD d;
+    hdr::GBufferView gb;
+    hdr::ReservoirView rv;
+    float4 *color;
+    int frame;
+    int trace_bsdf;
+    size_t count;
+    int n_closest, n_shadow;
+    uint4 *rng_state;
+    unsigned char *done;
+};
+
+hdr_status prepare_ris_job(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, const hdr_ris_params *p,
+                           RisJob &j) {
+    hdr_status st = check_camera(cam);
+    if (st != HDR_OK) return st;
+    if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_ris_path_trace_batch before hdr_scene_upload");
+    if (p->candidate_count < 1 || p->candidate_count > 4096)
+        return fail(HDR_EINVAL, "candidate_count %d out of range [1, 4096]", p->candidate_count);
+    if ((st = check_cancel(c)) != HDR_OK) return st;
+    j.c = c;
+    j.frame = frame_index;
+    j.count = (size_t)cam->width * cam->height;
+    if ((st = gbuffer_view(c, j.count, false, j.gb)) != HDR_OK) return st;
+    void *q = nullptr;
+    if ((st = ensure_buffer(c, "Color", j.count * 16, &q)) != HDR_OK) return st;
+    j.color = (float4 *)q;
+    j.rv = hdr::ReservoirView{};
+    if (p->use_reservoir) {
+        if ((st = ensure_buffer(c, "__ris_reservoir", j.count * kResPlanes * sizeof(float4), &q)) != HDR_OK) return st;
+        float4 *r = (float4 *)q;
+        j.rv = hdr::ReservoirView{r, r + j.count, r + 2 * j.count, r + 3 * j.count, r + 4 * j.count};
+    }
+    hdr::RisParamsD &d = j.d;
+    d = hdr::RisParamsD{};
+    d.candidate_count = p->candidate_count;
+    d.use_reservoir = p->use_reservoir;
+    d.skip_visibility = p->skip_visibility;
+    d.max_depth = p->path.max_depth;
+    d.enable_subsurface = p->path.enable_subsurface;
+    d.max_refl = p->path.max_reflection_bounces;
+    d.max_refr = p->path.max_refraction_bounces;
+    d.render_ibl_background = p->path.render_ibl_background;
+    d.roulette = p->path.roulette_aggressiveness;
+    d.m_cap = p->m_cap;
+    d.spatial_neighbors = p->spatial_neighbors;
+    d.spatial_radius = p->spatial_radius;
+    j.cd = make_camera(cam);
+    const int n_nee = std::max(1, p->candidate_count / 2);
+    j.n_closest = 1 + std::max(0, p->candidate_count - n_nee);
+    j.n_shadow = n_nee;
+    if ((st = ensure_buffer(c, "__wave_rng", j.count * 48, &q)) != HDR_OK) return st;
+    j.rng_state = (uint4 *)q;
+    if ((st = ensure_buffer(c, "__wave_done", j.count, &q)) != HDR_OK) return st;
+    j.done = (unsigned char *)q;
+    j.trace_bsdf = ((p->flags & HDR_RIS_TRACE_ALL_RAYS) || c->scene_light_geometry || c->scene.env_light >= 0) ? 1 : 0;
+    return HDR_OK;
+}
+
+}  // namespace
+
+hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camera *cams,
+                                    const int32_t *frame_indices, const hdr_ris_params *params) {
+    if (!ctxs || !cams || !frame_indices || !params || n < 1 || n > 1024) return fail(HDR_EINVAL, "bad argument");
+    for (int32_t i = 0; i < n; ++i)
+        if (!ctxs[i]) return fail(HDR_EINVAL, "ctx %d is NULL", i);
+    // one shared trace needs one resident scene, one device and the wavefront form for every image;
+    // otherwise the images are rendered one after another
+    bool together = n > 1;
+    for (int32_t i = 0; i < n && together; ++i) {
+        hdr_ctx *c = ctxs[i];
+        const hdr_ris_params *p = &params[i];
+        together = c->device == ctxs[0]->device && c->has_scene && c->scene_store &&
+                   c->scene_store == ctxs[0]->scene_store && c->scene.wide == ctxs[0]->scene.wide &&
+                   p->path.max_depth == 1 && c->scene_opaque && !(p->flags & HDR_RIS_ONE_KERNEL);
+    }
+    std::vector<hdr_ctx *> order(ctxs, ctxs + n);
+    std::sort(order.begin(), order.end());
+    if (std::adjacent_find(order.begin(), order.end()) != order.end())
+        return fail(HDR_EINVAL, "a context appears twice in the batch");
+    if (!together) {
+        for (int32_t i = 0; i < n; ++i) {
+            const hdr_status st = hdr_ris_path_trace(ctxs[i], &cams[i], frame_indices[i], &params[i]);
+            if (st != HDR_OK) return st;
+        }
+        return HDR_OK;
+    }
+    for (hdr_ctx *c : order) c->mu.lock();  // address order: no deadlock between batches
+    struct Unlock {
+        std::vector<hdr_ctx *> &v;
+        ~Unlock() {
+            for (hdr_ctx *c : v) c->mu.unlock();
+        }
+    } unlock{order};
+    hdr_ctx *lead = ctxs[0];
+    HDR_CUDA(cudaSetDevice(lead->device));
+    std::vector<RisJob> jobs((size_t)n);
+    std::vector<long long> base_c((size_t)n), base_s((size_t)n);
+    long long total_c = 0, total_s = 0;
+    hdr_status st;
+    for (int32_t i = 0; i < n; ++i) {
+        if ((st = prepare_ris_job(ctxs[i], &cams[i], frame_indices[i], &params[i], jobs[(size_t)i])) != HDR_OK)
+            return st;
+        base_c[(size_t)i] = total_c;
+        base_s[(size_t)i] = total_s;
+        total_c += (long long)jobs[(size_t)i].count * jobs[(size_t)i].n_closest;
+        total_s += (long long)jobs[(size_t)i].count * jobs[(size_t)i].n_shadow;
+    }
+    if (total_c >= (1ll << 31) || total_s >= (1ll << 31))
+        return fail(HDR_EINVAL, "batch of %lld closest / %lld shadow ray slots exceeds 2^31", total_c, total_s);
+    // the shared queues and result slots live on the lead ctx
+    hdr::WaveBuffers all{};
+    void *q;
+    if ((st = ensure_buffer(lead, "__batch_q_closest", (size_t)total_c * 32, &q)) != HDR_OK) return st;
+    all.q_closest = (float4 *)q;
+    if ((st = ensure_buffer(lead, "__batch_q_shadow", (size_t)total_s * 32, &q)) != HDR_OK) return st;
+    all.q_shadow = (float4 *)q;
+    if ((st = ensure_buffer(lead, "__batch_counts", 16, &q)) != HDR_OK) return st;
+    all.counts = (int *)q;
+    if ((st = ensure_buffer(lead, "__batch_hits", (size_t)total_c * 16, &q)) != HDR_OK) return st;
+    all.hits = (float4 *)q;
+    if ((st = ensure_buffer(lead, "__batch_hit_v", (size_t)total_c * 4, &q)) != HDR_OK) return st;
+    all.hit_v = (float *)q;
+    if ((st = ensure_buffer(lead, "__batch_occ", (size_t)total_s, &q)) != HDR_OK) return st;
+    all.occ = (unsigned char *)q;
+    // every image's earlier work (its raycast) runs on its own stream: the lead stream waits for it
+    for (int32_t i = 1; i < n; ++i) {
+        HDR_CUDA(cudaEventRecord(ctxs[i]->sync_ev, ctxs[i]->stream));
+        HDR_CUDA(cudaStreamWaitEvent(lead->stream, ctxs[i]->sync_ev, 0));
+    }
+    if ((st = begin_pass(lead, 1)) != HDR_OK) return st;
+    cudaStream_t s = lead->stream;
+    HDR_CUDA(cudaMemsetAsync(all.counts, 0, 16, s));
+    std::vector<hdr::WaveBuffers> wbs((size_t)n);
+    for (int32_t i = 0; i < n; ++i) {
+        const RisJob &j = jobs[(size_t)i];
+        hdr::WaveBuffers &wb = wbs[(size_t)i];
+        wb = all;
+        wb.hits = all.hits + base_c[(size_t)i];
+        wb.hit_v = all.hit_v + base_c[(size_t)i];
+        wb.occ = all.occ + base_s[(size_t)i];
+        wb.rng_state = j.rng_state;
+        wb.done = j.done;
+        wb.pixels = j.count;
+        wb.n_closest = j.n_closest;
+        wb.n_shadow = j.n_shadow;
+        wb.slot_base_closest = (int)base_c[(size_t)i];
+        wb.slot_base_shadow = (int)base_s[(size_t)i];
+        if (hdr::launch_ris_generate(lead->scene, j.cd, j.frame, j.d, j.gb, wb, j.color, j.trace_bsdf, j.c->d_err,
+                                     s) < 0)
+            return fail(HDR_ECUDA, "generate launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    if (hdr::launch_wave_trace(lead->scene, all, lead->tune, lead->d_err, s) < 0)
+        return fail(HDR_ECUDA, "trace launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    for (int32_t i = 0; i < n; ++i) {
+        const RisJob &j = jobs[(size_t)i];
+        if (hdr::launch_ris_shade(lead->scene, j.cd, j.frame, j.d, j.gb, j.rv, wbs[(size_t)i], j.color, j.trace_bsdf,
+                                  j.c->d_err, s, lead->tune) < 0)
+            return fail(HDR_ECUDA, "shade launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    // later work on each image's own stream (accumulate, download) waits for the batch
+    HDR_CUDA(cudaEventRecord(lead->sync_ev, s));
+    for (int32_t i = 1; i < n; ++i) HDR_CUDA(cudaStreamWaitEvent(ctxs[i]->stream, lead->sync_ev, 0));
+    lead->launches += (uint64_t)(2 * n + 2);
+    lead->last_wave = all;
+    lead->have_wave = true;
+    return end_pass(lead, 1);
 }
 
 hdr_status hdr_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, const hdr_path_settings *p) {

@@ -112,7 +112,8 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
     {
         const int q = queue_append(&wb.counts[0], fb.ok);
         if (q >= 0) {
-            wb.q_closest[2 * (size_t)q] = make_float4(fb.origin.x, fb.origin.y, fb.origin.z, __int_as_float((int)cbase));
+            wb.q_closest[2 * (size_t)q] =
+                make_float4(fb.origin.x, fb.origin.y, fb.origin.z, __int_as_float(wb.slot_base_closest + (int)cbase));
             wb.q_closest[2 * (size_t)q + 1] = make_float4(fb.dir.x, fb.dir.y, fb.dir.z, 0.0f);
         }
     }
@@ -128,7 +129,8 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
                           ris_nee_shadow_ray(s, sf, li, ls, ris.skip_vis, o, d, lim);
         const int q = queue_append(&wb.counts[1], want);
         if (q >= 0) {
-            wb.q_shadow[2 * (size_t)q] = make_float4(o.x, o.y, o.z, __int_as_float((int)(sbase + j)));
+            wb.q_shadow[2 * (size_t)q] =
+                make_float4(o.x, o.y, o.z, __int_as_float(wb.slot_base_shadow + (int)(sbase + j)));
             wb.q_shadow[2 * (size_t)q + 1] = make_float4(d.x, d.y, d.z, lim);
         }
     }
@@ -140,7 +142,7 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
         const int q = queue_append(&wb.counts[0], b.ok && trace_bsdf);
         if (q >= 0) {
             wb.q_closest[2 * (size_t)q] = make_float4(b.origin.x, b.origin.y, b.origin.z,
-                                                      __int_as_float((int)(cbase + 1 + k)));
+                                                      __int_as_float(wb.slot_base_closest + (int)(cbase + 1 + k)));
             wb.q_closest[2 * (size_t)q + 1] = make_float4(b.dir.x, b.dir.y, b.dir.z, 0.0f);
         }
     }
@@ -382,10 +384,8 @@ int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &t
     return cudaGetLastError() == cudaSuccess ? 2 : -1;
 }
 
-int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
-                         GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
-                         unsigned *err, cudaStream_t st, const TraceTuning &tune, cudaEvent_t *ev_begin,
-                         cudaEvent_t *ev_end) {
+namespace {
+PathRun path_run(const RisParamsD &p) {
     PathRun pr;
     pr.max_depth = p.max_depth;
     pr.enable_subsurface = p.enable_subsurface != 0;
@@ -393,21 +393,33 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
     pr.max_refr = p.max_refr;
     pr.render_ibl_background = p.render_ibl_background != 0;
     pr.roulette = p.roulette;
+    return pr;
+}
+RisRun ris_run(const RisParamsD &p) {
     RisRun ris;
     ris.candidate_count = p.candidate_count;
     ris.use_reservoir = p.use_reservoir != 0;
     ris.skip_vis = p.skip_visibility != 0;
     ris.m_cap = p.m_cap;
-    // [0] closest rays queued, [1] shadow rays queued, [2] / [3] shadow / closest rays handed out
-    if (cudaMemsetAsync(wb.counts, 0, 4 * sizeof(int), st) != cudaSuccess) return -1;
+    return ris;
+}
+}  // namespace
+
+int launch_ris_generate(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                        GBufferView gb, WaveBuffers wb, float4 *color, int trace_bsdf, unsigned *err,
+                        cudaStream_t st) {
+    ris_generate_kernel<<<tile_blocks(cam.width, cam.height), 256, 0, st>>>(s, cam, frame_index, path_run(p),
+                                                                             ris_run(p), gb, wb, color, trace_bsdf,
+                                                                             err);
+    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+}
+
+int launch_ris_shade(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                     GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf, unsigned *err,
+                     cudaStream_t st, const TraceTuning &tune) {
+    const PathRun pr = path_run(p);
+    const RisRun ris = ris_run(p);
     const int blocks = tile_blocks(cam.width, cam.height);
-    auto mark = [&](cudaEvent_t *ev, int k) { return !ev || cudaEventRecord(ev[k], st) == cudaSuccess; };
-    if (!mark(ev_begin, 0)) return -1;
-    ris_generate_kernel<<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, wb, color, trace_bsdf, err);
-    if (!mark(ev_end, 0)) return -1;
-    if (launch_wave_trace(s, wb, tune, err, st, ev_begin ? ev_begin + 1 : nullptr, ev_end ? ev_end + 1 : nullptr) < 0)
-        return -1;
-    if (!mark(ev_begin, 3)) return -1;
     switch (tune.shade_shape) {
         case 1:
             ris_shade_kernel<256, 2><<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color,
@@ -425,8 +437,25 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
             ris_shade_kernel<256, 1><<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color,
                                                              trace_bsdf, err);
     }
+    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+}
+
+int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                         GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
+                         unsigned *err, cudaStream_t st, const TraceTuning &tune, cudaEvent_t *ev_begin,
+                         cudaEvent_t *ev_end) {
+    // [0] closest rays queued, [1] shadow rays queued, [2] / [3] shadow / closest rays handed out
+    if (cudaMemsetAsync(wb.counts, 0, 4 * sizeof(int), st) != cudaSuccess) return -1;
+    auto mark = [&](cudaEvent_t *ev, int k) { return !ev || cudaEventRecord(ev[k], st) == cudaSuccess; };
+    if (!mark(ev_begin, 0)) return -1;
+    if (launch_ris_generate(s, cam, frame_index, p, gb, wb, color, trace_bsdf, err, st) < 0) return -1;
+    if (!mark(ev_end, 0)) return -1;
+    if (launch_wave_trace(s, wb, tune, err, st, ev_begin ? ev_begin + 1 : nullptr, ev_end ? ev_end + 1 : nullptr) < 0)
+        return -1;
+    if (!mark(ev_begin, 3)) return -1;
+    if (launch_ris_shade(s, cam, frame_index, p, gb, rv, wb, color, trace_bsdf, err, st, tune) < 0) return -1;
     if (!mark(ev_end, 3)) return -1;
-    return cudaGetLastError() == cudaSuccess ? 4 : -1;
+    return 4;
 }
 
 }  // namespace hdr

@@ -243,6 +243,12 @@ const char *hdr_last_error(void);
  * the scene stays resident until the next upload. */
 hdr_status hdr_scene_upload(hdr_ctx *ctx, const hdr_scene_desc *scene);
 
+/* No reference counterpart (the reference builds a Scene per delegate). dst
+ * renders src's resident scene without a second copy in HBM; both must be on
+ * one device. The memory lives until the last context holding it uploads
+ * another scene or is destroyed. Required for hdr_ris_path_trace_batch. */
+hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src);
+
 /* RaycastPass::_execute (passes/raycast_pass.cpp:57-162): GBuffer (+AOVs). */
 hdr_status hdr_raycast(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_index, uint32_t aov_mask);
 
@@ -251,6 +257,19 @@ hdr_status hdr_raycast(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_index,
  * reads GBuffer and "__ris_reservoir", writes "Color" and the reservoirs. */
 hdr_status hdr_ris_path_trace(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_index,
                               const hdr_ris_params *params);
+
+/* Batched RISPathTracePass, no reference counterpart: n images (one ctx each,
+ * all sharing one resident scene through hdr_scene_share, each after its own
+ * hdr_raycast) in one wavefront frame. Every image's generate kernel appends
+ * its rays to one queue, one closest-hit and one shadow launch trace them all,
+ * then each image is resampled into its own "Color" and "__ris_reservoir".
+ * Each image's results are those of hdr_ris_path_trace on its ctx. Images
+ * that cannot take the wavefront form (max_depth > 1, non-opaque scene,
+ * HDR_RIS_ONE_KERNEL) or do not share the scene are rendered one after
+ * another instead. The work runs on ctxs[0]'s stream; the other ctxs' streams
+ * are ordered before and after it. A context may appear only once. */
+hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camera *cams,
+                                    const int32_t *frame_indices, const hdr_ris_params *params);
 
 /* PathTracePass (passes/path_trace_pass.h:12-39) with MisDirectLightIntegrator. */
 hdr_status hdr_path_trace(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_index,
