@@ -86,6 +86,20 @@ class TraceTuning(C.Structure):
     _fields_ = [("node_quorum", _i), ("blocks_per_sm", _i), ("trace_ms", _f), ("shade_shape", _i)]
 
 
+class ServerDesc(C.Structure):
+    _fields_ = [("device", _i), ("flags", C.c_uint32), ("hbm_budget_bytes", C.c_size_t), ("max_batch", _i)]
+
+
+class JobDesc(C.Structure):
+    _fields_ = [("scene", _i), ("pipeline", _i), ("frames", _i), ("firefly", _i), ("camera", CameraDesc),
+                ("ris", RisParams)]
+
+
+SERVER_SERIAL = 1
+JOB_PATH_TRACER, JOB_RIS = 0, 1
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
+
 class CtxDesc(C.Structure):
     _fields_ = [("device", _i), ("flags", C.c_uint32), ("hbm_budget_bytes", C.c_size_t)]
 
@@ -148,6 +162,14 @@ def lib() -> C.CDLL:
             "hdr_region_begin": (C.c_int, [vp, i32]),
             "hdr_region_end": (C.c_int, [vp, i32]),
             "hdr_region_elapsed": (C.c_int, [vp, i32, C.POINTER(C.c_float)]),
+            "hdr_server_create": (C.c_int, [C.POINTER(vp), C.POINTER(ServerDesc)]),
+            "hdr_server_destroy": (None, [vp]),
+            "hdr_server_add_scene": (C.c_int, [vp, C.POINTER(SceneDesc), C.POINTER(i32)]),
+            "hdr_server_submit": (C.c_int, [vp, C.POINTER(JobDesc), C.POINTER(C.c_int64)]),
+            "hdr_server_step": (C.c_int, [vp, C.POINTER(i32)]),
+            "hdr_server_job_state": (C.c_int, [vp, C.c_int64, C.POINTER(i32), C.POINTER(i32)]),
+            "hdr_server_take_result": (C.c_int, [vp, C.c_int64, vp, sz]),
+            "hdr_server_load": (C.c_int, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(sz)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

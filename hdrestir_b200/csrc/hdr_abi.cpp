@@ -173,6 +173,27 @@ hdr_status ensure_buffer(hdr_ctx *c, const char *name, size_t bytes, void **out)
     return HDR_OK;
 }
 
+// Per-frame scratch: reused while large enough, replaced (not copied) when it
+// must grow; every frame writes what it reads, so contents are not kept.
+hdr_status ensure_scratch(hdr_ctx *c, const char *name, size_t bytes, void **out) {
+    auto it = c->buffers.find(name);
+    if (it != c->buffers.end() && it->second.bytes >= bytes) {
+        *out = it->second.ptr;
+        return HDR_OK;
+    }
+    if (it != c->buffers.end()) {
+        HDR_CUDA(cudaStreamSynchronize(c->stream));
+        dev_free(c, it->second);
+        c->buffers.erase(it);
+    }
+    DevBuf nb;
+    hdr_status st = dev_alloc(c, nb, std::max<size_t>(bytes, 16));
+    if (st != HDR_OK) return st;
+    c->buffers[name] = nb;
+    *out = nb.ptr;
+    return HDR_OK;
+}
+
 void *find_buffer(hdr_ctx *c, const char *name, size_t *bytes) {
     auto it = c->buffers.find(name);
     if (it == c->buffers.end()) return nullptr;
@@ -689,17 +710,17 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
     // the shared queues and result slots live on the lead ctx
     hdr::WaveBuffers all{};
     void *q;
-    if ((st = ensure_buffer(lead, "__batch_q_closest", (size_t)total_c * 32, &q)) != HDR_OK) return st;
+    if ((st = ensure_scratch(lead, "__batch_q_closest", (size_t)total_c * 32, &q)) != HDR_OK) return st;
     all.q_closest = (float4 *)q;
-    if ((st = ensure_buffer(lead, "__batch_q_shadow", (size_t)total_s * 32, &q)) != HDR_OK) return st;
+    if ((st = ensure_scratch(lead, "__batch_q_shadow", (size_t)total_s * 32, &q)) != HDR_OK) return st;
     all.q_shadow = (float4 *)q;
-    if ((st = ensure_buffer(lead, "__batch_counts", 16, &q)) != HDR_OK) return st;
+    if ((st = ensure_scratch(lead, "__batch_counts", 16, &q)) != HDR_OK) return st;
     all.counts = (int *)q;
-    if ((st = ensure_buffer(lead, "__batch_hits", (size_t)total_c * 16, &q)) != HDR_OK) return st;
+    if ((st = ensure_scratch(lead, "__batch_hits", (size_t)total_c * 16, &q)) != HDR_OK) return st;
     all.hits = (float4 *)q;
-    if ((st = ensure_buffer(lead, "__batch_hit_v", (size_t)total_c * 4, &q)) != HDR_OK) return st;
+    if ((st = ensure_scratch(lead, "__batch_hit_v", (size_t)total_c * 4, &q)) != HDR_OK) return st;
     all.hit_v = (float *)q;
-    if ((st = ensure_buffer(lead, "__batch_occ", (size_t)total_s, &q)) != HDR_OK) return st;
+    if ((st = ensure_scratch(lead, "__batch_occ", (size_t)total_s, &q)) != HDR_OK) return st;
     all.occ = (unsigned char *)q;
     // every image's earlier work (its raycast) runs on its own stream: the lead stream waits for it
     for (int32_t i = 1; i < n; ++i) {

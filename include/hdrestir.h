@@ -271,6 +271,51 @@ hdr_status hdr_ris_path_trace(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame
 hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camera *cams,
                                     const int32_t *frame_indices, const hdr_ris_params *params);
 
+/* ---------------------------------------------------------------------------
+ * Render-job server (no reference counterpart; the reference renders one job
+ * per Hydra delegate). Scenes are uploaded once and shared; jobs are admitted
+ * first-in first-out while the estimate of their frame buffers fits the HBM
+ * budget; each hdr_server_step advances every admitted job by one frame, with
+ * the RIS jobs of one scene traced in one batched launch and path-traced jobs
+ * side by side on their own streams. HDR_SERVER_SERIAL runs one job at a
+ * time, each frame alone (the plain per-frame pipeline). A job's image is the
+ * same in both modes. Calls on one server are serialised by its mutex.
+ * ------------------------------------------------------------------------- */
+typedef struct hdr_server hdr_server;
+#define HDR_SERVER_SERIAL 1u
+
+typedef struct hdr_server_desc {
+    int32_t device;
+    uint32_t flags;            /* HDR_SERVER_* */
+    size_t hbm_budget_bytes;   /* admission budget for the jobs' frame buffers, 0 = unlimited */
+    int32_t max_batch;         /* images per batched RIS launch, 0 = 64 */
+} hdr_server_desc;
+
+enum { HDR_JOB_PATH_TRACER = 0, HDR_JOB_RIS = 1 };
+enum { HDR_JOB_QUEUED = 0, HDR_JOB_RUNNING = 1, HDR_JOB_DONE = 2, HDR_JOB_FAILED = 3 };
+
+typedef struct hdr_job_desc {
+    int32_t scene;             /* id from hdr_server_add_scene */
+    int32_t pipeline;          /* HDR_JOB_PATH_TRACER or HDR_JOB_RIS */
+    int32_t frames;            /* frames to accumulate (samples per pixel), >= 1 */
+    int32_t firefly;           /* AccumulationPass firefly filter */
+    hdr_camera camera;         /* static over the job's frames */
+    hdr_ris_params ris;        /* RIS settings; ris.path also configures the PathTracer pipeline */
+} hdr_job_desc;
+
+hdr_status hdr_server_create(hdr_server **out, const hdr_server_desc *desc);
+void hdr_server_destroy(hdr_server *server);
+hdr_status hdr_server_add_scene(hdr_server *server, const hdr_scene_desc *scene, int32_t *scene_id);
+hdr_status hdr_server_submit(hdr_server *server, const hdr_job_desc *job, int64_t *job_id);
+/* Admits what fits, renders one frame of every admitted job, and returns the
+ * number of jobs that finished (DONE or FAILED) in this step. */
+hdr_status hdr_server_step(hdr_server *server, int32_t *jobs_finished);
+hdr_status hdr_server_job_state(hdr_server *server, int64_t job_id, int32_t *state, int32_t *frames_done);
+/* Copies a finished job's "Color" (width*height RGBA f32; rgba may be NULL to
+ * discard it) and frees the job. */
+hdr_status hdr_server_take_result(hdr_server *server, int64_t job_id, float *rgba, size_t bytes);
+hdr_status hdr_server_load(hdr_server *server, int32_t *queued, int32_t *running, size_t *bytes_in_use);
+
 /* PathTracePass (passes/path_trace_pass.h:12-39) with MisDirectLightIntegrator. */
 hdr_status hdr_path_trace(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_index,
                           const hdr_path_settings *settings);
