@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the batched and served legs")
+    ap.add_argument("--serving-jobs", type=int, default=40, help="config-4 jobs per serving leg")
     ap.add_argument("--width", type=int, default=1920, help="smaller frames only for profiler captures")
     ap.add_argument("--height", type=int, default=1080)
     return ap.parse_args()
@@ -204,6 +206,119 @@ def config_block():
             "parallelism": "replicas"}
 
 
+def batched_leg(ctx, n_images=4, frames=4, warm=2):
+    """4 orbit views of the config-2 scene at 1920x1080, ReSTIR as in the headline:
+    rendered one after another (plain) and as one batched frame (one trace launch
+    for all images). Device-synchronised wall time around each leg (the images
+    run on several streams); images are identical (tests/test_gpu_batch.py)."""
+    import torch
+    from hdrestir_b200 import configs
+    from hdrestir_b200.context import Context, ris_path_trace_batch
+    ris = configs.RIS_CONFIG2
+    cams = [configs.orbit_camera(0.9 * k, WIDTH, HEIGHT) for k in range(n_images)]
+    ctxs = [Context(device=torch.cuda.current_device(), timings=False) for _ in cams]
+    out = {}
+    try:
+        for c in ctxs:
+            c.share_scene(ctx)
+        for mode in ("plain", "batched"):
+            for c in ctxs:
+                c.clear_persistent()
+
+            def frame(k):
+                for c, cam in zip(ctxs, cams):
+                    c.raycast(cam, k)
+                if mode == "batched":
+                    ris_path_trace_batch(ctxs, cams, [k] * len(cams), **ris)
+                else:
+                    for c, cam in zip(ctxs, cams):
+                        c.ris_path_trace(cam, k, **ris)
+                for c in ctxs:
+                    c.accumulate(k)
+
+            for k in range(warm):
+                frame(k)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for k in range(warm, warm + frames):
+                frame(k)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            out[mode] = {"frames_per_s": n_images * frames / dt, "ms_per_batch_frame": 1000.0 * dt / frames}
+    finally:
+        for c in ctxs:
+            c.close()
+    out["workload"] = f"{n_images} views of config 2 at {WIDTH}x{HEIGHT}, {frames} timed frames each"
+    return out
+
+
+def serving_leg(n_jobs: int):
+    """Config-4 serving: the same Poisson job stream (200 jobs/s) through the
+    server in serial mode (the plain per-frame pipeline, one job at a time) and
+    in served mode (continuous batching). Latency = host wall time from a job's
+    arrival to the step that finished it; images are identical in both modes
+    (tests/test_gpu_server.py), so the comparison is at equal MSE."""
+    from hdrestir_b200 import abi, configs
+    from hdrestir_b200.server import Server
+    jobs = configs.config4_jobs(n_jobs)
+    scenes = [configs.config0()[0], configs.config1()[0], configs.config2()[0]]
+    cams = [configs.config_camera(j["cfg"], j["width"], j["height"]) for j in jobs]
+    mpx_frames = sum(j["width"] * j["height"] * j["frames"] for j in jobs) / 1e6
+    out = {"workload": f"config 4: {n_jobs} jobs, Poisson 200 jobs/s, scenes config 0-2, "
+                       "256^2..2048x1152, 1-16 frames, ReSTIR (32 cand) or PathTracer (maxDepth 4); "
+                       "HBM admission budget 120 GB",
+           "mpx_frames": mpx_frames}
+    step_px = {"plain": 0, "served_all": 0, "served": 8 << 20}
+    for mode in ("plain", "served_all", "served"):
+        with Server(device=0, hbm_budget=120 << 30, serial=(mode == "plain"), step_pixels=step_px[mode]) as sv:
+            sids = [sv.add_scene(s) for s in scenes]
+            # untimed warm-up: one job of each (scene, pipeline) pair loads the kernels and the allocator
+            warm = []
+            for cfg in range(3):
+                for pipe in ("ris", "pt"):
+                    kw = configs.RIS_CONFIG2 if pipe == "ris" else configs.PT_CONFIG4
+                    warm.append(sv.submit(sids[cfg], configs.config_camera(cfg, 256, 256), 2, pipe, **kw))
+            while sv.load()[:2] != (0, 0):
+                sv.step()
+            for jid in warm:
+                sv.take(jid, keep_image=False)
+            lat, pending, nxt = [], {}, 0
+            steps = 0
+            t0 = time.perf_counter()
+            while len(lat) < n_jobs:
+                now = time.perf_counter() - t0
+                while nxt < n_jobs and jobs[nxt]["arrival"] <= now:
+                    j = jobs[nxt]
+                    kw = configs.RIS_CONFIG2 if j["pipeline"] == "ris" else configs.PT_CONFIG4
+                    jid = sv.submit(sids[j["cfg"]], cams[nxt], j["frames"], j["pipeline"], **kw)
+                    pending[jid] = j["arrival"]
+                    nxt += 1
+                if not pending:
+                    time.sleep(max(0.0, jobs[nxt]["arrival"] - now))
+                    continue
+                if sv.step() == 0:
+                    steps += 1
+                    continue
+                steps += 1
+                now = time.perf_counter() - t0
+                for jid in list(pending):
+                    st, _ = sv.state(jid)
+                    if st in (abi.JOB_DONE, abi.JOB_FAILED):
+                        if st == abi.JOB_FAILED:
+                            raise RuntimeError(f"serving job {jid} failed")
+                        lat.append(now - pending.pop(jid))
+                        sv.take(jid, keep_image=False)
+            makespan = time.perf_counter() - t0
+        lat.sort()
+        out[mode] = {"jobs_per_s": n_jobs / makespan, "mpx_frames_per_s": mpx_frames / makespan,
+                     "makespan_s": makespan, "latency_p50_ms": 1000.0 * statistics.median(lat),
+                     "latency_p99_ms": 1000.0 * lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))],
+                     "steps": steps}
+    out["modes"] = ("plain: one job at a time, each frame rendered alone; served_all: every admitted job "
+                    "advances each step; served: least remaining work first, 8 Mpx per step")
+    return out
+
+
 def run_ours(args, rank, local_rank, world):
     import numpy as np
     import torch
@@ -345,6 +460,9 @@ def run_ours(args, rank, local_rank, world):
                 "light geometry and no environment, where their result cannot change the image (bit-identical, "
                 "tested); 'trace_all_rays' casts them as the reference does",
     }
+    if world == 1 and not args.no_serving:
+        out["batched"] = batched_leg(ctx)
+        out["serving"] = serving_leg(args.serving_jobs)
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         if _ref_available():

@@ -258,3 +258,35 @@ def orbit_camera(angle: float, width: int, height: int) -> Camera:
 def small_variant(cfg: int, width: int, height: int, **kw):
     """The same scene at a test-sized resolution (and optionally fewer lights / spheres)."""
     return {0: config0, 1: config1, 2: config2}[cfg](width=width, height=height, **kw)
+
+
+def config_camera(cfg: int, width: int, height: int) -> Camera:
+    """The camera of config 0 / 1 / 2 at another resolution."""
+    if cfg == 0:
+        return make_camera((0.0, 0.0, 0.95), (0.0, -0.2, 0.0), width, height, fov=70.0)
+    if cfg == 1:
+        return make_camera((0.0, 6.0, 9.0), (0.0, 0.0, 0.0), width, height, fov=55.0)
+    return orbit_camera(0.0, width, height)
+
+
+CONFIG4_RESOLUTIONS = ((256, 256), (512, 512), (1280, 720), (1920, 1080), (2048, 1152))
+CONFIG4_SEED = 0xC0FFEE04
+
+
+def config4_jobs(n_jobs: int, rate: float = 200.0, seed: int = CONFIG4_SEED) -> list[dict]:
+    """Serving workload (config 4): Poisson arrivals at `rate` jobs/s; scene uniform
+    over configs 0-2; resolution uniform over CONFIG4_RESOLUTIONS; frames (spp)
+    uniform over 1..16; pipeline ReSTIR (config-2 settings: 32 candidates, reservoir,
+    maxDepth 1) or PathTracer (maxDepth 4) with equal odds."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n_jobs))
+    jobs = []
+    for k in range(n_jobs):
+        w, h = CONFIG4_RESOLUTIONS[int(rng.integers(len(CONFIG4_RESOLUTIONS)))]
+        jobs.append({"arrival": float(t[k]), "cfg": int(rng.integers(3)), "width": w, "height": h,
+                     "frames": int(rng.integers(1, 17)), "pipeline": "ris" if rng.random() < 0.5 else "pt"})
+    return jobs
+
+
+RIS_CONFIG2 = dict(candidate_count=32, use_reservoir=True, max_depth=1)
+PT_CONFIG4 = dict(max_depth=4)

@@ -64,6 +64,7 @@ struct hdr_server {
     size_t budget = 0;
     size_t in_use = 0;
     int max_batch = 64;
+    int64_t step_pixels = 0;
     std::vector<hdr_ctx *> scenes;  // one owner ctx per uploaded scene
     std::deque<std::unique_ptr<Job>> queued;
     std::vector<std::unique_ptr<Job>> active;
@@ -128,6 +129,7 @@ hdr_status hdr_server_create(hdr_server **out, const hdr_server_desc *desc) {
     sv->flags = desc->flags;
     sv->budget = desc->hbm_budget_bytes;
     sv->max_batch = desc->max_batch > 0 ? desc->max_batch : 64;
+    sv->step_pixels = desc->step_pixels > 0 ? desc->step_pixels : 0;
     *out = sv;
     return HDR_OK;
 }
@@ -187,15 +189,27 @@ hdr_status hdr_server_step(hdr_server *sv, int32_t *jobs_finished) {
     if (st != HDR_OK) return st;
     if (sv->active.empty()) return HDR_OK;
     const bool serial = (sv->flags & HDR_SERVER_SERIAL) != 0;
-    // 1. primary rays of every job, each on its own stream
-    for (auto &j : sv->active)
+    // this step's jobs: all admitted ones, or the least remaining work first up to step_pixels
+    std::vector<Job *> run;
+    for (auto &j : sv->active) run.push_back(j.get());
+    if (sv->step_pixels > 0) {
+        auto left = [](const Job *j) { return (int64_t)(j->d.frames - j->frames_done) * (int64_t)pixels_of(j->d); };
+        std::stable_sort(run.begin(), run.end(), [&](const Job *a, const Job *b) { return left(a) < left(b); });
+        int64_t px = 0;
+        size_t k = 0;
+        while (k < run.size() && (k == 0 || px + (int64_t)pixels_of(run[k]->d) <= sv->step_pixels))
+            px += (int64_t)pixels_of(run[k++]->d);
+        run.resize(k);
+    }
+    // 1. primary rays, each job on its own stream
+    for (Job *j : run)
         if (hdr_raycast(j->ctx, &j->d.camera, j->frames_done, 0) != HDR_OK) fail_job(sv, *j);
     // 2. integration: RIS jobs of one scene in batched launches, path tracing side by side
     std::map<int32_t, std::vector<Job *>> ris_by_scene;
-    for (auto &j : sv->active) {
+    for (Job *j : run) {
         if (j->state != HDR_JOB_RUNNING) continue;
         if (j->d.pipeline == HDR_JOB_RIS && !serial) {
-            ris_by_scene[j->d.scene].push_back(j.get());
+            ris_by_scene[j->d.scene].push_back(j);
         } else if (j->d.pipeline == HDR_JOB_RIS) {
             if (hdr_ris_path_trace(j->ctx, &j->d.camera, j->frames_done, &j->d.ris) != HDR_OK) fail_job(sv, *j);
         } else if (hdr_path_trace(j->ctx, &j->d.camera, j->frames_done, &j->d.ris.path) != HDR_OK) {
@@ -223,7 +237,7 @@ hdr_status hdr_server_step(hdr_server *sv, int32_t *jobs_finished) {
         }
     }
     // 3. accumulation, then the jobs that have all their frames leave the active set
-    for (auto &j : sv->active) {
+    for (Job *j : run) {
         if (j->state != HDR_JOB_RUNNING) continue;
         if (hdr_accumulate(j->ctx, j->frames_done, j->d.firefly, HDR_ACCUM_PARITY) != HDR_OK) {
             fail_job(sv, *j);

@@ -275,8 +275,9 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
  * Render-job server (no reference counterpart; the reference renders one job
  * per Hydra delegate). Scenes are uploaded once and shared; jobs are admitted
  * first-in first-out while the estimate of their frame buffers fits the HBM
- * budget; each hdr_server_step advances every admitted job by one frame, with
- * the RIS jobs of one scene traced in one batched launch and path-traced jobs
+ * budget; each hdr_server_step advances admitted jobs by one frame (all of
+ * them, or those with the least remaining work up to step_pixels), with the
+ * RIS jobs of one scene traced in one batched launch and path-traced jobs
  * side by side on their own streams. HDR_SERVER_SERIAL runs one job at a
  * time, each frame alone (the plain per-frame pipeline). A job's image is the
  * same in both modes. Calls on one server are serialised by its mutex.
@@ -289,6 +290,8 @@ typedef struct hdr_server_desc {
     uint32_t flags;            /* HDR_SERVER_* */
     size_t hbm_budget_bytes;   /* admission budget for the jobs' frame buffers, 0 = unlimited */
     int32_t max_batch;         /* images per batched RIS launch, 0 = 64 */
+    int64_t step_pixels;       /* pixels rendered per step, 0 = every admitted job; the jobs with the
+                                  least remaining work (frames left x pixels) go first */
 } hdr_server_desc;
 
 enum { HDR_JOB_PATH_TRACER = 0, HDR_JOB_RIS = 1 };

@@ -44,12 +44,12 @@ def _alone(scene, cam, frames, pipeline, settings):
         return ctx.download("Color").copy()
 
 
-@pytest.mark.parametrize("serial", [False, True])
-def test_server_images_equal_jobs_rendered_alone(serial):
+@pytest.mark.parametrize("serial,step_pixels", [(False, 0), (True, 0), (False, 6000)])
+def test_server_images_equal_jobs_rendered_alone(serial, step_pixels):
     s2, s0, c0 = _scenes()
     scenes = [s2, s0]
     jobs = _jobs(c0)
-    with Server(device=0, serial=serial) as sv:
+    with Server(device=0, serial=serial, step_pixels=step_pixels) as sv:
         ids = [sv.add_scene(s) for s in scenes]
         jid = [sv.submit(ids[si], cam, fr, pipe, **kw) for si, cam, fr, pipe, kw in jobs]
         done, steps = 0, 0
@@ -61,6 +61,8 @@ def test_server_images_equal_jobs_rendered_alone(serial):
         got = [sv.take(j) for j in jid]
     if serial:
         assert steps == sum(j[2] for j in jobs)  # one frame of one job per step
+    elif step_pixels:
+        assert steps > max(j[2] for j in jobs)  # fewer jobs per step
     else:
         assert steps == max(j[2] for j in jobs)  # every admitted job advances each step
     for (si, cam, fr, pipe, kw), g in zip(jobs, got):
