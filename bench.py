@@ -252,6 +252,48 @@ def batched_leg(ctx, n_images=4, frames=4, warm=2):
     return out
 
 
+def config3_leg(reps: int = 2):
+    """Config 3: one 3840x2160 frame and 64 frames of 512x512 (orbit views), PathTracer
+    maxDepth 16 on the config-2 scene plus a 2048x1024 dome: as 65 PathTracePass launches
+    (plain) and as one launch over all tiles (batched). Device-synchronised wall time of the
+    integration pass; the primary rays (raycast) run before it, untimed."""
+    import torch
+    from hdrestir_b200 import configs
+    from hdrestir_b200.context import Context, path_trace_batch
+    sc, cam, cams = configs.config3()
+    cams = [cam] + cams
+    paths = sum(c.width * c.height for c in cams)
+    ctxs = [Context(device=torch.cuda.current_device(), timings=False) for _ in cams]
+    out = {"workload": "config 3: 3840x2160 + 64 x 512x512, PathTracer maxDepth 16, dome 2048x1024",
+           "paths": paths}
+    try:
+        ctxs[0].upload_scene(sc)
+        for x in ctxs[1:]:
+            x.share_scene(ctxs[0])
+        best = {}
+        for rep in range(reps + 1):  # the first round warms up
+            for mode in ("plain", "batched"):
+                for x, c in zip(ctxs, cams):
+                    x.raycast(c, rep)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                if mode == "batched":
+                    path_trace_batch(ctxs, cams, [rep] * len(cams), **configs.PT_CONFIG3)
+                else:
+                    for x, c in zip(ctxs, cams):
+                        x.path_trace(c, rep, **configs.PT_CONFIG3)
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - t0
+                if rep > 0:
+                    best[mode] = min(best.get(mode, 1e30), dt)
+        for mode, dt in best.items():
+            out[mode] = {"ms": 1000.0 * dt, "paths_per_s": paths / dt}
+    finally:
+        for x in ctxs:
+            x.close()
+    return out
+
+
 def serving_leg(n_jobs: int):
     """Config-4 serving: the same Poisson job stream (200 jobs/s) through the
     server in serial mode (the plain per-frame pipeline, one job at a time) and
@@ -463,6 +505,7 @@ def run_ours(args, rank, local_rank, world):
     if world == 1 and not args.no_serving:
         out["batched"] = batched_leg(ctx)
         out["serving"] = serving_leg(args.serving_jobs)
+        out["config3"] = config3_leg()
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         if _ref_available():

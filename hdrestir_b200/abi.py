@@ -139,6 +139,8 @@ def lib() -> C.CDLL:
             "hdr_ctx_destroy": (None, [vp]),
             "hdr_scene_upload": (C.c_int, [vp, C.POINTER(SceneDesc)]),
             "hdr_scene_share": (C.c_int, [vp, vp]),
+            "hdr_path_trace_batch": (C.c_int, [C.POINTER(vp), i32, C.POINTER(CameraDesc), C.POINTER(i32),
+                                               C.POINTER(PathSettings)]),
             "hdr_ris_path_trace_batch": (C.c_int, [C.POINTER(vp), i32, C.POINTER(CameraDesc), C.POINTER(i32),
                                                    C.POINTER(RisParams)]),
             "hdr_raycast": (C.c_int, [vp, C.POINTER(CameraDesc), i32, C.c_uint32]),

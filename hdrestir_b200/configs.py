@@ -290,3 +290,38 @@ def config4_jobs(n_jobs: int, rate: float = 200.0, seed: int = CONFIG4_SEED) -> 
 
 RIS_CONFIG2 = dict(candidate_count=32, use_reservoir=True, max_depth=1)
 PT_CONFIG4 = dict(max_depth=4)
+
+
+def dome_texture(width: int = 2048, height: int = 1024, sun_uv=(0.3, 0.28), sun_radius=0.012,
+                 sun_radiance=400.0) -> np.ndarray:
+    """Procedural environment map (H, W, 3) f32, rows from the top of the lat-long
+    image: a sky gradient (bluish at the top, warm at the horizon row, dim ground
+    below it) and a Gaussian sun lobe."""
+    v = (np.arange(height, dtype=np.float64) + 0.5) / height
+    u = (np.arange(width, dtype=np.float64) + 0.5) / width
+    vv, uu = np.meshgrid(v, u, indexing="ij")
+    up = np.clip(1.0 - 2.0 * vv, -1.0, 1.0)  # +1 at the top row, -1 at the bottom
+    zen = np.array([0.25, 0.45, 0.95])
+    hor = np.array([0.95, 0.85, 0.70])
+    gnd = np.array([0.12, 0.10, 0.08])
+    t = np.clip(up, 0.0, 1.0)[..., None] ** 0.6
+    sky = hor * (1.0 - t) + zen * t
+    img = np.where((up >= 0.0)[..., None], sky, gnd * (1.0 + up[..., None]))
+    du = np.minimum(np.abs(uu - sun_uv[0]), 1.0 - np.abs(uu - sun_uv[0]))
+    d2 = (du * 2.0) ** 2 + (vv - sun_uv[1]) ** 2
+    img = img + (sun_radiance * np.exp(-d2 / (2.0 * sun_radius ** 2)))[..., None] * np.array([1.0, 0.95, 0.85])
+    return np.ascontiguousarray(img, np.float32)
+
+
+def config3(width=3840, height=2160, n_small=64, small=512, grid=512, n_spheres=2000, n_lights=10000,
+            dome_size=(2048, 1024)):
+    """Config 3: the config-2 scene lit also by a procedural 2048x1024 dome; one
+    width x height camera and n_small orbit cameras of small x small pixels."""
+    sc, cam = config2(width, height, grid=grid, n_spheres=n_spheres, n_lights=n_lights)
+    sc.lights.append(Light(abi.LIGHT_DOME, color=(1.0, 1.0, 1.0), intensity=1.0,
+                           texture=dome_texture(*dome_size)))
+    cams = [orbit_camera(2.0 * np.pi * k / max(1, n_small), small, small) for k in range(n_small)]
+    return sc, cam, cams
+
+
+PT_CONFIG3 = dict(max_depth=16)

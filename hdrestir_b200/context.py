@@ -42,6 +42,17 @@ def ris_path_trace_batch(contexts, cameras, frame_indices, **ris) -> None:
     abi.check(lib.hdr_ris_path_trace_batch(ctxs, n, cams, frames, params))
 
 
+def path_trace_batch(contexts, cameras, frame_indices, **settings) -> None:
+    """One PathTracePass launch for several images (Contexts sharing one scene)."""
+    n = len(contexts)
+    ctxs = (C.c_void_p * n)(*[c._h for c in contexts])
+    cams = (abi.CameraDesc * n)(*[cam.c_desc() for cam in cameras])
+    frames = (C.c_int32 * n)(*[int(f) for f in frame_indices])
+    p = path_settings(**settings)
+    params = (abi.PathSettings * n)(*([p] * n))
+    abi.check(abi.lib().hdr_path_trace_batch(ctxs, n, cams, frames, params))
+
+
 def path_settings(max_depth=32, enable_subsurface=True, max_reflection_bounces=8, max_refraction_bounces=8,
                   render_ibl_background=True, roulette_aggressiveness=1.0) -> abi.PathSettings:
     """PathTracePassSettings (integrators/path_integrator.h:12-19) + maxDepth, with the reference defaults."""

@@ -58,6 +58,16 @@ struct RisParamsD {
     float spatial_radius;
 };
 
+// PathTracePassSettings + maxDepth as the integrators read them
+// (integrators/path_integrator.h:12-19)
+struct PathRun {
+    int max_depth;
+    bool enable_subsurface;
+    int max_refl, max_refr;
+    bool render_ibl_background;
+    float roulette;
+};
+
 struct PathParamsD {
     int max_depth;
     int enable_subsurface;
@@ -132,6 +142,19 @@ void launch_trace_stats(const DeviceScene &s, const float *rays, const float *tm
 void launch_rng_floats(const uint32_t *seeds, int n, int count, float *out, cudaStream_t st);
 void launch_ris_path_trace(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                            GBufferView gb, ReservoirView res, float4 *color, unsigned *err, cudaStream_t st);
+// One image of a batched PathTracePass launch (a table in device memory).
+struct PtJobD {
+    CameraD cam;
+    GBufferView gb;
+    float4 *color;
+    unsigned *err;
+    PathRun pr;
+    int frame_index;
+    int tile_begin;  // first tile of this image in the batch grid
+};
+PathRun path_run_of(const PathParamsD &p);
+void launch_path_trace_batch(const DeviceScene &s, const PtJobD *jobs, int n_jobs, int total_tiles,
+                             cudaStream_t st);
 void launch_path_trace(const DeviceScene &s, const CameraD &cam, int frame_index, const PathParamsD &p,
                        GBufferView gb, float4 *color, unsigned *err, cudaStream_t st);
 // Returns the number of kernels launched.
@@ -141,10 +164,10 @@ int launch_accumulate(float4 *color, float4 *accum, float4 *scratch, int *flag_d
 // Pixel of thread t in a 16x16 tile: each warp covers an 8x4 sub-tile so the
 // rays it traces start close together.
 template <int kThreads = 256>
-__device__ __forceinline__ bool tile_pixel(int width, int height, int &x, int &y) {
+__device__ __forceinline__ bool tile_pixel(int width, int height, int &x, int &y, int tile = -1) {
     constexpr int kTileH = kThreads / 16;  // tiles 16 pixels wide, one 8x4 patch per warp
     const int tiles_x = (width + 15) >> 4;
-    const int tile = blockIdx.x;
+    if (tile < 0) tile = blockIdx.x;
     const int tx = tile % tiles_x, ty = tile / tiles_x;
     const int t = threadIdx.x;
     const int w = t >> 5, lane = t & 31;

@@ -705,14 +705,6 @@ __device__ inline Spec ris_direct_li(const DeviceScene &s, const RP &rp, const S
 // ============================================================================
 // PathIntegrator (integrators/path_integrator.cpp:48-209)
 // ============================================================================
-struct PathRun {
-    int max_depth;
-    bool enable_subsurface;
-    int max_refl, max_refr;
-    bool render_ibl_background;
-    float roulette;
-};
-
 template <bool kRis, class RP>
 __device__ __forceinline__ Spec direct_li(const DeviceScene &s, const RP &rp, const Surface &sf, bool has_conn,
                                           const Connection &cn, const SpectralCtx &sc, MtStream &rng, bool primary,

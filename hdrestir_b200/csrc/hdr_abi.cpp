@@ -794,6 +794,86 @@ hdr_status hdr_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index
     return end_pass(c, 1);
 }
 
+hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camera *cams,
+                                const int32_t *frame_indices, const hdr_path_settings *settings) {
+    if (!ctxs || !cams || !frame_indices || !settings || n < 1 || n > 4096) return fail(HDR_EINVAL, "bad argument");
+    for (int32_t i = 0; i < n; ++i)
+        if (!ctxs[i]) return fail(HDR_EINVAL, "ctx %d is NULL", i);
+    bool together = n > 1;
+    for (int32_t i = 0; i < n && together; ++i)
+        together = ctxs[i]->device == ctxs[0]->device && ctxs[i]->has_scene && ctxs[i]->scene_store &&
+                   ctxs[i]->scene_store == ctxs[0]->scene_store && ctxs[i]->scene.wide == ctxs[0]->scene.wide;
+    std::vector<hdr_ctx *> order(ctxs, ctxs + n);
+    std::sort(order.begin(), order.end());
+    if (std::adjacent_find(order.begin(), order.end()) != order.end())
+        return fail(HDR_EINVAL, "a context appears twice in the batch");
+    if (!together) {
+        for (int32_t i = 0; i < n; ++i) {
+            const hdr_status st = hdr_path_trace(ctxs[i], &cams[i], frame_indices[i], &settings[i]);
+            if (st != HDR_OK) return st;
+        }
+        return HDR_OK;
+    }
+    for (hdr_ctx *c : order) c->mu.lock();
+    struct Unlock {
+        std::vector<hdr_ctx *> &v;
+        ~Unlock() {
+            for (hdr_ctx *c : v) c->mu.unlock();
+        }
+    } unlock{order};
+    hdr_ctx *lead = ctxs[0];
+    HDR_CUDA(cudaSetDevice(lead->device));
+    std::vector<hdr::PtJobD> jobs((size_t)n);
+    long long tiles = 0;
+    hdr_status st;
+    for (int32_t i = 0; i < n; ++i) {
+        hdr_ctx *c = ctxs[i];
+        const hdr_camera *cam = &cams[i];
+        const hdr_path_settings *p = &settings[i];
+        if ((st = check_camera(cam)) != HDR_OK) return st;
+        if (p->max_depth < 1) return fail(HDR_EINVAL, "max_depth must be >= 1");
+        if ((st = check_cancel(c)) != HDR_OK) return st;
+        const size_t count = (size_t)cam->width * cam->height;
+        hdr::PtJobD &j = jobs[(size_t)i];
+        if ((st = gbuffer_view(c, count, false, j.gb)) != HDR_OK) return st;
+        void *color = nullptr;
+        if ((st = ensure_buffer(c, "Color", count * 16, &color)) != HDR_OK) return st;
+        hdr::PathParamsD d{};
+        d.max_depth = p->max_depth;
+        d.enable_subsurface = p->enable_subsurface;
+        d.max_refl = p->max_reflection_bounces;
+        d.max_refr = p->max_refraction_bounces;
+        d.render_ibl_background = p->render_ibl_background;
+        d.roulette = p->roulette_aggressiveness;
+        j.cam = make_camera(cam);
+        j.color = (float4 *)color;
+        j.err = c->d_err;
+        j.pr = hdr::path_run_of(d);
+        j.frame_index = frame_indices[i];
+        j.tile_begin = (int)tiles;
+        tiles += (long long)hdr::tile_blocks(cam->width, cam->height);
+    }
+    if (tiles >= (1ll << 31)) return fail(HDR_EINVAL, "batch of %lld tiles is too large", tiles);
+    void *table = nullptr;
+    if ((st = ensure_scratch(lead, "__batch_pt_jobs", jobs.size() * sizeof(hdr::PtJobD), &table)) != HDR_OK)
+        return st;
+    for (int32_t i = 1; i < n; ++i) {
+        HDR_CUDA(cudaEventRecord(ctxs[i]->sync_ev, ctxs[i]->stream));
+        HDR_CUDA(cudaStreamWaitEvent(lead->stream, ctxs[i]->sync_ev, 0));
+    }
+    if ((st = begin_pass(lead, 1)) != HDR_OK) return st;
+    // the table is read by the launch below; the host vector stays alive until the copy is done
+    HDR_CUDA(cudaMemcpyAsync(table, jobs.data(), jobs.size() * sizeof(hdr::PtJobD), cudaMemcpyHostToDevice,
+                             lead->stream));
+    hdr::launch_path_trace_batch(lead->scene, (const hdr::PtJobD *)table, n, (int)tiles, lead->stream);
+    HDR_CUDA(cudaGetLastError());
+    HDR_CUDA(cudaEventRecord(lead->sync_ev, lead->stream));
+    for (int32_t i = 1; i < n; ++i) HDR_CUDA(cudaStreamWaitEvent(ctxs[i]->stream, lead->sync_ev, 0));
+    HDR_CUDA(cudaStreamSynchronize(lead->stream));  // the pageable table copy must finish before `jobs` goes
+    lead->launches += 1;
+    return end_pass(lead, 1);
+}
+
 hdr_status hdr_accumulate(hdr_ctx *c, int32_t frame_index, int32_t firefly, int32_t mode) {
     if (!c) return fail(HDR_EINVAL, "ctx is NULL");
     std::lock_guard<std::mutex> lock(c->mu);

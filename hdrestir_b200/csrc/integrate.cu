@@ -11,11 +11,9 @@
 namespace hdr {
 
 template <bool kRis>
-__global__ void __launch_bounds__(256) integrate_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
-                                                        RisRun ris, GBufferView gb, ReservoirView rv, float4 *color,
-                                                        unsigned *err) {
-    int x, y;
-    if (!tile_pixel(cam.width, cam.height, x, y)) return;
+__device__ __forceinline__ void integrate_pixel(const DeviceScene &s, const CameraD &cam, int frame_index,
+                                                const PathRun &pr, const RisRun &ris, const GBufferView &gb,
+                                                const ReservoirView &rv, float4 *color, int x, int y, unsigned &e) {
     const size_t i = (size_t)y * (size_t)cam.width + (size_t)x;
     uint64_t spill[312];
     MtStream rng;
@@ -24,7 +22,6 @@ __global__ void __launch_bounds__(256) integrate_kernel(DeviceScene s, CameraD c
     const float py = (float)y + rng.next_float();
     const RayF ray = camera_ray(cam, px, py, rng);
     const SpectralCtx sc = make_spectral_ctx(rng.next_float());
-    unsigned e = 0;
     Hit h;
     const bool has = load_gbuffer_hit(s, gb, i, h);
     const TraceNow now{&s};
@@ -32,7 +29,39 @@ __global__ void __launch_bounds__(256) integrate_kernel(DeviceScene s, CameraD c
     V3 rgb = spectrum_to_rgb(L, sc.cie);
     if (cam.p.has_params && cam.p.enable_exposure) rgb = rgb * cam.p.exposure_mult;
     color[i] = make_float4(rgb.x, rgb.y, rgb.z, 1.0f);
+}
+
+template <bool kRis>
+__global__ void __launch_bounds__(256) integrate_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
+                                                        RisRun ris, GBufferView gb, ReservoirView rv, float4 *color,
+                                                        unsigned *err) {
+    int x, y;
+    if (!tile_pixel(cam.width, cam.height, x, y)) return;
+    unsigned e = 0;
+    integrate_pixel<kRis>(s, cam, frame_index, pr, ris, gb, rv, color, x, y, e);
     if (e) atomicOr(err, e);
+}
+
+// Batched PathTracePass: the 16x16 tiles of every image of the batch in one
+// grid; a block finds its image by binary search over the images' first tiles.
+__global__ void __launch_bounds__(256) path_trace_batch_kernel(DeviceScene s, const PtJobD *__restrict__ jobs,
+                                                               int n_jobs) {
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {  // last job whose tile_begin <= blockIdx.x
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&jobs[mid].tile_begin) <= (int)blockIdx.x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const PtJobD &j = jobs[lo];
+    int x, y;
+    if (!tile_pixel(j.cam.width, j.cam.height, x, y, (int)blockIdx.x - j.tile_begin)) return;
+    unsigned e = 0;
+    const RisRun ris{};
+    const ReservoirView rv{};
+    integrate_pixel<false>(s, j.cam, j.frame_index, j.pr, ris, j.gb, rv, j.color, x, y, e);
+    if (e) atomicOr(j.err, e);
 }
 
 static PathRun make_path_run(int max_depth, int subsurface, int max_refl, int max_refr, int ibl, float roulette) {
@@ -57,6 +86,16 @@ void launch_ris_path_trace(const DeviceScene &s, const CameraD &cam, int frame_i
     ris.m_cap = p.m_cap;
     integrate_kernel<true><<<tile_blocks(cam.width, cam.height), 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, res,
                                                                              color, err);
+}
+
+PathRun path_run_of(const PathParamsD &p) {
+    return make_path_run(p.max_depth, p.enable_subsurface, p.max_refl, p.max_refr, p.render_ibl_background,
+                         p.roulette);
+}
+
+void launch_path_trace_batch(const DeviceScene &s, const PtJobD *jobs, int n_jobs, int total_tiles,
+                             cudaStream_t st) {
+    path_trace_batch_kernel<<<total_tiles, 256, 0, st>>>(s, jobs, n_jobs);
 }
 
 void launch_path_trace(const DeviceScene &s, const CameraD &cam, int frame_index, const PathParamsD &p,

@@ -271,6 +271,13 @@ hdr_status hdr_ris_path_trace(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame
 hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camera *cams,
                                     const int32_t *frame_indices, const hdr_ris_params *params);
 
+/* Batched PathTracePass, no reference counterpart: n images (one ctx each,
+ * sharing one resident scene, each after its own hdr_raycast) in one launch
+ * over all their tiles. Each image's "Color" is that of hdr_path_trace on its
+ * ctx. Images that do not share the scene are rendered one after another. */
+hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camera *cams,
+                                const int32_t *frame_indices, const hdr_path_settings *settings);
+
 /* ---------------------------------------------------------------------------
  * Render-job server (no reference counterpart; the reference renders one job
  * per Hydra delegate). Scenes are uploaded once and shared; jobs are admitted

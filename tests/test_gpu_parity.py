@@ -246,3 +246,69 @@ def test_autotune_trace_keeps_results():
         assert best["trace_ms"] > 0.0 and ctx.trace_tuning()["node_quorum"] == best["node_quorum"]
         ctx.ris_path_trace(cam, 0, **ris)
         assert np.array_equal(ctx.download("Color").view(np.uint32), before.view(np.uint32))
+
+
+def _dome_scene(w=64, h=48):
+    sc, cam, cams = configs.config3(w, h, n_small=3, small=32, grid=96, n_spheres=60, n_lights=300,
+                                    dome_size=(128, 64))
+    return sc, cam, cams
+
+
+@pytest.mark.parametrize("ris", [True, False])
+def test_dome_lit_scene_matches_oracle(ris):
+    """Config-3 family (terrain, spheres, rect lights and a lat-long dome): ReSTIR
+    (BSDF candidates traced, the environment is a light) and PathTracer."""
+    from hdrestir_b200.context import Context
+    sc, cam, _ = _dome_scene()
+    orc = Oracle(sc)
+    kw = dict(candidate_count=16, use_reservoir=True, max_depth=1) if ris else dict(max_depth=6)
+    with Context(device=0) as ctx:
+        ctx.upload_scene(sc)
+        for frame in range(2):
+            ctx.raycast(cam, frame)
+            if ris:
+                ctx.ris_path_trace(cam, frame, **kw)
+            else:
+                ctx.path_trace(cam, frame, **kw)
+            gpu = ctx.download("Color")
+            orc.raycast(cam, frame)
+            ref, _ = orc.integrate(cam, frame, ris=ris, **kw)
+            if ris:
+                m_gpu = ctx.download("__ris_reservoir")[4, :, 2].view(np.int32)
+                assert np.array_equal(m_gpu, orc.res["m"])
+            frac = _color_outliers(gpu, ref)
+            print(f"dome {'ReSTIR' if ris else 'PT'} frame {frame}: outlier fraction {frac:.4f}")
+            assert frac <= MAX_OUTLIERS
+
+
+def test_path_trace_batch_equals_images_alone():
+    """One PathTracePass launch over several images gives each image its own result."""
+    from hdrestir_b200.context import Context, path_trace_batch
+    sc, cam, cams = _dome_scene()
+    cams = [cam] + cams
+    want = []
+    for c in cams:
+        with Context(device=0) as ctx:
+            ctx.upload_scene(sc)
+            for f in range(2):
+                ctx.raycast(c, f)
+                ctx.path_trace(c, f, max_depth=8)
+                ctx.accumulate(f)
+            want.append(ctx.download("Color").copy())
+    ctxs = [Context(device=0) for _ in cams]
+    try:
+        ctxs[0].upload_scene(sc)
+        for x in ctxs[1:]:
+            x.share_scene(ctxs[0])
+        for f in range(2):
+            for x, c in zip(ctxs, cams):
+                x.raycast(c, f)
+            path_trace_batch(ctxs, cams, [f] * len(cams), max_depth=8)
+            for x in ctxs:
+                x.accumulate(f)
+        got = [x.download("Color").copy() for x in ctxs]
+    finally:
+        for x in ctxs:
+            x.close()
+    for g, w in zip(got, want):
+        assert np.array_equal(g.view(np.uint32), w.view(np.uint32))

@@ -81,3 +81,20 @@ def test_reference_harness_survives_frame_size_changes():
                              resolution_level=level, outputs=("color",))
         assert np.isfinite(c).all()
     ref.close()
+
+
+@pytest.mark.parametrize("kw", [dict(ris=True, candidate_count=8, use_reservoir=True, max_depth=1),
+                                dict(ris=False, max_depth=4)])
+def test_oracle_equals_reference_with_dome(kw):
+    """Config-3 family: rect lights plus a lat-long dome (DomeLight::Prepare CDF,
+    Sample, EvalPdf, background)."""
+    sc, cam, _ = configs.config3(40, 30, n_small=0, grid=48, n_spheres=20, n_lights=60, dome_size=(64, 32))
+    ref = refharness.Reference(sc)
+    o = orc.Oracle(sc, threads=4)
+    for f in range(2):
+        g, c, r = ref.render(cam, f, accumulate=True, firefly=True, **kw)
+        o.raycast(cam, f)
+        o.integrate(cam, f, **kw)
+        o.accumulate(cam, f, firefly=True)
+        assert np.array_equal(bits(o.color), bits(c))
+        assert np.array_equal(o.res["m"], r["m"])
