@@ -51,6 +51,10 @@ __device__ __forceinline__ bool occluded(const DeviceScene &s, V3 o, V3 d, float
     return shadow_ray(s, o, d, limit, err);
 }
 
+// The same query behind a call: kernels that cast a shadow ray only on a rare
+// path keep the traversal's registers out of their hot loop.
+__device__ __noinline__ bool occluded_call(const DeviceScene &s, V3 o, V3 d, float limit, unsigned &err);
+
 // Where the integrators get ray results from. Every ray a pixel casts has a
 // slot: closest-hit slot 0 is the path's bounce ray, closest-hit slot 1 + k
 // the k-th generated BSDF candidate, shadow slot j the j-th NEE candidate.
@@ -86,7 +90,7 @@ struct TracedResults {
     }
     // the winner's visibility test of a skipVisibility selection is cast on the spot
     __device__ __forceinline__ bool winner_shadow(V3 o, V3 d, float limit, unsigned &err) const {
-        return occluded(*s, o, d, limit, err);
+        return occluded_call(*s, o, d, limit, err);
     }
 };
 
@@ -715,8 +719,9 @@ __device__ __forceinline__ Spec direct_li(const DeviceScene &s, const RP &rp, co
 }
 
 // _li (:92-209). Later bounces query the scene directly (they only run in the
-// one-thread-per-pixel form).
-template <bool kRis, class RP>
+// one-thread-per-pixel form). kDirectOnly: the caller guarantees maxDepth 1
+// (the wavefront form), so the later-bounce loop is not compiled.
+template <bool kRis, class RP, bool kDirectOnly = false>
 __device__ Spec path_li_shaded(const DeviceScene &s, const RP &rp, const Surface &sf0, const SpectralCtx &sc,
                                MtStream &rng, const PathRun &pr, const RisRun &ris, const ReservoirView &rv,
                                size_t pixel, const MtStream *gen_end_state, unsigned &err) {
@@ -726,6 +731,7 @@ __device__ Spec path_li_shaded(const DeviceScene &s, const RP &rp, const Surface
     const Connection first = sample_bounce_with_connection(rp, 0, sf0, pr.max_refl, pr.max_refr, st, sc, rng, err);
     total = total + direct_li<kRis>(s, rp, sf0, first.b.ok, first, sc, rng, true, ris, rv, pixel, gen_end_state, err);
     if (!first.b.ok) return total;
+    if (kDirectOnly) return total;  // maxDepth 1: the loop below would not run
     tp = tp * first.b.tmul;
     V3 ro = first.b.origin, rd = first.b.dir;
     bool has_next = first.has_hit;
@@ -764,7 +770,9 @@ __device__ Spec path_li_shaded(const DeviceScene &s, const RP &rp, const Surface
 }
 
 // PathIntegrator::Li (:48-90): opacity skip at the GBuffer hit, Beer, then _li.
-template <bool kRis, class RP>
+// kDirectOnly also means an opaque scene (opacity >= 0.999 everywhere, checked
+// at upload), where the skip never triggers and never draws.
+template <bool kRis, class RP, bool kDirectOnly = false>
 __device__ Spec path_li(const DeviceScene &s, const RP &rp, V3 ray_o, V3 ray_d, bool has_hit, Hit hit,
                         const SpectralCtx &sc, MtStream &rng, const PathRun &pr, const RisRun &ris,
                         const ReservoirView &rv, size_t pixel, const MtStream *gen_end_state, unsigned &err) {
@@ -772,11 +780,12 @@ __device__ Spec path_li(const DeviceScene &s, const RP &rp, V3 ray_o, V3 ray_d, 
     while (has_hit) {
         Closure c = get_closure(s, hit);
         if (!pr.enable_subsurface) c.subsurface = 0.0f;
-        if (c.opacity >= 0.999f || rng.next_float() <= c.opacity) {
+        if (kDirectOnly || c.opacity >= 0.999f || rng.next_float() <= c.opacity) {
             const bool inside = dot(c.normal, ray_d) > 0.0f;
             beer_absorption(tp, c, hit.depth, inside, sc);
             const Surface sf = make_surface(s, ray_o, ray_d, hit, c, inside);
-            return tp * path_li_shaded<kRis>(s, rp, sf, sc, rng, pr, ris, rv, pixel, gen_end_state, err);
+            return tp * path_li_shaded<kRis, RP, kDirectOnly>(s, rp, sf, sc, rng, pr, ris, rv, pixel, gen_end_state,
+                                                              err);
         }
         has_hit = intersect(s, hit.position + ray_d * 1e-4f, ray_d, hit, err);
     }

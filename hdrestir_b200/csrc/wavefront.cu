@@ -149,6 +149,10 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
     store_stream(wb.rng_state, i, wb.pixels, rng);
 }
 
+__device__ __noinline__ bool occluded_call(const DeviceScene &s, V3 o, V3 d, float limit, unsigned &err) {
+    return occluded(s, o, d, limit, err);
+}
+
 // Trace kernels. Rays of a warp take very different numbers of steps (shadow
 // rays towards random lights: 43 % of lane-steps did work when each lane
 // traced a fixed ray), so the default form is persistent: a lane whose ray is
@@ -349,7 +353,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) ris_shade_kernel(DeviceS
     const MtStream gen_end = load_stream(wb.rng_state, i, wb.pixels);
     // past 311 draws the state lives in local memory only: replay instead
     const MtStream *gen_end_ptr = gen_end.k < 312 ? &gen_end : nullptr;
-    const Spec L = path_li<true>(s, tr, ps.ray.o, ps.ray.d, true, ps.hit, ps.sc, rng, pr, ris, rv, i, gen_end_ptr, e);
+    // the wavefront form runs only for maxDepth 1 and opaque scenes
+    const Spec L =
+        path_li<true, TracedResults, true>(s, tr, ps.ray.o, ps.ray.d, true, ps.hit, ps.sc, rng, pr, ris, rv, i, gen_end_ptr, e);
     V3 rgb = spectrum_to_rgb(L, ps.sc.cie);
     if (cam.p.has_params && cam.p.enable_exposure) rgb = rgb * cam.p.exposure_mult;
     color[i] = make_float4(rgb.x, rgb.y, rgb.z, 1.0f);
