@@ -142,6 +142,24 @@ void launch_trace_stats(const DeviceScene &s, const float *rays, const float *tm
 void launch_rng_floats(const uint32_t *seeds, int n, int count, float *out, cudaStream_t st);
 void launch_ris_path_trace(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                            GBufferView gb, ReservoirView res, float4 *color, unsigned *err, cudaStream_t st);
+// Per-path state of the wavefront PathTracePass (pathtrace.cu), one entry
+// per pixel, plus its ray queues and hit slots (slot = pixel index).
+struct PtBuffers {
+    uint4 *rng;             // 3 planes: stream state between kernels
+    float4 *tp, *total;     // throughput and running radiance of _li (4 wavelengths)
+    float4 *outer;          // PathIntegrator::Li's throughput (primary Beer), applied at the end
+    float4 *ray_o, *ray_d;  // the current vertex's incoming ray; ray_o.w: the wavelength draw
+    float4 *b_origin_pdf, *b_dir, *b_tmul;  // the vertex's BSDF sample
+    float4 *nee_add;        // the vertex's NEE term, added if its shadow ray is unoccluded
+    int4 *state;            // BounceState refl, refr; flags; spare
+    int *active[2];         // live-path lists (ping-pong)
+    int *counts;            // [0..3] queue lengths and fetch counters, [4..5] active-list lengths
+    float4 *q_closest, *q_shadow, *hits;
+    float *hit_v;
+    unsigned char *occ;
+    size_t pixels;
+};
+
 // One image of a batched PathTracePass launch (a table in device memory).
 struct PtJobD {
     CameraD cam;
@@ -150,9 +168,16 @@ struct PtJobD {
     unsigned *err;
     PathRun pr;
     int frame_index;
-    int tile_begin;  // first tile of this image in the batch grid
+    int tile_begin;    // first tile of this image in the batch grid
+    int pixel_begin;   // first path of this image in the wavefront planes
 };
 PathRun path_run_of(const PathParamsD &p);
+// Wavefront PathTracePass over n images (jobs[k].tile_begin / pixel_begin
+// laid out by the caller; all with the same PathRun). One image: the job goes
+// by value and `table` may be null; several: `table` is a device copy of jobs.
+int launch_path_trace_wavefront(const DeviceScene &s, const PtJobD *jobs, int n_jobs, const PtJobD *table,
+                                int total_tiles, PtBuffers B, const TraceTuning &tune, unsigned *err,
+                                cudaStream_t st);
 void launch_path_trace_batch(const DeviceScene &s, const PtJobD *jobs, int n_jobs, int total_tiles,
                              cudaStream_t st);
 void launch_path_trace(const DeviceScene &s, const CameraD &cam, int frame_index, const PathParamsD &p,

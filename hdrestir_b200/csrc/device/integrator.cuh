@@ -142,16 +142,26 @@ __device__ __forceinline__ Connection sample_bounce_with_connection(const RP &rp
 // ============================================================================
 // MisDirectLightIntegrator (PathTracePass)
 // ============================================================================
-struct MisNee {
-    Spec radiance;
-    float p_nee, p_bsdf;
-    bool delta;
+// _evaluateNEE (mis_direct_light_integrator.cpp:70-120) up to its shadow ray:
+// the light sample's draws and what it adds to the vertex if the ray from
+// (o, d) reaches `limit` unoccluded (`add` = radiance x MIS weight of
+// _integrateNEE, :122-178). cast = false: no shadow ray, nothing added.
+struct MisNeePart {
+    bool cast;
+    V3 o, d;
+    float limit;
+    Spec add;
 };
 
-// _evaluateNEE (mis_direct_light_integrator.cpp:70-120)
-__device__ inline MisNee mis_evaluate_nee(const DeviceScene &s, const Surface &sf, int li, const LightSampleD &ls,
-                                   const SpectralCtx &sc, unsigned &err) {
-    MisNee r{spec(0.0f), 0.0f, 0.0f, false};
+__device__ inline MisNeePart mis_nee_part(const DeviceScene &s, const Surface &sf, bool has_conn,
+                                          const SpectralCtx &sc, MtStream &rng) {
+    MisNeePart r;
+    r.cast = false;
+    r.add = spec(0.0f);
+    // the environment, when present, is a scene light and so part of the sampler
+    int li;
+    LightSampleD ls;
+    if (!propose_candidate(s, sf.hit.position, rng, li, ls)) return r;
     const float n_l = dot(sf.sn, ls.dir);
     if (n_l <= 0.0f) return r;
     const bool delta = light_is_delta(s, li);
@@ -160,32 +170,22 @@ __device__ inline MisNee mis_evaluate_nee(const DeviceScene &s, const Surface &s
     if (cos_y <= 0.0f && !delta) return r;
     const float p_nee = pdf_to_solid_angle(ls.pdf, ls.pdf_solid_angle, dist2, smaxf(cos_y, 1e-6f));
     if (p_nee <= 0.0f) return r;
-    if (occluded(s, sf.hit.position + sf.sn * 1e-4f, ls.dir, ls.dist - 1e-3f, err)) return r;
     const V3 wo = -sf.ray_d;
     const float bpdf = ggx_pdf(sf.c, sf.sn, wo, ls.dir);
     const V3 bval = ggx_eval(sf.c, sf.sn, wo, ls.dir);
-    r.radiance = rgb_to_spectrum(bval, sc.up) * rgb_to_spectrum(ls.color, sc.up) * (n_l / p_nee);
-    r.p_nee = p_nee;
-    r.p_bsdf = bpdf;
-    r.delta = delta;
+    const Spec radiance = rgb_to_spectrum(bval, sc.up) * rgb_to_spectrum(ls.color, sc.up) * (n_l / p_nee);
+    const float w = (delta || !has_conn) ? 1.0f : power_heuristic2(p_nee, bpdf);
+    r.cast = true;
+    r.o = sf.hit.position + sf.sn * 1e-4f;
+    r.d = ls.dir;
+    r.limit = ls.dist - 1e-3f;
+    r.add = radiance * w;
     return r;
 }
 
-// MisDirectLightIntegrator::Li (per-bounce form, :250-269) = _integrateNEE + _integrateBSDFConnection
-__device__ inline Spec mis_direct_li(const DeviceScene &s, const Surface &sf, bool has_conn, const Connection &cn,
-                              const SpectralCtx &sc, MtStream &rng, unsigned &err) {
-    Spec total = spec(0.0f);
-    // _integrateNEE (:122-178); the environment, when present, is a scene light
-    // and so part of the sampler (no separate sky technique)
-    int li;
-    LightSampleD ls;
-    if (propose_candidate(s, sf.hit.position, rng, li, ls)) {
-        const MisNee nee = mis_evaluate_nee(s, sf, li, ls, sc, err);
-        if (nee.p_nee > 0.0f) {
-            const float w = (nee.delta || !has_conn) ? 1.0f : power_heuristic2(nee.p_nee, nee.p_bsdf);
-            total = total + nee.radiance * w;
-        }
-    }
+// _integrateBSDFConnection (:180-248) added to what the NEE part gave (`total`).
+__device__ inline Spec mis_conn_part(const DeviceScene &s, Spec total, bool has_conn, const Connection &cn,
+                                     const SpectralCtx &sc) {
     if (!has_conn) return total;
     // _integrateBSDFConnection (:180-248)
     const Bounce &b = cn.b;
@@ -224,6 +224,16 @@ __device__ inline Spec mis_direct_li(const DeviceScene &s, const Surface &sf, bo
     if (p_sampler + p_env <= 0.0f) return total + radiance * b.tmul;
     const float w = power_heuristic3(b.pdf, 1, p_sampler, 1, p_env, 1);
     return total + radiance * w * b.tmul;
+}
+
+
+// MisDirectLightIntegrator::Li (per-bounce form, :250-269) = _integrateNEE + _integrateBSDFConnection
+__device__ inline Spec mis_direct_li(const DeviceScene &s, const Surface &sf, bool has_conn, const Connection &cn,
+                                     const SpectralCtx &sc, MtStream &rng, unsigned &err) {
+    const MisNeePart nee = mis_nee_part(s, sf, has_conn, sc, rng);
+    Spec total = spec(0.0f);
+    if (nee.cast && !occluded(s, nee.o, nee.d, nee.limit, err)) total = total + nee.add;
+    return mis_conn_part(s, total, has_conn, cn, sc);
 }
 
 // ============================================================================
@@ -718,26 +728,16 @@ __device__ __forceinline__ Spec direct_li(const DeviceScene &s, const RP &rp, co
     return mis_direct_li(s, sf, has_conn, cn, sc, rng, err);
 }
 
-// _li (:92-209). Later bounces query the scene directly (they only run in the
-// one-thread-per-pixel form). kDirectOnly: the caller guarantees maxDepth 1
-// (the wavefront form), so the later-bounce loop is not compiled.
-template <bool kRis, class RP, bool kDirectOnly = false>
-__device__ Spec path_li_shaded(const DeviceScene &s, const RP &rp, const Surface &sf0, const SpectralCtx &sc,
-                               MtStream &rng, const PathRun &pr, const RisRun &ris, const ReservoirView &rv,
-                               size_t pixel, const MtStream *gen_end_state, unsigned &err) {
-    Spec total = rgb_to_spectrum(sf0.c.emission, sc.up);
-    Spec tp = spec(1.0f);
-    BounceState st{0, 0};
-    const Connection first = sample_bounce_with_connection(rp, 0, sf0, pr.max_refl, pr.max_refr, st, sc, rng, err);
-    total = total + direct_li<kRis>(s, rp, sf0, first.b.ok, first, sc, rng, true, ris, rv, pixel, gen_end_state, err);
-    if (!first.b.ok) return total;
-    if (kDirectOnly) return total;  // maxDepth 1: the loop below would not run
-    tp = tp * first.b.tmul;
-    V3 ro = first.b.origin, rd = first.b.dir;
-    bool has_next = first.has_hit;
-    Hit next = first.hit;
+// The bounce loop of _li (:114-207) from vertex `first_bounce` on: `next` is
+// that vertex's hit (of the ray ro, rd), tp and total the path so far. Later
+// vertices query the scene on the spot.
+template <bool kRis>
+__device__ Spec path_li_continue(const DeviceScene &s, Spec total, Spec tp, V3 ro, V3 rd, bool has_next, Hit next,
+                                 BounceState st, const SpectralCtx &sc, MtStream &rng, const PathRun &pr,
+                                 const RisRun &ris, const ReservoirView &rv, size_t pixel, int first_bounce,
+                                 unsigned &err) {
     const TraceNow now{&s};
-    for (int bounce = 1; bounce < pr.max_depth; ++bounce) {
+    for (int bounce = first_bounce; bounce < pr.max_depth; ++bounce) {
         if (!has_next) break;
         const Hit bh = next;
         Closure c = get_closure(s, bh);
@@ -767,6 +767,25 @@ __device__ Spec path_li_shaded(const DeviceScene &s, const RP &rp, const Surface
         }
     }
     return total;
+}
+
+// _li (:92-209). Later bounces query the scene directly (they only run in the
+// one-thread-per-pixel form). kDirectOnly: the caller guarantees maxDepth 1
+// (the wavefront form), so the later-bounce loop is not compiled.
+template <bool kRis, class RP, bool kDirectOnly = false>
+__device__ Spec path_li_shaded(const DeviceScene &s, const RP &rp, const Surface &sf0, const SpectralCtx &sc,
+                               MtStream &rng, const PathRun &pr, const RisRun &ris, const ReservoirView &rv,
+                               size_t pixel, const MtStream *gen_end_state, unsigned &err) {
+    Spec total = rgb_to_spectrum(sf0.c.emission, sc.up);
+    Spec tp = spec(1.0f);
+    BounceState st{0, 0};
+    const Connection first = sample_bounce_with_connection(rp, 0, sf0, pr.max_refl, pr.max_refr, st, sc, rng, err);
+    total = total + direct_li<kRis>(s, rp, sf0, first.b.ok, first, sc, rng, true, ris, rv, pixel, gen_end_state, err);
+    if (!first.b.ok) return total;
+    if (kDirectOnly) return total;  // maxDepth 1: the loop below would not run
+    tp = tp * first.b.tmul;
+    return path_li_continue<kRis>(s, total, tp, first.b.origin, first.b.dir, first.has_hit, first.hit, st, sc, rng, pr,
+                                  ris, rv, pixel, 1, err);
 }
 
 // PathIntegrator::Li (:48-90): opacity skip at the GBuffer hit, Beer, then _li.

@@ -571,6 +571,52 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
     return end_pass(c, 1);
 }
 
+namespace {
+// The per-path planes, queues and hit slots of the wavefront PathTracePass for
+// `count` paths (per-frame scratch on ctx c).
+hdr_status pt_buffers(hdr_ctx *c, size_t count, hdr::PtBuffers &B) {
+    B = hdr::PtBuffers{};
+    B.pixels = count;
+    struct Plane {
+        const char *name;
+        size_t bytes;
+        void **dst;
+    };
+    void *rng, *tp, *total, *outer, *ro, *rd, *bo, *bd, *bt, *nee, *state, *a0, *a1, *cnt, *qc, *qs, *hits, *hv, *occ;
+    const Plane planes[] = {
+        {"__pt_rng", count * 48, &rng},     {"__pt_tp", count * 16, &tp},       {"__pt_total", count * 16, &total},
+        {"__pt_outer", count * 16, &outer}, {"__pt_ray_o", count * 16, &ro},    {"__pt_ray_d", count * 16, &rd},
+        {"__pt_b_origin", count * 16, &bo}, {"__pt_b_dir", count * 16, &bd},    {"__pt_b_tmul", count * 16, &bt},
+        {"__pt_nee", count * 16, &nee},     {"__pt_state", count * 16, &state}, {"__pt_active0", count * 4, &a0},
+        {"__pt_active1", count * 4, &a1},   {"__pt_counts", 32, &cnt},          {"__pt_q_closest", count * 32, &qc},
+        {"__pt_q_shadow", count * 32, &qs}, {"__pt_hits", count * 16, &hits},   {"__pt_hit_v", count * 4, &hv},
+        {"__pt_occ", count, &occ}};
+    hdr_status st;
+    for (const Plane &pl : planes)
+        if ((st = ensure_scratch(c, pl.name, pl.bytes, pl.dst)) != HDR_OK) return st;
+    B.rng = (uint4 *)rng;
+    B.tp = (float4 *)tp;
+    B.total = (float4 *)total;
+    B.outer = (float4 *)outer;
+    B.ray_o = (float4 *)ro;
+    B.ray_d = (float4 *)rd;
+    B.b_origin_pdf = (float4 *)bo;
+    B.b_dir = (float4 *)bd;
+    B.b_tmul = (float4 *)bt;
+    B.nee_add = (float4 *)nee;
+    B.state = (int4 *)state;
+    B.active[0] = (int *)a0;
+    B.active[1] = (int *)a1;
+    B.counts = (int *)cnt;
+    B.q_closest = (float4 *)qc;
+    B.q_shadow = (float4 *)qs;
+    B.hits = (float4 *)hits;
+    B.hit_v = (float *)hv;
+    B.occ = (unsigned char *)occ;
+    return HDR_OK;
+}
+}  // namespace
+
 hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src) {
     if (!dst || !src || dst == src) return fail(HDR_EINVAL, "need two distinct contexts");
     if (dst->device != src->device) return fail(HDR_EINVAL, "contexts are on different devices");
@@ -788,6 +834,24 @@ hdr_status hdr_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index
     d.render_ibl_background = p->render_ibl_background;
     d.roulette = p->roulette_aggressiveness;
     const hdr::CameraD cd = make_camera(cam);
+    if (c->scene_opaque && !(c->flags & HDR_CTX_PT_ONE_KERNEL)) {
+        hdr::PtBuffers B{};
+        if ((st = pt_buffers(c, count, B)) != HDR_OK) return st;
+        if ((st = begin_pass(c, 1)) != HDR_OK) return st;
+        hdr::PtJobD job{};
+        job.cam = cd;
+        job.gb = gb;
+        job.color = (float4 *)color;
+        job.err = c->d_err;
+        job.pr = hdr::path_run_of(d);
+        job.frame_index = frame_index;
+        const int n = hdr::launch_path_trace_wavefront(c->scene, &job, 1, nullptr,
+                                                       hdr::tile_blocks(cam->width, cam->height), B, c->tune,
+                                                       c->d_err, c->stream);
+        if (n < 0) return fail(HDR_ECUDA, "path trace launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        c->launches += (uint64_t)n;
+        return end_pass(c, 1);
+    }
     if ((st = begin_pass(c, 1)) != HDR_OK) return st;
     hdr::launch_path_trace(c->scene, cd, frame_index, d, gb, (float4 *)color, c->d_err, c->stream);
     c->launches += 1;
@@ -854,6 +918,18 @@ hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camer
         tiles += (long long)hdr::tile_blocks(cam->width, cam->height);
     }
     if (tiles >= (1ll << 31)) return fail(HDR_EINVAL, "batch of %lld tiles is too large", tiles);
+    // the wavefront form needs an opaque scene and one set of path settings for all images
+    bool wave = lead->scene_opaque && !(lead->flags & HDR_CTX_PT_ONE_KERNEL);
+    long long paths = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        hdr::PtJobD &j = jobs[(size_t)i];
+        j.pixel_begin = (int)paths;
+        paths += (long long)j.cam.width * j.cam.height;
+        wave = wave && std::memcmp(&settings[i], &settings[0], sizeof(hdr_path_settings)) == 0;
+    }
+    if (paths >= (1ll << 31)) return fail(HDR_EINVAL, "batch of %lld paths is too large", paths);
+    hdr::PtBuffers B{};
+    if (wave && (st = pt_buffers(lead, (size_t)paths, B)) != HDR_OK) return st;
     void *table = nullptr;
     if ((st = ensure_scratch(lead, "__batch_pt_jobs", jobs.size() * sizeof(hdr::PtJobD), &table)) != HDR_OK)
         return st;
@@ -865,7 +941,14 @@ hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camer
     // the table is read by the launch below; the host vector stays alive until the copy is done
     HDR_CUDA(cudaMemcpyAsync(table, jobs.data(), jobs.size() * sizeof(hdr::PtJobD), cudaMemcpyHostToDevice,
                              lead->stream));
-    hdr::launch_path_trace_batch(lead->scene, (const hdr::PtJobD *)table, n, (int)tiles, lead->stream);
+    if (wave) {
+        const int nl = hdr::launch_path_trace_wavefront(lead->scene, jobs.data(), n, (const hdr::PtJobD *)table,
+                                                        (int)tiles, B, lead->tune, lead->d_err, lead->stream);
+        if (nl < 0) return fail(HDR_ECUDA, "path trace launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        lead->launches += (uint64_t)nl - 1;
+    } else {
+        hdr::launch_path_trace_batch(lead->scene, (const hdr::PtJobD *)table, n, (int)tiles, lead->stream);
+    }
     HDR_CUDA(cudaGetLastError());
     HDR_CUDA(cudaEventRecord(lead->sync_ev, lead->stream));
     for (int32_t i = 1; i < n; ++i) HDR_CUDA(cudaStreamWaitEvent(ctxs[i]->stream, lead->sync_ev, 0));

@@ -38,24 +38,6 @@ __device__ __forceinline__ int queue_append(int *counter, bool want) {
     return base + __popc(mask & ((1u << lane) - 1u));
 }
 
-__device__ __forceinline__ void store_stream(uint4 *st, size_t i, size_t n, const MtStream &r) {
-    st[i] = make_uint4((unsigned)r.a, (unsigned)(r.a >> 32), (unsigned)r.b, (unsigned)(r.b >> 32));
-    st[n + i] = make_uint4((unsigned)r.c, (unsigned)(r.c >> 32), (unsigned)r.d, (unsigned)(r.d >> 32));
-    st[2 * n + i] = make_uint4((unsigned)r.new0, (unsigned)(r.new0 >> 32), r.k, r.seed);
-}
-__device__ __forceinline__ MtStream load_stream(const uint4 *st, size_t i, size_t n) {
-    const uint4 p = st[i], q = st[n + i], w = st[2 * n + i];
-    MtStream r;
-    r.a = (uint64_t)p.x | ((uint64_t)p.y << 32);
-    r.b = (uint64_t)p.z | ((uint64_t)p.w << 32);
-    r.c = (uint64_t)q.x | ((uint64_t)q.y << 32);
-    r.d = (uint64_t)q.z | ((uint64_t)q.w << 32);
-    r.new0 = (uint64_t)w.x | ((uint64_t)w.y << 32);
-    r.k = w.z;
-    r.seed = w.w;
-    r.spill = nullptr;
-    return r;
-}
 
 // Per-pixel prologue shared by generate and shade: stream, jittered camera
 // ray, wavelengths, GBuffer hit (integration_pass.cpp:210-233).

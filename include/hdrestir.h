@@ -218,6 +218,8 @@ typedef struct hdr_gbuffer_texel {
                                     A/B timing) */
 #define HDR_CTX_LANE_PER_RAY 8u  /* wavefront trace kernels keep each lane on one ray until it is
                                     done instead of refilling idle lanes (for A/B timing) */
+#define HDR_CTX_PT_ONE_KERNEL 32u /* PathTracePass in one thread per pixel (rays cast on the spot)
+                                     instead of the wavefront form; same image (for A/B checks) */
 #define HDR_CTX_UNPHASED 16u     /* wavefront trace kernels step each lane's whole walk every
                                     iteration instead of serving leaves, instance entries and ray
                                     starts in their own phases (for A/B timing) */

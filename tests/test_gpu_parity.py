@@ -312,3 +312,28 @@ def test_path_trace_batch_equals_images_alone():
             x.close()
     for g, w in zip(got, want):
         assert np.array_equal(g.view(np.uint32), w.view(np.uint32))
+
+
+@pytest.mark.parametrize("case", ["cfg0", "cfg2", "dome"])
+def test_wavefront_path_trace_equals_one_thread_form(case):
+    """PathTracePass in wavefront form (per-vertex kernels, compacted live paths)
+    gives the one-thread-per-pixel form's image bit for bit, roulette included."""
+    from hdrestir_b200.context import Context
+    if case == "dome":
+        sc, cam, _ = _dome_scene()
+        depth = 16
+    else:
+        sc, cam = _scene(0 if case == "cfg0" else 2)
+        depth = 6 if case == "cfg0" else 8
+    outs = []
+    for one in (False, True):
+        with Context(device=0, pt_one_kernel=one) as ctx:
+            ctx.upload_scene(sc)
+            frames = []
+            for f in range(3):
+                ctx.raycast(cam, f)
+                ctx.path_trace(cam, f, max_depth=depth)
+                ctx.accumulate(f)
+                frames.append(ctx.download("Color").copy())
+            outs.append(np.stack(frames))
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
