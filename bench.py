@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched and served legs")
-    ap.add_argument("--serving-jobs", type=int, default=40, help="config-4 jobs per serving leg")
+    ap.add_argument("--serving-jobs", type=int, default=80, help="config-4 jobs per serving leg")
     ap.add_argument("--width", type=int, default=1920, help="smaller frames only for profiler captures")
     ap.add_argument("--height", type=int, default=1080)
     return ap.parse_args()
@@ -310,7 +310,7 @@ def serving_leg(n_jobs: int):
                        "256^2..2048x1152, 1-16 frames, ReSTIR (32 cand) or PathTracer (maxDepth 4); "
                        "HBM admission budget 120 GB",
            "mpx_frames": mpx_frames}
-    step_px = {"plain": 0, "served_all": 0, "served": 8 << 20}
+    step_px = {"plain": 0, "served_all": 0, "served": 16 << 20}
     for mode in ("plain", "served_all", "served"):
         with Server(device=0, hbm_budget=120 << 30, serial=(mode == "plain"), step_pixels=step_px[mode]) as sv:
             sids = [sv.add_scene(s) for s in scenes]
@@ -324,6 +324,7 @@ def serving_leg(n_jobs: int):
                 sv.step()
             for jid in warm:
                 sv.take(jid, keep_image=False)
+            sv.finished()
             lat, pending, nxt = [], {}, 0
             steps = 0
             t0 = time.perf_counter()
@@ -338,18 +339,15 @@ def serving_leg(n_jobs: int):
                 if not pending:
                     time.sleep(max(0.0, jobs[nxt]["arrival"] - now))
                     continue
-                if sv.step() == 0:
-                    steps += 1
-                    continue
                 steps += 1
+                if sv.step() == 0:
+                    continue
                 now = time.perf_counter() - t0
-                for jid in list(pending):
-                    st, _ = sv.state(jid)
-                    if st in (abi.JOB_DONE, abi.JOB_FAILED):
-                        if st == abi.JOB_FAILED:
-                            raise RuntimeError(f"serving job {jid} failed")
-                        lat.append(now - pending.pop(jid))
-                        sv.take(jid, keep_image=False)
+                for jid in sv.finished():
+                    if sv.state(jid)[0] == abi.JOB_FAILED:
+                        raise RuntimeError(f"serving job {jid} failed")
+                    lat.append(now - pending.pop(jid))
+                    sv.take(jid, keep_image=False)
             makespan = time.perf_counter() - t0
         lat.sort()
         out[mode] = {"jobs_per_s": n_jobs / makespan, "mpx_frames_per_s": mpx_frames / makespan,
@@ -357,7 +355,7 @@ def serving_leg(n_jobs: int):
                      "latency_p99_ms": 1000.0 * lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))],
                      "steps": steps}
     out["modes"] = ("plain: one job at a time, each frame rendered alone; served_all: every admitted job "
-                    "advances each step; served: least remaining work first, 8 Mpx per step")
+                    "advances each step; served: least remaining work first, 16 Mpx per step")
     return out
 
 

@@ -173,6 +173,7 @@ def lib() -> C.CDLL:
             "hdr_server_job_state": (C.c_int, [vp, C.c_int64, C.POINTER(i32), C.POINTER(i32)]),
             "hdr_server_take_result": (C.c_int, [vp, C.c_int64, vp, sz]),
             "hdr_server_load": (C.c_int, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(sz)]),
+            "hdr_server_drain_finished": (C.c_int, [vp, C.POINTER(C.c_int64), i32, C.POINTER(i32)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -69,6 +69,7 @@ struct hdr_server {
     std::deque<std::unique_ptr<Job>> queued;
     std::vector<std::unique_ptr<Job>> active;
     std::map<int64_t, std::unique_ptr<Job>> finished;
+    std::vector<int64_t> unreported;  // finished jobs not yet returned by hdr_server_drain_finished
     int64_t next_id = 1;
     std::mutex mu;
 };
@@ -101,6 +102,7 @@ hdr_status admit(hdr_server *sv) {
             job->state = HDR_JOB_FAILED;
             const int64_t id = job->id;
             sv->finished[id] = std::move(job);
+            sv->unreported.push_back(id);
             continue;
         }
         job->ctx = c;
@@ -239,7 +241,9 @@ hdr_status hdr_server_step(hdr_server *sv, int32_t *jobs_finished) {
     // 3. accumulation, then the jobs that have all their frames leave the active set
     for (Job *j : run) {
         if (j->state != HDR_JOB_RUNNING) continue;
-        if (hdr_accumulate(j->ctx, j->frames_done, j->d.firefly, HDR_ACCUM_PARITY) != HDR_OK) {
+        // GpuAccumulationPass semantics (the reference's accumulation when its GPU is enabled): no
+        // host round trip per frame, so the step's work stays queued on the streams
+        if (hdr_accumulate(j->ctx, j->frames_done, j->d.firefly, HDR_ACCUM_SHADER) != HDR_OK) {
             fail_job(sv, *j);
             continue;
         }
@@ -258,6 +262,7 @@ hdr_status hdr_server_step(hdr_server *sv, int32_t *jobs_finished) {
             ++done;
             const int64_t id = j->id;
             sv->finished[id] = std::move(j);
+            sv->unreported.push_back(id);
         }
     }
     sv->active = std::move(keep);
@@ -299,6 +304,16 @@ hdr_status hdr_server_take_result(hdr_server *sv, int64_t job_id, float *rgba, s
     release(sv, j);
     sv->finished.erase(it);
     return st;
+}
+
+hdr_status hdr_server_drain_finished(hdr_server *sv, int64_t *ids, int32_t cap, int32_t *n) {
+    if (!sv || !n || (cap > 0 && !ids) || cap < 0) return hdr::set_last_error(HDR_EINVAL, "bad argument");
+    std::lock_guard<std::mutex> lock(sv->mu);
+    const size_t k = std::min(sv->unreported.size(), (size_t)cap);
+    for (size_t q = 0; q < k; ++q) ids[q] = sv->unreported[q];
+    sv->unreported.erase(sv->unreported.begin(), sv->unreported.begin() + (long)k);
+    *n = (int32_t)k;
+    return HDR_OK;
 }
 
 hdr_status hdr_server_load(hdr_server *sv, int32_t *queued, int32_t *running, size_t *bytes_in_use) {

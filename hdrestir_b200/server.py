@@ -59,6 +59,17 @@ class Server:
         abi.check(self._lib.hdr_server_step(self._h, C.byref(n)))
         return n.value
 
+    def finished(self) -> list[int]:
+        """Ids of the jobs that finished since the last call."""
+        out: list[int] = []
+        buf = (C.c_int64 * 256)()
+        n = C.c_int32()
+        while True:
+            abi.check(self._lib.hdr_server_drain_finished(self._h, buf, 256, C.byref(n)))
+            out.extend(buf[k] for k in range(n.value))
+            if n.value < 256:
+                return out
+
     def state(self, job_id: int) -> tuple[int, int]:
         st, fr = C.c_int32(), C.c_int32()
         abi.check(self._lib.hdr_server_job_state(self._h, C.c_int64(job_id), C.byref(st), C.byref(fr)))

@@ -287,8 +287,9 @@ hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camer
  * budget; each hdr_server_step advances admitted jobs by one frame (all of
  * them, or those with the least remaining work up to step_pixels), with the
  * RIS jobs of one scene traced in one batched launch and path-traced jobs
- * side by side on their own streams. HDR_SERVER_SERIAL runs one job at a
- * time, each frame alone (the plain per-frame pipeline). A job's image is the
+ * side by side on their own streams. Accumulation follows GpuAccumulationPass
+ * (HDR_ACCUM_SHADER). HDR_SERVER_SERIAL runs one job at a time, each frame
+ * alone (the plain per-frame pipeline). A job's image is the
  * same in both modes. Calls on one server are serialised by its mutex.
  * ------------------------------------------------------------------------- */
 typedef struct hdr_server hdr_server;
@@ -326,6 +327,8 @@ hdr_status hdr_server_job_state(hdr_server *server, int64_t job_id, int32_t *sta
 /* Copies a finished job's "Color" (width*height RGBA f32; rgba may be NULL to
  * discard it) and frees the job. */
 hdr_status hdr_server_take_result(hdr_server *server, int64_t job_id, float *rgba, size_t bytes);
+/* Up to cap ids of jobs that finished (DONE or FAILED) since the last call. */
+hdr_status hdr_server_drain_finished(hdr_server *server, int64_t *ids, int32_t cap, int32_t *n);
 hdr_status hdr_server_load(hdr_server *server, int32_t *queued, int32_t *running, size_t *bytes_in_use);
 
 /* PathTracePass (passes/path_trace_pass.h:12-39) with MisDirectLightIntegrator. */

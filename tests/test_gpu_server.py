@@ -40,7 +40,7 @@ def _alone(scene, cam, frames, pipeline, settings):
                 ctx.ris_path_trace(cam, f, **settings)
             else:
                 ctx.path_trace(cam, f, **settings)
-            ctx.accumulate(f)
+            ctx.accumulate(f, mode="shader")  # the server accumulates as GpuAccumulationPass
         return ctx.download("Color").copy()
 
 
@@ -52,11 +52,16 @@ def test_server_images_equal_jobs_rendered_alone(serial, step_pixels):
     with Server(device=0, serial=serial, step_pixels=step_pixels) as sv:
         ids = [sv.add_scene(s) for s in scenes]
         jid = [sv.submit(ids[si], cam, fr, pipe, **kw) for si, cam, fr, pipe, kw in jobs]
-        done, steps = 0, 0
+        done, steps, drained = 0, 0, []
         while done < len(jobs):
-            done += sv.step()
+            n = sv.step()
+            done += n
             steps += 1
+            fin = sv.finished()
+            assert len(fin) == n  # each finished job is reported once, in the step that ends it
+            drained += fin
             assert steps < 100
+        assert sorted(drained) == sorted(jid) and sv.finished() == []
         assert all(sv.state(j)[0] == abi.JOB_DONE for j in jid)
         got = [sv.take(j) for j in jid]
     if serial:
