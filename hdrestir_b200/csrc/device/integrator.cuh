@@ -53,7 +53,8 @@ __device__ __forceinline__ bool occluded(const DeviceScene &s, V3 o, V3 d, float
 
 // The same query behind a call: kernels that cast a shadow ray only on a rare
 // path keep the traversal's registers out of their hot loop.
-__device__ __noinline__ bool occluded_call(const DeviceScene &s, V3 o, V3 d, float limit, unsigned &err);
+// occluded() behind a call: bit 0 the answer, the error bits shifted up by one
+__device__ __noinline__ unsigned occluded_call(const DeviceScene *s, V3 o, V3 d, float limit);
 
 // Where the integrators get ray results from. Every ray a pixel casts has a
 // slot: closest-hit slot 0 is the path's bounce ray, closest-hit slot 1 + k
@@ -90,7 +91,9 @@ struct TracedResults {
     }
     // the winner's visibility test of a skipVisibility selection is cast on the spot
     __device__ __forceinline__ bool winner_shadow(V3 o, V3 d, float limit, unsigned &err) const {
-        return occluded_call(*s, o, d, limit, err);
+        const unsigned r = occluded_call(s->dev, o, d, limit);
+        err |= r >> 1;
+        return (r & 1u) != 0;
     }
 };
 

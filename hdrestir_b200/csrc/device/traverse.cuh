@@ -48,6 +48,12 @@ struct DeviceScene {
     const float4 *tlas4;       // 8 per wide node
     float4 tlas_root_lo, tlas_root_hi;
     int wide;                  // 1: walk the wide trees, 0: the binary ones (same results)
+    int proper_boxes;          // 1: no node box of any tree is empty (min > max on some axis)
+    // This struct's own copy in device memory. Kernels take the scene by value
+    // (parameter space); a non-inlined callee gets this pointer instead of the
+    // parameter's address, which would make every thread copy the parameter
+    // block to local memory.
+    const DeviceScene *dev;
 };
 
 __device__ __forceinline__ int fbits(float f) { return __float_as_int(f); }
@@ -56,6 +62,7 @@ struct SlabRay {
     V3 o;
     V3 inv;
     bool small[3];
+    bool any_small;
 };
 
 // IntersectAABB of scene.cpp:16-47 (float thresholds) or bvh.cpp:32-64 (double ones).
@@ -73,6 +80,7 @@ __device__ __forceinline__ SlabRay make_slab_ray(V3 o, V3 d) {
         inv[i] = 1.0f / dd[i];
     }
     r.inv = V3{inv[0], inv[1], inv[2]};
+    r.any_small = r.small[0] | r.small[1] | r.small[2];
     return r;
 }
 
@@ -101,6 +109,25 @@ __device__ __forceinline__ bool slab_test(const SlabRay &r, float4 lo, float4 hi
     }
     t_entry = tmin;
     return !fail & !(tmin > tmax) & (tmax > 1e-4f);
+}
+
+// slab_test for a ray without small axes against a box that is not empty
+// (DeviceScene::proper_boxes): the two checks that cannot fire are left out,
+// the rest is the same arithmetic, so answer and entry distance are equal.
+__device__ __forceinline__ bool slab_test_regular(const SlabRay &r, float4 lo, float4 hi, float &t_entry) {
+    const float t1x = (lo.x - r.o.x) * r.inv.x, t2x = (hi.x - r.o.x) * r.inv.x;
+    const float t1y = (lo.y - r.o.y) * r.inv.y, t2y = (hi.y - r.o.y) * r.inv.y;
+    const float t1z = (lo.z - r.o.z) * r.inv.z, t2z = (hi.z - r.o.z) * r.inv.z;
+    const float tmin = fmaxf(fmaxf(fmaxf(-1e30f, fminf(t1x, t2x)), fminf(t1y, t2y)), fminf(t1z, t2z));
+    const float tmax = fminf(fminf(fminf(1e30f, fmaxf(t1x, t2x)), fmaxf(t1y, t2y)), fmaxf(t1z, t2z));
+    t_entry = tmin;
+    return !(tmin > tmax) & (tmax > 1e-4f);
+}
+
+// slab_test, or slab_test_regular where kRegular says the ray and the scene allow it
+template <bool kRegular>
+__device__ __forceinline__ bool box_test(const SlabRay &r, float4 lo, float4 hi, float &t_entry) {
+    return kRegular ? slab_test_regular(r, lo, hi, t_entry) : slab_test(r, lo, hi, t_entry);
 }
 
 // IntersectTriangle (bvh.cpp:8-30)
@@ -328,9 +355,13 @@ struct PhasedWalk {
         mode = sp > 0 ? kModeNode : kModeDone;
     }
     __device__ __forceinline__ bool shadow_answer() const { return hit.inst >= 0 && hit.t < t_limit; }
+    // both rays of the walk may use slab_test_regular
+    __device__ __forceinline__ bool regular(const DeviceScene &s) const {
+        return s.proper_boxes && !wr.any_small && !br.any_small;
+    }
 
     // one stack entry of a lane in kModeNode
-    template <class St>
+    template <bool kRegular, class St>
     __device__ __forceinline__ void node_step(const DeviceScene &s, unsigned &err, St &st) {
         if (sp <= 0) {
             mode = kModeDone;
@@ -348,7 +379,7 @@ struct PhasedWalk {
         const float4 *np = blas ? s.blas_nodes + 2 * (size_t)(node_base + idx) : s.tlas_nodes + 2 * (size_t)idx;
         const float4 lo = __ldg(np), hi = __ldg(np + 1);
         float ta;
-        if (!slab_test(blas ? br : wr, lo, hi, ta) || ta > hit.t) return;
+        if (!box_test<kRegular>(blas ? br : wr, lo, hi, ta) || ta > hit.t) return;
         const int left = fbits(lo.w);
         if (left >= 0 || !blas) {
             if (sp + 2 > kTraceStack) {
@@ -432,6 +463,7 @@ __device__ bool trace_ray_binary(const DeviceScene &s, V3 o, V3 d, float t_limit
 // the closest t of that moment, as in the binary walk.
 constexpr int kWideStack = 96;
 
+template <bool kRegular = false>
 __device__ __forceinline__ int wide_children(const SlabRay &r, const float4 *n, int codes_out[4], float ta_out[4]) {
     const float4 lx = __ldg(n), ly = __ldg(n + 1), lz = __ldg(n + 2);
     const float4 hx = __ldg(n + 3), hy = __ldg(n + 4), hz = __ldg(n + 5);
@@ -443,8 +475,8 @@ __device__ __forceinline__ int wide_children(const SlabRay &r, const float4 *n, 
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         float ta = 0.0f;
-        const bool pass = cs[k] >= 0 && slab_test(r, make_float4(lxs[k], lys[k], lzs[k], 0.0f),
-                                                  make_float4(hxs[k], hys[k], hzs[k], 0.0f), ta);
+        const bool pass = cs[k] >= 0 && box_test<kRegular>(r, make_float4(lxs[k], lys[k], lzs[k], 0.0f),
+                                                           make_float4(hxs[k], hys[k], hzs[k], 0.0f), ta);
         codes_out[k] = pass ? cs[k] : -1;
         ta_out[k] = ta;
         m += pass ? 1 : 0;
@@ -555,6 +587,135 @@ struct WideWalk {
             if (code >= 0 && slab_test(br, rlo, rhi, ta)) stack.set(sp++, make_int2(code, fbits(ta)));
         }
         return sp > 0;
+    }
+};
+
+// WideWalk split into phases like PhasedWalk: node steps (a wide node's four
+// slab tests and pushes, or a TLAS leaf's instance pushes) run for the lanes
+// that have them; a lane that pops a BLAS leaf or an instance entry parks it.
+// Each lane handles its own entries in its own order with the same running t,
+// so the results are WideWalk's, which are BinaryWalk's.
+template <bool kAnyHit, class Stk>
+struct PhasedWideWalk {
+    V3 o, d, oo, od;
+    SlabRay wr, br;
+    int cur_inst, wide_base, tri_base, sp;
+    float t_limit;
+    HitId hit;
+    int mode;
+    int pend;  // kModeLeaf: BLAS leaf payload; kModeInst: TLAS instance slot
+    Stk stack;
+
+    __device__ __forceinline__ void start(const DeviceScene &s, V3 ro, V3 rd, float limit) {
+        o = ro;
+        d = rd;
+        t_limit = limit;
+        hit.t = 1e30f;
+        hit.inst = -1;
+        hit.tri = -1;
+        hit.u = hit.v = 0.0f;
+        wr = make_slab_ray<false>(o, d);
+        br = wr;
+        oo = o;
+        od = d;
+        cur_inst = -1;
+        wide_base = tri_base = 0;
+        sp = 0;
+        if (s.has_tlas) {
+            float ta = 0.0f;
+            const int code = fbits(s.tlas_root_lo.w);
+            if (code >= 0 && slab_test(wr, s.tlas_root_lo, s.tlas_root_hi, ta))
+                stack.set(sp++, make_int2(code, fbits(ta)));
+        }
+        mode = sp > 0 ? kModeNode : kModeDone;
+    }
+    __device__ __forceinline__ bool shadow_answer() const { return hit.inst >= 0 && hit.t < t_limit; }
+    __device__ __forceinline__ bool regular(const DeviceScene &s) const {
+        return s.proper_boxes && !wr.any_small && !br.any_small;
+    }
+
+    template <bool kRegular, class St>
+    __device__ __forceinline__ void node_step(const DeviceScene &s, unsigned &err, St &st) {
+        if (sp <= 0) {
+            mode = kModeDone;
+            return;
+        }
+        const int2 e = stack.get(--sp);
+        st.pop();
+        if (__int_as_float(e.y) > hit.t) return;  // entry beyond the closest hit so far
+        const int tag = e.x & ((1 << kWideTagBits) - 1), pay = e.x >> kWideTagBits;
+        if (tag == kWTagBlasNode || tag == kWTagTlasNode) {
+            if (sp + 4 > kWideStack) {
+                err |= (tag == kWTagBlasNode) ? kErrBlasStack : kErrTlasStack;
+                sp = 0;
+                mode = kModeDone;
+                return;
+            }
+            const bool blas = tag == kWTagBlasNode;
+            const float4 *n = blas ? s.blas4 + 8 * (size_t)(wide_base + pay) : s.tlas4 + 8 * (size_t)pay;
+            int cs[4];
+            float ts[4];
+            wide_children<kRegular>(blas ? br : wr, n, cs, ts);
+#pragma unroll
+            for (int k = 3; k >= 0; --k)
+                if (cs[k] >= 0) stack.set(sp++, make_int2(cs[k], fbits(ts[k])));
+        } else if (tag == kWTagTlasLeaf) {
+            if (sp + 2 > kWideStack) {
+                err |= kErrTlasStack;
+                sp = 0;
+                mode = kModeDone;
+                return;
+            }
+            const int first = pay >> kTlasLeafCountBits;
+            const int cnt = (pay & ((1 << kTlasLeafCountBits) - 1)) + 1;
+            // instances pop in leaf order; no entry-distance cull at this level
+            for (int k = cnt - 1; k >= 0; --k)
+                stack.set(sp++, make_int2(((first + k) << kWideTagBits) | kWTagInst, fbits(-3.402823466e+38f)));
+        } else {
+            pend = pay;
+            mode = tag == kWTagBlasLeaf ? kModeLeaf : kModeInst;
+        }
+    }
+    template <class St>
+    __device__ __forceinline__ void leaf(const DeviceScene &s, St &st) {
+        const int first = pend >> kBlasLeafCountBits;
+        const int cnt = (pend & ((1 << kBlasLeafCountBits) - 1)) + 1;
+        st.leaf();
+        for (int q = 0; q < cnt; ++q) {
+            float tt, uu, vv;
+            st.tri();
+            if (tri_test(oo, od, s.tri_geo + 3 * (size_t)(tri_base + first + q), tt, uu, vv) && tt < hit.t) {
+                hit.t = tt;
+                hit.inst = cur_inst;
+                hit.tri = first + q;
+                hit.u = uu;
+                hit.v = vv;
+            }
+        }
+        if (kAnyHit && hit.inst >= 0 && hit.t < t_limit) sp = 0;
+        mode = sp > 0 ? kModeNode : kModeDone;
+    }
+    __device__ __forceinline__ void inst(const DeviceScene &s) {
+        const int ii = __ldg(&s.tlas_inst[pend]);
+        const float4 *ip = s.instances + 8 * ii;
+        const float4 r7 = __ldg(ip + 7);
+        if (fbits(r7.y) != 0) {  // a mesh without triangles has an empty BVH
+            const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2), m3 = __ldg(ip + 3);
+            const float inv[16] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w,
+                                   m2.x, m2.y, m2.z, m2.w, m3.x, m3.y, m3.z, m3.w};
+            oo = m4f_transform(inv, o);
+            od = m4f_transform_dir(inv, d);
+            br = make_slab_ray<true>(oo, od);
+            wide_base = fbits(r7.z);
+            tri_base = fbits(__ldg(&ip[5].w));
+            cur_inst = ii;
+            const int mesh = fbits(r7.w);
+            const float4 rlo = __ldg(&s.blas_roots[2 * mesh]), rhi = __ldg(&s.blas_roots[2 * mesh + 1]);
+            float ta = 0.0f;
+            const int code = fbits(rlo.w);
+            if (code >= 0 && slab_test(br, rlo, rhi, ta)) stack.set(sp++, make_int2(code, fbits(ta)));
+        }
+        mode = sp > 0 ? kModeNode : kModeDone;
     }
 };
 

@@ -69,6 +69,8 @@ struct SceneStore {
     int device = 0;
     std::vector<void *> ptrs;
     size_t bytes = 0;
+    // the scene descriptor in device memory, [0] for the binary walk, [1] for the wide one
+    const hdr::DeviceScene *desc_dev = nullptr;
     ~SceneStore() {
         if (ptrs.empty()) return;
         int prev = 0;
@@ -363,6 +365,36 @@ void hdr_ctx_destroy(hdr_ctx *c) {
     delete c;
 }
 
+namespace {
+// True when no node box of the flat scene's trees is empty (min > max on an
+// axis): the traversal may then leave GfRange3f::IsEmpty out of its slab tests.
+bool boxes_proper(const hdr::FlatScene &f) {
+    auto empty = [](const float *lo, const float *hi) { return lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]; };
+    for (size_t k = 0; k + 8 <= f.blas_nodes.size(); k += 8)
+        if (empty(&f.blas_nodes[k], &f.blas_nodes[k + 4])) return false;
+    for (size_t k = 0; k + 8 <= f.tlas_nodes.size(); k += 8)
+        if (empty(&f.tlas_nodes[k], &f.tlas_nodes[k + 4])) return false;
+    for (const std::vector<float> *w : {&f.blas4, &f.tlas4})
+        for (size_t k = 0; k + hdr::kWideNodeFloats <= w->size(); k += hdr::kWideNodeFloats) {
+            const float *n = w->data() + k;
+            for (int j = 0; j < 4; ++j) {
+                int code;
+                std::memcpy(&code, &n[24 + j], sizeof(code));
+                const float lo[3] = {n[j], n[4 + j], n[8 + j]}, hi[3] = {n[12 + j], n[16 + j], n[20 + j]};
+                if (code >= 0 && empty(lo, hi)) return false;
+            }
+        }
+    for (size_t k = 0; k + 8 <= f.blas_roots.size(); k += 8) {
+        int code;
+        std::memcpy(&code, &f.blas_roots[k + 3], sizeof(code));
+        if (code >= 0 && empty(&f.blas_roots[k], &f.blas_roots[k + 4])) return false;
+    }
+    int root;
+    std::memcpy(&root, &f.tlas_root[3], sizeof(root));
+    return !(root >= 0 && empty(&f.tlas_root[0], &f.tlas_root[4]));
+}
+}  // namespace
+
 hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     if (!c || !desc) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);
@@ -433,6 +465,27 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     s.dome_height = f.dome_height;
     s.dome_total_lum = f.dome_total_lum;
     s.has_tlas = f.num_instances > 0 ? 1 : 0;
+    s.proper_boxes = boxes_proper(f) ? 1 : 0;
+    // the descriptor itself, for callees that are not inlined into a kernel
+    hdr::DeviceScene copies[2] = {s, s};
+    {
+        DevBuf b;
+        st = dev_alloc(c, b, sizeof(copies));
+        if (st != HDR_OK) {
+            cudaStreamSynchronize(c->stream);
+            c->allocated -= store->bytes;
+            return st;
+        }
+        store->ptrs.push_back(b.ptr);
+        store->bytes += b.bytes;
+        store->desc_dev = (const hdr::DeviceScene *)b.ptr;
+        for (int w = 0; w < 2; ++w) {  // each copy points at itself
+            copies[w].wide = w;
+            copies[w].dev = store->desc_dev + w;
+        }
+        HDR_CUDA(cudaMemcpyAsync(b.ptr, copies, sizeof(copies), cudaMemcpyHostToDevice, c->stream));
+    }
+    s.dev = store->desc_dev + s.wide;
     const cudaError_t sync_err = cudaStreamSynchronize(c->stream);
     c->scene_store = store;  // owns the buffers from here on, also on the error path below
     c->scene_bytes_accounted = store->bytes;
@@ -630,6 +683,7 @@ hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src) {
     dst->scene_bytes_accounted = 0;
     dst->scene = src->scene;
     dst->scene.wide = (dst->flags & HDR_CTX_WIDE_BVH) ? 1 : 0;
+    dst->scene.dev = dst->scene_store->desc_dev + dst->scene.wide;
     dst->scene_opaque = src->scene_opaque;
     dst->scene_light_geometry = src->scene_light_geometry;
     dst->has_scene = true;

@@ -105,17 +105,21 @@ __device__ __forceinline__ int job_of_block(const PtJobD *table, int n_jobs) {
 
 }  // namespace
 
-// the rest of a path in one thread (its stream may now pass draw 311)
-__device__ __noinline__ Spec pt_finish_in_thread(const DeviceScene &s, Spec total, Spec tp, V3 ro, V3 rd,
-                                                 bool has_next, const Hit &next, BounceState st,
-                                                 const SpectralCtx &sc, MtStream rng, const PathRun &pr,
-                                                 int first_bounce, unsigned &err) {
+// The rest of a path in one thread (its stream may now pass draw 311). Its
+// arguments are values and a device-memory scene, so that no variable of the
+// caller has its address taken (which would keep it in local memory).
+__device__ __noinline__ Spec pt_finish_in_thread(const DeviceScene *s, Spec total, Spec tp, V3 ro, V3 rd, Hit next,
+                                                 BounceState st, SpectralCtx sc, MtStream rng, PathRun pr,
+                                                 int first_bounce, unsigned *err) {
     uint64_t spill[312];
     rng.spill = spill;
     const RisRun ris{};
     const ReservoirView rv{};
-    return path_li_continue<false>(s, total, tp, ro, rd, has_next, next, st, sc, rng, pr, ris, rv, 0, first_bounce,
-                                   err);
+    unsigned e = 0;
+    const Spec r = path_li_continue<false>(*s, total, tp, ro, rd, true, next, st, sc, rng, pr, ris, rv, 0, first_bounce,
+                                           e);
+    if (e) atomicOr(err, e);
+    return r;
 }
 
 template <bool kBatch>
@@ -254,8 +258,8 @@ __global__ void __launch_bounds__(256) pt_connect_kernel(DeviceScene s, PtJobD o
             alive = alive && vertex + 1 < pr.max_depth && cn.has_hit;
             if (alive && rng.k >= kStreamHandOffLimit) {
                 const BounceState st{stt.x, stt.y};
-                total = pt_finish_in_thread(s, total, tp, cn.b.origin, cn.b.dir, true, cn.hit, st, sc, rng, pr,
-                                            vertex + 1, e);
+                total = pt_finish_in_thread(s.dev, total, tp, cn.b.origin, cn.b.dir, cn.hit, st, sc, rng, pr,
+                                            vertex + 1, err);
                 alive = false;
             }
             if (alive) {

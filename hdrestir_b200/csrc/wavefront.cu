@@ -131,8 +131,10 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
     store_stream(wb.rng_state, i, wb.pixels, rng);
 }
 
-__device__ __noinline__ bool occluded_call(const DeviceScene &s, V3 o, V3 d, float limit, unsigned &err) {
-    return occluded(s, o, d, limit, err);
+__device__ __noinline__ unsigned occluded_call(const DeviceScene *s, V3 o, V3 d, float limit) {
+    unsigned e = 0;
+    const bool occ = occluded(*s, o, d, limit, e);
+    return (occ ? 1u : 0u) | (e << 1);
 }
 
 // Trace kernels. Rays of a warp take very different numbers of steps (shadow
@@ -173,12 +175,25 @@ struct TraceWalk {
 // of the warp are stepping nodes; then the parked leaves, instance entries and
 // finished rays of all lanes are served, and finished lanes take the next
 // queued rays.
-template <bool kAnyHit, class Put>
+// Shared-memory stack entries per thread of the phased wide walk (8-byte
+// entries: the same 12 KB per block as the binary walk's 24 four-byte ones).
+constexpr int kSharedDepthWide = 12;
+
+template <bool kWide, bool kAnyHit>
+struct PhasedTraceWalk {
+    using Entry = typename std::conditional<kWide, int2, int>::type;
+    static constexpr int kShared = kWide ? kSharedDepthWide : kSharedDepth;
+    using Stack = SplitStack<Entry, kShared, kTraceThreads>;
+    using type = typename std::conditional<kWide, PhasedWideWalk<kAnyHit, Stack>, PhasedWalk<kAnyHit, Stack>>::type;
+};
+
+template <bool kWide, bool kAnyHit, class Put>
 __device__ __forceinline__ void phased_trace(const DeviceScene &s, const float4 *__restrict__ q, int n,
                                              int *fetch_at, int quorum, Put put, unsigned &e) {
-    __shared__ int col[kSharedDepth * kTraceThreads];
-    int deep[kTraceStack - kSharedDepth];
-    PhasedWalk<kAnyHit, SplitStack<int, kSharedDepth, kTraceThreads>> w;
+    using PW = PhasedTraceWalk<kWide, kAnyHit>;
+    __shared__ typename PW::Entry col[PW::kShared * kTraceThreads];
+    typename PW::Entry deep[kTraceStack - PW::kShared];
+    typename PW::type w;
     w.stack.col = col + threadIdx.x;
     w.stack.deep = deep;
     w.mode = kModeDone;
@@ -203,18 +218,31 @@ __device__ __forceinline__ void phased_trace(const DeviceScene &s, const float4 
         }
         if (!__any_sync(kFullMask, w.mode != kModeIdle)) break;
         do {
-            if (w.mode == kModeNode) w.node_step(s, e, ns);
+            if (w.mode == kModeNode) {
+                if (w.regular(s))
+                    w.template node_step<true>(s, e, ns);
+                else
+                    w.template node_step<false>(s, e, ns);
+            }
         } while (__popc(__ballot_sync(kFullMask, w.mode == kModeNode)) >= quorum);
         if (w.mode == kModeLeaf) w.leaf(s, ns);
         if (w.mode == kModeInst) w.inst(s);
     }
 }
 
-__global__ void __launch_bounds__(kTraceThreads) trace_closest_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
+// Resident blocks per SM the phased kernels are compiled for (64 registers for
+// the binary walk, 80 for the wide one).
+template <bool kWide>
+constexpr int phased_min_blocks() {
+    return kWide ? 6 : 8;
+}
+
+template <bool kWide>
+__global__ void __launch_bounds__(kTraceThreads, phased_min_blocks<kWide>()) trace_closest_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
                                                                              int *counts, float4 *hits, float *hit_v,
                                                                              int quorum, unsigned *err) {
     unsigned e = 0;
-    phased_trace<false>(
+    phased_trace<kWide, false>(
         s, q, counts[0], &counts[3], quorum,
         [&](int slot, const auto &w) {
             hits[slot] = make_float4(w.hit.t, __int_as_float(w.hit.inst), __int_as_float(w.hit.tri), w.hit.u);
@@ -224,11 +252,12 @@ __global__ void __launch_bounds__(kTraceThreads) trace_closest_phased_kernel(Dev
     if (e) atomicOr(err, e);
 }
 
-__global__ void __launch_bounds__(kTraceThreads) trace_shadow_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
+template <bool kWide>
+__global__ void __launch_bounds__(kTraceThreads, phased_min_blocks<kWide>()) trace_shadow_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
                                                                             int *counts, unsigned char *occ, int quorum,
                                                                             unsigned *err) {
     unsigned e = 0;
-    phased_trace<true>(
+    phased_trace<kWide, true>(
         s, q, counts[1], &counts[2], quorum,
         [&](int slot, const auto &w) { occ[slot] = w.shadow_answer() ? 1 : 0; }, e);
     if (e) atomicOr(err, e);
@@ -349,11 +378,11 @@ int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &t
     auto mark = [&](cudaEvent_t *ev, int k) { return !ev || cudaEventRecord(ev[k], st) == cudaSuccess; };
     const int tgrid = tune.sm_count * tune.blocks_per_sm;
     const bool refill = (tune.mode & kTraceLanePerRay) == 0;
-    const bool phased = !s.wide && refill && (tune.mode & kTraceUnphased) == 0;
+    const bool phased = refill && (tune.mode & kTraceUnphased) == 0;
     if (!mark(ev_begin, 0)) return -1;
     if (phased) {
-        trace_closest_phased_kernel<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v,
-                                                                      tune.node_quorum, err);
+        auto closest = s.wide ? trace_closest_phased_kernel<true> : trace_closest_phased_kernel<false>;
+        closest<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, tune.node_quorum, err);
     } else {
         auto closest = s.wide ? (refill ? trace_closest_kernel<true, true> : trace_closest_kernel<true, false>)
                               : (refill ? trace_closest_kernel<false, true> : trace_closest_kernel<false, false>);
@@ -361,8 +390,8 @@ int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &t
     }
     if (!mark(ev_end, 0) || !mark(ev_begin, 1)) return -1;
     if (phased) {
-        trace_shadow_phased_kernel<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ,
-                                                                     tune.node_quorum, err);
+        auto shadow = s.wide ? trace_shadow_phased_kernel<true> : trace_shadow_phased_kernel<false>;
+        shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ, tune.node_quorum, err);
     } else {
         auto shadow = s.wide ? (refill ? trace_shadow_kernel<true, true> : trace_shadow_kernel<true, false>)
                              : (refill ? trace_shadow_kernel<false, true> : trace_shadow_kernel<false, false>);

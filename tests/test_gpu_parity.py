@@ -210,7 +210,8 @@ def test_trace_kernel_forms_give_identical_images():
     sc, cam = configs.small_variant(2, 160, 96, grid=128, n_spheres=200, n_lights=2000)
     outs = []
     for kw in ({}, dict(unphased=True), dict(lane_per_ray=True), dict(wide_bvh=True),
-               dict(wide_bvh=True, lane_per_ray=True), dict(tuning=(3, 2)), dict(tuning=(16, 16, 1)),
+               dict(wide_bvh=True, unphased=True), dict(wide_bvh=True, lane_per_ray=True), dict(tuning=(3, 2)),
+               dict(wide_bvh=True, tuning=(8, 6)), dict(tuning=(16, 16, 1)),
                dict(tuning=(16, 16, 2)), dict(tuning=(16, 16, 3))):
         tuning = kw.pop("tuning", None)
         with Context(device=0, **kw) as ctx:
