@@ -99,9 +99,10 @@ struct WaveBuffers {
 // on one ray until it is done (default: lanes take the next queued ray as soon
 // as theirs is finished); kTraceUnphased steps every lane's whole walk each
 // iteration instead of serving leaves, instance entries and ray starts in
-// separate phases. node_quorum: the phased kernels keep stepping nodes while
+// separate phases; kTraceSplitStack keeps the binary walk's split shared/local
+// stack on scenes shallow enough for the shared-memory-only one. node_quorum: the phased kernels keep stepping nodes while
 // this many lanes of a warp do. Grid: sm_count x blocks_per_sm persistent blocks.
-constexpr int kTraceLanePerRay = 1, kTraceUnphased = 2;
+constexpr int kTraceLanePerRay = 1, kTraceUnphased = 2, kTraceSplitStack = 4;
 struct TraceTuning {
     int mode = 0;
     int node_quorum = 16;

@@ -49,6 +49,7 @@ struct DeviceScene {
     float4 tlas_root_lo, tlas_root_hi;
     int wide;                  // 1: walk the wide trees, 0: the binary ones (same results)
     int proper_boxes;          // 1: no node box of any tree is empty (min > max on some axis)
+    int shallow;               // 1: the binary walk's stack never exceeds kShallowStack entries
     // This struct's own copy in device memory. Kernels take the scene by value
     // (parameter space); a non-inlined callee gets this pointer instead of the
     // parameter's address, which would make every thread copy the parameter
@@ -189,6 +190,7 @@ constexpr int kTagTlas = 0, kTagInst = 1, kTagBlas = 2;
 // state stays in registers; the entries live where the stack object says.
 template <class T>
 struct LocalStack {  // all entries in per-thread local memory
+    static constexpr int kCapacity = kTraceStack;
     T *e;
     __device__ __forceinline__ T get(int k) const { return e[k]; }
     __device__ __forceinline__ void set(int k, T v) { e[k] = v; }
@@ -198,6 +200,7 @@ struct LocalStack {  // all entries in per-thread local memory
 // depth-first walks rarely go deep, so the hot entries stay on chip.
 template <class T, int kDepth, int kThreads>
 struct SplitStack {
+    static constexpr int kCapacity = kTraceStack;
     T *col;
     T *deep;
     __device__ __forceinline__ T get(int k) const { return k < kDepth ? col[k * kThreads] : deep[k - kDepth]; }
@@ -207,6 +210,18 @@ struct SplitStack {
         else
             deep[k - kDepth] = v;
     }
+};
+
+// All entries in this thread's shared-memory column, for trees shallow enough
+// that kDepth entries always suffice (checked at upload; a deeper walk stops
+// with a stack error instead of writing past the column).
+constexpr int kShallowStack = 40;
+template <class T, int kDepth, int kThreads>
+struct ColumnStack {
+    static constexpr int kCapacity = kDepth;
+    T *col;
+    __device__ __forceinline__ T get(int k) const { return col[k * kThreads]; }
+    __device__ __forceinline__ void set(int k, T v) { col[k * kThreads] = v; }
 };
 
 // The binary walk as a resumable state machine: start() takes a ray, each
@@ -382,7 +397,7 @@ struct PhasedWalk {
         if (!box_test<kRegular>(blas ? br : wr, lo, hi, ta) || ta > hit.t) return;
         const int left = fbits(lo.w);
         if (left >= 0 || !blas) {
-            if (sp + 2 > kTraceStack) {
+            if (sp + 2 > Stk::kCapacity) {
                 err |= blas ? kErrBlasStack : kErrTlasStack;
                 sp = 0;
                 mode = kModeDone;
@@ -645,7 +660,7 @@ struct PhasedWideWalk {
         if (__int_as_float(e.y) > hit.t) return;  // entry beyond the closest hit so far
         const int tag = e.x & ((1 << kWideTagBits) - 1), pay = e.x >> kWideTagBits;
         if (tag == kWTagBlasNode || tag == kWTagTlasNode) {
-            if (sp + 4 > kWideStack) {
+            if (sp + 4 > Stk::kCapacity) {
                 err |= (tag == kWTagBlasNode) ? kErrBlasStack : kErrTlasStack;
                 sp = 0;
                 mode = kModeDone;
@@ -660,7 +675,7 @@ struct PhasedWideWalk {
             for (int k = 3; k >= 0; --k)
                 if (cs[k] >= 0) stack.set(sp++, make_int2(cs[k], fbits(ts[k])));
         } else if (tag == kWTagTlasLeaf) {
-            if (sp + 2 > kWideStack) {
+            if (sp + 2 > Stk::kCapacity) {
                 err |= kErrTlasStack;
                 sp = 0;
                 mode = kModeDone;

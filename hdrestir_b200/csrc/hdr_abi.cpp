@@ -341,7 +341,8 @@ hdr_status hdr_ctx_create(hdr_ctx **out, const hdr_ctx_desc *desc) {
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
         c->tune.sm_count = sms;
     c->tune.mode = ((c->flags & HDR_CTX_LANE_PER_RAY) ? hdr::kTraceLanePerRay : 0) |
-                   ((c->flags & HDR_CTX_UNPHASED) ? hdr::kTraceUnphased : 0);
+                   ((c->flags & HDR_CTX_UNPHASED) ? hdr::kTraceUnphased : 0) |
+                   ((c->flags & HDR_CTX_SPLIT_STACK) ? hdr::kTraceSplitStack : 0);
     *out = c;
     return HDR_OK;
 }
@@ -466,6 +467,7 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     s.dome_total_lum = f.dome_total_lum;
     s.has_tlas = f.num_instances > 0 ? 1 : 0;
     s.proper_boxes = boxes_proper(f) ? 1 : 0;
+    s.shallow = (f.max_blas_depth + f.max_tlas_depth + 4 <= hdr::kShallowStack) ? 1 : 0;
     // the descriptor itself, for callees that are not inlined into a kernel
     hdr::DeviceScene copies[2] = {s, s};
     {

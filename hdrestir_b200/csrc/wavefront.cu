@@ -179,23 +179,34 @@ struct TraceWalk {
 // entries: the same 12 KB per block as the binary walk's 24 four-byte ones).
 constexpr int kSharedDepthWide = 12;
 
-template <bool kWide, bool kAnyHit>
+// kShallow (binary walk only): the scene's trees fit a kShallowStack-entry
+// stack, which then lives wholly in shared memory (20 KB per block).
+template <bool kWide, bool kAnyHit, bool kShallow>
 struct PhasedTraceWalk {
+    static_assert(!(kWide && kShallow), "the shallow stack serves the binary walk");
     using Entry = typename std::conditional<kWide, int2, int>::type;
-    static constexpr int kShared = kWide ? kSharedDepthWide : kSharedDepth;
-    using Stack = SplitStack<Entry, kShared, kTraceThreads>;
+    static constexpr int kShared = kShallow ? kShallowStack : (kWide ? kSharedDepthWide : kSharedDepth);
+    using Stack = typename std::conditional<kShallow, ColumnStack<Entry, kShared, kTraceThreads>,
+                                            SplitStack<Entry, kShared, kTraceThreads>>::type;
     using type = typename std::conditional<kWide, PhasedWideWalk<kAnyHit, Stack>, PhasedWalk<kAnyHit, Stack>>::type;
 };
 
-template <bool kWide, bool kAnyHit, class Put>
+template <class Stk, class Entry>
+__device__ __forceinline__ void bind_deep(Stk &, Entry *) {}
+template <class Entry, int kDepth, int kThreads>
+__device__ __forceinline__ void bind_deep(SplitStack<Entry, kDepth, kThreads> &st, Entry *deep) {
+    st.deep = deep;
+}
+
+template <bool kWide, bool kShallow, bool kAnyHit, class Put>
 __device__ __forceinline__ void phased_trace(const DeviceScene &s, const float4 *__restrict__ q, int n,
                                              int *fetch_at, int quorum, Put put, unsigned &e) {
-    using PW = PhasedTraceWalk<kWide, kAnyHit>;
+    using PW = PhasedTraceWalk<kWide, kAnyHit, kShallow>;
     __shared__ typename PW::Entry col[PW::kShared * kTraceThreads];
-    typename PW::Entry deep[kTraceStack - PW::kShared];
+    typename PW::Entry deep[kShallow ? 1 : kTraceStack - PW::kShared];
     typename PW::type w;
     w.stack.col = col + threadIdx.x;
-    w.stack.deep = deep;
+    bind_deep(w.stack, deep);
     w.mode = kModeDone;
     NoStats ns;
     int slot = -1;
@@ -237,12 +248,12 @@ constexpr int phased_min_blocks() {
     return kWide ? 6 : 8;
 }
 
-template <bool kWide>
+template <bool kWide, bool kShallow>
 __global__ void __launch_bounds__(kTraceThreads, phased_min_blocks<kWide>()) trace_closest_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
                                                                              int *counts, float4 *hits, float *hit_v,
                                                                              int quorum, unsigned *err) {
     unsigned e = 0;
-    phased_trace<kWide, false>(
+    phased_trace<kWide, kShallow, false>(
         s, q, counts[0], &counts[3], quorum,
         [&](int slot, const auto &w) {
             hits[slot] = make_float4(w.hit.t, __int_as_float(w.hit.inst), __int_as_float(w.hit.tri), w.hit.u);
@@ -252,12 +263,12 @@ __global__ void __launch_bounds__(kTraceThreads, phased_min_blocks<kWide>()) tra
     if (e) atomicOr(err, e);
 }
 
-template <bool kWide>
+template <bool kWide, bool kShallow>
 __global__ void __launch_bounds__(kTraceThreads, phased_min_blocks<kWide>()) trace_shadow_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
                                                                             int *counts, unsigned char *occ, int quorum,
                                                                             unsigned *err) {
     unsigned e = 0;
-    phased_trace<kWide, true>(
+    phased_trace<kWide, kShallow, true>(
         s, q, counts[1], &counts[2], quorum,
         [&](int slot, const auto &w) { occ[slot] = w.shadow_answer() ? 1 : 0; }, e);
     if (e) atomicOr(err, e);
@@ -379,9 +390,12 @@ int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &t
     const int tgrid = tune.sm_count * tune.blocks_per_sm;
     const bool refill = (tune.mode & kTraceLanePerRay) == 0;
     const bool phased = refill && (tune.mode & kTraceUnphased) == 0;
+    const bool shallow = s.shallow && (tune.mode & kTraceSplitStack) == 0;
     if (!mark(ev_begin, 0)) return -1;
     if (phased) {
-        auto closest = s.wide ? trace_closest_phased_kernel<true> : trace_closest_phased_kernel<false>;
+        auto closest = s.wide      ? trace_closest_phased_kernel<true, false>
+                       : shallow   ? trace_closest_phased_kernel<false, true>
+                                   : trace_closest_phased_kernel<false, false>;
         closest<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, tune.node_quorum, err);
     } else {
         auto closest = s.wide ? (refill ? trace_closest_kernel<true, true> : trace_closest_kernel<true, false>)
@@ -390,7 +404,9 @@ int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &t
     }
     if (!mark(ev_end, 0) || !mark(ev_begin, 1)) return -1;
     if (phased) {
-        auto shadow = s.wide ? trace_shadow_phased_kernel<true> : trace_shadow_phased_kernel<false>;
+        auto shadow = s.wide      ? trace_shadow_phased_kernel<true, false>
+                       : shallow   ? trace_shadow_phased_kernel<false, true>
+                                   : trace_shadow_phased_kernel<false, false>;
         shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ, tune.node_quorum, err);
     } else {
         auto shadow = s.wide ? (refill ? trace_shadow_kernel<true, true> : trace_shadow_kernel<true, false>)

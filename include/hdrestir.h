@@ -223,6 +223,9 @@ typedef struct hdr_gbuffer_texel {
 #define HDR_CTX_UNPHASED 16u     /* wavefront trace kernels step each lane's whole walk every
                                     iteration instead of serving leaves, instance entries and ray
                                     starts in their own phases (for A/B timing) */
+#define HDR_CTX_SPLIT_STACK 64u  /* phased binary walk keeps its deeper stack entries in local
+                                    memory even when the scene's trees are shallow enough for a
+                                    shared-memory-only stack; same results (for A/B checks) */
 
 typedef struct hdr_ctx_desc {
     int32_t device;              /* CUDA ordinal */

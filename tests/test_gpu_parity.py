@@ -209,7 +209,7 @@ def test_trace_kernel_forms_give_identical_images():
     from hdrestir_b200.context import Context
     sc, cam = configs.small_variant(2, 160, 96, grid=128, n_spheres=200, n_lights=2000)
     outs = []
-    for kw in ({}, dict(unphased=True), dict(lane_per_ray=True), dict(wide_bvh=True),
+    for kw in ({}, dict(split_stack=True), dict(unphased=True), dict(lane_per_ray=True), dict(wide_bvh=True),
                dict(wide_bvh=True, unphased=True), dict(wide_bvh=True, lane_per_ray=True), dict(tuning=(3, 2)),
                dict(wide_bvh=True, tuning=(8, 6)), dict(tuning=(16, 16, 1)),
                dict(tuning=(16, 16, 2)), dict(tuning=(16, 16, 3))):
