@@ -31,6 +31,7 @@ struct Surface {  // RayIntersection with its ShadingPoint
     Closure c;
     V3 sn;  // shading normal
     bool inside;
+    GgxFixed g;  // GGX terms of (c, sn, -ray_d), shared by every light direction evaluated here
 };
 
 struct Connection {  // BsdfBounceConnection
@@ -106,6 +107,7 @@ __device__ __forceinline__ Surface make_surface(const DeviceScene &s, V3 ro, V3 
     sf.c = c;
     sf.inside = inside;
     sf.sn = inside ? -c.normal : c.normal;
+    sf.g = ggx_fixed(c, sf.sn, -rd);
     return sf;
 }
 
@@ -174,8 +176,8 @@ __device__ inline MisNeePart mis_nee_part(const DeviceScene &s, const Surface &s
     const float p_nee = pdf_to_solid_angle(ls.pdf, ls.pdf_solid_angle, dist2, smaxf(cos_y, 1e-6f));
     if (p_nee <= 0.0f) return r;
     const V3 wo = -sf.ray_d;
-    const float bpdf = ggx_pdf(sf.c, sf.sn, wo, ls.dir);
-    const V3 bval = ggx_eval(sf.c, sf.sn, wo, ls.dir);
+    const float bpdf = ggx_pdf_f(sf.g, sf.sn, wo, ls.dir);
+    const V3 bval = ggx_eval_f(sf.g, sf.sn, wo, ls.dir);
     const Spec radiance = rgb_to_spectrum(bval, sc.up) * rgb_to_spectrum(ls.color, sc.up) * (n_l / p_nee);
     const float w = (delta || !has_conn) ? 1.0f : power_heuristic2(p_nee, bpdf);
     r.cast = true;
@@ -290,8 +292,8 @@ __device__ inline RisContrib ris_evaluate_light_sample(const DeviceScene &s, con
     const float dist2 = ls.dist * ls.dist;
     const float cos_y = smaxf(0.0f, dot(-ls.dir, ls.normal));
     const float p_nee = pdf_to_solid_angle(ls.pdf, ls.pdf_solid_angle, dist2, smaxf(cos_y, 1e-6f));
-    const float p_bsdf = ggx_pdf(sf.c, sf.sn, wo, ls.dir);
-    const V3 bval = ggx_eval(sf.c, sf.sn, wo, ls.dir);
+    const float p_bsdf = ggx_pdf_f(sf.g, sf.sn, wo, ls.dir);
+    const V3 bval = ggx_eval_f(sf.g, sf.sn, wo, ls.dir);
     const bool delta = light_is_delta(s, li);
     RisContrib r{spec(0.0f), spec(0.0f), p_nee, p_bsdf, !delta, true};
     if (n_l <= 0.0f || p_nee <= 0.0f || (cos_y <= 0.0f && !delta)) return r;
@@ -335,7 +337,7 @@ __device__ inline Spec ris_reevaluate(const DeviceScene &s, const Surface &sf, i
     const float cos_y = smaxf(0.0f, dot(-ls.dir, ls.normal));
     const float p_nee = pdf_to_solid_angle(ls.pdf, ls.pdf_solid_angle, dist2, smaxf(cos_y, 1e-6f));
     if (n_l <= 0.0f || p_nee <= 0.0f || (cos_y <= 0.0f && !light_is_delta(s, li))) return spec(0.0f);
-    const V3 bval = ggx_eval(sf.c, sf.sn, wo, ls.dir);
+    const V3 bval = ggx_eval_f(sf.g, sf.sn, wo, ls.dir);
     return rgb_to_spectrum(ls.color, sc.up) * rgb_to_spectrum(bval * n_l, sc.up);
 }
 

@@ -100,6 +100,67 @@ __device__ __forceinline__ float fresnel_dielectric(float cos_i, float ior) {
     return (r_parl * r_parl + r_perp * r_perp) / 2.0f;
 }
 
+// x^5 for the Schlick terms (the reference's std::pow(x, 5.0f)). x*x is exact
+// in double and x^4, x^5 are rounded once each there, so the float result is
+// the correctly rounded x^5 except within ~2^-50 of a rounding boundary.
+HDR_HD float hdr_pow5(float x) {
+    const double xd = (double)x;
+    const double x2 = xd * xd;
+    return (float)(x2 * x2 * xd);
+}
+
+// The terms of GGXBsdf::Eval and ::Pdf (ggx.cpp:20-67) that depend only on the
+// closure, the normal and wo, each with the reference's expression: a surface
+// computes them once and reuses them for every light direction it evaluates.
+struct GgxFixed {
+    float n_v, alpha2, k_g, one_minus_k_g, g_v, reflect_prob, diff_w;
+    V3 F0, one_minus_F0, diff;
+};
+__device__ __forceinline__ GgxFixed ggx_fixed(const Closure &c, V3 n, V3 wo) {
+    GgxFixed g;
+    g.n_v = smaxf(0.001f, dot(n, wo));
+    const float alpha = smaxf(0.001f, c.roughness * c.roughness);
+    g.alpha2 = alpha * alpha;
+    g.k_g = alpha / 2.0f;
+    g.one_minus_k_g = 1.0f - g.k_g;
+    g.g_v = g.n_v / (g.n_v * g.one_minus_k_g + g.k_g);
+    g.F0 = c.specular_color * (1.0f - c.metallic) * 0.04f + c.base_color * c.metallic;
+    g.one_minus_F0 = v3s(1.0f) - g.F0;
+    const V3 fd = c.base_color * (1.0f - c.subsurface) + c.subsurface_color * c.subsurface;
+    g.diff = div_d(fd * (1.0f - c.metallic) * (1.0f - c.transmission), (double)kPiF);
+    float reflect_prob = fresnel_dielectric(g.n_v, c.ior) * c.specular;
+    if (c.metallic > 0.0f) reflect_prob = smaxf(reflect_prob, c.metallic);
+    g.reflect_prob = reflect_prob;
+    g.diff_w = (1.0f - reflect_prob) * (1.0f - c.transmission);
+    return g;
+}
+// GGXBsdf::Eval with the surface's fixed terms
+__device__ __forceinline__ V3 ggx_eval_f(const GgxFixed &g, V3 n, V3 wo, V3 wi) {
+    const V3 h = normalized(wo + wi);
+    const float n_l = smaxf(0.001f, dot(n, wi));
+    const float n_h = smaxf(0.001f, dot(n, h));
+    const float l_h = smaxf(0.001f, dot(wi, h));
+    const float denom = n_h * n_h * (g.alpha2 - 1.0f) + 1.0f;
+    const float D = g.alpha2 / (kPiF * denom * denom);
+    const float g_l = n_l / (n_l * g.one_minus_k_g + g.k_g);
+    const float G = g_l * g.g_v;
+    const V3 F = g.F0 + g.one_minus_F0 * hdr_pow5(1.0f - l_h);
+    const V3 spec = div_d(F * D * G, (double)(4.0f * n_l * g.n_v));
+    return g.diff + spec;
+}
+// GGXBsdf::Pdf with the surface's fixed terms
+__device__ __forceinline__ float ggx_pdf_f(const GgxFixed &g, V3 n, V3 wo, V3 wi) {
+    const V3 h = normalized(wo + wi);
+    const float n_l = smaxf(0.001f, dot(n, wi));
+    const float n_h = smaxf(0.001f, dot(n, h));
+    const float l_h = smaxf(0.001f, dot(wi, h));
+    const float denom = n_h * n_h * (g.alpha2 - 1.0f) + 1.0f;
+    const float D = g.alpha2 / (kPiF * denom * denom);
+    const float diff_pdf = n_l / kPiF;
+    const float spec_pdf = (D * n_h) / (4.0f * l_h);
+    return g.reflect_prob * spec_pdf + g.diff_w * diff_pdf;
+}
+
 // GGXBsdf::Eval (ggx.cpp:20-44)
 __device__ __forceinline__ V3 ggx_eval(const Closure &c, V3 n, V3 wo, V3 wi) {
     const V3 h = normalized(wo + wi);
@@ -116,7 +177,7 @@ __device__ __forceinline__ V3 ggx_eval(const Closure &c, V3 n, V3 wo, V3 wi) {
     const float g_v = n_v / (n_v * (1.0f - k_g) + k_g);
     const float G = g_l * g_v;
     const V3 F0 = c.specular_color * (1.0f - c.metallic) * 0.04f + c.base_color * c.metallic;
-    const V3 F = F0 + (v3s(1.0f) - F0) * HDR_POWF(1.0f - l_h, 5.0f);
+    const V3 F = F0 + (v3s(1.0f) - F0) * hdr_pow5(1.0f - l_h);
     const V3 spec = div_d(F * D * G, (double)(4.0f * n_l * n_v));
     const V3 fd = c.base_color * (1.0f - c.subsurface) + c.subsurface_color * c.subsurface;
     const V3 diff = div_d(fd * (1.0f - c.metallic) * (1.0f - c.transmission), (double)kPiF);
@@ -329,7 +390,7 @@ __device__ inline Bounce sample_bounce(const Closure &c, V3 sn, bool inside, V3 
     // --- sheen (preview_surface.cpp:198-256)
     if (c.sheen > 0.0f && !inside) {
         const float cos_t = smaxf(0.0f, dot(-ray_dir, sn));
-        const float sheen_f = c.sheen * HDR_POWF(1.0f - cos_t, 5.0f);
+        const float sheen_f = c.sheen * hdr_pow5(1.0f - cos_t);
         if (rng.next_float() < sheen_f) {
             if (st.refl >= max_refl) return bounce_error();
             ++st.refl;
