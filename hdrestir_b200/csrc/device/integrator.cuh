@@ -53,8 +53,8 @@ __device__ __forceinline__ bool occluded(const DeviceScene &s, V3 o, V3 d, float
 }
 
 // The same query behind a call: kernels that cast a shadow ray only on a rare
-// path keep the traversal's registers out of their hot loop.
-// occluded() behind a call: bit 0 the answer, the error bits shifted up by one
+// path keep the traversal's registers out of their hot loop. Returns the answer
+// in bit 0 and the error bits shifted up by one.
 __device__ __noinline__ unsigned occluded_call(const DeviceScene *s, V3 o, V3 d, float limit);
 
 // Where the integrators get ray results from. Every ray a pixel casts has a
@@ -64,6 +64,7 @@ __device__ __noinline__ unsigned occluded_call(const DeviceScene *s, V3 o, V3 d,
 // what the wavefront trace kernels wrote for the pixel's slots.
 struct TraceNow {
     const DeviceScene *s;
+    __device__ __forceinline__ bool fresh_bsdf_empty() const { return false; }
     __device__ __forceinline__ bool shadow(int, V3 o, V3 d, float limit, unsigned &err) const {
         return occluded(*s, o, d, limit, err);
     }
@@ -81,6 +82,9 @@ struct TracedResults {
     const float *hit_v;        // and v
     const unsigned char *occ;  // this pixel's shadow slots
     bool bsdf_traced;          // false: BSDF-candidate slots were not cast (their result cannot matter)
+    // Every generated BSDF candidate is invalid whatever it samples: its ray was
+    // not cast because the scene has no light geometry and no environment.
+    __device__ __forceinline__ bool fresh_bsdf_empty() const { return !bsdf_traced; }
     __device__ __forceinline__ bool shadow(int slot, V3, V3, float, unsigned &) const { return occ[slot] != 0; }
     __device__ __forceinline__ bool closest(int slot, V3 o, V3 d, Hit &h, unsigned &) const {
         if (slot > 0 && !bsdf_traced) return false;
@@ -616,6 +620,11 @@ __device__ inline Spec ris_direct_li(const DeviceScene &s, const RP &rp, const S
     x.conn_cand = has_conn && cn.b.pdf > 0.0f;
     const int n_fresh = x.strat.n_bsdf - (x.conn_cand ? 1 : 0);
     x.n_total = x.strat.n_nee + x.strat.n_sky + (x.conn_cand ? 1 : 0) + smaxi(0, n_fresh);
+    // When the generated BSDF candidates (the last ones) are all invalid and the
+    // stream state after generation is known, they are counted as misses and the
+    // stream jumps to that state instead of replaying their samples.
+    const bool skip_fresh = gen_end_state != nullptr && rp.fresh_bsdf_empty();
+    const int n_eval = skip_fresh ? x.n_total - smaxi(0, n_fresh) : x.n_total;
 
     if (run.use_reservoir && primary) {
         // ---- reservoir branch (:267-331)
@@ -632,14 +641,18 @@ __device__ inline Spec ris_direct_li(const DeviceScene &s, const RP &rp, const S
         r.wsum = 0.0f;
         r.m = 0;
         r.w = 0.0f;
-        for (int j = 0; j < x.n_total; ++j) {
+        for (int j = 0; j < n_eval; ++j) {
             const Cand c = ris_candidate<true>(x, j, rng, err);
             if (c.valid)
                 reservoir_update(r, c, (float)c.ris_weight, upd);
             else
                 ++r.m;  // CountMiss
         }
-        if (rng.k != gen_end) err |= kErrRngDesync;
+        if (skip_fresh) {
+            r.m += x.n_total - n_eval;  // CountMiss of each generated BSDF candidate
+        } else if (rng.k != gen_end) {
+            err |= kErrRngDesync;
+        }
         rng = upd;
         // temporal reuse (:284-305)
         Reservoir prev;
@@ -688,11 +701,17 @@ __device__ inline Spec ris_direct_li(const DeviceScene &s, const RP &rp, const S
     const MtStream start = rng;
     double weights[kMaxPlainRisCandidates];
     double wsum = 0.0;
-    for (int j = 0; j < x.n_total; ++j) {
+    for (int j = 0; j < n_eval; ++j) {
         const Cand c = ris_candidate<true>(x, j, rng, err);
         const double w = c.valid ? c.ris_weight : 0.0;
         weights[j] = w;
         if (w > 0.0) wsum += w;
+    }
+    if (skip_fresh) {  // the generated BSDF candidates weigh nothing; the stream continues after them
+        for (int j = n_eval; j < x.n_total; ++j) weights[j] = 0.0;
+        uint64_t *const spill = rng.spill;
+        rng = *gen_end_state;
+        rng.spill = spill;
     }
     if (wsum <= 0.0) return spec(0.0f);
     double remaining = (double)rng.next_float() * wsum;
