@@ -507,4 +507,99 @@ __device__ inline Bounce sample_bounce(const Closure &c, V3 sn, bool inside, V3 
     return r;
 }
 
+// The draws of sample_bounce without the bounce itself, for callers that only
+// need the stream to end where the sampling would have left it. Every branch
+// that decides how many numbers are drawn depends on the surface alone, so a
+// surface computes those quantities once (same expressions as sample_bounce)
+// and each call only draws and compares.
+struct BounceDraws {
+    bool is_default, coat_on, coat_rough, sheen_on, sheen_rough, rough, trans_on, refract_ok;
+    float coat_f, sheen_f, reflect_prob, transmission;
+};
+__device__ __forceinline__ BounceDraws bounce_draws_of(const Closure &c, V3 sn, bool inside, V3 ray_dir,
+                                                       const SpectralCtx &sc) {
+    BounceDraws d;
+    d.is_default = c.is_default;
+    d.coat_on = c.coat > 0.0f && !inside;
+    d.coat_f = d.coat_on ? c.coat * fresnel_dielectric(dot(ray_dir, sn), c.coat_ior) : 0.0f;
+    d.coat_rough = c.coat_roughness > 0.0f;
+    d.sheen_on = c.sheen > 0.0f && !inside;
+    d.sheen_f = d.sheen_on ? c.sheen * hdr_pow5(1.0f - smaxf(0.0f, dot(-ray_dir, sn))) : 0.0f;
+    d.sheen_rough = c.sheen_roughness > 0.0f;
+    float local_ior = c.ior;
+    {
+        const float C = 10000.0f;
+        const float B = local_ior - C / (589.3f * 589.3f);
+        local_ior = B + C / (sc.lambda.l[0] * sc.lambda.l[0]);
+    }
+    float reflect_prob = fresnel_dielectric(dot(ray_dir, sn), local_ior) * c.specular;
+    if (c.metallic > 0.0f) reflect_prob = smaxf(reflect_prob, c.metallic);
+    d.reflect_prob = reflect_prob;
+    d.rough = c.roughness > 0.0f;
+    d.trans_on = c.transmission > 1e-6f;
+    d.transmission = c.transmission;
+    float eta_i = 1.0f, eta_t = local_ior;
+    if (inside) {
+        const float t = eta_i;
+        eta_i = eta_t;
+        eta_t = t;
+    }
+    const float eta = eta_i / eta_t;
+    const float cos_i = dot(ray_dir, sn);
+    d.refract_ok = 1.0f - eta * eta * (1.0f - cos_i * cos_i) >= 0;
+    return d;
+}
+__device__ __forceinline__ void bounce_draws(const BounceDraws &d, int max_refl, int max_refr, BounceState &st,
+                                             MtStream &rng) {
+    if (d.is_default) {
+        (void)rng.next_raw();
+        (void)rng.next_raw();
+        return;
+    }
+    if (d.coat_on && rng.next_float() < d.coat_f) {
+        if (st.refl >= max_refl) return;
+        ++st.refl;
+        if (d.coat_rough) {
+            (void)rng.next_raw();
+            (void)rng.next_raw();
+        }
+        return;
+    }
+    if (d.sheen_on && rng.next_float() < d.sheen_f) {
+        if (st.refl >= max_refl) return;
+        ++st.refl;
+        if (d.sheen_rough) {
+            (void)rng.next_raw();
+            (void)rng.next_raw();
+        }
+        return;
+    }
+    const float rv = rng.next_float();
+    if (rv < d.reflect_prob) {
+        if (st.refl >= max_refl) return;
+        ++st.refl;
+        if (d.rough) {
+            (void)rng.next_raw();
+            (void)rng.next_raw();
+        }
+        return;
+    }
+    const float remaining = (rv - d.reflect_prob) / (1.0f - d.reflect_prob);
+    if (d.trans_on && remaining < d.transmission) {
+        if (d.refract_ok) {
+            if (st.refr >= max_refr) return;
+            ++st.refr;
+            if (d.rough) {
+                (void)rng.next_raw();
+                (void)rng.next_raw();
+            }
+            return;
+        }
+        if (st.refl < max_refl) ++st.refl;
+        return;
+    }
+    (void)rng.next_raw();
+    (void)rng.next_raw();
+}
+
 }  // namespace hdr

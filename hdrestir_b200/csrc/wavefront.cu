@@ -118,6 +118,15 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
     }
     // generated BSDF candidates (:442-450)
     const int n_fresh = n_bsdf - ((fb.ok && fb.pdf > 0.0f) ? 1 : 0);
+    if (!trace_bsdf) {  // their rays are not cast: only the stream has to advance
+        const BounceDraws bd = bounce_draws_of(c, sf.sn, inside, ps.ray.d, ps.sc);
+        for (int k = 0; k < n_fresh; ++k) {
+            BounceState st2{0, 0};
+            bounce_draws(bd, 1, 1, st2, rng);
+        }
+        store_stream(wb.rng_state, i, wb.pixels, rng);
+        return;
+    }
     for (int k = 0; k < n_fresh; ++k) {
         BounceState st2{0, 0};
         const Bounce b = sample_bounce(c, sf.sn, inside, ps.hit.position, ps.ray.d, 1, 1, st2, ps.sc, rng);
