@@ -118,19 +118,25 @@ constexpr int kShadeShapes = 4;
 // caller zeroes counts[2..3] before a rerun); returns the launches, -1 on error.
 int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &tune, unsigned *err, cudaStream_t st,
                       cudaEvent_t *ev_begin = nullptr, cudaEvent_t *ev_end = nullptr);
+// Which closest-hit rays of a pixel the wavefront RIS pass casts (trace_level).
+// Without light geometry and environment no generated BSDF candidate can
+// contribute, and without emissive materials either, neither can the
+// connection candidate (the path's bounce ray): their weights are the same
+// whatever the rays hit, so those rays are not cast.
+constexpr int kTraceNoBsdfRays = 0, kTraceBounceRay = 1, kTraceAllBsdfRays = 2;
 // The three stages of the wavefront RIS pass on their own (a batch of images
 // runs every image's generate, one trace over their shared queues, then every
 // image's shade). Return the launches, -1 on a launch error.
 int launch_ris_generate(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
-                        GBufferView gb, WaveBuffers wb, float4 *color, int trace_bsdf, unsigned *err,
+                        GBufferView gb, WaveBuffers wb, float4 *color, int trace_level, unsigned *err,
                         cudaStream_t st);
 int launch_ris_shade(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
-                     GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf, unsigned *err,
+                     GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_level, unsigned *err,
                      cudaStream_t st, const TraceTuning &tune);
 // ev_begin / ev_end (4 events each, or null): recorded around the generate,
 // trace-closest, trace-shadow and shade launches for per-kernel device times.
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
-                         GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
+                         GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_level,
                          unsigned *err, cudaStream_t st, const TraceTuning &tune, cudaEvent_t *ev_begin = nullptr,
                          cudaEvent_t *ev_end = nullptr);
 

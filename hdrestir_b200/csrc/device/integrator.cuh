@@ -81,13 +81,13 @@ struct TracedResults {
     const float4 *hits;        // this pixel's closest-hit slots: t, instance bits, triangle bits, u
     const float *hit_v;        // and v
     const unsigned char *occ;  // this pixel's shadow slots
-    bool bsdf_traced;          // false: BSDF-candidate slots were not cast (their result cannot matter)
+    int trace_level;           // kTrace*: which closest-hit slots were cast (the others cannot matter)
     // Every generated BSDF candidate is invalid whatever it samples: its ray was
     // not cast because the scene has no light geometry and no environment.
-    __device__ __forceinline__ bool fresh_bsdf_empty() const { return !bsdf_traced; }
+    __device__ __forceinline__ bool fresh_bsdf_empty() const { return trace_level < kTraceAllBsdfRays; }
     __device__ __forceinline__ bool shadow(int slot, V3, V3, float, unsigned &) const { return occ[slot] != 0; }
     __device__ __forceinline__ bool closest(int slot, V3 o, V3 d, Hit &h, unsigned &) const {
-        if (slot > 0 && !bsdf_traced) return false;
+        if (trace_level < (slot > 0 ? kTraceAllBsdfRays : kTraceBounceRay)) return false;
         const float4 r = hits[slot];
         const HitId id{r.x, fbits(r.y), fbits(r.z), r.w, hit_v[slot]};
         if (id.inst < 0) return false;

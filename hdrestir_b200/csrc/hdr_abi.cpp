@@ -101,6 +101,7 @@ struct hdr_ctx {
     bool has_scene = false;
     bool scene_opaque = true;          // every material has opacity >= 0.999 (no stochastic pass-through)
     bool scene_light_geometry = false; // some instance is a light's geometry (GetLightAtHit can succeed)
+    bool scene_emissive = false;       // some material emits
 
     // named frame buffers
     std::map<std::string, DevBuf> buffers;
@@ -396,6 +397,15 @@ bool boxes_proper(const hdr::FlatScene &f) {
 }
 }  // namespace
 
+namespace {
+// Which closest-hit rays the wavefront RIS pass casts (hdr::kTrace*).
+int ris_trace_level(const hdr_ctx *c, const hdr_ris_params *p) {
+    if ((p->flags & HDR_RIS_TRACE_ALL_RAYS) || c->scene_light_geometry || c->scene.env_light >= 0)
+        return hdr::kTraceAllBsdfRays;
+    return c->scene_emissive ? hdr::kTraceBounceRay : hdr::kTraceNoBsdfRays;
+}
+}  // namespace
+
 hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     if (!c || !desc) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);
@@ -501,6 +511,10 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     c->scene_light_geometry = false;
     for (int i = 0; i < desc->num_instances; ++i)
         if (desc->instances[i].light >= 0) c->scene_light_geometry = true;
+    c->scene_emissive = false;
+    for (int i = 0; i < desc->num_materials; ++i)  // the closure's emission, as the scene builder computes it
+        for (int k = 0; k < 3; ++k)
+            if (!(desc->materials[i].emission_color[k] * desc->materials[i].emission == 0.0f)) c->scene_emissive = true;
     return HDR_OK;
 }
 
@@ -601,15 +615,14 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
         wb.rng_state = (uint4 *)q;
         if ((st = ensure_buffer(c, "__wave_done", count, &q)) != HDR_OK) return st;
         wb.done = (unsigned char *)q;
-        const int trace_bsdf =
-            ((p->flags & HDR_RIS_TRACE_ALL_RAYS) || c->scene_light_geometry || c->scene.env_light >= 0) ? 1 : 0;
+        const int trace_level = ris_trace_level(c, p);
         if ((st = begin_pass(c, 1)) != HDR_OK) return st;
         const bool timed = (c->flags & 1u) != 0;
         if (timed)
             for (int k = kSlotWaveFirst; k < kSlotWaveFirst + 4; ++k)
                 if ((st = fold_pass_time(c, k)) != HDR_OK) return st;
         const int n = hdr::launch_ris_wavefront(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color,
-                                                trace_bsdf, c->d_err, c->stream, c->tune,
+                                                trace_level, c->d_err, c->stream, c->tune,
                                                 timed ? c->ev_start + kSlotWaveFirst : nullptr,
                                                 timed ? c->ev_stop + kSlotWaveFirst : nullptr);
         if (n < 0) return fail(HDR_ECUDA, "wavefront launch failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -688,6 +701,7 @@ hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src) {
     dst->scene.dev = dst->scene_store->desc_dev + dst->scene.wide;
     dst->scene_opaque = src->scene_opaque;
     dst->scene_light_geometry = src->scene_light_geometry;
+    dst->scene_emissive = src->scene_emissive;
     dst->has_scene = true;
     dst->have_wave = false;
     return HDR_OK;
@@ -704,7 +718,7 @@ struct RisJob {
     hdr::ReservoirView rv;
     float4 *color;
     int frame;
-    int trace_bsdf;
+    int trace_level;
     size_t count;
     int n_closest, n_shadow;
     uint4 *rng_state;
@@ -754,7 +768,7 @@ hdr_status prepare_ris_job(hdr_ctx *c, const hdr_camera *cam, int32_t frame_inde
     j.rng_state = (uint4 *)q;
     if ((st = ensure_buffer(c, "__wave_done", j.count, &q)) != HDR_OK) return st;
     j.done = (unsigned char *)q;
-    j.trace_bsdf = ((p->flags & HDR_RIS_TRACE_ALL_RAYS) || c->scene_light_geometry || c->scene.env_light >= 0) ? 1 : 0;
+    j.trace_level = ris_trace_level(c, p);
     return HDR_OK;
 }
 
@@ -847,7 +861,7 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
         wb.n_shadow = j.n_shadow;
         wb.slot_base_closest = (int)base_c[(size_t)i];
         wb.slot_base_shadow = (int)base_s[(size_t)i];
-        if (hdr::launch_ris_generate(lead->scene, j.cd, j.frame, j.d, j.gb, wb, j.color, j.trace_bsdf, j.c->d_err,
+        if (hdr::launch_ris_generate(lead->scene, j.cd, j.frame, j.d, j.gb, wb, j.color, j.trace_level, j.c->d_err,
                                      s) < 0)
             return fail(HDR_ECUDA, "generate launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     }
@@ -855,7 +869,7 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
         return fail(HDR_ECUDA, "trace launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     for (int32_t i = 0; i < n; ++i) {
         const RisJob &j = jobs[(size_t)i];
-        if (hdr::launch_ris_shade(lead->scene, j.cd, j.frame, j.d, j.gb, j.rv, wbs[(size_t)i], j.color, j.trace_bsdf,
+        if (hdr::launch_ris_shade(lead->scene, j.cd, j.frame, j.d, j.gb, j.rv, wbs[(size_t)i], j.color, j.trace_level,
                                   j.c->d_err, s, lead->tune) < 0)
             return fail(HDR_ECUDA, "shade launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     }

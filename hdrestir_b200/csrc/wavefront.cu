@@ -66,7 +66,7 @@ __device__ __forceinline__ bool pixel_start(const DeviceScene &s, const CameraD 
 
 __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
                                                            RisRun ris, GBufferView gb, WaveBuffers wb, float4 *color,
-                                                           int trace_bsdf, unsigned *err) {
+                                                           int trace_level, unsigned *err) {
     uint64_t spill[312];
     MtStream rng;
     PixelStart ps;
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
     const Bounce fb = sample_bounce(c, sf.sn, inside, ps.hit.position, ps.ray.d, pr.max_refl, pr.max_refr, st, ps.sc,
                                     rng);
     {
-        const int q = queue_append(&wb.counts[0], fb.ok);
+        const int q = queue_append(&wb.counts[0], fb.ok && trace_level >= kTraceBounceRay);
         if (q >= 0) {
             wb.q_closest[2 * (size_t)q] =
                 make_float4(fb.origin.x, fb.origin.y, fb.origin.z, __int_as_float(wb.slot_base_closest + (int)cbase));
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
     }
     // generated BSDF candidates (:442-450)
     const int n_fresh = n_bsdf - ((fb.ok && fb.pdf > 0.0f) ? 1 : 0);
-    if (!trace_bsdf) {  // their rays are not cast: only the stream has to advance
+    if (trace_level < kTraceAllBsdfRays) {  // their rays are not cast: only the stream has to advance
         const BounceDraws bd = bounce_draws_of(c, sf.sn, inside, ps.ray.d, ps.sc);
         for (int k = 0; k < n_fresh; ++k) {
             BounceState st2{0, 0};
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
     for (int k = 0; k < n_fresh; ++k) {
         BounceState st2{0, 0};
         const Bounce b = sample_bounce(c, sf.sn, inside, ps.hit.position, ps.ray.d, 1, 1, st2, ps.sc, rng);
-        const int q = queue_append(&wb.counts[0], b.ok && trace_bsdf);
+        const int q = queue_append(&wb.counts[0], b.ok);
         if (q >= 0) {
             wb.q_closest[2 * (size_t)q] = make_float4(b.origin.x, b.origin.y, b.origin.z,
                                                       __int_as_float(wb.slot_base_closest + (int)(cbase + 1 + k)));
@@ -371,7 +371,7 @@ template <int kThreads, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) ris_shade_kernel(DeviceScene s, CameraD cam, int frame_index,
                                                                          PathRun pr, RisRun ris, GBufferView gb,
                                                                          ReservoirView rv, WaveBuffers wb, float4 *color,
-                                                                         int trace_bsdf, unsigned *err) {
+                                                                         int trace_level, unsigned *err) {
     uint64_t spill[312];
     MtStream rng;
     PixelStart ps;
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) ris_shade_kernel(DeviceS
     if (wb.done[i]) return;
     unsigned e = 0;
     const TracedResults tr{&s, wb.hits + i * (size_t)wb.n_closest, wb.hit_v + i * (size_t)wb.n_closest,
-                           wb.occ + i * (size_t)wb.n_shadow, trace_bsdf != 0};
+                           wb.occ + i * (size_t)wb.n_shadow, trace_level};
     const MtStream gen_end = load_stream(wb.rng_state, i, wb.pixels);
     // past 311 draws the state lives in local memory only: replay instead
     const MtStream *gen_end_ptr = gen_end.k < 312 ? &gen_end : nullptr;
@@ -448,16 +448,16 @@ RisRun ris_run(const RisParamsD &p) {
 }  // namespace
 
 int launch_ris_generate(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
-                        GBufferView gb, WaveBuffers wb, float4 *color, int trace_bsdf, unsigned *err,
+                        GBufferView gb, WaveBuffers wb, float4 *color, int trace_level, unsigned *err,
                         cudaStream_t st) {
     ris_generate_kernel<<<tile_blocks(cam.width, cam.height), 256, 0, st>>>(s, cam, frame_index, path_run(p),
-                                                                             ris_run(p), gb, wb, color, trace_bsdf,
+                                                                             ris_run(p), gb, wb, color, trace_level,
                                                                              err);
     return cudaGetLastError() == cudaSuccess ? 1 : -1;
 }
 
 int launch_ris_shade(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
-                     GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf, unsigned *err,
+                     GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_level, unsigned *err,
                      cudaStream_t st, const TraceTuning &tune) {
     const PathRun pr = path_run(p);
     const RisRun ris = ris_run(p);
@@ -465,37 +465,37 @@ int launch_ris_shade(const DeviceScene &s, const CameraD &cam, int frame_index, 
     switch (tune.shade_shape) {
         case 1:
             ris_shade_kernel<256, 2><<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color,
-                                                             trace_bsdf, err);
+                                                             trace_level, err);
             break;
         case 2:
             ris_shade_kernel<128, 3><<<tile_blocks<128>(cam.width, cam.height), 128, 0, st>>>(
-                s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_bsdf, err);
+                s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_level, err);
             break;
         case 3:
             ris_shade_kernel<128, 4><<<tile_blocks<128>(cam.width, cam.height), 128, 0, st>>>(
-                s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_bsdf, err);
+                s, cam, frame_index, pr, ris, gb, rv, wb, color, trace_level, err);
             break;
         default:
             ris_shade_kernel<256, 1><<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color,
-                                                             trace_bsdf, err);
+                                                             trace_level, err);
     }
     return cudaGetLastError() == cudaSuccess ? 1 : -1;
 }
 
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
-                         GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_bsdf,
+                         GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_level,
                          unsigned *err, cudaStream_t st, const TraceTuning &tune, cudaEvent_t *ev_begin,
                          cudaEvent_t *ev_end) {
     // [0] closest rays queued, [1] shadow rays queued, [2] / [3] shadow / closest rays handed out
     if (cudaMemsetAsync(wb.counts, 0, 4 * sizeof(int), st) != cudaSuccess) return -1;
     auto mark = [&](cudaEvent_t *ev, int k) { return !ev || cudaEventRecord(ev[k], st) == cudaSuccess; };
     if (!mark(ev_begin, 0)) return -1;
-    if (launch_ris_generate(s, cam, frame_index, p, gb, wb, color, trace_bsdf, err, st) < 0) return -1;
+    if (launch_ris_generate(s, cam, frame_index, p, gb, wb, color, trace_level, err, st) < 0) return -1;
     if (!mark(ev_end, 0)) return -1;
     if (launch_wave_trace(s, wb, tune, err, st, ev_begin ? ev_begin + 1 : nullptr, ev_end ? ev_end + 1 : nullptr) < 0)
         return -1;
     if (!mark(ev_begin, 3)) return -1;
-    if (launch_ris_shade(s, cam, frame_index, p, gb, rv, wb, color, trace_bsdf, err, st, tune) < 0) return -1;
+    if (launch_ris_shade(s, cam, frame_index, p, gb, rv, wb, color, trace_level, err, st, tune) < 0) return -1;
     if (!mark(ev_end, 3)) return -1;
     return 4;
 }

@@ -178,8 +178,9 @@ typedef struct hdr_ris_params {
 } hdr_ris_params;
 
 /* hdr_ris_params.flags. Neither changes the image.
- * TRACE_ALL_RAYS: also cast the rays of generated BSDF candidates in scenes
- *   without light geometry or environment, where their result cannot matter.
+ * TRACE_ALL_RAYS: also cast the rays whose result cannot matter: those of
+ *   generated BSDF candidates in scenes without light geometry or environment,
+ *   and the path's bounce ray when, besides, no material emits.
  * ONE_KERNEL: integrate each pixel in one thread that casts its own rays,
  *   instead of the generate / trace / shade wavefront. */
 enum { HDR_RIS_TRACE_ALL_RAYS = 1, HDR_RIS_ONE_KERNEL = 2 };

@@ -340,10 +340,11 @@ def test_wavefront_path_trace_equals_one_thread_form(case):
     assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
 
 
-def _lobe_scene():
+def _lobe_scene(emissive=False):
     """The config-2 family with spheres of every PreviewSurface lobe: coat and sheen (rough
     and mirror), transmission (refraction and total internal reflection), mirror specular,
-    metal, and DefaultMaterial instances."""
+    metal, and DefaultMaterial instances; `emissive` adds glowing spheres (emissive
+    materials that are no light's geometry)."""
     import dataclasses
     from hdrestir_b200.scene import Material
     sc, cam = configs.small_variant(2, 96, 64, grid=64, n_spheres=80, n_lights=200)
@@ -353,7 +354,7 @@ def _lobe_scene():
         dict(transmission=0.7, ior=1.3, roughness=0.3), dict(transmission=0.9, ior=2.4, roughness=0.0),
         dict(roughness=0.0, specular=0.8), dict(metallic=1.0, roughness=0.15),
         dict(subsurface=0.5, subsurface_color=(0.9, 0.3, 0.2)),
-    ]
+    ] + ([dict(emission=4.0, emission_color=(1.0, 0.6, 0.2))] if emissive else [])
     for k, inst in enumerate(sc.instances[1:]):
         if k % (len(kinds) + 1) == len(kinds):
             inst.material = -1
@@ -362,12 +363,13 @@ def _lobe_scene():
     return sc, cam
 
 
-@pytest.mark.parametrize("use_reservoir", [True, False])
-def test_wavefront_modes_identical_on_every_lobe(gpu_ctx, use_reservoir):
+@pytest.mark.parametrize("use_reservoir,emissive", [(True, False), (False, False), (True, True)])
+def test_wavefront_modes_identical_on_every_lobe(gpu_ctx, use_reservoir, emissive):
     """Where BSDF-candidate rays are not cast, the resampling pass only advances the stream past
-    those candidates (or jumps to the saved end of generation); images stay bit-identical to
-    casting every ray and to the one-kernel form on materials that take every sampling branch."""
-    sc, cam = _lobe_scene()
+    those candidates (or jumps to the saved end of generation), and where nothing emits the
+    path's bounce ray is not cast either; images stay bit-identical to casting every ray and
+    to the one-kernel form on materials that take every sampling branch."""
+    sc, cam = _lobe_scene(emissive)
     gpu_ctx.upload_scene(sc)
     outs = []
     for mode in MODES.values():
