@@ -118,6 +118,11 @@ constexpr int kShadeShapes = 4;
 // caller zeroes counts[2..3] before a rerun); returns the launches, -1 on error.
 int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &tune, unsigned *err, cudaStream_t st,
                       cudaEvent_t *ev_begin = nullptr, cudaEvent_t *ev_end = nullptr);
+// Spatial reuse (extension, spatial.cu): merges up to p.spatial_neighbors
+// neighbours' reservoirs of `in` into `out` and rewrites the colour.
+int launch_ris_spatial(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                       GBufferView gb, ReservoirView in, ReservoirView out, float4 *color, unsigned *err,
+                       cudaStream_t st);
 // Which closest-hit rays of a pixel the wavefront RIS pass casts (trace_level).
 // Without light geometry and environment no generated BSDF candidate can
 // contribute, and without emissive materials either, neither can the

@@ -54,8 +54,13 @@ __device__ __forceinline__ bool occluded(const DeviceScene &s, V3 o, V3 d, float
 
 // The same query behind a call: kernels that cast a shadow ray only on a rare
 // path keep the traversal's registers out of their hot loop. Returns the answer
-// in bit 0 and the error bits shifted up by one.
-__device__ __noinline__ unsigned occluded_call(const DeviceScene *s, V3 o, V3 d, float limit);
+// in bit 0 and the error bits shifted up by one. (Each translation unit gets its
+// own copy: the library is compiled without device linking.)
+__device__ __noinline__ static unsigned occluded_call(const DeviceScene *s, V3 o, V3 d, float limit) {
+    unsigned e = 0;
+    const bool occ = occluded(*s, o, d, limit, e);
+    return (occ ? 1u : 0u) | (e << 1);
+}
 
 // Where the integrators get ray results from. Every ray a pixel casts has a
 // slot: closest-hit slot 0 is the path's bounce ray, closest-hit slot 1 + k

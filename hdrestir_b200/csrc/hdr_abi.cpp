@@ -561,6 +561,14 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
     if (p->candidate_count < 1 || p->candidate_count > 4096)
         return fail(HDR_EINVAL, "candidate_count %d out of range [1, 4096]", p->candidate_count);
     if (p->path.max_depth < 1) return fail(HDR_EINVAL, "max_depth must be >= 1");
+    if (p->spatial_neighbors < 0 || p->spatial_neighbors > 64 || !(p->spatial_radius >= 0.0f))
+        return fail(HDR_EINVAL, "spatial_neighbors %d / spatial_radius out of range ([0, 64], >= 0)",
+                    p->spatial_neighbors);
+    // wavefront form: direct light only (no later bounces) and no stochastic opacity
+    const bool wave = p->path.max_depth == 1 && c->scene_opaque && !(p->flags & HDR_RIS_ONE_KERNEL);
+    const bool spatial = p->spatial_neighbors > 0 && p->use_reservoir;
+    if (spatial && !wave)
+        return fail(HDR_EINVAL, "spatial reuse runs in the wavefront form only (max_depth 1, opaque scene)");
     if ((st = check_cancel(c)) != HDR_OK) return st;
     HDR_CUDA(cudaSetDevice(c->device));
     const size_t count = (size_t)cam->width * cam->height;
@@ -589,8 +597,14 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
     d.spatial_neighbors = p->spatial_neighbors;
     d.spatial_radius = p->spatial_radius;
     const hdr::CameraD cd = make_camera(cam);
-    // wavefront form: direct light only (no later bounces) and no stochastic opacity
-    const bool wave = p->path.max_depth == 1 && c->scene_opaque && !(p->flags & HDR_RIS_ONE_KERNEL);
+    hdr::ReservoirView rv_spatial{};
+    if (spatial) {  // neighbours read this frame's reservoirs while the merged ones are written here
+        void *q;
+        if ((st = ensure_buffer(c, "__ris_reservoir_spatial", count * kResPlanes * sizeof(float4), &q)) != HDR_OK)
+            return st;
+        float4 *r = (float4 *)q;
+        rv_spatial = hdr::ReservoirView{r, r + count, r + 2 * count, r + 3 * count, r + 4 * count};
+    }
     if (wave) {
         const int n_nee = std::max(1, p->candidate_count / 2);
         const int n_bsdf = std::max(0, p->candidate_count - n_nee);
@@ -629,6 +643,14 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
         if (timed)
             for (int k = kSlotWaveFirst; k < kSlotWaveFirst + 4; ++k) c->ev_pending[k] = true;
         c->launches += (uint64_t)n;
+        if (spatial) {
+            if (hdr::launch_ris_spatial(c->scene, cd, frame_index, d, gb, rv, rv_spatial, (float4 *)color, c->d_err,
+                                        c->stream) < 0)
+                return fail(HDR_ECUDA, "spatial reuse launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+            HDR_CUDA(cudaMemcpyAsync(rv.dir_dist, rv_spatial.dir_dist, count * kResPlanes * sizeof(float4),
+                                     cudaMemcpyDeviceToDevice, c->stream));
+            c->launches += 1;
+        }
         c->last_wave = wb;
         c->have_wave = true;
         return end_pass(c, 1);
@@ -785,7 +807,7 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
     for (int32_t i = 0; i < n && together; ++i) {
         hdr_ctx *c = ctxs[i];
         const hdr_ris_params *p = &params[i];
-        together = c->device == ctxs[0]->device && c->has_scene && c->scene_store &&
+        together = p->spatial_neighbors == 0 && c->device == ctxs[0]->device && c->has_scene && c->scene_store &&
                    c->scene_store == ctxs[0]->scene_store && c->scene.wide == ctxs[0]->scene.wide &&
                    p->path.max_depth == 1 && c->scene_opaque && !(p->flags & HDR_RIS_ONE_KERNEL);
     }

@@ -16,13 +16,19 @@
 //              of tracing, and runs the reference's resampling, temporal merge and
 //              colour write-back with the saved stream state supplying the
 //              update numbers.
-// The shade kernel checks that its own stream ends where generate's did.
+// The shade kernel checks that its own stream ends where generate's did
+// whenever it replays every candidate.
 //
 // Rays whose result cannot reach the image are not queued unless the caller
 // asks for them: a generated BSDF candidate contributes only when its ray hits
 // light geometry or escapes to an environment, so a scene with neither makes
-// every such candidate an empty one whatever the ray hits.
+// every such candidate an empty one whatever the ray hits; without emissive
+// materials either, the path's bounce ray cannot change the connection
+// candidate's weight. Generate then only advances the stream past those
+// candidates, and shade counts them as misses and continues from the stream
+// state generate saved.
 #include "device/integrator.cuh"
+#include "device/pixel.cuh"
 
 namespace hdr {
 
@@ -36,32 +42,6 @@ __device__ __forceinline__ int queue_append(int *counter, bool want) {
     if (lane == leader) base = atomicAdd(counter, __popc(mask));
     base = __shfl_sync(mask, base, leader);
     return base + __popc(mask & ((1u << lane) - 1u));
-}
-
-
-// Per-pixel prologue shared by generate and shade: stream, jittered camera
-// ray, wavelengths, GBuffer hit (integration_pass.cpp:210-233).
-struct PixelStart {
-    size_t i;
-    RayF ray;
-    SpectralCtx sc;
-    Hit hit;
-    bool has_hit;
-};
-
-template <int kThreads = 256>
-__device__ __forceinline__ bool pixel_start(const DeviceScene &s, const CameraD &cam, int frame_index,
-                                            const GBufferView &gb, MtStream &rng, uint64_t *spill, PixelStart &ps) {
-    int x, y;
-    if (!tile_pixel<kThreads>(cam.width, cam.height, x, y)) return false;
-    ps.i = (size_t)y * (size_t)cam.width + (size_t)x;
-    rng.init((uint32_t)ps.i ^ (uint32_t)((unsigned long long)frame_index * 12345ULL), spill);
-    const float px = (float)x + rng.next_float();
-    const float py = (float)y + rng.next_float();
-    ps.ray = camera_ray(cam, px, py, rng);
-    ps.sc = make_spectral_ctx(rng.next_float());
-    ps.has_hit = load_gbuffer_hit(s, gb, ps.i, ps.hit);
-    return true;
 }
 
 __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
@@ -140,11 +120,6 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
     store_stream(wb.rng_state, i, wb.pixels, rng);
 }
 
-__device__ __noinline__ unsigned occluded_call(const DeviceScene *s, V3 o, V3 d, float limit) {
-    unsigned e = 0;
-    const bool occ = occluded(*s, o, d, limit, e);
-    return (occ ? 1u : 0u) | (e << 1);
-}
 
 // Trace kernels. Rays of a warp take very different numbers of steps (shadow
 // rays towards random lights: 43 % of lane-steps did work when each lane

@@ -171,8 +171,10 @@ typedef struct hdr_ris_params {
     int32_t use_reservoir;
     int32_t skip_visibility;
     int32_t m_cap;               /* 0 = unbounded CandidateCount (reservoir.h:147-155) */
-    int32_t spatial_neighbors;   /* 0 = temporal-only, same-pixel reuse */
-    float spatial_radius;
+    int32_t spatial_neighbors;   /* 0 = temporal-only, same-pixel reuse; 1..64 = after the temporal
+                                    merge, merge that many random neighbours' reservoirs (spatial
+                                    reuse; wavefront form only: maxDepth 1, opaque scene) */
+    float spatial_radius;        /* neighbour radius in pixels; 0 = 30 */
     uint32_t flags;              /* HDR_RIS_* execution options; 0 = defaults */
     int32_t reserved;
 } hdr_ris_params;

@@ -402,3 +402,44 @@ def test_every_lobe_matches_oracle(gpu_ctx):
         frac = _color_outliers(got, want)
         print(f"every lobe, frame {frame}: outlier fraction {frac:.4f}")
         assert frac <= MAX_OUTLIERS
+
+
+def _mse_vs(img, ref):
+    peak = max(float(ref[:, :3].max()), 1e-12)
+    return float(np.mean(((img[:, :3].astype(np.float64) - ref[:, :3]) / peak) ** 2))
+
+
+def test_spatial_reuse_off_is_identical_and_on_lowers_error():
+    """Spatial reuse (extension): spatial_neighbors = 0 gives the reference's images bit for bit;
+    with 5 neighbours the frames after warm-up are closer to a high-sample image than temporal
+    reuse alone, and the pass rejects the one-kernel form."""
+    from hdrestir_b200.context import Context
+    sc, cam = configs.small_variant(2, 128, 96, grid=96, n_spheres=120, n_lights=1500)
+    ris = dict(candidate_count=32, use_reservoir=True, max_depth=1)
+
+    def run(frames, start=0, accumulate=False, **kw):
+        with Context(device=0) as ctx:
+            ctx.upload_scene(sc)
+            out = []
+            for f in range(start, start + frames):
+                ctx.raycast(cam, f)
+                ctx.ris_path_trace(cam, f, **ris, **kw)
+                if accumulate:
+                    ctx.accumulate(f - start)
+                out.append(ctx.download("Color").astype(np.float64))
+            return out
+
+    plain = run(4)
+    off = run(4, spatial_neighbors=0, spatial_radius=12.0)
+    assert all(np.array_equal(a, b) for a, b in zip(plain, off))
+    high = run(256, start=50_000, accumulate=True)[-1]  # converged image of the same estimator
+    on = run(4, spatial_neighbors=5, spatial_radius=20.0)
+    e_plain = np.mean([_mse_vs(x, high) for x in plain[1:]])
+    e_on = np.mean([_mse_vs(x, high) for x in on[1:]])
+    print(f"per-frame MSE vs converged: temporal only {e_plain:.4e}, + spatial {e_on:.4e}")
+    assert np.isfinite(e_on) and e_on < e_plain
+    with Context(device=0) as ctx:
+        ctx.upload_scene(sc)
+        ctx.raycast(cam, 0)
+        with pytest.raises(abi.HdrError):
+            ctx.ris_path_trace(cam, 0, **ris, spatial_neighbors=4, one_kernel=True)
