@@ -21,6 +21,7 @@ AOV_DEPTH, AOV_ALBEDO, AOV_NORMAL = 1, 2, 4
 ACCUM_PARITY, ACCUM_SHADER = 0, 1
 CTX_TIMINGS, CTX_WIDE_BVH, CTX_LANE_PER_RAY, CTX_UNPHASED, CTX_PT_ONE_KERNEL = 1, 2, 8, 16, 32
 CTX_SPLIT_STACK = 64
+RIS_REPROJECT = 4
 
 _f = C.c_float
 _i = C.c_int32

@@ -19,14 +19,16 @@ BUFFER_LAYOUT = {  # name -> (dtype, trailing shape)
 
 
 def ris_params(candidate_count=16, use_reservoir=True, skip_visibility=False, m_cap=0, trace_all_rays=False,
-               one_kernel=False, spatial_neighbors=0, spatial_radius=0.0, **settings) -> abi.RisParams:
+               one_kernel=False, spatial_neighbors=0, spatial_radius=0.0, reproject=False,
+               **settings) -> abi.RisParams:
     p = abi.RisParams()
     p.path = path_settings(**settings)
     p.candidate_count, p.use_reservoir, p.skip_visibility = int(candidate_count), int(use_reservoir), int(
         skip_visibility)
     p.m_cap = int(m_cap)
     p.spatial_neighbors, p.spatial_radius = int(spatial_neighbors), float(spatial_radius)
-    p.flags = (abi.RIS_TRACE_ALL_RAYS if trace_all_rays else 0) | (abi.RIS_ONE_KERNEL if one_kernel else 0)
+    p.flags = ((abi.RIS_TRACE_ALL_RAYS if trace_all_rays else 0) | (abi.RIS_ONE_KERNEL if one_kernel else 0)
+               | (abi.RIS_REPROJECT if reproject else 0))
     return p
 
 

@@ -44,6 +44,18 @@ constexpr unsigned kResPdfSolidAngle = 1u << 3; // Ls.Pdf.space == SolidAngle
 constexpr unsigned kResOriginShift = 4;         // CandidateOrigin (2 bits)
 constexpr unsigned kResLightShift = 8;          // light index (24 bits)
 
+// Temporal reuse across camera motion (extension, no reference counterpart;
+// the reference's renderer resets its reservoirs when the camera moves). Mode 0
+// is the reference's same-pixel reuse; mode 1 takes the history from where the
+// pixel's hit point was in the previous frame's image; mode 2 has no history.
+struct ReprojD {
+    int mode;
+    int width, height;         // previous frame's image
+    double view[16], proj[16];  // previous frame's camera (GfMatrix4d row-major)
+    const float4 *prev_pos;    // previous frame's GBuffer position.xyz, depth
+    ReservoirView prev;        // previous frame's reservoirs
+};
+
 struct RisParamsD {
     int candidate_count;
     int use_reservoir;
@@ -56,6 +68,7 @@ struct RisParamsD {
     int m_cap;
     int spatial_neighbors;
     float spatial_radius;
+    ReprojD reproj;
 };
 
 // PathTracePassSettings + maxDepth as the integrators read them

@@ -595,8 +595,39 @@ struct RisRun {
     int candidate_count;
     bool use_reservoir;
     bool skip_vis;
-    int m_cap;  // extension: 0 = unbounded (reference)
+    int m_cap;       // extension: 0 = unbounded (reference)
+    ReprojD reproj;  // extension: mode 0 = the reference's same-pixel history
 };
+
+// The previous frame's reservoir for a hit point at p (ReprojD mode 1): the
+// pixel p projected to with the previous camera, if that pixel saw the same
+// surface point (within 2 % of its depth). Its light sample is moved to p
+// (same point on the light, direction and distance from p) and marked
+// untested, so a winner taken from it gets a shadow ray from here.
+__device__ __forceinline__ bool reprojected_history(const ReprojD &rj, V3 p, Reservoir &out) {
+    if (rj.mode != 1) return false;
+    const D3 c = m4d_transform(rj.view, f3_to_d(p));
+    const D3 ndc = m4d_transform(rj.proj, c);
+    if (!(fabs(ndc.x) <= 1.0) || !(fabs(ndc.y) <= 1.0)) return false;
+    const int ix = (int)floor((ndc.x + 1.0) * 0.5 * (double)rj.width);
+    const int iy = (int)floor((ndc.y + 1.0) * 0.5 * (double)rj.height);
+    if (ix < 0 || iy < 0 || ix >= rj.width || iy >= rj.height) return false;
+    const size_t q = (size_t)iy * (size_t)rj.width + (size_t)ix;
+    const float4 pp = rj.prev_pos[q];
+    const V3 prev_p{pp.x, pp.y, pp.z};
+    if (!(pp.w < 3.0e38f) || !(length(prev_p - p) <= 0.02f * pp.w)) return false;
+    reservoir_load(rj.prev, q, out);
+    LightSampleD &ls = out.chosen.ls;
+    if (out.chosen.valid && out.chosen.has_lc && !ls.pdf_solid_angle) {
+        const V3 v = (prev_p + ls.dir * ls.dist) - p;
+        const float dist = length(v);
+        if (!(dist > 0.0f)) return false;
+        ls.dir = v * (1.0f / dist);
+        ls.dist = dist;
+    }
+    out.chosen.vis_tested = false;
+    return true;
+}
 
 // RisDirectLightIntegrator::Li, per-bounce form (:230-361). primary == (callId.id < callId.stride).
 // gen_end: the stream state right after candidate generation when the caller
@@ -661,8 +692,12 @@ __device__ inline Spec ris_direct_li(const DeviceScene &s, const RP &rp, const S
         rng = upd;
         // temporal reuse (:284-305)
         Reservoir prev;
-        reservoir_load(rv, pixel, prev);
-        if (prev.chosen.valid && prev.chosen.has_lc) {
+        bool have_prev = true;
+        if (run.reproj.mode == 0)
+            reservoir_load(rv, pixel, prev);
+        else
+            have_prev = reprojected_history(run.reproj, sf.hit.position, prev);
+        if (have_prev && prev.chosen.valid && prev.chosen.has_lc) {
             const Spec reeval = ris_reevaluate(s, sf, prev.chosen.light, prev.chosen.ls, sc);
             const float phat_curr = spectrum_luminance(reeval, sc.cie);
             const float phat_gen = prev.chosen.target;

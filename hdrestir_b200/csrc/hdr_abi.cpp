@@ -102,6 +102,10 @@ struct hdr_ctx {
     bool scene_opaque = true;          // every material has opacity >= 0.999 (no stochastic pass-through)
     bool scene_light_geometry = false; // some instance is a light's geometry (GetLightAtHit can succeed)
     bool scene_emissive = false;       // some material emits
+    // camera of the last RIS frame with HDR_RIS_REPROJECT (its hit points are in "__prev_pos_depth")
+    bool reproj_valid = false;
+    int reproj_w = 0, reproj_h = 0;
+    double reproj_view[16] = {}, reproj_proj[16] = {};
 
     // named frame buffers
     std::map<std::string, DevBuf> buffers;
@@ -597,6 +601,41 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
     d.spatial_neighbors = p->spatial_neighbors;
     d.spatial_radius = p->spatial_radius;
     const hdr::CameraD cd = make_camera(cam);
+    const bool reproject = (p->flags & HDR_RIS_REPROJECT) && p->use_reservoir;
+    hdr::GBufferView gb_prev{};
+    if (reproject) {  // this frame's temporal history comes from where its hit points were last frame
+        void *q, *pos;
+        if ((st = ensure_buffer(c, "__ris_reservoir_prev", count * kResPlanes * sizeof(float4), &q)) != HDR_OK)
+            return st;
+        if ((st = ensure_buffer(c, "__prev_pos_depth", count * sizeof(float4), &pos)) != HDR_OK) return st;
+        gb_prev.pos_depth = (float4 *)pos;
+        hdr::ReprojD &rj = d.reproj;
+        rj.mode = 2;
+        if (c->reproj_valid && c->reproj_w == cam->width && c->reproj_h == cam->height) {
+            HDR_CUDA(cudaMemcpyAsync(q, rv.dir_dist, count * kResPlanes * sizeof(float4), cudaMemcpyDeviceToDevice,
+                                     c->stream));
+            float4 *r = (float4 *)q;
+            rj.mode = 1;
+            rj.width = c->reproj_w;
+            rj.height = c->reproj_h;
+            std::memcpy(rj.view, c->reproj_view, sizeof(rj.view));
+            std::memcpy(rj.proj, c->reproj_proj, sizeof(rj.proj));
+            rj.prev_pos = gb_prev.pos_depth;
+            rj.prev = hdr::ReservoirView{r, r + count, r + 2 * count, r + 3 * count, r + 4 * count};
+        }
+    }
+    // after the pass: this frame's hit points and camera become the next frame's history
+    auto keep_history = [&]() -> hdr_status {
+        if (!reproject) return HDR_OK;
+        HDR_CUDA(cudaMemcpyAsync(gb_prev.pos_depth, gb.pos_depth, count * sizeof(float4), cudaMemcpyDeviceToDevice,
+                                 c->stream));
+        c->reproj_valid = true;
+        c->reproj_w = cam->width;
+        c->reproj_h = cam->height;
+        std::memcpy(c->reproj_view, cam->view, sizeof(c->reproj_view));
+        std::memcpy(c->reproj_proj, cam->proj, sizeof(c->reproj_proj));
+        return HDR_OK;
+    };
     hdr::ReservoirView rv_spatial{};
     if (spatial) {  // neighbours read this frame's reservoirs while the merged ones are written here
         void *q;
@@ -653,11 +692,13 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
         }
         c->last_wave = wb;
         c->have_wave = true;
+        if ((st = keep_history()) != HDR_OK) return st;
         return end_pass(c, 1);
     }
     if ((st = begin_pass(c, 1)) != HDR_OK) return st;
     hdr::launch_ris_path_trace(c->scene, cd, frame_index, d, gb, rv, (float4 *)color, c->d_err, c->stream);
     c->launches += 1;
+    if ((st = keep_history()) != HDR_OK) return st;
     return end_pass(c, 1);
 }
 
@@ -807,7 +848,7 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
     for (int32_t i = 0; i < n && together; ++i) {
         hdr_ctx *c = ctxs[i];
         const hdr_ris_params *p = &params[i];
-        together = p->spatial_neighbors == 0 && c->device == ctxs[0]->device && c->has_scene && c->scene_store &&
+        together = p->spatial_neighbors == 0 && !(p->flags & HDR_RIS_REPROJECT) && c->device == ctxs[0]->device && c->has_scene && c->scene_store &&
                    c->scene_store == ctxs[0]->scene_store && c->scene.wide == ctxs[0]->scene.wide &&
                    p->path.max_depth == 1 && c->scene_opaque && !(p->flags & HDR_RIS_ONE_KERNEL);
     }
@@ -1078,10 +1119,11 @@ hdr_status hdr_clear_persistent(hdr_ctx *c) {
     if (!c) return fail(HDR_EINVAL, "ctx is NULL");
     std::lock_guard<std::mutex> lock(c->mu);
     HDR_CUDA(cudaSetDevice(c->device));
-    for (const char *name : {"__accum_color", "__ris_reservoir"}) {
+    for (const char *name : {"__accum_color", "__ris_reservoir", "__ris_reservoir_prev", "__prev_pos_depth"}) {
         auto it = c->buffers.find(name);
         if (it != c->buffers.end()) dev_free(c, it->second), c->buffers.erase(it);
     }
+    c->reproj_valid = false;
     return HDR_OK;
 }
 

@@ -84,6 +84,7 @@ void launch_ris_path_trace(const DeviceScene &s, const CameraD &cam, int frame_i
     ris.use_reservoir = p.use_reservoir != 0;
     ris.skip_vis = p.skip_visibility != 0;
     ris.m_cap = p.m_cap;
+    ris.reproj = p.reproj;
     integrate_kernel<true><<<tile_blocks(cam.width, cam.height), 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, res,
                                                                              color, err);
 }

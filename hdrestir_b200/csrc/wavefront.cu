@@ -418,6 +418,7 @@ RisRun ris_run(const RisParamsD &p) {
     ris.use_reservoir = p.use_reservoir != 0;
     ris.skip_vis = p.skip_visibility != 0;
     ris.m_cap = p.m_cap;
+    ris.reproj = p.reproj;
     return ris;
 }
 }  // namespace

@@ -184,8 +184,14 @@ typedef struct hdr_ris_params {
  *   generated BSDF candidates in scenes without light geometry or environment,
  *   and the path's bounce ray when, besides, no material emits.
  * ONE_KERNEL: integrate each pixel in one thread that casts its own rays,
- *   instead of the generate / trace / shade wavefront. */
-enum { HDR_RIS_TRACE_ALL_RAYS = 1, HDR_RIS_ONE_KERNEL = 2 };
+ *   instead of the generate / trace / shade wavefront.
+ * REPROJECT (extension; changes the image, no reference counterpart): for a
+ *   moving camera, take a pixel's temporal history from where its hit point was
+ *   in the previous frame of this ctx (same surface point within 2 % of depth),
+ *   move the history's light sample to the new hit point and test its
+ *   visibility again. Without it the reference's same-pixel history is used
+ *   (the reference's renderer clears the reservoirs when the camera moves). */
+enum { HDR_RIS_TRACE_ALL_RAYS = 1, HDR_RIS_ONE_KERNEL = 2, HDR_RIS_REPROJECT = 4 };
 
 /* AOV selection for hdr_raycast (RaycastPass requestedOutputs, raycast_pass.cpp:39-55) */
 enum { HDR_AOV_DEPTH = 1, HDR_AOV_ALBEDO = 2, HDR_AOV_NORMAL = 4 };

@@ -443,3 +443,37 @@ def test_spatial_reuse_off_is_identical_and_on_lowers_error():
         ctx.raycast(cam, 0)
         with pytest.raises(abi.HdrError):
             ctx.ris_path_trace(cam, 0, **ris, spatial_neighbors=4, one_kernel=True)
+
+
+def test_reprojected_history_lowers_error_on_an_orbit():
+    """Temporal reuse across camera motion (extension): on a slow orbit, history reprojected
+    from the previous frame brings each frame closer to that pose's converged image than
+    starting without history (what the reference's renderer does on a camera change); a
+    static camera with the flag off keeps the reference's images."""
+    from hdrestir_b200.context import Context
+    sc, _ = configs.small_variant(2, 128, 96, grid=96, n_spheres=120, n_lights=1500)
+    cams = [configs.orbit_camera(0.004 * k, 128, 96) for k in range(6)]
+    ris = dict(candidate_count=32, use_reservoir=True, max_depth=1)
+    with Context(device=0) as ctx:
+        ctx.upload_scene(sc)
+        conv = []
+        for k, cam in enumerate(cams):
+            ctx.clear_persistent()
+            for f in range(160):
+                ctx.raycast(cam, 70_000 + 1000 * k + f)
+                ctx.ris_path_trace(cam, 70_000 + 1000 * k + f, **ris)
+                ctx.accumulate(f)
+            conv.append(ctx.download("Color").astype(np.float64))
+        errs = {}
+        for name, kw in (("reset", {}), ("reproject", dict(reproject=True))):
+            ctx.clear_persistent()
+            e = []
+            for k, cam in enumerate(cams):
+                if name == "reset":
+                    ctx.clear_persistent()
+                ctx.raycast(cam, k)
+                ctx.ris_path_trace(cam, k, **ris, **kw)
+                e.append(_mse_vs(ctx.download("Color"), conv[k]))
+            errs[name] = float(np.mean(e[2:]))
+    print(f"per-frame MSE on the orbit: no history {errs['reset']:.4e}, reprojected {errs['reproject']:.4e}")
+    assert np.isfinite(errs["reproject"]) and errs["reproject"] < errs["reset"]
