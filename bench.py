@@ -252,6 +252,37 @@ def batched_leg(ctx, n_images=4, frames=4, warm=2):
     return out
 
 
+def orbit_leg(ctx, frames=8, warm=3):
+    """Config 2's orbit run (extensions): the camera circles the terrain by 0.002 rad per
+    frame; temporal reuse reprojected from the previous frame, M-cap 20, 5 spatial neighbours
+    within 30 px; firefly accumulation restarted at each pose. Device-timed with CUDA events
+    around each frame's passes."""
+    import torch
+    from hdrestir_b200 import configs
+    from hdrestir_b200.context import Context
+    ris = dict(configs.RIS_CONFIG2, m_cap=20, spatial_neighbors=5, spatial_radius=30.0, reproject=True)
+    c = Context(device=torch.cuda.current_device(), timings=False)
+    try:
+        c.share_scene(ctx)
+        ms = []
+        for k in range(warm + frames):
+            cam = configs.orbit_camera(0.002 * k, WIDTH, HEIGHT)
+            c.region_begin(0)
+            c.raycast(cam, k)
+            c.ris_path_trace(cam, k, **ris)
+            c.accumulate(0)
+            c.region_end(0)
+            c.synchronize()
+            if k >= warm:
+                ms.append(c.region_elapsed(0))
+    finally:
+        c.close()
+    avg = sum(ms) / len(ms)
+    return {"frames_per_s": 1000.0 / avg, "ms_per_frame": avg,
+            "workload": f"config 2 orbit at {WIDTH}x{HEIGHT}: reprojected temporal reuse, M-cap 20, "
+                        f"5 spatial neighbours within 30 px, {frames} timed frames"}
+
+
 def config3_leg(reps: int = 2):
     """Config 3: one 3840x2160 frame and 64 frames of 512x512 (orbit views), PathTracer
     maxDepth 16 on the config-2 scene plus a 2048x1024 dome: as 65 PathTracePass launches
@@ -502,6 +533,7 @@ def run_ours(args, rank, local_rank, world):
     }
     if world == 1 and not args.no_serving:
         out["batched"] = batched_leg(ctx)
+        out["orbit"] = orbit_leg(ctx)
         out["serving"] = serving_leg(args.serving_jobs)
         out["config3"] = config3_leg()
     if world == 1 and not args.no_cpu_baseline:
