@@ -22,6 +22,8 @@ ACCUM_PARITY, ACCUM_SHADER = 0, 1
 CTX_TIMINGS, CTX_WIDE_BVH, CTX_LANE_PER_RAY, CTX_UNPHASED, CTX_PT_ONE_KERNEL = 1, 2, 8, 16, 32
 CTX_SPLIT_STACK = 64
 RIS_REPROJECT = 4
+FMT_FLOAT32, FMT_FLOAT16, FMT_UNORM8, FMT_SNORM8, FMT_INT32 = 0, 1, 2, 3, 4
+FMT_DTYPES = {0: np.float32, 1: np.uint16, 2: np.uint8, 3: np.int8, 4: np.int32}
 
 _f = C.c_float
 _i = C.c_int32
@@ -152,6 +154,7 @@ def lib() -> C.CDLL:
             "hdr_accumulate_noalloc": (C.c_int, [vp, vp, i32, i32, i32, i32, i32, vp]),
             "hdr_clear_persistent": (C.c_int, [vp]),
             "hdr_download": (C.c_int, [vp, C.c_char_p, vp, sz]),
+            "hdr_resolve": (C.c_int, [vp, C.c_char_p, i32, i32, i32, vp, sz, i32]),
             "hdr_upload": (C.c_int, [vp, C.c_char_p, vp, sz]),
             "hdr_buffer_size": (C.c_int, [vp, C.c_char_p, C.POINTER(sz)]),
             "hdr_synchronize": (C.c_int, [vp]),

@@ -157,6 +157,22 @@ class Context:
         abi.check(self._lib.hdr_download(self._h, name.encode(), arr.ctypes.data_as(C.c_void_p), nbytes))
         return arr
 
+    def resolve(self, name: str, src_components: int, component_format: int, dst_components: int,
+                device_ptr: int | None = None) -> np.ndarray | None:
+        """The named float frame buffer in a render buffer's format (hdr_resolve): a host array,
+        or written to `device_ptr` (device memory of this ctx's GPU, ordered on the ctx stream)."""
+        pixels = self.buffer_size(name) // (4 * src_components)
+        dt = abi.FMT_DTYPES[component_format]
+        nbytes = pixels * dst_components * np.dtype(dt).itemsize
+        if device_ptr is not None:
+            abi.check(self._lib.hdr_resolve(self._h, name.encode(), int(src_components), int(component_format),
+                                            int(dst_components), C.c_void_p(device_ptr), nbytes, 1))
+            return None
+        out = np.empty((pixels, dst_components), dt)
+        abi.check(self._lib.hdr_resolve(self._h, name.encode(), int(src_components), int(component_format),
+                                        int(dst_components), out.ctypes.data_as(C.c_void_p), nbytes, 0))
+        return out
+
     def upload(self, name: str, arr: np.ndarray) -> None:
         arr = np.ascontiguousarray(arr)
         abi.check(self._lib.hdr_upload(self._h, name.encode(), arr.ctypes.data_as(C.c_void_p), arr.nbytes))

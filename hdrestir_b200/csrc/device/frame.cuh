@@ -136,6 +136,10 @@ int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &t
 int launch_ris_spatial(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                        GBufferView gb, ReservoirView in, ReservoirView out, float4 *color, unsigned *err,
                        cudaStream_t st);
+// Render-buffer conversion (resolve.cu): kResolve* are the HDR_FMT_* values.
+constexpr int kResolveFloat32 = 0, kResolveFloat16 = 1, kResolveUNorm8 = 2, kResolveSNorm8 = 3, kResolveInt32 = 4;
+int launch_resolve(const float *src, int src_comps, int format, int dst_comps, void *dst, size_t pixels,
+                   int sm_count, cudaStream_t st);
 // Which closest-hit rays of a pixel the wavefront RIS pass casts (trace_level).
 // Without light geometry and environment no generated BSDF candidate can
 // contribute, and without emissive materials either, neither can the

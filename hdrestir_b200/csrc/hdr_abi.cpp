@@ -1134,6 +1134,51 @@ hdr_status hdr_buffer_size(hdr_ctx *c, const char *name, size_t *bytes) {
     return HDR_OK;
 }
 
+hdr_status hdr_resolve(hdr_ctx *c, const char *name, int32_t src_components, int32_t component_format,
+                       int32_t dst_components, void *dst, size_t dst_bytes, int32_t dst_on_device) {
+    if (!c || !name || (!dst && dst_bytes)) return fail(HDR_EINVAL, "NULL argument");
+    if (src_components < 1 || src_components > 4 || dst_components < 1 || dst_components > 4)
+        return fail(HDR_EINVAL, "components must be 1..4 (source %d, destination %d)", src_components,
+                    dst_components);
+    static const size_t kSize[] = {4, 2, 1, 1, 4};
+    if (component_format < HDR_FMT_FLOAT32 || component_format > HDR_FMT_INT32)
+        return fail(HDR_EINVAL, "unknown component format %d", component_format);
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaSetDevice(c->device));
+    size_t have = 0;
+    void *src = find_buffer(c, name, &have);
+    if (!src) return fail(HDR_EINVAL, "no buffer named '%s'", name);
+    if (std::strcmp(name, "GBuffer") == 0 || std::strncmp(name, "__", 2) == 0)
+        return fail(HDR_EINVAL, "'%s' is not a float frame buffer", name);
+    const size_t src_px = (size_t)src_components * sizeof(float);
+    if (have % src_px != 0) return fail(HDR_EINVAL, "buffer '%s' (%zu bytes) is not %d floats per pixel", name, have,
+                                        src_components);
+    const size_t pixels = have / src_px;
+    const size_t want = pixels * (size_t)dst_components * kSize[component_format];
+    if (dst_bytes != want)
+        return fail(HDR_EINVAL, "resolve of '%s' writes %zu bytes, %zu given", name, want, dst_bytes);
+    void *out = dst;
+    DevBuf staging;
+    if (!dst_on_device && want) {
+        hdr_status st = dev_alloc(c, staging, want);
+        if (st != HDR_OK) return st;
+        out = staging.ptr;
+    }
+    const int n = hdr::launch_resolve((const float *)src, src_components, component_format, dst_components, out, pixels,
+                                      c->tune.sm_count, c->stream);
+    hdr_status st = HDR_OK;
+    if (n < 0) st = fail(HDR_ECUDA, "resolve launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    c->launches += n > 0 ? (uint64_t)n : 0;
+    if (!dst_on_device && want) {
+        cudaError_t e = cudaSuccess;
+        if (st == HDR_OK) e = cudaMemcpyAsync(dst, out, want, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        dev_free(c, staging);
+        if (st == HDR_OK && e != cudaSuccess) st = fail(HDR_ECUDA, "resolve read-back: %s", cudaGetErrorString(e));
+    }
+    return st;
+}
+
 hdr_status hdr_download(hdr_ctx *c, const char *name, void *dst, size_t bytes) {
     if (!c || !name || (!dst && bytes)) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);

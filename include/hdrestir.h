@@ -374,6 +374,18 @@ hdr_status hdr_clear_persistent(hdr_ctx *ctx);
  * float4: light dir + dist, light colour + pdf, light normal + target
  * function, throughput, then WSum, W, candidate count and flag bits). */
 hdr_status hdr_download(hdr_ctx *ctx, const char *name, void *dst, size_t bytes);
+
+/* Component formats of a Hydra render buffer (HdFormat component types). */
+enum { HDR_FMT_FLOAT32 = 0, HDR_FMT_FLOAT16 = 1, HDR_FMT_UNORM8 = 2, HDR_FMT_SNORM8 = 3, HDR_FMT_INT32 = 4 };
+/* HdRestirRenderBuffer::CopyFromFrameBuffer (hydra/hd_restir_render_buffer.cpp:46-73,113-148)
+ * on the device: the named float frame buffer (src_components floats per pixel: "Color" 4,
+ * "Depth" 1, "Albedo" / "Normal" 3) converted per component as the render buffer's
+ * _WriteOutput does, dst_components components of component_format per pixel (components
+ * the source lacks are 0). dst is device memory on this ctx's GPU when dst_on_device
+ * (ordered on the ctx stream; hdr_synchronize waits for it), else host memory (filled
+ * before the call returns). dst_bytes must be exactly the converted image's size. */
+hdr_status hdr_resolve(hdr_ctx *ctx, const char *name, int32_t src_components, int32_t component_format,
+                       int32_t dst_components, void *dst, size_t dst_bytes, int32_t dst_on_device);
 hdr_status hdr_upload(hdr_ctx *ctx, const char *name, const void *src, size_t bytes);
 hdr_status hdr_buffer_size(hdr_ctx *ctx, const char *name, size_t *bytes);
 
