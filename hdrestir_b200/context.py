@@ -173,6 +173,15 @@ class Context:
                                         int(dst_components), out.ctypes.data_as(C.c_void_p), nbytes, 0))
         return out
 
+    def upscale(self, name: str, components: int, src_w: int, src_h: int, dst_w: int, dst_h: int) -> None:
+        """UpscalePass on the device buffer `name` (hdr_upscale)."""
+        abi.check(self._lib.hdr_upscale(self._h, name.encode(), int(components), int(src_w), int(src_h), int(dst_w),
+                                        int(dst_h)))
+
+    def denoise(self, name: str, width: int, height: int, chromaticity_blur: bool = True) -> None:
+        """Denoiser without OIDN (the chromaticity blur) on the RGBA buffer `name` (hdr_denoise)."""
+        abi.check(self._lib.hdr_denoise(self._h, name.encode(), int(width), int(height), int(chromaticity_blur)))
+
     def upload(self, name: str, arr: np.ndarray) -> None:
         arr = np.ascontiguousarray(arr)
         abi.check(self._lib.hdr_upload(self._h, name.encode(), arr.ctypes.data_as(C.c_void_p), arr.nbytes))

@@ -140,6 +140,11 @@ int launch_ris_spatial(const DeviceScene &s, const CameraD &cam, int frame_index
 constexpr int kResolveFloat32 = 0, kResolveFloat16 = 1, kResolveUNorm8 = 2, kResolveSNorm8 = 3, kResolveInt32 = 4;
 int launch_resolve(const float *src, int src_comps, int format, int dst_comps, void *dst, size_t pixels,
                    int sm_count, cudaStream_t st);
+// Post passes (post.cu): UpscalePass's nearest-pixel upscale and the
+// Denoiser's chromaticity blur.
+int launch_upscale(const float *src, float *dst, int comps, int src_w, int src_h, int dst_w, int dst_h, int sm_count,
+                   cudaStream_t st);
+int launch_chroma_blur(const float4 *src, float4 *dst, int w, int h, int sm_count, cudaStream_t st);
 // Which closest-hit rays of a pixel the wavefront RIS pass casts (trace_level).
 // Without light geometry and environment no generated BSDF candidate can
 // contribute, and without emissive materials either, neither can the

@@ -1179,6 +1179,57 @@ hdr_status hdr_resolve(hdr_ctx *c, const char *name, int32_t src_components, int
     return st;
 }
 
+hdr_status hdr_upscale(hdr_ctx *c, const char *name, int32_t components, int32_t src_w, int32_t src_h,
+                       int32_t dst_w, int32_t dst_h) {
+    if (!c || !name) return fail(HDR_EINVAL, "NULL argument");
+    if (components < 1 || components > 4 || src_w < 1 || src_h < 1 || dst_w < 1 || dst_h < 1 ||
+        (size_t)dst_w * dst_h > ((size_t)1 << 31))
+        return fail(HDR_EINVAL, "bad upscale sizes");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaSetDevice(c->device));
+    auto it = c->buffers.find(name);
+    if (it == c->buffers.end()) return fail(HDR_EINVAL, "no buffer named '%s'", name);
+    const size_t want = (size_t)src_w * src_h * components * sizeof(float);
+    if (it->second.bytes != want)
+        return fail(HDR_EINVAL, "buffer '%s' holds %zu bytes, %d x %d x %d floats expected", name, it->second.bytes,
+                    src_w, src_h, components);
+    DevBuf nb;
+    hdr_status st = dev_alloc(c, nb, (size_t)dst_w * dst_h * components * sizeof(float));
+    if (st != HDR_OK) return st;
+    if (hdr::launch_upscale((const float *)it->second.ptr, (float *)nb.ptr, components, src_w, src_h, dst_w, dst_h,
+                            c->tune.sm_count, c->stream) < 0) {
+        dev_free(c, nb);
+        return fail(HDR_ECUDA, "upscale launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    c->launches += 1;
+    HDR_CUDA(cudaStreamSynchronize(c->stream));  // the source is freed next
+    dev_free(c, it->second);
+    it->second = nb;
+    return HDR_OK;
+}
+
+hdr_status hdr_denoise(hdr_ctx *c, const char *name, int32_t width, int32_t height, int32_t chromaticity_blur) {
+    if (!c || !name) return fail(HDR_EINVAL, "NULL argument");
+    if (width < 0 || height < 0) return fail(HDR_EINVAL, "bad size");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (width == 0 || height == 0 || !chromaticity_blur) return HDR_OK;  // Denoiser::Run: nothing to do
+    HDR_CUDA(cudaSetDevice(c->device));
+    size_t have = 0;
+    void *buf = find_buffer(c, name, &have);
+    if (!buf) return fail(HDR_EINVAL, "no buffer named '%s'", name);
+    const size_t bytes = (size_t)width * height * sizeof(float4);
+    if (have != bytes) return fail(HDR_EINVAL, "buffer '%s' holds %zu bytes, %zu for RGBA %d x %d", name, have, bytes,
+                                   width, height);
+    void *tmp = nullptr;
+    hdr_status st = ensure_buffer(c, "__denoise_scratch", bytes, &tmp);
+    if (st != HDR_OK) return st;
+    if (hdr::launch_chroma_blur((const float4 *)buf, (float4 *)tmp, width, height, c->tune.sm_count, c->stream) < 0)
+        return fail(HDR_ECUDA, "denoise launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    HDR_CUDA(cudaMemcpyAsync(buf, tmp, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    c->launches += 1;
+    return HDR_OK;
+}
+
 hdr_status hdr_download(hdr_ctx *c, const char *name, void *dst, size_t bytes) {
     if (!c || !name || (!dst && bytes)) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);

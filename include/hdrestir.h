@@ -386,6 +386,19 @@ enum { HDR_FMT_FLOAT32 = 0, HDR_FMT_FLOAT16 = 1, HDR_FMT_UNORM8 = 2, HDR_FMT_SNO
  * before the call returns). dst_bytes must be exactly the converted image's size. */
 hdr_status hdr_resolve(hdr_ctx *ctx, const char *name, int32_t src_components, int32_t component_format,
                        int32_t dst_components, void *dst, size_t dst_bytes, int32_t dst_on_device);
+
+/* UpscalePass::_execute (passes/upscale_pass.cpp:13-95) on one named float buffer of this ctx:
+ * its src_w x src_h pixels of `components` floats (the frame's RenderedWidth/Height at its
+ * resolution level) become dst_w x dst_h (the window), each taking the source pixel
+ * (min(src_w - 1, x * src_w / dst_w), min(src_h - 1, y * src_h / dst_h)). The buffer keeps its
+ * name at the new size. */
+hdr_status hdr_upscale(hdr_ctx *ctx, const char *name, int32_t components, int32_t src_w, int32_t src_h,
+                       int32_t dst_w, int32_t dst_h);
+/* Denoiser::Run without OIDN (passes/denoiser.cpp:54-96,164-201) on the named RGBA float buffer
+ * of width x height pixels, in place: with chromaticity_blur, each pixel keeps its luma and takes
+ * the 3x3 mean chroma; alpha is kept. chromaticity_blur = 0 leaves the image as it is, like the
+ * reference without OIDN. */
+hdr_status hdr_denoise(hdr_ctx *ctx, const char *name, int32_t width, int32_t height, int32_t chromaticity_blur);
 hdr_status hdr_upload(hdr_ctx *ctx, const char *name, const void *src, size_t bytes);
 hdr_status hdr_buffer_size(hdr_ctx *ctx, const char *name, size_t *bytes);
 

@@ -19,6 +19,8 @@
 
 #include "../include/hdrestir.h"
 #include "accumulation_pass.h"
+#include "denoiser.h"
+#include "upscale_pass.h"
 #include "path_trace_pass.h"
 #include "pxr/imaging/hio/image.h"
 #include "raycast_pass.h"
@@ -372,6 +374,52 @@ float ref_reservoir_known_answer(float weight, float phat, int candidates_per_fr
     r.Update(S{0, phat}, weight, rng);
     r.Finalize(candidates_per_frame);
     return r.W;
+}
+
+// UpscalePass::_execute on one named buffer ("Color" RGBA, "Albedo" / "Normal"
+// RGB, "Depth" float, as GetOutputDataType types them): src holds the frame at
+// `level` (RenderedWidth x RenderedHeight floats), dst receives window_w x
+// window_h pixels. Returns the components per pixel, or -1.
+int ref_upscale(const char *name, const float *src, int window_w, int window_h, int level, float *dst) {
+    static Scene empty_scene;
+    const GfMatrix4d ident(1.0);
+    Rng rng{0u};
+    RenderContext ctx{
+        .scene = &empty_scene,
+        .viewMatrix = ident,
+        .projMatrix = ident,
+        .frame = CameraFrame{.windowWidth = window_w, .windowHeight = window_h, .resolutionLevel = level,
+                             .visibleMinX = 0, .visibleMinY = 0, .visibleMaxX = window_w, .visibleMaxY = window_h},
+        .frameIndex = 0,
+        .rng = rng,
+        .buffers = FrameBuffersMap{},
+        .OutputNames = {name},
+        .cameraParams = std::nullopt,
+    };
+    int comps = 0;
+    switch (GetOutputDataType(name)) {
+        case OutputDataType::Color4: comps = 4; break;
+        case OutputDataType::Vec3: comps = 3; break;
+        case OutputDataType::Float1: comps = 1; break;
+        default: return -1;
+    }
+    const size_t n_src = ctx.frame.PixelCount();
+    ctx.buffers.Add(name, sizeof(float) * comps, n_src);
+    std::memcpy(ctx.buffers.GetFrameBuffer(name).Data(), src, n_src * comps * sizeof(float));
+    UpscalePass pass{{name}};
+    pass.Execute(ctx);
+    const FrameBuffer &out = ctx.buffers.GetFrameBuffer(name);
+    std::memcpy(dst, out.Data(), out.SizeBytes());
+    return comps;
+}
+
+// Denoiser::Run without OIDN (the chromaticity blur alone, alpha kept) on an
+// RGBA float frame, in place.
+void ref_denoise(float *rgba, int width, int height, int chromaticity_blur) {
+    Denoiser::Config cfg;
+    cfg.EnableChromaticityBlur = chromaticity_blur != 0;
+    Denoiser::Run(gsl::span<pxr::GfVec4f>{reinterpret_cast<pxr::GfVec4f *>(rgba), (size_t)width * (size_t)height},
+                  width, height, cfg);
 }
 
 const char *ref_version(void) { return "hdRestir reference sources compiled in place with the oracle shim"; }

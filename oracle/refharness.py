@@ -70,6 +70,9 @@ def lib() -> C.CDLL:
         L.ref_rng_floats.argtypes = [vp, C.c_int, C.c_int, vp]
         L.ref_reservoir_known_answer.restype = C.c_float
         L.ref_reservoir_known_answer.argtypes = [C.c_float, C.c_float, C.c_int]
+        L.ref_upscale.restype = C.c_int
+        L.ref_upscale.argtypes = [C.c_char_p, vp, C.c_int, C.c_int, C.c_int, vp]
+        L.ref_denoise.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         _lib = L
     return _lib
 
@@ -190,3 +193,21 @@ def cpu_sample(scene, cam, budget_s: float, threads: int, frame: int = 0, ref: "
     if own:
         ref.close()
     return sec, rows
+
+
+def upscale(name: str, src: np.ndarray, window_w: int, window_h: int, level: int) -> np.ndarray:
+    """The reference's UpscalePass on one buffer: src at the level's rendered size -> window size."""
+    comps = {"Color": 4, "Albedo": 3, "Normal": 3, "Depth": 1}[name]
+    src = np.ascontiguousarray(src, np.float32)
+    out = np.empty((window_w * window_h, comps), np.float32)
+    got = lib().ref_upscale(name.encode(), src.ctypes.data_as(C.c_void_p), window_w, window_h, level,
+                            out.ctypes.data_as(C.c_void_p))
+    assert got == comps
+    return out
+
+
+def denoise(rgba: np.ndarray, width: int, height: int, chromaticity_blur: bool = True) -> np.ndarray:
+    """The reference's Denoiser::Run (no OIDN) on an RGBA float image."""
+    img = np.ascontiguousarray(rgba, np.float32).copy()
+    lib().ref_denoise(img.ctypes.data_as(C.c_void_p), width, height, int(chromaticity_blur))
+    return img
