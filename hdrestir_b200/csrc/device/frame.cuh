@@ -121,7 +121,7 @@ struct TraceTuning {
     int node_quorum = 16;
     int blocks_per_sm = 16;
     int sm_count = 148;
-    int shade_shape = 1;  // ris_shade launch shape, 0 .. kShadeShapes - 1
+    int shade_shape = 2;  // ris_shade launch shape, 0 .. kShadeShapes - 1 (128 x 3: fastest at 1080p)
 };
 // ris_shade launch shapes: (threads per block, minimum resident blocks per SM)
 // = (256, 1), (256, 2), (128, 3), (128, 4)

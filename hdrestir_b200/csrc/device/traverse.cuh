@@ -272,7 +272,7 @@ struct BinaryWalk {
             if (!slab_test(blas ? br : wr, lo, hi, ta) || ta > hit.t) return sp > 0;
             const int left = fbits(lo.w);
             if (left >= 0) {
-                if (sp + 2 > kTraceStack) {
+                if (sp + 2 > Stk::kCapacity) {
                     err |= blas ? kErrBlasStack : kErrTlasStack;
                     sp = 0;
                     return false;
@@ -300,7 +300,7 @@ struct BinaryWalk {
                     return false;
                 }
             } else {
-                if (sp + 2 > kTraceStack) {
+                if (sp + 2 > Stk::kCapacity) {
                     err |= kErrTlasStack;
                     sp = 0;
                     return false;
