@@ -155,6 +155,8 @@ def lib() -> C.CDLL:
             "hdr_clear_persistent": (C.c_int, [vp]),
             "hdr_download": (C.c_int, [vp, C.c_char_p, vp, sz]),
             "hdr_resolve": (C.c_int, [vp, C.c_char_p, i32, i32, i32, vp, sz, i32]),
+            "hdr_download_async": (C.c_int, [vp, C.c_char_p, vp, sz]),
+            "hdr_download_wait": (C.c_int, [vp]),
             "hdr_upscale": (C.c_int, [vp, C.c_char_p, i32, i32, i32, i32, i32]),
             "hdr_denoise": (C.c_int, [vp, C.c_char_p, i32, i32, i32]),
             "hdr_upload": (C.c_int, [vp, C.c_char_p, vp, sz]),

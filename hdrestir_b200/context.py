@@ -157,6 +157,16 @@ class Context:
         abi.check(self._lib.hdr_download(self._h, name.encode(), arr.ctypes.data_as(C.c_void_p), nbytes))
         return arr
 
+    def download_async(self, name: str, out: np.ndarray) -> None:
+        """Starts copying `name` into `out` (pinned memory overlaps) while later passes run."""
+        if not out.flags.c_contiguous or out.nbytes != self.buffer_size(name):
+            raise ValueError(f"{name}: need a contiguous array of {self.buffer_size(name)} bytes")
+        abi.check(self._lib.hdr_download_async(self._h, name.encode(), out.ctypes.data_as(C.c_void_p), out.nbytes))
+
+    def download_wait(self) -> None:
+        """Waits for the last download_async."""
+        abi.check(self._lib.hdr_download_wait(self._h))
+
     def resolve(self, name: str, src_components: int, component_format: int, dst_components: int,
                 device_ptr: int | None = None) -> np.ndarray | None:
         """The named float frame buffer in a render buffer's format (hdr_resolve): a host array,

@@ -130,6 +130,10 @@ struct hdr_ctx {
     hdr::WaveBuffers last_wave{};
     bool have_wave = false;
     cudaEvent_t sync_ev = nullptr;  // orders this ctx's stream against a batch's lead stream
+    // hdr_download_async: a snapshot of the buffer on the ctx stream, copied to the host on a
+    // copy stream while the ctx stream goes on (created at the first call)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_ready = nullptr, copy_done = nullptr;
 };
 
 namespace {
@@ -356,6 +360,7 @@ void hdr_ctx_destroy(hdr_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);  // a read-back may still use a buffer
     c->scene_store.reset();
     for (auto &kv : c->buffers) dev_free(c, kv.second);
     if (c->d_err) cudaFree(c->d_err);
@@ -367,6 +372,9 @@ void hdr_ctx_destroy(hdr_ctx *c) {
         for (auto &e : pair)
             if (e) cudaEventDestroy(e);
     if (c->sync_ev) cudaEventDestroy(c->sync_ev);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->copy_ready) cudaEventDestroy(c->copy_ready);
+    if (c->copy_done) cudaEventDestroy(c->copy_done);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -1227,6 +1235,48 @@ hdr_status hdr_denoise(hdr_ctx *c, const char *name, int32_t width, int32_t heig
         return fail(HDR_ECUDA, "denoise launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     HDR_CUDA(cudaMemcpyAsync(buf, tmp, bytes, cudaMemcpyDeviceToDevice, c->stream));
     c->launches += 1;
+    return HDR_OK;
+}
+
+hdr_status hdr_download_async(hdr_ctx *c, const char *name, void *dst, size_t bytes) {
+    if (!c || !name || (!dst && bytes)) return fail(HDR_EINVAL, "NULL argument");
+    if (std::strcmp(name, "GBuffer") == 0) return fail(HDR_EINVAL, "GBuffer is read with hdr_download");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaSetDevice(c->device));
+    size_t have = 0;
+    void *src = find_buffer(c, name, &have);
+    if (!src) return fail(HDR_EINVAL, "no buffer named '%s'", name);
+    if (have != bytes) return fail(HDR_EINVAL, "buffer '%s' holds %zu bytes, %zu requested", name, have, bytes);
+    if (!c->copy_stream) {
+        HDR_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        HDR_CUDA(cudaEventCreateWithFlags(&c->copy_ready, cudaEventDisableTiming));
+        HDR_CUDA(cudaEventCreateWithFlags(&c->copy_done, cudaEventDisableTiming));
+        HDR_CUDA(cudaEventRecord(c->copy_done, c->copy_stream));
+    }
+    if (!bytes) return HDR_OK;
+    size_t staged = 0;
+    if (find_buffer(c, "__download_staging", &staged) && staged != bytes)
+        HDR_CUDA(cudaEventSynchronize(c->copy_done));  // the staging buffer is about to be replaced
+    void *snap = nullptr;
+    hdr_status st = ensure_buffer(c, "__download_staging", bytes, &snap);
+    if (st != HDR_OK) return st;
+    // the previous read-back of the staging buffer ends before the next snapshot overwrites it
+    HDR_CUDA(cudaStreamWaitEvent(c->stream, c->copy_done, 0));
+    HDR_CUDA(cudaMemcpyAsync(snap, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    HDR_CUDA(cudaEventRecord(c->copy_ready, c->stream));
+    HDR_CUDA(cudaStreamWaitEvent(c->copy_stream, c->copy_ready, 0));
+    HDR_CUDA(cudaMemcpyAsync(dst, snap, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
+    HDR_CUDA(cudaEventRecord(c->copy_done, c->copy_stream));
+    return HDR_OK;
+}
+
+hdr_status hdr_download_wait(hdr_ctx *c) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (!c->copy_stream) return HDR_OK;
+    HDR_CUDA(cudaSetDevice(c->device));
+    HDR_CUDA(cudaStreamWaitEvent(c->stream, c->copy_done, 0));  // later work on the ctx stream follows the copy
+    HDR_CUDA(cudaEventSynchronize(c->copy_done));
     return HDR_OK;
 }
 

@@ -374,6 +374,13 @@ hdr_status hdr_clear_persistent(hdr_ctx *ctx);
  * float4: light dir + dist, light colour + pdf, light normal + target
  * function, throughput, then WSum, W, candidate count and flag bits). */
 hdr_status hdr_download(hdr_ctx *ctx, const char *name, void *dst, size_t bytes);
+/* hdr_download without waiting (no reference counterpart): the buffer as the ctx stream has it
+ * now is copied to dst (pinned host memory for the copy to overlap) on a separate copy stream,
+ * while later passes run. dst may be read after hdr_download_wait; a second call first lets the
+ * previous copy finish on the device. Not for "GBuffer". */
+hdr_status hdr_download_async(hdr_ctx *ctx, const char *name, void *dst, size_t bytes);
+/* Waits for the last hdr_download_async; later work on the ctx stream is ordered after it. */
+hdr_status hdr_download_wait(hdr_ctx *ctx);
 
 /* Component formats of a Hydra render buffer (HdFormat component types). */
 enum { HDR_FMT_FLOAT32 = 0, HDR_FMT_FLOAT16 = 1, HDR_FMT_UNORM8 = 2, HDR_FMT_SNORM8 = 3, HDR_FMT_INT32 = 4 };

@@ -477,3 +477,24 @@ def test_reprojected_history_lowers_error_on_an_orbit():
             errs[name] = float(np.mean(e[2:]))
     print(f"per-frame MSE on the orbit: no history {errs['reset']:.4e}, reprojected {errs['reproject']:.4e}")
     assert np.isfinite(errs["reproject"]) and errs["reproject"] < errs["reset"]
+
+
+def test_download_async_equals_download():
+    """The overlapped read-back returns each frame's image as hdr_download does, with later
+    passes running while it copies."""
+    from hdrestir_b200.context import Context
+    sc, cam = _scene(2)
+    with Context(device=0) as ctx:
+        ctx.upload_scene(sc)
+        n = cam.width * cam.height
+        outs, want = [np.empty((n, 4), np.float32) for _ in range(3)], []
+        for f in range(3):
+            ctx.raycast(cam, f)
+            ctx.ris_path_trace(cam, f, candidate_count=32, use_reservoir=True, max_depth=1)
+            ctx.accumulate(f)
+            ctx.download_async("Color", outs[f])
+            ctx.synchronize()
+            want.append(ctx.download("Color").copy())
+        ctx.download_wait()
+        for o, w in zip(outs, want):
+            assert np.array_equal(o.view(np.uint32), w.view(np.uint32))
