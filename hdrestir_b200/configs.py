@@ -249,6 +249,25 @@ def config2(width=1920, height=1080, grid=512, n_spheres=2000, n_lights=10000, o
     return sc, cam
 
 
+def mixed_lights(width=64, height=48, seed=0xC0FFEE05):
+    """The config-1 boxes lit by every analytic light type: rect lights, point lights (some
+    shaped by a cone with soft edges) and distant lights. Test scene for the light models."""
+    sc, cam = config1(width, height, n_lights=12)
+    rng = np.random.default_rng(seed)
+    for k in range(10):
+        pos = (float(rng.uniform(-4, 4)), float(rng.uniform(1.0, 3.5)), float(rng.uniform(-4, 4)))
+        cone = 180.0 if k % 2 == 0 else float(rng.uniform(30.0, 80.0))
+        sc.lights.append(Light(abi.LIGHT_POINT, color=tuple(float(v) for v in rng.uniform(0.3, 1.0, 3)),
+                               intensity=float(rng.uniform(2.0, 20.0)), transform=rect_light_transform(pos, (0, -1, 0)),
+                               shaping_cone_angle=cone, shaping_cone_softness=0.0 if k % 4 == 1 else 0.3))
+    for k in range(3):
+        d = rng.normal(size=3)
+        d[1] = -abs(d[1]) - 0.5
+        sc.lights.append(Light(abi.LIGHT_DISTANT, color=(1.0, 0.95, 0.9), intensity=float(rng.uniform(0.5, 2.0)),
+                               transform=rect_light_transform((0.0, 0.0, 0.0), tuple(d / np.linalg.norm(d)))))
+    return sc, cam
+
+
 def orbit_camera(angle: float, width: int, height: int) -> Camera:
     """Config-2 camera on a circle of radius 22 at height 9 around the terrain centre."""
     eye = (22.0 * np.sin(angle), 9.0, 22.0 * np.cos(angle))

@@ -498,3 +498,32 @@ def test_download_async_equals_download():
         ctx.download_wait()
         for o, w in zip(outs, want):
             assert np.array_equal(o.view(np.uint32), w.view(np.uint32))
+
+
+@pytest.mark.parametrize("kw", [dict(ris=True, candidate_count=16, use_reservoir=True, max_depth=1),
+                                dict(ris=True, candidate_count=16, use_reservoir=False, skip_visibility=True,
+                                     max_depth=1),
+                                dict(ris=False, max_depth=4)])
+def test_point_and_distant_lights_match_oracle(gpu_ctx, kw):
+    """Rect, point (cone-shaped) and distant lights: the GPU passes against the oracle (pinned
+    to the reference on the same scene), reservoir M exactly, colour within the tolerance."""
+    sc, cam = configs.mixed_lights(96, 64)
+    gpu_ctx.upload_scene(sc)
+    gpu_ctx.clear_persistent()
+    orc = Oracle(sc)
+    kw = dict(kw)
+    ris = kw.pop("ris")
+    for frame in range(2):
+        gpu_ctx.raycast(cam, frame)
+        if ris:
+            gpu_ctx.ris_path_trace(cam, frame, **kw)
+        else:
+            gpu_ctx.path_trace(cam, frame, **kw)
+        gpu = gpu_ctx.download("Color")
+        orc.raycast(cam, frame)
+        ref, _ = orc.integrate(cam, frame, ris=ris, **kw)
+        if ris and kw.get("use_reservoir"):
+            assert np.array_equal(gpu_ctx.download("__ris_reservoir")[4, :, 2].view(np.int32), orc.res["m"])
+        frac = _color_outliers(gpu, ref)
+        print(f"mixed lights {kw}, frame {frame}: outlier fraction {frac:.4f}")
+        assert frac <= MAX_OUTLIERS and float(ref[:, :3].mean()) > 0.0

@@ -98,3 +98,23 @@ def test_oracle_equals_reference_with_dome(kw):
         o.accumulate(cam, f, firefly=True)
         assert np.array_equal(bits(o.color), bits(c))
         assert np.array_equal(o.res["m"], r["m"])
+
+
+@pytest.mark.parametrize("kw", [dict(ris=True, candidate_count=8, use_reservoir=True, max_depth=1),
+                                dict(ris=True, candidate_count=8, use_reservoir=False, skip_visibility=True,
+                                     max_depth=1),
+                                dict(ris=False, max_depth=4)])
+def test_oracle_equals_reference_with_point_and_distant_lights(kw):
+    """Rect, point (cone-shaped, soft and hard edges) and distant lights (PointLight,
+    DistantLight: SampleLight, EvalPdf, delta handling in NEE and MIS)."""
+    sc, cam = configs.mixed_lights(40, 30)
+    ref = refharness.Reference(sc)
+    o = orc.Oracle(sc, threads=4)
+    for f in range(2):
+        g, c, r = ref.render(cam, f, accumulate=True, firefly=True, **kw)
+        o.raycast(cam, f)
+        o.integrate(cam, f, **kw)
+        o.accumulate(cam, f, firefly=True)
+        assert np.array_equal(bits(o.color), bits(c))
+        assert np.array_equal(o.res["m"], r["m"])
+        assert float(c[:, :3].mean()) > 0.0
