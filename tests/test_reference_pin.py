@@ -118,3 +118,29 @@ def test_oracle_equals_reference_with_point_and_distant_lights(kw):
         assert np.array_equal(bits(o.color), bits(c))
         assert np.array_equal(o.res["m"], r["m"])
         assert float(c[:, :3].mean()) > 0.0
+
+
+CAMERA_PARAMS = [
+    dict(enable_dof=1, focal_length=50.0, f_stop=1.4, focus_distance=9.0, bokeh_blades=0),
+    dict(enable_dof=1, focal_length=35.0, f_stop=2.0, focus_distance=7.5, bokeh_blades=6),
+    dict(lens_distortion=-0.15),
+    dict(enable_exposure=1, f_stop=4.0, iso=400.0, shutter_speed=0.01),
+]
+
+
+@pytest.mark.parametrize("params", CAMERA_PARAMS)
+def test_oracle_equals_reference_with_camera_params(params):
+    """GenerateCameraRay with thin-lens depth of field (disc and polygonal bokeh), lens
+    distortion, and the exposure multiplier (scene/camera_ray.cpp, camera_params.h)."""
+    from hdrestir_b200.scene import make_camera
+    sc, _ = configs.small_variant(1, 40, 30, n_lights=64)
+    cam = make_camera((0.0, 6.0, 9.0), (0.0, 0.0, 0.0), 40, 30, fov=55.0, params=params)
+    kw = dict(ris=True, candidate_count=8, use_reservoir=True, max_depth=1)
+    ref = refharness.Reference(sc)
+    o = orc.Oracle(sc, threads=4)
+    for f in range(2):
+        g, c, r = ref.render(cam, f, accumulate=True, firefly=True, **kw)
+        assert np.array_equal(o.raycast(cam, f)["prim_id"], g["prim_id"])
+        o.integrate(cam, f, **kw)
+        o.accumulate(cam, f, firefly=True)
+        assert np.array_equal(bits(o.color), bits(c))
