@@ -268,6 +268,21 @@ def mixed_lights(width=64, height=48, seed=0xC0FFEE05):
     return sc, cam
 
 
+def translucent_variant(width=64, height=48):
+    """The config-2 family with see-through and absorbing spheres: partial opacity (stochastic
+    pass-through), transmission with Beer absorption (transmission depth), thin-walled
+    transmission. Test scene for the non-opaque paths."""
+    import dataclasses
+    sc, cam = config2(width, height, grid=64, n_spheres=80, n_lights=200)
+    kinds = [dict(opacity=0.5), dict(opacity=0.2, roughness=0.3),
+             dict(transmission=0.9, ior=1.4, transmission_depth=0.5, transmission_color=(0.9, 0.4, 0.2),
+                  roughness=0.1),
+             dict(transmission=0.8, ior=1.5, thin_walled=True, roughness=0.0)]
+    for k, inst in enumerate(sc.instances[1:]):
+        sc.materials[inst.material] = dataclasses.replace(sc.materials[inst.material], **kinds[k % len(kinds)])
+    return sc, cam
+
+
 def orbit_camera(angle: float, width: int, height: int) -> Camera:
     """Config-2 camera on a circle of radius 22 at height 9 around the terrain centre."""
     eye = (22.0 * np.sin(angle), 9.0, 22.0 * np.cos(angle))

@@ -557,3 +557,32 @@ def test_camera_params_match_oracle(gpu_ctx, params):
         gpu_ctx.ris_path_trace(cam, frame, candidate_count=16, use_reservoir=True, max_depth=1)
         ref, _ = orc.integrate(cam, frame, ris=True, candidate_count=16, use_reservoir=True, max_depth=1)
         assert _color_outliers(gpu_ctx.download("Color"), ref) <= MAX_OUTLIERS
+
+
+
+@pytest.mark.parametrize("kw", [dict(ris=True, candidate_count=16, use_reservoir=True, max_depth=1),
+                                dict(ris=True, candidate_count=16, use_reservoir=True, max_depth=3),
+                                dict(ris=False, max_depth=6)])
+def test_translucent_scene_matches_oracle(gpu_ctx, kw):
+    """Partial opacity, Beer absorption and thin-walled transmission: a scene that is not opaque
+    runs the one-thread forms (rays cast on the spot); against the oracle."""
+    sc, cam = configs.translucent_variant(96, 64)
+    gpu_ctx.upload_scene(sc)
+    gpu_ctx.clear_persistent()
+    orc = Oracle(sc)
+    kw = dict(kw)
+    ris = kw.pop("ris")
+    for frame in range(2):
+        gpu_ctx.raycast(cam, frame)
+        if ris:
+            gpu_ctx.ris_path_trace(cam, frame, **kw)
+        else:
+            gpu_ctx.path_trace(cam, frame, **kw)
+        gpu = gpu_ctx.download("Color")
+        orc.raycast(cam, frame)
+        ref, _ = orc.integrate(cam, frame, ris=ris, **kw)
+        if ris:
+            assert np.array_equal(gpu_ctx.download("__ris_reservoir")[4, :, 2].view(np.int32), orc.res["m"])
+        frac = _color_outliers(gpu, ref)
+        print(f"translucent {kw}, frame {frame}: outlier fraction {frac:.4f}")
+        assert frac <= MAX_OUTLIERS

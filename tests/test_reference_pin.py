@@ -144,3 +144,20 @@ def test_oracle_equals_reference_with_camera_params(params):
         o.integrate(cam, f, **kw)
         o.accumulate(cam, f, firefly=True)
         assert np.array_equal(bits(o.color), bits(c))
+
+
+@pytest.mark.parametrize("kw", [dict(ris=True, candidate_count=8, use_reservoir=True, max_depth=3),
+                                dict(ris=False, max_depth=6)])
+def test_oracle_equals_reference_translucent(kw):
+    """Partial opacity (stochastic skip of a hit), Beer absorption and thin-walled transmission
+    (PathIntegrator::Li opacity loop, BeerAbsorption, PreviewSurface refraction)."""
+    sc, cam = configs.translucent_variant(40, 30)
+    ref = refharness.Reference(sc)
+    o = orc.Oracle(sc, threads=4)
+    for f in range(2):
+        g, c, r = ref.render(cam, f, accumulate=True, firefly=True, **kw)
+        assert np.array_equal(o.raycast(cam, f)["prim_id"], g["prim_id"])
+        o.integrate(cam, f, **kw)
+        o.accumulate(cam, f, firefly=True)
+        assert np.array_equal(bits(o.color), bits(c))
+        assert np.array_equal(o.res["m"], r["m"])
