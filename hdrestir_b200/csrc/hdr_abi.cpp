@@ -1166,11 +1166,9 @@ hdr_status hdr_resolve(hdr_ctx *c, const char *name, int32_t src_components, int
     if (dst_bytes != want)
         return fail(HDR_EINVAL, "resolve of '%s' writes %zu bytes, %zu given", name, want, dst_bytes);
     void *out = dst;
-    DevBuf staging;
-    if (!dst_on_device && want) {
-        hdr_status st = dev_alloc(c, staging, want);
+    if (!dst_on_device && want) {  // converted on the device, then copied out
+        hdr_status st = ensure_buffer(c, "__resolve_staging", want, &out);
         if (st != HDR_OK) return st;
-        out = staging.ptr;
     }
     const int n = hdr::launch_resolve((const float *)src, src_components, component_format, dst_components, out, pixels,
                                       c->tune.sm_count, c->stream);
@@ -1181,7 +1179,6 @@ hdr_status hdr_resolve(hdr_ctx *c, const char *name, int32_t src_components, int
         cudaError_t e = cudaSuccess;
         if (st == HDR_OK) e = cudaMemcpyAsync(dst, out, want, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-        dev_free(c, staging);
         if (st == HDR_OK && e != cudaSuccess) st = fail(HDR_ECUDA, "resolve read-back: %s", cudaGetErrorString(e));
     }
     return st;
