@@ -9,6 +9,7 @@
 //   GpuRISPathTracePass     <- RISPathTracePass  (restir_passes/ris_path_trace_pass.h)
 //   GpuPathTracePass        <- PathTracePass     (passes/path_trace_pass.h)
 //   GpuAccumulationPassB200 <- AccumulationPass / GpuAccumulationPass
+//   GpuUpscalePass          <- UpscalePass       (passes/upscale_pass.h)
 // Frame buffers stay on the device between passes and frames; the last pass
 // copies "Color" into ctx.buffers so the renderer's AOV resolve
 // (renderer.cpp:462-475) finds it where the CPU pipeline leaves it.
@@ -186,6 +187,48 @@ class GpuAccumulationPassB200 final : public RenderPass {
   private:
     std::shared_ptr<DeviceContext> _dev;
     bool _firefly;
+};
+
+// UpscalePass on the device: the named buffers the GPU passes left at the frame's
+// rendered size are upscaled in HBM and handed to ctx.buffers at window size.
+class GpuUpscalePass final : public RenderPass {
+  public:
+    explicit GpuUpscalePass(std::shared_ptr<DeviceContext> dev, std::vector<std::string> outputNames = {})
+        : RenderPass{"UpscalePass"}, _dev{std::move(dev)}, _outputNames{std::move(outputNames)} {}
+    static std::vector<std::string> StaticInputs() {
+        return {std::string{kColorOutputName}, std::string{kDepthOutputName}, std::string{kAlbedoOutputName},
+                std::string{kNormalOutputName}};
+    }
+    static std::vector<std::string> StaticOutputs() { return StaticInputs(); }
+    std::vector<std::string> Inputs() const override { return _outputNames; }
+    std::vector<std::string> Outputs() const override { return _outputNames; }
+
+  protected:
+    void _execute(RenderContext &ctx) override {
+        if (!ctx.frame.NeedsUpscale()) return;
+        const int sw = ctx.frame.RenderedWidth(), sh = ctx.frame.RenderedHeight();
+        const int dw = ctx.frame.windowWidth, dh = ctx.frame.windowHeight;
+        for (const std::string &name : Outputs()) {
+            int comps = 0;
+            switch (GetOutputDataType(name)) {
+                case OutputDataType::Color4: comps = 4; break;
+                case OutputDataType::Vec3: comps = 3; break;
+                case OutputDataType::Float1: comps = 1; break;
+                default: continue;
+            }
+            std::size_t have = 0;
+            if (hdr_buffer_size(_dev->Get(), name.c_str(), &have) != HDR_OK) continue;  // not produced this frame
+            Check(hdr_upscale(_dev->Get(), name.c_str(), comps, sw, sh, dw, dh), "hdr_upscale");
+            ctx.buffers.Add(name, sizeof(float) * comps, (std::size_t)dw * (std::size_t)dh);
+            FrameBuffer &fb = ctx.buffers.GetFrameBuffer(name);
+            Check(hdr_download(_dev->Get(), name.c_str(), fb.Data(), fb.SizeBytes()), "hdr_download");
+        }
+        ctx.frame.MarkUpscaled();
+    }
+
+  private:
+    std::shared_ptr<DeviceContext> _dev;
+    std::vector<std::string> _outputNames;
 };
 
 }  // namespace Restir::B200

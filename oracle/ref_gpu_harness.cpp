@@ -22,6 +22,7 @@ struct ref_gpu_params {
     int32_t pipeline;  // 0 PathTracer, 1 RIS
     int32_t candidate_count, use_reservoir, skip_visibility, max_depth;
     int32_t firefly;
+    int32_t resolution_level;  // > 0: render at ceil(window / 2^level) and end with the upscale pass
 };
 
 extern "C" int refgpu_render(const hdr_scene_desc *desc, const hdr_camera *cam, int frames, const ref_gpu_params *p,
@@ -38,6 +39,8 @@ extern "C" int refgpu_render(const hdr_scene_desc *desc, const hdr_camera *cam, 
         else
             pipe.Add(std::make_unique<B200::GpuPathTracePass>(dev, settings, p->max_depth));
         pipe.Add(std::make_unique<B200::GpuAccumulationPassB200>(dev, p->firefly != 0));
+        if (p->resolution_level > 0)
+            pipe.Add(std::make_unique<B200::GpuUpscalePass>(dev, std::vector<std::string>{"Color"}));
         GfMatrix4d view, proj;
         for (int r = 0; r < 4; ++r)
             for (int c = 0; c < 4; ++c) view[r][c] = cam->view[4 * r + c], proj[r][c] = cam->proj[4 * r + c];
@@ -49,7 +52,8 @@ extern "C" int refgpu_render(const hdr_scene_desc *desc, const hdr_camera *cam, 
                 .scene = &unused_cpu_scene,
                 .viewMatrix = view,
                 .projMatrix = proj,
-                .frame = CameraFrame{.windowWidth = cam->width, .windowHeight = cam->height, .resolutionLevel = 0,
+                .frame = CameraFrame{.windowWidth = cam->width, .windowHeight = cam->height,
+                                     .resolutionLevel = p->resolution_level,
                                      .visibleMinX = 0, .visibleMinY = 0, .visibleMaxX = cam->width,
                                      .visibleMaxY = cam->height},
                 .frameIndex = f,

@@ -136,7 +136,8 @@ GPU_LIB = HERE / "_ref" / "libhdr_ref_gpu.so"
 
 class RefGpuParams(C.Structure):
     _fields_ = [("pipeline", C.c_int32), ("candidate_count", C.c_int32), ("use_reservoir", C.c_int32),
-                ("skip_visibility", C.c_int32), ("max_depth", C.c_int32), ("firefly", C.c_int32)]
+                ("skip_visibility", C.c_int32), ("max_depth", C.c_int32), ("firefly", C.c_int32),
+                ("resolution_level", C.c_int32)]
 
 
 def gpu_pipeline_available() -> bool:
@@ -144,9 +145,10 @@ def gpu_pipeline_available() -> bool:
 
 
 def gpu_pipeline_render(scene, cam, frames, ris=True, candidate_count=16, use_reservoir=True, skip_visibility=False,
-                        max_depth=1, firefly=True) -> np.ndarray:
+                        max_depth=1, firefly=True, resolution_level=0) -> np.ndarray:
     """The reference's RenderPipeline with the GPU passes of
-    hdrestir_b200/integration/gpu_passes.h; returns "Color" after `frames` frames."""
+    hdrestir_b200/integration/gpu_passes.h; returns "Color" after `frames` frames (window size:
+    with resolution_level > 0 the pipeline ends with the GPU upscale pass)."""
     L = C.CDLL(str(GPU_LIB))
     L.refgpu_render.restype = C.c_int
     L.refgpu_render.argtypes = [C.POINTER(abi.SceneDesc), C.POINTER(abi.CameraDesc), C.c_int,
@@ -154,7 +156,7 @@ def gpu_pipeline_render(scene, cam, frames, ris=True, candidate_count=16, use_re
     desc = scene.c_desc()
     out = np.zeros((cam.width * cam.height, 4), np.float32)
     p = RefGpuParams(1 if ris else 0, candidate_count, int(use_reservoir), int(skip_visibility), max_depth,
-                     int(firefly))
+                     int(firefly), int(resolution_level))
     n = L.refgpu_render(C.byref(desc), C.byref(cam.c_desc()), int(frames), C.byref(p), _p(out))
     if n != len(out):
         raise RuntimeError("GPU pipeline render failed")

@@ -29,3 +29,21 @@ def test_reference_pipeline_with_gpu_passes(cfg, kw):
     bad = (np.abs(a - b) > 1e-6 + 1e-4 * np.maximum(np.abs(a), np.abs(b))).any(1).mean()
     print(f"cfg{cfg}: GPU-pass pipeline vs CPU pipeline, outlier fraction {bad:.4f}")
     assert bad <= 0.01
+
+
+def test_reference_pipeline_with_gpu_upscale():
+    """A pipeline rendering at resolution level 1 ends with GpuUpscalePass (UpscalePass on the
+    device); its window-size "Color" is the CPU pipeline's image upscaled by the reference's own
+    UpscalePass."""
+    sc, cam = configs.small_variant(2, 48, 32, grid=96, n_spheres=60, n_lights=300)
+    kw = dict(ris=True, candidate_count=32, use_reservoir=True, max_depth=1)
+    frames, level = 2, 1
+    gpu = refharness.gpu_pipeline_render(sc, cam, frames, resolution_level=level, **kw)
+    ref = refharness.Reference(sc)
+    for f in range(frames):
+        _, cpu, _ = ref.render(cam, f, accumulate=True, firefly=True, resolution_level=level, **kw)
+    want = refharness.upscale("Color", cpu, cam.width, cam.height, level)
+    a, b = gpu[:, :3].astype(np.float64), want[:, :3].astype(np.float64)
+    bad = (np.abs(a - b) > 1e-6 + 1e-4 * np.maximum(np.abs(a), np.abs(b))).any(1).mean()
+    print(f"upscaled GPU-pass pipeline vs CPU pipeline + UpscalePass: outlier fraction {bad:.4f}")
+    assert gpu.shape == (48 * 32, 4) and bad <= 0.01
