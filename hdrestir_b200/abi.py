@@ -153,6 +153,7 @@ def lib() -> C.CDLL:
             "hdr_accumulate": (C.c_int, [vp, i32, i32, i32]),
             "hdr_accumulate_noalloc": (C.c_int, [vp, vp, i32, i32, i32, i32, i32, vp]),
             "hdr_clear_persistent": (C.c_int, [vp]),
+            "hdr_zero_persistent": (C.c_int, [vp]),
             "hdr_download": (C.c_int, [vp, C.c_char_p, vp, sz]),
             "hdr_resolve": (C.c_int, [vp, C.c_char_p, i32, i32, i32, vp, sz, i32]),
             "hdr_download_async": (C.c_int, [vp, C.c_char_p, vp, sz]),

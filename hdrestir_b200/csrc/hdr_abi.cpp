@@ -1135,6 +1135,19 @@ hdr_status hdr_clear_persistent(hdr_ctx *c) {
     return HDR_OK;
 }
 
+hdr_status hdr_zero_persistent(hdr_ctx *c) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_CUDA(cudaSetDevice(c->device));
+    for (const char *name : {"__accum_color", "__ris_reservoir", "__ris_reservoir_prev", "__prev_pos_depth"}) {
+        auto it = c->buffers.find(name);
+        if (it != c->buffers.end() && it->second.bytes)
+            HDR_CUDA(cudaMemsetAsync(it->second.ptr, 0, it->second.bytes, c->stream));
+    }
+    c->reproj_valid = false;
+    return HDR_OK;
+}
+
 hdr_status hdr_buffer_size(hdr_ctx *c, const char *name, size_t *bytes) {
     if (!c || !name || !bytes) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);

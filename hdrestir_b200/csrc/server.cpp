@@ -11,6 +11,10 @@
 //    path-traced jobs on their own streams side by side, then accumulation.
 //    Jobs that arrive while others are running join at the next step
 //    (continuous batching).
+// The context of a job whose result was taken is kept (persistent buffers
+// zeroed in stream order) and given to the next job of the same size, so
+// steady serving allocates and frees nothing: a cudaFree synchronises the whole
+// device and would stall every job in flight.
 // HDR_SERVER_SERIAL runs one job at a time, each frame alone: the plain
 // per-frame pipeline, kept as the baseline the batched form is measured
 // against. A job's images are the same in both modes.
@@ -70,18 +74,61 @@ struct hdr_server {
     std::vector<std::unique_ptr<Job>> active;
     std::map<int64_t, std::unique_ptr<Job>> finished;
     std::vector<int64_t> unreported;  // finished jobs not yet returned by hdr_server_drain_finished
+    // Contexts of released jobs, kept for the next jobs: a released context keeps its stream and
+    // frame buffers, so a job of the same size allocates nothing (a cudaFree would synchronise
+    // the whole device and stall every job in flight). Their bytes count against the budget.
+    struct Pooled {
+        hdr_ctx *ctx;
+        hdr_job_desc d;
+        size_t bytes;
+    };
+    std::vector<Pooled> pool;
+    size_t pooled_bytes = 0;
     int64_t next_id = 1;
     std::mutex mu;
 };
 
 namespace {
 
-// frees an admitted job's context and its share of the budget
-void release(hdr_server *sv, Job &j) {
+// Frame buffers of two jobs have the same sizes when these agree.
+bool same_buffers(const hdr_job_desc &a, const hdr_job_desc &b) {
+    return a.camera.width == b.camera.width && a.camera.height == b.camera.height && a.pipeline == b.pipeline &&
+           (a.pipeline != HDR_JOB_RIS || a.ris.candidate_count == b.ris.candidate_count);
+}
+
+// hands an admitted job's context to the pool (or frees it: pool full, or the job failed)
+void release(hdr_server *sv, Job &j, bool keep = true) {
     if (!j.ctx) return;
-    hdr_ctx_destroy(j.ctx);
-    j.ctx = nullptr;
     sv->in_use -= std::min(sv->in_use, j.bytes);
+    if (keep && j.state == HDR_JOB_DONE && sv->pool.size() < (size_t)sv->max_batch &&
+        hdr_zero_persistent(j.ctx) == HDR_OK) {
+        sv->pool.push_back(hdr_server::Pooled{j.ctx, j.d, j.bytes});
+        sv->pooled_bytes += j.bytes;
+    } else {
+        hdr_ctx_destroy(j.ctx);
+    }
+    j.ctx = nullptr;
+}
+
+// a pooled context whose buffers have job j's sizes (nullptr if none)
+hdr_ctx *take_pooled(hdr_server *sv, const Job &j) {
+    for (size_t k = 0; k < sv->pool.size(); ++k)
+        if (same_buffers(sv->pool[k].d, j.d)) {
+            hdr_ctx *c = sv->pool[k].ctx;
+            sv->pooled_bytes -= std::min(sv->pooled_bytes, sv->pool[k].bytes);
+            sv->pool.erase(sv->pool.begin() + (long)k);
+            return c;
+        }
+    return nullptr;
+}
+
+// frees pooled contexts until `need` more bytes fit the budget (or the pool is empty)
+void shrink_pool(hdr_server *sv, size_t need) {
+    while (!sv->pool.empty() && sv->budget && sv->in_use + sv->pooled_bytes + need > sv->budget) {
+        sv->pooled_bytes -= std::min(sv->pooled_bytes, sv->pool.front().bytes);
+        hdr_ctx_destroy(sv->pool.front().ctx);
+        sv->pool.erase(sv->pool.begin());
+    }
 }
 
 hdr_status admit(hdr_server *sv) {
@@ -90,10 +137,14 @@ hdr_status admit(hdr_server *sv) {
         Job &j = *sv->queued.front();
         if (serial && !sv->active.empty()) break;
         if (sv->budget && !sv->active.empty() && sv->in_use + j.bytes > sv->budget) break;
-        hdr_ctx_desc cd{};
-        cd.device = sv->device;
-        hdr_ctx *c = nullptr;
-        hdr_status st = hdr_ctx_create(&c, &cd);
+        hdr_ctx *c = take_pooled(sv, j);
+        hdr_status st = HDR_OK;
+        if (!c) {  // a new context: pooled ones of other sizes give way when the budget needs it
+            shrink_pool(sv, j.bytes);
+            hdr_ctx_desc cd{};
+            cd.device = sv->device;
+            st = hdr_ctx_create(&c, &cd);
+        }
         if (st == HDR_OK) st = hdr_scene_share(c, sv->scenes[(size_t)j.d.scene]);
         std::unique_ptr<Job> job = std::move(sv->queued.front());
         sv->queued.pop_front();
@@ -115,7 +166,7 @@ hdr_status admit(hdr_server *sv) {
 
 void fail_job(hdr_server *sv, Job &j) {
     j.state = HDR_JOB_FAILED;
-    release(sv, j);
+    release(sv, j, false);
 }
 
 }  // namespace
@@ -138,8 +189,10 @@ hdr_status hdr_server_create(hdr_server **out, const hdr_server_desc *desc) {
 
 void hdr_server_destroy(hdr_server *sv) {
     if (!sv) return;
-    for (auto &j : sv->active) release(sv, *j);
-    for (auto &kv : sv->finished) release(sv, *kv.second);
+    for (auto &j : sv->active) release(sv, *j, false);
+    for (auto &kv : sv->finished) release(sv, *kv.second, false);
+    for (auto &p : sv->pool) hdr_ctx_destroy(p.ctx);
+    sv->pool.clear();
     for (hdr_ctx *c : sv->scenes) hdr_ctx_destroy(c);
     delete sv;
 }

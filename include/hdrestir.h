@@ -408,6 +408,10 @@ hdr_status hdr_upscale(hdr_ctx *ctx, const char *name, int32_t components, int32
 hdr_status hdr_denoise(hdr_ctx *ctx, const char *name, int32_t width, int32_t height, int32_t chromaticity_blur);
 hdr_status hdr_upload(hdr_ctx *ctx, const char *name, const void *src, size_t bytes);
 hdr_status hdr_buffer_size(hdr_ctx *ctx, const char *name, size_t *bytes);
+/* hdr_clear_persistent without giving the memory back (no reference counterpart): the
+ * persistent buffers are zeroed in stream order, which a freshly created buffer also is, so the
+ * next frame starts without history. No device-wide synchronisation (cudaFree has one). */
+hdr_status hdr_zero_persistent(hdr_ctx *ctx);
 
 /* Waits for all work queued on the ctx stream. */
 hdr_status hdr_synchronize(hdr_ctx *ctx);

@@ -104,3 +104,23 @@ def test_server_rejects_bad_jobs():
         with pytest.raises(abi.HdrError) as e:  # above the whole budget
             sv.submit(sid, configs.orbit_camera(0.0, 512, 512), 1, "ris", **RIS)
         assert e.value.status == abi.HDR_ENOMEM
+
+
+@pytest.mark.parametrize("serial", [False, True])
+def test_reused_contexts_give_the_images_of_fresh_ones(serial):
+    """Jobs taken one after another hand their contexts (buffers kept, history zeroed) to the
+    next jobs of the same size; every image equals the job rendered alone."""
+    s2, _, _ = _scenes()
+    jobs = [(configs.orbit_camera(0.3 * k, 64, 48), 2 + (k % 2), "ris", RIS) for k in range(4)]
+    jobs += [(configs.orbit_camera(0.5 * k, 48, 48), 2, "pt", PT) for k in range(2)]
+    with Server(device=0, serial=serial) as sv:
+        sid = sv.add_scene(s2)
+        for cam, fr, pipe, kw in jobs:
+            jid = sv.submit(sid, cam, fr, pipe, **kw)
+            for _ in range(20):
+                if sv.state(jid)[0] == abi.JOB_DONE:
+                    break
+                sv.step()
+            got = sv.take(jid)
+            want = _alone(s2, cam, fr, pipe, kw)
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
