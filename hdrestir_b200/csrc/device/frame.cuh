@@ -105,6 +105,11 @@ struct WaveBuffers {
     // batch of images shares one queue and one result array (0 for one image,
     // whose hits / hit_v / occ then start at its own slot 0)
     int slot_base_closest, slot_base_shadow;
+    // winner visibility queued for the shadow kernel instead of cast on the spot
+    // (nullptr: on the spot): 2 float4 per entry like q_shadow, slot = pixel;
+    // counts[4] entries queued, counts[5] handed out; answers in occ_winner[pixel]
+    float4 *q_winner;
+    unsigned char *occ_winner;
 };
 
 // Returns the number of kernels launched, or -1 on a launch error.

@@ -87,6 +87,9 @@ struct TracedResults {
     const float *hit_v;        // and v
     const unsigned char *occ;  // this pixel's shadow slots
     int trace_level;           // kTrace*: which closest-hit slots were cast (the others cannot matter)
+    float4 *q_winner;          // non-null: the winner's shadow ray is queued (answer fixed up later)
+    int *winner_count;
+    int pixel;
     // Every generated BSDF candidate is invalid whatever it samples: its ray was
     // not cast because the scene has no light geometry and no environment.
     __device__ __forceinline__ bool fresh_bsdf_empty() const { return trace_level < kTraceAllBsdfRays; }
@@ -99,8 +102,17 @@ struct TracedResults {
         h = make_hit(*s, o, d, id);
         return true;
     }
-    // the winner's visibility test of a skipVisibility selection is cast on the spot
+    // The winner's visibility test (skipVisibility, or a sample taken from history): queued for
+    // the shadow kernel and answered "visible" here; a pixel whose ray turns out occluded is
+    // fixed up afterwards (its throughput is then 0, as the test on the spot would have made it).
+    // Without a queue the ray is cast on the spot.
     __device__ __forceinline__ bool winner_shadow(V3 o, V3 d, float limit, unsigned &err) const {
+        if (q_winner) {
+            const int k = atomicAdd(winner_count, 1);
+            q_winner[2 * (size_t)k] = make_float4(o.x, o.y, o.z, __int_as_float(pixel));
+            q_winner[2 * (size_t)k + 1] = make_float4(d.x, d.y, d.z, limit);
+            return false;
+        }
         const unsigned r = occluded_call(s->dev, o, d, limit);
         err |= r >> 1;
         return (r & 1u) != 0;

@@ -664,7 +664,7 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
         wb.q_closest = (float4 *)q;
         if ((st = ensure_buffer(c, "__wave_q_shadow", count * wb.n_shadow * 32, &q)) != HDR_OK) return st;
         wb.q_shadow = (float4 *)q;
-        if ((st = ensure_buffer(c, "__wave_counts", 16, &q)) != HDR_OK) return st;
+        if ((st = ensure_buffer(c, "__wave_counts", 32, &q)) != HDR_OK) return st;
         wb.counts = (int *)q;
         if ((st = ensure_buffer(c, "__wave_hits", count * wb.n_closest * 16, &q)) != HDR_OK) return st;
         wb.hits = (float4 *)q;
@@ -676,6 +676,12 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
         wb.rng_state = (uint4 *)q;
         if ((st = ensure_buffer(c, "__wave_done", count, &q)) != HDR_OK) return st;
         wb.done = (unsigned char *)q;
+        if (p->skip_visibility || reproject) {  // winners whose visibility is still to be tested: one per pixel
+            if ((st = ensure_buffer(c, "__wave_q_winner", count * 32, &q)) != HDR_OK) return st;
+            wb.q_winner = (float4 *)q;
+            if ((st = ensure_buffer(c, "__wave_occ_winner", count, &q)) != HDR_OK) return st;
+            wb.occ_winner = (unsigned char *)q;
+        }
         const int trace_level = ris_trace_level(c, p);
         if ((st = begin_pass(c, 1)) != HDR_OK) return st;
         const bool timed = (c->flags & 1u) != 0;

@@ -249,11 +249,12 @@ __global__ void __launch_bounds__(kTraceThreads, phased_min_blocks<kWide>()) tra
 
 template <bool kWide, bool kShallow>
 __global__ void __launch_bounds__(kTraceThreads, phased_min_blocks<kWide>()) trace_shadow_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
-                                                                            int *counts, unsigned char *occ, int quorum,
+                                                                            const int *count, int *fetch,
+                                                                            unsigned char *occ, int quorum,
                                                                             unsigned *err) {
     unsigned e = 0;
     phased_trace<kWide, kShallow, true>(
-        s, q, counts[1], &counts[2], quorum,
+        s, q, *count, fetch, quorum,
         [&](int slot, const auto &w) { occ[slot] = w.shadow_answer() ? 1 : 0; }, e);
     if (e) atomicOr(err, e);
 }
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) ris_shade_kernel(DeviceS
     if (wb.done[i]) return;
     unsigned e = 0;
     const TracedResults tr{&s, wb.hits + i * (size_t)wb.n_closest, wb.hit_v + i * (size_t)wb.n_closest,
-                           wb.occ + i * (size_t)wb.n_shadow, trace_level};
+                           wb.occ + i * (size_t)wb.n_shadow, trace_level, wb.q_winner, wb.counts + 4, (int)i};
     const MtStream gen_end = load_stream(wb.rng_state, i, wb.pixels);
     // past 311 draws the state lives in local memory only: replay instead
     const MtStream *gen_end_ptr = gen_end.k < 312 ? &gen_end : nullptr;
@@ -391,7 +392,8 @@ int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &t
         auto shadow = s.wide      ? trace_shadow_phased_kernel<true, false>
                        : shallow   ? trace_shadow_phased_kernel<false, true>
                                    : trace_shadow_phased_kernel<false, false>;
-        shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ, tune.node_quorum, err);
+        shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts + 1, wb.counts + 2, wb.occ,
+                                                tune.node_quorum, err);
     } else {
         auto shadow = s.wide ? (refill ? trace_shadow_kernel<true, true> : trace_shadow_kernel<true, false>)
                              : (refill ? trace_shadow_kernel<false, true> : trace_shadow_kernel<false, false>);
@@ -458,12 +460,46 @@ int launch_ris_shade(const DeviceScene &s, const CameraD &cam, int frame_index, 
     return cudaGetLastError() == cudaSuccess ? 1 : -1;
 }
 
+// After the queued winner shadow rays: a pixel whose winner turned out occluded
+// gets what the test on the spot would have given it, throughput 0 (so the
+// direct term is 0) and Color = Beer * emission of its surface.
+__global__ void __launch_bounds__(256) ris_winner_fixup_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
+                                                              GBufferView gb, ReservoirView rv, const float4 *q,
+                                                              const int *count, const unsigned char *occ,
+                                                              float4 *color) {
+    const int n = *count;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int px = __float_as_int(q[2 * (size_t)k].w);
+        if (!occ[px]) continue;
+        const int x = px % cam.width, y = px / cam.width;
+        MtStream rng;
+        rng.init((uint32_t)px ^ (uint32_t)((unsigned long long)frame_index * 12345ULL), nullptr);
+        const float fx = (float)x + rng.next_float();
+        const float fy = (float)y + rng.next_float();
+        const RayF ray = camera_ray(cam, fx, fy, rng);
+        const SpectralCtx sc = make_spectral_ctx(rng.next_float());
+        Hit h;
+        if (!load_gbuffer_hit(s, gb, (size_t)px, h)) continue;
+        Closure c = get_closure(s, h);
+        if (!pr.enable_subsurface) c.subsurface = 0.0f;
+        const bool inside = dot(c.normal, ray.d) > 0.0f;
+        Spec tp = spec(1.0f);
+        beer_absorption(tp, c, h.depth, inside, sc);
+        if (rv.throughput) rv.throughput[px] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const Spec L = tp * (rgb_to_spectrum(c.emission, sc.up) + spec(0.0f));
+        V3 rgb = spectrum_to_rgb(L, sc.cie);
+        if (cam.p.has_params && cam.p.enable_exposure) rgb = rgb * cam.p.exposure_mult;
+        color[px] = make_float4(rgb.x, rgb.y, rgb.z, 1.0f);
+    }
+}
+
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                          GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_level,
                          unsigned *err, cudaStream_t st, const TraceTuning &tune, cudaEvent_t *ev_begin,
                          cudaEvent_t *ev_end) {
-    // [0] closest rays queued, [1] shadow rays queued, [2] / [3] shadow / closest rays handed out
-    if (cudaMemsetAsync(wb.counts, 0, 4 * sizeof(int), st) != cudaSuccess) return -1;
+    // [0] closest rays queued, [1] shadow rays queued, [2] / [3] shadow / closest rays handed out,
+    // [4] / [5] winner shadow rays queued / handed out
+    if (cudaMemsetAsync(wb.counts, 0, (wb.q_winner ? 6 : 4) * sizeof(int), st) != cudaSuccess) return -1;
     auto mark = [&](cudaEvent_t *ev, int k) { return !ev || cudaEventRecord(ev[k], st) == cudaSuccess; };
     if (!mark(ev_begin, 0)) return -1;
     if (launch_ris_generate(s, cam, frame_index, p, gb, wb, color, trace_level, err, st) < 0) return -1;
@@ -472,8 +508,21 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
         return -1;
     if (!mark(ev_begin, 3)) return -1;
     if (launch_ris_shade(s, cam, frame_index, p, gb, rv, wb, color, trace_level, err, st, tune) < 0) return -1;
+    int launches = 4;
+    if (wb.q_winner) {  // the winners' shadow rays, then the pixels they found occluded
+        const int tgrid = tune.sm_count * tune.blocks_per_sm;
+        const bool shallow = s.shallow && (tune.mode & kTraceSplitStack) == 0;
+        auto shadow = s.wide ? trace_shadow_phased_kernel<true, false>
+                             : (shallow ? trace_shadow_phased_kernel<false, true> : trace_shadow_phased_kernel<false, false>);
+        shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_winner, wb.counts + 4, wb.counts + 5, wb.occ_winner,
+                                                tune.node_quorum, err);
+        ris_winner_fixup_kernel<<<tune.sm_count * 4, 256, 0, st>>>(s, cam, frame_index, path_run(p), gb, rv, wb.q_winner,
+                                                                   wb.counts + 4, wb.occ_winner, color);
+        if (cudaGetLastError() != cudaSuccess) return -1;
+        launches += 2;
+    }
     if (!mark(ev_end, 3)) return -1;
-    return 4;
+    return launches;
 }
 
 }  // namespace hdr

@@ -586,3 +586,27 @@ def test_translucent_scene_matches_oracle(gpu_ctx, kw):
         frac = _color_outliers(gpu, ref)
         print(f"translucent {kw}, frame {frame}: outlier fraction {frac:.4f}")
         assert frac <= MAX_OUTLIERS
+
+
+@pytest.mark.parametrize("kw", [dict(use_reservoir=False, skip_visibility=True),
+                                dict(use_reservoir=True, skip_visibility=True),
+                                dict(use_reservoir=True, skip_visibility=False, reproject=True)])
+def test_queued_winner_visibility_equals_on_the_spot(kw):
+    """Winners whose visibility is still untested (skipVisibility, or taken from reprojected
+    history) have their shadow rays traced by the shadow kernel in the wavefront form and cast on
+    the spot in the one-kernel form; the frames of an orbit are bit-identical."""
+    from hdrestir_b200.context import Context
+    sc, _ = configs.small_variant(1, 96, 64, n_lights=256)
+    outs = []
+    for mode in ({}, dict(one_kernel=True)):
+        with Context(device=0) as ctx:
+            ctx.upload_scene(sc)
+            frames = []
+            for f in range(3):
+                cam = configs.config_camera(1, 96, 64) if not kw.get("reproject") else \
+                    configs.make_camera((0.3 * f, 6.0, 9.0), (0.0, 0.0, 0.0), 96, 64, fov=55.0)
+                ctx.raycast(cam, f)
+                ctx.ris_path_trace(cam, f, candidate_count=16, max_depth=1, **kw, **mode)
+                frames.append(ctx.download("Color").copy())
+            outs.append(np.stack(frames))
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
