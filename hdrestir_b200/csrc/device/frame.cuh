@@ -137,10 +137,17 @@ constexpr int kShadeShapes = 4;
 int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &tune, unsigned *err, cudaStream_t st,
                       cudaEvent_t *ev_begin = nullptr, cudaEvent_t *ev_end = nullptr);
 // Spatial reuse (extension, spatial.cu): merges up to p.spatial_neighbors
-// neighbours' reservoirs of `in` into `out` and rewrites the colour.
+// neighbours' reservoirs of `in` into `out` and rewrites the colour. With a
+// winner queue (q_winner, counts[4]) the shadow rays of moved samples are
+// queued for launch_winner_visibility instead of cast in the kernel.
 int launch_ris_spatial(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
-                       GBufferView gb, ReservoirView in, ReservoirView out, float4 *color, unsigned *err,
-                       cudaStream_t st);
+                       GBufferView gb, ReservoirView in, ReservoirView out, float4 *color, float4 *q_winner,
+                       int *winner_count, unsigned *err, cudaStream_t st);
+// The queued winner shadow rays (wb.q_winner, counts[4] / [5]) traced, then the
+// pixels found occluded fixed up in rv and color.
+int launch_winner_visibility(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                             GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, unsigned *err,
+                             cudaStream_t st, const TraceTuning &tune);
 // Render-buffer conversion (resolve.cu): kResolve* are the HDR_FMT_* values.
 constexpr int kResolveFloat32 = 0, kResolveFloat16 = 1, kResolveUNorm8 = 2, kResolveSNorm8 = 3, kResolveInt32 = 4;
 int launch_resolve(const float *src, int src_comps, int format, int dst_comps, void *dst, size_t pixels,

@@ -676,7 +676,7 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
         wb.rng_state = (uint4 *)q;
         if ((st = ensure_buffer(c, "__wave_done", count, &q)) != HDR_OK) return st;
         wb.done = (unsigned char *)q;
-        if (p->skip_visibility || reproject) {  // winners whose visibility is still to be tested: one per pixel
+        if (p->skip_visibility || reproject || spatial) {  // winners whose visibility is still untested: one per pixel
             if ((st = ensure_buffer(c, "__wave_q_winner", count * 32, &q)) != HDR_OK) return st;
             wb.q_winner = (float4 *)q;
             if ((st = ensure_buffer(c, "__wave_occ_winner", count, &q)) != HDR_OK) return st;
@@ -696,13 +696,17 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
         if (timed)
             for (int k = kSlotWaveFirst; k < kSlotWaveFirst + 4; ++k) c->ev_pending[k] = true;
         c->launches += (uint64_t)n;
-        if (spatial) {
-            if (hdr::launch_ris_spatial(c->scene, cd, frame_index, d, gb, rv, rv_spatial, (float4 *)color, c->d_err,
-                                        c->stream) < 0)
+        if (spatial) {  // merged reservoirs, copied back, then the moved samples' shadow rays
+            HDR_CUDA(cudaMemsetAsync(wb.counts + 4, 0, 2 * sizeof(int), c->stream));
+            if (hdr::launch_ris_spatial(c->scene, cd, frame_index, d, gb, rv, rv_spatial, (float4 *)color,
+                                        wb.q_winner, wb.counts + 4, c->d_err, c->stream) < 0)
                 return fail(HDR_ECUDA, "spatial reuse launch failed: %s", cudaGetErrorString(cudaGetLastError()));
             HDR_CUDA(cudaMemcpyAsync(rv.dir_dist, rv_spatial.dir_dist, count * kResPlanes * sizeof(float4),
                                      cudaMemcpyDeviceToDevice, c->stream));
-            c->launches += 1;
+            if (hdr::launch_winner_visibility(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color, c->d_err,
+                                              c->stream, c->tune) < 0)
+                return fail(HDR_ECUDA, "winner visibility launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+            c->launches += 3;
         }
         c->last_wave = wb;
         c->have_wave = true;

@@ -57,7 +57,8 @@ template <int kThreads>
 __global__ void __launch_bounds__(kThreads) ris_spatial_kernel(DeviceScene s, CameraD cam, int frame_index,
                                                                PathRun pr, int cpf, int m_cap, int neighbours,
                                                                float radius, GBufferView gb, ReservoirView in,
-                                                               ReservoirView out, float4 *color, unsigned *err) {
+                                                               ReservoirView out, float4 *color, float4 *q_winner,
+                                                               int *winner_count, unsigned *err) {
     MtStream rng;
     PixelStart ps;
     if (!pixel_start<kThreads>(s, cam, frame_index, gb, rng, nullptr, ps)) return;
@@ -120,9 +121,16 @@ __global__ void __launch_bounds__(kThreads) ris_spatial_kernel(DeviceScene s, Ca
     reservoir_finalize(r, cpf);
     if (shifted && r.chosen.valid && r.w > 0.0f) {  // the moved sample's visibility from this pixel
         const V3 so = sf.hit.position + sf.sn * 1e-4f;
-        const unsigned oc = occluded_call(s.dev, so, r.chosen.ls.dir, r.chosen.ls.dist - 1e-3f);
-        e |= oc >> 1;
-        if (oc & 1u) r.chosen.tp = spec(0.0f);
+        if (q_winner) {  // queued; an occluded pixel is fixed up after the shadow kernel
+            const int k = atomicAdd(winner_count, 1);
+            q_winner[2 * (size_t)k] = make_float4(so.x, so.y, so.z, __int_as_float((int)i));
+            q_winner[2 * (size_t)k + 1] =
+                make_float4(r.chosen.ls.dir.x, r.chosen.ls.dir.y, r.chosen.ls.dir.z, r.chosen.ls.dist - 1e-3f);
+        } else {
+            const unsigned oc = occluded_call(s.dev, so, r.chosen.ls.dir, r.chosen.ls.dist - 1e-3f);
+            e |= oc >> 1;
+            if (oc & 1u) r.chosen.tp = spec(0.0f);
+        }
         r.chosen.vis_tested = true;
     }
     reservoir_store(out, i, r);
@@ -137,8 +145,8 @@ __global__ void __launch_bounds__(kThreads) ris_spatial_kernel(DeviceScene s, Ca
 }  // namespace
 
 int launch_ris_spatial(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
-                       GBufferView gb, ReservoirView in, ReservoirView out, float4 *color, unsigned *err,
-                       cudaStream_t st) {
+                       GBufferView gb, ReservoirView in, ReservoirView out, float4 *color, float4 *q_winner,
+                       int *winner_count, unsigned *err, cudaStream_t st) {
     PathRun pr{};
     pr.max_depth = p.max_depth;
     pr.enable_subsurface = p.enable_subsurface != 0;
@@ -147,7 +155,8 @@ int launch_ris_spatial(const DeviceScene &s, const CameraD &cam, int frame_index
     const int cpf = n_nee + (p.candidate_count - n_nee > 0 ? p.candidate_count - n_nee : 0);
     const float radius = p.spatial_radius > 0.0f ? p.spatial_radius : 30.0f;
     ris_spatial_kernel<256><<<tile_blocks(cam.width, cam.height), 256, 0, st>>>(
-        s, cam, frame_index, pr, cpf, p.m_cap, p.spatial_neighbors, radius, gb, in, out, color, err);
+        s, cam, frame_index, pr, cpf, p.m_cap, p.spatial_neighbors, radius, gb, in, out, color, q_winner,
+        winner_count, err);
     return cudaGetLastError() == cudaSuccess ? 1 : -1;
 }
 

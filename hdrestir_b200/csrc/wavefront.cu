@@ -493,6 +493,20 @@ __global__ void __launch_bounds__(256) ris_winner_fixup_kernel(DeviceScene s, Ca
     }
 }
 
+int launch_winner_visibility(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                             GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, unsigned *err,
+                             cudaStream_t st, const TraceTuning &tune) {
+    const int tgrid = tune.sm_count * tune.blocks_per_sm;
+    const bool shallow = s.shallow && (tune.mode & kTraceSplitStack) == 0;
+    auto shadow = s.wide ? trace_shadow_phased_kernel<true, false>
+                         : (shallow ? trace_shadow_phased_kernel<false, true> : trace_shadow_phased_kernel<false, false>);
+    shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_winner, wb.counts + 4, wb.counts + 5, wb.occ_winner,
+                                            tune.node_quorum, err);
+    ris_winner_fixup_kernel<<<tune.sm_count * 4, 256, 0, st>>>(s, cam, frame_index, path_run(p), gb, rv, wb.q_winner,
+                                                               wb.counts + 4, wb.occ_winner, color);
+    return cudaGetLastError() == cudaSuccess ? 2 : -1;
+}
+
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                          GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_level,
                          unsigned *err, cudaStream_t st, const TraceTuning &tune, cudaEvent_t *ev_begin,
@@ -510,15 +524,7 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
     if (launch_ris_shade(s, cam, frame_index, p, gb, rv, wb, color, trace_level, err, st, tune) < 0) return -1;
     int launches = 4;
     if (wb.q_winner) {  // the winners' shadow rays, then the pixels they found occluded
-        const int tgrid = tune.sm_count * tune.blocks_per_sm;
-        const bool shallow = s.shallow && (tune.mode & kTraceSplitStack) == 0;
-        auto shadow = s.wide ? trace_shadow_phased_kernel<true, false>
-                             : (shallow ? trace_shadow_phased_kernel<false, true> : trace_shadow_phased_kernel<false, false>);
-        shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_winner, wb.counts + 4, wb.counts + 5, wb.occ_winner,
-                                                tune.node_quorum, err);
-        ris_winner_fixup_kernel<<<tune.sm_count * 4, 256, 0, st>>>(s, cam, frame_index, path_run(p), gb, rv, wb.q_winner,
-                                                                   wb.counts + 4, wb.occ_winner, color);
-        if (cudaGetLastError() != cudaSuccess) return -1;
+        if (launch_winner_visibility(s, cam, frame_index, p, gb, rv, wb, color, err, st, tune) < 0) return -1;
         launches += 2;
     }
     if (!mark(ev_end, 3)) return -1;

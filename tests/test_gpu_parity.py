@@ -610,3 +610,22 @@ def test_queued_winner_visibility_equals_on_the_spot(kw):
                 frames.append(ctx.download("Color").copy())
             outs.append(np.stack(frames))
     assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+
+
+def test_spatial_reuse_queued_visibility_is_deterministic():
+    """Spatial reuse with its moved samples' shadow rays queued for the shadow kernel: two runs of
+    the same frames give the same images (the queue order may differ; the answers may not)."""
+    from hdrestir_b200.context import Context
+    sc, cam = configs.small_variant(2, 96, 64, grid=64, n_spheres=60, n_lights=400)
+    outs = []
+    for _ in range(2):
+        with Context(device=0) as ctx:
+            ctx.upload_scene(sc)
+            frames = []
+            for f in range(3):
+                ctx.raycast(cam, f)
+                ctx.ris_path_trace(cam, f, candidate_count=32, use_reservoir=True, max_depth=1,
+                                   spatial_neighbors=5, spatial_radius=16.0)
+                frames.append(ctx.download("Color").copy())
+            outs.append(np.stack(frames))
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
