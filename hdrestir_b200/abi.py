@@ -143,6 +143,7 @@ def lib() -> C.CDLL:
             "hdr_ctx_destroy": (None, [vp]),
             "hdr_scene_upload": (C.c_int, [vp, C.POINTER(SceneDesc)]),
             "hdr_scene_share": (C.c_int, [vp, vp]),
+            "hdr_scene_set_instance_transforms": (C.c_int, [vp, C.POINTER(C.c_float), i32, i32]),
             "hdr_path_trace_batch": (C.c_int, [C.POINTER(vp), i32, C.POINTER(CameraDesc), C.POINTER(i32),
                                                C.POINTER(PathSettings)]),
             "hdr_ris_path_trace_batch": (C.c_int, [C.POINTER(vp), i32, C.POINTER(CameraDesc), C.POINTER(i32),

@@ -22,7 +22,8 @@ LIB = PKG / "libhdrestir_b200.so"
 INCLUDE = PKG.parent / "include"
 
 SOURCES = ["hdr_abi.cpp", "host/scene_build.cpp", "raycast.cu", "integrate.cu", "wavefront.cu", "accumulate.cu",
-           "accumulate_noalloc.cu", "server.cpp", "pathtrace.cu", "spatial.cu", "resolve.cu", "post.cu"]
+           "accumulate_noalloc.cu", "server.cpp", "pathtrace.cu", "spatial.cu", "resolve.cu", "post.cu",
+           "tlas.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [

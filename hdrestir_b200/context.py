@@ -104,6 +104,25 @@ class Context:
         """Render `other`'s resident scene (no second copy in HBM)."""
         abi.check(self._lib.hdr_scene_share(self._h, other._h))
 
+    def set_instance_transforms(self, transforms) -> None:
+        """Move the uploaded scene's instances: `transforms` holds one row-major 4x4
+        per instance, in instance order, as a host array (n, 4, 4) / (n, 16) or a
+        CUDA tensor of float32 (read after torch's current stream is drained). The
+        instance records and the TLAS are rebuilt on the device; the images equal a
+        fresh upload of the scene with these transforms."""
+        if getattr(transforms, "is_cuda", False):
+            import torch
+
+            if transforms.dtype != torch.float32 or not transforms.is_contiguous() or transforms.numel() % 16:
+                raise ValueError("transforms: a contiguous float32 tensor of n x 16 values")
+            torch.cuda.current_stream(transforms.device).synchronize()
+            ptr = C.cast(C.c_void_p(transforms.data_ptr()), C.POINTER(C.c_float))
+            abi.check(self._lib.hdr_scene_set_instance_transforms(self._h, ptr, transforms.numel() // 16, 1))
+            return
+        xf = np.ascontiguousarray(np.asarray(transforms, dtype=np.float32).reshape(-1, 16))
+        ptr = xf.ctypes.data_as(C.POINTER(C.c_float))
+        abi.check(self._lib.hdr_scene_set_instance_transforms(self._h, ptr, xf.shape[0], 0))
+
     # ------------------------------------------------------------ passes
     def raycast(self, cam: Camera, frame_index: int = 0, aovs=()) -> None:
         mask = 0

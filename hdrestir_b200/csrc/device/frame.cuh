@@ -157,6 +157,14 @@ int launch_resolve(const float *src, int src_comps, int format, int dst_comps, v
 int launch_upscale(const float *src, float *dst, int comps, int src_w, int src_h, int dst_w, int dst_h, int sm_count,
                    cudaStream_t st);
 int launch_chroma_blur(const float4 *src, float4 *dst, int w, int h, int sm_count, cudaStream_t st);
+// Moved instances (tlas.cu): the n instance records rewritten from the n row-major
+// transforms xf (device memory), their world boxes and centres into bounds (9
+// floats each), then the binary TLAS rebuilt into tlas_nodes / tlas_inst as the
+// host scene builder builds it. info (device, 4 ints): nodes, maximum depth,
+// capacity overflow, an empty visited box. Returns the launches, -1 on error.
+int launch_tlas_rebuild(const float *xf, float4 *instances, const float *mesh_ranges, float *bounds, int n,
+                        float4 *tlas_nodes, int cap_nodes, int *tlas_inst, int4 *stack, int cap_stack, int *info,
+                        cudaStream_t st);
 // Which closest-hit rays of a pixel the wavefront RIS pass casts (trace_level).
 // Without light geometry and environment no generated BSDF candidate can
 // contribute, and without emissive materials either, neither can the

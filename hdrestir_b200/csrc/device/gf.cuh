@@ -12,6 +12,7 @@
 // kernels round identically.
 #pragma once
 
+#include <math.h>
 #include <stdint.h>
 
 #if defined(__CUDACC__)
@@ -106,5 +107,54 @@ HDR_HD D3 m4d_transform(const double *m, D3 v) {
 }
 HDR_HD V3 d3_to_f(D3 a) { return V3{(float)a.x, (float)a.y, (float)a.z}; }
 HDR_HD D3 f3_to_d(V3 a) { return D3{(double)a.x, (double)a.y, (double)a.z}; }
+
+// Inverse of a 4x4 (row-major) by cofactor expansion in double; singular
+// matrices yield a scale of FLT_MAX like GfMatrix4d::GetInverse. Shared by the
+// host scene builder and the device instance update, so both give the same bits.
+HDR_HD void gf_inverse4d(const double *m, double *out) {
+    const double s0 = m[0] * m[5] - m[4] * m[1];
+    const double s1 = m[0] * m[6] - m[4] * m[2];
+    const double s2 = m[0] * m[7] - m[4] * m[3];
+    const double s3 = m[1] * m[6] - m[5] * m[2];
+    const double s4 = m[1] * m[7] - m[5] * m[3];
+    const double s5 = m[2] * m[7] - m[6] * m[3];
+    const double c5 = m[10] * m[15] - m[14] * m[11];
+    const double c4 = m[9] * m[15] - m[13] * m[11];
+    const double c3 = m[9] * m[14] - m[13] * m[10];
+    const double c2 = m[8] * m[15] - m[12] * m[11];
+    const double c1 = m[8] * m[14] - m[12] * m[10];
+    const double c0 = m[8] * m[13] - m[12] * m[9];
+    const double det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+    if (!(fabs(det) > 0.0)) {
+        for (int i = 0; i < 16; ++i) out[i] = 0.0;
+        out[0] = out[5] = out[10] = 3.402823466e+38;
+        out[15] = 1.0;
+        return;
+    }
+    const double r = 1.0 / det;
+    out[0] = (m[5] * c5 - m[6] * c4 + m[7] * c3) * r;
+    out[1] = (-m[1] * c5 + m[2] * c4 - m[3] * c3) * r;
+    out[2] = (m[13] * s5 - m[14] * s4 + m[15] * s3) * r;
+    out[3] = (-m[9] * s5 + m[10] * s4 - m[11] * s3) * r;
+    out[4] = (-m[4] * c5 + m[6] * c2 - m[7] * c1) * r;
+    out[5] = (m[0] * c5 - m[2] * c2 + m[3] * c1) * r;
+    out[6] = (-m[12] * s5 + m[14] * s2 - m[15] * s1) * r;
+    out[7] = (m[8] * s5 - m[10] * s2 + m[11] * s1) * r;
+    out[8] = (m[4] * c4 - m[5] * c2 + m[7] * c0) * r;
+    out[9] = (-m[0] * c4 + m[1] * c2 - m[3] * c0) * r;
+    out[10] = (m[12] * s4 - m[13] * s2 + m[15] * s0) * r;
+    out[11] = (-m[8] * s4 + m[9] * s2 - m[11] * s0) * r;
+    out[12] = (-m[4] * c3 + m[5] * c1 - m[6] * c0) * r;
+    out[13] = (m[0] * c3 - m[1] * c1 + m[2] * c0) * r;
+    out[14] = (-m[12] * s3 + m[13] * s1 - m[14] * s0) * r;
+    out[15] = (m[8] * s3 - m[9] * s1 + m[10] * s0) * r;
+}
+
+HDR_HD void gf_inverse4f(const float *m, float *out) {
+    double md[16], od[16];
+    for (int i = 0; i < 16; ++i) md[i] = (double)m[i];
+    gf_inverse4d(md, od);
+    for (int i = 0; i < 16; ++i) out[i] = (float)od[i];
+}
 
 }  // namespace hdr

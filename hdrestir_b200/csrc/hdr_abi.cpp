@@ -71,6 +71,16 @@ struct SceneStore {
     size_t bytes = 0;
     // the scene descriptor in device memory, [0] for the binary walk, [1] for the wide one
     const hdr::DeviceScene *desc_dev = nullptr;
+    // hdr_scene_set_instance_transforms: what the device rebuild of the instances and the TLAS needs
+    int num_instances = 0, max_blas_depth = 0;
+    int tlas_capacity = 0;          // TLAS nodes the upload reserved (4 per instance)
+    bool blas_proper = true;        // no BLAS node box is empty (the TLAS is checked at each build)
+    bool wide_stale = false;        // the wide TLAS no longer matches the binary one
+    float *mesh_ranges = nullptr;   // 6 floats per mesh
+    float *inst_bounds = nullptr;   // 9 floats per instance: world box, centre
+    float *xf_staging = nullptr;    // 16 floats per instance
+    int4 *tlas_stack = nullptr;     // num_instances + 2 entries
+    int *tlas_info = nullptr;       // 4 ints
     ~SceneStore() {
         if (ptrs.empty()) return;
         int prev = 0;
@@ -380,32 +390,52 @@ void hdr_ctx_destroy(hdr_ctx *c) {
 }
 
 namespace {
-// True when no node box of the flat scene's trees is empty (min > max on an
-// axis): the traversal may then leave GfRange3f::IsEmpty out of its slab tests.
-bool boxes_proper(const hdr::FlatScene &f) {
-    auto empty = [](const float *lo, const float *hi) { return lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]; };
-    for (size_t k = 0; k + 8 <= f.blas_nodes.size(); k += 8)
-        if (empty(&f.blas_nodes[k], &f.blas_nodes[k + 4])) return false;
-    for (size_t k = 0; k + 8 <= f.tlas_nodes.size(); k += 8)
-        if (empty(&f.tlas_nodes[k], &f.tlas_nodes[k + 4])) return false;
-    for (const std::vector<float> *w : {&f.blas4, &f.tlas4})
-        for (size_t k = 0; k + hdr::kWideNodeFloats <= w->size(); k += hdr::kWideNodeFloats) {
-            const float *n = w->data() + k;
-            for (int j = 0; j < 4; ++j) {
-                int code;
-                std::memcpy(&code, &n[24 + j], sizeof(code));
-                const float lo[3] = {n[j], n[4 + j], n[8 + j]}, hi[3] = {n[12 + j], n[16 + j], n[20 + j]};
-                if (code >= 0 && empty(lo, hi)) return false;
-            }
+// True when no node box of the flat scene's BLAS trees is empty (min > max on an axis).
+bool empty_box(const float *lo, const float *hi) { return lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]; }
+bool wide_boxes_proper(const std::vector<float> &w) {
+    for (size_t k = 0; k + hdr::kWideNodeFloats <= w.size(); k += hdr::kWideNodeFloats) {
+        const float *n = w.data() + k;
+        for (int j = 0; j < 4; ++j) {
+            int code;
+            std::memcpy(&code, &n[24 + j], sizeof(code));
+            const float lo[3] = {n[j], n[4 + j], n[8 + j]}, hi[3] = {n[12 + j], n[16 + j], n[20 + j]};
+            if (code >= 0 && empty_box(lo, hi)) return false;
         }
+    }
+    return true;
+}
+bool blas_boxes_proper(const hdr::FlatScene &f) {
+    for (size_t k = 0; k + 8 <= f.blas_nodes.size(); k += 8)
+        if (empty_box(&f.blas_nodes[k], &f.blas_nodes[k + 4])) return false;
+    if (!wide_boxes_proper(f.blas4)) return false;
     for (size_t k = 0; k + 8 <= f.blas_roots.size(); k += 8) {
         int code;
         std::memcpy(&code, &f.blas_roots[k + 3], sizeof(code));
-        if (code >= 0 && empty(&f.blas_roots[k], &f.blas_roots[k + 4])) return false;
+        if (code >= 0 && empty_box(&f.blas_roots[k], &f.blas_roots[k + 4])) return false;
     }
+    return true;
+}
+// The same for the TLAS, over the nodes a walk can reach: the two children
+// every TLAS leaf allocates (scene.cpp:344-349) keep their default empty boxes
+// but are never visited.
+bool tlas_boxes_proper(const hdr::FlatScene &f) {
+    if (f.tlas_nodes.empty()) return true;
+    std::vector<int> todo{0};
+    while (!todo.empty()) {
+        const int n = todo.back();
+        todo.pop_back();
+        const float *rec = &f.tlas_nodes[8 * (size_t)n];
+        if (empty_box(rec, rec + 4)) return false;
+        int left;
+        std::memcpy(&left, &rec[3], sizeof(left));
+        if (left < 0) continue;
+        todo.push_back(left);
+        todo.push_back(left + 1);
+    }
+    if (!wide_boxes_proper(f.tlas4)) return false;
     int root;
     std::memcpy(&root, &f.tlas_root[3], sizeof(root));
-    return !(root >= 0 && empty(&f.tlas_root[0], &f.tlas_root[4]));
+    return !(root >= 0 && empty_box(&f.tlas_root[0], &f.tlas_root[4]));
 }
 }  // namespace
 
@@ -449,7 +479,7 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
         if (st != HDR_OK) return st;
         store->ptrs.push_back(b.ptr);
         store->bytes += b.bytes;
-        if (bytes) HDR_CUDA(cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, c->stream));
+        if (bytes && src) HDR_CUDA(cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, c->stream));
         *dst = b.ptr;
         return HDR_OK;
     };
@@ -466,6 +496,10 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     UP(f.tri_geo, tri_geo);
     UP(f.tri_attr, tri_attr);
     UP(f.instances, instances);
+    // room for the TLAS of any transforms of the same instances (hdr_scene_set_instance_transforms):
+    // each visited node allocates two, and at most 2n - 1 nodes are visited
+    const int tlas_capacity = 4 * f.num_instances;
+    if (f.tlas_nodes.size() < 8 * (size_t)tlas_capacity) f.tlas_nodes.resize(8 * (size_t)tlas_capacity, 0.0f);
     UP(f.tlas_nodes, tlas_nodes);
     UP(f.tlas_inst, tlas_inst);
     UP(f.materials, materials);
@@ -477,6 +511,28 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     UP(f.blas_roots, blas_roots);
     UP(f.tlas4, tlas4);
 #undef UP
+    {  // the device TLAS rebuild's inputs and scratch
+        const size_t n = (size_t)f.num_instances;
+        const void *ranges = nullptr, *bounds = nullptr, *xf = nullptr, *stk = nullptr, *info = nullptr;
+        if ((st = upload(f.mesh_ranges.data(), f.mesh_ranges.size() * sizeof(float), &ranges)) != HDR_OK ||
+            (st = upload(nullptr, n * 9 * sizeof(float), &bounds)) != HDR_OK ||
+            (st = upload(nullptr, n * 16 * sizeof(float), &xf)) != HDR_OK ||
+            (st = upload(nullptr, (n + 2) * sizeof(int4), &stk)) != HDR_OK ||
+            (st = upload(nullptr, 4 * sizeof(int), &info)) != HDR_OK) {
+            cudaStreamSynchronize(c->stream);
+            c->allocated -= store->bytes;
+            return st;
+        }
+        store->mesh_ranges = (float *)ranges;
+        store->inst_bounds = (float *)bounds;
+        store->xf_staging = (float *)xf;
+        store->tlas_stack = (int4 *)stk;
+        store->tlas_info = (int *)info;
+        store->num_instances = f.num_instances;
+        store->max_blas_depth = f.max_blas_depth;
+        store->tlas_capacity = tlas_capacity;
+        store->blas_proper = blas_boxes_proper(f);
+    }
     std::memcpy(&s.tlas_root_lo, f.tlas_root, sizeof(float4));
     std::memcpy(&s.tlas_root_hi, f.tlas_root + 4, sizeof(float4));
     s.wide = (c->flags & HDR_CTX_WIDE_BVH) ? 1 : 0;
@@ -488,7 +544,7 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     s.dome_height = f.dome_height;
     s.dome_total_lum = f.dome_total_lum;
     s.has_tlas = f.num_instances > 0 ? 1 : 0;
-    s.proper_boxes = boxes_proper(f) ? 1 : 0;
+    s.proper_boxes = (store->blas_proper && tlas_boxes_proper(f)) ? 1 : 0;
     s.shallow = (f.max_blas_depth + f.max_tlas_depth + 4 <= hdr::kShallowStack) ? 1 : 0;
     // the descriptor itself, for callees that are not inlined into a kernel
     hdr::DeviceScene copies[2] = {s, s};
@@ -772,6 +828,8 @@ hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src) {
     std::lock(dst->mu, src->mu);
     std::lock_guard<std::mutex> l1(dst->mu, std::adopt_lock), l2(src->mu, std::adopt_lock);
     if (!src->has_scene) return fail(HDR_ENOSCENE, "the source context has no scene");
+    if ((dst->flags & HDR_CTX_WIDE_BVH) && src->scene_store->wide_stale)
+        return fail(HDR_EINVAL, "the scene's instances moved on the device: its wide TLAS is not rebuilt");
     HDR_CUDA(cudaSetDevice(dst->device));
     HDR_CUDA(cudaStreamSynchronize(dst->stream));  // dst's old scene may still be in use on its stream
     dst->scene_store = src->scene_store;
@@ -785,6 +843,61 @@ hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src) {
     dst->scene_emissive = src->scene_emissive;
     dst->has_scene = true;
     dst->have_wave = false;
+    return HDR_OK;
+}
+
+// Scene::BuildRenderState after HdRestirMesh::Sync took new transforms
+// (hd_restir_mesh.cpp:160-162, scene.cpp:118-244, 333-407): the instance records
+// and the binary TLAS rebuilt in place on the ctx stream, the same bits a fresh
+// hdr_scene_upload of the scene with these transforms would give.
+hdr_status hdr_scene_set_instance_transforms(hdr_ctx *c, const float *transforms, int32_t num_instances,
+                                             int32_t transforms_on_device) {
+    if (!c || !transforms) return fail(HDR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_scene_set_instance_transforms before hdr_scene_upload");
+    SceneStore *store = c->scene_store.get();
+    if (num_instances != store->num_instances)
+        return fail(HDR_EINVAL, "%d transforms for a scene of %d instances", num_instances, store->num_instances);
+    if (c->scene.wide) return fail(HDR_EINVAL, "no device TLAS rebuild for the wide BVH walk (HDR_CTX_WIDE_BVH)");
+    if (c->scene_store.use_count() > 1)
+        return fail(HDR_EINVAL, "the scene is shared with another context (hdr_scene_share)");
+    if (num_instances == 0) return HDR_OK;
+    HDR_CUDA(cudaSetDevice(c->device));
+    const float *xf = transforms;
+    if (!transforms_on_device) {
+        HDR_CUDA(cudaMemcpyAsync(store->xf_staging, transforms, (size_t)num_instances * 16 * sizeof(float),
+                                 cudaMemcpyHostToDevice, c->stream));
+        xf = store->xf_staging;
+    }
+    hdr::DeviceScene &s = c->scene;
+    const int launched = hdr::launch_tlas_rebuild(
+        xf, const_cast<float4 *>(s.instances), store->mesh_ranges, store->inst_bounds, num_instances,
+        const_cast<float4 *>(s.tlas_nodes), store->tlas_capacity, const_cast<int *>(s.tlas_inst), store->tlas_stack,
+        num_instances + 2, store->tlas_info, c->stream);
+    if (launched < 0) {
+        c->has_scene = false;
+        return fail(HDR_ECUDA, "TLAS rebuild launch: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    c->launches += (uint64_t)launched;
+    int info[4] = {};
+    HDR_CUDA(cudaMemcpyAsync(info, store->tlas_info, sizeof(info), cudaMemcpyDeviceToHost, c->stream));
+    HDR_CUDA(cudaStreamSynchronize(c->stream));
+    store->wide_stale = true;
+    if (info[2] || store->max_blas_depth + info[1] + 4 > hdr::kTraceStack) {
+        c->has_scene = false;  // the records are rewritten but the TLAS cannot be walked: upload again
+        return fail(HDR_EINVAL, "TLAS depth %d + BVH depth %d exceeds the device traversal stack (%d)", info[1],
+                    store->max_blas_depth, hdr::kTraceStack);
+    }
+    s.proper_boxes = (store->blas_proper && !info[3]) ? 1 : 0;
+    s.shallow = (store->max_blas_depth + info[1] + 4 <= hdr::kShallowStack) ? 1 : 0;
+    hdr::DeviceScene copies[2] = {s, s};
+    for (int w = 0; w < 2; ++w) {
+        copies[w].wide = w;
+        copies[w].dev = store->desc_dev + w;
+    }
+    HDR_CUDA(cudaMemcpyAsync(const_cast<hdr::DeviceScene *>(store->desc_dev), copies, sizeof(copies),
+                             cudaMemcpyHostToDevice, c->stream));
+    HDR_CUDA(cudaStreamSynchronize(c->stream));  // `copies` is a host stack buffer
     return HDR_OK;
 }
 

@@ -87,6 +87,7 @@ struct FlatScene {
     std::vector<float> instances;   // 32 floats per instance
     std::vector<float> tlas_nodes;  // 8 floats per node
     std::vector<int> tlas_inst;
+    std::vector<float> mesh_ranges; // 6 floats per mesh: MeshSubset::range min.xyz, max.xyz
     std::vector<float> materials;   // kMaterialFloats per material
     std::vector<float> lights;      // kLightFloats per light
     std::vector<float> dome_pixels, dome_row_cdf, dome_col_cdf;
@@ -100,11 +101,6 @@ struct FlatScene {
 
 constexpr int kMaterialFloats = 48;
 constexpr int kLightFloats = 48;
-
-// Inverse of a 4x4 (row-major) by cofactor expansion in double; singular
-// matrices yield a scale of FLT_MAX like GfMatrix4d::GetInverse.
-void gf_inverse4d(const double *m, double *out);
-void gf_inverse4f(const float *m, float *out);
 
 Blas build_blas(const hdr_mesh_desc &mesh);
 bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &err);

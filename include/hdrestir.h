@@ -263,6 +263,22 @@ hdr_status hdr_scene_upload(hdr_ctx *ctx, const hdr_scene_desc *scene);
  * another scene or is destroyed. Required for hdr_ris_path_trace_batch. */
 hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src);
 
+/* Moved instances: HdRestirMesh::Sync taking a dirty transform
+ * (hydra/hd_restir_mesh.cpp:160-162) followed by the TLAS rebuild of
+ * Scene::BuildRenderState (scene/scene.cpp:118-244, 333-407), on the device.
+ * `transforms` holds num_instances row-major 4x4 floats (the layout of
+ * hdr_instance_desc.transform), in device memory when transforms_on_device is
+ * non-zero (read on the ctx stream), else host memory. The instance records and
+ * the binary TLAS are rebuilt in place: the images equal those of a fresh
+ * hdr_scene_upload with these transforms, bit for bit. num_instances must be the
+ * uploaded scene's; the ctx must walk the binary trees (no HDR_CTX_WIDE_BVH) and
+ * hold the scene alone (not shared through hdr_scene_share), and afterwards the
+ * scene cannot be shared into a wide-walk ctx. Synchronises the ctx stream (the
+ * new TLAS depth sizes the traversal stack). A TLAS too deep for the traversal
+ * stack fails with HDR_EINVAL and leaves the ctx without a scene. */
+hdr_status hdr_scene_set_instance_transforms(hdr_ctx *ctx, const float *transforms, int32_t num_instances,
+                                             int32_t transforms_on_device);
+
 /* RaycastPass::_execute (passes/raycast_pass.cpp:57-162): GBuffer (+AOVs). */
 hdr_status hdr_raycast(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_index, uint32_t aov_mask);
 
