@@ -21,6 +21,7 @@ AOV_DEPTH, AOV_ALBEDO, AOV_NORMAL = 1, 2, 4
 ACCUM_PARITY, ACCUM_SHADER = 0, 1
 CTX_TIMINGS, CTX_WIDE_BVH, CTX_LANE_PER_RAY, CTX_UNPHASED, CTX_PT_ONE_KERNEL = 1, 2, 8, 16, 32
 CTX_SPLIT_STACK = 64
+CTX_DEVICE_BUILD = 128
 RIS_REPROJECT = 4
 FMT_FLOAT32, FMT_FLOAT16, FMT_UNORM8, FMT_SNORM8, FMT_INT32 = 0, 1, 2, 3, 4
 FMT_DTYPES = {0: np.float32, 1: np.uint16, 2: np.uint8, 3: np.int8, 4: np.int32}
@@ -144,6 +145,7 @@ def lib() -> C.CDLL:
             "hdr_scene_upload": (C.c_int, [vp, C.POINTER(SceneDesc)]),
             "hdr_scene_share": (C.c_int, [vp, vp]),
             "hdr_scene_set_instance_transforms": (C.c_int, [vp, C.POINTER(C.c_float), i32, i32]),
+            "hdr_scene_array": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, C.POINTER(C.c_size_t)]),
             "hdr_path_trace_batch": (C.c_int, [C.POINTER(vp), i32, C.POINTER(CameraDesc), C.POINTER(i32),
                                                C.POINTER(PathSettings)]),
             "hdr_ris_path_trace_batch": (C.c_int, [C.POINTER(vp), i32, C.POINTER(CameraDesc), C.POINTER(i32),

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/hdrestir.h"
+#include "device/blas_build.h"
 #include "device/frame.cuh"
 #include "host/scene_build.h"
 
@@ -81,6 +82,8 @@ struct SceneStore {
     float *xf_staging = nullptr;    // 16 floats per instance
     int4 *tlas_stack = nullptr;     // num_instances + 2 entries
     int *tlas_info = nullptr;       // 4 ints
+    // the scene's arrays by DeviceScene field name, for hdr_scene_array
+    std::map<std::string, std::pair<const void *, size_t>> arrays;
     ~SceneStore() {
         if (ptrs.empty()) return;
         int prev = 0;
@@ -334,6 +337,8 @@ hdr_status hdr_ctx_create(hdr_ctx **out, const hdr_ctx_desc *desc) {
     HDR_CUDA(cudaGetDeviceCount(&ndev));
     const int dev = desc ? desc->device : 0;
     if (dev < 0 || dev >= ndev) return fail(HDR_EINVAL, "device %d not present (%d devices)", dev, ndev);
+    if (desc && (desc->flags & HDR_CTX_DEVICE_BUILD) && (desc->flags & HDR_CTX_WIDE_BVH))
+        return fail(HDR_EINVAL, "HDR_CTX_DEVICE_BUILD builds the binary trees only (no HDR_CTX_WIDE_BVH)");
     HDR_CUDA(cudaSetDevice(dev));
     hdr_ctx *c = new hdr_ctx();
     c->device = dev;
@@ -452,9 +457,35 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     if (!c || !desc) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);
     HDR_CUDA(cudaSetDevice(c->device));
+    const bool device_build = (c->flags & HDR_CTX_DEVICE_BUILD) != 0;
+    // HDR_CTX_DEVICE_BUILD: every mesh's BLAS and triangle records built on the device first
+    std::vector<std::unique_ptr<hdr::DeviceBlasBuild>> dev_blas;
+    std::vector<hdr::ExternalBlas> ext;
+    bool dev_empty_box = false;
+    if (device_build) {
+        if (desc->num_meshes < 0) return fail(HDR_EINVAL, "negative count in hdr_scene_desc");
+        for (int mi = 0; mi < desc->num_meshes; ++mi) {
+            const hdr_mesh_desc &m = desc->meshes[mi];
+            if ((m.num_points > 0 && !m.points) || (m.num_triangles > 0 && !m.indices) || (m.num_uvs > 0 && !m.uvs) ||
+                (m.num_normals > 0 && !m.normals) || (m.num_colors > 0 && !m.colors))
+                return fail(HDR_EINVAL, "mesh %d: NULL array with non-zero count", mi);
+        }
+        ext.resize((size_t)desc->num_meshes);
+        for (int mi = 0; mi < desc->num_meshes; ++mi) {
+            dev_blas.emplace_back(new hdr::DeviceBlasBuild);
+            const cudaError_t e = dev_blas.back()->run(desc->meshes[mi], c->stream);
+            if (e != cudaSuccess) return fail(HDR_ECUDA, "device BLAS build of mesh %d: %s", mi, cudaGetErrorString(e));
+            const hdr::DeviceBlasResult &r = dev_blas.back()->result;
+            ext[mi].num_nodes = r.num_nodes;
+            ext[mi].num_tris = r.num_tris;
+            ext[mi].max_depth = r.max_depth;
+            dev_empty_box = dev_empty_box || r.empty_box;
+        }
+    }
     hdr::FlatScene f;
     std::string err;
-    if (!hdr::build_flat_scene(*desc, f, err)) return fail(HDR_EINVAL, "%s", err.c_str());
+    if (!hdr::build_flat_scene(*desc, f, err, device_build ? ext.data() : nullptr))
+        return fail(HDR_EINVAL, "%s", err.c_str());
     // binary walk: one pending sibling per level of each tree, plus the two instance slots of a TLAS leaf
     if (f.max_blas_depth + f.max_tlas_depth + 4 > hdr::kTraceStack)
         return fail(HDR_EINVAL, "BVH depth %d + TLAS depth %d exceeds the device traversal stack (%d)",
@@ -491,10 +522,40 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
         cudaStreamSynchronize(c->stream);                                                           \
         c->allocated -= store->bytes;                                                               \
         return st;                                                                                  \
+    }                                                                                               \
+    store->arrays[#field] = {s.field, vec.size() * sizeof(vec[0])};
+    if (device_build) {
+        const size_t node_bytes = f.num_blas_nodes * 2 * sizeof(float4);
+        const size_t geo_bytes = f.num_triangles * (hdr::kTriGeoFloats * sizeof(float));
+        const size_t attr_bytes = f.num_triangles * (hdr::kTriAttrFloats * sizeof(float));
+        if ((st = upload(nullptr, node_bytes, (const void **)&s.blas_nodes)) != HDR_OK ||
+            (st = upload(nullptr, geo_bytes, (const void **)&s.tri_geo)) != HDR_OK ||
+            (st = upload(nullptr, attr_bytes, (const void **)&s.tri_attr)) != HDR_OK) {
+            cudaStreamSynchronize(c->stream);
+            c->allocated -= store->bytes;
+            return st;
+        }
+        size_t node_base = 0, tri_base = 0;
+        for (size_t mi = 0; mi < dev_blas.size(); ++mi) {
+            const cudaError_t e = dev_blas[mi]->write(const_cast<float4 *>(s.blas_nodes) + 2 * node_base,
+                                                      const_cast<float4 *>(s.tri_geo) + 3 * tri_base,
+                                                      const_cast<float4 *>(s.tri_attr) + 9 * tri_base);
+            if (e != cudaSuccess) {
+                cudaStreamSynchronize(c->stream);
+                c->allocated -= store->bytes;
+                return fail(HDR_ECUDA, "device BLAS build of mesh %zu: %s", mi, cudaGetErrorString(e));
+            }
+            node_base += (size_t)ext[mi].num_nodes;
+            tri_base += (size_t)ext[mi].num_tris;
+        }
+        store->arrays["blas_nodes"] = {s.blas_nodes, node_bytes};
+        store->arrays["tri_geo"] = {s.tri_geo, geo_bytes};
+        store->arrays["tri_attr"] = {s.tri_attr, attr_bytes};
+    } else {
+        UP(f.blas_nodes, blas_nodes);
+        UP(f.tri_geo, tri_geo);
+        UP(f.tri_attr, tri_attr);
     }
-    UP(f.blas_nodes, blas_nodes);
-    UP(f.tri_geo, tri_geo);
-    UP(f.tri_attr, tri_attr);
     UP(f.instances, instances);
     // room for the TLAS of any transforms of the same instances (hdr_scene_set_instance_transforms):
     // each visited node allocates two, and at most 2n - 1 nodes are visited
@@ -531,7 +592,8 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
         store->num_instances = f.num_instances;
         store->max_blas_depth = f.max_blas_depth;
         store->tlas_capacity = tlas_capacity;
-        store->blas_proper = blas_boxes_proper(f);
+        store->blas_proper = blas_boxes_proper(f) && !dev_empty_box;
+        store->wide_stale = device_build;  // the device build makes no wide trees
     }
     std::memcpy(&s.tlas_root_lo, f.tlas_root, sizeof(float4));
     std::memcpy(&s.tlas_root_hi, f.tlas_root + 4, sizeof(float4));
@@ -898,6 +960,22 @@ hdr_status hdr_scene_set_instance_transforms(hdr_ctx *c, const float *transforms
     HDR_CUDA(cudaMemcpyAsync(const_cast<hdr::DeviceScene *>(store->desc_dev), copies, sizeof(copies),
                              cudaMemcpyHostToDevice, c->stream));
     HDR_CUDA(cudaStreamSynchronize(c->stream));  // `copies` is a host stack buffer
+    return HDR_OK;
+}
+
+hdr_status hdr_scene_array(hdr_ctx *c, const char *name, void *dst, size_t bytes, size_t *size) {
+    if (!c || !name) return fail(HDR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_scene_array before hdr_scene_upload");
+    const auto it = c->scene_store->arrays.find(name);
+    if (it == c->scene_store->arrays.end()) return fail(HDR_EINVAL, "no scene array named '%s'", name);
+    if (size) *size = it->second.second;
+    if (!dst) return HDR_OK;
+    if (bytes != it->second.second)
+        return fail(HDR_EINVAL, "scene array '%s' holds %zu bytes, not %zu", name, it->second.second, bytes);
+    HDR_CUDA(cudaSetDevice(c->device));
+    if (bytes) HDR_CUDA(cudaMemcpyAsync(dst, it->second.first, bytes, cudaMemcpyDeviceToHost, c->stream));
+    HDR_CUDA(cudaStreamSynchronize(c->stream));
     return HDR_OK;
 }
 

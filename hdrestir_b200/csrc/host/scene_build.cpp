@@ -18,85 +18,6 @@ inline float as_float(int i) {
     return f;
 }
 
-// Tangent frame and per-triangle data of BVH::Build (bvh.cpp:81-179).
-bool make_triangle(const hdr_mesh_desc &m, int i, BlasTriangle &tri) {
-    const int ntri = m.num_triangles;
-    const int i0 = m.indices[3 * i + 0], i1 = m.indices[3 * i + 1], i2 = m.indices[3 * i + 2];
-    const int np = m.num_points;
-    if (i0 < 0 || i0 >= np || i1 < 0 || i1 >= np || i2 < 0 || i2 >= np) return false;
-    auto P = [&](int k) { return V3{m.points[3 * k], m.points[3 * k + 1], m.points[3 * k + 2]}; };
-    tri.v0 = P(i0);
-    tri.v1 = P(i1);
-    tri.v2 = P(i2);
-
-    if (m.num_uvs > 0) {
-        auto UV = [&](int k) { return V2{m.uvs[2 * k], m.uvs[2 * k + 1]}; };
-        if (m.num_uvs == ntri * 3) {
-            tri.uv0 = UV(i * 3 + 0);
-            tri.uv1 = UV(i * 3 + 1);
-            tri.uv2 = UV(i * 3 + 2);
-        } else {
-            tri.uv0 = (i0 < m.num_uvs) ? UV(i0) : V2{0.0f, 0.0f};
-            tri.uv1 = (i1 < m.num_uvs) ? UV(i1) : V2{0.0f, 0.0f};
-            tri.uv2 = (i2 < m.num_uvs) ? UV(i2) : V2{0.0f, 0.0f};
-        }
-    } else {
-        tri.uv0 = tri.uv1 = tri.uv2 = V2{0.0f, 0.0f};
-    }
-
-    auto N = [&](const float *a, int k) { return V3{a[3 * k], a[3 * k + 1], a[3 * k + 2]}; };
-    if (m.num_normals > 0) {
-        if (m.num_normals == ntri * 3) {
-            tri.n0 = N(m.normals, i * 3 + 0);
-            tri.n1 = N(m.normals, i * 3 + 1);
-            tri.n2 = N(m.normals, i * 3 + 2);
-        } else {
-            const V3 up{0.0f, 1.0f, 0.0f};
-            tri.n0 = (i0 < m.num_normals) ? N(m.normals, i0) : up;
-            tri.n1 = (i1 < m.num_normals) ? N(m.normals, i1) : up;
-            tri.n2 = (i2 < m.num_normals) ? N(m.normals, i2) : up;
-        }
-    } else {
-        tri.n0 = tri.n1 = tri.n2 = V3{0.0f, 0.0f, 0.0f};
-    }
-
-    if (m.num_colors > 0) {
-        if (m.num_colors == ntri * 3) {
-            tri.c0 = N(m.colors, i * 3 + 0);
-            tri.c1 = N(m.colors, i * 3 + 1);
-            tri.c2 = N(m.colors, i * 3 + 2);
-        } else {
-            const V3 one{1.0f, 1.0f, 1.0f};
-            tri.c0 = (i0 < m.num_colors) ? N(m.colors, i0) : one;
-            tri.c1 = (i1 < m.num_colors) ? N(m.colors, i1) : one;
-            tri.c2 = (i2 < m.num_colors) ? N(m.colors, i2) : one;
-        }
-    } else {
-        tri.c0 = tri.c1 = tri.c2 = V3{1.0f, 1.0f, 1.0f};
-    }
-
-    const V3 edge1 = tri.v1 - tri.v0;
-    const V3 edge2 = tri.v2 - tri.v0;
-    const V2 duv1{tri.uv1.x - tri.uv0.x, tri.uv1.y - tri.uv0.y};
-    const V2 duv2{tri.uv2.x - tri.uv0.x, tri.uv2.y - tri.uv0.y};
-    float f = duv1.x * duv2.y - duv2.x * duv1.y;
-    if (std::abs(f) > 1e-8f) {
-        f = 1.0f / f;
-        tri.dpdu = (edge1 * duv2.y - edge2 * duv1.y) * f;
-        tri.dpdv = (edge2 * duv1.x - edge1 * duv2.x) * f;
-        tri.dpdu = normalized(tri.dpdu);
-        tri.dpdv = normalized(tri.dpdv);
-    } else {
-        const V3 n = normalized(cross(edge1, edge2));
-        const V3 up = std::abs(n.y) < 0.999f ? V3{0, 1, 0} : V3{1, 0, 0};
-        tri.dpdu = normalized(cross(up, n));
-        tri.dpdv = normalized(cross(n, tri.dpdu));
-    }
-    tri.material = (i < m.num_material_indices && m.material_indices) ? m.material_indices[i] : -1;
-    tri.centroid = div_d(tri.v0 + tri.v1 + tri.v2, 3.0);
-    return true;
-}
-
 struct BlasBuilder {
     Blas &b;
     void subdivide(int node_idx, int start, int end, int depth) {
@@ -284,15 +205,21 @@ struct WideBuilder {
 
 }  // namespace
 
-Blas build_blas(const hdr_mesh_desc &m) {
-    Blas b;
-    // MeshSubset::range over the referenced points (hd_restir_mesh.cpp:523-529)
+// MeshSubset::range over the referenced points (hd_restir_mesh.cpp:523-529)
+Range3 mesh_range(const hdr_mesh_desc &m) {
+    Range3 r;
     for (int i = 0; i < m.num_triangles; ++i) {
         for (int k = 0; k < 3; ++k) {
             const int p = m.indices[3 * i + k];
-            if (p >= 0 && p < m.num_points) b.range.extend(V3{m.points[3 * p], m.points[3 * p + 1], m.points[3 * p + 2]});
+            if (p >= 0 && p < m.num_points) r.extend(V3{m.points[3 * p], m.points[3 * p + 1], m.points[3 * p + 2]});
         }
     }
+    return r;
+}
+
+Blas build_blas(const hdr_mesh_desc &m) {
+    Blas b;
+    b.range = mesh_range(m);
     if (m.num_triangles <= 0 || m.num_points <= 0) return b;
     b.tris.reserve((size_t)m.num_triangles);
     for (int i = 0; i < m.num_triangles; ++i) {
@@ -307,7 +234,7 @@ Blas build_blas(const hdr_mesh_desc &m) {
     return b;
 }
 
-bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &err) {
+bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &err, const ExternalBlas *ext) {
     out = FlatScene{};
     if (desc.num_meshes < 0 || desc.num_instances < 0 || desc.num_materials < 0 || desc.num_lights < 0) {
         err = "negative count in hdr_scene_desc";
@@ -323,6 +250,21 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
             (m.num_normals > 0 && !m.normals) || (m.num_colors > 0 && !m.colors)) {
             err = "mesh " + std::to_string(mi) + ": NULL array with non-zero count";
             return false;
+        }
+        if (ext) {  // the trees and triangle records are built elsewhere (on the device)
+            const ExternalBlas &e = ext[mi];
+            ranges[mi] = mesh_range(m);
+            const Range3 &r = ranges[mi];
+            const float r6[6] = {r.mn.x, r.mn.y, r.mn.z, r.mx.x, r.mx.y, r.mx.z};
+            out.mesh_ranges.insert(out.mesh_ranges.end(), r6, r6 + 6);
+            node_base[mi] = (int)out.num_blas_nodes;
+            tri_base[mi] = (int)out.num_triangles;
+            blas_ok[mi] = e.num_nodes > 0 ? 1 : 0;
+            wide_base[mi] = 0;
+            if (e.max_depth > out.max_blas_depth) out.max_blas_depth = e.max_depth;
+            out.num_blas_nodes += (size_t)e.num_nodes;
+            out.num_triangles += (size_t)e.num_tris;
+            continue;
         }
         Blas b = build_blas(m);
         ranges[mi] = b.range;
@@ -347,18 +289,10 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
         }
         out.blas_roots.insert(out.blas_roots.end(), root, root + 8);
         for (const BlasTriangle &t : b.tris) {
-            const V3 e1 = t.v1 - t.v0, e2 = t.v2 - t.v0;
-            const float g[12] = {t.v0.x, t.v0.y, t.v0.z, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z, 0.0f, 0.0f, 0.0f};
-            out.tri_geo.insert(out.tri_geo.end(), g, g + 12);
-            // geometric normal of bvh.cpp:277 and the smooth-normal switch of bvh.cpp:281
-            const V3 ng = normalized(cross(t.v1 - t.v0, t.v2 - t.v0));
-            const float smooth = (length_sq(t.n0) > 1e-6f) ? 1.0f : 0.0f;
-            const float a[36] = {ng.x,     ng.y,     ng.z,     smooth,   t.n0.x,  t.n0.y,  t.n0.z,  t.uv0.x,  t.n1.x,
-                                 t.n1.y,   t.n1.z,   t.uv0.y,  t.n2.x,   t.n2.y,  t.n2.z,  t.uv1.x, t.c0.x,   t.c0.y,
-                                 t.c0.z,   t.uv1.y,  t.c1.x,   t.c1.y,   t.c1.z,  t.uv2.x, t.c2.x,  t.c2.y,   t.c2.z,
-                                 t.uv2.y,  t.dpdu.x, t.dpdu.y, t.dpdu.z, as_float(t.material), t.dpdv.x, t.dpdv.y,
-                                 t.dpdv.z, 0.0f};
-            out.tri_attr.insert(out.tri_attr.end(), a, a + 36);
+            float g[kTriGeoFloats], a[kTriAttrFloats];
+            pack_triangle(t, g, a);
+            out.tri_geo.insert(out.tri_geo.end(), g, g + kTriGeoFloats);
+            out.tri_attr.insert(out.tri_attr.end(), a, a + kTriAttrFloats);
         }
         out.num_blas_nodes += b.nodes.size();
         out.num_triangles += b.tris.size();

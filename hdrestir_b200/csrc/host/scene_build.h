@@ -17,6 +17,7 @@
 #include "../../../include/hdrestir.h"
 #include "../device/bvh_layout.h"
 #include "../device/gf.cuh"
+#include "../device/tri_setup.cuh"
 
 namespace hdr {
 
@@ -34,16 +35,6 @@ struct Range3 {  // GfRange3f semantics (default = empty)
     }
     bool empty() const { return mn.x > mx.x || mn.y > mx.y || mn.z > mx.z; }
     V3 size() const { return mx - mn; }
-};
-
-struct BlasTriangle {  // BVHTriangle (bvh.h:22-31)
-    V3 v0, v1, v2;
-    V2 uv0, uv1, uv2;
-    V3 n0, n1, n2;
-    V3 c0, c1, c2;
-    V3 dpdu, dpdv;
-    V3 centroid;
-    int material = -1;
 };
 
 struct BlasNode {  // BVHNode (bvh.h:15-20)
@@ -102,7 +93,17 @@ struct FlatScene {
 constexpr int kMaterialFloats = 48;
 constexpr int kLightFloats = 48;
 
+// A mesh's BLAS built elsewhere (the device build): what the instance records need.
+struct ExternalBlas {
+    int num_nodes = 0, num_tris = 0, max_depth = 0;
+};
+
+Range3 mesh_range(const hdr_mesh_desc &mesh);
 Blas build_blas(const hdr_mesh_desc &mesh);
-bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &err);
+// ext (one per mesh, or null): the BLAS trees and triangle records are not built
+// here; blas_nodes, tri_geo, tri_attr, blas4 and blas_roots stay empty and the
+// instance records take their node and triangle bases from ext's counts.
+bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &err,
+                      const ExternalBlas *ext = nullptr);
 
 }  // namespace hdr

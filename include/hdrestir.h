@@ -235,6 +235,13 @@ typedef struct hdr_gbuffer_texel {
 #define HDR_CTX_SPLIT_STACK 64u  /* phased binary walk keeps its deeper stack entries in local
                                     memory even when the scene's trees are shallow enough for a
                                     shared-memory-only stack; same results (for A/B checks) */
+#define HDR_CTX_DEVICE_BUILD 128u /* hdr_scene_upload builds each mesh's BVH (BVH::Build,
+                                     renderContext/bvh.cpp:66-208) and triangle records on the
+                                     device instead of the host: the same trees, node order and
+                                     triangle order, bit for bit. Binary trees only: not with
+                                     HDR_CTX_WIDE_BVH, and the scene cannot be shared into a
+                                     wide-walk ctx. Its scratch (about 0.5 KB per triangle while
+                                     building) is outside the ctx's HBM budget. */
 
 typedef struct hdr_ctx_desc {
     int32_t device;              /* CUDA ordinal */
@@ -278,6 +285,13 @@ hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src);
  * stack fails with HDR_EINVAL and leaves the ctx without a scene. */
 hdr_status hdr_scene_set_instance_transforms(hdr_ctx *ctx, const float *transforms, int32_t num_instances,
                                              int32_t transforms_on_device);
+
+/* No reference counterpart (inspection and tests): a copy of one of the resident
+ * scene's device arrays, by its DeviceScene field name ("blas_nodes", "tri_geo",
+ * "tri_attr", "instances", "tlas_nodes", "tlas_inst", "materials", "lights", ...).
+ * *size (if not NULL) receives the array's bytes; with dst NULL nothing is copied,
+ * else bytes must equal that size. */
+hdr_status hdr_scene_array(hdr_ctx *ctx, const char *name, void *dst, size_t bytes, size_t *size);
 
 /* RaycastPass::_execute (passes/raycast_pass.cpp:57-162): GBuffer (+AOVs). */
 hdr_status hdr_raycast(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_index, uint32_t aov_mask);
