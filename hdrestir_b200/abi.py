@@ -50,7 +50,8 @@ class MaterialDesc(C.Structure):
                 ("coat_roughness", _f), ("coat_ior", _f), ("sheen", _f), ("sheen_color", _f * 3),
                 ("sheen_roughness", _f), ("subsurface", _f), ("subsurface_color", _f * 3),
                 ("subsurface_radius", _f * 3), ("subsurface_scale", _f), ("subsurface_anisotropy", _f),
-                ("thin_walled", _i), ("diffuse_roughness", _f)]
+                ("thin_walled", _i), ("diffuse_roughness", _f), ("textures", _pf * 4), ("tex_width", _i * 4),
+                ("tex_height", _i * 4)]
 
 
 class LightDesc(C.Structure):

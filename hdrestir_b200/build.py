@@ -23,7 +23,7 @@ INCLUDE = PKG.parent / "include"
 
 SOURCES = ["hdr_abi.cpp", "host/scene_build.cpp", "raycast.cu", "integrate.cu", "wavefront.cu", "accumulate.cu",
            "accumulate_noalloc.cu", "server.cpp", "pathtrace.cu", "spatial.cu", "resolve.cu", "post.cu",
-           "tlas.cu", "blas_build.cu"]
+           "tlas.cu", "blas_build.cu", "wavefront_tex.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [

@@ -283,6 +283,45 @@ def translucent_variant(width=64, height=48):
     return sc, cam
 
 
+def textured_variant(width=64, height=48, seed=7):
+    """The config-2 family with UVs and PreviewSurface textures (diffuse, metallic, roughness,
+    tangent-space normal map; preview_surface.cpp:68-95): the terrain's UVs wrap several
+    times, each sphere material takes one or all four textures. Seeded texels of odd sizes
+    stand in for decoded image files."""
+    import dataclasses
+    rng = np.random.default_rng(seed)
+    sc, cam = config2(width, height, grid=64, n_spheres=80, n_lights=200)
+    ground, sphere = sc.meshes[0], sc.meshes[1]
+    gp = ground.points
+    ext = float(np.abs(gp[:, 0]).max())
+    g_uv = np.stack([gp[:, 0] / ext * 1.7 + 0.3, gp[:, 2] / ext * 2.3 - 0.1], -1).astype(np.float32)
+    sp = sphere.points
+    s_uv = np.stack([np.arctan2(sp[:, 2], sp[:, 0]) / (2 * np.pi) + 0.5,
+                     np.arccos(np.clip(sp[:, 1], -1, 1)) / np.pi], -1).astype(np.float32)
+    sc.meshes[0] = dataclasses.replace(ground, uvs=g_uv)
+    sc.meshes[1] = dataclasses.replace(sphere, uvs=s_uv)
+
+    def tex(h, w, lo=0.0, hi=1.0):
+        base = rng.uniform(lo, hi, (h, w, 3)).astype(np.float32)
+        return (0.5 * base + 0.5 * np.roll(base, 1, axis=1)).astype(np.float32)
+
+    def normal_map(h, w):
+        t = rng.normal(0.0, 0.25, (h, w, 2))
+        return np.concatenate([0.5 + 0.5 * t, np.ones((h, w, 1))], -1).astype(np.float32)
+
+    kinds = [dict(diffuse_texture=tex(37, 23)),
+             dict(metallic_texture=tex(16, 16), roughness_texture=tex(9, 31, 0.05, 1.0)),
+             dict(normal_texture=normal_map(24, 24), roughness=0.2),
+             dict(diffuse_texture=tex(5, 7), metallic_texture=tex(3, 3), roughness_texture=tex(12, 4, 0.1, 0.9),
+                  normal_texture=normal_map(19, 13))]
+    g_mat = sc.instances[0].material
+    sc.materials[g_mat] = dataclasses.replace(sc.materials[g_mat], diffuse_texture=tex(64, 48),
+                                              roughness_texture=tex(33, 17, 0.2, 1.0))
+    for k, inst in enumerate(sc.instances[1:]):
+        sc.materials[inst.material] = dataclasses.replace(sc.materials[inst.material], **kinds[k % len(kinds)])
+    return sc, cam
+
+
 def orbit_camera(angle: float, width: int, height: int) -> Camera:
     """Config-2 camera on a circle of radius 22 at height 9 around the terrain centre."""
     eye = (22.0 * np.sin(angle), 9.0, 22.0 * np.cos(angle))

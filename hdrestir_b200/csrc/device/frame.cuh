@@ -186,6 +186,25 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
                          GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_level,
                          unsigned *err, cudaStream_t st, const TraceTuning &tune, cudaEvent_t *ev_begin = nullptr,
                          cudaEvent_t *ev_end = nullptr);
+// The same launchers with the closures' texture overrides compiled in
+// (wavefront_tex.cu); the ones above leave them out, for scenes without textures.
+namespace textured {
+int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &tune, unsigned *err, cudaStream_t st,
+                      cudaEvent_t *ev_begin = nullptr, cudaEvent_t *ev_end = nullptr);
+int launch_winner_visibility(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                             GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, unsigned *err,
+                             cudaStream_t st, const TraceTuning &tune);
+int launch_ris_generate(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                        GBufferView gb, WaveBuffers wb, float4 *color, int trace_level, unsigned *err,
+                        cudaStream_t st);
+int launch_ris_shade(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                     GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_level, unsigned *err,
+                     cudaStream_t st, const TraceTuning &tune);
+int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
+                         GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, int trace_level,
+                         unsigned *err, cudaStream_t st, const TraceTuning &tune, cudaEvent_t *ev_begin = nullptr,
+                         cudaEvent_t *ev_end = nullptr);
+}  // namespace textured
 
 void launch_raycast(const DeviceScene &s, const CameraD &cam, int frame_index, GBufferView gb, AovView aov,
                     unsigned *err, cudaStream_t st);

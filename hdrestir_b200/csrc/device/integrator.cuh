@@ -143,8 +143,15 @@ __device__ inline bool load_gbuffer_hit(const DeviceScene &s, const GBufferView 
     h.smooth_normal = V3{c.x, c.y, c.z};
     h.tri = fbits(c.w);
     h.albedo = V3{d.x, d.y, d.z};
-    h.uv = V2{d.w, 0.0f};
-    h.dpdu = h.dpdv = v3s(0.0f);
+    if (s.has_textures) {  // a texture lookup needs uv.y and the tangents (the only readers of them)
+        const float4 e = gb.aux0[i], f = gb.aux1[i];
+        h.uv = V2{d.w, e.x};
+        h.dpdu = V3{e.y, e.z, e.w};
+        h.dpdv = V3{f.x, f.y, f.z};
+    } else {
+        h.uv = V2{d.w, 0.0f};
+        h.dpdu = h.dpdv = v3s(0.0f);
+    }
     const float4 r = __ldg(&s.instances[8 * h.prim + 6]);
     const float4 r7 = __ldg(&s.instances[8 * h.prim + 7]);
     h.material = fbits(r.w);

@@ -11,6 +11,13 @@
 // receives the first draw (same for SampleCosineHemisphere).
 #pragma once
 
+// HDR_TEXTURES 0 compiles closures without the texture overrides: the translation
+// unit's kernels then serve scenes without textures only (the host picks them by
+// DeviceScene::has_textures).
+#ifndef HDR_TEXTURES
+#define HDR_TEXTURES 1
+#endif
+
 #include "rng.cuh"
 #include "spectrum.cuh"
 #include "traverse.cuh"
@@ -24,6 +31,55 @@ struct Closure {
     bool thin_walled;
     bool is_default;  // DefaultMaterial: cosine-only SampleBounce
 };
+
+// BoundTextureSampler::Sample (scene/image_texture_sampler.h:41-68): bilinear, u wrapped,
+// v wrapped and flipped, texel (x, y) at (y * width + x) * 3. Corner indices are clamped to
+// the texture, which changes nothing for a finite uv (the reference has no defined texel
+// for a non-finite one).
+__device__ __forceinline__ V3 texture_sample(const float *tex, int w, int h, V2 uv) {
+    const float u = uv.x - floorf(uv.x);
+    const float v = 1.0f - (uv.y - floorf(uv.y));
+    const float px = u * (float)(w - 1);
+    const float py = v * (float)(h - 1);
+    const int x0 = sclampi((int)floorf(px), 0, w - 1);
+    const int y0 = sclampi((int)floorf(py), 0, h - 1);
+    const int x1 = smini(x0 + 1, w - 1);
+    const int y1 = smini(y0 + 1, h - 1);
+    const float fx = px - (float)x0;
+    const float fy = py - (float)y0;
+    auto texel = [&](int x, int y) {
+        const float *t = tex + (size_t)((y * w + x) * 3);
+        return V3{__ldg(t), __ldg(t + 1), __ldg(t + 2)};
+    };
+    return (texel(x0, y0) * (1 - fx) + texel(x1, y0) * fx) * (1 - fy) +
+           (texel(x0, y1) * (1 - fx) + texel(x1, y1) * fx) * fy;
+}
+
+struct TexturedParams {
+    V3 base_color;
+    float metallic, roughness;
+    V3 normal;
+};
+
+// The texture overrides of PreviewSurfaceMaterial::GetClosure (preview_surface.cpp:68-95);
+// out of line so the kernels of untextured scenes keep their registers.
+static __device__ __forceinline__ TexturedParams apply_textures(const float *textures, int4 off, int4 tw, int4 th, V2 uv,
+                                                      V3 smooth_normal, V3 dpdu, V3 dpdv, TexturedParams p) {
+    if (off.x >= 0) p.base_color = cmul(p.base_color, texture_sample(textures + off.x, tw.x, th.x, uv));
+    if (off.y >= 0) p.metallic = texture_sample(textures + off.y, tw.y, th.y, uv).x;
+    if (off.z >= 0) p.roughness = texture_sample(textures + off.z, tw.z, th.z, uv).x;
+    if (off.w >= 0) {  // tangent-space normal map
+        V3 nt = texture_sample(textures + off.w, tw.w, th.w, uv);
+        nt = nt * 2.0f - v3s(1.0f);
+        const V3 n = smooth_normal;
+        V3 t = dpdu, b = dpdv;
+        t = normalized(t - n * dot(t, n));
+        b = normalized(b - n * dot(b, n) - t * dot(b, t));
+        if (dot(cross(n, t), b) < 0.0f) b = -b;
+        p.normal = normalized(t * nt.x + b * nt.y + n * nt.z);
+    }
+    return p;
+}
 
 __device__ __forceinline__ Closure get_closure(const DeviceScene &s, const Hit &h) {
     Closure c;
@@ -79,6 +135,22 @@ __device__ __forceinline__ Closure get_closure(const DeviceScene &s, const Hit &
     c.sheen_roughness = m8.z;
     c.normal = h.smooth_normal;
     c.is_default = false;
+#if HDR_TEXTURES
+    if (!s.has_textures) return c;
+    const float4 m9 = __ldg(m + 9);  // texture offsets, -1 = none
+    const int4 off = make_int4(fbits(m9.x), fbits(m9.y), fbits(m9.z), fbits(m9.w));
+    if ((off.x & off.y & off.z & off.w) != -1) {
+        const float4 m10 = __ldg(m + 10), m11 = __ldg(m + 11);
+        const TexturedParams t = apply_textures(
+            s.textures, off, make_int4(fbits(m10.x), fbits(m10.y), fbits(m10.z), fbits(m10.w)),
+            make_int4(fbits(m11.x), fbits(m11.y), fbits(m11.z), fbits(m11.w)), h.uv, h.smooth_normal, h.dpdu,
+            h.dpdv, TexturedParams{c.base_color, c.metallic, c.roughness, c.normal});
+        c.base_color = t.base_color;
+        c.metallic = t.metallic;
+        c.roughness = t.roughness;
+        c.normal = t.normal;
+    }
+#endif
     return c;
 }
 

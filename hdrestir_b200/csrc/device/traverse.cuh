@@ -31,6 +31,7 @@ struct DeviceScene {
     const float4 *tlas_nodes;  // 2 per node
     const int *tlas_inst;
     const float4 *materials;   // 12 per material
+    const float *textures;     // material texels (RGB f32), located by the material records
     const float4 *lights;      // 12 per light
     const float *dome_pixels;
     const float *dome_row_cdf;
@@ -50,6 +51,7 @@ struct DeviceScene {
     int wide;                  // 1: walk the wide trees, 0: the binary ones (same results)
     int proper_boxes;          // 1: no node box of any tree is empty (min > max on some axis)
     int shallow;               // 1: the binary walk's stack never exceeds kShallowStack entries
+    int has_textures;          // 1: some material has a texture (closures read uv and tangents)
     // This struct's own copy in device memory. Kernels take the scene by value
     // (parameter space); a non-inlined callee gets this pointer instead of the
     // parameter's address, which would make every thread copy the parameter

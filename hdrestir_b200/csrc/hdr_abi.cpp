@@ -564,6 +564,7 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     UP(f.tlas_nodes, tlas_nodes);
     UP(f.tlas_inst, tlas_inst);
     UP(f.materials, materials);
+    UP(f.textures, textures);
     UP(f.lights, lights);
     UP(f.dome_pixels, dome_pixels);
     UP(f.dome_row_cdf, dome_row_cdf);
@@ -608,6 +609,7 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     s.has_tlas = f.num_instances > 0 ? 1 : 0;
     s.proper_boxes = (store->blas_proper && tlas_boxes_proper(f)) ? 1 : 0;
     s.shallow = (f.max_blas_depth + f.max_tlas_depth + 4 <= hdr::kShallowStack) ? 1 : 0;
+    s.has_textures = f.textures.empty() ? 0 : 1;
     // the descriptor itself, for callees that are not inlined into a kernel
     hdr::DeviceScene copies[2] = {s, s};
     {
@@ -806,7 +808,7 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
         if (timed)
             for (int k = kSlotWaveFirst; k < kSlotWaveFirst + 4; ++k)
                 if ((st = fold_pass_time(c, k)) != HDR_OK) return st;
-        const int n = hdr::launch_ris_wavefront(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color,
+        const int n = (c->scene.has_textures ? hdr::textured::launch_ris_wavefront : hdr::launch_ris_wavefront)(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color,
                                                 trace_level, c->d_err, c->stream, c->tune,
                                                 timed ? c->ev_start + kSlotWaveFirst : nullptr,
                                                 timed ? c->ev_stop + kSlotWaveFirst : nullptr);
@@ -821,7 +823,7 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
                 return fail(HDR_ECUDA, "spatial reuse launch failed: %s", cudaGetErrorString(cudaGetLastError()));
             HDR_CUDA(cudaMemcpyAsync(rv.dir_dist, rv_spatial.dir_dist, count * kResPlanes * sizeof(float4),
                                      cudaMemcpyDeviceToDevice, c->stream));
-            if (hdr::launch_winner_visibility(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color, c->d_err,
+            if ((c->scene.has_textures ? hdr::textured::launch_winner_visibility : hdr::launch_winner_visibility)(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color, c->d_err,
                                               c->stream, c->tune) < 0)
                 return fail(HDR_ECUDA, "winner visibility launch failed: %s", cudaGetErrorString(cudaGetLastError()));
             c->launches += 3;
@@ -1133,7 +1135,7 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
         wb.n_shadow = j.n_shadow;
         wb.slot_base_closest = (int)base_c[(size_t)i];
         wb.slot_base_shadow = (int)base_s[(size_t)i];
-        if (hdr::launch_ris_generate(lead->scene, j.cd, j.frame, j.d, j.gb, wb, j.color, j.trace_level, j.c->d_err,
+        if ((lead->scene.has_textures ? hdr::textured::launch_ris_generate : hdr::launch_ris_generate)(lead->scene, j.cd, j.frame, j.d, j.gb, wb, j.color, j.trace_level, j.c->d_err,
                                      s) < 0)
             return fail(HDR_ECUDA, "generate launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     }
@@ -1141,7 +1143,7 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
         return fail(HDR_ECUDA, "trace launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     for (int32_t i = 0; i < n; ++i) {
         const RisJob &j = jobs[(size_t)i];
-        if (hdr::launch_ris_shade(lead->scene, j.cd, j.frame, j.d, j.gb, j.rv, wbs[(size_t)i], j.color, j.trace_level,
+        if ((lead->scene.has_textures ? hdr::textured::launch_ris_shade : hdr::launch_ris_shade)(lead->scene, j.cd, j.frame, j.d, j.gb, j.rv, wbs[(size_t)i], j.color, j.trace_level,
                                   j.c->d_err, s, lead->tune) < 0)
             return fail(HDR_ECUDA, "shade launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     }

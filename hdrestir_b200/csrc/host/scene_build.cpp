@@ -366,6 +366,23 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
                              p.coat_roughness, p.coat_ior, p.sheen_roughness, p.roughness,
                              0.0f, 0.0f, 0.0f, 0.0f};
         std::memcpy(r, v, sizeof(v));
+        // textures (preview_surface.cpp:68-95): float offset into `textures` (-1 = none), width, height
+        for (int k = 0; k < 4; ++k) {
+            int off = -1;
+            const int w = p.tex_width[k], h = p.tex_height[k];
+            if (p.textures[k] && w > 0 && h > 0) {
+                const size_t n = (size_t)w * (size_t)h * 3;
+                if (out.textures.size() + n > (size_t)0x7fffffff || (size_t)w * (size_t)h > (size_t)0x7fffffff / 3) {
+                    err = "material " + std::to_string(i) + ": textures exceed 2^31 floats";
+                    return false;
+                }
+                off = (int)out.textures.size();
+                out.textures.insert(out.textures.end(), p.textures[k], p.textures[k] + n);
+            }
+            r[36 + k] = as_float(off);
+            r[40 + k] = as_float(off >= 0 ? w : 0);
+            r[44 + k] = as_float(off >= 0 ? h : 0);
+        }
     }
     // ---- lights (rect_light.cpp, point_light.cpp, distant_light.cpp, dome_light.cpp)
     out.num_lights = desc.num_lights;

@@ -80,6 +80,7 @@ struct FlatScene {
     std::vector<int> tlas_inst;
     std::vector<float> mesh_ranges; // 6 floats per mesh: MeshSubset::range min.xyz, max.xyz
     std::vector<float> materials;   // kMaterialFloats per material
+    std::vector<float> textures;    // every material texture's RGB texels, back to back
     std::vector<float> lights;      // kLightFloats per light
     std::vector<float> dome_pixels, dome_row_cdf, dome_col_cdf;
     int dome_width = 0, dome_height = 0;

@@ -27,10 +27,20 @@
 // candidate's weight. Generate then only advances the stream past those
 // candidates, and shade counts them as misses and continues from the stream
 // state generate saved.
+// Compiled twice: here (namespace hdr) with closures that leave the texture code
+// out, for scenes without textures, and in wavefront_tex.cu (namespace
+// hdr::textured) with it. Untextured frames keep the registers they had.
+#ifndef HDR_WAVE_TEXTURED
+#define HDR_TEXTURES 0
+#endif
+
 #include "device/integrator.cuh"
 #include "device/pixel.cuh"
 
 namespace hdr {
+#ifdef HDR_WAVE_TEXTURED
+namespace textured {
+#endif
 
 __device__ __forceinline__ int queue_append(int *counter, bool want) {
     const unsigned active = __activemask();
@@ -516,19 +526,24 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
     if (cudaMemsetAsync(wb.counts, 0, (wb.q_winner ? 6 : 4) * sizeof(int), st) != cudaSuccess) return -1;
     auto mark = [&](cudaEvent_t *ev, int k) { return !ev || cudaEventRecord(ev[k], st) == cudaSuccess; };
     if (!mark(ev_begin, 0)) return -1;
-    if (launch_ris_generate(s, cam, frame_index, p, gb, wb, color, trace_level, err, st) < 0) return -1;
+    // callee names in parentheses: no argument-dependent lookup, so the hdr::textured build
+    // calls its own launchers, not hdr::'s
+    if ((launch_ris_generate)(s, cam, frame_index, p, gb, wb, color, trace_level, err, st) < 0) return -1;
     if (!mark(ev_end, 0)) return -1;
-    if (launch_wave_trace(s, wb, tune, err, st, ev_begin ? ev_begin + 1 : nullptr, ev_end ? ev_end + 1 : nullptr) < 0)
+    if ((launch_wave_trace)(s, wb, tune, err, st, ev_begin ? ev_begin + 1 : nullptr, ev_end ? ev_end + 1 : nullptr) < 0)
         return -1;
     if (!mark(ev_begin, 3)) return -1;
-    if (launch_ris_shade(s, cam, frame_index, p, gb, rv, wb, color, trace_level, err, st, tune) < 0) return -1;
+    if ((launch_ris_shade)(s, cam, frame_index, p, gb, rv, wb, color, trace_level, err, st, tune) < 0) return -1;
     int launches = 4;
     if (wb.q_winner) {  // the winners' shadow rays, then the pixels they found occluded
-        if (launch_winner_visibility(s, cam, frame_index, p, gb, rv, wb, color, err, st, tune) < 0) return -1;
+        if ((launch_winner_visibility)(s, cam, frame_index, p, gb, rv, wb, color, err, st, tune) < 0) return -1;
         launches += 2;
     }
     if (!mark(ev_end, 3)) return -1;
     return launches;
 }
 
+#ifdef HDR_WAVE_TEXTURED
+}  // namespace textured
+#endif
 }  // namespace hdr

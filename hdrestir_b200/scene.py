@@ -57,6 +57,15 @@ class Material:  # PreviewSurfaceParams defaults (materials/preview_surface_para
     subsurface: float = 0.0
     subsurface_color: tuple = (1.0, 1.0, 1.0)
     thin_walled: bool = False
+    # (H, W, 3) f32 texels as ImageTextureSamplerFactory decodes them, or None
+    # (DiffuseTexture / MetallicTexture / RoughnessTexture / NormalTexture, preview_surface_params.h:48-51)
+    diffuse_texture: np.ndarray | None = None
+    metallic_texture: np.ndarray | None = None
+    roughness_texture: np.ndarray | None = None
+    normal_texture: np.ndarray | None = None
+
+
+TEXTURE_FIELDS = ("diffuse_texture", "metallic_texture", "roughness_texture", "normal_texture")
 
 
 @dataclass
@@ -125,6 +134,8 @@ class Scene:
         for k, m in enumerate(self.materials):
             d = mats[k]
             for f in Material.__dataclass_fields__:
+                if f in TEXTURE_FIELDS:
+                    continue
                 v = getattr(m, f)
                 if isinstance(v, tuple):
                     getattr(d, f)[:] = [float(x) for x in v]
@@ -135,6 +146,16 @@ class Scene:
             d.subsurface_scale = 1.0
             d.subsurface_anisotropy = 0.0
             d.diffuse_roughness = 0.0
+            for slot, f in enumerate(TEXTURE_FIELDS):
+                tex = getattr(m, f)
+                if tex is None:
+                    continue
+                tex = np.ascontiguousarray(tex, np.float32)
+                if tex.ndim != 3 or tex.shape[2] != 3:
+                    raise ValueError(f"{f}: (H, W, 3) texels expected")
+                keep.append(tex)
+                d.textures[slot] = tex.ctypes.data_as(C.POINTER(C.c_float))
+                d.tex_height[slot], d.tex_width[slot] = tex.shape[0], tex.shape[1]
         lights = (abi.LightDesc * max(1, len(self.lights)))()
         for k, L in enumerate(self.lights):
             d = lights[k]

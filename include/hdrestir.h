@@ -104,7 +104,17 @@ typedef struct hdr_material_desc { /* PreviewSurfaceParams field for field */
     float subsurface_anisotropy;
     int32_t thin_walled;
     float diffuse_roughness;
+    /* PreviewSurfaceParams DiffuseTexture / MetallicTexture / RoughnessTexture /
+     * NormalTexture (materials/preview_surface_params.h:48-51), indexed by HDR_TEX_*,
+     * as the RGB f32 texels ImageTextureSamplerFactory decodes for them
+     * (scene/image_texture_sampler.cpp:14-123): width*height*3 floats, row 0 first;
+     * the diffuse texture in its sRGB-decoded variant (Linear = false), the other
+     * three linear. NULL (or a zero size) = no texture, the parameter is used. */
+    const float *textures[4];
+    int32_t tex_width[4], tex_height[4];
 } hdr_material_desc;
+
+enum { HDR_TEX_DIFFUSE = 0, HDR_TEX_METALLIC = 1, HDR_TEX_ROUGHNESS = 2, HDR_TEX_NORMAL = 3 };
 
 /* LightType order of scene/light_factory.h */
 enum { HDR_LIGHT_DISTANT = 0, HDR_LIGHT_DOME = 1, HDR_LIGHT_RECT = 2, HDR_LIGHT_POINT = 3 };

@@ -421,6 +421,18 @@ orc_scene *orc_scene_create(const hdr_scene_desc *d) {
     s->n_mat = d->num_materials;
     s->mat = (hdr_material_desc *)calloc((size_t)(d->num_materials > 0 ? d->num_materials : 1), sizeof(hdr_material_desc));
     if (d->num_materials > 0) memcpy(s->mat, d->materials, (size_t)d->num_materials * sizeof(hdr_material_desc));
+    for (int i = 0; i < d->num_materials; ++i) /* the texels are copied: the scene outlives the caller's arrays */
+        for (int k = 0; k < 4; ++k) {
+            hdr_material_desc *m = &s->mat[i];
+            if (!m->textures[k] || m->tex_width[k] <= 0 || m->tex_height[k] <= 0) {
+                m->textures[k] = NULL;
+                continue;
+            }
+            const size_t n = (size_t)m->tex_width[k] * (size_t)m->tex_height[k] * 3;
+            float *copy = (float *)malloc(n * sizeof(float));
+            memcpy(copy, m->textures[k], n * sizeof(float));
+            m->textures[k] = copy;
+        }
     s->n_lights = d->num_lights;
     s->lights = (olight *)calloc((size_t)(d->num_lights > 0 ? d->num_lights : 1), sizeof(olight));
     s->env = -1;
@@ -461,6 +473,8 @@ void orc_scene_destroy(orc_scene *s) {
     free(s->inst);
     free(s->tlas);
     free(s->tlas_idx);
+    for (int i = 0; i < s->n_mat; ++i)
+        for (int k = 0; k < 4; ++k) free((void *)s->mat[i].textures[k]);
     free(s->mat);
     free(s->lights);
     free(s);

@@ -20,7 +20,25 @@ typedef struct {
     int thin, is_default;
 } oclosure;
 
-/* PreviewSurfaceMaterial::GetClosure (preview_surface.cpp:61-127, no textures) /
+/* BoundTextureSampler::Sample (scene/image_texture_sampler.h:41-68): bilinear, u wrapped,
+ * v wrapped and flipped; (1 - fx) etc. are float, each product rounds once. */
+static ov3 tex_sample(const float *px, int w, int h, ov2 uv) {
+    const float u = uv.x - floorf(uv.x);
+    const float v = 1.0f - (uv.y - floorf(uv.y));
+    const float fxp = u * (float)(w - 1);
+    const float fyp = v * (float)(h - 1);
+    const int x0 = (int)floorf(fxp), y0 = (int)floorf(fyp);
+    const int x1 = x0 + 1 < w - 1 ? x0 + 1 : w - 1;
+    const int y1 = y0 + 1 < h - 1 ? y0 + 1 : h - 1;
+    const float fx = fxp - (float)x0, fy = fyp - (float)y0;
+#define TX(x, y) V(px[((y) * w + (x)) * 3], px[((y) * w + (x)) * 3 + 1], px[((y) * w + (x)) * 3 + 2])
+    const ov3 top = vadd(vmulf(TX(x0, y0), 1 - fx), vmulf(TX(x1, y0), fx));
+    const ov3 bot = vadd(vmulf(TX(x0, y1), 1 - fx), vmulf(TX(x1, y1), fx));
+#undef TX
+    return vadd(vmulf(top, 1 - fy), vmulf(bot, fy));
+}
+
+/* PreviewSurfaceMaterial::GetClosure (preview_surface.cpp:61-127, textures at 68-95) /
  * DefaultMaterial::GetClosure (default_material.cpp:55-64) */
 static oclosure closure_of(const orc_scene *s, const ohit *h) {
     oclosure c;
@@ -77,6 +95,22 @@ static oclosure closure_of(const orc_scene *s, const ohit *h) {
     c.opacity = p->opacity;
     c.thin = p->thin_walled != 0;
     c.is_default = 0;
+    if (p->textures[HDR_TEX_DIFFUSE])
+        c.base = vcmul(c.base, tex_sample(p->textures[0], p->tex_width[0], p->tex_height[0], h->uv));
+    if (p->textures[HDR_TEX_METALLIC])
+        c.metallic = tex_sample(p->textures[1], p->tex_width[1], p->tex_height[1], h->uv).x;
+    if (p->textures[HDR_TEX_ROUGHNESS])
+        c.roughness = tex_sample(p->textures[2], p->tex_width[2], p->tex_height[2], h->uv).x;
+    if (p->textures[HDR_TEX_NORMAL]) {
+        ov3 nt = tex_sample(p->textures[3], p->tex_width[3], p->tex_height[3], h->uv);
+        nt = vsub(vmulf(nt, 2.0f), V(1.0f, 1.0f, 1.0f));
+        const ov3 n = h->smooth_normal;
+        ov3 t = h->dpdu, b = h->dpdv;
+        t = vnorm(vsub(t, vmulf(n, vdot(t, n))));
+        b = vnorm(vsub(vsub(b, vmulf(n, vdot(b, n))), vmulf(t, vdot(b, t))));
+        if (vdot(vcross(n, t), b) < 0.0f) b = vneg(b);
+        c.normal = vnorm(vadd(vadd(vmulf(t, nt.x), vmulf(b, nt.y)), vmulf(n, nt.z)));
+    }
     return c;
 }
 

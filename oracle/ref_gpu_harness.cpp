@@ -11,11 +11,6 @@
 #include "render_pipeline.h"
 #include "scene.h"
 
-// Texture loading is out of scope; the factory's loader is referenced by the scene code.
-const Restir::detail::Texture *Restir::ImageTextureSamplerFactory::_getOrLoad(std::string_view, bool) const {
-    return nullptr;
-}
-
 using namespace Restir;
 
 struct ref_gpu_params {

@@ -34,9 +34,9 @@
 
 using namespace Restir;
 
-// Texture loading is out of scope (no benchmark scene uses textures); the
-// factory's loader is the only ImageTextureSamplerFactory symbol referenced.
-const detail::Texture *ImageTextureSamplerFactory::_getOrLoad(std::string_view, bool) const { return nullptr; }
+// Material textures load through the reference's own ImageTextureSamplerFactory
+// (scene/image_texture_sampler.cpp, compiled in), reading the HioImage stand-in,
+// where this harness registers each material's texels.
 
 namespace {
 
@@ -150,6 +150,15 @@ RefScene *ref_create(const hdr_scene_desc *d) {
             q.Subsurface = p.subsurface;
             q.SubsurfaceColor = GfVec3f(p.subsurface_color[0], p.subsurface_color[1], p.subsurface_color[2]);
             q.ThinWalled = p.thin_walled != 0;
+            // textures: registered in the HioImage stand-in under a path the material names; the
+            // reference's own ImageTextureSamplerFactory loads them from there
+            SdfAssetPath *slots[4] = {&q.DiffuseTexture, &q.MetallicTexture, &q.RoughnessTexture, &q.NormalTexture};
+            for (int t = 0; t < 4; ++t) {
+                if (!p.textures[t] || p.tex_width[t] <= 0 || p.tex_height[t] <= 0) continue;
+                const std::string path = "mem://" + path_of("mat", k) + "/tex" + std::to_string(t);
+                HioImage::Register(path, p.tex_width[t], p.tex_height[t], p.textures[t]);
+                *slots[t] = SdfAssetPath(path);
+            }
             rs->scene.SetMaterialParams(SdfPath(path_of("mat", k)), q);
         }
         for (int i = 0; i < d->num_instances; ++i) {

@@ -13,7 +13,27 @@
 
 PXR_NAMESPACE_OPEN_SCOPE
 
-enum HioFormat { HioFormatInvalid = -1, HioFormatFloat32Vec3 = 1 };
+// The formats ImageTextureSamplerFactory distinguishes; registered images are Float32Vec3.
+enum HioFormat {
+    HioFormatInvalid = -1,
+    HioFormatUNorm8, HioFormatUNorm8Vec2, HioFormatUNorm8Vec3, HioFormatUNorm8Vec4,
+    HioFormatUNorm8srgb, HioFormatUNorm8Vec2srgb, HioFormatUNorm8Vec3srgb, HioFormatUNorm8Vec4srgb,
+    HioFormatFloat16, HioFormatFloat16Vec2, HioFormatFloat16Vec3, HioFormatFloat16Vec4,
+    HioFormatFloat32, HioFormatFloat32Vec2, HioFormatFloat32Vec3, HioFormatFloat32Vec4,
+};
+
+inline int HioGetComponentCount(HioFormat f) {
+    switch (f) {
+    case HioFormatUNorm8: case HioFormatUNorm8srgb: case HioFormatFloat16: case HioFormatFloat32: return 1;
+    case HioFormatUNorm8Vec2: case HioFormatUNorm8Vec2srgb: case HioFormatFloat16Vec2: case HioFormatFloat32Vec2:
+        return 2;
+    case HioFormatUNorm8Vec3: case HioFormatUNorm8Vec3srgb: case HioFormatFloat16Vec3: case HioFormatFloat32Vec3:
+        return 3;
+    case HioFormatUNorm8Vec4: case HioFormatUNorm8Vec4srgb: case HioFormatFloat16Vec4: case HioFormatFloat32Vec4:
+        return 4;
+    default: return 0;
+    }
+}
 
 class HioImage;
 using HioImageSharedPtr = std::shared_ptr<HioImage>;

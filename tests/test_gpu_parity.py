@@ -629,3 +629,32 @@ def test_spatial_reuse_queued_visibility_is_deterministic():
                 frames.append(ctx.download("Color").copy())
             outs.append(np.stack(frames))
     assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+
+
+@pytest.mark.parametrize("kw", [dict(ris=True, candidate_count=16, use_reservoir=True, max_depth=1),
+                                dict(ris=True, candidate_count=8, use_reservoir=True, max_depth=3),
+                                dict(ris=False, max_depth=4)])
+def test_textured_scene_matches_oracle(gpu_ctx, kw):
+    """PreviewSurface textures (diffuse, metallic, roughness, normal maps) through the wavefront
+    RIS pass, the one-thread RIS form and path tracing; against the oracle, which is pinned to
+    the reference's own texture sampler."""
+    sc, cam = configs.textured_variant(96, 64)
+    gpu_ctx.upload_scene(sc)
+    gpu_ctx.clear_persistent()
+    orc = Oracle(sc)
+    kw = dict(kw)
+    ris = kw.pop("ris")
+    for frame in range(2):
+        gpu_ctx.raycast(cam, frame)
+        if ris:
+            gpu_ctx.ris_path_trace(cam, frame, **kw)
+        else:
+            gpu_ctx.path_trace(cam, frame, **kw)
+        gpu = gpu_ctx.download("Color")
+        orc.raycast(cam, frame)
+        ref, _ = orc.integrate(cam, frame, ris=ris, **kw)
+        if ris:
+            assert np.array_equal(gpu_ctx.download("__ris_reservoir")[4, :, 2].view(np.int32), orc.res["m"])
+        frac = _color_outliers(gpu, ref)
+        print(f"textured {kw}, frame {frame}: outlier fraction {frac:.4f}")
+        assert frac <= MAX_OUTLIERS

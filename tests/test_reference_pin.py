@@ -161,3 +161,30 @@ def test_oracle_equals_reference_translucent(kw):
         o.accumulate(cam, f, firefly=True)
         assert np.array_equal(bits(o.color), bits(c))
         assert np.array_equal(o.res["m"], r["m"])
+
+
+@pytest.mark.parametrize("kw", [dict(ris=True, candidate_count=8, use_reservoir=True, max_depth=1),
+                                dict(ris=False, max_depth=4)])
+def test_oracle_equals_reference_textured(kw):
+    """PreviewSurface textures: diffuse, metallic, roughness and normal maps, sampled by the
+    reference's own BoundTextureSampler from texels its ImageTextureSamplerFactory loads
+    (preview_surface.cpp:68-95, image_texture_sampler.h:41-68)."""
+    import dataclasses
+
+    from hdrestir_b200.scene import TEXTURE_FIELDS
+
+    sc, cam = configs.textured_variant(40, 30)
+    ref = refharness.Reference(sc)
+    o = orc.Oracle(sc, threads=4)
+    for f in range(2):
+        g, c, r = ref.render(cam, f, accumulate=True, firefly=True, **kw)
+        assert np.array_equal(o.raycast(cam, f)["prim_id"], g["prim_id"])
+        o.integrate(cam, f, **kw)
+        o.accumulate(cam, f, firefly=True)
+        assert np.array_equal(bits(o.color), bits(c))
+        assert np.array_equal(o.res["m"], r["m"])
+    # the textures take effect on both sides
+    plain = dataclasses.replace(sc, materials=[dataclasses.replace(m, **{k: None for k in TEXTURE_FIELDS})
+                                               for m in sc.materials])
+    _, c_plain, _ = refharness.Reference(plain).render(cam, 1, accumulate=True, firefly=True, **kw)
+    assert np.abs(c_plain[..., :3] - c[..., :3]).mean() > 1e-3 * np.abs(c[..., :3]).mean()
