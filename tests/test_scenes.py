@@ -39,3 +39,29 @@ def test_blackbody_normalised():
     lum = rgb @ np.array([0.2126, 0.7152, 0.0722])
     np.testing.assert_allclose(lum, 1.0, rtol=1e-12)
     assert rgb[0, 0] > rgb[0, 2] and rgb[2, 2] > rgb[2, 0]  # warm vs cool
+
+
+def test_textured_variant_descriptor():
+    """Texture arrays reach hdr_material_desc: pointer, width and height per slot (HDR_TEX_*),
+    untextured slots NULL; the descriptor keeps the texel arrays alive."""
+    import ctypes as C
+
+    from hdrestir_b200 import abi
+    from hdrestir_b200.scene import TEXTURE_FIELDS
+
+    sc, _ = configs.textured_variant(16, 16)
+    desc = sc.c_desc()
+    seen = 0
+    for k, m in enumerate(sc.materials):
+        d = desc.materials[k]
+        for slot, f in enumerate(TEXTURE_FIELDS):
+            tex = getattr(m, f)
+            if tex is None:
+                assert not d.textures[slot]
+                continue
+            seen += 1
+            assert (d.tex_height[slot], d.tex_width[slot]) == tex.shape[:2]
+            got = np.ctypeslib.as_array(d.textures[slot], shape=(tex.size,))
+            assert np.array_equal(got, np.ascontiguousarray(tex, np.float32).reshape(-1))
+    assert seen >= 8
+    assert C.sizeof(abi.MaterialDesc) % 8 == 0
