@@ -11,6 +11,9 @@ Outputs (small, committed):
                      of the reference passes on test-sized variants of the
                      benchmark scenes, frames 0-2
   reservoir_kat.npz  WeightedReservoir known answers (tests/test_reservoir.cpp)
+  frames_textured.npz
+                     the same for the textured config-2 variant (PreviewSurface
+                     diffuse / metallic / roughness / normal textures), frames 0-1
 """
 from __future__ import annotations
 
@@ -35,8 +38,21 @@ CASES = {
         dict(ris=True, candidate_count=32, use_reservoir=True, max_depth=1)),
 }
 FRAMES = 3
+TEXTURED = (dict(width=32, height=24), dict(ris=True, candidate_count=16, use_reservoir=True, max_depth=1))
 RNG_SEEDS = np.array([0, 1, 7, 1234 ^ 56, 0xFFFFFFFF, 0xC0FFEE00, 12345 * 3 ^ 77] + list(range(1000, 1025)), np.uint32)
 RNG_COUNT = 700
+
+
+def textured():
+    scene_kw, kw = TEXTURED
+    sc, cam = configs.textured_variant(**scene_kw)
+    ref = refharness.Reference(sc)
+    out = {}
+    for f in range(2):
+        g, c, r = ref.render(cam, f, accumulate=True, firefly=True, **kw)
+        out[f"gbuf{f}"], out[f"color{f}"], out[f"res{f}"] = g, c, r
+    np.savez_compressed(HERE / "frames_textured.npz", **out)
+    ref.close()
 
 
 def main():
@@ -56,8 +72,13 @@ def main():
             out[f"gbuf{f}"], out[f"color{f}"], out[f"res{f}"] = g, c, r
         np.savez_compressed(HERE / f"frames_cfg{cfg}.npz", **out)
         ref.close()
+    textured()
     print("golden fixtures written to", HERE)
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["textured"]:  # only the textured fixture
+        refharness.build()
+        textured()
+    else:
+        main()

@@ -71,3 +71,21 @@ def test_frames_match_reference(cfg):
             lc = s & (r["has_lc"] == 1)
             for field in RES_FIELDS_LIGHT:
                 assert np.array_equal(bits(o.res[field][lc]), bits(r[field][lc])), field
+
+
+def test_textured_frames_match_reference():
+    """The oracle's texture sampling against the reference's own loader and sampler
+    (fixture from tests/golden/make_golden.py textured)."""
+    scene_kw, kw = dict(width=32, height=24), dict(ris=True, candidate_count=16, use_reservoir=True, max_depth=1)
+    g = np.load(GOLDEN / "frames_textured.npz")
+    sc, cam = configs.textured_variant(**scene_kw)
+    o = orc.Oracle(sc, threads=2)
+    for f in range(2):
+        gb = o.raycast(cam, f)
+        assert np.array_equal(gb["prim_id"], g[f"gbuf{f}"]["prim_id"])
+        o.integrate(cam, f, **kw)
+        o.accumulate(cam, f, firefly=True)
+        assert np.array_equal(bits(o.color), bits(g[f"color{f}"])), f"colour frame {f}"
+        r = g[f"res{f}"]
+        for field in RES_FIELDS_ALWAYS:
+            assert np.array_equal(bits(o.res[field]), bits(r[field])), field
