@@ -6,6 +6,8 @@
 
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <tuple>
 #include <utility>
 
 namespace hdr {
@@ -351,6 +353,9 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
     // ---- materials: PreviewSurfaceMaterial::GetClosure inputs (preview_surface.cpp:61-127)
     out.num_materials = desc.num_materials;
     out.materials.assign((size_t)desc.num_materials * kMaterialFloats, 0.0f);
+    // one copy per distinct texel array, as ImageTextureSamplerFactory loads each path once
+    // (image_texture_sampler.cpp:14-33)
+    std::map<std::tuple<const float *, int, int>, int> texture_offsets;
     for (int i = 0; i < desc.num_materials; ++i) {
         const hdr_material_desc &p = desc.materials[i];
         float *r = &out.materials[(size_t)i * kMaterialFloats];
@@ -370,7 +375,10 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
         for (int k = 0; k < 4; ++k) {
             int off = -1;
             const int w = p.tex_width[k], h = p.tex_height[k];
-            if (p.textures[k] && w > 0 && h > 0) {
+            const auto known = texture_offsets.find(std::make_tuple(p.textures[k], w, h));
+            if (p.textures[k] && w > 0 && h > 0 && known != texture_offsets.end()) {
+                off = known->second;
+            } else if (p.textures[k] && w > 0 && h > 0) {
                 const size_t n = (size_t)w * (size_t)h * 3;
                 if (out.textures.size() + n > (size_t)0x7fffffff || (size_t)w * (size_t)h > (size_t)0x7fffffff / 3) {
                     err = "material " + std::to_string(i) + ": textures exceed 2^31 floats";
@@ -378,6 +386,7 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
                 }
                 off = (int)out.textures.size();
                 out.textures.insert(out.textures.end(), p.textures[k], p.textures[k] + n);
+                texture_offsets[std::make_tuple(p.textures[k], w, h)] = off;
             }
             r[36 + k] = as_float(off);
             r[40 + k] = as_float(off >= 0 ? w : 0);
