@@ -59,7 +59,6 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched and served legs")
     ap.add_argument("--serving-jobs", type=int, default=80, help="config-4 jobs per serving leg")
@@ -131,32 +130,54 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_sample(scene, cam, budget_s: float, threads: int, frame: int = 0):
-    """Renders evenly spread row bands of one 1080p frame with the CPU restatement
-    until the budget is spent; returns (seconds per full frame, rows sampled)."""
-    from oracle.oracle import Oracle
-    orc = Oracle(scene, threads=threads)
-    band = 4 * threads
-    starts = list(range(0, HEIGHT, band))
-    # visit bands in a stride order so any prefix is spread over the whole frame
-    order = []
-    step = max(1, len(starts) // 7)
-    for off in range(step):
-        order += starts[off::step]
-    rows, t_used = 0, 0.0
-    for y0 in order:
-        y1 = min(HEIGHT, y0 + band)
-        t0 = time.perf_counter()
-        orc.frame_band(cam, frame, y0, y1, ris=True, candidate_count=CANDIDATES, use_reservoir=True)
-        t_used += time.perf_counter() - t0
-        rows += y1 - y0
-        if t_used >= budget_s:
-            break
+# the CPU sample: tile rows 3, 11, 19, ... (every 8th 16-pixel row of tiles, 144 of the 1080
+# image rows) of the real frame, the same rows every frame so their reservoirs keep history
+SAMPLE_STRIDE, SAMPLE_OFFSET, TILE = 8, 3, 16
+
+
+def sample_rows(height):
+    return [y for ty in range(SAMPLE_OFFSET, (height + TILE - 1) // TILE, SAMPLE_STRIDE)
+            for y in range(ty * TILE, min(height, ty * TILE + TILE))]
+
+
+def cpu_sample_port(orc, cam, frame: int):
+    """The C restatement on the sampled tile rows of one frame (raycast + ReSTIR
+    integration; reservoirs of those rows persist in `orc` from frame to frame)
+    and its accumulation over the whole frame; returns seconds per full frame."""
+    rows = sample_rows(cam.height)
+    t0 = time.perf_counter()
+    for ty in range(SAMPLE_OFFSET, (cam.height + TILE - 1) // TILE, SAMPLE_STRIDE):
+        orc.frame_band(cam, frame, ty * TILE, min(cam.height, ty * TILE + TILE), ris=True,
+                       candidate_count=CANDIDATES, use_reservoir=True)
+    t_rows = time.perf_counter() - t0
     t0 = time.perf_counter()
     orc.accumulate(cam, frame, firefly=True)
-    t_acc = time.perf_counter() - t0
-    orc.close()
-    return t_used * HEIGHT / rows + t_acc, rows
+    return t_rows * cam.height / len(rows) + (time.perf_counter() - t0)
+
+
+def cpu_frames(scene, cam, frames, threads):
+    """Seconds per full 1920x1080 frame for each of `frames` (consecutive frame
+    indices: the sampled rows carry their reservoir history) on the host cores:
+    the reference's own passes compiled in place when built, else the restatement."""
+    if _ref_available():
+        from oracle import refharness
+        got = refharness.cpu_sample(scene, cam, threads, frames=frames, stride=SAMPLE_STRIDE, offset=SAMPLE_OFFSET,
+                                    candidate_count=CANDIDATES)
+        return [sec for _, sec, _ in got], "reference"
+    from oracle.oracle import Oracle
+    orc = Oracle(scene, threads=threads)
+    try:
+        return [cpu_sample_port(orc, cam, f) for f in frames], "port"
+    finally:
+        orc.close()
+
+
+def cpu_sample_label(height, frames_desc):
+    rows = len(sample_rows(height))
+    return (f"tile rows {SAMPLE_OFFSET}, {SAMPLE_OFFSET + SAMPLE_STRIDE}, ... (every {SAMPLE_STRIDE}th row of "
+            f"16x16 tiles: {rows} of {height} image rows) of the real {WIDTH}x{height} frame, the same rows every "
+            f"frame so their reservoirs keep history; RaycastPass + RISPathTracePass on those rows scaled by "
+            f"{height}/{rows}, plus AccumulationPass over the whole frame; {frames_desc}")
 
 
 def _ref_available() -> bool:
@@ -164,28 +185,30 @@ def _ref_available() -> bool:
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference's CPU path on the host cores (rank 0 only)."""
+    """--impl reference: the reference's CPU path on the host cores (rank 0 only).
+    Each step is one frame (consecutive frame indices, history carried) on the
+    sampled tile rows, with all the host threads."""
     if rank != 0:
         return None
     from hdrestir_b200 import configs
     threads = os.cpu_count() or 1
     scene, cam = configs.config2(WIDTH, HEIGHT)
-    use_ref = _ref_available()
-    per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
-    fps = []
-    ref = None
-    if use_ref:
+    n = args.warmup + args.steps
+    if _ref_available():
         from oracle import refharness
         ref = refharness.Reference(scene)  # scene build, untimed like the GPU arm's upload
-    for k in range(args.warmup + args.steps):
-        if use_ref:
-            sec, rows = refharness.cpu_sample(scene, cam, per_step, threads, frame=k, ref=ref)
-        else:
-            sec, rows = cpu_sample(scene, cam, per_step, threads, frame=0)
-        if k >= args.warmup:
-            fps.append(1.0 / sec)
-    value = statistics.mean(fps)
-    kind = "reference" if use_ref else "port"
+        secs = [s for _, s, _ in refharness.cpu_sample(scene, cam, threads, frames=range(n), stride=SAMPLE_STRIDE,
+                                                        offset=SAMPLE_OFFSET, ref=ref, candidate_count=CANDIDATES)]
+        ref.close()
+        kind = "reference"
+    else:
+        from oracle.oracle import Oracle
+        orc = Oracle(scene, threads=threads)
+        secs = [cpu_sample_port(orc, cam, f) for f in range(n)]
+        orc.close()
+        kind = "port"
+    timed = secs[args.warmup:]
+    value = len(timed) / sum(timed)
     return {
         "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
@@ -193,8 +216,8 @@ def run_reference(args, rank, world):
         "data": "synthetic seeded config-2 scene (1.03M triangles, 10k rect lights)",
         "config": config_block(),
         "cpu_baseline": {"value": value, "unit": "frames/s", "cores": threads, "kind": kind,
-                         "sample": f"row bands of a 1920x1080 frame, ~{per_step:.0f} s of CPU work per step, "
-                                   "extrapolated to the full frame"},
+                         "sample": cpu_sample_label(HEIGHT, f"frames {args.warmup}..{n - 1} timed after "
+                                                            f"{args.warmup} warm-up frames")},
         "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -542,16 +565,10 @@ def run_ours(args, rank, local_rank, world):
         out["config3"] = config3_leg()
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        if _ref_available():
-            from oracle import refharness
-            sec, rows = refharness.cpu_sample(scene, cam, args.cpu_seconds, threads)
-            kind = "reference"
-        else:
-            sec, rows = cpu_sample(scene, cam, args.cpu_seconds, threads)
-            kind = "port"
-        out["cpu_baseline"] = {"value": 1.0 / sec, "unit": "frames/s", "cores": threads, "kind": kind,
-                               "sample": f"{rows} of {HEIGHT} rows of frame 0 (bands spread over the image), "
-                                         "raycast + ReSTIR integration + full-frame accumulation, extrapolated"}
+        secs, kind = cpu_frames(scene, cam, range(3), threads)
+        value = 2.0 / sum(secs[1:])
+        out["cpu_baseline"] = {"value": value, "unit": "frames/s", "cores": threads, "kind": kind,
+                               "sample": cpu_sample_label(HEIGHT, "frames 1 and 2 timed after frame 0")}
     ctx.close()
     if world > 1:
         import torch.distributed as dist

@@ -22,6 +22,7 @@ ACCUM_PARITY, ACCUM_SHADER = 0, 1
 CTX_TIMINGS, CTX_WIDE_BVH, CTX_LANE_PER_RAY, CTX_UNPHASED, CTX_PT_ONE_KERNEL = 1, 2, 8, 16, 32
 CTX_SPLIT_STACK = 64
 CTX_DEVICE_BUILD = 128
+CTX_RECORD_LIGHTS = 256
 RIS_REPROJECT = 4
 FMT_FLOAT32, FMT_FLOAT16, FMT_UNORM8, FMT_SNORM8, FMT_INT32 = 0, 1, 2, 3, 4
 FMT_DTYPES = {0: np.float32, 1: np.uint16, 2: np.uint8, 3: np.int8, 4: np.int32}

@@ -66,13 +66,13 @@ def path_settings(max_depth=32, enable_subsurface=True, max_reflection_bounces=8
 class Context:
     def __init__(self, device: int = 0, timings: bool = True, hbm_budget: int = 0, wide_bvh: bool = False,
                  lane_per_ray: bool = False, unphased: bool = False, pt_one_kernel: bool = False,
-                 split_stack: bool = False, device_build: bool = False):
+                 split_stack: bool = False, device_build: bool = False, record_lights: bool = False):
         self._lib = abi.lib()
         self._h = C.c_void_p()
         flags = ((abi.CTX_TIMINGS if timings else 0) | (abi.CTX_WIDE_BVH if wide_bvh else 0)
                  | (abi.CTX_LANE_PER_RAY if lane_per_ray else 0) | (abi.CTX_UNPHASED if unphased else 0)
                  | (abi.CTX_PT_ONE_KERNEL if pt_one_kernel else 0) | (abi.CTX_SPLIT_STACK if split_stack else 0)
-                 | (abi.CTX_DEVICE_BUILD if device_build else 0))
+                 | (abi.CTX_DEVICE_BUILD if device_build else 0) | (abi.CTX_RECORD_LIGHTS if record_lights else 0))
         desc = abi.CtxDesc(int(device), flags, int(hbm_budget))
         abi.check(self._lib.hdr_ctx_create(C.byref(self._h), C.byref(desc)))
         self.width = self.height = 0

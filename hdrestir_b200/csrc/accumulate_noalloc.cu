@@ -7,28 +7,38 @@
 // memory-pool budget, where a cudaMalloc would fail, and one that cannot pay
 // the device-wide synchronisation a cudaMalloc/cudaFree may cause between
 // frames. hdr_accumulate keeps its scratch in context-owned buffers that it
-// grows on demand. This entry point instead takes the firefly scratch (two RGBA
-// f32 planes) and the fallback flag from a file-scope __device__ array of fixed
-// size.
+// grows on demand. This entry point instead takes the firefly scratch (one RGBA
+// f32 plane) and the in-place-order flag from a file-scope __device__ array of
+// fixed size.
 //
 // Limits and set-up:
 //  * at most kNoAllocMaxPixels = 2,097,152 pixels (2^21, covers 1920x1080)
 //    when the firefly clamp is on; larger frames are rejected with HDR_EINVAL.
-//    The scratch is 64 MiB of static device memory, reserved when this module
-//    loads.
+//    Without the clamp any size is accepted (the scratch is not used).
+//  * the scratch is 32 MiB of static device memory, held until the process
+//    exits on every GPU that loads this module. With CUDA's lazy module loading
+//    (the default; CUDA_MODULE_LOADING=LAZY) that happens at the first call on a
+//    device; with eager loading (CUDA_MODULE_LOADING=EAGER) when the process
+//    creates its context on that device, whether or not this entry point is
+//    ever called. Either way the memory is outside every hdr_ctx's
+//    hbm_budget_bytes and the server's admission budget.
 //  * the first call on a device (made with that device current) resolves the
 //    scratch address with cudaGetSymbolAddress, which loads this module. Make
 //    one call per device (any size, e.g. 1x1 with firefly on) before any stream
 //    capture or allocation-restricted region if the module load must not happen
-//    there.
+//    there. The address is cached per device together with the CUDA context it
+//    was resolved in; a call in a new context (after cudaDeviceReset, say)
+//    resolves it again.
+//  * neither mode reads anything back to the host or waits for the stream: the
+//    in-place-order check and its fallback run on the device.
 //  * nothing in the scratch has to start at zero: the clamp pass writes the
-//    first plane in full before anything reads it, the fallback loop writes the
-//    other plane in full before reading it, and the flag is zeroed on the
+//    plane in full before anything reads it, and the flag is zeroed on the
 //    stream before every use. The caller's accum plane must be zero before
 //    frame 0, as "__accum_color" is after hdr_clear_persistent.
 //  * one scratch per device, shared by all callers: calls that overlap on the
 //    same device (different streams or host threads) race on it. Serialise
 //    them.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -37,7 +47,7 @@
 
 namespace hdr {
 int launch_accumulate(float4 *color, float4 *accum, float4 *scratch, int *flag_dev, int width, int height,
-                      int frame_index, int firefly, int mode, cudaStream_t st);
+                      int frame_index, int firefly, int mode, cudaStream_t st, cudaError_t *err);
 hdr_status set_last_error(hdr_status st, const char *fmt, ...);
 }  // namespace hdr
 
@@ -45,8 +55,8 @@ namespace {
 
 constexpr size_t kNoAllocMaxPixels = size_t(1) << 21;
 
-// two planes of kNoAllocMaxPixels RGBA f32 (firefly output, fallback ping-pong)
-static __device__ __align__(256) float4 g_accum_scratch[2 * kNoAllocMaxPixels];
+// one plane of kNoAllocMaxPixels RGBA f32 (the clamped frame)
+static __device__ __align__(256) float4 g_accum_scratch[kNoAllocMaxPixels];
 static __device__ __align__(256) int g_accum_flag[64];
 
 constexpr int kMaxDevices = 64;
@@ -54,16 +64,36 @@ constexpr int kMaxDevices = 64;
 struct ScratchAddr {
     float4 *planes = nullptr;
     int *flag = nullptr;
+    CUcontext ctx = nullptr;  // the context the addresses belong to
 };
 
 std::mutex g_addr_mu;
 ScratchAddr g_addr[kMaxDevices];
 
-// Resolves this device's scratch address once (the current device must be `dev`).
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link to libcuda).
+CUcontext current_context() {
+    static CtxGetCurrentFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
+
+// Resolves this device's scratch address once per context (the current device
+// must be `dev`, with its context current).
 hdr_status scratch_for(int dev, ScratchAddr &out) {
     std::lock_guard<std::mutex> lock(g_addr_mu);
     ScratchAddr &a = g_addr[dev];
-    if (!a.planes) {
+    const CUcontext now = current_context();
+    if (!a.planes || a.ctx != now) {
         void *planes = nullptr, *flag = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&planes, g_accum_scratch);
         if (e == cudaSuccess) e = cudaGetSymbolAddress(&flag, g_accum_flag);
@@ -72,6 +102,7 @@ hdr_status scratch_for(int dev, ScratchAddr &out) {
                                        cudaGetErrorString(e));
         a.planes = static_cast<float4 *>(planes);
         a.flag = static_cast<int *>(flag);
+        a.ctx = current_context();  // the symbol lookup may have created the primary context
     }
     out = a;
     return HDR_OK;
@@ -103,8 +134,7 @@ extern "C" hdr_status hdr_accumulate_noalloc(float *color, float *accum, int32_t
     if (st != HDR_OK) return st;
     const int n = hdr::launch_accumulate(reinterpret_cast<float4 *>(color), reinterpret_cast<float4 *>(accum),
                                          s.planes, s.flag, width, height, frame_index, firefly, mode,
-                                         static_cast<cudaStream_t>(stream));
-    if (n < 0)
-        return hdr::set_last_error(HDR_ECUDA, "accumulation launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+                                         static_cast<cudaStream_t>(stream), &e);
+    if (n < 0) return hdr::set_last_error(HDR_ECUDA, "accumulation launch failed: %s", cudaGetErrorString(e));
     return HDR_OK;
 }

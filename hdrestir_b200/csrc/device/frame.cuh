@@ -110,6 +110,10 @@ struct WaveBuffers {
     // counts[4] entries queued, counts[5] handed out; answers in occ_winner[pixel]
     float4 *q_winner;
     unsigned char *occ_winner;
+    // diagnostic (nullptr: off): pixels * n_shadow light indices the NEE
+    // candidates selected (UniformLightSampler::ProposeCandidate), -1 where the
+    // proposal failed or the pixel has no hit
+    int *nee_light;
 };
 
 // Returns the number of kernels launched, or -1 on a launch error.
@@ -255,9 +259,9 @@ void launch_path_trace_batch(const DeviceScene &s, const PtJobD *jobs, int n_job
                              cudaStream_t st);
 void launch_path_trace(const DeviceScene &s, const CameraD &cam, int frame_index, const PathParamsD &p,
                        GBufferView gb, float4 *color, unsigned *err, cudaStream_t st);
-// Returns the number of kernels launched.
+// Returns the number of kernels launched, or -1 with the CUDA error in *err.
 int launch_accumulate(float4 *color, float4 *accum, float4 *scratch, int *flag_dev, int width, int height,
-                      int frame_index, int firefly, int mode, cudaStream_t st);
+                      int frame_index, int firefly, int mode, cudaStream_t st, cudaError_t *err);
 
 // Pixel of thread t in a 16x16 tile: each warp covers an 8x4 sub-tile so the
 // rays it traces start close together.

@@ -796,6 +796,10 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
         wb.rng_state = (uint4 *)q;
         if ((st = ensure_buffer(c, "__wave_done", count, &q)) != HDR_OK) return st;
         wb.done = (unsigned char *)q;
+        if (c->flags & HDR_CTX_RECORD_LIGHTS) {
+            if ((st = ensure_buffer(c, "__ris_nee_lights", count * wb.n_shadow * 4, &q)) != HDR_OK) return st;
+            wb.nee_light = (int *)q;
+        }
         if (p->skip_visibility || reproject || spatial) {  // winners whose visibility is still untested: one per pixel
             if ((st = ensure_buffer(c, "__wave_q_winner", count * 32, &q)) != HDR_OK) return st;
             wb.q_winner = (float4 *)q;
@@ -1317,11 +1321,12 @@ hdr_status hdr_accumulate(hdr_ctx *c, int32_t frame_index, int32_t firefly, int3
     void *accum = nullptr, *scratch = nullptr;
     if ((st = ensure_buffer(c, "__accum_color", count * 16, &accum)) != HDR_OK) return st;
     if (firefly)
-        if ((st = ensure_buffer(c, "__firefly_scratch", count * 32, &scratch)) != HDR_OK) return st;
+        if ((st = ensure_buffer(c, "__firefly_scratch", count * 16, &scratch)) != HDR_OK) return st;
     if ((st = begin_pass(c, 2)) != HDR_OK) return st;
+    cudaError_t err = cudaSuccess;
     const int n = hdr::launch_accumulate((float4 *)color, (float4 *)accum, (float4 *)scratch, c->d_flag, c->width,
-                                         c->height, frame_index, firefly, mode, c->stream);
-    if (n < 0) return fail(HDR_ECUDA, "accumulation launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+                                         c->height, frame_index, firefly, mode, c->stream, &err);
+    if (n < 0) return fail(HDR_ECUDA, "accumulation launch failed: %s", cudaGetErrorString(err));
     c->launches += (uint64_t)n;
     return end_pass(c, 2);
 }

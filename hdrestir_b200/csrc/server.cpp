@@ -46,12 +46,12 @@ struct Job {
 size_t pixels_of(const hdr_job_desc &d) { return (size_t)d.camera.width * (size_t)d.camera.height; }
 
 // Device bytes a job's context allocates, per pixel: GBuffer 96, Color 16,
-// accumulator 16, firefly scratch 32; RIS adds the reservoir (80), the
+// accumulator 16, firefly scratch 16; RIS adds the reservoir (80), the
 // stream state and done flag (49) and its share of the batch's ray queues and
 // result slots (52 per closest-hit slot, 33 per shadow slot).
 size_t job_bytes(const hdr_job_desc &d) {
     const size_t px = pixels_of(d);
-    size_t per = 96 + 16 + 16 + (d.firefly ? 32 : 0);
+    size_t per = 96 + 16 + 16 + (d.firefly ? 16 : 0);
     if (d.pipeline == HDR_JOB_RIS) {
         const int n_nee = std::max(1, d.ris.candidate_count / 2);
         const int n_closest = 1 + std::max(0, d.ris.candidate_count - n_nee);

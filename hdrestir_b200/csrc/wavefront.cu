@@ -69,6 +69,8 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
         if (cam.p.has_params && cam.p.enable_exposure) rgb = rgb * cam.p.exposure_mult;
         color[i] = make_float4(rgb.x, rgb.y, rgb.z, 1.0f);
         wb.done[i] = 1;
+        if (wb.nee_light)
+            for (int j = 0; j < wb.n_shadow; ++j) wb.nee_light[i * (size_t)wb.n_shadow + j] = -1;
         return;
     }
     wb.done[i] = 0;
@@ -97,8 +99,9 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
         LightSampleD ls;
         V3 o, d;
         float lim = 0.0f;
-        const bool want = propose_candidate(s, ps.hit.position, rng, li, ls) &&
-                          ris_nee_shadow_ray(s, sf, li, ls, ris.skip_vis, o, d, lim);
+        const bool proposed = propose_candidate(s, ps.hit.position, rng, li, ls);
+        if (wb.nee_light) wb.nee_light[sbase + j] = proposed ? li : -1;
+        const bool want = proposed && ris_nee_shadow_ray(s, sf, li, ls, ris.skip_vis, o, d, lim);
         const int q = queue_append(&wb.counts[1], want);
         if (q >= 0) {
             wb.q_shadow[2 * (size_t)q] =

@@ -252,6 +252,14 @@ typedef struct hdr_gbuffer_texel {
                                      HDR_CTX_WIDE_BVH, and the scene cannot be shared into a
                                      wide-walk ctx. Its scratch (about 0.5 KB per triangle while
                                      building) is outside the ctx's HBM budget. */
+#define HDR_CTX_RECORD_LIGHTS 256u /* diagnostic, no reference counterpart: the wavefront
+                                     hdr_ris_path_trace records the light index each NEE candidate
+                                     selected (UniformLightSampler::ProposeCandidate,
+                                     lighting_core/uniform_light_sampler.cpp:22-35; -1 where the
+                                     proposal failed or the pixel has no hit) in
+                                     "__ris_nee_lights": width*height x (candidate_count/2, at least
+                                     1) int32, pixel-major. Not recorded by batched or one-kernel
+                                     frames. */
 
 typedef struct hdr_ctx_desc {
     int32_t device;              /* CUDA ordinal */
@@ -389,17 +397,22 @@ hdr_status hdr_path_trace(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_ind
 
 /* AccumulationPass::_execute (passes/accumulation_pass.cpp:64-139) and
  * GpuAccumulationPass (accumulation.slang:39-97): optional firefly clamp,
- * "__accum_color" += "Color", "Color" = accum / (frame_index+1). */
+ * "__accum_color" += "Color", "Color" = accum / (frame_index+1). Enqueued on the
+ * ctx stream; neither mode reads back or waits (parity mode checks the in-place
+ * order and, where it differs, clamps in that order, all on the device). */
 hdr_status hdr_accumulate(hdr_ctx *ctx, int32_t frame_index, int32_t firefly, int32_t mode);
 
 /* No reference counterpart. hdr_accumulate on caller-owned device planes
  * (color, accum: width*height RGBA f32, 16-byte aligned, on the current
  * device) that allocates nothing: the firefly scratch is a fixed static device
- * array, so frames above 2,097,152 pixels with firefly != 0 are rejected
- * (HDR_EINVAL). For callers that may not allocate device memory while they
- * accumulate. The first call on a device loads the scratch (make it before any
- * stream capture); accum must be zero before frame 0; calls that overlap on one
- * device race on the shared scratch. stream: a cudaStream_t (NULL = default). */
+ * array (32 MiB, held on every GPU that loads it until the process exits,
+ * outside any HBM budget), so frames above 2,097,152 pixels with firefly != 0
+ * are rejected (HDR_EINVAL). For callers that may not allocate device memory
+ * while they accumulate. The first call on a device (and in a new context on
+ * it) resolves the scratch's address (make it before any stream capture);
+ * accum must be zero before frame 0; calls that overlap on one device race on
+ * the shared scratch. Neither mode reads back or waits for the stream.
+ * stream: a cudaStream_t (NULL = default). */
 hdr_status hdr_accumulate_noalloc(float *color, float *accum, int32_t width, int32_t height, int32_t frame_index,
                                   int32_t firefly, int32_t mode, void *stream);
 

@@ -75,6 +75,7 @@ def lib() -> C.CDLL:
         L.orc_integrate_band.argtypes = [vp, C.POINTER(abi.CameraDesc), C.c_int, C.POINTER(FrameParams), vp, vp,
                                          vp, vp, C.c_int, C.c_int, C.c_int]
         L.orc_accumulate.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.orc_accumulate_shader.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_rng_floats.argtypes = [vp, C.c_int, C.c_int, vp]
         L.orc_reservoir_known_answer.restype = C.c_float
         L.orc_reservoir_known_answer.argtypes = [C.c_float, C.c_float, C.c_int]
@@ -143,16 +144,21 @@ class Oracle:
         return self.color, tr
 
     def frame_band(self, cam, frame, y0, y1, ris=True, candidate_count=32, use_reservoir=True,
-                   skip_visibility=False, max_depth=1):
-        """Raycast + integration of image rows [y0, y1) (a bounded CPU sample of one frame)."""
+                   skip_visibility=False, max_depth=1, trace=None):
+        """Raycast + integration of image rows [y0, y1) (a bounded CPU sample of one frame).
+        The pixels of those rows in gbuf / color / res (full-frame arrays) and, when given,
+        in `trace` (a full-frame TRACE_DTYPE array) are written; the others are left alone,
+        so the reservoirs of a band keep their history from frame to frame."""
         n = cam.width * cam.height
         self._ensure(n)
         cd = cam.c_desc()
         fp = FrameParams(int(ris), PathParams(max_depth, 1, 8, 8, 1, 1.0),
                          RisParams(candidate_count, int(use_reservoir), int(skip_visibility), 0))
+        if trace is not None:
+            assert trace.dtype == TRACE_DTYPE and len(trace) == n
         self._lib.orc_raycast_band(self._s, C.byref(cd), int(frame), _p(self.gbuf), int(y0), int(y1), self.threads)
         self._lib.orc_integrate_band(self._s, C.byref(cd), int(frame), C.byref(fp), _p(self.gbuf), _p(self.color),
-                                     _p(self.res), None, int(y0), int(y1), self.threads)
+                                     _p(self.res), _p(trace), int(y0), int(y1), self.threads)
 
     def accumulate(self, cam, frame, firefly=True):
         self._lib.orc_accumulate(_p(self.color), _p(self.accum), cam.width, cam.height, int(frame), int(firefly))
@@ -164,6 +170,17 @@ class Oracle:
         tm = None if tmax is None else np.ascontiguousarray(tmax, np.float32)
         self._lib.orc_trace_rays(self._s, _p(rays), _p(tm), len(rays), int(any_hit), _p(out))
         return out
+
+
+def accumulate_frame(color, accum, width, height, frame, firefly=True, mode="parity"):
+    """AccumulationPass (mode "parity": the in-place row-major clamp) or the
+    GpuAccumulationPass shader (mode "shader") on caller arrays, in place:
+    color and accum are (width*height, 4) float32."""
+    fn = lib().orc_accumulate if mode == "parity" else lib().orc_accumulate_shader
+    assert color.dtype == np.float32 and accum.dtype == np.float32
+    assert color.flags.c_contiguous and accum.flags.c_contiguous
+    fn(_p(color), _p(accum), int(width), int(height), int(frame), int(firefly))
+    return color
 
 
 def rng_floats(seeds, count) -> np.ndarray:

@@ -60,6 +60,7 @@ void orc_integrate_band(const orc_scene *s, const hdr_camera *cam, int frame, co
                         hdr_gbuffer_texel *gbuf, float *color, orc_reservoir *res, orc_pixel_trace *trace, int y0,
                         int y1, int threads);
 void orc_accumulate(float *color, float *accum, int width, int height, int frame, int firefly);
+void orc_accumulate_shader(float *color, float *accum, int width, int height, int frame, int firefly);
 void orc_rng_floats(const uint32_t *seeds, int n, int count, float *out);
 float orc_reservoir_known_answer(float weight, float phat, int candidates_per_frame);
 void orc_trace_rays(const orc_scene *s, const float *rays, const float *tmax, int n, int any_hit,

@@ -1389,6 +1389,44 @@ void orc_accumulate(float *color, float *accum, int width, int height, int frame
     }
 }
 
+/* GpuAccumulationPass's shader (gpu_functions/shaders/accumulation.slang:55-97):
+ * the same firefly rule, but every pixel clamps against the unclamped input
+ * (colorIn), then acc = accum + colour, out = acc * invN. Metrics off. */
+void orc_accumulate_shader(float *color, float *accum, int width, int height, int frame, int firefly) {
+    size_t n = (size_t)width * height;
+    float *out = (float *)malloc(n * 4 * sizeof(float));
+    float inv = 1.0f / (float)(frame + 1);
+    for (int y = 0; y < height; ++y)
+        for (int x = 0; x < width; ++x) {
+            size_t i = (size_t)y * width + x;
+            float c[4] = {color[4 * i], color[4 * i + 1], color[4 * i + 2], color[4 * i + 3]};
+            if (firefly) {
+                float mx = 0.0f;
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        if (dx == 0 && dy == 0) continue;
+                        int nx = oclampi(x + dx, 0, width - 1), ny = oclampi(y + dy, 0, height - 1);
+                        const float *q = &color[4 * ((size_t)ny * width + nx)];
+                        mx = omax(mx, 0.2126f * q[0] + 0.7152f * q[1] + 0.0722f * q[2]);
+                    }
+                float thr = mx * 4.0f + 0.5f;
+                float lum = 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2];
+                if (lum > thr && lum > 0.0f) {
+                    float sc = thr / lum;
+                    c[0] *= sc;
+                    c[1] *= sc;
+                    c[2] *= sc;
+                }
+            }
+            for (int k = 0; k < 4; ++k) {
+                accum[4 * i + k] += c[k];
+                out[4 * i + k] = accum[4 * i + k] * inv;
+            }
+        }
+    memcpy(color, out, n * 4 * sizeof(float));
+    free(out);
+}
+
 /* WeightedReservoir::Update + Finalize (restir/reservoir.h:76-125) for one
  * candidate with the given weight and target function; returns W. The draw
  * comes from Rng{777} as in tests/test_reservoir.cpp:67-76. */

@@ -8,6 +8,7 @@
 // buffer store of RenderPipeline::Execute (pipeline/render_pipeline.cpp:24-40),
 // and exports GBuffer, Color and "__ris_reservoir" through a C interface for
 // the parity tests and the CPU baseline. Nothing here is part of the product.
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -18,6 +19,7 @@
 #include <vector>
 
 #include "../include/hdrestir.h"
+#include "pxr/base/work/loops.h"
 #include "accumulation_pass.h"
 #include "denoiser.h"
 #include "upscale_pass.h"
@@ -243,8 +245,18 @@ static void texel_from_hit(hdr_gbuffer_texel &t, const std::optional<HitRecord> 
 
 // One frame through the reference passes. Outputs may be NULL; sizes are
 // RenderedWidth x RenderedHeight of the chosen resolution level.
-int ref_render_frame(RefScene *rs, const hdr_camera *cam, int frame_index, const ref_params *p,
-                     hdr_gbuffer_texel *gbuf_out, float *color_out, ref_reservoir *res_out) {
+//
+// tile_row_stride > 0 renders a bounded sample of the frame for CPU timing: the
+// passes' 16x16 tile loops (WorkParallelForN over the tiles) run only the tile
+// rows tile_row_offset, +stride, +2 stride, ... of the real frame (the shim's
+// loop selection); every other pixel keeps a miss in "GBuffer" and zero in
+// "Color", and the persistent store carries those rows' reservoirs from frame
+// to frame like any frame's. times (if not NULL) receives the wall seconds of
+// RaycastPass + the integration pass [0] and of AccumulationPass [1] (the full
+// frame: it loops over every pixel on one thread), and [2] the tile rows run.
+static int render_frame(RefScene *rs, const hdr_camera *cam, int frame_index, const ref_params *p,
+                        hdr_gbuffer_texel *gbuf_out, float *color_out, ref_reservoir *res_out, int tile_row_stride,
+                        int tile_row_offset, double *times) {
     try {
         GfMatrix4d view, proj;
         for (int r = 0; r < 4; ++r)
@@ -297,12 +309,32 @@ int ref_render_frame(RefScene *rs, const hdr_camera *cam, int frame_index, const
             rs->store.Clear();
             rs->store_pixels = ctx.frame.PixelCount();
         }
+        // the sampled tile rows (the passes tile the rendered frame by 16x16)
+        const int tiles_x = (ctx.frame.RenderedWidth() + 15) / 16, tiles_y = (ctx.frame.RenderedHeight() + 15) / 16;
+        WorkShimSelection &sel = WorkShimSelected();
+        sel = WorkShimSelection{};
+        int rows_run = tiles_y;
+        if (tile_row_stride > 0) {
+            sel.total = (size_t)tiles_x * (size_t)tiles_y;
+            rows_run = 0;
+            for (int ty = tile_row_offset % tile_row_stride; ty < tiles_y; ty += tile_row_stride, ++rows_run)
+                sel.ranges.emplace_back((size_t)ty * tiles_x, (size_t)(ty + 1) * tiles_x);
+        }
         // RenderPipeline::Execute (pipeline/render_pipeline.cpp:24-40)
         ctx.buffers.InjectFrom(rs->store);
+        const auto t0 = std::chrono::steady_clock::now();
         raycast.Execute(ctx);
         integ->Execute(ctx);
+        const auto t1 = std::chrono::steady_clock::now();
+        sel = WorkShimSelection{};
         if (p->accumulate) accum.Execute(ctx);
+        const auto t2 = std::chrono::steady_clock::now();
         ctx.buffers.ExtractPersistentTo(rs->store);
+        if (times) {
+            times[0] = std::chrono::duration<double>(t1 - t0).count();
+            times[1] = std::chrono::duration<double>(t2 - t1).count();
+            times[2] = rows_run;
+        }
 
         const size_t n = ctx.frame.PixelCount();
         if (gbuf_out) {
@@ -350,9 +382,23 @@ int ref_render_frame(RefScene *rs, const hdr_camera *cam, int frame_index, const
         }
         return (int)n;
     } catch (const std::exception &e) {
+        WorkShimSelected() = WorkShimSelection{};
         std::fprintf(stderr, "ref_render_frame: %s\n", e.what());
         return -1;
     }
+}
+
+int ref_render_frame(RefScene *rs, const hdr_camera *cam, int frame_index, const ref_params *p,
+                     hdr_gbuffer_texel *gbuf_out, float *color_out, ref_reservoir *res_out) {
+    return render_frame(rs, cam, frame_index, p, gbuf_out, color_out, res_out, 0, 0, nullptr);
+}
+
+// A timed sample of one frame (see render_frame): the chosen tile rows through
+// RaycastPass and the integration pass, then AccumulationPass over the frame.
+int ref_render_frame_sampled(RefScene *rs, const hdr_camera *cam, int frame_index, const ref_params *p,
+                             int tile_row_stride, int tile_row_offset, float *color_out, double *times) {
+    return render_frame(rs, cam, frame_index, p, nullptr, color_out, nullptr, tile_row_stride, tile_row_offset,
+                        times);
 }
 
 int ref_trace_rays(RefScene *rs, const float *rays, int n, hdr_gbuffer_texel *out) {
@@ -429,6 +475,36 @@ void ref_denoise(float *rgba, int width, int height, int chromaticity_blur) {
     cfg.EnableChromaticityBlur = chromaticity_blur != 0;
     Denoiser::Run(gsl::span<pxr::GfVec4f>{reinterpret_cast<pxr::GfVec4f *>(rgba), (size_t)width * (size_t)height},
                   width, height, cfg);
+}
+
+// AccumulationPass::Execute on a caller frame: "Color" (width x height RGBA
+// floats, in place) and the persistent "__accum_color" (accum, in and out), as
+// RenderPipeline::Execute hands them to the pass from frame to frame.
+void ref_accumulate(float *color, float *accum, int width, int height, int frame_index, int firefly) {
+    static Scene empty_scene;
+    const GfMatrix4d ident(1.0);
+    Rng rng{0u};
+    RenderContext ctx{
+        .scene = &empty_scene,
+        .viewMatrix = ident,
+        .projMatrix = ident,
+        .frame = CameraFrame{.windowWidth = width, .windowHeight = height, .resolutionLevel = 0,
+                             .visibleMinX = 0, .visibleMinY = 0, .visibleMaxX = width, .visibleMaxY = height},
+        .frameIndex = frame_index,
+        .rng = rng,
+        .buffers = FrameBuffersMap{},
+        .OutputNames = {"Color"},
+        .cameraParams = std::nullopt,
+    };
+    const size_t n = ctx.frame.PixelCount();
+    ctx.buffers.Add(kColorOutputName, sizeof(GfVec4f), n);
+    std::memcpy(ctx.buffers.GetFrameBuffer(kColorOutputName).Data(), color, n * sizeof(GfVec4f));
+    ctx.buffers.AddOrGetPersistent(kAccumColorBuf, sizeof(GfVec4f), n);
+    std::memcpy(ctx.buffers.GetFrameBuffer(kAccumColorBuf).Data(), accum, n * sizeof(GfVec4f));
+    AccumulationPass pass{firefly != 0};
+    pass.Execute(ctx);
+    std::memcpy(color, ctx.buffers.GetFrameBuffer(kColorOutputName).Data(), n * sizeof(GfVec4f));
+    std::memcpy(accum, ctx.buffers.GetFrameBuffer(kAccumColorBuf).Data(), n * sizeof(GfVec4f));
 }
 
 const char *ref_version(void) { return "hdRestir reference sources compiled in place with the oracle shim"; }

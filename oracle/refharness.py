@@ -17,7 +17,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_ref" / "libhdr_ref.so"
-REFERENCE_TREE = Path(os.environ.get("HDR_REFERENCE_TREE", "/root/reference"))
+# the reference checkout: HDR_REFERENCE_TREE, else "reference" beside this repository
+REFERENCE_TREE = Path(os.environ.get("HDR_REFERENCE_TREE", str(HERE.parent.parent / "reference")))
 
 import sys  # noqa: E402
 
@@ -66,6 +67,9 @@ def lib() -> C.CDLL:
         L.ref_clear_persistent.argtypes = [vp]
         L.ref_render_frame.restype = C.c_int
         L.ref_render_frame.argtypes = [vp, C.POINTER(abi.CameraDesc), C.c_int, C.POINTER(RefParams), vp, vp, vp]
+        L.ref_render_frame_sampled.restype = C.c_int
+        L.ref_render_frame_sampled.argtypes = [vp, C.POINTER(abi.CameraDesc), C.c_int, C.POINTER(RefParams),
+                                               C.c_int, C.c_int, vp, C.POINTER(C.c_double)]
         L.ref_trace_rays.argtypes = [vp, vp, C.c_int, vp]
         L.ref_rng_floats.argtypes = [vp, C.c_int, C.c_int, vp]
         L.ref_reservoir_known_answer.restype = C.c_float
@@ -73,6 +77,7 @@ def lib() -> C.CDLL:
         L.ref_upscale.restype = C.c_int
         L.ref_upscale.argtypes = [C.c_char_p, vp, C.c_int, C.c_int, C.c_int, vp]
         L.ref_denoise.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        L.ref_accumulate.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int]
         _lib = L
     return _lib
 
@@ -170,31 +175,42 @@ def rng_floats(seeds, count) -> np.ndarray:
     return out
 
 
-def cpu_sample(scene, cam, budget_s: float, threads: int, frame: int = 0, ref: "Reference | None" = None):
-    """Times the reference pipeline (Raycast -> RISPathTrace(32, reservoir) ->
-    Accumulation) on the host cores at the finest resolution level whose frame
-    fits the budget; returns (seconds per full-resolution frame, rows). `ref`
-    reuses an already built reference scene (its build is not timed)."""
+TILE = 16  # the passes' tile size (integration_pass.cpp:184-190, raycast_pass.cpp:91-97)
+
+
+def cpu_sample(scene, cam, threads: int, frames=(0,), stride: int = 8, offset: int = 3,
+               ref: "Reference | None" = None, candidate_count: int = 32, accumulate: bool = True,
+               color_out: np.ndarray | None = None):
+    """Times the reference pipeline (RaycastPass -> RISPathTracePass(32 candidates,
+    reservoir) -> AccumulationPass) on a bounded sample of the real frame.
+
+    Each frame in `frames` runs the reference's own passes on the full-size frame,
+    with their 16x16 tile loops restricted to the tile rows offset, offset+stride,
+    ... (the shim's WorkParallelForN selection), and AccumulationPass over the whole
+    frame. The persistent store carries those rows' reservoirs from frame to frame,
+    so later frames do the temporal merge as the GPU frames do. A frame's time is
+    (raycast + integration time) x (image rows / rows run) + accumulation time.
+    Returns a list of (frame, seconds per full frame, image rows run); `color_out`
+    (width*height x 4 float32), when given, receives the last frame's "Color"."""
     os.environ["HDR_REF_THREADS"] = str(threads)
     own = ref is None
     if own:
         ref = Reference(scene)
-    level, sec = 4, None
-    while True:
-        div = 1 << level
-        rows = (cam.height + div - 1) // div
-        t0 = time.perf_counter()
-        ref.render(cam, frame, ris=True, candidate_count=32, use_reservoir=True, max_depth=1,
-                   resolution_level=level, outputs=())
-        dt = time.perf_counter() - t0
-        px = ((cam.width + div - 1) // div) * rows
-        sec = dt * (cam.width * cam.height) / px
-        if level == 0 or dt * 4 > budget_s:
-            break
-        level -= 1
+    p = RefParams(1, candidate_count, 1, 0, 1, 1, 8, 8, 1, 1.0, 1, int(accumulate), 0)
+    tiles_y = (cam.height + TILE - 1) // TILE
+    out = []
+    times = (C.c_double * 3)()
+    for f in frames:
+        got = ref._lib.ref_render_frame_sampled(ref._s, C.byref(cam.c_desc()), int(f), C.byref(p), stride, offset,
+                                                _p(color_out), times)
+        if got != cam.width * cam.height:
+            raise RuntimeError(f"reference render failed ({got})")
+        rows = sum(min(TILE, cam.height - ty * TILE) for ty in range(offset % stride, tiles_y, stride))
+        assert int(times[2]) == len(range(offset % stride, tiles_y, stride))
+        out.append((int(f), times[0] * cam.height / rows + times[1], rows))
     if own:
         ref.close()
-    return sec, rows
+    return out
 
 
 def upscale(name: str, src: np.ndarray, window_w: int, window_h: int, level: int) -> np.ndarray:
@@ -213,3 +229,13 @@ def denoise(rgba: np.ndarray, width: int, height: int, chromaticity_blur: bool =
     img = np.ascontiguousarray(rgba, np.float32).copy()
     lib().ref_denoise(img.ctypes.data_as(C.c_void_p), width, height, int(chromaticity_blur))
     return img
+
+
+def accumulate(color: np.ndarray, accum: np.ndarray, width: int, height: int, frame: int,
+               firefly: bool = True) -> None:
+    """The reference's AccumulationPass on a caller frame, in place: color and
+    accum are (width*height, 4) float32 arrays ("Color" and "__accum_color")."""
+    assert color.dtype == np.float32 and accum.dtype == np.float32
+    assert color.flags.c_contiguous and accum.flags.c_contiguous
+    lib().ref_accumulate(color.ctypes.data_as(C.c_void_p), accum.ctypes.data_as(C.c_void_p), width, height,
+                         int(frame), int(firefly))

@@ -12,6 +12,7 @@ import pytest
 
 from hdrestir_b200 import abi, configs
 from oracle.oracle import Oracle, rng_floats
+from tests.parity_checks import check_nee, check_reservoirs
 
 pytestmark = pytest.mark.gpu
 
@@ -149,23 +150,32 @@ def test_ris_plain_matches_oracle(gpu_ctx, mode):
 
 
 @pytest.mark.parametrize("mode", list(MODES))
-def test_restir_temporal_matches_oracle(gpu_ctx, mode):
+def test_restir_temporal_matches_oracle(mode):
+    """Reservoir M bit-exact, winner (light index) and WSum / W per the parity
+    contract, NEE light-selection indices bit-exact (recorded by the wavefront
+    forms), colour within the tolerance."""
+    from hdrestir_b200.context import Context
     sc, cam = _scene(2)
-    gpu_ctx.upload_scene(sc)
-    gpu_ctx.clear_persistent()
     orc = Oracle(sc)
-    for frame in range(3):
-        gpu_ctx.raycast(cam, frame)
-        gpu_ctx.ris_path_trace(cam, frame, candidate_count=32, use_reservoir=True, max_depth=1, **MODES[mode])
-        gpu = gpu_ctx.download("Color")
-        res = gpu_ctx.download("__ris_reservoir")
-        orc.raycast(cam, frame)
-        ref, _ = orc.integrate(cam, frame, ris=True, candidate_count=32, use_reservoir=True, max_depth=1)
-        m_gpu = res[4, :, 2].view(np.int32)
-        assert np.array_equal(m_gpu, orc.res["m"]), "reservoir CandidateCount (M) must be bit-exact"
-        frac = _color_outliers(gpu, ref)
-        print(f"ReSTIR frame {frame}: outlier fraction {frac:.4f}")
-        assert frac <= MAX_OUTLIERS
+    idx = np.arange(cam.width * cam.height)
+    with Context(device=0, record_lights=True) as ctx:
+        ctx.upload_scene(sc)
+        ctx.clear_persistent()
+        for frame in range(3):
+            ctx.raycast(cam, frame)
+            ctx.ris_path_trace(cam, frame, candidate_count=32, use_reservoir=True, max_depth=1, **MODES[mode])
+            gpu = ctx.download("Color")
+            res = ctx.download("__ris_reservoir")
+            o = orc.raycast(cam, frame)
+            ref, tr = orc.integrate(cam, frame, ris=True, candidate_count=32, use_reservoir=True, max_depth=1,
+                                    trace=True)
+            check_reservoirs(res, orc.res, idx, f"ReSTIR {mode} frame {frame}")
+            if mode != "one_kernel":
+                lights = ctx.download("__ris_nee_lights").view(np.int32)
+                check_nee(lights, tr, o["hit"] == 1, 16, f"ReSTIR {mode} frame {frame}")
+            frac = _color_outliers(gpu, ref)
+            print(f"ReSTIR frame {frame}: outlier fraction {frac:.4f}")
+            assert frac <= MAX_OUTLIERS
 
 
 def test_restir_multibounce_one_kernel_matches_oracle(gpu_ctx):
@@ -399,6 +409,7 @@ def test_every_lobe_matches_oracle(gpu_ctx):
         orc.raycast(cam, frame)
         want, _ = orc.integrate(cam, frame, ris=True, candidate_count=32, use_reservoir=True, max_depth=1)
         assert np.array_equal(res[4, :, 2].view(np.int32), orc.res["m"])
+        check_reservoirs(res, orc.res, np.arange(len(orc.res)), f"every lobe frame {frame}")
         frac = _color_outliers(got, want)
         print(f"every lobe, frame {frame}: outlier fraction {frac:.4f}")
         assert frac <= MAX_OUTLIERS
