@@ -158,18 +158,59 @@ def cpu_sample_port(orc, cam, frame: int):
 def cpu_frames(scene, cam, frames, threads):
     """Seconds per full 1920x1080 frame for each of `frames` (consecutive frame
     indices: the sampled rows carry their reservoir history) on the host cores:
-    the reference's own passes compiled in place when built, else the restatement."""
+    the reference's own passes compiled in place when built, else the restatement.
+    Also returns the accumulated "Color" after the last frame (valid on the
+    sampled rows)."""
+    import numpy as np
+    color = np.zeros((cam.width * cam.height, 4), np.float32)
     if _ref_available():
         from oracle import refharness
         got = refharness.cpu_sample(scene, cam, threads, frames=frames, stride=SAMPLE_STRIDE, offset=SAMPLE_OFFSET,
-                                    candidate_count=CANDIDATES)
-        return [sec for _, sec, _ in got], "reference"
+                                    candidate_count=CANDIDATES, color_out=color)
+        return [sec for _, sec, _ in got], "reference", color
     from oracle.oracle import Oracle
     orc = Oracle(scene, threads=threads)
     try:
-        return [cpu_sample_port(orc, cam, f) for f in frames], "port"
+        secs = [cpu_sample_port(orc, cam, f) for f in frames]
+        return secs, "port", orc.color.copy()
     finally:
         orc.close()
+
+
+def mse_block(ctx, cam, cpu_color, frames, high_frames=64):
+    """Equal MSE at the headline workload: the GPU image after `frames` accumulated
+    frames and the CPU reference's image after the same frames, each against a
+    high-sample image of the same estimator (GPU, `high_frames` frames of other
+    random streams), over the sampled tile rows without their first and last row
+    (the firefly clamp there sees the unrendered neighbours of the CPU sample).
+    MSE normalised by the high-sample image's peak, as the reference's image tests do."""
+    import numpy as np
+    from hdrestir_b200 import configs
+    from hdrestir_b200.context import Context
+    ris = dict(candidate_count=CANDIDATES, use_reservoir=True, skip_visibility=False, max_depth=1)
+    rows = [y for ty in range(SAMPLE_OFFSET, (cam.height + TILE - 1) // TILE, SAMPLE_STRIDE)
+            for y in range(ty * TILE + 1, min(cam.height, ty * TILE + TILE) - 1)]
+    imgs = {}
+    c = Context(device=ctx.device, timings=False)
+    try:
+        c.share_scene(ctx)
+        for name, start, n in (("gpu", 0, frames), ("high", 10_000, high_frames)):
+            c.clear_persistent()
+            for f in range(start, start + n):
+                c.raycast(cam, f)
+                c.ris_path_trace(cam, f, **ris)
+                c.accumulate(f - start, firefly=True, mode="parity")
+            imgs[name] = c.download("Color").reshape(cam.height, cam.width, 4)[rows, :, :3].astype(np.float64)
+    finally:
+        c.close()
+    cpu = cpu_color.reshape(cam.height, cam.width, 4)[rows, :, :3].astype(np.float64)
+    peak = max(float(imgs["high"].max()), 1e-12)
+    m_gpu = float(np.mean(((imgs["gpu"] - imgs["high"]) / peak) ** 2))
+    m_cpu = float(np.mean(((cpu - imgs["high"]) / peak) ** 2))
+    return {"frames": frames, "high_sample_frames": high_frames, "rows": len(rows), "mse_gpu": m_gpu,
+            "mse_cpu_reference": m_cpu, "ratio": m_gpu / m_cpu if m_cpu > 0 else None,
+            "note": "same estimator and random streams on both sides, so equal MSE; the frames/s above are at "
+                    "this MSE"}
 
 
 def cpu_sample_label(height, frames_desc):
@@ -525,7 +566,8 @@ def run_ours(args, rank, local_rank, world):
     px = WIDTH * HEIGHT
     achieved = SHADOW_BYTES_PER_RAY * n_shadow / (t_shadow / 1000.0) / 1e9
     traffic, traffic_src = ncu_traffic("trace_shadow")
-    rays = 33 * px  # 1 primary (raycast) + 1 first bounce + 15 BSDF candidates + 16 shadow rays
+    # rays traced per frame: the primary (raycast) rays and the two queues of the last frame
+    rays = px + n_closest + n_shadow
     out = {
         "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -539,6 +581,7 @@ def run_ours(args, rank, local_rank, world):
                       "ris_shade": t_shade},
         "rays_per_frame": {"primary": px, "closest": n_closest, "shadow": n_shadow},
         "rays_per_s": rays / (total_ms / args.steps / 1000.0),
+        "rays_per_s_note": "rays traced: primary + closest-hit queue + shadow queue of a frame",
         "roofline": {"kernel": "trace_shadow_kernel (NEE shadow rays, any-hit)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": traffic, "traffic_source": traffic_src,
@@ -565,10 +608,14 @@ def run_ours(args, rank, local_rank, world):
         out["config3"] = config3_leg()
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        secs, kind = cpu_frames(scene, cam, range(3), threads)
+        secs, kind, cpu_color = cpu_frames(scene, cam, range(3), threads)
         value = 2.0 / sum(secs[1:])
+        out["mse"] = mse_block(ctx, cam, cpu_color, 3)
         out["cpu_baseline"] = {"value": value, "unit": "frames/s", "cores": threads, "kind": kind,
                                "sample": cpu_sample_label(HEIGHT, "frames 1 and 2 timed after frame 0")}
+        for v in out["variants"].values():  # every execution form against the same CPU baseline
+            v["vs_cpu_baseline"] = v["frames_per_s"] / value
+        out["vs_cpu_baseline"] = {"value": fps / value, "e2e": e2e_fps / value}
     ctx.close()
     if world > 1:
         import torch.distributed as dist

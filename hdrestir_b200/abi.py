@@ -23,6 +23,7 @@ CTX_TIMINGS, CTX_WIDE_BVH, CTX_LANE_PER_RAY, CTX_UNPHASED, CTX_PT_ONE_KERNEL = 1
 CTX_SPLIT_STACK = 64
 CTX_DEVICE_BUILD = 128
 CTX_RECORD_LIGHTS = 256
+CTX_REFERENCE_SHADOWS = 512
 RIS_REPROJECT = 4
 FMT_FLOAT32, FMT_FLOAT16, FMT_UNORM8, FMT_SNORM8, FMT_INT32 = 0, 1, 2, 3, 4
 FMT_DTYPES = {0: np.float32, 1: np.uint16, 2: np.uint8, 3: np.int8, 4: np.int32}
@@ -90,7 +91,8 @@ RIS_TRACE_ALL_RAYS, RIS_ONE_KERNEL = 1, 2
 
 
 class TraceTuning(C.Structure):
-    _fields_ = [("node_quorum", _i), ("blocks_per_sm", _i), ("trace_ms", _f), ("shade_shape", _i)]
+    _fields_ = [("node_quorum", _i), ("blocks_per_sm", _i), ("trace_ms", _f), ("shade_shape", _i),
+                ("shadow_shape", _i)]
 
 
 class ServerDesc(C.Structure):

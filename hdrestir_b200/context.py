@@ -66,13 +66,16 @@ def path_settings(max_depth=32, enable_subsurface=True, max_reflection_bounces=8
 class Context:
     def __init__(self, device: int = 0, timings: bool = True, hbm_budget: int = 0, wide_bvh: bool = False,
                  lane_per_ray: bool = False, unphased: bool = False, pt_one_kernel: bool = False,
-                 split_stack: bool = False, device_build: bool = False, record_lights: bool = False):
+                 split_stack: bool = False, device_build: bool = False, record_lights: bool = False,
+                 reference_shadows: bool = False):
         self._lib = abi.lib()
+        self.device = int(device)
         self._h = C.c_void_p()
         flags = ((abi.CTX_TIMINGS if timings else 0) | (abi.CTX_WIDE_BVH if wide_bvh else 0)
                  | (abi.CTX_LANE_PER_RAY if lane_per_ray else 0) | (abi.CTX_UNPHASED if unphased else 0)
                  | (abi.CTX_PT_ONE_KERNEL if pt_one_kernel else 0) | (abi.CTX_SPLIT_STACK if split_stack else 0)
-                 | (abi.CTX_DEVICE_BUILD if device_build else 0) | (abi.CTX_RECORD_LIGHTS if record_lights else 0))
+                 | (abi.CTX_DEVICE_BUILD if device_build else 0) | (abi.CTX_RECORD_LIGHTS if record_lights else 0)
+                 | (abi.CTX_REFERENCE_SHADOWS if reference_shadows else 0))
         desc = abi.CtxDesc(int(device), flags, int(hbm_budget))
         abi.check(self._lib.hdr_ctx_create(C.byref(self._h), C.byref(desc)))
         self.width = self.height = 0
@@ -228,21 +231,26 @@ class Context:
     def trace_tuning(self) -> dict:
         t = abi.TraceTuning()
         abi.check(self._lib.hdr_get_trace_tuning(self._h, C.byref(t)))
-        return {"node_quorum": t.node_quorum, "blocks_per_sm": t.blocks_per_sm, "shade_shape": t.shade_shape}
+        return {"node_quorum": t.node_quorum, "blocks_per_sm": t.blocks_per_sm, "shade_shape": t.shade_shape,
+                "shadow_shape": t.shadow_shape}
 
-    def set_trace_tuning(self, node_quorum: int, blocks_per_sm: int, shade_shape: int = 0) -> None:
-        t = abi.TraceTuning(int(node_quorum), int(blocks_per_sm), 0.0, int(shade_shape))
+    def set_trace_tuning(self, node_quorum: int, blocks_per_sm: int, shade_shape: int = 0,
+                         shadow_shape: int | None = None) -> None:
+        if shadow_shape is None:
+            shadow_shape = self.trace_tuning()["shadow_shape"]
+        t = abi.TraceTuning(int(node_quorum), int(blocks_per_sm), 0.0, int(shade_shape), int(shadow_shape))
         abi.check(self._lib.hdr_set_trace_tuning(self._h, C.byref(t)))
 
     def autotune_trace(self) -> dict:
         """Picks the fastest trace schedule on the last wavefront frame's ray queues."""
         t = abi.TraceTuning()
         abi.check(self._lib.hdr_autotune_trace(self._h, C.byref(t)))
-        return {"node_quorum": t.node_quorum, "blocks_per_sm": t.blocks_per_sm, "trace_ms": t.trace_ms}
+        return {"node_quorum": t.node_quorum, "blocks_per_sm": t.blocks_per_sm, "trace_ms": t.trace_ms,
+                "shadow_shape": t.shadow_shape}
 
     def trace_stats(self, rays: np.ndarray, walk: int, tmax: np.ndarray | None = None) -> np.ndarray:
         """Per-ray (nodes popped, leaves, triangles tested, answer) of one traversal form
-        (0 closest binary, 1 closest wide, 2 shadow binary, 3 shadow wide)."""
+        (0 closest binary, 1 closest wide, 2 shadow binary, 3 shadow wide, 4 shadow BVH)."""
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
         out = np.empty((len(rays), 4), np.int32)
         tp = None

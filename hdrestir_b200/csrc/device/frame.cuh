@@ -125,12 +125,14 @@ struct WaveBuffers {
 // stack on scenes shallow enough for the shared-memory-only one. node_quorum: the phased kernels keep stepping nodes while
 // this many lanes of a warp do. Grid: sm_count x blocks_per_sm persistent blocks.
 constexpr int kTraceLanePerRay = 1, kTraceUnphased = 2, kTraceSplitStack = 4;
+constexpr int kShadowShapes = 3;
 struct TraceTuning {
     int mode = 0;
     int node_quorum = 16;
     int blocks_per_sm = 16;
     int sm_count = 148;
     int shade_shape = 2;  // ris_shade launch shape, 0 .. kShadeShapes - 1 (128 x 3: fastest at 1080p)
+    int shadow_shape = 1; // shadow-BVH walk register budget, 0 .. kShadowShapes - 1: 64 / 80 / 90 registers
 };
 // ris_shade launch shapes: (threads per block, minimum resident blocks per SM)
 // = (256, 1), (256, 2), (128, 3), (128, 4)
@@ -138,6 +140,10 @@ constexpr int kShadeShapes = 4;
 // The two trace kernels over the queues of the last ris_generate (they read
 // the queue counts and reset nothing but their own fetch counters' use, so the
 // caller zeroes counts[2..3] before a rerun); returns the launches, -1 on error.
+// The shadow-ray queue q over the shadow BVH when the scene has it (s.sh4), else the
+// phased walk of the reference trees; *count rays, *fetch the hand-out counter.
+int launch_shadow_queue(const DeviceScene &s, const float4 *q, const int *count, int *fetch, unsigned char *occ,
+                        const TraceTuning &tune, unsigned *err, cudaStream_t st);
 int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &tune, unsigned *err, cudaStream_t st,
                       cudaEvent_t *ev_begin = nullptr, cudaEvent_t *ev_end = nullptr);
 // Spatial reuse (extension, spatial.cu): merges up to p.spatial_neighbors
@@ -193,6 +199,8 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
 // The same launchers with the closures' texture overrides compiled in
 // (wavefront_tex.cu); the ones above leave them out, for scenes without textures.
 namespace textured {
+int launch_shadow_queue(const DeviceScene &s, const float4 *q, const int *count, int *fetch, unsigned char *occ,
+                        const TraceTuning &tune, unsigned *err, cudaStream_t st);
 int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &tune, unsigned *err, cudaStream_t st,
                       cudaEvent_t *ev_begin = nullptr, cudaEvent_t *ev_end = nullptr);
 int launch_winner_visibility(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,

@@ -52,6 +52,12 @@ struct DeviceScene {
     int proper_boxes;          // 1: no node box of any tree is empty (min > max on some axis)
     int shallow;               // 1: the binary walk's stack never exceeds kShallowStack entries
     int has_textures;          // 1: some material has a texture (closures read uv and tangents)
+    // shadow-ray BVH (host/shadow_bvh.h): 4-wide SAH trees over the same triangles,
+    // walked for "hit nearer than the limit" queries when sh4 is 1
+    const float4 *sh4_nodes;   // 7 per node
+    const float4 *sh4_tris;    // 3 per triangle (tri_geo records in leaf order)
+    const int *sh4_inst_root;  // per instance: its mesh's root node, -1 = no triangles
+    int sh4;
     // This struct's own copy in device memory. Kernels take the scene by value
     // (parameter space); a non-inlined callee gets this pointer instead of the
     // parameter's address, which would make every thread copy the parameter
@@ -756,11 +762,20 @@ __device__ __forceinline__ bool trace_ray(const DeviceScene &s, V3 o, V3 d, floa
                   : trace_ray_binary<kAnyHit>(s, o, d, t_limit, hit, err);
 }
 
+}  // namespace hdr
+#include "shadow4.cuh"
+namespace hdr {
+
 // Shadow query of the reference, "IntersectScene(o, d) && Depth < limit"
-// (ris_direct_light_integrator.cpp:513-515): the closest-hit walk, stopped as
-// soon as its running closest t drops below limit (the running t only
-// decreases, so the answer is the full walk's).
+// (ris_direct_light_integrator.cpp:513-515). With the shadow BVH (s.sh4) its
+// 4-wide walk answers it; otherwise the closest-hit walk of the reference's
+// trees, stopped as soon as its running closest t drops below limit (the running
+// t only decreases, so the answer is the full walk's).
 __device__ __forceinline__ bool shadow_ray(const DeviceScene &s, V3 o, V3 d, float limit, unsigned &err) {
+    if (s.sh4) {
+        NoStats ns;
+        return shadow4_ray(s, o, d, limit, err, ns);
+    }
     HitId h;
     return trace_ray<true>(s, o, d, limit, h, err) && h.t < limit;
 }

@@ -22,6 +22,7 @@
 #include "device/blas_build.h"
 #include "device/frame.cuh"
 #include "host/scene_build.h"
+#include "host/shadow_bvh.h"
 
 namespace {
 
@@ -70,7 +71,8 @@ struct SceneStore {
     int device = 0;
     std::vector<void *> ptrs;
     size_t bytes = 0;
-    // the scene descriptor in device memory, [0] for the binary walk, [1] for the wide one
+    // the scene descriptor in device memory: [wide + 2 * sh4] (binary / wide walk, reference
+    // trees / shadow BVH for shadow rays)
     const hdr::DeviceScene *desc_dev = nullptr;
     // hdr_scene_set_instance_transforms: what the device rebuild of the instances and the TLAS needs
     int num_instances = 0, max_blas_depth = 0;
@@ -82,6 +84,11 @@ struct SceneStore {
     float *xf_staging = nullptr;    // 16 floats per instance
     int4 *tlas_stack = nullptr;     // num_instances + 2 entries
     int *tlas_info = nullptr;       // 4 ints
+    // shadow-ray BVH (host/shadow_bvh.h): present when sh4 is true; the TLAS part is
+    // rebuilt on the host when instances move
+    bool sh4 = false;
+    std::vector<int> sh4_inst_root;
+    int sh4_tlas_capacity = 0, sh4_blas_depth = 0;
     // the scene's arrays by DeviceScene field name, for hdr_scene_array
     std::map<std::string, std::pair<const void *, size_t>> arrays;
     ~SceneStore() {
@@ -572,6 +579,24 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     UP(f.blas4, blas4);
     UP(f.blas_roots, blas_roots);
     UP(f.tlas4, tlas4);
+    // shadow-ray BVH: built unless this ctx walks the reference trees for shadow rays
+    hdr::ShadowBvh sb;
+    if (!(c->flags & HDR_CTX_REFERENCE_SHADOWS)) {
+        if (!hdr::build_shadow_bvh(*desc, f.inst_bounds, sb, err)) {
+            cudaStreamSynchronize(c->stream);
+            c->allocated -= store->bytes;
+            return fail(HDR_EINVAL, "%s", err.c_str());
+        }
+    }
+    if (sb.ok) {
+        UP(sb.nodes, sh4_nodes);
+        UP(sb.tris, sh4_tris);
+        UP(sb.inst_root, sh4_inst_root);
+        store->sh4 = true;
+        store->sh4_inst_root = sb.inst_root;
+        store->sh4_tlas_capacity = sb.tlas_capacity;
+        store->sh4_blas_depth = sb.blas_depth;
+    }
 #undef UP
     {  // the device TLAS rebuild's inputs and scratch
         const size_t n = (size_t)f.num_instances;
@@ -610,8 +635,9 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     s.proper_boxes = (store->blas_proper && tlas_boxes_proper(f)) ? 1 : 0;
     s.shallow = (f.max_blas_depth + f.max_tlas_depth + 4 <= hdr::kShallowStack) ? 1 : 0;
     s.has_textures = f.textures.empty() ? 0 : 1;
+    s.sh4 = store->sh4 ? 1 : 0;
     // the descriptor itself, for callees that are not inlined into a kernel
-    hdr::DeviceScene copies[2] = {s, s};
+    hdr::DeviceScene copies[4] = {s, s, s, s};
     {
         DevBuf b;
         st = dev_alloc(c, b, sizeof(copies));
@@ -623,13 +649,14 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
         store->ptrs.push_back(b.ptr);
         store->bytes += b.bytes;
         store->desc_dev = (const hdr::DeviceScene *)b.ptr;
-        for (int w = 0; w < 2; ++w) {  // each copy points at itself
-            copies[w].wide = w;
+        for (int w = 0; w < 4; ++w) {  // each copy points at itself
+            copies[w].wide = w & 1;
+            copies[w].sh4 = (w >> 1) & s.sh4;
             copies[w].dev = store->desc_dev + w;
         }
         HDR_CUDA(cudaMemcpyAsync(b.ptr, copies, sizeof(copies), cudaMemcpyHostToDevice, c->stream));
     }
-    s.dev = store->desc_dev + s.wide;
+    s.dev = store->desc_dev + s.wide + 2 * s.sh4;
     const cudaError_t sync_err = cudaStreamSynchronize(c->stream);
     c->scene_store = store;  // owns the buffers from here on, also on the error path below
     c->scene_bytes_accounted = store->bytes;
@@ -905,7 +932,8 @@ hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src) {
     dst->scene_bytes_accounted = 0;
     dst->scene = src->scene;
     dst->scene.wide = (dst->flags & HDR_CTX_WIDE_BVH) ? 1 : 0;
-    dst->scene.dev = dst->scene_store->desc_dev + dst->scene.wide;
+    dst->scene.sh4 = (dst->scene_store->sh4 && !(dst->flags & HDR_CTX_REFERENCE_SHADOWS)) ? 1 : 0;
+    dst->scene.dev = dst->scene_store->desc_dev + dst->scene.wide + 2 * dst->scene.sh4;
     dst->scene_opaque = src->scene_opaque;
     dst->scene_light_geometry = src->scene_light_geometry;
     dst->scene_emissive = src->scene_emissive;
@@ -958,9 +986,30 @@ hdr_status hdr_scene_set_instance_transforms(hdr_ctx *c, const float *transforms
     }
     s.proper_boxes = (store->blas_proper && !info[3]) ? 1 : 0;
     s.shallow = (store->max_blas_depth + info[1] + 4 <= hdr::kShallowStack) ? 1 : 0;
-    hdr::DeviceScene copies[2] = {s, s};
-    for (int w = 0; w < 2; ++w) {
-        copies[w].wide = w;
+    if (store->sh4) {  // the shadow BVH's TLAS over the moved instances' world boxes
+        std::vector<float> b9((size_t)num_instances * 9), b6((size_t)num_instances * 6);
+        HDR_CUDA(cudaMemcpyAsync(b9.data(), store->inst_bounds, b9.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                                 c->stream));
+        HDR_CUDA(cudaStreamSynchronize(c->stream));
+        for (int i = 0; i < num_instances; ++i)
+            for (int k = 0; k < 6; ++k) b6[6 * (size_t)i + k] = b9[9 * (size_t)i + k];
+        std::vector<float> tlas;
+        int depth = 0;
+        if (hdr::rebuild_shadow_tlas(b6, store->sh4_inst_root, store->sh4_blas_depth, tlas, store->sh4_tlas_capacity,
+                                     depth)) {
+            HDR_CUDA(cudaMemcpyAsync(const_cast<float4 *>(s.sh4_nodes), tlas.data(), tlas.size() * sizeof(float),
+                                     cudaMemcpyHostToDevice, c->stream));
+            HDR_CUDA(cudaStreamSynchronize(c->stream));  // `tlas` is a host buffer
+        } else {
+            store->sh4 = false;  // too deep for the shadow walk's stack: the reference trees serve shadow rays
+        }
+    }
+    s.sh4 = (store->sh4 && !(c->flags & HDR_CTX_REFERENCE_SHADOWS)) ? 1 : 0;
+    s.dev = store->desc_dev + s.wide + 2 * s.sh4;
+    hdr::DeviceScene copies[4] = {s, s, s, s};
+    for (int w = 0; w < 4; ++w) {
+        copies[w].wide = w & 1;
+        copies[w].sh4 = (w >> 1) & (store->sh4 ? 1 : 0);
         copies[w].dev = store->desc_dev + w;
     }
     HDR_CUDA(cudaMemcpyAsync(const_cast<hdr::DeviceScene *>(store->desc_dev), copies, sizeof(copies),
@@ -1615,9 +1664,10 @@ hdr_status hdr_trace_rays(hdr_ctx *c, const float *rays, const float *tmax, int3
 
 hdr_status hdr_trace_stats(hdr_ctx *c, const float *rays, const float *tmax, int32_t n, int32_t walk,
                            int32_t *out) {
-    if (!c || (n > 0 && (!rays || !out)) || n < 0 || walk < 0 || walk > 3) return fail(HDR_EINVAL, "bad argument");
+    if (!c || (n > 0 && (!rays || !out)) || n < 0 || walk < 0 || walk > 4) return fail(HDR_EINVAL, "bad argument");
     std::lock_guard<std::mutex> lock(c->mu);
     if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_trace_stats before hdr_scene_upload");
+    if (walk == 4 && !c->scene.sh4) return fail(HDR_EINVAL, "walk 4: the scene has no shadow BVH on this ctx");
     if (n == 0) return HDR_OK;
     HDR_CUDA(cudaSetDevice(c->device));
     DevBuf dr, dt, dout;
@@ -1649,19 +1699,22 @@ hdr_status hdr_get_trace_tuning(hdr_ctx *c, hdr_trace_tuning *out) {
     out->blocks_per_sm = c->tune.blocks_per_sm;
     out->trace_ms = 0.0f;
     out->shade_shape = c->tune.shade_shape;
+    out->shadow_shape = c->tune.shadow_shape;
     return HDR_OK;
 }
 
 hdr_status hdr_set_trace_tuning(hdr_ctx *c, const hdr_trace_tuning *t) {
     if (!c || !t) return fail(HDR_EINVAL, "NULL argument");
     if (t->node_quorum < 1 || t->node_quorum > 32 || t->blocks_per_sm < 1 || t->blocks_per_sm > 64 ||
-        t->shade_shape < 0 || t->shade_shape >= hdr::kShadeShapes)
-        return fail(HDR_EINVAL, "node_quorum must be 1..32, blocks_per_sm 1..64, shade_shape 0..%d",
-                    hdr::kShadeShapes - 1);
+        t->shade_shape < 0 || t->shade_shape >= hdr::kShadeShapes || t->shadow_shape < 0 ||
+        t->shadow_shape >= hdr::kShadowShapes)
+        return fail(HDR_EINVAL, "node_quorum must be 1..32, blocks_per_sm 1..64, shade_shape 0..%d, shadow_shape 0..%d",
+                    hdr::kShadeShapes - 1, hdr::kShadowShapes - 1);
     std::lock_guard<std::mutex> lock(c->mu);
     c->tune.node_quorum = t->node_quorum;
     c->tune.blocks_per_sm = t->blocks_per_sm;
     c->tune.shade_shape = t->shade_shape;
+    c->tune.shadow_shape = t->shadow_shape;
     return HDR_OK;
 }
 
@@ -1677,10 +1730,13 @@ hdr_status hdr_autotune_trace(hdr_ctx *c, hdr_trace_tuning *best) {
     hdr::TraceTuning pick = c->tune;
     float pick_ms = 3.4e38f;
     cudaEvent_t ev[2] = {c->region_ev[3][0], c->region_ev[3][1]};
+    const int n_shapes = c->scene.sh4 ? hdr::kShadowShapes : 1;
+    for (int si = 0; si < n_shapes; ++si)
     for (int qi = 0; qi < (int)(sizeof(kQuorum) / sizeof(int)); ++qi) {
         for (int bi = 0; bi < (int)(sizeof(kBlocks) / sizeof(int)); ++bi) {
             t.node_quorum = kQuorum[qi];
             t.blocks_per_sm = kBlocks[bi];
+            if (c->scene.sh4) t.shadow_shape = si;
             float ms_min = 3.4e38f;
             for (int rep = 0; rep < 2; ++rep) {
                 // the trace kernels only read the queues and rewrite the same results; rerunning them
@@ -1701,11 +1757,13 @@ hdr_status hdr_autotune_trace(hdr_ctx *c, hdr_trace_tuning *best) {
     }
     c->tune.node_quorum = pick.node_quorum;
     c->tune.blocks_per_sm = pick.blocks_per_sm;
+    c->tune.shadow_shape = pick.shadow_shape;
     if (best) {
         best->node_quorum = pick.node_quorum;
         best->blocks_per_sm = pick.blocks_per_sm;
         best->trace_ms = pick_ms;
         best->shade_shape = c->tune.shade_shape;
+        best->shadow_shape = c->tune.shadow_shape;
     }
     return read_device_error(c);
 }

@@ -319,6 +319,8 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
         gf_inverse4f(h.xf, h.inv);
         h.bounds = transform_bounds(ranges[d.mesh], h.xf);
         h.centroid = (h.bounds.mn + h.bounds.mx) * 0.5f;
+        const float b6[6] = {h.bounds.mn.x, h.bounds.mn.y, h.bounds.mn.z, h.bounds.mx.x, h.bounds.mx.y, h.bounds.mx.z};
+        out.inst_bounds.insert(out.inst_bounds.end(), b6, b6 + 6);
         float rec[32];
         std::memcpy(rec, h.inv, sizeof(h.inv));
         const float *T = h.xf;

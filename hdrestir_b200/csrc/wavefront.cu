@@ -272,6 +272,74 @@ __global__ void __launch_bounds__(kTraceThreads, phased_min_blocks<kWide>()) tra
     if (e) atomicOr(err, e);
 }
 
+// Shadow queue over the shadow BVH (DeviceScene::sh4): persistent lanes, each on
+// its own ray's 4-wide walk. Node steps run while at least `quorum` lanes of
+// the warp are on node entries; then the parked leaves (triangle tests) and
+// instance entries of all lanes are served, and finished lanes take new rays.
+constexpr int kSh4Shared = 32;
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) trace_shadow4_kernel(DeviceScene s, const float4 *__restrict__ q,
+                                                                       const int *count, int *fetch,
+                                                                       unsigned char *occ, int quorum,
+                                                                       unsigned *err) {
+    __shared__ int col[kSh4Shared * kTraceThreads];
+    int deep[kSh4Stack - kSh4Shared];
+    Shadow4Walk<Sh4SplitStack<kSh4Shared, kTraceThreads>> w;
+    w.stack.col = col + threadIdx.x;
+    w.stack.deep = deep;
+    w.mode = kSh4ModeDone;
+    w.blocked = false;
+    const int n = *count;
+    unsigned e = 0;
+    NoStats ns;
+    int slot = -1;
+    bool drained = false;
+    for (;;) {
+        const bool done = w.mode == kSh4ModeDone;
+        if (done && slot >= 0) {
+            occ[slot] = w.blocked ? 1 : 0;
+            slot = -1;
+        }
+        const int k = fetch_ray(fetch, n, done, drained);
+        if (done) {
+            if (k >= 0) {
+                const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
+                w.start(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, b.w);
+                slot = __float_as_int(a.w);
+            } else {
+                w.mode = kSh4ModeIdle;
+            }
+        }
+        if (!__any_sync(kFullMask, w.mode != kSh4ModeIdle)) break;
+        do {
+            if (w.mode == kSh4ModeNode) w.node_step(s, e, ns);
+        } while (__popc(__ballot_sync(kFullMask, w.mode == kSh4ModeNode)) >= quorum);
+        if (w.mode == kSh4ModeLeaf) w.leaf(s, ns);
+        if (w.mode == kSh4ModeInst) w.inst(s, ns);
+    }
+    if (e) atomicOr(err, e);
+}
+
+// The shadow-ray queue q (count / fetch counters on the device, answers into occ).
+int launch_shadow_queue(const DeviceScene &s, const float4 *q, const int *count, int *fetch, unsigned char *occ,
+                        const TraceTuning &tune, unsigned *err, cudaStream_t st) {
+    const int tgrid = tune.sm_count * tune.blocks_per_sm;
+    if (s.sh4) {
+        // register budget: 64 (8 resident blocks), 80 (6) or 90 (5) per thread
+        auto k = tune.shadow_shape == 0 ? trace_shadow4_kernel<8>
+                                        : (tune.shadow_shape == 1 ? trace_shadow4_kernel<6> : trace_shadow4_kernel<5>);
+        k<<<tgrid, kTraceThreads, 0, st>>>(s, q, count, fetch, occ, tune.node_quorum, err);
+    } else {
+        const bool shallow = s.shallow && (tune.mode & kTraceSplitStack) == 0;
+        auto shadow = s.wide ? trace_shadow_phased_kernel<true, false>
+                             : (shallow ? trace_shadow_phased_kernel<false, true>
+                                        : trace_shadow_phased_kernel<false, false>);
+        shadow<<<tgrid, kTraceThreads, 0, st>>>(s, q, count, fetch, occ, tune.node_quorum, err);
+    }
+    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+}
+
 template <bool kWide, bool kRefill>
 __global__ void __launch_bounds__(kTraceThreads) trace_closest_kernel(DeviceScene s, const float4 *__restrict__ q,
                                                                       int *counts, float4 *hits, float *hit_v,
@@ -401,12 +469,8 @@ int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &t
         closest<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, err);
     }
     if (!mark(ev_end, 0) || !mark(ev_begin, 1)) return -1;
-    if (phased) {
-        auto shadow = s.wide      ? trace_shadow_phased_kernel<true, false>
-                       : shallow   ? trace_shadow_phased_kernel<false, true>
-                                   : trace_shadow_phased_kernel<false, false>;
-        shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts + 1, wb.counts + 2, wb.occ,
-                                                tune.node_quorum, err);
+    if (phased || s.sh4) {
+        if ((launch_shadow_queue)(s, wb.q_shadow, wb.counts + 1, wb.counts + 2, wb.occ, tune, err, st) < 0) return -1;
     } else {
         auto shadow = s.wide ? (refill ? trace_shadow_kernel<true, true> : trace_shadow_kernel<true, false>)
                              : (refill ? trace_shadow_kernel<false, true> : trace_shadow_kernel<false, false>);
@@ -509,12 +573,8 @@ __global__ void __launch_bounds__(256) ris_winner_fixup_kernel(DeviceScene s, Ca
 int launch_winner_visibility(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
                              GBufferView gb, ReservoirView rv, WaveBuffers wb, float4 *color, unsigned *err,
                              cudaStream_t st, const TraceTuning &tune) {
-    const int tgrid = tune.sm_count * tune.blocks_per_sm;
-    const bool shallow = s.shallow && (tune.mode & kTraceSplitStack) == 0;
-    auto shadow = s.wide ? trace_shadow_phased_kernel<true, false>
-                         : (shallow ? trace_shadow_phased_kernel<false, true> : trace_shadow_phased_kernel<false, false>);
-    shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_winner, wb.counts + 4, wb.counts + 5, wb.occ_winner,
-                                            tune.node_quorum, err);
+    if ((launch_shadow_queue)(s, wb.q_winner, wb.counts + 4, wb.counts + 5, wb.occ_winner, tune, err, st) < 0)
+        return -1;
     ris_winner_fixup_kernel<<<tune.sm_count * 4, 256, 0, st>>>(s, cam, frame_index, path_run(p), gb, rv, wb.q_winner,
                                                                wb.counts + 4, wb.occ_winner, color);
     return cudaGetLastError() == cudaSuccess ? 2 : -1;

@@ -252,6 +252,10 @@ typedef struct hdr_gbuffer_texel {
                                      HDR_CTX_WIDE_BVH, and the scene cannot be shared into a
                                      wide-walk ctx. Its scratch (about 0.5 KB per triangle while
                                      building) is outside the ctx's HBM budget. */
+#define HDR_CTX_REFERENCE_SHADOWS 512u /* shadow rays walk the reference's trees (closest-hit walk
+                                     stopped below the light distance) instead of the shadow BVH,
+                                     a 4-wide SAH tree over the same triangles built at upload;
+                                     the answers agree (same triangle test, conservative boxes) */
 #define HDR_CTX_RECORD_LIGHTS 256u /* diagnostic, no reference counterpart: the wavefront
                                      hdr_ris_path_trace records the light index each NEE candidate
                                      selected (UniformLightSampler::ProposeCandidate,
@@ -486,25 +490,30 @@ hdr_status hdr_trace_rays(hdr_ctx *ctx, const float *rays, const float *tmax, in
  * trace_ms: device time of the two trace kernels (autotune output).
  * shade_shape: launch shape of the resampling kernel: 0 = 256 threads with the
  * register file of one block per SM, 1 = 256 threads for two blocks,
- * 2 (default) / 3 = 128 threads for three / four blocks (no effect on results). */
+ * 2 (default) / 3 = 128 threads for three / four blocks (no effect on results).
+ * shadow_shape: register budget of the shadow-BVH walk kernel: 0 = 64 registers
+ * (8 resident blocks of 128 threads), 1 (default) = 80 (6 blocks), 2 = 90 (5 blocks). */
 typedef struct hdr_trace_tuning {
     int32_t node_quorum;
     int32_t blocks_per_sm;
     float trace_ms;
     int32_t shade_shape;
+    int32_t shadow_shape;
 } hdr_trace_tuning;
 hdr_status hdr_get_trace_tuning(hdr_ctx *ctx, hdr_trace_tuning *out);
 hdr_status hdr_set_trace_tuning(hdr_ctx *ctx, const hdr_trace_tuning *tuning);
 /* Autotuner: reruns the trace kernels of the last wavefront hdr_ris_path_trace
  * (they only read its ray queues and rewrite the same hit / occlusion slots)
- * over a grid of schedules, keeps the fastest in the ctx and returns it. */
+ * over a grid of schedules (node quorum x blocks per SM, and the shadow-BVH
+ * walk's register budget), keeps the fastest in the ctx and returns it. */
 hdr_status hdr_autotune_trace(hdr_ctx *ctx, hdr_trace_tuning *best);
 
 /* Diagnostic, no reference counterpart: the work one traversal form does per
  * ray. walk: 0 closest hit on the binary trees, 1 closest hit on their 4-wide
  * collapse, 2 shadow query on the binary trees, 3 shadow query on the 4-wide
- * collapse. out = n x int32[4]: nodes popped, leaves entered, triangles
- * tested, answer (hit / occluded). */
+ * collapse, 4 shadow query on the shadow BVH (stack entries popped, leaves and
+ * instances entered, triangles tested). out = n x int32[4]: nodes popped,
+ * leaves entered, triangles tested, answer (hit / occluded). */
 hdr_status hdr_trace_stats(hdr_ctx *ctx, const float *rays, const float *tmax, int32_t n, int32_t walk,
                            int32_t *out);
 
