@@ -110,6 +110,35 @@ JOB_PATH_TRACER, JOB_RIS = 0, 1
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
 
 
+MTL_FLOAT, MTL_FLOAT3, MTL_BOOL, MTL_ASSET = 0, 1, 2, 3
+
+
+class MtlParam(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("type", _i), ("value", _f * 3), ("asset", C.c_char_p)]
+
+
+class MtlConnection(C.Structure):
+    _fields_ = [("input", C.c_char_p), ("upstream_node", C.c_char_p)]
+
+
+class MtlNode(C.Structure):
+    _fields_ = [("path", C.c_char_p), ("shader_id", C.c_char_p), ("params", C.POINTER(MtlParam)),
+                ("num_params", _i), ("inputs", C.POINTER(MtlConnection)), ("num_inputs", _i)]
+
+
+class MtlTerminal(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("upstream_node", C.c_char_p)]
+
+
+class MtlNetwork(C.Structure):
+    _fields_ = [("nodes", C.POINTER(MtlNode)), ("num_nodes", _i), ("terminals", C.POINTER(MtlTerminal)),
+                ("num_terminals", _i)]
+
+
+class MtlTextures(C.Structure):
+    _fields_ = [("path", (C.c_char * 1024) * 4)]
+
+
 class CtxDesc(C.Structure):
     _fields_ = [("device", _i), ("flags", C.c_uint32), ("hbm_budget_bytes", C.c_size_t)]
 
@@ -191,6 +220,8 @@ def lib() -> C.CDLL:
             "hdr_server_take_result": (C.c_int, [vp, C.c_int64, vp, sz]),
             "hdr_server_load": (C.c_int, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(sz)]),
             "hdr_server_drain_finished": (C.c_int, [vp, C.POINTER(C.c_int64), i32, C.POINTER(i32)]),
+            "hdr_material_from_network": (C.c_int, [C.POINTER(MtlNetwork), C.POINTER(MaterialDesc),
+                                                    C.POINTER(MtlTextures)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

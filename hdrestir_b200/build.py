@@ -21,7 +21,7 @@ OBJ = PKG / "_build"
 LIB = PKG / "libhdrestir_b200.so"
 INCLUDE = PKG.parent / "include"
 
-SOURCES = ["hdr_abi.cpp", "host/scene_build.cpp", "host/shadow_bvh.cpp", "raycast.cu", "integrate.cu", "wavefront.cu", "accumulate.cu",
+SOURCES = ["hdr_abi.cpp", "host/scene_build.cpp", "host/shadow_bvh.cpp", "host/material_network.cpp", "raycast.cu", "integrate.cu", "wavefront.cu", "accumulate.cu",
            "accumulate_noalloc.cu", "server.cpp", "pathtrace.cu", "spatial.cu", "resolve.cu", "post.cu",
            "tlas.cu", "blas_build.cu", "wavefront_tex.cu"]
 

@@ -1435,6 +1435,15 @@ hdr_status hdr_resolve(hdr_ctx *c, const char *name, int32_t src_components, int
     const size_t want = pixels * (size_t)dst_components * kSize[component_format];
     if (dst_bytes != want)
         return fail(HDR_EINVAL, "resolve of '%s' writes %zu bytes, %zu given", name, want, dst_bytes);
+    // CopyFromFrameBuffer (hd_restir_render_buffer.cpp:117-127): a pixel of the frame buffer the size of a
+    // render-buffer pixel is copied as bytes, whatever the formats
+    if (src_px == (size_t)dst_components * kSize[component_format]) {
+        if (want)
+            HDR_CUDA(cudaMemcpyAsync(dst, src, want, dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                     c->stream));
+        if (!dst_on_device) HDR_CUDA(cudaStreamSynchronize(c->stream));
+        return HDR_OK;
+    }
     void *out = dst;
     if (!dst_on_device && want) {  // converted on the device, then copied out
         hdr_status st = ensure_buffer(c, "__resolve_staging", want, &out);

@@ -2,7 +2,9 @@
 // (hydra/hd_restir_render_buffer.cpp:46-73,113-148): a float frame buffer
 // ("Color", "Depth", "Albedo", "Normal") converted to the render buffer's
 // component format, so the renderer's resolve can take the image from HBM
-// instead of a host frame buffer. Per component c of a pixel:
+// instead of a host frame buffer. (A source pixel of the destination pixel's
+// size is copied as bytes by the caller, as CopyFromFrameBuffer does.) Per
+// component c of a pixel:
 //   c >= the source's components : 0
 //   Float32 : the value
 //   Float16 : GfHalf(value) (round to nearest even)

@@ -116,6 +116,51 @@ typedef struct hdr_material_desc { /* PreviewSurfaceParams field for field */
 
 enum { HDR_TEX_DIFFUSE = 0, HDR_TEX_METALLIC = 1, HDR_TEX_ROUGHNESS = 2, HDR_TEX_NORMAL = 3 };
 
+/* ---------------------------------------------------------------------------
+ * Material networks (HdRestirMaterial::Sync, hydra/hd_restir_material.cpp:22-424):
+ * a Hydra material network (UsdPreviewSurface, MaterialX standard_surface or
+ * open_pbr_surface, image nodes) mapped to the PreviewSurface parameters the
+ * passes shade with. Plain-C view of an HdMaterialNetwork2.
+ * ------------------------------------------------------------------------- */
+enum { HDR_MTL_FLOAT = 0, HDR_MTL_FLOAT3 = 1, HDR_MTL_BOOL = 2, HDR_MTL_ASSET = 3 };
+
+typedef struct hdr_mtl_param {  /* one entry of HdMaterialNode2::parameters */
+    const char *name;
+    int32_t type;                /* HDR_MTL_*: the type the VtValue holds (others are skipped) */
+    float value[3];              /* FLOAT: [0]; FLOAT3: [0..2]; BOOL: [0] != 0 */
+    const char *asset;           /* ASSET: the SdfAssetPath's asset path */
+} hdr_mtl_param;
+
+typedef struct hdr_mtl_connection {  /* HdMaterialNode2::inputConnections, one upstream node each */
+    const char *input;
+    const char *upstream_node;   /* node path */
+} hdr_mtl_connection;
+
+typedef struct hdr_mtl_node {
+    const char *path;            /* SdfPath of the node */
+    const char *shader_id;       /* the shader identifier the Sdr registry resolves (else the node type id) */
+    const hdr_mtl_param *params;
+    int32_t num_params;
+    const hdr_mtl_connection *inputs;
+    int32_t num_inputs;
+} hdr_mtl_node;
+
+typedef struct hdr_mtl_terminal {   /* HdMaterialNetwork2::terminals */
+    const char *name;            /* "mtlx:surface", "surface", ... */
+    const char *upstream_node;
+} hdr_mtl_terminal;
+
+typedef struct hdr_mtl_network {
+    const hdr_mtl_node *nodes;
+    int32_t num_nodes;
+    const hdr_mtl_terminal *terminals;
+    int32_t num_terminals;
+} hdr_mtl_network;
+
+typedef struct hdr_mtl_textures {  /* asset paths per HDR_TEX_* slot ("" = none) */
+    char path[4][1024];
+} hdr_mtl_textures;
+
 /* LightType order of scene/light_factory.h */
 enum { HDR_LIGHT_DISTANT = 0, HDR_LIGHT_DOME = 1, HDR_LIGHT_RECT = 2, HDR_LIGHT_POINT = 3 };
 
@@ -278,6 +323,18 @@ void hdr_ctx_destroy(hdr_ctx *ctx);
 int hdr_abi_version(void);
 /* Thread-local text of the last failure on this thread ("" if none). */
 const char *hdr_last_error(void);
+
+/* HdRestirMaterial::Sync's network walk (hydra/hd_restir_material.cpp:22-424), host only:
+ * from the surface terminal ("mtlx:surface", else "surface", else "outputs:surface",
+ * else the first by name) every upstream node once, depth first, inputs and parameters
+ * in name order; UsdPreviewSurface, standard_surface and open_pbr_surface parameters set
+ * the PreviewSurface fields (diffuse = base_color x base weight for the MaterialX
+ * surfaces), image nodes give the texture slot of the surface input their chain starts
+ * from. out starts from the PreviewSurfaceParams defaults (a material's first Sync); its
+ * texture pointers stay NULL: textures (may be NULL) receives the asset paths, which the
+ * host decodes into out->textures. */
+hdr_status hdr_material_from_network(const hdr_mtl_network *net, hdr_material_desc *out,
+                                     hdr_mtl_textures *textures);
 
 /* Uploads and builds the device scene: BLAS per mesh (BVH::Build,
  * renderContext/bvh.cpp:66-241), instances and TLAS (Scene::_BuildTLAS,
@@ -443,9 +500,11 @@ hdr_status hdr_download_wait(hdr_ctx *ctx);
 enum { HDR_FMT_FLOAT32 = 0, HDR_FMT_FLOAT16 = 1, HDR_FMT_UNORM8 = 2, HDR_FMT_SNORM8 = 3, HDR_FMT_INT32 = 4 };
 /* HdRestirRenderBuffer::CopyFromFrameBuffer (hydra/hd_restir_render_buffer.cpp:46-73,113-148)
  * on the device: the named float frame buffer (src_components floats per pixel: "Color" 4,
- * "Depth" 1, "Albedo" / "Normal" 3) converted per component as the render buffer's
- * _WriteOutput does, dst_components components of component_format per pixel (components
- * the source lacks are 0). dst is device memory on this ctx's GPU when dst_on_device
+ * "Depth" 1, "Albedo" / "Normal" 3) into dst_components components of component_format per
+ * pixel. As in the reference, a source pixel of the destination pixel's size is copied as
+ * bytes; otherwise each component is converted as _WriteOutput does (components the source
+ * lacks are 0). (For a multi-component source of another size the reference's conversion
+ * stops at a precondition of FrameBuffer::As; here it converts component by component.) dst is device memory on this ctx's GPU when dst_on_device
  * (ordered on the ctx stream; hdr_synchronize waits for it), else host memory (filled
  * before the call returns). dst_bytes must be exactly the converted image's size. */
 hdr_status hdr_resolve(hdr_ctx *ctx, const char *name, int32_t src_components, int32_t component_format,

@@ -22,6 +22,7 @@
 #include "pxr/base/work/loops.h"
 #include "accumulation_pass.h"
 #include "denoiser.h"
+#include "hydra/hd_restir_render_buffer.h"
 #include "upscale_pass.h"
 #include "path_trace_pass.h"
 #include "pxr/imaging/hio/image.h"
@@ -505,6 +506,24 @@ void ref_accumulate(float *color, float *accum, int width, int height, int frame
     pass.Execute(ctx);
     std::memcpy(color, ctx.buffers.GetFrameBuffer(kColorOutputName).Data(), n * sizeof(GfVec4f));
     std::memcpy(accum, ctx.buffers.GetFrameBuffer(kAccumColorBuf).Data(), n * sizeof(GfVec4f));
+}
+
+// HdRestirRenderBuffer::CopyFromFrameBuffer + Resolve (hydra/hd_restir_render_buffer.cpp:
+// 46-73, 113-148, 176-186) on a float frame buffer of `pixels` x src_components:
+// the render buffer is allocated with `format` (the HdFormat of the shim:
+// component type x 4 + components - 1), filled from the frame buffer and
+// resolved; dst receives Map()'s bytes. Returns the bytes written, or -1.
+int ref_resolve(const float *src, int pixels, int src_components, int format, unsigned char *dst) {
+    HdRestirRenderBuffer rb{SdfPath("/renderBuffer")};
+    if (!rb.Allocate(GfVec3i(pixels, 1, 1), (HdFormat)format, false)) return -1;
+    FrameBuffer fb{"Color", sizeof(float) * (size_t)src_components, (size_t)pixels};
+    std::memcpy(fb.Data(), src, sizeof(float) * (size_t)src_components * (size_t)pixels);
+    rb.CopyFromFrameBuffer(fb);
+    rb.Resolve();
+    const size_t bytes = HdDataSizeOfFormat((HdFormat)format) * (size_t)pixels;
+    std::memcpy(dst, rb.Map(), bytes);
+    rb.Unmap();
+    return (int)bytes;
 }
 
 const char *ref_version(void) { return "hdRestir reference sources compiled in place with the oracle shim"; }

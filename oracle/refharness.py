@@ -78,6 +78,8 @@ def lib() -> C.CDLL:
         L.ref_upscale.argtypes = [C.c_char_p, vp, C.c_int, C.c_int, C.c_int, vp]
         L.ref_denoise.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.ref_accumulate.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.ref_resolve.restype = C.c_int
+        L.ref_resolve.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp]
         _lib = L
     return _lib
 
@@ -239,3 +241,22 @@ def accumulate(color: np.ndarray, accum: np.ndarray, width: int, height: int, fr
     assert color.flags.c_contiguous and accum.flags.c_contiguous
     lib().ref_accumulate(color.ctypes.data_as(C.c_void_p), accum.ctypes.data_as(C.c_void_p), width, height,
                          int(frame), int(firefly))
+
+
+# component type order of the HdFormat shim (each followed by its 2/3/4-component variants)
+_HD_TYPES = {"unorm8": (0, np.uint8), "snorm8": (1, np.int8), "float16": (2, np.uint16), "float32": (3, np.float32),
+             "int32": (4, np.int32)}
+
+
+def resolve(values: np.ndarray, component_type: str, components: int) -> np.ndarray:
+    """The reference's HdRestirRenderBuffer filled from a float frame buffer
+    (CopyFromFrameBuffer) and resolved: values (pixels, source components) float32
+    -> (pixels, components) in the render buffer's component type (float16 as bits)."""
+    values = np.ascontiguousarray(values, np.float32)
+    pixels, src = values.shape
+    code, dt = _HD_TYPES[component_type]
+    fmt = 4 * code + components - 1
+    out = np.zeros((pixels, components), dt)
+    got = lib().ref_resolve(values.ctypes.data_as(C.c_void_p), pixels, src, fmt, out.ctypes.data_as(C.c_void_p))
+    assert got == out.nbytes, got
+    return out

@@ -1,12 +1,12 @@
-"""CPU restatement of HdRestirRenderBuffer's _WriteOutput — TEST INFRASTRUCTURE.
+"""CPU restatement of HdRestirRenderBuffer::CopyFromFrameBuffer and its
+_WriteOutput — TEST INFRASTRUCTURE.
 
 Only tests/ import this module, as the checker of hdr_resolve. It restates
-hydra/hd_restir_render_buffer.cpp:46-73 (the per-component conversion) as
-CopyFromFrameBuffer (:113-148) applies it to a float frame buffer. Parity
-unpinned: the reference's tests hold no render-buffer vectors and the Hydra
-plugin needs OpenUSD, which is not built here; the known answers in
-tests/test_render_buffer.py follow the source's arithmetic (float32 products,
-std::clamp, truncating integer casts, GfHalf rounding to nearest even).
+hydra/hd_restir_render_buffer.cpp:46-73 (the per-component conversion) and
+:113-148 (CopyFromFrameBuffer: a raw byte copy when the frame buffer's stride
+equals the render buffer's, else the conversion). Pinned bit for bit to the
+reference's own render buffer compiled in place against the HdFormat and GfHalf
+stand-ins (tests/test_render_buffer.py).
 """
 from __future__ import annotations
 
@@ -46,3 +46,18 @@ def write_output(values: np.ndarray, component_format: int, dst_components: int)
             raise ValueError(f"unknown component format {component_format}")
     out[:, ~have] = 0
     return out
+
+
+_COMPONENT_BYTES = {FLOAT32: 4, FLOAT16: 2, UNORM8: 1, SNORM8: 1, INT32: 4}
+_DTYPES = {FLOAT32: np.float32, FLOAT16: np.uint16, UNORM8: np.uint8, SNORM8: np.int8, INT32: np.int32}
+
+
+def copy_from_frame_buffer(values: np.ndarray, component_format: int, dst_components: int) -> np.ndarray:
+    """CopyFromFrameBuffer (hd_restir_render_buffer.cpp:113-148): when a pixel of the
+    frame buffer (source components x 4 bytes) has the render buffer's size the
+    bytes are copied as they are, otherwise each pixel goes through _WriteOutput."""
+    values = np.ascontiguousarray(values, np.float32)
+    pixels, src = values.shape
+    if src * 4 == dst_components * _COMPONENT_BYTES[component_format]:
+        return values.view(np.uint8).view(_DTYPES[component_format]).reshape(pixels, dst_components).copy()
+    return write_output(values, component_format, dst_components)
