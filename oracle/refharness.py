@@ -152,22 +152,35 @@ def gpu_pipeline_available() -> bool:
 
 
 def gpu_pipeline_render(scene, cam, frames, ris=True, candidate_count=16, use_reservoir=True, skip_visibility=False,
-                        max_depth=1, firefly=True, resolution_level=0) -> np.ndarray:
+                        max_depth=1, firefly=True, resolution_level=0, via_scene=False) -> np.ndarray:
     """The reference's RenderPipeline with the GPU passes of
     hdrestir_b200/integration/gpu_passes.h; returns "Color" after `frames` frames (window size:
-    with resolution_level > 0 the pipeline ends with the GPU upscale pass)."""
+    with resolution_level > 0 the pipeline ends with the GPU upscale pass). via_scene: the
+    device scene comes only from the reference's Scene inputs, through the scene hand-off of
+    hdrestir_b200/integration/scene_handoff.h, and the frames carry that reference Scene."""
     L = C.CDLL(str(GPU_LIB))
-    L.refgpu_render.restype = C.c_int
-    L.refgpu_render.argtypes = [C.POINTER(abi.SceneDesc), C.POINTER(abi.CameraDesc), C.c_int,
-                                C.POINTER(RefGpuParams), C.c_void_p]
+    fn = L.refgpu_render_scene if via_scene else L.refgpu_render
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(abi.SceneDesc), C.POINTER(abi.CameraDesc), C.c_int, C.POINTER(RefGpuParams),
+                   C.c_void_p]
     desc = scene.c_desc()
     out = np.zeros((cam.width * cam.height, 4), np.float32)
     p = RefGpuParams(1 if ris else 0, candidate_count, int(use_reservoir), int(skip_visibility), max_depth,
                      int(firefly), int(resolution_level))
-    n = L.refgpu_render(C.byref(desc), C.byref(cam.c_desc()), int(frames), C.byref(p), _p(out))
+    n = fn(C.byref(desc), C.byref(cam.c_desc()), int(frames), C.byref(p), _p(out))
     if n != len(out):
         raise RuntimeError("GPU pipeline render failed")
     return out
+
+
+def handoff_compare(scene) -> int:
+    """The scene hand-off's descriptor, built from the reference Scene inputs the
+    prims of `scene` make, against `scene`'s own descriptor (host only); 0 = equal."""
+    L = C.CDLL(str(GPU_LIB))
+    L.refgpu_handoff_compare.restype = C.c_int
+    L.refgpu_handoff_compare.argtypes = [C.POINTER(abi.SceneDesc)]
+    desc = scene.c_desc()
+    return int(L.refgpu_handoff_compare(C.byref(desc)))
 
 
 def rng_floats(seeds, count) -> np.ndarray:
