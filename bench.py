@@ -391,19 +391,21 @@ def config3_leg(reps: int = 2):
     return out
 
 
-def serving_leg(n_jobs: int):
-    """Config-4 serving: the same Poisson job stream (200 jobs/s) through the
+def serving_leg(n_jobs: int, rate: float = 200.0):
+    """Config-4 serving: the same Poisson job stream (`rate` jobs/s) through the
     server in serial mode (the plain per-frame pipeline, one job at a time) and
     in served mode (continuous batching). Latency = host wall time from a job's
     arrival to the step that finished it; images are identical in both modes
-    (tests/test_gpu_server.py), so the comparison is at equal MSE."""
+    (tests/test_gpu_server.py), so the comparison is at equal MSE. At 200 jobs/s
+    the jobs arrive faster than any mode serves them and the latencies measure
+    the drain of that backlog; at a rate the box sustains they measure service."""
     from hdrestir_b200 import abi, configs
     from hdrestir_b200.server import Server
-    jobs = configs.config4_jobs(n_jobs)
+    jobs = configs.config4_jobs(n_jobs, rate=rate)
     scenes = [configs.config0()[0], configs.config1()[0], configs.config2()[0]]
     cams = [configs.config_camera(j["cfg"], j["width"], j["height"]) for j in jobs]
     mpx_frames = sum(j["width"] * j["height"] * j["frames"] for j in jobs) / 1e6
-    out = {"workload": f"config 4: {n_jobs} jobs, Poisson 200 jobs/s, scenes config 0-2, "
+    out = {"workload": f"config 4: {n_jobs} jobs, Poisson {rate:g} jobs/s, scenes config 0-2, "
                        "256^2..2048x1152, 1-16 frames, ReSTIR (32 cand) or PathTracer (maxDepth 4); "
                        "HBM admission budget 120 GB",
            "mpx_frames": mpx_frames}
@@ -605,6 +607,7 @@ def run_ours(args, rank, local_rank, world):
         out["batched"] = batched_leg(ctx)
         out["orbit"] = orbit_leg(ctx)
         out["serving"] = serving_leg(args.serving_jobs)
+        out["serving_sustained"] = serving_leg(max(8, args.serving_jobs // 2), rate=8.0)
         out["config3"] = config3_leg()
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -91,11 +91,23 @@ struct SceneStore {
     int sh4_tlas_capacity = 0, sh4_blas_depth = 0;
     // the scene's arrays by DeviceScene field name, for hdr_scene_array
     std::map<std::string, std::pair<const void *, size_t>> arrays;
+    // hdr_ris_path_trace_batch's shared ray queues and result slots: one grow-only set per
+    // resident scene, whichever context leads a batch, so batches of changing images (a
+    // server's steps) allocate nothing once the set is large enough. batch_done orders the
+    // batches that use it across the leads' streams.
+    std::mutex batch_mu;
+    std::map<std::string, std::pair<void *, size_t>> batch_bufs;
+    cudaEvent_t batch_done = nullptr;
     ~SceneStore() {
-        if (ptrs.empty()) return;
+        if (ptrs.empty() && batch_bufs.empty()) return;
         int prev = 0;
         cudaGetDevice(&prev);
         cudaSetDevice(device);
+        if (batch_done) {
+            cudaEventSynchronize(batch_done);
+            cudaEventDestroy(batch_done);
+        }
+        for (auto &kv : batch_bufs) cudaFree(kv.second.first);
         for (void *p : ptrs) cudaFree(p);
         cudaSetDevice(prev);
     }
@@ -222,6 +234,31 @@ hdr_status ensure_scratch(hdr_ctx *c, const char *name, size_t bytes, void **out
     if (st != HDR_OK) return st;
     c->buffers[name] = nb;
     *out = nb.ptr;
+    return HDR_OK;
+}
+
+// A batch buffer of the scene store (batch_mu held): kept while large enough; grown
+// with a quarter of headroom once every batch that used the old one has finished.
+// Its bytes count toward the scene's memory.
+hdr_status ensure_batch_scratch(SceneStore *store, const char *name, size_t bytes, void **out) {
+    auto it = store->batch_bufs.find(name);
+    if (it != store->batch_bufs.end() && it->second.second >= bytes) {
+        *out = it->second.first;
+        return HDR_OK;
+    }
+    if (it != store->batch_bufs.end()) {
+        if (store->batch_done) HDR_CUDA(cudaEventSynchronize(store->batch_done));
+        cudaFree(it->second.first);
+        store->bytes -= it->second.second;
+        store->batch_bufs.erase(it);
+    }
+    const size_t want = std::max<size_t>(16, bytes + bytes / 4);
+    void *p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) return fail(HDR_ENOMEM, "cudaMalloc(%zu) for batch queues: %s", want, cudaGetErrorString(e));
+    store->batch_bufs[name] = {p, want};
+    store->bytes += want;
+    *out = p;
     return HDR_OK;
 }
 
@@ -1150,21 +1187,26 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
     }
     if (total_c >= (1ll << 31) || total_s >= (1ll << 31))
         return fail(HDR_EINVAL, "batch of %lld closest / %lld shadow ray slots exceeds 2^31", total_c, total_s);
-    // the shared queues and result slots live on the lead ctx
+    // the shared queues and result slots belong to the resident scene, whichever ctx leads
+    SceneStore *store = lead->scene_store.get();
+    std::lock_guard<std::mutex> batch_lock(store->batch_mu);
     hdr::WaveBuffers all{};
     void *q;
-    if ((st = ensure_scratch(lead, "__batch_q_closest", (size_t)total_c * 32, &q)) != HDR_OK) return st;
+    if ((st = ensure_batch_scratch(store, "q_closest", (size_t)total_c * 32, &q)) != HDR_OK) return st;
     all.q_closest = (float4 *)q;
-    if ((st = ensure_scratch(lead, "__batch_q_shadow", (size_t)total_s * 32, &q)) != HDR_OK) return st;
+    if ((st = ensure_batch_scratch(store, "q_shadow", (size_t)total_s * 32, &q)) != HDR_OK) return st;
     all.q_shadow = (float4 *)q;
-    if ((st = ensure_scratch(lead, "__batch_counts", 16, &q)) != HDR_OK) return st;
+    if ((st = ensure_batch_scratch(store, "counts", 32, &q)) != HDR_OK) return st;
     all.counts = (int *)q;
-    if ((st = ensure_scratch(lead, "__batch_hits", (size_t)total_c * 16, &q)) != HDR_OK) return st;
+    if ((st = ensure_batch_scratch(store, "hits", (size_t)total_c * 16, &q)) != HDR_OK) return st;
     all.hits = (float4 *)q;
-    if ((st = ensure_scratch(lead, "__batch_hit_v", (size_t)total_c * 4, &q)) != HDR_OK) return st;
+    if ((st = ensure_batch_scratch(store, "hit_v", (size_t)total_c * 4, &q)) != HDR_OK) return st;
     all.hit_v = (float *)q;
-    if ((st = ensure_scratch(lead, "__batch_occ", (size_t)total_s, &q)) != HDR_OK) return st;
+    if ((st = ensure_batch_scratch(store, "occ", (size_t)total_s, &q)) != HDR_OK) return st;
     all.occ = (unsigned char *)q;
+    if (!store->batch_done) HDR_CUDA(cudaEventCreateWithFlags(&store->batch_done, cudaEventDisableTiming));
+    // the previous batch on this scene (another lead's stream) has finished with the queues
+    HDR_CUDA(cudaStreamWaitEvent(lead->stream, store->batch_done, 0));
     // every image's earlier work (its raycast) runs on its own stream: the lead stream waits for it
     for (int32_t i = 1; i < n; ++i) {
         HDR_CUDA(cudaEventRecord(ctxs[i]->sync_ev, ctxs[i]->stream));
@@ -1202,10 +1244,11 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
     }
     // later work on each image's own stream (accumulate, download) waits for the batch
     HDR_CUDA(cudaEventRecord(lead->sync_ev, s));
+    HDR_CUDA(cudaEventRecord(store->batch_done, s));
     for (int32_t i = 1; i < n; ++i) HDR_CUDA(cudaStreamWaitEvent(ctxs[i]->stream, lead->sync_ev, 0));
     lead->launches += (uint64_t)(2 * n + 2);
-    lead->last_wave = all;
-    lead->have_wave = true;
+    // the queues belong to the scene and the next batch reuses them: no autotuning rerun of this one
+    lead->have_wave = false;
     return end_pass(lead, 1);
 }
 

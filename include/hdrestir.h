@@ -390,7 +390,10 @@ hdr_status hdr_ris_path_trace(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame
  * that cannot take the wavefront form (max_depth > 1, non-opaque scene,
  * HDR_RIS_ONE_KERNEL) or do not share the scene are rendered one after
  * another instead. The work runs on ctxs[0]'s stream; the other ctxs' streams
- * are ordered before and after it. A context may appear only once. */
+ * are ordered before and after it. A context may appear only once. The shared
+ * ray queues and result slots belong to the resident scene (grow-only, outside
+ * the contexts' HBM budgets), so batches of changing images allocate nothing once
+ * they are large enough; batches on one scene are ordered by an event. */
 hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camera *cams,
                                     const int32_t *frame_indices, const hdr_ris_params *params);
 
