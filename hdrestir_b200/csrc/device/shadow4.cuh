@@ -262,6 +262,142 @@ struct Sh4LocalStack {
     __device__ __forceinline__ void set(int k, T v) { e[k] = v; }
 };
 
+// Closest-hit walk over the same trees (IntersectScene, scene.cpp:409-535), with
+// the reference's answer: boxes are culled only beyond the running closest t
+// (conservatively, as above), every triangle test is IntersectTriangle in its
+// instance's space, and among hits at equal t the smallest (instance position in
+// the reference TLAS's leaf order, triangle index in the reference BLAS order)
+// wins, the hit the reference's left-first walks meet first with their strict
+// `<`. Same phases as the shadow walk.
+template <class Stk>
+struct Closest4Walk {
+    V3 o, d, oo, od;
+    Sh4Ray wr, br;
+    float best_t, best_u, best_v;
+    int best_inst, best_tri, best_rank;
+    int cur_inst, cur_rank;
+    int sp, cur, mode;
+    Stk stack;
+
+    __device__ __forceinline__ void take(int e) {
+        cur = e;
+        const int tag = e & 3;
+        mode = e < 0 ? kSh4ModeDone : (tag == kSh4Leaf ? kSh4ModeLeaf : (tag == kSh4Inst ? kSh4ModeInst : kSh4ModeNode));
+    }
+    __device__ __forceinline__ void next() { take(sp > 0 ? stack.get(--sp) : -1); }
+
+    __device__ __forceinline__ void start(const DeviceScene &s, V3 ro, V3 rd) {
+        o = ro;
+        d = rd;
+        oo = ro;
+        od = rd;
+        wr = sh4_ray(ro, rd);
+        br = wr;
+        best_t = 1e30f;  // IntersectScene's initial closest distance
+        best_u = best_v = 0.0f;
+        best_inst = best_tri = -1;
+        best_rank = 0x7fffffff;
+        cur_inst = -1;
+        cur_rank = 0x7fffffff;
+        sp = 0;
+        take(s.has_tlas ? ((0 << 2) | kSh4Tlas) : -1);
+    }
+
+    template <class St>
+    __device__ __forceinline__ void node_step(const DeviceScene &s, unsigned &err, St &st) {
+        st.pop();
+        const int tag = cur & 3, idx = cur >> 2;
+        const bool blas = tag == kSh4Blas;
+        float tn[4];
+        int4 code;
+        const unsigned hits = sh4_children(s.sh4_nodes + 7 * (size_t)idx, blas ? br : wr, best_t, tn, code);
+        if (!hits) {
+            next();
+            return;
+        }
+        if (sp + 4 > Stk::kCapacity) {
+            err |= kErrShadowStack;
+            sp = 0;
+            take(-1);
+            return;
+        }
+        const int codes[4] = {code.x, code.y, code.z, code.w};
+        int ent[4];
+        int pick = -1, second = -1;
+        float t_pick = 3.402823466e+38f, t_second = 3.402823466e+38f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int c = codes[k];
+            ent[k] = c >= 0 ? ((c << 2) | tag) : (blas ? (((~c) << 2) | kSh4Leaf) : ((((~c) >> 2) << 2) | kSh4Inst));
+            if (!((hits >> k) & 1u)) continue;
+            if (tn[k] < t_pick) {
+                t_second = t_pick;
+                second = pick;
+                t_pick = tn[k];
+                pick = k;
+            } else if (tn[k] < t_second) {
+                t_second = tn[k];
+                second = k;
+            }
+        }
+        // the nearest in hand, the next nearest pushed last (taken next), the others below it
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k != pick && k != second && ((hits >> k) & 1u)) stack.set(sp++, ent[k]);
+        if (second >= 0) stack.set(sp++, ent[second]);
+        take(ent[pick]);
+    }
+
+    template <class St>
+    __device__ __forceinline__ void leaf(const DeviceScene &s, St &st) {
+        const int p = cur >> 2, first = p >> 2, cnt = (p & 3) + 1;
+        st.leaf();
+        for (int q = 0; q < cnt; ++q) {
+            st.tri();
+            const float4 *g = s.sh4_tris + 3 * (size_t)(first + q);
+            float t, u, v;
+            if (!tri_test(oo, od, g, t, u, v)) continue;
+            const int tri = __float_as_int(__ldg(&g[2].y));
+            if (t < best_t || (t == best_t && (cur_rank < best_rank || (cur_rank == best_rank && tri < best_tri)))) {
+                best_t = t;
+                best_u = u;
+                best_v = v;
+                best_inst = cur_inst;
+                best_rank = cur_rank;
+                best_tri = tri;
+            }
+        }
+        next();
+    }
+
+    template <class St>
+    __device__ __forceinline__ void inst(const DeviceScene &s, St &st) {
+        const int ii = cur >> 2;
+        st.leaf();
+        const float4 *ip = s.instances + 8 * (size_t)ii;
+        const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2), m3 = __ldg(ip + 3);
+        const float inv[16] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w,
+                               m2.x, m2.y, m2.z, m2.w, m3.x, m3.y, m3.z, m3.w};
+        oo = m4f_transform(inv, o);
+        od = m4f_transform_dir(inv, d);
+        br = sh4_ray(oo, od);
+        cur_inst = ii;
+        cur_rank = __ldg(&s.sh4_inst_rank[ii]);
+        take((__ldg(&s.sh4_inst_root[ii]) << 2) | kSh4Blas);
+    }
+
+    template <class St>
+    __device__ __forceinline__ void step(const DeviceScene &s, unsigned &err, St &st) {
+        if (mode == kSh4ModeNode)
+            node_step(s, err, st);
+        else if (mode == kSh4ModeLeaf)
+            leaf(s, st);
+        else if (mode == kSh4ModeInst)
+            inst(s, st);
+    }
+    __device__ __forceinline__ bool found() const { return best_inst >= 0; }
+};
+
 // One ray's answer (callers outside the wavefront trace kernels).
 template <class St>
 __device__ inline bool shadow4_ray(const DeviceScene &s, V3 o, V3 d, float limit, unsigned &err, St &st) {
@@ -271,4 +407,20 @@ __device__ inline bool shadow4_ray(const DeviceScene &s, V3 o, V3 d, float limit
     return w.blocked;
 }
 
+}  // namespace hdr
+
+namespace hdr {
+// Closest hit of one ray (callers outside the wavefront trace kernels).
+template <class St>
+__device__ inline bool closest4_ray(const DeviceScene &s, V3 o, V3 d, HitId &hit, unsigned &err, St &st) {
+    Closest4Walk<Sh4LocalStack<int, kSh4Stack>> w;
+    w.start(s, o, d);
+    while (w.mode != kSh4ModeDone) w.step(s, err, st);
+    hit.t = w.best_t;
+    hit.inst = w.best_inst;
+    hit.tri = w.best_tri;
+    hit.u = w.best_u;
+    hit.v = w.best_v;
+    return w.found();
+}
 }  // namespace hdr

@@ -57,7 +57,9 @@ struct DeviceScene {
     const float4 *sh4_nodes;   // 7 per node
     const float4 *sh4_tris;    // 3 per triangle (tri_geo records in leaf order)
     const int *sh4_inst_root;  // per instance: its mesh's root node, -1 = no triangles
-    int sh4;
+    const int *sh4_inst_rank;  // per instance: its position in the reference TLAS's leaf order
+    int sh4;                   // 1: shadow queries walk the 4-wide SAH trees
+    int sh4_closest;           // 1: closest hits walk them too (opt-in, HDR_CTX_SAH_CLOSEST)
     // This struct's own copy in device memory. Kernels take the scene by value
     // (parameter space); a non-inlined callee gets this pointer instead of the
     // parameter's address, which would make every thread copy the parameter
@@ -755,16 +757,25 @@ __device__ bool trace_ray_wide(const DeviceScene &s, V3 o, V3 d, float t_limit, 
     return hit.inst >= 0;
 }
 
+}  // namespace hdr
+#include "shadow4.cuh"
+namespace hdr {
+
+// A ray's walk: the reference's own trees (binary, or their 4-wide collapse),
+// or, for closest hits with s.sh4_closest, the Closest4Walk over the 4-wide SAH
+// trees (the reference's answer except where the reference's own rounded box
+// tests cull a hit, e.g. on coplanar surfaces).
 template <bool kAnyHit>
 __device__ __forceinline__ bool trace_ray(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId &hit,
                                           unsigned &err) {
+    if (!kAnyHit && s.sh4_closest) {
+        NoStats ns;
+        return closest4_ray(s, o, d, hit, err, ns);
+    }
     return s.wide ? trace_ray_wide<kAnyHit>(s, o, d, t_limit, hit, err)
                   : trace_ray_binary<kAnyHit>(s, o, d, t_limit, hit, err);
 }
 
-}  // namespace hdr
-#include "shadow4.cuh"
-namespace hdr {
 
 // Shadow query of the reference, "IntersectScene(o, d) && Depth < limit"
 // (ris_direct_light_integrator.cpp:513-515). With the shadow BVH (s.sh4) its

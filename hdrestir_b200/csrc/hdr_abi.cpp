@@ -71,8 +71,8 @@ struct SceneStore {
     int device = 0;
     std::vector<void *> ptrs;
     size_t bytes = 0;
-    // the scene descriptor in device memory: [wide + 2 * sh4] (binary / wide walk, reference
-    // trees / shadow BVH for shadow rays)
+    // the scene descriptor in device memory: [wide + 2 * sh4 + 4 * sh4_closest] (binary / wide
+    // walk of the reference trees; shadow and closest-hit queries on the 4-wide SAH trees)
     const hdr::DeviceScene *desc_dev = nullptr;
     // hdr_scene_set_instance_transforms: what the device rebuild of the instances and the TLAS needs
     int num_instances = 0, max_blas_depth = 0;
@@ -619,7 +619,7 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     // shadow-ray BVH: built unless this ctx walks the reference trees for shadow rays
     hdr::ShadowBvh sb;
     if (!(c->flags & HDR_CTX_REFERENCE_SHADOWS)) {
-        if (!hdr::build_shadow_bvh(*desc, f.inst_bounds, sb, err)) {
+        if (!hdr::build_shadow_bvh(*desc, f, sb, err)) {
             cudaStreamSynchronize(c->stream);
             c->allocated -= store->bytes;
             return fail(HDR_EINVAL, "%s", err.c_str());
@@ -629,6 +629,7 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
         UP(sb.nodes, sh4_nodes);
         UP(sb.tris, sh4_tris);
         UP(sb.inst_root, sh4_inst_root);
+        UP(sb.inst_rank, sh4_inst_rank);
         store->sh4 = true;
         store->sh4_inst_root = sb.inst_root;
         store->sh4_tlas_capacity = sb.tlas_capacity;
@@ -673,8 +674,9 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     s.shallow = (f.max_blas_depth + f.max_tlas_depth + 4 <= hdr::kShallowStack) ? 1 : 0;
     s.has_textures = f.textures.empty() ? 0 : 1;
     s.sh4 = store->sh4 ? 1 : 0;
+    s.sh4_closest = (s.sh4 && (c->flags & HDR_CTX_SAH_CLOSEST)) ? 1 : 0;
     // the descriptor itself, for callees that are not inlined into a kernel
-    hdr::DeviceScene copies[4] = {s, s, s, s};
+    hdr::DeviceScene copies[8] = {s, s, s, s, s, s, s, s};
     {
         DevBuf b;
         st = dev_alloc(c, b, sizeof(copies));
@@ -686,14 +688,15 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
         store->ptrs.push_back(b.ptr);
         store->bytes += b.bytes;
         store->desc_dev = (const hdr::DeviceScene *)b.ptr;
-        for (int w = 0; w < 4; ++w) {  // each copy points at itself
+        for (int w = 0; w < 8; ++w) {  // each copy points at itself
             copies[w].wide = w & 1;
             copies[w].sh4 = (w >> 1) & s.sh4;
+            copies[w].sh4_closest = (w >> 2) & copies[w].sh4;
             copies[w].dev = store->desc_dev + w;
         }
         HDR_CUDA(cudaMemcpyAsync(b.ptr, copies, sizeof(copies), cudaMemcpyHostToDevice, c->stream));
     }
-    s.dev = store->desc_dev + s.wide + 2 * s.sh4;
+    s.dev = store->desc_dev + s.wide + 2 * s.sh4 + 4 * s.sh4_closest;
     const cudaError_t sync_err = cudaStreamSynchronize(c->stream);
     c->scene_store = store;  // owns the buffers from here on, also on the error path below
     c->scene_bytes_accounted = store->bytes;
@@ -970,7 +973,9 @@ hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src) {
     dst->scene = src->scene;
     dst->scene.wide = (dst->flags & HDR_CTX_WIDE_BVH) ? 1 : 0;
     dst->scene.sh4 = (dst->scene_store->sh4 && !(dst->flags & HDR_CTX_REFERENCE_SHADOWS)) ? 1 : 0;
-    dst->scene.dev = dst->scene_store->desc_dev + dst->scene.wide + 2 * dst->scene.sh4;
+    dst->scene.sh4_closest = (dst->scene.sh4 && (dst->flags & HDR_CTX_SAH_CLOSEST)) ? 1 : 0;
+    dst->scene.dev =
+        dst->scene_store->desc_dev + dst->scene.wide + 2 * dst->scene.sh4 + 4 * dst->scene.sh4_closest;
     dst->scene_opaque = src->scene_opaque;
     dst->scene_light_geometry = src->scene_light_geometry;
     dst->scene_emissive = src->scene_emissive;
@@ -1032,21 +1037,31 @@ hdr_status hdr_scene_set_instance_transforms(hdr_ctx *c, const float *transforms
             for (int k = 0; k < 6; ++k) b6[6 * (size_t)i + k] = b9[9 * (size_t)i + k];
         std::vector<float> tlas;
         int depth = 0;
+        // closest-hit tie-breaks follow the rebuilt reference TLAS's instance order
+        std::vector<int> tlas_inst((size_t)num_instances), rank;
+        HDR_CUDA(cudaMemcpyAsync(tlas_inst.data(), s.tlas_inst, tlas_inst.size() * sizeof(int),
+                                 cudaMemcpyDeviceToHost, c->stream));
+        HDR_CUDA(cudaStreamSynchronize(c->stream));
+        hdr::shadow_ranks(tlas_inst, num_instances, rank);
         if (hdr::rebuild_shadow_tlas(b6, store->sh4_inst_root, store->sh4_blas_depth, tlas, store->sh4_tlas_capacity,
                                      depth)) {
             HDR_CUDA(cudaMemcpyAsync(const_cast<float4 *>(s.sh4_nodes), tlas.data(), tlas.size() * sizeof(float),
                                      cudaMemcpyHostToDevice, c->stream));
-            HDR_CUDA(cudaStreamSynchronize(c->stream));  // `tlas` is a host buffer
+            HDR_CUDA(cudaMemcpyAsync(const_cast<int *>(s.sh4_inst_rank), rank.data(), rank.size() * sizeof(int),
+                                     cudaMemcpyHostToDevice, c->stream));
+            HDR_CUDA(cudaStreamSynchronize(c->stream));  // `tlas` and `rank` are host buffers
         } else {
             store->sh4 = false;  // too deep for the shadow walk's stack: the reference trees serve shadow rays
         }
     }
     s.sh4 = (store->sh4 && !(c->flags & HDR_CTX_REFERENCE_SHADOWS)) ? 1 : 0;
-    s.dev = store->desc_dev + s.wide + 2 * s.sh4;
-    hdr::DeviceScene copies[4] = {s, s, s, s};
-    for (int w = 0; w < 4; ++w) {
+    s.sh4_closest = (s.sh4 && (c->flags & HDR_CTX_SAH_CLOSEST)) ? 1 : 0;
+    s.dev = store->desc_dev + s.wide + 2 * s.sh4 + 4 * s.sh4_closest;
+    hdr::DeviceScene copies[8] = {s, s, s, s, s, s, s, s};
+    for (int w = 0; w < 8; ++w) {
         copies[w].wide = w & 1;
         copies[w].sh4 = (w >> 1) & (store->sh4 ? 1 : 0);
+        copies[w].sh4_closest = (w >> 2) & copies[w].sh4;
         copies[w].dev = store->desc_dev + w;
     }
     HDR_CUDA(cudaMemcpyAsync(const_cast<hdr::DeviceScene *>(store->desc_dev), copies, sizeof(copies),
@@ -1716,10 +1731,10 @@ hdr_status hdr_trace_rays(hdr_ctx *c, const float *rays, const float *tmax, int3
 
 hdr_status hdr_trace_stats(hdr_ctx *c, const float *rays, const float *tmax, int32_t n, int32_t walk,
                            int32_t *out) {
-    if (!c || (n > 0 && (!rays || !out)) || n < 0 || walk < 0 || walk > 4) return fail(HDR_EINVAL, "bad argument");
+    if (!c || (n > 0 && (!rays || !out)) || n < 0 || walk < 0 || walk > 5) return fail(HDR_EINVAL, "bad argument");
     std::lock_guard<std::mutex> lock(c->mu);
     if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_trace_stats before hdr_scene_upload");
-    if (walk == 4 && !c->scene.sh4) return fail(HDR_EINVAL, "walk 4: the scene has no shadow BVH on this ctx");
+    if (walk >= 4 && !c->scene.sh4) return fail(HDR_EINVAL, "walk %d: the scene has no 4-wide SAH trees on this ctx", walk);
     if (n == 0) return HDR_OK;
     HDR_CUDA(cudaSetDevice(c->device));
     DevBuf dr, dt, dout;

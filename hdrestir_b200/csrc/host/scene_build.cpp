@@ -261,6 +261,8 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
             out.mesh_ranges.insert(out.mesh_ranges.end(), r6, r6 + 6);
             node_base[mi] = (int)out.num_blas_nodes;
             tri_base[mi] = (int)out.num_triangles;
+            out.mesh_tri_base.push_back((int)out.num_triangles);
+            out.mesh_tri_count.push_back(e.num_tris);
             blas_ok[mi] = e.num_nodes > 0 ? 1 : 0;
             wide_base[mi] = 0;
             if (e.max_depth > out.max_blas_depth) out.max_blas_depth = e.max_depth;
@@ -274,6 +276,8 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
         out.mesh_ranges.insert(out.mesh_ranges.end(), r6, r6 + 6);
         node_base[mi] = (int)out.num_blas_nodes;
         tri_base[mi] = (int)out.num_triangles;
+        out.mesh_tri_base.push_back((int)out.num_triangles);
+        out.mesh_tri_count.push_back((int)b.tris.size());
         blas_ok[mi] = b.nodes.empty() ? 0 : 1;
         if (b.max_depth > out.max_blas_depth) out.max_blas_depth = b.max_depth;
         for (const BlasNode &n : b.nodes) put_node(out.blas_nodes, n.bounds, n.left, n.count);

@@ -80,6 +80,7 @@ struct FlatScene {
     std::vector<int> tlas_inst;
     std::vector<float> mesh_ranges; // 6 floats per mesh: MeshSubset::range min.xyz, max.xyz
     std::vector<float> inst_bounds; // 6 floats per instance: world box min.xyz, max.xyz
+    std::vector<int> mesh_tri_base, mesh_tri_count;  // per mesh: its triangle records in tri_geo
     std::vector<float> materials;   // kMaterialFloats per material
     std::vector<float> textures;    // every material texture's RGB texels, back to back
     std::vector<float> lights;      // kLightFloats per light

@@ -1,8 +1,11 @@
 // Shadow-ray BVH builder (see shadow_bvh.h).
 #include "shadow_bvh.h"
 
+#include "scene_build.h"
+
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <cstring>
 
 #include "../device/tri_setup.cuh"
@@ -237,55 +240,78 @@ bool rebuild_shadow_tlas(const std::vector<float> &inst_bounds, const std::vecto
     return 1 + 3 * (tlas_depth + blas_depth) <= kSh4Stack;
 }
 
-bool build_shadow_bvh(const hdr_scene_desc &desc, const std::vector<float> &inst_bounds, ShadowBvh &out,
-                      std::string &err) {
+void shadow_ranks(const std::vector<int> &tlas_inst, int num_instances, std::vector<int> &rank) {
+    rank.assign((size_t)std::max(0, num_instances), 0x7fffffff);
+    for (size_t k = 0; k < tlas_inst.size(); ++k) {
+        const int i = tlas_inst[k];
+        if (i >= 0 && i < num_instances && rank[(size_t)i] == 0x7fffffff) rank[(size_t)i] = (int)k;
+    }
+}
+
+bool build_shadow_bvh(const hdr_scene_desc &desc, const FlatScene &flat, ShadowBvh &out, std::string &err) {
     out = ShadowBvh{};
     const int n_inst = desc.num_instances;
     out.tlas_capacity = std::max(1, n_inst);
     out.nodes.assign((size_t)out.tlas_capacity * kSh4NodeFloats, 0.0f);
     std::vector<int> mesh_root((size_t)std::max(0, desc.num_meshes), -1);
+    const bool host_geo = !flat.tri_geo.empty() || flat.num_triangles == 0;
     for (int mi = 0; mi < desc.num_meshes; ++mi) {
-        const hdr_mesh_desc &m = desc.meshes[mi];
-        std::vector<PrimBox> prims;
+        // the mesh's triangle records in the reference's BLAS order
         std::vector<float> geo;
-        prims.reserve((size_t)std::max(0, m.num_triangles));
-        geo.reserve((size_t)std::max(0, m.num_triangles) * kTriGeoFloats);
-        for (int i = 0; i < m.num_triangles; ++i) {
-            BlasTriangle t;
-            if (!make_triangle(m, i, t)) continue;
-            float g[kTriGeoFloats], a[kTriAttrFloats];
-            pack_triangle(t, g, a);
-            geo.insert(geo.end(), g, g + kTriGeoFloats);
-            PrimBox p;
-            const V3 vs[3] = {t.v0, t.v1, t.v2};
-            for (int k = 0; k < 3; ++k) p.lo[k] = FLT_MAX, p.hi[k] = -FLT_MAX;
-            for (const V3 &v : vs) {
-                const float xyz[3] = {v.x, v.y, v.z};
-                grow(p.lo, p.hi, xyz, xyz);
-            }
-            for (int k = 0; k < 3; ++k) p.c[k] = 0.5f * (p.lo[k] + p.hi[k]);
-            prims.push_back(p);
+        if (host_geo) {
+            const size_t b = (size_t)flat.mesh_tri_base[(size_t)mi], n = (size_t)flat.mesh_tri_count[(size_t)mi];
+            geo.assign(flat.tri_geo.begin() + (long)(b * kTriGeoFloats),
+                       flat.tri_geo.begin() + (long)((b + n) * kTriGeoFloats));
+        } else {  // the BLAS was built on the device: the host build gives the same order
+            const Blas blas = build_blas(desc.meshes[mi]);
+            geo.resize(blas.tris.size() * kTriGeoFloats);
+            float a[kTriAttrFloats];
+            for (size_t t = 0; t < blas.tris.size(); ++t) pack_triangle(blas.tris[t], &geo[t * kTriGeoFloats], a);
         }
-        if (prims.empty()) continue;
+        const size_t nt = geo.size() / kTriGeoFloats;
+        if (nt == 0) continue;
+        std::vector<PrimBox> prims(nt);
+        for (size_t t = 0; t < nt; ++t) {
+            const float *g = &geo[t * kTriGeoFloats];
+            const float v[3][3] = {{g[0], g[1], g[2]},
+                                   {g[0] + g[3], g[1] + g[4], g[2] + g[5]},
+                                   {g[0] + g[6], g[1] + g[7], g[2] + g[8]}};
+            PrimBox &p = prims[t];
+            for (int k = 0; k < 3; ++k) p.lo[k] = FLT_MAX, p.hi[k] = -FLT_MAX;
+            // vertices v0 + e1 / v0 + e2 may round: widen the box by a relative ulp margin
+            for (const auto &x : v) grow(p.lo, p.hi, x, x);
+            for (int k = 0; k < 3; ++k) {
+                const float m = (std::fabs(p.lo[k]) + std::fabs(p.hi[k])) * 2.4e-7f + 1e-30f;
+                p.lo[k] -= m;
+                p.hi[k] += m;
+                p.c[k] = 0.5f * (p.lo[k] + p.hi[k]);
+            }
+        }
         std::vector<BNode> bn;
         std::vector<int> order;
         build_binary(prims, 4, bn, order);
         Collapser col{bn, out.nodes, 0};
         int root = 0;
         const size_t tri_base = out.tris.size() / kTriGeoFloats;
-        if (tri_base + prims.size() >= ((size_t)1 << 27)) {  // leaf entries: (first << 4) | ... fits 31 bits
+        if (tri_base + nt >= ((size_t)1 << 27)) {  // leaf entries: (first << 4) | ... fits 31 bits
             err = "too many triangles for the shadow BVH encoding";
             return false;
         }
-        // leaf triangles go to `tris` in leaf order as the collapse meets them
+        // leaf triangles go to `tris` in leaf order as the collapse meets them, each
+        // with its reference-order index in float 9
         const int depth = col.emit(
             0,
             [&](int b) {
                 const BNode &lf = bn[(size_t)b];
                 const int first = (int)(out.tris.size() / kTriGeoFloats);
                 for (int q = 0; q < lf.count; ++q) {
-                    const float *g = &geo[(size_t)order[(size_t)(lf.first + q)] * kTriGeoFloats];
-                    out.tris.insert(out.tris.end(), g, g + kTriGeoFloats);
+                    const int t = order[(size_t)(lf.first + q)];
+                    const float *g = &geo[(size_t)t * kTriGeoFloats];
+                    float rec[kTriGeoFloats];
+                    std::memcpy(rec, g, sizeof(rec));
+                    rec[9] = bits_float(t);
+                    rec[10] = rec[11] = 0.0f;
+                    out.tris.insert(out.tris.end(), rec, rec + kTriGeoFloats);
                 }
                 return ~((first << 2) | (lf.count - 1));
             },
@@ -298,10 +324,11 @@ bool build_shadow_bvh(const hdr_scene_desc &desc, const std::vector<float> &inst
         const int mesh = desc.instances[i].mesh;
         if (mesh >= 0 && mesh < desc.num_meshes) out.inst_root[(size_t)i] = mesh_root[(size_t)mesh];
     }
+    shadow_ranks(flat.tlas_inst, n_inst, out.inst_rank);
     std::vector<float> tlas;
-    const bool fits = rebuild_shadow_tlas(inst_bounds, out.inst_root, out.blas_depth, tlas, out.tlas_capacity,
+    const bool fits = rebuild_shadow_tlas(flat.inst_bounds, out.inst_root, out.blas_depth, tlas, out.tlas_capacity,
                                           out.tlas_depth);
-    if (!fits) return true;  // not an error: the reference trees serve shadow rays too
+    if (!fits) return true;  // not an error: the reference trees serve these queries too
     std::memcpy(out.nodes.data(), tlas.data(), tlas.size() * sizeof(float));
     out.ok = true;
     return true;

@@ -13,6 +13,13 @@
 // descending), triangles in leaf order. Closest hits keep walking the
 // reference-order trees, whose tie-breaks they need.
 //
+// The same trees answer closest-hit queries with the reference's result: every
+// triangle record carries its index in the reference's BLAS triangle order, and
+// every instance its position in the reference TLAS's leaf order; among hits at
+// equal distance the walk keeps the smallest (instance position, triangle
+// index), which is the one the reference's left-first walks find first
+// (bvh.cpp:262-304, scene.cpp:414-510, strict `<` on t).
+//
 // Node record: 28 floats = 7 float4
 //   [0] min.x of children 0..3   [1] max.x   [2] min.y   [3] max.y
 //   [4] min.z                    [5] max.z   [6] child codes (int bits)
@@ -21,7 +28,9 @@
 // An empty slot has min = +FLT_MAX, max = -FLT_MAX (no ray hits it).
 // Nodes: the TLAS region first (its root is node 0; room for a rebuild over the
 // same instances), then every mesh's BLAS. Triangles: 12 floats each, the
-// tri_geo record (v0, e1 = v1 - v0, e2 = v2 - v0) the closest-hit walk tests.
+// tri_geo record (v0, e1 = v1 - v0, e2 = v2 - v0) the reference-order walk
+// tests, with float 9 holding (as int bits) the triangle's index in its mesh's
+// reference BLAS order.
 #pragma once
 
 #include <string>
@@ -32,21 +41,28 @@
 
 namespace hdr {
 
+struct FlatScene;
+
 struct ShadowBvh {
     std::vector<float> nodes;
     std::vector<float> tris;
     std::vector<int> inst_root;  // per instance: its mesh's BLAS root node, or -1 (no triangles)
+    std::vector<int> inst_rank;  // per instance: its position in the reference TLAS's leaf order
     int tlas_capacity = 0;       // nodes reserved for the TLAS at the front of `nodes`
     int tlas_depth = 0, blas_depth = 0;
     bool ok = false;             // false: not built (the scene is walked with the reference trees)
 };
 
-// Builds the BLAS of every mesh and the TLAS over the instances' world boxes
-// (6 floats per instance: min.xyz, max.xyz; instances whose mesh has no
-// triangles are left out). Returns false (and leaves out.ok false) when the
-// trees would need more than kSh4Stack stack entries.
-bool build_shadow_bvh(const hdr_scene_desc &desc, const std::vector<float> &inst_bounds, ShadowBvh &out,
-                      std::string &err);
+// Builds the BLAS of every mesh over its triangles in the reference's BLAS order
+// (the flat scene's tri_geo records when the host built them, else a host
+// build of the reference's tree for the order) and the TLAS over the instances'
+// world boxes (instances whose mesh has no triangles are left out). Returns
+// false only on error; out.ok stays false when the trees would need more than
+// kSh4Stack stack entries.
+bool build_shadow_bvh(const hdr_scene_desc &desc, const FlatScene &flat, ShadowBvh &out, std::string &err);
+
+// inst_rank from the reference TLAS's instance order (tlas_inst: instance per leaf slot).
+void shadow_ranks(const std::vector<int> &tlas_inst, int num_instances, std::vector<int> &rank);
 
 // Rebuilds the TLAS part of `nodes` (into the first tlas_capacity nodes) over new
 // instance boxes; returns false when it does not fit the reserved room or the

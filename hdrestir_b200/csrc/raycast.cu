@@ -124,7 +124,8 @@ __global__ void trace_stats_kernel(DeviceScene s, const float *rays, const float
         case 1: r = trace_ray_wide<false>(s, o, d, 0.0f, h, e, st); break;
         case 2: r = trace_ray_binary<true>(s, o, d, lim, h, e, st) && h.t < lim; break;
         case 3: r = trace_ray_wide<true>(s, o, d, lim, h, e, st) && h.t < lim; break;
-        default: r = shadow4_ray(s, o, d, lim, e, st); break;
+        case 4: r = shadow4_ray(s, o, d, lim, e, st); break;
+        default: r = closest4_ray(s, o, d, h, e, st); break;
     }
     out[k] = make_int4(st.pops, st.leaves, st.tris, r ? 1 : 0);
     if (e) atomicOr(err, e);

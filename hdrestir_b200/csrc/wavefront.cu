@@ -321,6 +321,52 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) trace_shadow4_kerne
     if (e) atomicOr(err, e);
 }
 
+// Closest-hit queue over the 4-wide SAH trees (DeviceScene::sh4_closest, opt-in),
+// scheduled like trace_shadow4_kernel (Closest4Walk).
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) trace_closest4_kernel(DeviceScene s, const float4 *__restrict__ q,
+                                                                                 int *counts, float4 *hits,
+                                                                                 float *hit_v, int quorum,
+                                                                                 unsigned *err) {
+    __shared__ int col[kSh4Shared * kTraceThreads];
+    int deep[kSh4Stack - kSh4Shared];
+    Closest4Walk<Sh4SplitStack<kSh4Shared, kTraceThreads>> w;
+    w.stack.col = col + threadIdx.x;
+    w.stack.deep = deep;
+    w.mode = kSh4ModeDone;
+    w.best_inst = -1;
+    const int n = counts[0];
+    unsigned e = 0;
+    NoStats ns;
+    int slot = -1;
+    bool drained = false;
+    for (;;) {
+        const bool done = w.mode == kSh4ModeDone;
+        if (done && slot >= 0) {
+            hits[slot] = make_float4(w.best_t, __int_as_float(w.best_inst), __int_as_float(w.best_tri), w.best_u);
+            hit_v[slot] = w.best_v;
+            slot = -1;
+        }
+        const int k = fetch_ray(&counts[3], n, done, drained);
+        if (done) {
+            if (k >= 0) {
+                const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
+                w.start(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z});
+                slot = __float_as_int(a.w);
+            } else {
+                w.mode = kSh4ModeIdle;
+            }
+        }
+        if (!__any_sync(kFullMask, w.mode != kSh4ModeIdle)) break;
+        do {
+            if (w.mode == kSh4ModeNode) w.node_step(s, e, ns);
+        } while (__popc(__ballot_sync(kFullMask, w.mode == kSh4ModeNode)) >= quorum);
+        if (w.mode == kSh4ModeLeaf) w.leaf(s, ns);
+        if (w.mode == kSh4ModeInst) w.inst(s, ns);
+    }
+    if (e) atomicOr(err, e);
+}
+
 // The shadow-ray queue q (count / fetch counters on the device, answers into occ).
 int launch_shadow_queue(const DeviceScene &s, const float4 *q, const int *count, int *fetch, unsigned char *occ,
                         const TraceTuning &tune, unsigned *err, cudaStream_t st) {
@@ -458,7 +504,12 @@ int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &t
     const bool phased = refill && (tune.mode & kTraceUnphased) == 0;
     const bool shallow = s.shallow && (tune.mode & kTraceSplitStack) == 0;
     if (!mark(ev_begin, 0)) return -1;
-    if (phased) {
+    if (s.sh4_closest) {
+        auto closest = tune.shadow_shape == 0 ? trace_closest4_kernel<8>
+                                              : (tune.shadow_shape == 1 ? trace_closest4_kernel<6>
+                                                                        : trace_closest4_kernel<5>);
+        closest<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, tune.node_quorum, err);
+    } else if (phased) {
         auto closest = s.wide      ? trace_closest_phased_kernel<true, false>
                        : shallow   ? trace_closest_phased_kernel<false, true>
                                    : trace_closest_phased_kernel<false, false>;

@@ -297,10 +297,18 @@ typedef struct hdr_gbuffer_texel {
                                      HDR_CTX_WIDE_BVH, and the scene cannot be shared into a
                                      wide-walk ctx. Its scratch (about 0.5 KB per triangle while
                                      building) is outside the ctx's HBM budget. */
-#define HDR_CTX_REFERENCE_SHADOWS 512u /* shadow rays walk the reference's trees (closest-hit walk
-                                     stopped below the light distance) instead of the shadow BVH,
-                                     a 4-wide SAH tree over the same triangles built at upload;
-                                     the answers agree (same triangle test, conservative boxes) */
+#define HDR_CTX_REFERENCE_SHADOWS 512u /* every ray walks the reference's own trees instead of the
+                                     4-wide SAH trees built at upload over the same triangles
+                                     (shadow queries: the closest-hit walk stopped below the light
+                                     distance). The answers agree: the same triangle test in the
+                                     same instance space, conservative boxes, and closest-hit ties
+                                     broken in the reference's walk order. */
+#define HDR_CTX_SAH_CLOSEST 1024u /* closest hits too walk the 4-wide SAH trees (ties broken in
+                                     the reference's walk order). Faster, and the reference's
+                                     answer except where the reference's own rounded box tests cull
+                                     the nearest hit (coplanar surfaces): about 1e-3 of random rays
+                                     in config 1's scene, 5e-6 in config 2's. Off by default:
+                                     closest hits are held to the reference bit for bit. */
 #define HDR_CTX_RECORD_LIGHTS 256u /* diagnostic, no reference counterpart: the wavefront
                                      hdr_ris_path_trace records the light index each NEE candidate
                                      selected (UniformLightSampler::ProposeCandidate,
@@ -573,9 +581,10 @@ hdr_status hdr_autotune_trace(hdr_ctx *ctx, hdr_trace_tuning *best);
 /* Diagnostic, no reference counterpart: the work one traversal form does per
  * ray. walk: 0 closest hit on the binary trees, 1 closest hit on their 4-wide
  * collapse, 2 shadow query on the binary trees, 3 shadow query on the 4-wide
- * collapse, 4 shadow query on the shadow BVH (stack entries popped, leaves and
- * instances entered, triangles tested). out = n x int32[4]: nodes popped,
- * leaves entered, triangles tested, answer (hit / occluded). */
+ * collapse, 4 shadow query on the 4-wide SAH trees, 5 closest hit on them
+ * (for 4 and 5: stack entries popped, leaves and instances entered, triangles
+ * tested). out = n x int32[4]: nodes popped, leaves entered, triangles tested,
+ * answer (hit / occluded). */
 hdr_status hdr_trace_stats(hdr_ctx *ctx, const float *rays, const float *tmax, int32_t n, int32_t walk,
                            int32_t *out);
 
