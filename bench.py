@@ -47,7 +47,7 @@ INTEGRATE_BYTES_PER_PX = 80 + 80 + 64 + 16
 # accumulation: colour in 16 + accum in 16 + accum out 16 + colour out 16, plus the firefly
 # clamp and its check (colour in 16 + clamped out 16; clamped in 16 + colour in 16)
 ACCUM_BYTES_PER_PX = 64 + 32 + 32
-# trace_shadow_kernel, the dominant kernel: per shadow ray it must read its queue record
+# trace_shadow4_kernel, the dominant kernel: per shadow ray it must read its queue record
 # (origin, slot, direction, limit: 32 B) and write one occlusion byte; the BVH and the
 # triangles it reads are the scene's, shared by all rays of the launch
 SHADOW_BYTES_PER_RAY = 32 + 1
@@ -458,6 +458,71 @@ def serving_leg(n_jobs: int, rate: float = 200.0):
     return out
 
 
+def graph_leg(ctx, cam, ris, world, n_frames=10):
+    """Each frame's pass chain submitted eagerly (one call per pass) and as one CUDA
+    graph (hdr_graph_*: one frame recorded, then replayed per frame with its frame
+    index: a frame-slot store and one graph launch). Device time of n_frames
+    consecutive frames (CUDA events around the loop: the stream idles where the host
+    submits slower than the device runs) and the host's median submit time per frame,
+    for the headline frame and for config 0's 256x256 PathTracer frame (maxDepth 4:
+    4 rounds of small wavefront kernels)."""
+    from hdrestir_b200 import configs
+    from hdrestir_b200.context import Context
+    out = {}
+    sc0, cam0 = configs.config0()
+
+    def restir(c, k, cam=cam):
+        c.raycast(cam, k)
+        c.ris_path_trace(cam, k, **ris)
+        c.accumulate(k, firefly=True, mode="parity")
+
+    def pt(c, k, cam=cam0):
+        c.raycast(cam, k)
+        c.path_trace(cam, k, max_depth=4)
+        c.accumulate(k, firefly=True, mode="parity")
+
+    for name, passes, scene in (("config2_restir_1080p", restir, None), ("config0_pt_256", pt, sc0)):
+        g = Context(device=ctx.device, timings=False)
+        try:
+            if scene is None:
+                g.share_scene(ctx)
+            else:
+                g.upload_scene(scene)
+            res = {}
+            k = 0
+            for mode in ("eager", "graph"):
+                # warm-up: the first frame sizes the buffers; in graph mode the second is recorded
+                passes(g, k)
+                k += 1
+                if mode == "graph":
+                    g.record_frame(lambda: passes(g, k))
+                else:
+                    passes(g, k)
+                k += 1
+                g.synchronize()
+                host = []
+                g.region_begin(0)
+                for _ in range(n_frames):
+                    t0 = time.perf_counter()
+                    if mode == "graph":
+                        g.graph_launch(k)  # the recorded frame replayed with this frame index
+                    else:
+                        passes(g, k)
+                    host.append(time.perf_counter() - t0)
+                    k += 1
+                g.region_end(0)
+                ms = max_over_ranks(g.region_elapsed(0), world) / n_frames
+                res[mode] = {"frames_per_s": world * 1000.0 / ms, "ms_per_frame": ms,
+                             "host_submit_us_per_frame": 1e6 * statistics.median(host)}
+            res["graph_info"] = g.graph_info()
+            out[name] = res
+        finally:
+            g.close()
+    out["note"] = ("graph = the frame's passes recorded with hdr_graph_begin/_end and run with one "
+                   "hdr_graph_launch; images identical to eager (tests/test_gpu_graph.py)")
+    return out
+
+
 def run_ours(args, rank, local_rank, world):
     import numpy as np
     import torch
@@ -532,6 +597,7 @@ def run_ours(args, rank, local_rank, world):
         ctx.region_end(3)
         ms = max_over_ranks(ctx.region_elapsed(3), world) / n_var
         variants[name] = {"frames_per_s": world * 1000.0 / ms, "ms_per_frame": ms, "frames": n_var}
+    graph = graph_leg(ctx, cam, ris, world, n_frames=max(2, min(args.steps, 10)))
     ctx.pass_times(reset=True)
     ctx.clear_persistent()
     for k in range(args.warmup):
@@ -584,7 +650,8 @@ def run_ours(args, rank, local_rank, world):
         "rays_per_frame": {"primary": px, "closest": n_closest, "shadow": n_shadow},
         "rays_per_s": rays / (total_ms / args.steps / 1000.0),
         "rays_per_s_note": "rays traced: primary + closest-hit queue + shadow queue of a frame",
-        "roofline": {"kernel": "trace_shadow_kernel (NEE shadow rays, any-hit)", "bound": "hbm",
+        "roofline": {"kernel": "trace_shadow4_kernel (NEE shadow rays, any-hit, 4-wide SAH shadow BVH)",
+                     "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": traffic, "traffic_source": traffic_src,
                      "algorithmic_bytes": SHADOW_BYTES_PER_RAY * n_shadow, "launch_ms": t_shadow,
@@ -599,6 +666,7 @@ def run_ours(args, rank, local_rank, world):
         "gpu_launches": gpu_launches,
         "clocks": clk,
         "variants": variants,
+        "cuda_graph": graph,
         "note": "default = wavefront (generate/trace/shade); BSDF-candidate rays are not cast in scenes with no "
                 "light geometry and no environment, where their result cannot change the image (bit-identical, "
                 "tested); 'trace_all_rays' casts them as the reference does",

@@ -93,7 +93,7 @@ RIS_TRACE_ALL_RAYS, RIS_ONE_KERNEL = 1, 2
 
 class TraceTuning(C.Structure):
     _fields_ = [("node_quorum", _i), ("blocks_per_sm", _i), ("trace_ms", _f), ("shade_shape", _i),
-                ("shadow_shape", _i)]
+                ("shadow_shape", _i), ("shade_ms", _f)]
 
 
 class ServerDesc(C.Structure):
@@ -206,12 +206,18 @@ def lib() -> C.CDLL:
             "hdr_get_trace_tuning": (C.c_int, [vp, C.POINTER(TraceTuning)]),
             "hdr_set_trace_tuning": (C.c_int, [vp, C.POINTER(TraceTuning)]),
             "hdr_autotune_trace": (C.c_int, [vp, C.POINTER(TraceTuning)]),
+            "hdr_autotune_frame": (C.c_int, [vp, C.POINTER(CameraDesc), i32, C.POINTER(RisParams),
+                                             C.POINTER(TraceTuning)]),
             "hdr_rng_floats": (C.c_int, [vp, vp, i32, i32, vp]),
             "hdr_pass_times": (C.c_int, [vp, C.POINTER(C.c_float), C.POINTER(C.c_int32), i32, i32]),
             "hdr_launch_count": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
             "hdr_region_begin": (C.c_int, [vp, i32]),
             "hdr_region_end": (C.c_int, [vp, i32]),
             "hdr_region_elapsed": (C.c_int, [vp, i32, C.POINTER(C.c_float)]),
+            "hdr_graph_begin": (C.c_int, [vp]),
+            "hdr_graph_end": (C.c_int, [vp]),
+            "hdr_graph_launch": (C.c_int, [vp, i32]),
+            "hdr_graph_info": (C.c_int, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]),
             "hdr_server_create": (C.c_int, [C.POINTER(vp), C.POINTER(ServerDesc)]),
             "hdr_server_destroy": (None, [vp]),
             "hdr_server_add_scene": (C.c_int, [vp, C.POINTER(SceneDesc), C.POINTER(i32)]),

@@ -239,7 +239,7 @@ class Context:
                          shadow_shape: int | None = None) -> None:
         if shadow_shape is None:
             shadow_shape = self.trace_tuning()["shadow_shape"]
-        t = abi.TraceTuning(int(node_quorum), int(blocks_per_sm), 0.0, int(shade_shape), int(shadow_shape))
+        t = abi.TraceTuning(int(node_quorum), int(blocks_per_sm), 0.0, int(shade_shape), int(shadow_shape), 0.0)
         abi.check(self._lib.hdr_set_trace_tuning(self._h, C.byref(t)))
 
     def autotune_trace(self) -> dict:
@@ -248,6 +248,15 @@ class Context:
         abi.check(self._lib.hdr_autotune_trace(self._h, C.byref(t)))
         return {"node_quorum": t.node_quorum, "blocks_per_sm": t.blocks_per_sm, "trace_ms": t.trace_ms,
                 "shadow_shape": t.shadow_shape}
+
+    def autotune_frame(self, cam: Camera, frame_index: int, **ris) -> dict:
+        """One wavefront RIS frame (the buffers of ris_path_trace) that tunes the trace
+        schedule and the resampling kernel's launch shape while it renders."""
+        t = abi.TraceTuning()
+        abi.check(self._lib.hdr_autotune_frame(self._h, C.byref(cam.c_desc()), int(frame_index),
+                                               C.byref(ris_params(**ris)), C.byref(t)))
+        return {"node_quorum": t.node_quorum, "blocks_per_sm": t.blocks_per_sm, "trace_ms": t.trace_ms,
+                "shadow_shape": t.shadow_shape, "shade_shape": t.shade_shape, "shade_ms": t.shade_ms}
 
     def trace_stats(self, rays: np.ndarray, walk: int, tmax: np.ndarray | None = None) -> np.ndarray:
         """Per-ray (nodes popped, leaves, triangles tested, answer) of one traversal form
@@ -304,3 +313,37 @@ class Context:
         n = C.c_uint64()
         abi.check(self._lib.hdr_launch_count(self._h, C.byref(n)))
         return int(n.value)
+
+    # ---- a frame's pass chain as one CUDA graph (hdr_graph_*)
+    def graph_begin(self) -> None:
+        """Pass calls until graph_end are recorded, not run."""
+        abi.check(self._lib.hdr_graph_begin(self._h))
+
+    def graph_end(self) -> None:
+        """The record becomes the ctx's executable graph (updated in place when
+        it has the launches of the previous one)."""
+        abi.check(self._lib.hdr_graph_end(self._h))
+
+    def graph_launch(self, frame_index: int = -1) -> None:
+        """Runs the recorded graph for `frame_index` (-1: the recorded frame index)."""
+        abi.check(self._lib.hdr_graph_launch(self._h, int(frame_index)))
+
+    def graph_info(self) -> dict:
+        k, i, u = C.c_int32(), C.c_int32(), C.c_int32()
+        abi.check(self._lib.hdr_graph_info(self._h, C.byref(k), C.byref(i), C.byref(u)))
+        return {"kernels": k.value, "instantiations": i.value, "updates": u.value}
+
+    def record_frame(self, passes) -> None:
+        """Records the pass calls `passes()` makes on this ctx as its graph and
+        runs it: the same work as calling them, submitted as one launch."""
+        self.graph_begin()
+        try:
+            passes()
+        except BaseException:
+            try:
+                self.graph_end()
+            except abi.HdrError:
+                pass
+            raise
+        self.graph_end()
+        self.graph_launch()

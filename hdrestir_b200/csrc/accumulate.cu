@@ -105,7 +105,10 @@ __global__ void __launch_bounds__(1024) firefly_sequential_kernel(const float4 *
 }
 
 __global__ void __launch_bounds__(256) accumulate_kernel(const float4 *__restrict__ in, float4 *__restrict__ accum,
-                                                         float4 *__restrict__ out, size_t count, float inv_n) {
+                                                         float4 *__restrict__ out, size_t count, float inv_n,
+                                                         const int *frame_slot) {
+    // a recorded pass reads its frame index from the slot (the same float division the host does)
+    if (frame_slot) inv_n = 1.0f / (float)(*frame_slot + 1);
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
         const float4 c = in[i];
         float4 a = accum[i];
@@ -123,7 +126,8 @@ __global__ void __launch_bounds__(256) accumulate_kernel(const float4 *__restric
 // scratch holds one float4 plane of width*height (only used with firefly);
 // flag_dev one int, zeroed on the stream before each parity-mode check.
 int launch_accumulate(float4 *color, float4 *accum, float4 *scratch, int *flag_dev, int width, int height,
-                      int frame_index, int firefly, int mode, cudaStream_t st, cudaError_t *err) {
+                      int frame_index, int firefly, int mode, cudaStream_t st, cudaError_t *err,
+                      const int *frame_slot) {
     const size_t count = (size_t)width * height;
     const float inv_n = 1.0f / (float)(frame_index + 1);
     int launches = 0;
@@ -146,7 +150,7 @@ int launch_accumulate(float4 *color, float4 *accum, float4 *scratch, int *flag_d
         }
     }
     const int blocks = (int)std::min<size_t>((count + 255) / 256, (size_t)148 * 8);
-    accumulate_kernel<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(src, accum, color, count, inv_n);
+    accumulate_kernel<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(src, accum, color, count, inv_n, frame_slot);
     ++launches;
     if ((e = cudaGetLastError()) != cudaSuccess) {
         if (err) *err = e;

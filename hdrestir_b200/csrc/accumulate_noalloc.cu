@@ -47,7 +47,8 @@
 
 namespace hdr {
 int launch_accumulate(float4 *color, float4 *accum, float4 *scratch, int *flag_dev, int width, int height,
-                      int frame_index, int firefly, int mode, cudaStream_t st, cudaError_t *err);
+                      int frame_index, int firefly, int mode, cudaStream_t st, cudaError_t *err,
+                      const int *frame_slot);
 hdr_status set_last_error(hdr_status st, const char *fmt, ...);
 }  // namespace hdr
 
@@ -134,7 +135,7 @@ extern "C" hdr_status hdr_accumulate_noalloc(float *color, float *accum, int32_t
     if (st != HDR_OK) return st;
     const int n = hdr::launch_accumulate(reinterpret_cast<float4 *>(color), reinterpret_cast<float4 *>(accum),
                                          s.planes, s.flag, width, height, frame_index, firefly, mode,
-                                         static_cast<cudaStream_t>(stream), &e);
+                                         static_cast<cudaStream_t>(stream), &e, nullptr);
     if (n < 0) return hdr::set_last_error(HDR_ECUDA, "accumulation launch failed: %s", cudaGetErrorString(e));
     return HDR_OK;
 }

@@ -24,7 +24,16 @@ struct CameraD {
     double inv_proj[16];
     int width, height;
     CameraParamsD p;
+    // non-null in a pass recorded into a CUDA graph: the frame index lives in device
+    // memory there, so one recorded frame replays for any frame index
+    const int *frame_slot;
 };
+
+// The frame index a kernel renders: its argument, or the value stored in the
+// frame slot when the launch belongs to a recorded graph.
+__device__ __forceinline__ int live_frame(const CameraD &c, int frame_arg) {
+    return c.frame_slot ? *c.frame_slot : frame_arg;
+}
 
 struct RayF {
     V3 o, d;

@@ -268,8 +268,10 @@ void launch_path_trace_batch(const DeviceScene &s, const PtJobD *jobs, int n_job
 void launch_path_trace(const DeviceScene &s, const CameraD &cam, int frame_index, const PathParamsD &p,
                        GBufferView gb, float4 *color, unsigned *err, cudaStream_t st);
 // Returns the number of kernels launched, or -1 with the CUDA error in *err.
+// frame_slot (non-null in a pass recorded into a graph) holds the frame index.
 int launch_accumulate(float4 *color, float4 *accum, float4 *scratch, int *flag_dev, int width, int height,
-                      int frame_index, int firefly, int mode, cudaStream_t st, cudaError_t *err);
+                      int frame_index, int firefly, int mode, cudaStream_t st, cudaError_t *err,
+                      const int *frame_slot = nullptr);
 
 // Pixel of thread t in a 16x16 tile: each warp covers an 8x4 sub-tile so the
 // rays it traces start close together.

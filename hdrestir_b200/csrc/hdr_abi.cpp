@@ -49,6 +49,10 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// Stores the frame index a recorded graph renders (hdr_graph_launch); the
+// recorded kernels read it from the slot.
+__global__ void set_frame_slot_kernel(int *slot, int value) { *slot = value; }
+
 }  // namespace
 
 namespace hdr {
@@ -166,6 +170,23 @@ struct hdr_ctx {
     // copy stream while the ctx stream goes on (created at the first call)
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_ready = nullptr, copy_done = nullptr;
+    // hdr_graph_begin / hdr_graph_end / hdr_graph_launch: while `recording`, the pass calls
+    // are captured from the ctx stream instead of run; graph_exec is the executable chain
+    bool recording = false;
+    bool rec_failed = false;      // a pass failed while recording: its work is missing from the record
+    uint64_t rec_launches0 = 0;   // `launches` when the recording began
+    // the recorded passes read their frame index from d_frame_slot (device memory), which
+    // hdr_graph_launch sets; every pass of one recording renders the same frame index
+    int *d_frame_slot = nullptr;
+    bool rec_has_frame = false, graph_has_frame = false;
+    int32_t rec_frame = 0, graph_frame = 0;
+    uint64_t graph_kernels = 0;   // kernel launches one replay of graph_exec makes
+    cudaGraphExec_t graph_exec = nullptr;
+    int32_t graph_instantiations = 0, graph_updates = 0;
+    // hdr_autotune_frame: the wavefront RIS frame in progress searches the trace schedules and
+    // resampling launch shapes, reporting into tune_out
+    bool tune_frame = false;
+    hdr_trace_tuning *tune_out = nullptr;
 };
 
 namespace {
@@ -199,6 +220,9 @@ hdr_status ensure_buffer(hdr_ctx *c, const char *name, size_t bytes, void **out)
         *out = it->second.ptr;
         return HDR_OK;
     }
+    if (c->recording)
+        return fail(HDR_EINVAL, "buffer '%s' does not exist at %zu bytes: a recorded pass cannot allocate (run the "
+                    "same passes once outside hdr_graph_begin / hdr_graph_end first)", name, bytes);
     DevBuf nb;
     hdr_status st = dev_alloc(c, nb, bytes);
     if (st != HDR_OK) return st;
@@ -224,6 +248,9 @@ hdr_status ensure_scratch(hdr_ctx *c, const char *name, size_t bytes, void **out
         *out = it->second.ptr;
         return HDR_OK;
     }
+    if (c->recording)
+        return fail(HDR_EINVAL, "scratch '%s' is smaller than %zu bytes: a recorded pass cannot allocate (run the "
+                    "same passes once outside hdr_graph_begin / hdr_graph_end first)", name, bytes);
     if (it != c->buffers.end()) {
         HDR_CUDA(cudaStreamSynchronize(c->stream));
         dev_free(c, it->second);
@@ -271,6 +298,34 @@ void *find_buffer(hdr_ctx *c, const char *name, size_t *bytes) {
 
 hdr_status check_cancel(hdr_ctx *c) {
     if (c->cancel && *c->cancel) return fail(HDR_ECANCELLED, "render job cancelled");
+    return HDR_OK;
+}
+
+// Calls that wait for the device, read back to the host, allocate or free, or
+// order other streams cannot be recorded into a graph: they fail while the ctx
+// records (checked before they touch the stream, so the recording stays valid).
+hdr_status check_not_recording(const hdr_ctx *c, const char *what) {
+    if (c->recording)
+        return fail(HDR_EINVAL, "%s cannot run while the ctx records a graph (between hdr_graph_begin and "
+                    "hdr_graph_end)", what);
+    return HDR_OK;
+}
+#define HDR_NOT_RECORDING(c, what)                                   \
+    do {                                                             \
+        hdr_status s_ = check_not_recording((c), (what));            \
+        if (s_ != HDR_OK) return s_;                                 \
+    } while (0)
+
+// A pass recorded into a graph renders the recording's frame index, read from the
+// ctx's frame slot at run time (so hdr_graph_launch can replay it for any frame):
+// the first recorded pass fixes that index, the others must give the same one.
+hdr_status record_frame_index(hdr_ctx *c, int32_t frame_index, hdr::CameraD *cam) {
+    if (!c->recording) return HDR_OK;
+    if (c->rec_has_frame && c->rec_frame != frame_index)
+        return fail(HDR_EINVAL, "recorded passes render one frame index (%d), not %d", c->rec_frame, frame_index);
+    c->rec_has_frame = true;
+    c->rec_frame = frame_index;
+    if (cam) cam->frame_slot = c->d_frame_slot;
     return HDR_OK;
 }
 
@@ -338,8 +393,11 @@ hdr_status fold_pass_time(hdr_ctx *c, int slot) {
     c->ev_pending[slot] = false;
     return HDR_OK;
 }
+// Pass timing (HDR_CTX_TIMINGS) waits for the slot's previous events, so it is
+// not taken while passes are being recorded into a graph.
+bool timing_on(const hdr_ctx *c) { return (c->flags & 1u) && !c->recording && !c->tune_frame; }
 hdr_status begin_pass(hdr_ctx *c, int slot) {
-    if (c->flags & 1u) {
+    if (timing_on(c)) {
         hdr_status st = fold_pass_time(c, slot);
         if (st != HDR_OK) return st;
         HDR_CUDA(cudaEventRecord(c->ev_start[slot], c->stream));
@@ -348,7 +406,7 @@ hdr_status begin_pass(hdr_ctx *c, int slot) {
 }
 hdr_status end_pass(hdr_ctx *c, int slot) {
     HDR_CUDA(cudaGetLastError());
-    if (c->flags & 1u) {
+    if (timing_on(c)) {
         HDR_CUDA(cudaEventRecord(c->ev_stop[slot], c->stream));
         c->ev_pending[slot] = true;
     }
@@ -405,6 +463,7 @@ hdr_status hdr_ctx_create(hdr_ctx **out, const hdr_ctx_desc *desc) {
         return fail(HDR_ECUDA, "context setup: %s", cudaGetErrorString(e));
     }
     c->d_flag = (int *)((char *)c->d_err + 32);
+    c->d_frame_slot = (int *)((char *)c->d_err + 48);
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
         c->tune.sm_count = sms;
@@ -418,8 +477,15 @@ hdr_status hdr_ctx_create(hdr_ctx **out, const hdr_ctx_desc *desc) {
 void hdr_ctx_destroy(hdr_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
+    if (c->recording) {  // an unfinished recording is dropped
+        cudaGraph_t g = nullptr;
+        if (cudaStreamEndCapture(c->stream, &g) == cudaSuccess && g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        c->recording = false;
+    }
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);  // a read-back may still use a buffer
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     c->scene_store.reset();
     for (auto &kv : c->buffers) dev_free(c, kv.second);
     if (c->d_err) cudaFree(c->d_err);
@@ -495,11 +561,19 @@ int ris_trace_level(const hdr_ctx *c, const hdr_ris_params *p) {
         return hdr::kTraceAllBsdfRays;
     return c->scene_emissive ? hdr::kTraceBounceRay : hdr::kTraceNoBsdfRays;
 }
+// Closest-hit slots per pixel of the wavefront RIS queues: only the rays the trace
+// level casts get one (the resampling kernel reads no other slot), so a frame whose
+// BSDF-candidate rays cannot matter holds no closest-hit queue at all (1.8 GB at
+// 1920x1080 with 16 BSDF candidates).
+int closest_slots(int trace_level, int n_bsdf) {
+    return trace_level >= hdr::kTraceAllBsdfRays ? 1 + n_bsdf : (trace_level >= hdr::kTraceBounceRay ? 1 : 0);
+}
 }  // namespace
 
 hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     if (!c || !desc) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_scene_upload");
     HDR_CUDA(cudaSetDevice(c->device));
     const bool device_build = (c->flags & HDR_CTX_DEVICE_BUILD) != 0;
     // HDR_CTX_DEVICE_BUILD: every mesh's BLAS and triangle records built on the device first
@@ -717,7 +791,7 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     return HDR_OK;
 }
 
-hdr_status hdr_raycast(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, uint32_t aov_mask) {
+static hdr_status raycast_pass(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, uint32_t aov_mask) {
     if (!c) return fail(HDR_EINVAL, "ctx is NULL");
     std::lock_guard<std::mutex> lock(c->mu);
     hdr_status st = check_camera(cam);
@@ -742,18 +816,157 @@ hdr_status hdr_raycast(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, u
         if ((st = ensure_buffer(c, "Normal", count * 12, &p)) != HDR_OK) return st;
         aov.normal = (float *)p;
     }
+    hdr::CameraD d = make_camera(cam);
+    if ((st = record_frame_index(c, frame_index, &d)) != HDR_OK) return st;
     c->width = cam->width;
     c->height = cam->height;
-    const hdr::CameraD d = make_camera(cam);
     if ((st = begin_pass(c, 0)) != HDR_OK) return st;
     hdr::launch_raycast(c->scene, d, frame_index, gb, aov, c->d_err, c->stream);
     c->launches += 1;
     return end_pass(c, 0);
 }
 
-hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, const hdr_ris_params *p) {
+}  // extern "C"
+
+namespace {
+
+// Device time of `launch` (ms, best of two runs) on the ctx stream; `prepare`
+// runs before each run, outside the timed part. -1 on a launch failure.
+template <class Prepare, class Launch>
+hdr_status time_best_of_two(hdr_ctx *c, Prepare prepare, Launch launch, float &ms_out) {
+    cudaEvent_t ev[2] = {c->region_ev[3][0], c->region_ev[3][1]};
+    float best = 3.4e38f;
+    for (int rep = 0; rep < 2; ++rep) {
+        hdr_status st = prepare();
+        if (st != HDR_OK) return st;
+        HDR_CUDA(cudaEventRecord(ev[0], c->stream));
+        const int n = launch();
+        if (n < 0) return fail(HDR_ECUDA, "launch failed while tuning: %s", cudaGetErrorString(cudaGetLastError()));
+        c->launches += (uint64_t)n;
+        HDR_CUDA(cudaEventRecord(ev[1], c->stream));
+        HDR_CUDA(cudaEventSynchronize(ev[1]));
+        float ms = 0.0f;
+        HDR_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+        best = std::min(best, ms);
+    }
+    ms_out = best;
+    return HDR_OK;
+}
+
+// The trace-schedule search over queues the generate kernel filled: node quorum x
+// persistent blocks per SM (x the shadow walk's register budget on the 4-wide SAH
+// trees). The trace kernels only read the queues and rewrite the same hit and
+// occlusion slots, so each rerun needs nothing but its fetch counters at zero.
+hdr_status search_trace_schedule(hdr_ctx *c, const hdr::WaveBuffers &wb, hdr::TraceTuning &pick, float &pick_ms) {
+    static const int kQuorum[] = {8, 12, 16, 20, 24, 28};
+    static const int kBlocks[] = {4, 6, 8, 16};
+    hdr::TraceTuning t = c->tune;
+    pick = c->tune;
+    pick_ms = 3.4e38f;
+    const int n_shapes = c->scene.sh4 ? hdr::kShadowShapes : 1;
+    for (int si = 0; si < n_shapes; ++si)
+        for (int quorum : kQuorum)
+            for (int blocks : kBlocks) {
+                t.node_quorum = quorum;
+                t.blocks_per_sm = blocks;
+                if (c->scene.sh4) t.shadow_shape = si;
+                float ms = 0.0f;
+                hdr_status st = time_best_of_two(
+                    c,
+                    [&]() -> hdr_status {
+                        HDR_CUDA(cudaMemsetAsync(wb.counts + 2, 0, 2 * sizeof(int), c->stream));
+                        return HDR_OK;
+                    },
+                    [&]() { return hdr::launch_wave_trace(c->scene, wb, t, c->d_err, c->stream); }, ms);
+                if (st != HDR_OK) return st;
+                if (ms < pick_ms) pick_ms = ms, pick = t;
+            }
+    return HDR_OK;
+}
+
+// hdr_autotune_frame's wavefront frame: generate once, then the trace kernels once per
+// trace schedule and the resampling kernel once per launch shape, each shade run from a
+// copy of the reservoirs it reads (it merges into them in place) and with the winner
+// queue emptied; every run writes the same bytes. The fastest schedule and shape stay in
+// the ctx. Returns the kernel launches of one plain frame in *frame_launches.
+hdr_status tune_wave_frame(hdr_ctx *c, const hdr::CameraD &cd, int frame_index, const hdr::RisParamsD &d,
+                           const hdr::GBufferView &gb, const hdr::ReservoirView &rv, const hdr::WaveBuffers &wb,
+                           float4 *color, int trace_level, hdr_trace_tuning *best, int *frame_launches) {
+    const bool tex = c->scene.has_textures;
+    cudaStream_t s = c->stream;
+    HDR_CUDA(cudaMemsetAsync(wb.counts, 0, (wb.q_winner ? 6 : 4) * sizeof(int), s));
+    if ((tex ? hdr::textured::launch_ris_generate : hdr::launch_ris_generate)(c->scene, cd, frame_index, d, gb, wb,
+                                                                             color, trace_level, c->d_err, s) < 0)
+        return fail(HDR_ECUDA, "generate launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    hdr::TraceTuning pick;
+    float trace_ms = 0.0f;
+    hdr_status st = search_trace_schedule(c, wb, pick, trace_ms);
+    if (st != HDR_OK) return st;
+    c->tune.node_quorum = pick.node_quorum;
+    c->tune.blocks_per_sm = pick.blocks_per_sm;
+    c->tune.shadow_shape = pick.shadow_shape;
+    void *snap = nullptr;
+    const size_t res_bytes = wb.pixels * kResPlanes * sizeof(float4);
+    if (rv.dir_dist) {
+        if ((st = ensure_scratch(c, "__tune_reservoir", res_bytes, &snap)) != HDR_OK) return st;
+        HDR_CUDA(cudaMemcpyAsync(snap, rv.dir_dist, res_bytes, cudaMemcpyDeviceToDevice, s));
+    }
+    hdr::TraceTuning t = c->tune;
+    int shade_pick = t.shade_shape;
+    float shade_ms = 3.4e38f;
+    for (int shape = 0; shape < hdr::kShadeShapes; ++shape) {
+        t.shade_shape = shape;
+        float ms = 0.0f;
+        st = time_best_of_two(
+            c,
+            [&]() -> hdr_status {
+                if (snap) HDR_CUDA(cudaMemcpyAsync(rv.dir_dist, snap, res_bytes, cudaMemcpyDeviceToDevice, s));
+                if (wb.q_winner) HDR_CUDA(cudaMemsetAsync(wb.counts + 4, 0, 2 * sizeof(int), s));
+                return HDR_OK;
+            },
+            [&]() {
+                return (tex ? hdr::textured::launch_ris_shade : hdr::launch_ris_shade)(
+                    c->scene, cd, frame_index, d, gb, rv, wb, color, trace_level, c->d_err, s, t);
+            },
+            ms);
+        if (st != HDR_OK) return st;
+        if (ms < shade_ms) shade_ms = ms, shade_pick = shape;
+    }
+    c->tune.shade_shape = shade_pick;
+    int n = 4;
+    if (wb.q_winner) {
+        if ((tex ? hdr::textured::launch_winner_visibility : hdr::launch_winner_visibility)(
+                c->scene, cd, frame_index, d, gb, rv, wb, color, c->d_err, s, c->tune) < 0)
+            return fail(HDR_ECUDA, "winner visibility launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        n += 2;
+    }
+    if (best) {
+        best->node_quorum = c->tune.node_quorum;
+        best->blocks_per_sm = c->tune.blocks_per_sm;
+        best->trace_ms = trace_ms;
+        best->shade_shape = c->tune.shade_shape;
+        best->shadow_shape = c->tune.shadow_shape;
+        best->shade_ms = shade_ms;
+    }
+    *frame_launches = n;
+    return HDR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+static hdr_status ris_path_trace_pass(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index,
+                                      const hdr_ris_params *p, hdr_trace_tuning *tune = nullptr) {
     if (!c || !p) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    struct TuneScope {  // hdr_autotune_frame: this call only
+        hdr_ctx *c;
+        ~TuneScope() { c->tune_frame = false, c->tune_out = nullptr; }
+    } tune_scope{c};
+    c->tune_frame = tune != nullptr;
+    c->tune_out = tune;
+    if (tune) HDR_NOT_RECORDING(c, "hdr_autotune_frame");
     hdr_status st = check_camera(cam);
     if (st != HDR_OK) return st;
     if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_ris_path_trace before hdr_scene_upload");
@@ -768,6 +981,9 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
     const bool spatial = p->spatial_neighbors > 0 && p->use_reservoir;
     if (spatial && !wave)
         return fail(HDR_EINVAL, "spatial reuse runs in the wavefront form only (max_depth 1, opaque scene)");
+    if (tune && !wave)
+        return fail(HDR_EINVAL, "hdr_autotune_frame tunes the wavefront form (max_depth 1, opaque scene, "
+                    "no HDR_RIS_ONE_KERNEL)");
     if ((st = check_cancel(c)) != HDR_OK) return st;
     HDR_CUDA(cudaSetDevice(c->device));
     const size_t count = (size_t)cam->width * cam->height;
@@ -795,7 +1011,8 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
     d.m_cap = p->m_cap;
     d.spatial_neighbors = p->spatial_neighbors;
     d.spatial_radius = p->spatial_radius;
-    const hdr::CameraD cd = make_camera(cam);
+    hdr::CameraD cd = make_camera(cam);
+    if ((st = record_frame_index(c, frame_index, &cd)) != HDR_OK) return st;
     const bool reproject = (p->flags & HDR_RIS_REPROJECT) && p->use_reservoir;
     hdr::GBufferView gb_prev{};
     if (reproject) {  // this frame's temporal history comes from where its hit points were last frame
@@ -842,9 +1059,10 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
     if (wave) {
         const int n_nee = std::max(1, p->candidate_count / 2);
         const int n_bsdf = std::max(0, p->candidate_count - n_nee);
+        const int trace_level = ris_trace_level(c, p);
         hdr::WaveBuffers wb{};
         wb.pixels = count;
-        wb.n_closest = 1 + n_bsdf;
+        wb.n_closest = closest_slots(trace_level, n_bsdf);
         wb.n_shadow = n_nee;
         void *q;
         if ((st = ensure_buffer(c, "__wave_q_closest", count * wb.n_closest * 32, &q)) != HDR_OK) return st;
@@ -873,17 +1091,22 @@ hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_i
             if ((st = ensure_buffer(c, "__wave_occ_winner", count, &q)) != HDR_OK) return st;
             wb.occ_winner = (unsigned char *)q;
         }
-        const int trace_level = ris_trace_level(c, p);
         if ((st = begin_pass(c, 1)) != HDR_OK) return st;
-        const bool timed = (c->flags & 1u) != 0;
+        const bool timed = timing_on(c);
         if (timed)
             for (int k = kSlotWaveFirst; k < kSlotWaveFirst + 4; ++k)
                 if ((st = fold_pass_time(c, k)) != HDR_OK) return st;
-        const int n = (c->scene.has_textures ? hdr::textured::launch_ris_wavefront : hdr::launch_ris_wavefront)(c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color,
-                                                trace_level, c->d_err, c->stream, c->tune,
-                                                timed ? c->ev_start + kSlotWaveFirst : nullptr,
-                                                timed ? c->ev_stop + kSlotWaveFirst : nullptr);
-        if (n < 0) return fail(HDR_ECUDA, "wavefront launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        int n = 0;
+        if (c->tune_frame) {  // hdr_autotune_frame: the same frame, its kernels run once per schedule and shape
+            if ((st = tune_wave_frame(c, cd, frame_index, d, gb, rv, wb, (float4 *)color, trace_level, c->tune_out,
+                                      &n)) != HDR_OK)
+                return st;
+        } else {
+            n = (c->scene.has_textures ? hdr::textured::launch_ris_wavefront : hdr::launch_ris_wavefront)(
+                c->scene, cd, frame_index, d, gb, rv, wb, (float4 *)color, trace_level, c->d_err, c->stream, c->tune,
+                timed ? c->ev_start + kSlotWaveFirst : nullptr, timed ? c->ev_stop + kSlotWaveFirst : nullptr);
+            if (n < 0) return fail(HDR_ECUDA, "wavefront launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        }
         if (timed)
             for (int k = kSlotWaveFirst; k < kSlotWaveFirst + 4; ++k) c->ev_pending[k] = true;
         c->launches += (uint64_t)n;
@@ -962,6 +1185,7 @@ hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src) {
     if (dst->device != src->device) return fail(HDR_EINVAL, "contexts are on different devices");
     std::lock(dst->mu, src->mu);
     std::lock_guard<std::mutex> l1(dst->mu, std::adopt_lock), l2(src->mu, std::adopt_lock);
+    HDR_NOT_RECORDING(dst, "hdr_scene_share");
     if (!src->has_scene) return fail(HDR_ENOSCENE, "the source context has no scene");
     if ((dst->flags & HDR_CTX_WIDE_BVH) && src->scene_store->wide_stale)
         return fail(HDR_EINVAL, "the scene's instances moved on the device: its wide TLAS is not rebuilt");
@@ -992,6 +1216,7 @@ hdr_status hdr_scene_set_instance_transforms(hdr_ctx *c, const float *transforms
                                              int32_t transforms_on_device) {
     if (!c || !transforms) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_scene_set_instance_transforms");
     if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_scene_set_instance_transforms before hdr_scene_upload");
     SceneStore *store = c->scene_store.get();
     if (num_instances != store->num_instances)
@@ -1073,6 +1298,7 @@ hdr_status hdr_scene_set_instance_transforms(hdr_ctx *c, const float *transforms
 hdr_status hdr_scene_array(hdr_ctx *c, const char *name, void *dst, size_t bytes, size_t *size) {
     if (!c || !name) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_scene_array");
     if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_scene_array before hdr_scene_upload");
     const auto it = c->scene_store->arrays.find(name);
     if (it == c->scene_store->arrays.end()) return fail(HDR_EINVAL, "no scene array named '%s'", name);
@@ -1141,13 +1367,13 @@ hdr_status prepare_ris_job(hdr_ctx *c, const hdr_camera *cam, int32_t frame_inde
     d.spatial_radius = p->spatial_radius;
     j.cd = make_camera(cam);
     const int n_nee = std::max(1, p->candidate_count / 2);
-    j.n_closest = 1 + std::max(0, p->candidate_count - n_nee);
+    j.trace_level = ris_trace_level(c, p);
+    j.n_closest = closest_slots(j.trace_level, std::max(0, p->candidate_count - n_nee));
     j.n_shadow = n_nee;
     if ((st = ensure_buffer(c, "__wave_rng", j.count * 48, &q)) != HDR_OK) return st;
     j.rng_state = (uint4 *)q;
     if ((st = ensure_buffer(c, "__wave_done", j.count, &q)) != HDR_OK) return st;
     j.done = (unsigned char *)q;
-    j.trace_level = ris_trace_level(c, p);
     return HDR_OK;
 }
 
@@ -1186,6 +1412,7 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
             for (hdr_ctx *c : v) c->mu.unlock();
         }
     } unlock{order};
+    for (hdr_ctx *c : order) HDR_NOT_RECORDING(c, "hdr_ris_path_trace_batch");
     hdr_ctx *lead = ctxs[0];
     HDR_CUDA(cudaSetDevice(lead->device));
     std::vector<RisJob> jobs((size_t)n);
@@ -1267,7 +1494,8 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
     return end_pass(lead, 1);
 }
 
-hdr_status hdr_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, const hdr_path_settings *p) {
+static hdr_status path_trace_pass(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index,
+                                  const hdr_path_settings *p) {
     if (!c || !p) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);
     hdr_status st = check_camera(cam);
@@ -1288,7 +1516,8 @@ hdr_status hdr_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index
     d.max_refr = p->max_refraction_bounces;
     d.render_ibl_background = p->render_ibl_background;
     d.roulette = p->roulette_aggressiveness;
-    const hdr::CameraD cd = make_camera(cam);
+    hdr::CameraD cd = make_camera(cam);
+    if ((st = record_frame_index(c, frame_index, &cd)) != HDR_OK) return st;
     if (c->scene_opaque && !(c->flags & HDR_CTX_PT_ONE_KERNEL)) {
         hdr::PtBuffers B{};
         if ((st = pt_buffers(c, count, B)) != HDR_OK) return st;
@@ -1340,6 +1569,7 @@ hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camer
             for (hdr_ctx *c : v) c->mu.unlock();
         }
     } unlock{order};
+    for (hdr_ctx *c : order) HDR_NOT_RECORDING(c, "hdr_path_trace_batch");
     hdr_ctx *lead = ctxs[0];
     HDR_CUDA(cudaSetDevice(lead->device));
     std::vector<hdr::PtJobD> jobs((size_t)n);
@@ -1412,7 +1642,7 @@ hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camer
     return end_pass(lead, 1);
 }
 
-hdr_status hdr_accumulate(hdr_ctx *c, int32_t frame_index, int32_t firefly, int32_t mode) {
+static hdr_status accumulate_pass(hdr_ctx *c, int32_t frame_index, int32_t firefly, int32_t mode) {
     if (!c) return fail(HDR_EINVAL, "ctx is NULL");
     std::lock_guard<std::mutex> lock(c->mu);
     if (mode != HDR_ACCUM_PARITY && mode != HDR_ACCUM_SHADER) return fail(HDR_EINVAL, "unknown accumulation mode");
@@ -1429,10 +1659,12 @@ hdr_status hdr_accumulate(hdr_ctx *c, int32_t frame_index, int32_t firefly, int3
     if ((st = ensure_buffer(c, "__accum_color", count * 16, &accum)) != HDR_OK) return st;
     if (firefly)
         if ((st = ensure_buffer(c, "__firefly_scratch", count * 16, &scratch)) != HDR_OK) return st;
+    if ((st = record_frame_index(c, frame_index, nullptr)) != HDR_OK) return st;
     if ((st = begin_pass(c, 2)) != HDR_OK) return st;
     cudaError_t err = cudaSuccess;
     const int n = hdr::launch_accumulate((float4 *)color, (float4 *)accum, (float4 *)scratch, c->d_flag, c->width,
-                                         c->height, frame_index, firefly, mode, c->stream, &err);
+                                         c->height, frame_index, firefly, mode, c->stream, &err,
+                                         c->recording ? c->d_frame_slot : nullptr);
     if (n < 0) return fail(HDR_ECUDA, "accumulation launch failed: %s", cudaGetErrorString(err));
     c->launches += (uint64_t)n;
     return end_pass(c, 2);
@@ -1441,6 +1673,7 @@ hdr_status hdr_accumulate(hdr_ctx *c, int32_t frame_index, int32_t firefly, int3
 hdr_status hdr_clear_persistent(hdr_ctx *c) {
     if (!c) return fail(HDR_EINVAL, "ctx is NULL");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_clear_persistent");
     HDR_CUDA(cudaSetDevice(c->device));
     for (const char *name : {"__accum_color", "__ris_reservoir", "__ris_reservoir_prev", "__prev_pos_depth"}) {
         auto it = c->buffers.find(name);
@@ -1470,8 +1703,8 @@ hdr_status hdr_buffer_size(hdr_ctx *c, const char *name, size_t *bytes) {
     return HDR_OK;
 }
 
-hdr_status hdr_resolve(hdr_ctx *c, const char *name, int32_t src_components, int32_t component_format,
-                       int32_t dst_components, void *dst, size_t dst_bytes, int32_t dst_on_device) {
+static hdr_status resolve_pass(hdr_ctx *c, const char *name, int32_t src_components, int32_t component_format,
+                               int32_t dst_components, void *dst, size_t dst_bytes, int32_t dst_on_device) {
     if (!c || !name || (!dst && dst_bytes)) return fail(HDR_EINVAL, "NULL argument");
     if (src_components < 1 || src_components > 4 || dst_components < 1 || dst_components > 4)
         return fail(HDR_EINVAL, "components must be 1..4 (source %d, destination %d)", src_components,
@@ -1480,6 +1713,7 @@ hdr_status hdr_resolve(hdr_ctx *c, const char *name, int32_t src_components, int
     if (component_format < HDR_FMT_FLOAT32 || component_format > HDR_FMT_INT32)
         return fail(HDR_EINVAL, "unknown component format %d", component_format);
     std::lock_guard<std::mutex> lock(c->mu);
+    if (!dst_on_device) HDR_NOT_RECORDING(c, "hdr_resolve into host memory");
     HDR_CUDA(cudaSetDevice(c->device));
     size_t have = 0;
     void *src = find_buffer(c, name, &have);
@@ -1528,6 +1762,7 @@ hdr_status hdr_upscale(hdr_ctx *c, const char *name, int32_t components, int32_t
         (size_t)dst_w * dst_h > ((size_t)1 << 31))
         return fail(HDR_EINVAL, "bad upscale sizes");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_upscale");
     HDR_CUDA(cudaSetDevice(c->device));
     auto it = c->buffers.find(name);
     if (it == c->buffers.end()) return fail(HDR_EINVAL, "no buffer named '%s'", name);
@@ -1550,7 +1785,8 @@ hdr_status hdr_upscale(hdr_ctx *c, const char *name, int32_t components, int32_t
     return HDR_OK;
 }
 
-hdr_status hdr_denoise(hdr_ctx *c, const char *name, int32_t width, int32_t height, int32_t chromaticity_blur) {
+static hdr_status denoise_pass(hdr_ctx *c, const char *name, int32_t width, int32_t height,
+                               int32_t chromaticity_blur) {
     if (!c || !name) return fail(HDR_EINVAL, "NULL argument");
     if (width < 0 || height < 0) return fail(HDR_EINVAL, "bad size");
     std::lock_guard<std::mutex> lock(c->mu);
@@ -1576,6 +1812,7 @@ hdr_status hdr_download_async(hdr_ctx *c, const char *name, void *dst, size_t by
     if (!c || !name || (!dst && bytes)) return fail(HDR_EINVAL, "NULL argument");
     if (std::strcmp(name, "GBuffer") == 0) return fail(HDR_EINVAL, "GBuffer is read with hdr_download");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_download_async");
     HDR_CUDA(cudaSetDevice(c->device));
     size_t have = 0;
     void *src = find_buffer(c, name, &have);
@@ -1607,6 +1844,7 @@ hdr_status hdr_download_async(hdr_ctx *c, const char *name, void *dst, size_t by
 hdr_status hdr_download_wait(hdr_ctx *c) {
     if (!c) return fail(HDR_EINVAL, "ctx is NULL");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_download_wait");
     if (!c->copy_stream) return HDR_OK;
     HDR_CUDA(cudaSetDevice(c->device));
     HDR_CUDA(cudaStreamWaitEvent(c->stream, c->copy_done, 0));  // later work on the ctx stream follows the copy
@@ -1617,6 +1855,7 @@ hdr_status hdr_download_wait(hdr_ctx *c) {
 hdr_status hdr_download(hdr_ctx *c, const char *name, void *dst, size_t bytes) {
     if (!c || !name || (!dst && bytes)) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_download");
     HDR_CUDA(cudaSetDevice(c->device));
     size_t have = 0;
     void *src = find_buffer(c, name, &have);
@@ -1656,6 +1895,7 @@ hdr_status hdr_download(hdr_ctx *c, const char *name, void *dst, size_t bytes) {
 hdr_status hdr_upload(hdr_ctx *c, const char *name, const void *src, size_t bytes) {
     if (!c || !name || (!src && bytes)) return fail(HDR_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_upload");
     HDR_CUDA(cudaSetDevice(c->device));
     if (std::strcmp(name, "GBuffer") == 0) return fail(HDR_EINVAL, "GBuffer is produced on the device only");
     void *dst = nullptr;
@@ -1668,6 +1908,7 @@ hdr_status hdr_upload(hdr_ctx *c, const char *name, const void *src, size_t byte
 hdr_status hdr_synchronize(hdr_ctx *c) {
     if (!c) return fail(HDR_EINVAL, "ctx is NULL");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_synchronize");
     HDR_CUDA(cudaSetDevice(c->device));
     HDR_CUDA(cudaStreamSynchronize(c->stream));
     return read_device_error(c);
@@ -1684,6 +1925,7 @@ hdr_status hdr_trace_rays(hdr_ctx *c, const float *rays, const float *tmax, int3
                           hdr_gbuffer_texel *out) {
     if (!c || (n > 0 && (!rays || !out)) || n < 0) return fail(HDR_EINVAL, "bad argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_trace_rays");
     if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_trace_rays before hdr_scene_upload");
     if (n == 0) return HDR_OK;
     HDR_CUDA(cudaSetDevice(c->device));
@@ -1733,6 +1975,7 @@ hdr_status hdr_trace_stats(hdr_ctx *c, const float *rays, const float *tmax, int
                            int32_t *out) {
     if (!c || (n > 0 && (!rays || !out)) || n < 0 || walk < 0 || walk > 5) return fail(HDR_EINVAL, "bad argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_trace_stats");
     if (!c->has_scene) return fail(HDR_ENOSCENE, "hdr_trace_stats before hdr_scene_upload");
     if (walk >= 4 && !c->scene.sh4) return fail(HDR_EINVAL, "walk %d: the scene has no 4-wide SAH trees on this ctx", walk);
     if (n == 0) return HDR_OK;
@@ -1767,6 +2010,7 @@ hdr_status hdr_get_trace_tuning(hdr_ctx *c, hdr_trace_tuning *out) {
     out->trace_ms = 0.0f;
     out->shade_shape = c->tune.shade_shape;
     out->shadow_shape = c->tune.shadow_shape;
+    out->shade_ms = 0.0f;
     return HDR_OK;
 }
 
@@ -1788,40 +2032,14 @@ hdr_status hdr_set_trace_tuning(hdr_ctx *c, const hdr_trace_tuning *t) {
 hdr_status hdr_autotune_trace(hdr_ctx *c, hdr_trace_tuning *best) {
     if (!c) return fail(HDR_EINVAL, "ctx is NULL");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_autotune_trace");
     if (!c->have_wave || !c->has_scene)
         return fail(HDR_EINVAL, "hdr_autotune_trace needs a previous wavefront hdr_ris_path_trace on this ctx");
     HDR_CUDA(cudaSetDevice(c->device));
-    static const int kQuorum[] = {8, 12, 16, 20, 24, 28};
-    static const int kBlocks[] = {4, 6, 8, 16};
-    hdr::TraceTuning t = c->tune;
-    hdr::TraceTuning pick = c->tune;
-    float pick_ms = 3.4e38f;
-    cudaEvent_t ev[2] = {c->region_ev[3][0], c->region_ev[3][1]};
-    const int n_shapes = c->scene.sh4 ? hdr::kShadowShapes : 1;
-    for (int si = 0; si < n_shapes; ++si)
-    for (int qi = 0; qi < (int)(sizeof(kQuorum) / sizeof(int)); ++qi) {
-        for (int bi = 0; bi < (int)(sizeof(kBlocks) / sizeof(int)); ++bi) {
-            t.node_quorum = kQuorum[qi];
-            t.blocks_per_sm = kBlocks[bi];
-            if (c->scene.sh4) t.shadow_shape = si;
-            float ms_min = 3.4e38f;
-            for (int rep = 0; rep < 2; ++rep) {
-                // the trace kernels only read the queues and rewrite the same results; rerunning them
-                // needs nothing but their fetch counters back at zero
-                HDR_CUDA(cudaMemsetAsync(c->last_wave.counts + 2, 0, 2 * sizeof(int), c->stream));
-                HDR_CUDA(cudaEventRecord(ev[0], c->stream));
-                if (hdr::launch_wave_trace(c->scene, c->last_wave, t, c->d_err, c->stream) < 0)
-                    return fail(HDR_ECUDA, "trace launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-                c->launches += 2;
-                HDR_CUDA(cudaEventRecord(ev[1], c->stream));
-                HDR_CUDA(cudaEventSynchronize(ev[1]));
-                float ms = 0.0f;
-                HDR_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
-                ms_min = std::min(ms_min, ms);
-            }
-            if (ms_min < pick_ms) pick_ms = ms_min, pick = t;
-        }
-    }
+    hdr::TraceTuning pick;
+    float pick_ms = 0.0f;
+    hdr_status st = search_trace_schedule(c, c->last_wave, pick, pick_ms);
+    if (st != HDR_OK) return st;
     c->tune.node_quorum = pick.node_quorum;
     c->tune.blocks_per_sm = pick.blocks_per_sm;
     c->tune.shadow_shape = pick.shadow_shape;
@@ -1831,13 +2049,24 @@ hdr_status hdr_autotune_trace(hdr_ctx *c, hdr_trace_tuning *best) {
         best->trace_ms = pick_ms;
         best->shade_shape = c->tune.shade_shape;
         best->shadow_shape = c->tune.shadow_shape;
+        best->shade_ms = 0.0f;  // not measured here (hdr_autotune_frame measures it)
     }
+    return read_device_error(c);
+}
+
+hdr_status hdr_autotune_frame(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, const hdr_ris_params *p,
+                              hdr_trace_tuning *best) {
+    hdr_trace_tuning local{};
+    hdr_status st = ris_path_trace_pass(c, cam, frame_index, p, best ? best : &local);
+    if (st != HDR_OK) return st;
+    std::lock_guard<std::mutex> lock(c->mu);
     return read_device_error(c);
 }
 
 hdr_status hdr_rng_floats(hdr_ctx *c, const uint32_t *seeds, int32_t n_seeds, int32_t count, float *out) {
     if (!c || n_seeds < 0 || count < 0 || (n_seeds > 0 && (!seeds || !out))) return fail(HDR_EINVAL, "bad argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_rng_floats");
     if (n_seeds == 0 || count == 0) return HDR_OK;
     HDR_CUDA(cudaSetDevice(c->device));
     DevBuf ds, dout;
@@ -1862,6 +2091,7 @@ hdr_status hdr_rng_floats(hdr_ctx *c, const uint32_t *seeds, int32_t n_seeds, in
 hdr_status hdr_pass_times(hdr_ctx *c, float *avg_ms, int32_t *counts, int32_t n, int32_t reset) {
     if (!c || (n > 0 && (!avg_ms || !counts))) return fail(HDR_EINVAL, "bad argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_pass_times");
     for (int k = 0; k < kTimeSlots; ++k) {
         hdr_status st = fold_pass_time(c, k);
         if (st != HDR_OK) return st;
@@ -1878,6 +2108,7 @@ hdr_status hdr_pass_times(hdr_ctx *c, float *avg_ms, int32_t *counts, int32_t n,
 hdr_status hdr_region_begin(hdr_ctx *c, int32_t slot) {
     if (!c || slot < 0 || slot >= 4) return fail(HDR_EINVAL, "bad region slot");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_region_begin");
     HDR_CUDA(cudaEventRecord(c->region_ev[slot][0], c->stream));
     return HDR_OK;
 }
@@ -1885,6 +2116,7 @@ hdr_status hdr_region_begin(hdr_ctx *c, int32_t slot) {
 hdr_status hdr_region_end(hdr_ctx *c, int32_t slot) {
     if (!c || slot < 0 || slot >= 4) return fail(HDR_EINVAL, "bad region slot");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_region_end");
     HDR_CUDA(cudaEventRecord(c->region_ev[slot][1], c->stream));
     return HDR_OK;
 }
@@ -1892,6 +2124,7 @@ hdr_status hdr_region_end(hdr_ctx *c, int32_t slot) {
 hdr_status hdr_region_elapsed(hdr_ctx *c, int32_t slot, float *ms) {
     if (!c || !ms || slot < 0 || slot >= 4) return fail(HDR_EINVAL, "bad argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_region_elapsed");
     HDR_CUDA(cudaEventSynchronize(c->region_ev[slot][1]));
     HDR_CUDA(cudaEventElapsedTime(ms, c->region_ev[slot][0], c->region_ev[slot][1]));
     return HDR_OK;
@@ -1899,7 +2132,129 @@ hdr_status hdr_region_elapsed(hdr_ctx *c, int32_t slot, float *ms) {
 
 hdr_status hdr_launch_count(hdr_ctx *c, uint64_t *count) {
     if (!c || !count) return fail(HDR_EINVAL, "bad argument");
-    *count = c->launches;
+    std::lock_guard<std::mutex> lock(c->mu);
+    *count = c->recording ? c->rec_launches0 : c->launches;  // recorded kernels count when the graph runs
+    return HDR_OK;
+}
+
+// A frame's pass chain as one CUDA graph. The passes' kernels take the frame
+// index and the camera by value, so a new frame is recorded again (stream
+// capture records launches without submitting them) and the executable graph
+// is updated in place (cudaGraphExecUpdate) rather than instantiated anew.
+hdr_status hdr_graph_begin(hdr_ctx *c) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (c->recording) return fail(HDR_EINVAL, "the ctx is already recording");
+    HDR_CUDA(cudaSetDevice(c->device));
+    HDR_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    c->recording = true;
+    c->rec_failed = false;
+    c->rec_has_frame = false;
+    c->rec_launches0 = c->launches;
+    return HDR_OK;
+}
+
+hdr_status hdr_graph_end(hdr_ctx *c) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (!c->recording) return fail(HDR_EINVAL, "hdr_graph_end without hdr_graph_begin");
+    HDR_CUDA(cudaSetDevice(c->device));
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->recording = false;
+    const uint64_t kernels = c->launches - c->rec_launches0;
+    c->launches = c->rec_launches0;  // the recorded kernels run at hdr_graph_launch
+    if (e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        return fail(HDR_ECUDA, "recording failed (a recorded call was not capturable): %s", cudaGetErrorString(e));
+    }
+    if (c->rec_failed) {  // the record lacks a failed pass's work: discarded, the previous graph is kept
+        cudaGraphDestroy(g);
+        return fail(HDR_EINVAL, "a pass failed while recording; the recording is discarded");
+    }
+    if (c->graph_exec) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(c->graph_exec, g, &info) == cudaSuccess) {
+            c->graph_updates += 1;
+        } else {  // another chain (other passes, sizes or launch shapes): instantiate it
+            (void)cudaGetLastError();
+            cudaGraphExecDestroy(c->graph_exec);
+            c->graph_exec = nullptr;
+        }
+    }
+    if (!c->graph_exec) {
+        e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+        if (e != cudaSuccess) {
+            c->graph_exec = nullptr;
+            cudaGraphDestroy(g);
+            return fail(HDR_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+        }
+        c->graph_instantiations += 1;
+    }
+    cudaGraphDestroy(g);
+    c->graph_kernels = kernels;
+    c->graph_has_frame = c->rec_has_frame;
+    c->graph_frame = c->rec_frame;
+    return HDR_OK;
+}
+
+hdr_status hdr_graph_launch(hdr_ctx *c, int32_t frame_index) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    HDR_NOT_RECORDING(c, "hdr_graph_launch");
+    if (!c->graph_exec) return fail(HDR_EINVAL, "no recorded graph (hdr_graph_begin / hdr_graph_end)");
+    hdr_status st;
+    if ((st = check_cancel(c)) != HDR_OK) return st;
+    HDR_CUDA(cudaSetDevice(c->device));
+    if (c->graph_has_frame) {  // the frame the recorded passes render, read by their kernels
+        set_frame_slot_kernel<<<1, 1, 0, c->stream>>>(c->d_frame_slot, frame_index >= 0 ? frame_index
+                                                                                       : c->graph_frame);
+        HDR_CUDA(cudaGetLastError());
+        c->launches += 1;
+    }
+    HDR_CUDA(cudaGraphLaunch(c->graph_exec, c->stream));
+    c->launches += c->graph_kernels;
+    return HDR_OK;
+}
+
+// The passes a graph may record. One that fails while its ctx records leaves
+// the record without its work, so the recording is marked and hdr_graph_end
+// discards it.
+static hdr_status noted(hdr_ctx *c, hdr_status st) {
+    if (st != HDR_OK && c) {
+        std::lock_guard<std::mutex> lock(c->mu);
+        if (c->recording) c->rec_failed = true;
+    }
+    return st;
+}
+hdr_status hdr_raycast(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, uint32_t aov_mask) {
+    return noted(c, raycast_pass(c, cam, frame_index, aov_mask));
+}
+hdr_status hdr_ris_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, const hdr_ris_params *p) {
+    return noted(c, ris_path_trace_pass(c, cam, frame_index, p));
+}
+hdr_status hdr_path_trace(hdr_ctx *c, const hdr_camera *cam, int32_t frame_index, const hdr_path_settings *p) {
+    return noted(c, path_trace_pass(c, cam, frame_index, p));
+}
+hdr_status hdr_accumulate(hdr_ctx *c, int32_t frame_index, int32_t firefly, int32_t mode) {
+    return noted(c, accumulate_pass(c, frame_index, firefly, mode));
+}
+hdr_status hdr_resolve(hdr_ctx *c, const char *name, int32_t src_components, int32_t component_format,
+                       int32_t dst_components, void *dst, size_t dst_bytes, int32_t dst_on_device) {
+    return noted(c, resolve_pass(c, name, src_components, component_format, dst_components, dst, dst_bytes,
+                                 dst_on_device));
+}
+hdr_status hdr_denoise(hdr_ctx *c, const char *name, int32_t width, int32_t height, int32_t chromaticity_blur) {
+    return noted(c, denoise_pass(c, name, width, height, chromaticity_blur));
+}
+
+hdr_status hdr_graph_info(hdr_ctx *c, int32_t *kernels, int32_t *instantiations, int32_t *updates) {
+    if (!c) return fail(HDR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (kernels) *kernels = (int32_t)c->graph_kernels;
+    if (instantiations) *instantiations = c->graph_instantiations;
+    if (updates) *updates = c->graph_updates;
     return HDR_OK;
 }
 

@@ -32,13 +32,13 @@ __device__ __forceinline__ void integrate_pixel(const DeviceScene &s, const Came
 }
 
 template <bool kRis>
-__global__ void __launch_bounds__(256) integrate_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
+__global__ void __launch_bounds__(256) integrate_kernel(DeviceScene s, CameraD cam, int frame_arg, PathRun pr,
                                                         RisRun ris, GBufferView gb, ReservoirView rv, float4 *color,
                                                         unsigned *err) {
     int x, y;
     if (!tile_pixel(cam.width, cam.height, x, y)) return;
     unsigned e = 0;
-    integrate_pixel<kRis>(s, cam, frame_index, pr, ris, gb, rv, color, x, y, e);
+    integrate_pixel<kRis>(s, cam, live_frame(cam, frame_arg), pr, ris, gb, rv, color, x, y, e);
     if (e) atomicOr(err, e);
 }
 

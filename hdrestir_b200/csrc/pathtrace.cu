@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(256) pt_start_kernel(DeviceScene s, PtJobD one
     uint64_t spill[312];
     MtStream rng;
     // IntegrationPass prologue (integration_pass.cpp:210-233), as integrate_kernel
-    rng.init((uint32_t)li ^ (uint32_t)((unsigned long long)job.frame_index * 12345ULL), spill);
+    rng.init((uint32_t)li ^ (uint32_t)((unsigned long long)live_frame(cam, job.frame_index) * 12345ULL), spill);
     const float px = (float)x + rng.next_float();
     const float py = (float)y + rng.next_float();
     const RayF ray = camera_ray(cam, px, py, rng);

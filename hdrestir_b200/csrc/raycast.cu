@@ -22,8 +22,9 @@ __device__ __forceinline__ void write_gbuffer(const GBufferView &gb, size_t i, b
     }
 }
 
-__global__ void __launch_bounds__(256) raycast_kernel(DeviceScene s, CameraD cam, int frame_index, GBufferView gb,
+__global__ void __launch_bounds__(256) raycast_kernel(DeviceScene s, CameraD cam, int frame_arg, GBufferView gb,
                                                       AovView aov, unsigned *err) {
+    const int frame_index = live_frame(cam, frame_arg);
     int x, y;
     if (!tile_pixel(cam.width, cam.height, x, y)) return;
     const size_t i = (size_t)y * (size_t)cam.width + (size_t)x;

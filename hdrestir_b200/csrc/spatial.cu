@@ -54,11 +54,12 @@ __device__ __forceinline__ void copy_record(const ReservoirView &in, const Reser
 }
 
 template <int kThreads>
-__global__ void __launch_bounds__(kThreads) ris_spatial_kernel(DeviceScene s, CameraD cam, int frame_index,
+__global__ void __launch_bounds__(kThreads) ris_spatial_kernel(DeviceScene s, CameraD cam, int frame_arg,
                                                                PathRun pr, int cpf, int m_cap, int neighbours,
                                                                float radius, GBufferView gb, ReservoirView in,
                                                                ReservoirView out, float4 *color, float4 *q_winner,
                                                                int *winner_count, unsigned *err) {
+    const int frame_index = live_frame(cam, frame_arg);
     MtStream rng;
     PixelStart ps;
     if (!pixel_start<kThreads>(s, cam, frame_index, gb, rng, nullptr, ps)) return;

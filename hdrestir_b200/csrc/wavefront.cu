@@ -54,13 +54,13 @@ __device__ __forceinline__ int queue_append(int *counter, bool want) {
     return base + __popc(mask & ((1u << lane) - 1u));
 }
 
-__global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
+__global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, CameraD cam, int frame_arg, PathRun pr,
                                                            RisRun ris, GBufferView gb, WaveBuffers wb, float4 *color,
                                                            int trace_level, unsigned *err) {
     uint64_t spill[312];
     MtStream rng;
     PixelStart ps;
-    if (!pixel_start(s, cam, frame_index, gb, rng, spill, ps)) return;
+    if (!pixel_start(s, cam, live_frame(cam, frame_arg), gb, rng, spill, ps)) return;
     const size_t i = ps.i;
     if (!ps.has_hit) {  // PathIntegrator::Li without a hit: background only, no reservoir access
         V3 rgb = v3s(0.0f);
@@ -471,14 +471,14 @@ __global__ void __launch_bounds__(kTraceThreads) trace_shadow_kernel(DeviceScene
 }
 
 template <int kThreads, int kMinBlocks>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) ris_shade_kernel(DeviceScene s, CameraD cam, int frame_index,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) ris_shade_kernel(DeviceScene s, CameraD cam, int frame_arg,
                                                                          PathRun pr, RisRun ris, GBufferView gb,
                                                                          ReservoirView rv, WaveBuffers wb, float4 *color,
                                                                          int trace_level, unsigned *err) {
     uint64_t spill[312];
     MtStream rng;
     PixelStart ps;
-    if (!pixel_start<kThreads>(s, cam, frame_index, gb, rng, spill, ps)) return;
+    if (!pixel_start<kThreads>(s, cam, live_frame(cam, frame_arg), gb, rng, spill, ps)) return;
     const size_t i = ps.i;
     if (wb.done[i]) return;
     unsigned e = 0;
@@ -591,10 +591,11 @@ int launch_ris_shade(const DeviceScene &s, const CameraD &cam, int frame_index, 
 // After the queued winner shadow rays: a pixel whose winner turned out occluded
 // gets what the test on the spot would have given it, throughput 0 (so the
 // direct term is 0) and Color = Beer * emission of its surface.
-__global__ void __launch_bounds__(256) ris_winner_fixup_kernel(DeviceScene s, CameraD cam, int frame_index, PathRun pr,
+__global__ void __launch_bounds__(256) ris_winner_fixup_kernel(DeviceScene s, CameraD cam, int frame_arg, PathRun pr,
                                                               GBufferView gb, ReservoirView rv, const float4 *q,
                                                               const int *count, const unsigned char *occ,
                                                               float4 *color) {
+    const int frame_index = live_frame(cam, frame_arg);
     const int n = *count;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const int px = __float_as_int(q[2 * (size_t)k].w);

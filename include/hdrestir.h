@@ -569,6 +569,7 @@ typedef struct hdr_trace_tuning {
     float trace_ms;
     int32_t shade_shape;
     int32_t shadow_shape;
+    float shade_ms;         /* hdr_autotune_frame: the resampling kernel's time at shade_shape */
 } hdr_trace_tuning;
 hdr_status hdr_get_trace_tuning(hdr_ctx *ctx, hdr_trace_tuning *out);
 hdr_status hdr_set_trace_tuning(hdr_ctx *ctx, const hdr_trace_tuning *tuning);
@@ -577,6 +578,20 @@ hdr_status hdr_set_trace_tuning(hdr_ctx *ctx, const hdr_trace_tuning *tuning);
  * over a grid of schedules (node quorum x blocks per SM, and the shadow-BVH
  * walk's register budget), keeps the fastest in the ctx and returns it. */
 hdr_status hdr_autotune_trace(hdr_ctx *ctx, hdr_trace_tuning *best);
+/* Autotuner over a whole frame: renders one hdr_ris_path_trace frame in the
+ * wavefront form (max_depth 1, opaque scene, no HDR_RIS_ONE_KERNEL; else
+ * HDR_EINVAL) and tunes while it renders. After the generate kernel has filled
+ * the ray queues, the trace kernels run once per trace schedule (as
+ * hdr_autotune_trace), then the resampling kernel runs once per launch shape,
+ * each time from a copy of the reservoirs it merges into and with the winner
+ * queue emptied. Every run writes the same bytes, so the frame's buffers are
+ * those of hdr_ris_path_trace. The fastest schedule and shape stay in the ctx
+ * and are returned in *best (may be NULL) with their times. The closest-hit
+ * queue needs no tuning: it holds a slot only for the rays the frame casts
+ * (none when BSDF-candidate rays cannot change the image). Takes about 150
+ * trace runs and 8 resampling runs; synchronises the ctx stream. */
+hdr_status hdr_autotune_frame(hdr_ctx *ctx, const hdr_camera *cam, int32_t frame_index,
+                              const hdr_ris_params *params, hdr_trace_tuning *best);
 
 /* Diagnostic, no reference counterpart: the work one traversal form does per
  * ray. walk: 0 closest hit on the binary trees, 1 closest hit on their 4-wide
@@ -612,6 +627,45 @@ hdr_status hdr_region_elapsed(hdr_ctx *ctx, int32_t slot, float *ms);
 
 /* Number of this library's kernels launched on the ctx so far. */
 hdr_status hdr_launch_count(hdr_ctx *ctx, uint64_t *count);
+
+/* ---------------------------------------------------------------------------
+ * A frame's pass chain as one CUDA graph. No reference counterpart: the
+ * reference's RenderPipeline::Execute (pipeline/render_pipeline.cpp:24-40)
+ * calls its passes one by one, and the calls here do the same by default.
+ *
+ * Between hdr_graph_begin and hdr_graph_end the pass calls on ctx
+ * (hdr_raycast, hdr_ris_path_trace, hdr_path_trace, hdr_accumulate,
+ * hdr_zero_persistent, hdr_denoise, hdr_resolve into device memory) are
+ * recorded from the ctx stream instead of run: they check their arguments,
+ * update the ctx's host-side state (frame size, reprojection history) and
+ * return. The recorded passes must render one frame index; their kernels read
+ * it from device memory, so the record replays for any frame.
+ * hdr_graph_end makes the record the ctx's executable graph: the first one is
+ * instantiated, a later one with the same launches (other camera or parameter
+ * values) updates it in place (cudaGraphExecUpdate), and one with other
+ * launches replaces it. hdr_graph_launch(ctx, frame_index) stores frame_index
+ * (-1: the recorded one) where the recorded kernels read it and runs the graph
+ * on the ctx stream: the results are those of the recorded calls made eagerly
+ * with that frame index, every other argument (camera included) as recorded.
+ * So a static camera's progressive frames are recorded once and replayed with
+ * two launches per frame; a moving camera records each frame again.
+ *
+ * While recording: every buffer a recorded pass uses must already exist at its
+ * size (run the same passes once eagerly first), else the pass fails with
+ * HDR_EINVAL; pass timing (flag bit 0) is not taken; calls that wait for the
+ * device, copy to or from the host, allocate or free (hdr_download*,
+ * hdr_upload, hdr_synchronize, hdr_region_*, hdr_pass_times, hdr_scene_*,
+ * hdr_clear_persistent, hdr_upscale, the batch calls, hdr_trace_*,
+ * hdr_autotune_trace, hdr_rng_floats, hdr_graph_launch) fail with HDR_EINVAL and
+ * leave the recording intact. A recorded pass that fails marks the recording,
+ * and hdr_graph_end then discards it (HDR_EINVAL) and keeps the previous graph.
+ * hdr_ctx_destroy drops an unfinished recording. */
+hdr_status hdr_graph_begin(hdr_ctx *ctx);
+hdr_status hdr_graph_end(hdr_ctx *ctx);
+hdr_status hdr_graph_launch(hdr_ctx *ctx, int32_t frame_index);
+/* The executable graph's kernel launches per replay, and how many times
+ * hdr_graph_end instantiated a graph and updated one in place (any may be NULL). */
+hdr_status hdr_graph_info(hdr_ctx *ctx, int32_t *kernels, int32_t *instantiations, int32_t *updates);
 
 #ifdef __cplusplus
 }

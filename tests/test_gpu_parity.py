@@ -259,6 +259,48 @@ def test_autotune_trace_keeps_results():
         assert np.array_equal(ctx.download("Color").view(np.uint32), before.view(np.uint32))
 
 
+@pytest.mark.parametrize("kw", [dict(), dict(skip_visibility=True), dict(trace_all_rays=True),
+                                dict(spatial_neighbors=4, spatial_radius=6.0, m_cap=20)])
+def test_autotune_frame_renders_the_frame(kw):
+    """A tuning frame (every trace schedule and resampling launch shape run on the
+    same queues and reservoir copies) leaves exactly the buffers of the plain
+    frame, reservoirs with history included, and the frames after it too."""
+    from hdrestir_b200.context import Context
+    sc, cam = configs.small_variant(2, 96, 64, grid=96, n_spheres=60, n_lights=300)
+    ris = dict(candidate_count=32, use_reservoir=True, max_depth=1, **kw)
+    out = []
+    for tune in (False, True):
+        with Context(device=0) as ctx:
+            ctx.upload_scene(sc)
+            snaps = []
+            for f in range(3):
+                ctx.raycast(cam, f)
+                if tune and f == 1:
+                    best = ctx.autotune_frame(cam, f, **ris)
+                    assert best["shade_shape"] in range(4) and best["shade_ms"] > 0.0 and best["trace_ms"] > 0.0
+                    assert ctx.trace_tuning()["shade_shape"] == best["shade_shape"]
+                else:
+                    ctx.ris_path_trace(cam, f, **ris)
+                ctx.accumulate(f)
+                snaps.append([ctx.download(n).copy() for n in ("Color", "__ris_reservoir", "__accum_color")])
+            out.append(snaps)
+    for f, (plain, tuned) in enumerate(zip(*out)):
+        for a, b in zip(plain, tuned):
+            assert np.array_equal(np.ascontiguousarray(a).view(np.uint32),
+                                  np.ascontiguousarray(b).view(np.uint32)), f"frame {f}"
+
+
+def test_autotune_frame_rejects_the_one_kernel_form():
+    from hdrestir_b200.context import Context
+    sc, cam = configs.small_variant(2, 32, 32, grid=64, n_spheres=10, n_lights=50)
+    with Context(device=0) as ctx:
+        ctx.upload_scene(sc)
+        ctx.raycast(cam, 0)
+        with pytest.raises(abi.HdrError) as e:
+            ctx.autotune_frame(cam, 0, candidate_count=8, use_reservoir=True, max_depth=2)
+        assert e.value.status == abi.HDR_EINVAL
+
+
 def _dome_scene(w=64, h=48):
     sc, cam, cams = configs.config3(w, h, n_small=3, small=32, grid=96, n_spheres=60, n_lights=300,
                                     dome_size=(128, 64))
