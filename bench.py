@@ -409,52 +409,49 @@ def serving_leg(n_jobs: int, rate: float = 200.0):
                        "256^2..2048x1152, 1-16 frames, ReSTIR (32 cand) or PathTracer (maxDepth 4); "
                        "HBM admission budget 120 GB",
            "mpx_frames": mpx_frames}
-    step_px = {"plain": 0, "served_all": 0, "served": 16 << 20}
+    step_px = {"plain": 0, "served_all": 0, "served": 32 << 20}
+
+    def stream(sv, sids):
+        lat, pending, nxt = [], {}, 0
+        steps = 0
+        t0 = time.perf_counter()
+        while len(lat) < n_jobs:
+            now = time.perf_counter() - t0
+            while nxt < n_jobs and jobs[nxt]["arrival"] <= now:
+                j = jobs[nxt]
+                kw = configs.RIS_CONFIG2 if j["pipeline"] == "ris" else configs.PT_CONFIG4
+                jid = sv.submit(sids[j["cfg"]], cams[nxt], j["frames"], j["pipeline"], **kw)
+                pending[jid] = j["arrival"]
+                nxt += 1
+            if not pending:
+                time.sleep(max(0.0, jobs[nxt]["arrival"] - now))
+                continue
+            steps += 1
+            if sv.step() == 0:
+                continue
+            now = time.perf_counter() - t0
+            for jid in sv.finished():
+                if sv.state(jid)[0] == abi.JOB_FAILED:
+                    raise RuntimeError(f"serving job {jid} failed")
+                lat.append(now - pending.pop(jid))
+                sv.take(jid, keep_image=False)
+        return lat, steps, time.perf_counter() - t0
+
     for mode in ("plain", "served_all", "served"):
         with Server(device=0, hbm_budget=120 << 30, serial=(mode == "plain"), step_pixels=step_px[mode]) as sv:
             sids = [sv.add_scene(s) for s in scenes]
-            # untimed warm-up: one job of each (scene, pipeline) pair loads the kernels and the allocator
-            warm = []
-            for cfg in range(3):
-                for pipe in ("ris", "pt"):
-                    kw = configs.RIS_CONFIG2 if pipe == "ris" else configs.PT_CONFIG4
-                    warm.append(sv.submit(sids[cfg], configs.config_camera(cfg, 256, 256), 2, pipe, **kw))
-            while sv.load()[:2] != (0, 0):
-                sv.step()
-            for jid in warm:
-                sv.take(jid, keep_image=False)
-            sv.finished()
-            lat, pending, nxt = [], {}, 0
-            steps = 0
-            t0 = time.perf_counter()
-            while len(lat) < n_jobs:
-                now = time.perf_counter() - t0
-                while nxt < n_jobs and jobs[nxt]["arrival"] <= now:
-                    j = jobs[nxt]
-                    kw = configs.RIS_CONFIG2 if j["pipeline"] == "ris" else configs.PT_CONFIG4
-                    jid = sv.submit(sids[j["cfg"]], cams[nxt], j["frames"], j["pipeline"], **kw)
-                    pending[jid] = j["arrival"]
-                    nxt += 1
-                if not pending:
-                    time.sleep(max(0.0, jobs[nxt]["arrival"] - now))
-                    continue
-                steps += 1
-                if sv.step() == 0:
-                    continue
-                now = time.perf_counter() - t0
-                for jid in sv.finished():
-                    if sv.state(jid)[0] == abi.JOB_FAILED:
-                        raise RuntimeError(f"serving job {jid} failed")
-                    lat.append(now - pending.pop(jid))
-                    sv.take(jid, keep_image=False)
-            makespan = time.perf_counter() - t0
+            # untimed warm-up: the same job stream once, so the timed pass sees the server at steady state
+            # (kernels loaded, contexts pooled, the frame-buffer pool and batch queues grown)
+            stream(sv, sids)
+            lat, steps, makespan = stream(sv, sids)
         lat.sort()
         out[mode] = {"jobs_per_s": n_jobs / makespan, "mpx_frames_per_s": mpx_frames / makespan,
                      "makespan_s": makespan, "latency_p50_ms": 1000.0 * statistics.median(lat),
                      "latency_p99_ms": 1000.0 * lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))],
                      "steps": steps}
     out["modes"] = ("plain: one job at a time, each frame rendered alone; served_all: every admitted job "
-                    "advances each step; served: least remaining work first, 16 Mpx per step")
+                    "advances each step; served: least remaining work first, 32 Mpx per step; each mode "
+                    "timed on its second pass over the job stream (the first warms the server up)")
     return out
 
 

@@ -214,6 +214,7 @@ def lib() -> C.CDLL:
             "hdr_region_begin": (C.c_int, [vp, i32]),
             "hdr_region_end": (C.c_int, [vp, i32]),
             "hdr_region_elapsed": (C.c_int, [vp, i32, C.POINTER(C.c_float)]),
+            "hdr_trim_frame_memory": (C.c_int, [i32, sz]),
             "hdr_graph_begin": (C.c_int, [vp]),
             "hdr_graph_end": (C.c_int, [vp]),
             "hdr_graph_launch": (C.c_int, [vp, i32]),

@@ -56,6 +56,11 @@ def path_trace_batch(contexts, cameras, frame_indices, **settings) -> None:
     abi.check(abi.lib().hdr_path_trace_batch(ctxs, n, cams, frames, params))
 
 
+def trim_frame_memory(device: int = 0, keep_bytes: int = 0) -> None:
+    """Returns the frame-buffer pool's unused memory beyond keep_bytes to the device."""
+    abi.check(abi.lib().hdr_trim_frame_memory(int(device), int(keep_bytes)))
+
+
 def path_settings(max_depth=32, enable_subsurface=True, max_reflection_bounces=8, max_refraction_bounces=8,
                   render_ibl_background=True, roulette_aggressiveness=1.0) -> abi.PathSettings:
     """PathTracePassSettings (integrators/path_integrator.h:12-19) + maxDepth, with the reference defaults."""

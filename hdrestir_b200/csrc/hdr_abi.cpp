@@ -102,16 +102,28 @@ struct SceneStore {
     std::mutex batch_mu;
     std::map<std::string, std::pair<void *, size_t>> batch_bufs;
     cudaEvent_t batch_done = nullptr;
+    // hdr_path_trace_batch's path planes, queues and job table likewise ("pt_*" in batch_bufs,
+    // batches ordered by pt_done); the job table goes up from one of two pinned host buffers,
+    // each reused once its last copy (pt_copied) has run
+    cudaEvent_t pt_done = nullptr;
+    void *pt_table_host[2] = {nullptr, nullptr};
+    size_t pt_table_cap[2] = {0, 0};
+    cudaEvent_t pt_copied[2] = {nullptr, nullptr};
+    int pt_slot = 0;
     ~SceneStore() {
         if (ptrs.empty() && batch_bufs.empty()) return;
         int prev = 0;
         cudaGetDevice(&prev);
         cudaSetDevice(device);
-        if (batch_done) {
-            cudaEventSynchronize(batch_done);
-            cudaEventDestroy(batch_done);
-        }
-        for (auto &kv : batch_bufs) cudaFree(kv.second.first);
+        for (cudaEvent_t ev : {batch_done, pt_done, pt_copied[0], pt_copied[1]})
+            if (ev) {
+                cudaEventSynchronize(ev);
+                cudaEventDestroy(ev);
+            }
+        for (void *h : pt_table_host)
+            if (h) cudaFreeHost(h);
+        // pool memory (stream-ordered); every batch that used it has finished (events above)
+        for (auto &kv : batch_bufs) cudaFreeAsync(kv.second.first, nullptr);
         for (void *p : ptrs) cudaFree(p);
         cudaSetDevice(prev);
     }
@@ -212,6 +224,58 @@ void dev_free(hdr_ctx *c, DevBuf &b) {
     b = DevBuf{};
 }
 
+// Frame buffers and batch buffers come from one stream-ordered memory pool per
+// device (cudaMallocFromPoolAsync / cudaFreeAsync): allocating or freeing one
+// orders itself on a stream and never synchronises the device, which cudaMalloc
+// and cudaFree may (a server creating and retiring job contexts would otherwise
+// stall every job in flight). Freed memory stays mapped in the pool for the next
+// allocations (no release threshold): giving physical memory back at a
+// synchronisation point waits for the device, which stalled a server's steps for
+// up to 0.7 s. hdr_trim_frame_memory returns it; the pools live until the process
+// exits.
+cudaMemPool_t frame_pool(int device) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[device] = p;
+    return p;
+}
+
+// A frame buffer of ctx c, allocated and freed in order on the ctx stream (another
+// stream that uses it is ordered after the ctx stream's work and before its later work).
+hdr_status frame_alloc(hdr_ctx *c, DevBuf &b, size_t bytes) {
+    if (c->budget && c->allocated + bytes > c->budget)
+        return fail(HDR_ENOMEM, "allocation of %zu bytes exceeds the HBM budget (%zu of %zu in use)", bytes,
+                    c->allocated, c->budget);
+    void *p = nullptr;
+    if (bytes) {
+        cudaMemPool_t pool = frame_pool(c->device);
+        if (!pool) return fail(HDR_ECUDA, "cannot create the frame-buffer memory pool on device %d", c->device);
+        const cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, c->stream);
+        if (e != cudaSuccess) return fail(HDR_ENOMEM, "frame buffer of %zu bytes: %s", bytes, cudaGetErrorString(e));
+    }
+    b.ptr = p;
+    b.bytes = bytes;
+    c->allocated += bytes;
+    return HDR_OK;
+}
+
+void frame_free(hdr_ctx *c, DevBuf &b) {
+    if (b.ptr) cudaFreeAsync(b.ptr, c->stream);
+    c->allocated -= b.bytes;
+    b = DevBuf{};
+}
+
 // FrameBuffersMap::Add / AddOrGetPersistent: create (zeroed) or resize keeping
 // the prefix; a same-size request returns the existing buffer untouched.
 hdr_status ensure_buffer(hdr_ctx *c, const char *name, size_t bytes, void **out) {
@@ -224,14 +288,14 @@ hdr_status ensure_buffer(hdr_ctx *c, const char *name, size_t bytes, void **out)
         return fail(HDR_EINVAL, "buffer '%s' does not exist at %zu bytes: a recorded pass cannot allocate (run the "
                     "same passes once outside hdr_graph_begin / hdr_graph_end first)", name, bytes);
     DevBuf nb;
-    hdr_status st = dev_alloc(c, nb, bytes);
+    hdr_status st = frame_alloc(c, nb, bytes);
     if (st != HDR_OK) return st;
     if (bytes) HDR_CUDA(cudaMemsetAsync(nb.ptr, 0, bytes, c->stream));
     if (it != c->buffers.end()) {
         const size_t keep = std::min(bytes, it->second.bytes);
         if (keep) HDR_CUDA(cudaMemcpyAsync(nb.ptr, it->second.ptr, keep, cudaMemcpyDeviceToDevice, c->stream));
         HDR_CUDA(cudaStreamSynchronize(c->stream));
-        dev_free(c, it->second);
+        frame_free(c, it->second);
         it->second = nb;
     } else {
         c->buffers[name] = nb;
@@ -253,11 +317,11 @@ hdr_status ensure_scratch(hdr_ctx *c, const char *name, size_t bytes, void **out
                     "same passes once outside hdr_graph_begin / hdr_graph_end first)", name, bytes);
     if (it != c->buffers.end()) {
         HDR_CUDA(cudaStreamSynchronize(c->stream));
-        dev_free(c, it->second);
+        frame_free(c, it->second);
         c->buffers.erase(it);
     }
     DevBuf nb;
-    hdr_status st = dev_alloc(c, nb, std::max<size_t>(bytes, 16));
+    hdr_status st = frame_alloc(c, nb, std::max<size_t>(bytes, 16));
     if (st != HDR_OK) return st;
     c->buffers[name] = nb;
     *out = nb.ptr;
@@ -265,24 +329,29 @@ hdr_status ensure_scratch(hdr_ctx *c, const char *name, size_t bytes, void **out
 }
 
 // A batch buffer of the scene store (batch_mu held): kept while large enough; grown
-// with a quarter of headroom once every batch that used the old one has finished.
-// Its bytes count toward the scene's memory.
-hdr_status ensure_batch_scratch(SceneStore *store, const char *name, size_t bytes, void **out) {
+// with a quarter of headroom. The old one is freed and the new one allocated in
+// order on `stream` (the batch's lead stream), after `done` (the event every batch
+// using the buffer records): no host wait and no device synchronisation. Its bytes
+// count toward the scene's memory.
+hdr_status ensure_batch_scratch(SceneStore *store, const char *name, size_t bytes, void **out,
+                                cudaEvent_t done, cudaStream_t stream) {
     auto it = store->batch_bufs.find(name);
     if (it != store->batch_bufs.end() && it->second.second >= bytes) {
         *out = it->second.first;
         return HDR_OK;
     }
     if (it != store->batch_bufs.end()) {
-        if (store->batch_done) HDR_CUDA(cudaEventSynchronize(store->batch_done));
-        cudaFree(it->second.first);
+        if (done) HDR_CUDA(cudaStreamWaitEvent(stream, done, 0));
+        HDR_CUDA(cudaFreeAsync(it->second.first, stream));
         store->bytes -= it->second.second;
         store->batch_bufs.erase(it);
     }
     const size_t want = std::max<size_t>(16, bytes + bytes / 4);
     void *p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, want);
-    if (e != cudaSuccess) return fail(HDR_ENOMEM, "cudaMalloc(%zu) for batch queues: %s", want, cudaGetErrorString(e));
+    cudaMemPool_t pool = frame_pool(store->device);
+    if (!pool) return fail(HDR_ECUDA, "cannot create the frame-buffer memory pool on device %d", store->device);
+    const cudaError_t e = cudaMallocFromPoolAsync(&p, want, pool, stream);
+    if (e != cudaSuccess) return fail(HDR_ENOMEM, "batch buffer of %zu bytes: %s", want, cudaGetErrorString(e));
     store->batch_bufs[name] = {p, want};
     store->bytes += want;
     *out = p;
@@ -447,8 +516,10 @@ hdr_status hdr_ctx_create(hdr_ctx **out, const hdr_ctx_desc *desc) {
     c->flags = desc ? desc->flags : 0;
     c->budget = desc ? desc->hbm_budget_bytes : 0;
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&c->d_err, 64);
-    if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, 64);
+    cudaMemPool_t pool = e == cudaSuccess ? frame_pool(dev) : nullptr;
+    if (e == cudaSuccess && !pool) e = cudaErrorMemoryAllocation;
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&c->d_err, 64, pool, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_err, 0, 64, c->stream);
     for (int k = 0; k < kTimeSlots && e == cudaSuccess; ++k) {
         e = cudaEventCreate(&c->ev_start[k]);
         if (e == cudaSuccess) e = cudaEventCreate(&c->ev_stop[k]);
@@ -487,8 +558,8 @@ void hdr_ctx_destroy(hdr_ctx *c) {
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);  // a read-back may still use a buffer
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     c->scene_store.reset();
-    for (auto &kv : c->buffers) dev_free(c, kv.second);
-    if (c->d_err) cudaFree(c->d_err);
+    for (auto &kv : c->buffers) frame_free(c, kv.second);
+    if (c->d_err) cudaFreeAsync(c->d_err, c->stream);
     for (int k = 0; k < kTimeSlots; ++k) {
         if (c->ev_start[k]) cudaEventDestroy(c->ev_start[k]);
         if (c->ev_stop[k]) cudaEventDestroy(c->ev_stop[k]);
@@ -1134,10 +1205,14 @@ static hdr_status ris_path_trace_pass(hdr_ctx *c, const hdr_camera *cam, int32_t
     return end_pass(c, 1);
 }
 
+}  // extern "C"
+
 namespace {
 // The per-path planes, queues and hit slots of the wavefront PathTracePass for
-// `count` paths (per-frame scratch on ctx c).
-hdr_status pt_buffers(hdr_ctx *c, size_t count, hdr::PtBuffers &B) {
+// `count` paths; alloc(name, bytes, &ptr) provides each (per-frame scratch of a
+// ctx, or a scene store's batch buffers).
+template <class Alloc>
+hdr_status pt_buffers_from(Alloc alloc, size_t count, hdr::PtBuffers &B) {
     B = hdr::PtBuffers{};
     B.pixels = count;
     struct Plane {
@@ -1156,7 +1231,7 @@ hdr_status pt_buffers(hdr_ctx *c, size_t count, hdr::PtBuffers &B) {
         {"__pt_occ", count, &occ}};
     hdr_status st;
     for (const Plane &pl : planes)
-        if ((st = ensure_scratch(c, pl.name, pl.bytes, pl.dst)) != HDR_OK) return st;
+        if ((st = alloc(pl.name, pl.bytes, pl.dst)) != HDR_OK) return st;
     B.rng = (uint4 *)rng;
     B.tp = (float4 *)tp;
     B.total = (float4 *)total;
@@ -1178,7 +1253,13 @@ hdr_status pt_buffers(hdr_ctx *c, size_t count, hdr::PtBuffers &B) {
     B.occ = (unsigned char *)occ;
     return HDR_OK;
 }
+hdr_status pt_buffers(hdr_ctx *c, size_t count, hdr::PtBuffers &B) {
+    return pt_buffers_from([c](const char *name, size_t bytes, void **p) { return ensure_scratch(c, name, bytes, p); },
+                           count, B);
+}
 }  // namespace
+
+extern "C" {
 
 hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src) {
     if (!dst || !src || dst == src) return fail(HDR_EINVAL, "need two distinct contexts");
@@ -1434,17 +1515,18 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
     std::lock_guard<std::mutex> batch_lock(store->batch_mu);
     hdr::WaveBuffers all{};
     void *q;
-    if ((st = ensure_batch_scratch(store, "q_closest", (size_t)total_c * 32, &q)) != HDR_OK) return st;
+    cudaEvent_t done = store->batch_done;
+    if ((st = ensure_batch_scratch(store, "q_closest", (size_t)total_c * 32, &q, done, lead->stream)) != HDR_OK) return st;
     all.q_closest = (float4 *)q;
-    if ((st = ensure_batch_scratch(store, "q_shadow", (size_t)total_s * 32, &q)) != HDR_OK) return st;
+    if ((st = ensure_batch_scratch(store, "q_shadow", (size_t)total_s * 32, &q, done, lead->stream)) != HDR_OK) return st;
     all.q_shadow = (float4 *)q;
-    if ((st = ensure_batch_scratch(store, "counts", 32, &q)) != HDR_OK) return st;
+    if ((st = ensure_batch_scratch(store, "counts", 32, &q, done, lead->stream)) != HDR_OK) return st;
     all.counts = (int *)q;
-    if ((st = ensure_batch_scratch(store, "hits", (size_t)total_c * 16, &q)) != HDR_OK) return st;
+    if ((st = ensure_batch_scratch(store, "hits", (size_t)total_c * 16, &q, done, lead->stream)) != HDR_OK) return st;
     all.hits = (float4 *)q;
-    if ((st = ensure_batch_scratch(store, "hit_v", (size_t)total_c * 4, &q)) != HDR_OK) return st;
+    if ((st = ensure_batch_scratch(store, "hit_v", (size_t)total_c * 4, &q, done, lead->stream)) != HDR_OK) return st;
     all.hit_v = (float *)q;
-    if ((st = ensure_batch_scratch(store, "occ", (size_t)total_s, &q)) != HDR_OK) return st;
+    if ((st = ensure_batch_scratch(store, "occ", (size_t)total_s, &q, done, lead->stream)) != HDR_OK) return st;
     all.occ = (unsigned char *)q;
     if (!store->batch_done) HDR_CUDA(cudaEventCreateWithFlags(&store->batch_done, cudaEventDisableTiming));
     // the previous batch on this scene (another lead's stream) has finished with the queues
@@ -1613,19 +1695,45 @@ hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camer
         wave = wave && std::memcmp(&settings[i], &settings[0], sizeof(hdr_path_settings)) == 0;
     }
     if (paths >= (1ll << 31)) return fail(HDR_EINVAL, "batch of %lld paths is too large", paths);
+    // the path planes, queues and job table belong to the resident scene, as the RIS batch's queues
+    // do: batches of changing images and leads (a server's steps) allocate nothing once large enough
+    SceneStore *store = lead->scene_store.get();
+    std::lock_guard<std::mutex> batch_lock(store->batch_mu);
+    if (!store->pt_done) HDR_CUDA(cudaEventCreateWithFlags(&store->pt_done, cudaEventDisableTiming));
+    for (cudaEvent_t &ev : store->pt_copied)
+        if (!ev) HDR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    auto alloc = [store, lead](const char *name, size_t bytes, void **p) {
+        return ensure_batch_scratch(store, (std::string("pt") + name).c_str(), bytes, p, store->pt_done,
+                                    lead->stream);
+    };
     hdr::PtBuffers B{};
-    if (wave && (st = pt_buffers(lead, (size_t)paths, B)) != HDR_OK) return st;
+    if (wave && (st = pt_buffers_from(alloc, (size_t)paths, B)) != HDR_OK) return st;
+    const size_t table_bytes = jobs.size() * sizeof(hdr::PtJobD);
     void *table = nullptr;
-    if ((st = ensure_scratch(lead, "__batch_pt_jobs", jobs.size() * sizeof(hdr::PtJobD), &table)) != HDR_OK)
-        return st;
+    if ((st = alloc("__jobs", table_bytes, &table)) != HDR_OK) return st;
+    // the table goes up from pinned memory: one of two staging buffers, reused once the copy that
+    // last read it has run, so the host never waits for the batch itself
+    const int slot = store->pt_slot;
+    store->pt_slot ^= 1;
+    HDR_CUDA(cudaEventSynchronize(store->pt_copied[slot]));
+    if (store->pt_table_cap[slot] < table_bytes) {
+        if (store->pt_table_host[slot]) HDR_CUDA(cudaFreeHost(store->pt_table_host[slot]));
+        store->pt_table_host[slot] = nullptr;
+        store->pt_table_cap[slot] = 0;
+        HDR_CUDA(cudaHostAlloc(&store->pt_table_host[slot], table_bytes, cudaHostAllocDefault));
+        store->pt_table_cap[slot] = table_bytes;
+    }
+    std::memcpy(store->pt_table_host[slot], jobs.data(), table_bytes);
+    // the previous batch on this scene (another lead's stream) has finished with the buffers, and
+    // every image's earlier work (its raycast, on its own stream) is done
+    HDR_CUDA(cudaStreamWaitEvent(lead->stream, store->pt_done, 0));
     for (int32_t i = 1; i < n; ++i) {
         HDR_CUDA(cudaEventRecord(ctxs[i]->sync_ev, ctxs[i]->stream));
         HDR_CUDA(cudaStreamWaitEvent(lead->stream, ctxs[i]->sync_ev, 0));
     }
     if ((st = begin_pass(lead, 1)) != HDR_OK) return st;
-    // the table is read by the launch below; the host vector stays alive until the copy is done
-    HDR_CUDA(cudaMemcpyAsync(table, jobs.data(), jobs.size() * sizeof(hdr::PtJobD), cudaMemcpyHostToDevice,
-                             lead->stream));
+    HDR_CUDA(cudaMemcpyAsync(table, store->pt_table_host[slot], table_bytes, cudaMemcpyHostToDevice, lead->stream));
+    HDR_CUDA(cudaEventRecord(store->pt_copied[slot], lead->stream));
     if (wave) {
         const int nl = hdr::launch_path_trace_wavefront(lead->scene, jobs.data(), n, (const hdr::PtJobD *)table,
                                                         (int)tiles, B, lead->tune, lead->d_err, lead->stream);
@@ -1636,8 +1744,8 @@ hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camer
     }
     HDR_CUDA(cudaGetLastError());
     HDR_CUDA(cudaEventRecord(lead->sync_ev, lead->stream));
+    HDR_CUDA(cudaEventRecord(store->pt_done, lead->stream));
     for (int32_t i = 1; i < n; ++i) HDR_CUDA(cudaStreamWaitEvent(ctxs[i]->stream, lead->sync_ev, 0));
-    HDR_CUDA(cudaStreamSynchronize(lead->stream));  // the pageable table copy must finish before `jobs` goes
     lead->launches += 1;
     return end_pass(lead, 1);
 }
@@ -1677,7 +1785,7 @@ hdr_status hdr_clear_persistent(hdr_ctx *c) {
     HDR_CUDA(cudaSetDevice(c->device));
     for (const char *name : {"__accum_color", "__ris_reservoir", "__ris_reservoir_prev", "__prev_pos_depth"}) {
         auto it = c->buffers.find(name);
-        if (it != c->buffers.end()) dev_free(c, it->second), c->buffers.erase(it);
+        if (it != c->buffers.end()) frame_free(c, it->second), c->buffers.erase(it);
     }
     c->reproj_valid = false;
     return HDR_OK;
@@ -1771,16 +1879,15 @@ hdr_status hdr_upscale(hdr_ctx *c, const char *name, int32_t components, int32_t
         return fail(HDR_EINVAL, "buffer '%s' holds %zu bytes, %d x %d x %d floats expected", name, it->second.bytes,
                     src_w, src_h, components);
     DevBuf nb;
-    hdr_status st = dev_alloc(c, nb, (size_t)dst_w * dst_h * components * sizeof(float));
+    hdr_status st = frame_alloc(c, nb, (size_t)dst_w * dst_h * components * sizeof(float));
     if (st != HDR_OK) return st;
     if (hdr::launch_upscale((const float *)it->second.ptr, (float *)nb.ptr, components, src_w, src_h, dst_w, dst_h,
                             c->tune.sm_count, c->stream) < 0) {
-        dev_free(c, nb);
+        frame_free(c, nb);
         return fail(HDR_ECUDA, "upscale launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     }
     c->launches += 1;
-    HDR_CUDA(cudaStreamSynchronize(c->stream));  // the source is freed next
-    dev_free(c, it->second);
+    frame_free(c, it->second);  // in stream order, after the upscale that reads it
     it->second = nb;
     return HDR_OK;
 }
@@ -2127,6 +2234,20 @@ hdr_status hdr_region_elapsed(hdr_ctx *c, int32_t slot, float *ms) {
     HDR_NOT_RECORDING(c, "hdr_region_elapsed");
     HDR_CUDA(cudaEventSynchronize(c->region_ev[slot][1]));
     HDR_CUDA(cudaEventElapsedTime(ms, c->region_ev[slot][0], c->region_ev[slot][1]));
+    return HDR_OK;
+}
+
+hdr_status hdr_trim_frame_memory(int32_t device, size_t keep_bytes) {
+    int ndev = 0;
+    HDR_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(HDR_EINVAL, "device %d not present (%d devices)", device, ndev);
+    int prev = 0;
+    HDR_CUDA(cudaGetDevice(&prev));
+    HDR_CUDA(cudaSetDevice(device));
+    cudaMemPool_t pool = frame_pool(device);
+    const cudaError_t e = pool ? cudaMemPoolTrimTo(pool, keep_bytes) : cudaErrorMemoryAllocation;
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return fail(HDR_ECUDA, "trimming the frame-buffer pool: %s", cudaGetErrorString(e));
     return HDR_OK;
 }
 

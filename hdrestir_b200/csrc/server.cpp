@@ -7,8 +7,10 @@
 //    buffers fits the HBM budget;
 //  * each hdr_server_step advances every admitted job by one frame:
 //    raycasts on the jobs' own streams, one batched RIS launch per scene
-//    (hdr_ris_path_trace_batch: all images' rays traced together),
-//    path-traced jobs on their own streams side by side, then accumulation.
+//    (hdr_ris_path_trace_batch: all images' rays traced together), one
+//    batched wavefront PathTracePass per scene and path settings
+//    (hdr_path_trace_batch: every image's live paths in each launch), then
+//    accumulation.
 //    Jobs that arrive while others are running join at the next step
 //    (continuous batching).
 // The context of a job whose result was taken is kept (persistent buffers
@@ -194,6 +196,7 @@ void hdr_server_destroy(hdr_server *sv) {
     for (auto &p : sv->pool) hdr_ctx_destroy(p.ctx);
     sv->pool.clear();
     for (hdr_ctx *c : sv->scenes) hdr_ctx_destroy(c);
+    hdr_trim_frame_memory(sv->device, 0);  // the jobs' frame buffers go back to the device
     delete sv;
 }
 
@@ -259,16 +262,44 @@ hdr_status hdr_server_step(hdr_server *sv, int32_t *jobs_finished) {
     // 1. primary rays, each job on its own stream
     for (Job *j : run)
         if (hdr_raycast(j->ctx, &j->d.camera, j->frames_done, 0) != HDR_OK) fail_job(sv, *j);
-    // 2. integration: RIS jobs of one scene in batched launches, path tracing side by side
+    // 2. integration: RIS jobs of one scene in batched launches; path-traced jobs of one scene
+    //    and one set of path settings in batched wavefront launches
     std::map<int32_t, std::vector<Job *>> ris_by_scene;
+    std::vector<std::vector<Job *>> pt_groups;
     for (Job *j : run) {
         if (j->state != HDR_JOB_RUNNING) continue;
         if (j->d.pipeline == HDR_JOB_RIS && !serial) {
             ris_by_scene[j->d.scene].push_back(j);
         } else if (j->d.pipeline == HDR_JOB_RIS) {
             if (hdr_ris_path_trace(j->ctx, &j->d.camera, j->frames_done, &j->d.ris) != HDR_OK) fail_job(sv, *j);
+        } else if (!serial) {
+            auto same = [j](const std::vector<Job *> &g) {
+                return g[0]->d.scene == j->d.scene &&
+                       std::memcmp(&g[0]->d.ris.path, &j->d.ris.path, sizeof(hdr_path_settings)) == 0;
+            };
+            auto g = std::find_if(pt_groups.begin(), pt_groups.end(), same);
+            if (g == pt_groups.end()) pt_groups.push_back({j});
+            else g->push_back(j);
         } else if (hdr_path_trace(j->ctx, &j->d.camera, j->frames_done, &j->d.ris.path) != HDR_OK) {
             fail_job(sv, *j);
+        }
+    }
+    for (const std::vector<Job *> &js : pt_groups) {
+        for (size_t k0 = 0; k0 < js.size(); k0 += (size_t)sv->max_batch) {
+            const size_t n = std::min(js.size() - k0, (size_t)sv->max_batch);
+            std::vector<hdr_ctx *> ctxs(n);
+            std::vector<hdr_camera> cams(n);
+            std::vector<int32_t> frames(n);
+            std::vector<hdr_path_settings> settings(n);
+            for (size_t k = 0; k < n; ++k) {
+                const Job &j = *js[k0 + k];
+                ctxs[k] = j.ctx;
+                cams[k] = j.d.camera;
+                frames[k] = j.frames_done;
+                settings[k] = j.d.ris.path;
+            }
+            if (hdr_path_trace_batch(ctxs.data(), (int32_t)n, cams.data(), frames.data(), settings.data()) != HDR_OK)
+                for (size_t k = 0; k < n; ++k) fail_job(sv, *js[k0 + k]);
         }
     }
     for (auto &kv : ris_by_scene) {

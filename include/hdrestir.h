@@ -408,7 +408,12 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
 /* Batched PathTracePass, no reference counterpart: n images (one ctx each,
  * sharing one resident scene, each after its own hdr_raycast) in one launch
  * over all their tiles. Each image's "Color" is that of hdr_path_trace on its
- * ctx. Images that do not share the scene are rendered one after another. */
+ * ctx. Images that do not share the scene are rendered one after another.
+ * With one set of path settings for all images and an opaque scene, every
+ * wavefront round traces all images' live paths together. The path planes,
+ * ray queues and job table belong to the resident scene, like the RIS batch's
+ * queues (grow-only, outside the contexts' HBM budgets; batches on one scene
+ * ordered by an event); the call does not wait for the device. */
 hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camera *cams,
                                 const int32_t *frame_indices, const hdr_path_settings *settings);
 
@@ -627,6 +632,13 @@ hdr_status hdr_region_elapsed(hdr_ctx *ctx, int32_t slot, float *ms);
 
 /* Number of this library's kernels launched on the ctx so far. */
 hdr_status hdr_launch_count(hdr_ctx *ctx, uint64_t *count);
+
+/* No reference counterpart. Frame buffers (and the batch calls' queues) come from
+ * one stream-ordered memory pool per device, so allocating and freeing them never
+ * synchronises the device; freed memory stays in the pool for later frames. This
+ * returns the pool's unused memory beyond keep_bytes to the device (it waits for
+ * work that frees memory; call it between jobs, not per frame). */
+hdr_status hdr_trim_frame_memory(int32_t device, size_t keep_bytes);
 
 /* ---------------------------------------------------------------------------
  * A frame's pass chain as one CUDA graph. No reference counterpart: the
