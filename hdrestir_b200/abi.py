@@ -67,7 +67,8 @@ class SceneDesc(C.Structure):
     _fields_ = [("meshes", C.POINTER(MeshDesc)), ("num_meshes", _i),
                 ("instances", C.POINTER(InstanceDesc)), ("num_instances", _i),
                 ("materials", C.POINTER(MaterialDesc)), ("num_materials", _i),
-                ("lights", C.POINTER(LightDesc)), ("num_lights", _i)]
+                ("lights", C.POINTER(LightDesc)), ("num_lights", _i),
+                ("enable_physical_sky", _i), ("physical_sky_time", _f)]
 
 
 class CameraDesc(C.Structure):

@@ -283,6 +283,18 @@ def translucent_variant(width=64, height=48):
     return sc, cam
 
 
+def sky_variant(cfg: int, width: int, height: int, hour: float = 15.5, **kw):
+    """A config-1 or config-2 scene under the physical sky (SceneBuildRenderStateConfig::
+    EnablePhysicalSky, its sun at `hour`): no configuration of the benchmark uses the sky,
+    so this family exercises the environment outside the light sampler (the RIS pass's sky
+    technique, the path tracer's separate sun sample, sky radiance on misses)."""
+    sc, cam = small_variant(cfg, width, height, **kw)
+    sc.physical_sky_time = float(hour)
+    if cfg == 2:  # a camera that sees the horizon, so misses show the sky
+        cam = make_camera((22.0 * np.sin(0.4), 3.0, 22.0 * np.cos(0.4)), (0.0, 3.0, 0.0), width, height, fov=70.0)
+    return sc, cam
+
+
 def textured_variant(width=64, height=48, seed=7):
     """The config-2 family with UVs and PreviewSurface textures (diffuse, metallic, roughness,
     tangent-space normal map; preview_surface.cpp:68-95): the terrain's UVs wrap several

@@ -191,7 +191,8 @@ __device__ inline MisNeePart mis_nee_part(const DeviceScene &s, const Surface &s
     MisNeePart r;
     r.cast = false;
     r.add = spec(0.0f);
-    // the environment, when present, is a scene light and so part of the sampler
+    // a dome environment is a scene light and so part of the sampler; the physical
+    // sky is not, and gets its own technique (mis_sky_part)
     int li;
     LightSampleD ls;
     if (!propose_candidate(s, sf.hit.position, rng, li, ls)) return r;
@@ -207,12 +208,41 @@ __device__ inline MisNeePart mis_nee_part(const DeviceScene &s, const Surface &s
     const float bpdf = ggx_pdf_f(sf.g, sf.sn, wo, ls.dir);
     const V3 bval = ggx_eval_f(sf.g, sf.sn, wo, ls.dir);
     const Spec radiance = rgb_to_spectrum(bval, sc.up) * rgb_to_spectrum(ls.color, sc.up) * (n_l / p_nee);
-    const float w = (delta || !has_conn) ? 1.0f : power_heuristic2(p_nee, bpdf);
+    const bool separate_env = env_present(s) && env_select_pdf(s) <= 0.0f;
+    const float w = (delta || !has_conn) ? 1.0f
+                    : separate_env       ? power_heuristic3(p_nee, 1, 0.0f, 1, bpdf, 1)
+                                         : power_heuristic2(p_nee, bpdf);
     r.cast = true;
     r.o = sf.hit.position + sf.sn * 1e-4f;
     r.d = ls.dir;
     r.limit = ls.dist - 1e-3f;
     r.add = radiance * w;
+    return r;
+}
+
+// The separate environment technique of _integrateNEE (:153-176): the physical
+// sky's sun (its SampleLight draws nothing), with what it adds if unoccluded.
+__device__ inline MisNeePart mis_sky_part(const DeviceScene &s, const Surface &sf, const SpectralCtx &sc) {
+    MisNeePart r;
+    r.cast = false;
+    r.add = spec(0.0f);
+    LightSampleD ls;
+    if (!(env_present(s) && env_select_pdf(s) <= 0.0f) || !sky_sun_sample(s, ls)) return r;
+    const float n_l = dot(sf.sn, ls.dir);
+    if (n_l <= 0.0f) return r;
+    const float dist2 = ls.dist * ls.dist;
+    const float cos_y = smaxf(0.0f, dot(-ls.dir, ls.normal));
+    const float p_nee = pdf_to_solid_angle(ls.pdf, ls.pdf_solid_angle, dist2, smaxf(cos_y, 1e-6f));
+    if (p_nee <= 0.0f) return r;
+    const V3 wo = -sf.ray_d;
+    const V3 bval = ggx_eval_f(sf.g, sf.sn, wo, ls.dir);
+    // the sun is a delta light: MIS weight 1
+    const Spec radiance = rgb_to_spectrum(bval, sc.up) * rgb_to_spectrum(ls.color, sc.up) * (n_l / p_nee);
+    r.cast = true;
+    r.o = sf.hit.position + sf.sn * 1e-4f;
+    r.d = ls.dir;
+    r.limit = ls.dist - 1e-3f;
+    r.add = radiance;
     return r;
 }
 
@@ -230,9 +260,9 @@ __device__ inline Spec mis_conn_part(const DeviceScene &s, Spec total, bool has_
     float p_sampler = 0.0f, p_env = 0.0f;
     Spec radiance;
     if (!cn.has_hit) {
-        if (s.env_light < 0) return total;
+        if (!env_present(s)) return total;
         radiance = rgb_to_spectrum(env_radiance(s, b.dir), sc.up);
-        const float sel = light_select_pdf(s);
+        const float sel = env_select_pdf(s);
         const float epdf = env_pdf(s, b.dir);
         p_sampler = sel * epdf;
         p_env = sel <= 0.0f ? epdf : 0.0f;
@@ -266,6 +296,10 @@ __device__ inline Spec mis_direct_li(const DeviceScene &s, const Surface &sf, bo
     const MisNeePart nee = mis_nee_part(s, sf, has_conn, sc, rng);
     Spec total = spec(0.0f);
     if (nee.cast && !occluded(s, nee.o, nee.d, nee.limit, err)) total = total + nee.add;
+    if (s.sky) {  // the physical sky's sun, after the sampler's candidate
+        const MisNeePart sun = mis_sky_part(s, sf, sc);
+        if (sun.cast && !occluded(s, sun.o, sun.d, sun.limit, err)) total = total + sun.add;
+    }
     return mis_conn_part(s, total, has_conn, cn, sc);
 }
 
@@ -376,15 +410,15 @@ __device__ inline RisContrib ris_evaluate_bsdf_connection(const DeviceScene &s, 
     RisContrib r{spec(0.0f), b.integrand, 0.0f, b.pdf, false, true};
     if (b.impossible_nee || b.pdf <= 0.0f) {
         if (!cn.has_hit) {
-            if (s.env_light >= 0) r.emission = rgb_to_spectrum(env_radiance(s, b.dir), sc.up);
+            if (env_present(s)) r.emission = rgb_to_spectrum(env_radiance(s, b.dir), sc.up);
             return r;
         }
         r.emission = rgb_to_spectrum(get_closure(s, cn.hit).emission, sc.up);
         return r;
     }
     if (!cn.has_hit) {
-        if (s.env_light < 0) return r;
-        const float sel = light_select_pdf(s);
+        if (!env_present(s)) return r;
+        const float sel = env_select_pdf(s);
         const float epdf = env_pdf(s, b.dir);
         const float p_nee = sel > 0.0f ? sel * epdf : (strat.n_sky > 0 ? epdf : 0.0f);
         r.emission = rgb_to_spectrum(env_radiance(s, b.dir), sc.up);
@@ -461,8 +495,29 @@ __device__ Cand ris_candidate(const RisCtx<RP> &x, int j, MtStream &rng, unsigne
     }
     j -= x.strat.n_nee;
     if (j < x.strat.n_sky) {
-        // sky NEE needs an environment outside the light sampler; every supported
-        // environment is a scene light, so this technique never has candidates.
+        // sky NEE (:445-475): the environment outside the light sampler is the physical
+        // sky, whose SampleLight is the sun and draws nothing; every sky candidate is
+        // the same sample, so they share one shadow slot (index n_nee of the pixel's)
+        if (!kFull) return c;
+        LightSampleD ls;
+        if (!sky_sun_sample(s, ls)) return c;
+        const int li = sky_light_index(s);
+        const RisContrib nee =
+            ris_evaluate_light_sample(s, *x.rp, x.strat.n_nee, sf, li, ls, x.strat.skip_vis, sc, err);
+        const Spec contribution = nee.emission * nee.tmul;
+        const float target = spectrum_luminance(contribution, sc.cie);
+        const float mis = nee.use_mis ? power_heuristic3(nee.p_nee, x.strat.n_sky, 0.0f, x.strat.n_nee, nee.p_bsdf,
+                                                         x.strat.n_bsdf)
+                                      : 1.0f;
+        c.valid = true;
+        c.has_lc = true;
+        c.light = li;
+        c.ls = ls;
+        c.origin = 1;
+        c.tp = contribution;
+        c.ris_weight = (double)(mis * target) / ((double)nee.p_nee + 1e-9);
+        c.target = target;
+        c.vis_tested = nee.vis_tested;
         return c;
     }
     j -= x.strat.n_sky;
@@ -473,7 +528,7 @@ __device__ Cand ris_candidate(const RisCtx<RP> &x, int j, MtStream &rng, unsigne
         const Spec contribution = bc.emission * bc.tmul;
         const double target = (double)spectrum_luminance(contribution, sc.cie);
         float p_sampler = bc.p_nee, p_sky = 0.0f;
-        if (!x.conn->has_hit && (s.env_light < 0 || light_select_pdf(s) <= 0.0f)) {
+        if (!x.conn->has_hit && (!env_present(s) || env_select_pdf(s) <= 0.0f)) {
             p_sampler = 0.0f;
             p_sky = bc.p_nee;
         }
@@ -497,13 +552,13 @@ __device__ Cand ris_candidate(const RisCtx<RP> &x, int j, MtStream &rng, unsigne
     const Connection cn = sample_bounce_with_connection(*x.rp, 1 + fresh, sf, 1, 1, st, sc, rng, err);
     if (!cn.b.ok) return c;
     if (!cn.has_hit) {
-        if (s.env_light < 0) return c;
+        if (!env_present(s)) return c;
         const Spec env_tp = cn.b.integrand;
         const V3 wi = cn.b.dir;
         const V3 env_rgb = env_radiance(s, wi);
         const Spec env_em = rgb_to_spectrum(env_rgb, sc.up);
         const float p_bsdf = cn.b.pdf;
-        const float sel = light_select_pdf(s);
+        const float sel = env_select_pdf(s);
         const float epdf = env_pdf(s, wi);
         const float p_sampler = sel * epdf;
         const float p_sky = (sel <= 0.0f && x.strat.n_sky > 0) ? epdf : 0.0f;
@@ -513,7 +568,7 @@ __device__ Cand ris_candidate(const RisCtx<RP> &x, int j, MtStream &rng, unsigne
             (double)power_heuristic3(p_bsdf, x.strat.n_bsdf, p_sampler, x.strat.n_nee, p_sky, x.strat.n_sky);
         c.valid = true;
         c.has_lc = p_nee > 0.0f;
-        c.light = s.env_light;
+        c.light = env_light_index(s);
         c.ls = LightSampleD{wi, env_rgb, -wi, 1e30f, p_nee, true};
         c.origin = 2;
         c.tp = env_em * env_tp;
@@ -657,18 +712,14 @@ __device__ inline Spec ris_direct_li(const DeviceScene &s, const RP &rp, const S
                                      const Connection &cn, const SpectralCtx &sc, MtStream &rng, bool primary,
                                      const RisRun &run, const ReservoirView &rv, size_t pixel,
                                      const MtStream *gen_end_state, unsigned &err) {
-    // technique split (:239-246); every supported environment is a scene light,
-    // so the sampler covers it and there is no separate sky technique
-    const int N = run.candidate_count;
-    const int n_tech = 2;
+    // technique split (:89-99): a dome environment is a scene light, covered by the
+    // sampler; the physical sky is not and gets the sky technique
     RisCtx<RP> x;
     x.s = &s;
     x.rp = &rp;
     x.sf = &sf;
     x.sc = &sc;
-    x.strat.n_nee = smaxi(1, N / n_tech);
-    x.strat.n_sky = 0;
-    x.strat.n_bsdf = smaxi(0, N - x.strat.n_nee - x.strat.n_sky);
+    ris_technique_split(s, run.candidate_count, x.strat.n_nee, x.strat.n_sky, x.strat.n_bsdf);
     x.strat.skip_vis = run.skip_vis;
     x.has_conn = has_conn;
     x.conn = &cn;
@@ -891,7 +942,7 @@ __device__ Spec path_li(const DeviceScene &s, const RP &rp, V3 ray_o, V3 ray_d, 
         }
         has_hit = intersect(s, hit.position + ray_d * 1e-4f, ray_d, hit, err);
     }
-    if (s.env_light >= 0 && pr.render_ibl_background) return rgb_to_spectrum(env_radiance(s, ray_d), sc.up);
+    if (env_present(s) && pr.render_ibl_background) return rgb_to_spectrum(env_radiance(s, ray_d), sc.up);
     return spec(0.0f);
 }
 

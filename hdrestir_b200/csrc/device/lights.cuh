@@ -15,6 +15,7 @@
 #pragma once
 
 #include "rng.cuh"
+#include "sky.cuh"
 #include "traverse.cuh"
 
 namespace hdr {
@@ -29,9 +30,20 @@ struct LightSampleD {  // LightSample
 };
 
 __device__ __forceinline__ int light_type(const DeviceScene &s, int li) { return fbits(__ldg(&s.lights[12 * li].x)); }
+// ILight::IsDeltaLight; light index num_lights is the physical sky's sun (a delta light)
 __device__ __forceinline__ bool light_is_delta(const DeviceScene &s, int li) {
-    return fbits(__ldg(&s.lights[12 * li].y)) != 0;
+    return li >= s.num_lights || fbits(__ldg(&s.lights[12 * li].y)) != 0;
 }
+
+// ---- PhysicalSky as a light (physical_sky.cpp:161-187) ----------------------
+// SampleLight: the sun, the same sample for every point (no random numbers).
+__device__ __forceinline__ bool sky_sun_sample(const DeviceScene &s, LightSampleD &ls) {
+    if (!s.sky || s.sky_sun.w == 0.0f) return false;
+    const V3 d{s.sky_sun.x, s.sky_sun.y, s.sky_sun.z};
+    ls = LightSampleD{d, V3{s.sky_sun_color.x, s.sky_sun_color.y, s.sky_sun_color.z}, -d, 1e30f, 1.0f, true};
+    return true;
+}
+__device__ __forceinline__ int sky_light_index(const DeviceScene &s) { return s.num_lights; }
 
 // Pdf::ConvertTo(SolidAngle, dist2, cosY)
 __device__ __forceinline__ float pdf_to_solid_angle(float value, bool solid, float dist2, float cos_y) {
@@ -71,17 +83,24 @@ __device__ __forceinline__ float dome_lum_pdf(const DeviceScene &s, V3 texel) {
     return smaxf(lum / (s.dome_total_lum * (kPiF / (float)s.dome_height) * (2.0f * kPiF / (float)s.dome_width)),
                  1e-6f);
 }
+// Scene::GetEnvironment (scene.cpp:248-268): the physical sky when enabled, else
+// the first dome light, else none.
+__device__ __forceinline__ bool env_present(const DeviceScene &s) { return s.sky || s.env_light >= 0; }
+// The environment's light index in a candidate (the dome's; the sky has none)
+__device__ __forceinline__ int env_light_index(const DeviceScene &s) { return s.sky ? -1 : s.env_light; }
 // IEnvironment::Sample (miss radiance)
 __device__ __forceinline__ V3 env_radiance(const DeviceScene &s, V3 dir) {
+    if (s.sky) return sky_radiance(V3{s.sky_sun_n.x, s.sky_sun_n.y, s.sky_sun_n.z}, dir);
     if (s.env_light < 0 || s.dome_width <= 0) return v3s(0.0f);
     int x, y;
     dome_xy(s, dir, x, y);
     const float4 p = __ldg(&s.lights[12 * s.env_light + 8]);
     return cmul(dome_pixel(s, x, y), V3{p.x, p.y, p.z}) * p.w;
 }
-// IEnvironment::EvalPdf(dir)
+// IEnvironment::EvalPdf(dir): the dome's importance-sampling pdf; the sky's is 0
+// (IEnvironment's default, sceneInterface/environment.h:19-24)
 __device__ __forceinline__ float env_pdf(const DeviceScene &s, V3 dir) {
-    if (s.env_light < 0 || s.dome_width <= 0 || s.dome_total_lum <= 0.f) return 0.f;
+    if (s.sky || s.env_light < 0 || s.dome_width <= 0 || s.dome_total_lum <= 0.f) return 0.f;
     int x, y;
     dome_xy(s, dir, x, y);
     return dome_lum_pdf(s, dome_pixel(s, x, y));
@@ -216,6 +235,22 @@ __device__ __forceinline__ void skip_propose_candidate(const DeviceScene &s, MtS
 // UniformLightSampler::EvalPdf: every scene light is in the sampler's set.
 __device__ __forceinline__ float light_select_pdf(const DeviceScene &s) {
     return s.num_lights <= 0 ? 0.0f : 1.0f / (float)s.num_lights;
+}
+// UniformLightSampler::EvalPdf(*environment): the dome is a scene light, the
+// physical sky is not (so it gets a technique of its own)
+__device__ __forceinline__ float env_select_pdf(const DeviceScene &s) {
+    return (s.sky || s.env_light < 0) ? 0.0f : light_select_pdf(s);
+}
+
+// The RIS technique split (ris_direct_light_integrator.cpp:89-99): light-sampler
+// NEE, sky NEE when the environment is outside the sampler, BSDF.
+__device__ __forceinline__ void ris_technique_split(const DeviceScene &s, int n, int &n_nee, int &n_sky,
+                                                    int &n_bsdf) {
+    const bool sep = env_present(s) && env_select_pdf(s) <= 0.0f;
+    const int n_tech = sep ? 3 : 2;
+    n_nee = smaxi(1, n / n_tech);
+    n_sky = sep ? n / n_tech : 0;
+    n_bsdf = smaxi(0, n - n_nee - n_sky);
 }
 
 }  // namespace hdr

@@ -39,7 +39,13 @@ struct DeviceScene {
     int num_instances;
     int num_materials;
     int num_lights;
-    int env_light;
+    int env_light;             // the first dome light (the environment unless `sky`), -1 = none
+    // PhysicalSky (sky.cuh): the environment when `sky` is 1. Its sun is light index
+    // num_lights for reservoirs and the delta-light test, outside the light sampler.
+    int sky;
+    float4 sky_sun;            // the sun direction; w = 1 when SampleDirect gives a sample
+    float4 sky_sun_n;          // the direction normalised again, as Sample() uses it
+    float4 sky_sun_color;      // SampleDirect's colour
     int dome_width, dome_height;
     float dome_total_lum;
     int has_tlas;

@@ -21,6 +21,7 @@
 #include "../../include/hdrestir.h"
 #include "device/blas_build.h"
 #include "device/frame.cuh"
+#include "device/sky.cuh"
 #include "host/scene_build.h"
 #include "host/shadow_bvh.h"
 
@@ -628,7 +629,7 @@ bool tlas_boxes_proper(const hdr::FlatScene &f) {
 namespace {
 // Which closest-hit rays the wavefront RIS pass casts (hdr::kTrace*).
 int ris_trace_level(const hdr_ctx *c, const hdr_ris_params *p) {
-    if ((p->flags & HDR_RIS_TRACE_ALL_RAYS) || c->scene_light_geometry || c->scene.env_light >= 0)
+    if ((p->flags & HDR_RIS_TRACE_ALL_RAYS) || c->scene_light_geometry || c->scene.env_light >= 0 || c->scene.sky)
         return hdr::kTraceAllBsdfRays;
     return c->scene_emissive ? hdr::kTraceBounceRay : hdr::kTraceNoBsdfRays;
 }
@@ -811,6 +812,16 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     s.num_materials = f.num_materials;
     s.num_lights = f.num_lights;
     s.env_light = f.env_light;
+    s.sky = desc->enable_physical_sky ? 1 : 0;
+    if (s.sky) {  // PhysicalSky's sun (scene.cpp:249-254, physical_sky.cpp:161-169), with the host's libm
+        const hdr::V3 sun = hdr::sky_sun_direction(desc->physical_sky_time);
+        const hdr::V3 sun_n = hdr::normalized(sun);
+        hdr::V3 color{0.0f, 0.0f, 0.0f};
+        const bool lit = hdr::sky_sun_color(sun, color);
+        s.sky_sun = make_float4(sun.x, sun.y, sun.z, lit ? 1.0f : 0.0f);
+        s.sky_sun_n = make_float4(sun_n.x, sun_n.y, sun_n.z, 0.0f);
+        s.sky_sun_color = make_float4(color.x, color.y, color.z, 0.0f);
+    }
     s.dome_width = f.dome_width;
     s.dome_height = f.dome_height;
     s.dome_total_lum = f.dome_total_lum;
@@ -1047,8 +1058,10 @@ static hdr_status ris_path_trace_pass(hdr_ctx *c, const hdr_camera *cam, int32_t
     if (p->spatial_neighbors < 0 || p->spatial_neighbors > 64 || !(p->spatial_radius >= 0.0f))
         return fail(HDR_EINVAL, "spatial_neighbors %d / spatial_radius out of range ([0, 64], >= 0)",
                     p->spatial_neighbors);
-    // wavefront form: direct light only (no later bounces) and no stochastic opacity
-    const bool wave = p->path.max_depth == 1 && c->scene_opaque && !(p->flags & HDR_RIS_ONE_KERNEL);
+    // wavefront form: direct light only (no later bounces), no stochastic opacity, and no
+    // physical sky (its sun technique is served by the one-kernel form only)
+    const bool wave =
+        p->path.max_depth == 1 && c->scene_opaque && !c->scene.sky && !(p->flags & HDR_RIS_ONE_KERNEL);
     const bool spatial = p->spatial_neighbors > 0 && p->use_reservoir;
     if (spatial && !wave)
         return fail(HDR_EINVAL, "spatial reuse runs in the wavefront form only (max_depth 1, opaque scene)");
@@ -1473,7 +1486,7 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
         const hdr_ris_params *p = &params[i];
         together = p->spatial_neighbors == 0 && !(p->flags & HDR_RIS_REPROJECT) && c->device == ctxs[0]->device && c->has_scene && c->scene_store &&
                    c->scene_store == ctxs[0]->scene_store && c->scene.wide == ctxs[0]->scene.wide &&
-                   p->path.max_depth == 1 && c->scene_opaque && !(p->flags & HDR_RIS_ONE_KERNEL);
+                   p->path.max_depth == 1 && c->scene_opaque && !c->scene.sky && !(p->flags & HDR_RIS_ONE_KERNEL);
     }
     std::vector<hdr_ctx *> order(ctxs, ctxs + n);
     std::sort(order.begin(), order.end());
@@ -1600,7 +1613,9 @@ static hdr_status path_trace_pass(hdr_ctx *c, const hdr_camera *cam, int32_t fra
     d.roulette = p->roulette_aggressiveness;
     hdr::CameraD cd = make_camera(cam);
     if ((st = record_frame_index(c, frame_index, &cd)) != HDR_OK) return st;
-    if (c->scene_opaque && !(c->flags & HDR_CTX_PT_ONE_KERNEL)) {
+    // wavefront form: opaque scenes without the physical sky (whose sun needs a second
+    // shadow ray per vertex, cast by the one-thread form)
+    if (c->scene_opaque && !c->scene.sky && !(c->flags & HDR_CTX_PT_ONE_KERNEL)) {
         hdr::PtBuffers B{};
         if ((st = pt_buffers(c, count, B)) != HDR_OK) return st;
         if ((st = begin_pass(c, 1)) != HDR_OK) return st;
@@ -1686,7 +1701,7 @@ hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camer
     }
     if (tiles >= (1ll << 31)) return fail(HDR_EINVAL, "batch of %lld tiles is too large", tiles);
     // the wavefront form needs an opaque scene and one set of path settings for all images
-    bool wave = lead->scene_opaque && !(lead->flags & HDR_CTX_PT_ONE_KERNEL);
+    bool wave = lead->scene_opaque && !lead->scene.sky && !(lead->flags & HDR_CTX_PT_ONE_KERNEL);
     long long paths = 0;
     for (int32_t i = 0; i < n; ++i) {
         hdr::PtJobD &j = jobs[(size_t)i];

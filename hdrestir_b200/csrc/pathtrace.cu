@@ -146,8 +146,8 @@ __global__ void __launch_bounds__(256) pt_start_kernel(DeviceScene s, PtJobD one
     const bool has = load_gbuffer_hit(s, job.gb, li, h);
     B.outer[i] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
     if (!has) {  // PathIntegrator::Li without a hit: the background
-        const Spec L = (s.env_light >= 0 && pr.render_ibl_background) ? rgb_to_spectrum(env_radiance(s, ray.d), sc.up)
-                                                                      : spec(0.0f);
+        const Spec L = (env_present(s) && pr.render_ibl_background) ? rgb_to_spectrum(env_radiance(s, ray.d), sc.up)
+                                                                    : spec(0.0f);
         finish_path(job, B, i, L, sc);
         return;
     }

@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, Camera
     const size_t i = ps.i;
     if (!ps.has_hit) {  // PathIntegrator::Li without a hit: background only, no reservoir access
         V3 rgb = v3s(0.0f);
-        if (s.env_light >= 0 && pr.render_ibl_background)
+        if (env_present(s) && pr.render_ibl_background)
             rgb = spectrum_to_rgb(rgb_to_spectrum(env_radiance(s, ps.ray.d), ps.sc.up), ps.sc.cie);
         if (cam.p.has_params && cam.p.enable_exposure) rgb = rgb * cam.p.exposure_mult;
         color[i] = make_float4(rgb.x, rgb.y, rgb.z, 1.0f);

@@ -93,6 +93,7 @@ class SceneHandoff {
     // descriptor of the same state is built and uploaded to `ctx`.
     void BuildRenderState(const SceneBuildRenderStateConfig &config, const IRenderJob &job, hdr_ctx *ctx) {
         if (_forward) _forward->BuildRenderState(config, job);
+        _config = config;
         Upload(ctx);
     }
     void Upload(hdr_ctx *ctx) {
@@ -178,6 +179,9 @@ class SceneHandoff {
         s.desc.num_materials = (int32_t)s.materials.size();
         s.desc.lights = s.lights.data();
         s.desc.num_lights = (int32_t)s.lights.size();
+        // SceneBuildRenderStateConfig (scene.cpp:248-268): the physical sky as the environment
+        s.desc.enable_physical_sky = _config.EnablePhysicalSky ? 1 : 0;
+        s.desc.physical_sky_time = _config.PhysicalSkyTime;
         return s.desc;
     }
 
@@ -304,6 +308,7 @@ class SceneHandoff {
     }
 
     Scene *_forward;
+    SceneBuildRenderStateConfig _config{};  // of the last BuildRenderState
     TextureLoader _loader;
     std::map<SdfPath, IMesh *> _meshes;
     std::map<SdfPath, IInstancer *> _instancers;

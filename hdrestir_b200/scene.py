@@ -97,6 +97,9 @@ class Scene:
     materials: list = field(default_factory=list)
     lights: list = field(default_factory=list)
     name: str = "scene"
+    # SceneBuildRenderStateConfig: the physical sky as the environment, its sun at this hour
+    # (12 = noon); None = off
+    physical_sky_time: float | None = None
 
     @property
     def num_triangles(self) -> int:
@@ -174,7 +177,8 @@ class Scene:
                 d.texture = C.cast(None, C.POINTER(C.c_float))
                 d.tex_width = d.tex_height = 0
         desc = abi.SceneDesc(meshes, len(self.meshes), inst, len(self.instances), mats, len(self.materials),
-                             lights, len(self.lights))
+                             lights, len(self.lights), int(self.physical_sky_time is not None),
+                             float(self.physical_sky_time if self.physical_sky_time is not None else 12.0))
         desc._keep = (keep, meshes, inst, mats, lights)
         return desc
 

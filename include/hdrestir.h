@@ -186,6 +186,14 @@ typedef struct hdr_scene_desc {
     int32_t num_materials;
     const hdr_light_desc *lights;
     int32_t num_lights;
+    /* SceneBuildRenderStateConfig (sceneInterface/scene_interface.h:30-34): with
+     * enable_physical_sky the environment is PhysicalSky (scene/physical_sky.cpp),
+     * its sun set from physical_sky_time (hours, 12 = noon; scene.cpp:248-256),
+     * instead of the first dome light. The sky is not one of the scene's lights: the
+     * RIS pass then splits its candidates over three techniques and the path tracer
+     * adds a sun sample per vertex. Zero-initialised descriptors leave it off. */
+    int32_t enable_physical_sky;
+    float physical_sky_time;
 } hdr_scene_desc;
 
 /* ---------------------------------------------------------------------------

@@ -80,6 +80,8 @@ def lib() -> C.CDLL:
         L.orc_reservoir_known_answer.restype = C.c_float
         L.orc_reservoir_known_answer.argtypes = [C.c_float, C.c_float, C.c_int]
         L.orc_trace_rays.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp]
+        L.orc_scene_sky.restype = C.c_int
+        L.orc_scene_sky.argtypes = [vp, vp, C.c_int, vp, vp]
         _lib = L
     return _lib
 
@@ -121,6 +123,17 @@ class Oracle:
         if self.accum is not None:
             self.accum[:] = 0
             self.res[:] = np.zeros(1, RESERVOIR_DTYPE)
+
+    def sky(self, dirs):
+        """The physical sky along each direction (n x 3 float32) and its sun
+        (direction + colour, or None)."""
+        d = np.ascontiguousarray(dirs, np.float32)
+        out = np.zeros_like(d)
+        sun = np.zeros(6, np.float32)
+        got = self._lib.orc_scene_sky(self._s, _p(d), len(d), _p(out), _p(sun))
+        if got < 0:
+            raise RuntimeError("the scene has no physical sky")
+        return out, (sun if got else None)
 
     def raycast(self, cam, frame=0) -> np.ndarray:
         n = cam.width * cam.height

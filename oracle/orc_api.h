@@ -65,6 +65,7 @@ void orc_rng_floats(const uint32_t *seeds, int n, int count, float *out);
 float orc_reservoir_known_answer(float weight, float phat, int candidates_per_frame);
 void orc_trace_rays(const orc_scene *s, const float *rays, const float *tmax, int n, int any_hit,
                     hdr_gbuffer_texel *out);
+int orc_scene_sky(const orc_scene *s, const float *dirs, int n, float *out, float *sun);
 
 #ifdef __cplusplus
 }

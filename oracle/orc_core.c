@@ -455,7 +455,135 @@ orc_scene *orc_scene_create(const hdr_scene_desc *d) {
             }
         }
     }
+    s->sky = d->enable_physical_sky != 0;
+    if (s->sky) {
+        s->sun_dir = orc_sky_sun_direction(d->physical_sky_time);
+        s->sun_dir_n = vnorm(s->sun_dir);
+        s->sun_lit = orc_sky_sun_color(s->sun_dir, &s->sun_color);
+    }
     return s;
+}
+
+/* ---- PhysicalSky (scene/physical_sky.cpp:14-208) ---------------------------- */
+#define SKY_RP 6371e3f  /* planet radius */
+#define SKY_RA 6471e3f  /* atmosphere radius */
+#define SKY_HR 7994.0f
+#define SKY_HM 1200.0f
+#define SKY_BM 21e-6f
+static ov3 sky_br(void) { return V(5.5e-6f, 13.0e-6f, 22.4e-6f); }
+static ov3 sky_o(void) { return V(0.0f, SKY_RP + 100.0f, 0.0f); }
+
+/* RaySphereIntersect (physical_sky.cpp:14-23): near and far distances, (1e5, -1e5) on a miss */
+static void sky_sphere(ov3 r0, ov3 rd, float sr, float *t0, float *t1) {
+    float a = vdot(rd, rd);
+    float b = 2.0f * vdot(rd, r0);
+    float c = vdot(r0, r0) - (sr * sr);
+    float d = (b * b) - 4.0f * a * c;
+    if (d < 0.0f) {
+        *t0 = 1e5f;
+        *t1 = -1e5f;
+        return;
+    }
+    *t0 = (-b - sqrtf(d)) / (2.0f * a);
+    *t1 = (-b + sqrtf(d)) / (2.0f * a);
+}
+static ov3 sky_att(float r, float m) {
+    ov3 tau = vadd(vmulf(sky_br(), r), vmulf(V(SKY_BM * 1.1f, SKY_BM * 1.1f, SKY_BM * 1.1f), m));
+    return V(expf(-tau.x), expf(-tau.y), expf(-tau.z));
+}
+
+/* The scene's sky along n directions (rgb into out) and its sun (direction, colour);
+ * -1 without a sky, else whether the sun gives a sample (the reference harness's ref_sky) */
+int orc_scene_sky(const orc_scene *s, const float *dirs, int n, float *out, float *sun) {
+    if (!s->sky) return -1;
+    for (int i = 0; i < n; ++i) {
+        ov3 c = orc_sky_sample(s->sun_dir_n, V(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]));
+        out[3 * i] = c.x, out[3 * i + 1] = c.y, out[3 * i + 2] = c.z;
+    }
+    if (!s->sun_lit) return 0;
+    sun[0] = s->sun_dir.x, sun[1] = s->sun_dir.y, sun[2] = s->sun_dir.z;
+    sun[3] = s->sun_color.x, sun[4] = s->sun_color.y, sun[5] = s->sun_color.z;
+    return 1;
+}
+
+/* Scene::BuildRenderState's sun (scene.cpp:249-253) */
+ov3 orc_sky_sun_direction(float hour) {
+    float a = (hour - 12.0f) / 12.0f * (float)M_PI;
+    return vnorm(V(sinf(a) * cosf(0.5f), cosf(a), sinf(a) * sinf(0.5f)));
+}
+
+/* GetSunTransmittance (:172-206) and SampleDirect (:161-169) */
+int orc_sky_sun_color(ov3 sun, ov3 *color) {
+    if (sun.y < -0.05f) return 0;
+    ov3 tr = V(0.0f, 0.0f, 0.0f);
+    if (!(sun.y < 0.0f)) {
+        ov3 o = sky_o();
+        float t0, t1;
+        sky_sphere(o, sun, SKY_RA, &t0, &t1);
+        float step = t1 / 16.0f, t = 0.0f, r = 0.0f, m = 0.0f;
+        for (int j = 0; j < 16; ++j) {
+            float mid = t + step * 0.5f;
+            float h = vlen(vadd(o, vmulf(sun, mid))) - SKY_RP;
+            if (h < 0.0f) break;
+            r += expf(-h / SKY_HR) * step;
+            m += expf(-h / SKY_HM) * step;
+            t += step;
+        }
+        tr = sky_att(r, m);
+    }
+    *color = vmulf(tr, 20.0f);
+    return !(color->x <= 0.0f && color->y <= 0.0f && color->z <= 0.0f);
+}
+
+/* Sample (:29-159): the sky radiance along rd; sun_n is the sun direction normalised again */
+ov3 orc_sky_sample(ov3 sun_n, ov3 rd) {
+    ov3 dir = vnorm(rd), o = sky_o(), br = sky_br();
+    float a0, a1, p0, p1;
+    sky_sphere(o, dir, SKY_RA, &a0, &a1);
+    if (a1 < 0.0f) return V(0.0f, 0.0f, 0.0f);
+    float tmin = omax(0.0f, a0), tmax = a1;
+    sky_sphere(o, dir, SKY_RP, &p0, &p1);
+    if (p0 >= 0.0f && p0 < tmax) tmax = p0;
+    float step = (tmax - tmin) / 16.0f, t = tmin, odr = 0.0f, odm = 0.0f;
+    ov3 tr_ = V(0.0f, 0.0f, 0.0f), tm_ = V(0.0f, 0.0f, 0.0f);
+    float mu = vdot(dir, sun_n);
+    float phr = 3.0f / (16.0f * (float)M_PI) * (1.0f + mu * mu);
+    float g = 0.76f;
+    float phm = 3.0f / (8.0f * (float)M_PI) * ((1.0f - g * g) * (1.0f + mu * mu)) /
+                ((2.0f + g * g) * powf(1.0f + g * g - 2.0f * g * mu, 1.5f));
+    for (int i = 0; i < 16; ++i) {
+        float mid = t + step * 0.5f;
+        ov3 p = vadd(o, vmulf(dir, mid));
+        float h = vlen(p) - SKY_RP;
+        if (h < 0.0f) break;
+        float hr = expf(-h / SKY_HR) * step, hm = expf(-h / SKY_HM) * step;
+        odr += hr;
+        odm += hm;
+        float s0, s1, q0, q1;
+        sky_sphere(p, sun_n, SKY_RA, &s0, &s1);
+        float sstep = s1 / 8.0f, st = 0.0f, sr = 0.0f, sm = 0.0f;
+        sky_sphere(p, sun_n, SKY_RP, &q0, &q1);
+        if (!(q0 > 0.0f)) {
+            for (int j = 0; j < 8; ++j) {
+                float smid = st + sstep * 0.5f;
+                float sh = vlen(vadd(p, vmulf(sun_n, smid))) - SKY_RP;
+                if (sh < 0.0f) break;
+                sr += expf(-sh / SKY_HR) * sstep;
+                sm += expf(-sh / SKY_HM) * sstep;
+                st += sstep;
+            }
+            ov3 at = sky_att(odr + sr, odm + sm);
+            tr_ = vadd(tr_, vmulf(at, hr));
+            tm_ = vadd(tm_, vmulf(at, hm));
+        }
+        t += step;
+    }
+    ov3 si = V(20.0f, 20.0f, 20.0f);
+    ov3 col = vcmul(vadd(vmulf(vcmul(tr_, br), phr), vmulf(vmulf(tm_, SKY_BM), phm)), si);
+    if (p0 >= 0.0f && p0 < tmax + step) col = vmulf(col, 0.5f);
+    if (acosf(oclamp(mu, -1.0f, 1.0f)) < 0.00465f && p0 < 0.0f)
+        col = vadd(col, vmulf(vcmul(si, sky_att(odr, odm)), 10.0f));
+    return col;
 }
 
 void orc_scene_destroy(orc_scene *s) {

@@ -153,7 +153,12 @@ typedef struct orc_scene {
     int n_mat;
     olight *lights;
     int n_lights;
-    int env; /* active environment light index or -1 */
+    int env; /* first dome light index or -1 (the environment unless sky) */
+    /* PhysicalSky (scene/physical_sky.cpp) as the environment (scene.cpp:248-256): its
+     * sun is light index n_lights, outside the light sampler */
+    int sky;
+    ov3 sun_dir, sun_dir_n, sun_color;
+    int sun_lit; /* SampleDirect gives a sample */
 } orc_scene;
 
 /* HitRecord (core/hit_record.h:15-27) plus the triangle index */
@@ -167,6 +172,11 @@ typedef struct {
 
 orc_scene *orc_scene_create(const hdr_scene_desc *d);
 void orc_scene_destroy(orc_scene *s);
+/* PhysicalSky (scene/physical_sky.cpp): the sun for an hour of the day, its colour
+ * (0 when SampleDirect gives none), and the sky radiance along a direction */
+ov3 orc_sky_sun_direction(float hour);
+int orc_sky_sun_color(ov3 sun, ov3 *color);
+ov3 orc_sky_sample(ov3 sun_n, ov3 rd);
 /* Scene::IntersectScene (scene/scene.cpp:515-535) */
 int orc_intersect(const orc_scene *s, ov3 o, ov3 d, ohit *out);
 

@@ -417,6 +417,10 @@ static ov3 light_color(const olight *L) {
     return vmulf(V(L->color[0], L->color[1], L->color[2]), L->intensity * exp2f(L->exposure));
 }
 static int is_delta(const olight *L) { return L->type == HDR_LIGHT_POINT || L->type == HDR_LIGHT_DISTANT; }
+/* ILight::IsDeltaLight by index: n_lights is the physical sky's sun (a delta light) */
+static int light_delta(const orc_scene *s, int li) { return li >= s->n_lights || is_delta(&s->lights[li]); }
+/* Scene::GetEnvironment: the physical sky, else the first dome, else none */
+static int has_env(const orc_scene *s) { return s->sky || s->env >= 0; }
 
 static void dome_xy(const olight *L, ov3 d, int *x, int *y) {
     const double PI = 3.14159265358979323846;
@@ -432,6 +436,7 @@ static float dome_pdf_lum(const olight *L, ov3 t) {
 }
 /* DomeLight::Sample / EvalPdf (dome_light.cpp:117-148) */
 static ov3 env_sample(const orc_scene *s, ov3 d) {
+    if (s->sky) return orc_sky_sample(s->sun_dir_n, d);
     if (s->env < 0) return V(0, 0, 0);
     const olight *L = &s->lights[s->env];
     if (!L->pixels) return V(0, 0, 0);
@@ -442,7 +447,7 @@ static ov3 env_sample(const orc_scene *s, ov3 d) {
                  L->intensity * exp2f(L->exposure));
 }
 static float env_pdf(const orc_scene *s, ov3 d) {
-    if (s->env < 0) return 0.f;
+    if (s->sky || s->env < 0) return 0.f; /* the sky: IEnvironment's default 0 */
     const olight *L = &s->lights[s->env];
     if (!L->pixels || L->total_lum <= 0.f) return 0.f;
     int x, y;
@@ -594,6 +599,19 @@ static int propose(const orc_scene *s, ov3 hp, orc_rng *r, int *li, olsample *ls
     return 1;
 }
 static float select_pdf(const orc_scene *s) { return s->n_lights == 0 ? 0.0f : 1.0f / (float)s->n_lights; }
+/* UniformLightSampler::EvalPdf(*environment): the dome is a scene light, the sky is not */
+static float env_sel(const orc_scene *s) { return (s->sky || s->env < 0) ? 0.0f : select_pdf(s); }
+/* PhysicalSky::SampleLight (physical_sky.cpp:171-178): the sun, no random numbers */
+static int sky_sun(const orc_scene *s, olsample *ls) {
+    if (!s->sky || !s->sun_lit) return 0;
+    ls->dir = s->sun_dir;
+    ls->color = s->sun_color;
+    ls->normal = vneg(s->sun_dir);
+    ls->dist = 1e30f;
+    ls->pdf = 1.0f;
+    ls->solid = 1;
+    return 1;
+}
 
 /* ---- shading point --------------------------------------------------------- */
 typedef struct {
@@ -628,29 +646,44 @@ static oconn bounce_with_connection(const orc_scene *s, const osurf *sf, int mr,
 static int hit_light(const orc_scene *s, const ohit *h) { return s->inst[h->prim].light; } /* GetLightAtHit */
 
 /* ---- MisDirectLightIntegrator (mis_direct_light_integrator.cpp) ----------- */
+/* _evaluateNEE (:80-120): the radiance a light sample adds, 0 (returns 0) when it
+ * cannot or is occluded; *pn / *bp: its NEE and BSDF pdfs */
+static int mis_nee(const orc_scene *s, const osurf *sf, int li, const olsample *ls, const olambda *w, ospec *rad,
+                   float *pn, float *bp) {
+    float nl = vdot(sf->sn, ls->dir);
+    if (nl <= 0.0f) return 0;
+    float d2 = ls->dist * ls->dist;
+    float cy = omax(0.0f, vdot(vneg(ls->dir), ls->normal));
+    if (cy <= 0.0f && !light_delta(s, li)) return 0;
+    *pn = pdf_sa(ls->pdf, ls->solid, d2, omax(cy, 1e-6f));
+    if (*pn <= 0.0f) return 0;
+    if (occluded(s, vadd(sf->hit.position, vmulf(sf->sn, 1e-4f)), ls->dir, ls->dist)) return 0;
+    ov3 wo = vneg(sf->rd);
+    *bp = ggx_pdf(&sf->c, sf->sn, wo, ls->dir);
+    ov3 bv = ggx_eval(&sf->c, sf->sn, wo, ls->dir);
+    *rad = smulf(smul(orc_rgb_to_spectrum(bv, w), orc_rgb_to_spectrum(ls->color, w)), nl / *pn);
+    return 1;
+}
+
 static ospec mis_li(const orc_scene *s, const osurf *sf, const oconn *cn, const olambda *w, orc_rng *r) {
     ospec total = S1(0.0f);
     int use_bsdf = cn != NULL;
+    /* _integrateNEE :122-178; the physical sky is outside the sampler: a technique of its own */
+    int separate = has_env(s) && env_sel(s) <= 0.0f;
     int li;
     olsample ls;
-    if (propose(s, sf->hit.position, r, &li, &ls)) { /* _integrateNEE :122-178 */
-        const olight *L = &s->lights[li];
-        float nl = vdot(sf->sn, ls.dir);
-        if (nl > 0.0f) {
-            float d2 = ls.dist * ls.dist;
-            float cy = omax(0.0f, vdot(vneg(ls.dir), ls.normal));
-            if (!(cy <= 0.0f && !is_delta(L))) {
-                float pn = pdf_sa(ls.pdf, ls.solid, d2, omax(cy, 1e-6f));
-                if (pn > 0.0f && !occluded(s, vadd(sf->hit.position, vmulf(sf->sn, 1e-4f)), ls.dir, ls.dist)) {
-                    ov3 wo = vneg(sf->rd);
-                    float bp = ggx_pdf(&sf->c, sf->sn, wo, ls.dir);
-                    ov3 bv = ggx_eval(&sf->c, sf->sn, wo, ls.dir);
-                    ospec rad = smulf(smul(orc_rgb_to_spectrum(bv, w), orc_rgb_to_spectrum(ls.color, w)), nl / pn);
-                    float mw = (is_delta(L) || !use_bsdf) ? 1.0f : ph2(pn, bp);
-                    total = sadd(total, smulf(rad, mw));
-                }
-            }
+    if (propose(s, sf->hit.position, r, &li, &ls)) {
+        ospec rad;
+        float pn, bp;
+        if (mis_nee(s, sf, li, &ls, w, &rad, &pn, &bp)) {
+            float mw = (light_delta(s, li) || !use_bsdf) ? 1.0f : (separate ? ph3(pn, 1, 0.0f, 1, bp, 1) : ph2(pn, bp));
+            total = sadd(total, smulf(rad, mw));
         }
+    }
+    if (separate && sky_sun(s, &ls)) { /* the sun: a delta light, weight 1 */
+        ospec rad;
+        float pn, bp;
+        if (mis_nee(s, sf, s->n_lights, &ls, w, &rad, &pn, &bp)) total = sadd(total, smulf(rad, 1.0f));
     }
     if (!cn) return total;
     /* _integrateBSDFConnection :180-248 */
@@ -663,9 +696,9 @@ static ospec mis_li(const orc_scene *s, const osurf *sf, const oconn *cn, const 
     float ps = 0.0f, pe = 0.0f;
     ospec rad;
     if (!cn->has_hit) {
-        if (s->env < 0) return total;
+        if (!has_env(s)) return total;
         rad = orc_rgb_to_spectrum(env_sample(s, b->d), w);
-        float sel = select_pdf(s), ep = env_pdf(s, b->d);
+        float sel = env_sel(s), ep = env_pdf(s, b->d);
         ps = sel * ep;
         pe = sel <= 0.0f ? ep : 0.0f;
     } else {
@@ -726,7 +759,7 @@ static ocontrib eval_light_sample(const orc_scene *s, const osurf *sf, int li, c
     float pn = pdf_sa(ls->pdf, ls->solid, d2, omax(cy, 1e-6f));
     float pb = ggx_pdf(&sf->c, sf->sn, wo, ls->dir);
     ov3 bv = ggx_eval(&sf->c, sf->sn, wo, ls->dir);
-    int delta = is_delta(&s->lights[li]);
+    int delta = light_delta(s, li);
     ocontrib r = {S1(0), S1(0), pn, pb, !delta, 1};
     if (nl <= 0.0f || pn <= 0.0f || (cy <= 0.0f && !delta)) return r;
     r.tmul = orc_rgb_to_spectrum(vmulf(bv, nl), w);
@@ -747,15 +780,15 @@ static ocontrib eval_bsdf_connection(const orc_scene *s, const osurf *sf, const 
     ocontrib r = {S1(0), b->integ, 0.0f, b->pdf, 0, 1};
     if (b->impossible || b->pdf <= 0.0f) {
         if (!cn->has_hit) {
-            if (s->env >= 0) r.emission = orc_rgb_to_spectrum(env_sample(s, b->d), w);
+            if (has_env(s)) r.emission = orc_rgb_to_spectrum(env_sample(s, b->d), w);
             return r;
         }
         r.emission = orc_rgb_to_spectrum(closure_of(s, &cn->hit).emission, w);
         return r;
     }
     if (!cn->has_hit) {
-        if (s->env < 0) return r;
-        float sel = select_pdf(s), ep = env_pdf(s, b->d);
+        if (!has_env(s)) return r;
+        float sel = env_sel(s), ep = env_pdf(s, b->d);
         float pn = sel > 0.0f ? sel * ep : (n_sky > 0 ? ep : 0.0f);
         r.emission = orc_rgb_to_spectrum(env_sample(s, b->d), w);
         r.p_nee = pn;
@@ -788,7 +821,7 @@ static ospec reeval(const orc_scene *s, const osurf *sf, int li, const olsample 
     float d2 = ls->dist * ls->dist;
     float cy = omax(0.0f, vdot(vneg(ls->dir), ls->normal));
     float pn = pdf_sa(ls->pdf, ls->solid, d2, omax(cy, 1e-6f));
-    if (nl <= 0.0f || pn <= 0.0f || (cy <= 0.0f && !is_delta(&s->lights[li]))) return S1(0.0f);
+    if (nl <= 0.0f || pn <= 0.0f || (cy <= 0.0f && !light_delta(s, li))) return S1(0.0f);
     ov3 bv = ggx_eval(&sf->c, sf->sn, wo, ls->dir);
     return smul(orc_rgb_to_spectrum(ls->color, w), orc_rgb_to_spectrum(vmulf(bv, nl), w));
 }
@@ -797,7 +830,10 @@ static ospec reeval(const orc_scene *s, const osurf *sf, int li, const olsample 
 static ospec ris_li(const orc_scene *s, const osurf *sf, const oconn *cn, const olambda *w, orc_rng *r,
                     int primary, const orc_ris_params *p, orc_reservoir *res, orc_pixel_trace *tr) {
     int N = p->candidate_count;
-    int n_nee = N / 2 > 1 ? N / 2 : 1, n_sky = 0;
+    /* technique split (:89-99): sky NEE when the environment is outside the light sampler */
+    int sep = has_env(s) && env_sel(s) <= 0.0f;
+    int n_tech = sep ? 3 : 2;
+    int n_nee = N / n_tech > 1 ? N / n_tech : 1, n_sky = sep ? N / n_tech : 0;
     int n_bsdf = N - n_nee - n_sky;
     if (n_bsdf < 0) n_bsdf = 0;
     int cap = n_nee + n_sky + n_bsdf + 1;
@@ -828,6 +864,27 @@ static ospec ris_li(const orc_scene *s, const osurf *sf, const oconn *cn, const 
         }
         all[n++] = c;
     }
+    /* sky NEE (:445-475): the physical sky's SampleLight, the sun */
+    for (int i = 0; i < n_sky; ++i) {
+        olsample ls;
+        ocand c = cand_none();
+        if (sky_sun(s, &ls)) {
+            ocontrib nee = eval_light_sample(s, sf, s->n_lights, &ls, p->skip_visibility, w);
+            ospec contrib = smul(nee.emission, nee.tmul);
+            float target = orc_spectrum_luminance(contrib, w);
+            float mis = nee.use_mis ? ph3(nee.p_nee, n_sky, 0.0f, n_nee, nee.p_bsdf, n_bsdf) : 1.0f;
+            c.valid = 1;
+            c.has_lc = 1;
+            c.light = s->n_lights;
+            c.ls = ls;
+            c.origin = 1;
+            c.tp = contrib;
+            c.ris_weight = (mis * target) / ((double)nee.p_nee + 1e-9);
+            c.target = (double)target;
+            c.vis_tested = nee.vis_tested;
+        }
+        all[n++] = c;
+    }
     /* _generateBSDFSamplingCandidates (:396-551) */
     int first = n;
     if (cn && cn->b.pdf > 0.0f) {
@@ -835,7 +892,7 @@ static ospec ris_li(const orc_scene *s, const osurf *sf, const oconn *cn, const 
         ospec contrib = smul(bc.emission, bc.tmul);
         double target = (double)orc_spectrum_luminance(contrib, w);
         float ps = bc.p_nee, pk = 0.0f;
-        if (!cn->has_hit && (s->env < 0 || select_pdf(s) <= 0.0f)) {
+        if (!cn->has_hit && (!has_env(s) || env_sel(s) <= 0.0f)) {
             ps = 0.0f;
             pk = bc.p_nee;
         }
@@ -857,20 +914,20 @@ static ospec ris_li(const orc_scene *s, const osurf *sf, const oconn *cn, const 
             continue;
         }
         if (!sc.has_hit) {
-            if (s->env < 0) {
+            if (!has_env(s)) {
                 all[n++] = c;
                 continue;
             }
             ov3 wi = sc.b.d;
             ov3 env_rgb = env_sample(s, wi);
             ospec em = orc_rgb_to_spectrum(env_rgb, w);
-            float pb = sc.b.pdf, sel = select_pdf(s), ep = env_pdf(s, wi);
+            float pb = sc.b.pdf, sel = env_sel(s), ep = env_pdf(s, wi);
             float ps = sel * ep, pk = (sel <= 0.0f && n_sky > 0) ? ep : 0.0f, pn = ps + pk;
             double target = (double)orc_spectrum_luminance(smul(em, sc.b.integ), w);
             double mis = (double)ph3(pb, n_bsdf, ps, n_nee, pk, n_sky);
             c.valid = 1;
             c.has_lc = pn > 0.0f;
-            c.light = s->env;
+            c.light = s->sky ? -1 : s->env;
             c.ls.dir = wi;
             c.ls.color = env_rgb;
             c.ls.normal = vneg(wi);
@@ -1103,7 +1160,7 @@ static ospec path_li(const orc_scene *s, ov3 ro, ov3 rd, int has, ohit hit, cons
         }
         has = orc_intersect(s, vadd(hit.position, vmulf(rd, 1e-4f)), rd, &hit);
     }
-    if (s->env >= 0 && pp->render_ibl_background) return orc_rgb_to_spectrum(env_sample(s, rd), w);
+    if (has_env(s) && pp->render_ibl_background) return orc_rgb_to_spectrum(env_sample(s, rd), w);
     return S1(0.0f);
 }
 

@@ -83,9 +83,14 @@ RefScene *ref_create(const hdr_scene_desc *d) {
             return nullptr;
         }
         for (auto &m : prims.meshes) rs->meshes.push_back(std::move(m));
-        rs->scene.BuildRenderState(SceneBuildRenderStateConfig{}, GetMainThreadRenderJob());
+        SceneBuildRenderStateConfig config{};
+        config.EnablePhysicalSky = d->enable_physical_sky != 0;
+        config.PhysicalSkyTime = d->physical_sky_time;
+        rs->scene.BuildRenderState(config, GetMainThreadRenderJob());
         const auto lights = rs->scene.GetLights();
         for (size_t k = 0; k < lights.size(); ++k) rs->light_index[lights[k]] = (int)k;
+        // the physical sky's sun is the light after the scene's own (it is not one of them)
+        if (const PhysicalSky *sky = rs->scene.GetPhysicalSky()) rs->light_index[sky] = (int)lights.size();
     } catch (const std::exception &e) {
         std::fprintf(stderr, "ref_create: %s\n", e.what());
         delete rs;
@@ -407,5 +412,21 @@ int ref_resolve(const float *src, int pixels, int src_components, int format, un
 }
 
 const char *ref_version(void) { return "hdRestir reference sources compiled in place with the oracle shim"; }
+
+// The scene's PhysicalSky (Scene::BuildRenderState with EnablePhysicalSky): Sample()
+// along each of n directions (xyz) into out (rgb), and SampleDirect's sun into
+// sun (direction, colour). Returns -1 without a sky, else whether the sun gave a sample.
+int ref_sky(RefScene *rs, const float *dirs, int n, float *out, float *sun) {
+    const PhysicalSky *sky = rs->scene.GetPhysicalSky();
+    if (!sky) return -1;
+    for (int i = 0; i < n; ++i) {
+        const GfVec3f c = sky->Sample(GfVec3f(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]));
+        for (int k = 0; k < 3; ++k) out[3 * i + k] = c[k];
+    }
+    const auto s = sky->SampleDirect();
+    if (!s) return 0;
+    for (int k = 0; k < 3; ++k) sun[k] = s->Dir[k], sun[3 + k] = s->Color[k];
+    return 1;
+}
 
 }  // extern "C"

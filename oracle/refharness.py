@@ -80,6 +80,8 @@ def lib() -> C.CDLL:
         L.ref_accumulate.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.ref_resolve.restype = C.c_int
         L.ref_resolve.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp]
+        L.ref_sky.restype = C.c_int
+        L.ref_sky.argtypes = [vp, vp, C.c_int, vp, vp]
         _lib = L
     return _lib
 
@@ -111,6 +113,17 @@ class Reference:
 
     def clear_persistent(self):
         self._lib.ref_clear_persistent(self._s)
+
+    def sky(self, dirs):
+        """PhysicalSky::Sample along each direction (n x 3 float32) and SampleDirect's
+        sun (direction + colour, or None)."""
+        d = np.ascontiguousarray(dirs, np.float32)
+        out = np.zeros_like(d)
+        sun = np.zeros(6, np.float32)
+        got = self._lib.ref_sky(self._s, _p(d), len(d), _p(out), _p(sun))
+        if got < 0:
+            raise RuntimeError("the scene has no physical sky")
+        return out, (sun if got else None)
 
     def render(self, cam, frame, ris=False, candidate_count=16, use_reservoir=True, skip_visibility=False,
                max_depth=32, firefly=True, accumulate=True, resolution_level=0, enable_subsurface=True,

@@ -54,6 +54,56 @@ def test_oracle_equals_reference(cfg, kw):
         assert np.array_equal(o.res["m"], r["m"])
 
 
+@pytest.mark.parametrize("hour", [6.5, 9.0, 12.0, 15.5, 17.9, 18.2, 2.0])
+def test_physical_sky_equals_reference(hour):
+    """PhysicalSky::Sample along 4000 directions and the sun of SampleDirect
+    (direction, colour, or none after sunset), bit for bit."""
+    sc, _ = configs.sky_variant(2, 16, 16, hour=hour, grid=32, n_spheres=4, n_lights=8)
+    d = np.random.default_rng(int(hour * 10)).normal(size=(4000, 3)).astype(np.float32)
+    a, sun_a = orc.Oracle(sc).sky(d)
+    b, sun_b = refharness.Reference(sc).sky(d)
+    assert np.array_equal(bits(a), bits(b))
+    assert (sun_a is None) == (sun_b is None) == (hour in (18.2, 2.0))
+    if sun_a is not None:
+        assert np.array_equal(bits(sun_a), bits(sun_b))
+        assert float(np.abs(a).max()) > 0.0
+
+
+@pytest.mark.parametrize("hour", [15.5, 6.5])
+@pytest.mark.parametrize("cfg,kw", [
+    (2, dict(ris=True, candidate_count=8, use_reservoir=True, skip_visibility=False, max_depth=1)),
+    (2, dict(ris=True, candidate_count=6, use_reservoir=True, skip_visibility=True, max_depth=1)),
+    (1, dict(ris=True, candidate_count=9, use_reservoir=False, skip_visibility=False, max_depth=1)),
+    (2, dict(ris=True, candidate_count=4, use_reservoir=True, skip_visibility=False, max_depth=2)),
+    (2, dict(ris=False, max_depth=3)),
+])
+def test_oracle_equals_reference_under_the_physical_sky(hour, cfg, kw):
+    """The environment outside the light sampler: RIS splits its candidates over
+    three techniques (sampler NEE, sky NEE = the sun, BSDF), the path tracer adds a
+    sun sample per vertex, misses see the sky. Colour bit for bit, reservoir M and
+    winner light (the sun is light index len(lights)) over three frames of history."""
+    extra = {1: dict(n_lights=64), 2: dict(grid=48, n_spheres=30, n_lights=60)}[cfg]
+    sc, cam = configs.sky_variant(cfg, 40, 30, hour=hour, **extra)
+    ref = refharness.Reference(sc)
+    o = orc.Oracle(sc, threads=4)
+    suns = 0
+    for f in range(3):
+        g, c, r = ref.render(cam, f, accumulate=True, firefly=True, **kw)
+        assert np.array_equal(o.raycast(cam, f)["prim_id"], g["prim_id"])
+        o.integrate(cam, f, **kw)
+        o.accumulate(cam, f, firefly=True)
+        assert np.array_equal(bits(o.color), bits(c))
+        if kw.get("ris") and kw.get("use_reservoir"):
+            assert np.array_equal(o.res["m"], r["m"])
+            has = r["has_sample"] == 1
+            assert np.array_equal(o.res["has_sample"], r["has_sample"])
+            assert np.array_equal(o.res["light"][has], r["light"][has])
+            suns += int((r["light"][has] == len(sc.lights)).sum())
+    assert (g["hit"] == 0).any()  # the camera sees the sky
+    if kw.get("ris") and kw.get("use_reservoir"):
+        assert suns > 0  # the sun wins some reservoirs
+
+
 def test_trace_rays_match_reference():
     sc, cam = configs.small_variant(2, 16, 16, grid=64, n_spheres=40, n_lights=50)
     rng = np.random.default_rng(3)
