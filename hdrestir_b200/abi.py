@@ -25,6 +25,7 @@ CTX_DEVICE_BUILD = 128
 CTX_RECORD_LIGHTS = 256
 CTX_REFERENCE_SHADOWS = 512
 CTX_SAH_CLOSEST = 1024
+CTX_REFERENCE_CLOSEST = 2048
 RIS_REPROJECT = 4
 FMT_FLOAT32, FMT_FLOAT16, FMT_UNORM8, FMT_SNORM8, FMT_INT32 = 0, 1, 2, 3, 4
 FMT_DTYPES = {0: np.float32, 1: np.uint16, 2: np.uint8, 3: np.int8, 4: np.int32}

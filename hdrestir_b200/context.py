@@ -72,7 +72,7 @@ class Context:
     def __init__(self, device: int = 0, timings: bool = True, hbm_budget: int = 0, wide_bvh: bool = False,
                  lane_per_ray: bool = False, unphased: bool = False, pt_one_kernel: bool = False,
                  split_stack: bool = False, device_build: bool = False, record_lights: bool = False,
-                 reference_shadows: bool = False, sah_closest: bool = False):
+                 reference_shadows: bool = False, sah_closest: bool = False, reference_closest: bool = False):
         self._lib = abi.lib()
         self.device = int(device)
         self._h = C.c_void_p()
@@ -81,7 +81,8 @@ class Context:
                  | (abi.CTX_PT_ONE_KERNEL if pt_one_kernel else 0) | (abi.CTX_SPLIT_STACK if split_stack else 0)
                  | (abi.CTX_DEVICE_BUILD if device_build else 0) | (abi.CTX_RECORD_LIGHTS if record_lights else 0)
                  | (abi.CTX_REFERENCE_SHADOWS if reference_shadows else 0)
-                 | (abi.CTX_SAH_CLOSEST if sah_closest else 0))
+                 | (abi.CTX_SAH_CLOSEST if sah_closest else 0)
+                 | (abi.CTX_REFERENCE_CLOSEST if reference_closest else 0))
         desc = abi.CtxDesc(int(device), flags, int(hbm_budget))
         abi.check(self._lib.hdr_ctx_create(C.byref(self._h), C.byref(desc)))
         self.width = self.height = 0

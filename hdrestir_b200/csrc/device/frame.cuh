@@ -93,7 +93,9 @@ struct PathParamsD {
 struct WaveBuffers {
     float4 *q_closest;    // 2 per entry: origin.xyz + slot bits | direction.xyz
     float4 *q_shadow;     // 2 per entry: origin.xyz + slot bits | direction.xyz + distance limit
-    int *counts;          // [0] closest-hit queue length, [1] shadow queue length
+    int *counts;          // [0] closest-hit queue length, [1] shadow queue length (8 ints)
+    int *fix;             // one per closest-hit queue entry: entries whose checked SAH hit the reference walk
+                          // redoes (nullptr exactly when the queue has no entries)
     float4 *hits;         // pixels * n_closest: t, instance bits, triangle bits, u
     float *hit_v;         // pixels * n_closest
     unsigned char *occ;   // pixels * n_shadow
@@ -137,9 +139,11 @@ struct TraceTuning {
 // ris_shade launch shapes: (threads per block, minimum resident blocks per SM)
 // = (256, 1), (256, 2), (128, 3), (128, 4)
 constexpr int kShadeShapes = 4;
-// The two trace kernels over the queues of the last ris_generate (they read
-// the queue counts and reset nothing but their own fetch counters' use, so the
-// caller zeroes counts[2..3] before a rerun); returns the launches, -1 on error.
+// The trace kernels over the queues of the last ris_generate: closest hits, then
+// shadow queries; with checked SAH closest hits (s.sh4_closest == 2) also the
+// check and the reference walk of the entries it rejected (counts[6..7], wb.fix).
+// They read the queue counts and reset nothing but their own fetch counters' use,
+// so the caller zeroes counts[2..3] before a rerun; returns the launches, -1 on error.
 // The shadow-ray queue q over the shadow BVH when the scene has it (s.sh4), else the
 // phased walk of the reference trees; *count rays, *fetch the hand-out counter.
 int launch_shadow_queue(const DeviceScene &s, const float4 *q, const int *count, int *fetch, unsigned char *occ,
@@ -239,6 +243,7 @@ struct PtBuffers {
     int4 *state;            // BounceState refl, refr; flags; spare
     int *active[2];         // live-path lists (ping-pong)
     int *counts;            // [0..3] queue lengths and fetch counters, [4..5] active-list lengths
+    int *fix;               // WaveBuffers::fix of the closest-hit queue
     float4 *q_closest, *q_shadow, *hits;
     float *hit_v;
     unsigned char *occ;

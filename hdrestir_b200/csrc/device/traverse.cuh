@@ -65,7 +65,15 @@ struct DeviceScene {
     const int *sh4_inst_root;  // per instance: its mesh's root node, -1 = no triangles
     const int *sh4_inst_rank;  // per instance: its position in the reference TLAS's leaf order
     int sh4;                   // 1: shadow queries walk the 4-wide SAH trees
-    int sh4_closest;           // 1: closest hits walk them too (opt-in, HDR_CTX_SAH_CLOSEST)
+    // closest hits: 0 walk the reference trees; 1 walk the SAH trees (HDR_CTX_SAH_CLOSEST);
+    // 2 walk the SAH trees and check each hit against the reference walk (ref_reaches),
+    // which then walks the reference trees for the rare ray whose answer it cannot vouch for
+    int sh4_closest;
+    // parent links of the reference trees for that check
+    const int *ref_tlas_parent;  // per TLAS node, -1 at the root
+    const int *ref_inst_leaf;    // per instance: its TLAS leaf
+    const int *ref_blas_parent;  // per BLAS node of all meshes: mesh-local parent, -1 at a root
+    const int *ref_tri_leaf;     // per triangle record: its mesh-local leaf
     // This struct's own copy in device memory. Kernels take the scene by value
     // (parameter space); a non-inlined callee gets this pointer instead of the
     // parameter's address, which would make every thread copy the parameter
@@ -767,16 +775,68 @@ __device__ bool trace_ray_wide(const DeviceScene &s, V3 o, V3 d, float t_limit, 
 #include "shadow4.cuh"
 namespace hdr {
 
+// The check of a closest hit found on the 4-wide SAH trees (DeviceScene::sh4_closest
+// == 2). The reference's walk (scene.cpp:414-510, bvh.cpp:243-305) skips a node only
+// when its slab test fails or its entry distance exceeds the running closest t. No
+// triangle lies nearer than the SAH walk's nearest hit t, so that running t never
+// drops below t before the hit's triangle is tested. Hence, if every box on the way
+// from the TLAS root down to the instance's leaf, and from the instance's BLAS root
+// down to the triangle's leaf (object-space ray, BLAS thresholds), passes the
+// reference's slab test with an entry distance no farther than t, the reference walk
+// tests the triangle and takes it: the same IntersectTriangle arithmetic gives the
+// same t, and the SAH walk breaks ties in the reference's walk order. A hit that
+// grazes a box the reference's rounding rejects fails the check.
+__device__ __noinline__ static bool ref_reaches(const DeviceScene *s, V3 o, V3 d, int inst, int tri, float t) {
+    const SlabRay wr = make_slab_ray<false>(o, d);
+    for (int n = __ldg(&s->ref_inst_leaf[inst]); n >= 0; n = __ldg(&s->ref_tlas_parent[n])) {
+        const float4 *np = s->tlas_nodes + 2 * (size_t)n;
+        float ta;
+        if (!slab_test(wr, __ldg(np), __ldg(np + 1), ta) || ta > t) return false;
+    }
+    const float4 *ip = s->instances + 8 * (size_t)inst;
+    const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2), m3 = __ldg(ip + 3);
+    const float inv[16] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w,
+                           m2.x, m2.y, m2.z, m2.w, m3.x, m3.y, m3.z, m3.w};
+    const SlabRay br = make_slab_ray<true>(m4f_transform(inv, o), m4f_transform_dir(inv, d));
+    const int node_base = fbits(__ldg(&ip[4].w)), tri_base = fbits(__ldg(&ip[5].w));
+    for (int n = __ldg(&s->ref_tri_leaf[tri_base + tri]); n >= 0; n = __ldg(&s->ref_blas_parent[node_base + n])) {
+        const float4 *np = s->blas_nodes + 2 * (size_t)(node_base + n);
+        float ta;
+        if (!slab_test(br, __ldg(np), __ldg(np + 1), ta) || ta > t) return false;
+    }
+    return true;
+}
+
+// The reference walk for a ray whose SAH hit the check could not vouch for.
+struct RefClosest {
+    HitId hit;
+    unsigned err;
+};
+__device__ __noinline__ static RefClosest reference_closest(const DeviceScene *s, V3 o, V3 d) {
+    RefClosest r;
+    r.err = 0;
+    trace_ray_binary<false>(*s, o, d, 0.0f, r.hit, r.err);
+    return r;
+}
+
 // A ray's walk: the reference's own trees (binary, or their 4-wide collapse),
 // or, for closest hits with s.sh4_closest, the Closest4Walk over the 4-wide SAH
-// trees (the reference's answer except where the reference's own rounded box
-// tests cull a hit, e.g. on coplanar surfaces).
+// trees: checked against the reference walk (mode 2, the reference's answer bit
+// for bit), or alone (mode 1, the reference's answer except where the reference's
+// own rounded box tests cull a hit, e.g. on coplanar surfaces).
 template <bool kAnyHit>
 __device__ __forceinline__ bool trace_ray(const DeviceScene &s, V3 o, V3 d, float t_limit, HitId &hit,
                                           unsigned &err) {
     if (!kAnyHit && s.sh4_closest) {
         NoStats ns;
-        return closest4_ray(s, o, d, hit, err, ns);
+        const bool found = closest4_ray(s, o, d, hit, err, ns);
+        if (s.sh4_closest == 2 && found && !ref_reaches(s.dev, o, d, hit.inst, hit.tri, hit.t)) {
+            const RefClosest r = reference_closest(s.dev, o, d);
+            hit = r.hit;
+            err |= r.err;
+            return hit.inst >= 0;
+        }
+        return found;
     }
     return s.wide ? trace_ray_wide<kAnyHit>(s, o, d, t_limit, hit, err)
                   : trace_ray_binary<kAnyHit>(s, o, d, t_limit, hit, err);

@@ -92,6 +92,9 @@ struct SceneStore {
     // shadow-ray BVH (host/shadow_bvh.h): present when sh4 is true; the TLAS part is
     // rebuilt on the host when instances move
     bool sh4 = false;
+    // the reference trees' parent links for exact SAH closest hits (closest_mode 2); they
+    // describe the uploaded TLAS, so moving instances on the device clears this
+    bool ref_links = false;
     std::vector<int> sh4_inst_root;
     int sh4_tlas_capacity = 0, sh4_blas_depth = 0;
     // the scene's arrays by DeviceScene field name, for hdr_scene_array
@@ -627,6 +630,107 @@ bool tlas_boxes_proper(const hdr::FlatScene &f) {
 }  // namespace
 
 namespace {
+// Parent links of the reference trees, for checking a closest hit found on the
+// 4-wide SAH trees against the reference's own walk (exact SAH closest hits):
+// per TLAS node its parent, per instance its TLAS leaf, per BLAS node (all meshes,
+// mesh-local indices) its parent, per triangle record its mesh-local leaf. Only
+// nodes a walk can reach are linked (-1 elsewhere). Needs the host-built trees.
+struct RefLinks {
+    std::vector<int> tlas_parent, inst_leaf, blas_parent, tri_leaf;
+};
+bool build_ref_links(const hdr::FlatScene &f, RefLinks &L) {
+    if (f.blas_nodes.empty() || f.tlas_nodes.empty() || f.num_instances <= 0) return false;
+    const size_t n_tlas = f.tlas_nodes.size() / 8, n_blas = f.blas_nodes.size() / 8, n_tri = f.tri_geo.size() / 12;
+    L.tlas_parent.assign(n_tlas, -1);
+    L.inst_leaf.assign((size_t)f.num_instances, -1);
+    L.blas_parent.assign(n_blas, -1);
+    L.tri_leaf.assign(n_tri, -1);
+    auto ibits = [](float v) {
+        int i;
+        std::memcpy(&i, &v, sizeof(i));
+        return i;
+    };
+    std::vector<int> todo{0};
+    while (!todo.empty()) {
+        const int n = todo.back();
+        todo.pop_back();
+        const float *rec = &f.tlas_nodes[8 * (size_t)n];
+        const int left = ibits(rec[3]), count = ibits(rec[7]);
+        if (left >= 0) {
+            for (int ch : {left, left + 1}) {
+                if ((size_t)ch >= n_tlas) return false;
+                L.tlas_parent[(size_t)ch] = n;
+                todo.push_back(ch);
+            }
+        } else {
+            const int first = -left - 1;
+            for (int k = 0; k < count; ++k) {
+                const int ii = f.tlas_inst[(size_t)(first + k)];
+                if (ii < 0 || ii >= f.num_instances) return false;
+                L.inst_leaf[(size_t)ii] = n;
+            }
+        }
+    }
+    std::vector<char> done_mesh(n_blas + 1, 0);
+    for (int i = 0; i < f.num_instances; ++i) {  // each mesh's tree once, from its instances' bases
+        const float *ir = &f.instances[32 * (size_t)i];
+        const int node_base = ibits(ir[19]), tri_base = ibits(ir[23]), blas_ok = ibits(ir[29]);
+        if (!blas_ok || node_base < 0 || (size_t)node_base >= n_blas || done_mesh[(size_t)node_base]) continue;
+        done_mesh[(size_t)node_base] = 1;
+        todo.assign(1, 0);
+        while (!todo.empty()) {
+            const int m = todo.back();
+            todo.pop_back();
+            const size_t g = (size_t)node_base + (size_t)m;
+            if (g >= n_blas) return false;
+            const float *rec = &f.blas_nodes[8 * g];
+            const int left = ibits(rec[3]), count = ibits(rec[7]);
+            if (left >= 0) {
+                for (int ch : {left, left + 1}) {
+                    if ((size_t)node_base + (size_t)ch >= n_blas) return false;
+                    L.blas_parent[(size_t)node_base + (size_t)ch] = m;
+                    todo.push_back(ch);
+                }
+            } else {
+                const int first = -left - 1;
+                for (int q = 0; q < count; ++q) {
+                    const size_t t = (size_t)tri_base + (size_t)(first + q);
+                    if (t >= n_tri) return false;
+                    L.tri_leaf[t] = m;
+                }
+            }
+        }
+    }
+    return true;
+}
+
+// The device copies of a scene descriptor, one per (wide, sh4, closest mode), each
+// pointing at itself; a ctx's DeviceScene::dev is the copy of its own walk choices.
+constexpr int kDescCopies = 12;
+int desc_index(const hdr::DeviceScene &s) { return s.wide + 2 * s.sh4 + 4 * s.sh4_closest; }
+void fill_desc_copies(const hdr::DeviceScene &s, const hdr::DeviceScene *base, hdr::DeviceScene *copies, bool sh4) {
+    for (int w = 0; w < kDescCopies; ++w) {
+        copies[w] = s;
+        copies[w].wide = w & 1;
+        copies[w].sh4 = (w >> 1) & (sh4 ? 1 : 0);
+        copies[w].sh4_closest = copies[w].sh4 ? (w >> 2) : 0;
+        copies[w].dev = base + w;
+    }
+}
+
+// How closest hits walk (DeviceScene::sh4_closest): 0 the reference's trees, 1 the 4-wide
+// SAH trees alone (HDR_CTX_SAH_CLOSEST), 2 the SAH trees with each hit checked against
+// the reference walk's box tests (the default where the shadow BVH and the links exist;
+// flags that select a form of the reference walk for A/B checks keep walk 0).
+int closest_mode(uint32_t flags, bool sh4, bool links) {
+    if (!sh4) return 0;
+    if (flags & HDR_CTX_SAH_CLOSEST) return 1;
+    const uint32_t reference_forms = HDR_CTX_REFERENCE_CLOSEST | HDR_CTX_WIDE_BVH | HDR_CTX_LANE_PER_RAY |
+                                     HDR_CTX_UNPHASED | HDR_CTX_SPLIT_STACK;
+    if (flags & reference_forms) return 0;
+    return links ? 2 : 0;
+}
+
 // Which closest-hit rays the wavefront RIS pass casts (hdr::kTrace*).
 int ris_trace_level(const hdr_ctx *c, const hdr_ris_params *p) {
     if ((p->flags & HDR_RIS_TRACE_ALL_RAYS) || c->scene_light_geometry || c->scene.env_light >= 0 || c->scene.sky)
@@ -780,6 +884,14 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
         store->sh4_inst_root = sb.inst_root;
         store->sh4_tlas_capacity = sb.tlas_capacity;
         store->sh4_blas_depth = sb.blas_depth;
+        RefLinks links;  // exact closest hits on the SAH trees (closest_mode 2)
+        if (build_ref_links(f, links)) {
+            UP(links.tlas_parent, ref_tlas_parent);
+            UP(links.inst_leaf, ref_inst_leaf);
+            UP(links.blas_parent, ref_blas_parent);
+            UP(links.tri_leaf, ref_tri_leaf);
+            store->ref_links = true;
+        }
     }
 #undef UP
     {  // the device TLAS rebuild's inputs and scratch
@@ -830,9 +942,9 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     s.shallow = (f.max_blas_depth + f.max_tlas_depth + 4 <= hdr::kShallowStack) ? 1 : 0;
     s.has_textures = f.textures.empty() ? 0 : 1;
     s.sh4 = store->sh4 ? 1 : 0;
-    s.sh4_closest = (s.sh4 && (c->flags & HDR_CTX_SAH_CLOSEST)) ? 1 : 0;
+    s.sh4_closest = closest_mode(c->flags, store->sh4, store->ref_links);
     // the descriptor itself, for callees that are not inlined into a kernel
-    hdr::DeviceScene copies[8] = {s, s, s, s, s, s, s, s};
+    hdr::DeviceScene copies[kDescCopies];
     {
         DevBuf b;
         st = dev_alloc(c, b, sizeof(copies));
@@ -844,15 +956,10 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
         store->ptrs.push_back(b.ptr);
         store->bytes += b.bytes;
         store->desc_dev = (const hdr::DeviceScene *)b.ptr;
-        for (int w = 0; w < 8; ++w) {  // each copy points at itself
-            copies[w].wide = w & 1;
-            copies[w].sh4 = (w >> 1) & s.sh4;
-            copies[w].sh4_closest = (w >> 2) & copies[w].sh4;
-            copies[w].dev = store->desc_dev + w;
-        }
+        fill_desc_copies(s, store->desc_dev, copies, store->sh4);
         HDR_CUDA(cudaMemcpyAsync(b.ptr, copies, sizeof(copies), cudaMemcpyHostToDevice, c->stream));
     }
-    s.dev = store->desc_dev + s.wide + 2 * s.sh4 + 4 * s.sh4_closest;
+    s.dev = store->desc_dev + desc_index(s);
     const cudaError_t sync_err = cudaStreamSynchronize(c->stream);
     c->scene_store = store;  // owns the buffers from here on, also on the error path below
     c->scene_bytes_accounted = store->bytes;
@@ -1155,6 +1262,8 @@ static hdr_status ris_path_trace_pass(hdr_ctx *c, const hdr_camera *cam, int32_t
         wb.q_shadow = (float4 *)q;
         if ((st = ensure_buffer(c, "__wave_counts", 32, &q)) != HDR_OK) return st;
         wb.counts = (int *)q;
+        if ((st = ensure_buffer(c, "__wave_fix", count * wb.n_closest * 4, &q)) != HDR_OK) return st;
+        wb.fix = (int *)q;
         if ((st = ensure_buffer(c, "__wave_hits", count * wb.n_closest * 16, &q)) != HDR_OK) return st;
         wb.hits = (float4 *)q;
         if ((st = ensure_buffer(c, "__wave_hit_v", count * wb.n_closest * 4, &q)) != HDR_OK) return st;
@@ -1233,7 +1342,8 @@ hdr_status pt_buffers_from(Alloc alloc, size_t count, hdr::PtBuffers &B) {
         size_t bytes;
         void **dst;
     };
-    void *rng, *tp, *total, *outer, *ro, *rd, *bo, *bd, *bt, *nee, *state, *a0, *a1, *cnt, *qc, *qs, *hits, *hv, *occ;
+    void *rng, *tp, *total, *outer, *ro, *rd, *bo, *bd, *bt, *nee, *state, *a0, *a1, *cnt, *qc, *qs, *hits, *hv, *occ,
+        *fix;
     const Plane planes[] = {
         {"__pt_rng", count * 48, &rng},     {"__pt_tp", count * 16, &tp},       {"__pt_total", count * 16, &total},
         {"__pt_outer", count * 16, &outer}, {"__pt_ray_o", count * 16, &ro},    {"__pt_ray_d", count * 16, &rd},
@@ -1241,7 +1351,7 @@ hdr_status pt_buffers_from(Alloc alloc, size_t count, hdr::PtBuffers &B) {
         {"__pt_nee", count * 16, &nee},     {"__pt_state", count * 16, &state}, {"__pt_active0", count * 4, &a0},
         {"__pt_active1", count * 4, &a1},   {"__pt_counts", 32, &cnt},          {"__pt_q_closest", count * 32, &qc},
         {"__pt_q_shadow", count * 32, &qs}, {"__pt_hits", count * 16, &hits},   {"__pt_hit_v", count * 4, &hv},
-        {"__pt_occ", count, &occ}};
+        {"__pt_occ", count, &occ},          {"__pt_fix", count * 4, &fix}};
     hdr_status st;
     for (const Plane &pl : planes)
         if ((st = alloc(pl.name, pl.bytes, pl.dst)) != HDR_OK) return st;
@@ -1259,6 +1369,7 @@ hdr_status pt_buffers_from(Alloc alloc, size_t count, hdr::PtBuffers &B) {
     B.active[0] = (int *)a0;
     B.active[1] = (int *)a1;
     B.counts = (int *)cnt;
+    B.fix = (int *)fix;
     B.q_closest = (float4 *)qc;
     B.q_shadow = (float4 *)qs;
     B.hits = (float4 *)hits;
@@ -1291,9 +1402,8 @@ hdr_status hdr_scene_share(hdr_ctx *dst, hdr_ctx *src) {
     dst->scene = src->scene;
     dst->scene.wide = (dst->flags & HDR_CTX_WIDE_BVH) ? 1 : 0;
     dst->scene.sh4 = (dst->scene_store->sh4 && !(dst->flags & HDR_CTX_REFERENCE_SHADOWS)) ? 1 : 0;
-    dst->scene.sh4_closest = (dst->scene.sh4 && (dst->flags & HDR_CTX_SAH_CLOSEST)) ? 1 : 0;
-    dst->scene.dev =
-        dst->scene_store->desc_dev + dst->scene.wide + 2 * dst->scene.sh4 + 4 * dst->scene.sh4_closest;
+    dst->scene.sh4_closest = closest_mode(dst->flags, dst->scene.sh4, dst->scene_store->ref_links);
+    dst->scene.dev = dst->scene_store->desc_dev + desc_index(dst->scene);
     dst->scene_opaque = src->scene_opaque;
     dst->scene_light_geometry = src->scene_light_geometry;
     dst->scene_emissive = src->scene_emissive;
@@ -1373,16 +1483,14 @@ hdr_status hdr_scene_set_instance_transforms(hdr_ctx *c, const float *transforms
             store->sh4 = false;  // too deep for the shadow walk's stack: the reference trees serve shadow rays
         }
     }
+    // the reference TLAS changed on the device: its parent links no longer describe it, so
+    // closest hits go back to the reference walk for this scene
+    store->ref_links = false;
     s.sh4 = (store->sh4 && !(c->flags & HDR_CTX_REFERENCE_SHADOWS)) ? 1 : 0;
-    s.sh4_closest = (s.sh4 && (c->flags & HDR_CTX_SAH_CLOSEST)) ? 1 : 0;
-    s.dev = store->desc_dev + s.wide + 2 * s.sh4 + 4 * s.sh4_closest;
-    hdr::DeviceScene copies[8] = {s, s, s, s, s, s, s, s};
-    for (int w = 0; w < 8; ++w) {
-        copies[w].wide = w & 1;
-        copies[w].sh4 = (w >> 1) & (store->sh4 ? 1 : 0);
-        copies[w].sh4_closest = (w >> 2) & copies[w].sh4;
-        copies[w].dev = store->desc_dev + w;
-    }
+    s.sh4_closest = closest_mode(c->flags, s.sh4, store->ref_links);
+    s.dev = store->desc_dev + desc_index(s);
+    hdr::DeviceScene copies[kDescCopies];
+    fill_desc_copies(s, store->desc_dev, copies, store->sh4);
     HDR_CUDA(cudaMemcpyAsync(const_cast<hdr::DeviceScene *>(store->desc_dev), copies, sizeof(copies),
                              cudaMemcpyHostToDevice, c->stream));
     HDR_CUDA(cudaStreamSynchronize(c->stream));  // `copies` is a host stack buffer
@@ -1535,6 +1643,8 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
     all.q_shadow = (float4 *)q;
     if ((st = ensure_batch_scratch(store, "counts", 32, &q, done, lead->stream)) != HDR_OK) return st;
     all.counts = (int *)q;
+    if ((st = ensure_batch_scratch(store, "fix", (size_t)total_c * 4, &q, done, lead->stream)) != HDR_OK) return st;
+    all.fix = (int *)q;
     if ((st = ensure_batch_scratch(store, "hits", (size_t)total_c * 16, &q, done, lead->stream)) != HDR_OK) return st;
     all.hits = (float4 *)q;
     if ((st = ensure_batch_scratch(store, "hit_v", (size_t)total_c * 4, &q, done, lead->stream)) != HDR_OK) return st;
@@ -1571,8 +1681,8 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
                                      s) < 0)
             return fail(HDR_ECUDA, "generate launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     }
-    if (hdr::launch_wave_trace(lead->scene, all, lead->tune, lead->d_err, s) < 0)
-        return fail(HDR_ECUDA, "trace launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    const int traced = hdr::launch_wave_trace(lead->scene, all, lead->tune, lead->d_err, s);
+    if (traced < 0) return fail(HDR_ECUDA, "trace launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     for (int32_t i = 0; i < n; ++i) {
         const RisJob &j = jobs[(size_t)i];
         if ((lead->scene.has_textures ? hdr::textured::launch_ris_shade : hdr::launch_ris_shade)(lead->scene, j.cd, j.frame, j.d, j.gb, j.rv, wbs[(size_t)i], j.color, j.trace_level,
@@ -1583,7 +1693,7 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
     HDR_CUDA(cudaEventRecord(lead->sync_ev, s));
     HDR_CUDA(cudaEventRecord(store->batch_done, s));
     for (int32_t i = 1; i < n; ++i) HDR_CUDA(cudaStreamWaitEvent(ctxs[i]->stream, lead->sync_ev, 0));
-    lead->launches += (uint64_t)(2 * n + 2);
+    lead->launches += (uint64_t)(2 * n + traced);
     // the queues belong to the scene and the next batch reuses them: no autotuning rerun of this one
     lead->have_wave = false;
     return end_pass(lead, 1);

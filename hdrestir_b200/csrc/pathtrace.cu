@@ -292,6 +292,7 @@ int launch_path_trace_wavefront(const DeviceScene &s, const PtJobD *jobs, int n_
     wb.q_closest = B.q_closest;
     wb.q_shadow = B.q_shadow;
     wb.counts = B.counts;
+    wb.fix = B.fix;
     wb.hits = B.hits;
     wb.hit_v = B.hit_v;
     wb.occ = B.occ;
@@ -312,7 +313,7 @@ int launch_path_trace_wavefront(const DeviceScene &s, const PtJobD *jobs, int n_
             s, jobs[0], table, pr, B, B.active[cur], &B.counts[4 + cur], B.active[nxt], &B.counts[4 + nxt], v, err);
         ++launches;
     }
-    return cudaGetLastError() == cudaSuccess ? launches : -1;
+    return cudaPeekAtLastError() == cudaSuccess ? launches : -1;
 }
 
 }  // namespace hdr

@@ -58,12 +58,12 @@ int launch_upscale(const float *src, float *dst, int comps, int src_w, int src_h
                    cudaStream_t st) {
     upscale_kernel<<<grid_for((size_t)dst_w * dst_h, sm_count), 256, 0, st>>>(src, dst, comps, src_w, src_h, dst_w,
                                                                               dst_h);
-    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
 int launch_chroma_blur(const float4 *src, float4 *dst, int w, int h, int sm_count, cudaStream_t st) {
     chroma_blur_kernel<<<grid_for((size_t)w * h, sm_count), 256, 0, st>>>(src, dst, w, h);
-    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
 }  // namespace hdr

@@ -61,7 +61,7 @@ int launch_resolve(const float *src, int src_comps, int format, int dst_comps, v
         case kResolveInt32: resolve_kernel<kResolveInt32><<<blocks, 256, 0, st>>>(src, src_comps, dst, dst_comps, pixels); break;
         default: return -1;
     }
-    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
 }  // namespace hdr

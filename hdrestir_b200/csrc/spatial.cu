@@ -158,7 +158,7 @@ int launch_ris_spatial(const DeviceScene &s, const CameraD &cam, int frame_index
     ris_spatial_kernel<256><<<tile_blocks(cam.width, cam.height), 256, 0, st>>>(
         s, cam, frame_index, pr, cpf, p.m_cap, p.spatial_neighbors, radius, gb, in, out, color, q_winner,
         winner_count, err);
-    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
 }  // namespace hdr

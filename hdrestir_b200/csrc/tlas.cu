@@ -162,7 +162,7 @@ int launch_tlas_rebuild(const float *xf, float4 *instances, const float *mesh_ra
     if (staged) cudaFuncSetAttribute(tlas_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     tlas_build_kernel<<<1, 256, staged ? smem : 0, st>>>(bounds, n, tlas_nodes, cap_nodes, tlas_inst, stack,
                                                          cap_stack, info, staged);
-    return cudaGetLastError() == cudaSuccess ? 2 : -1;
+    return cudaPeekAtLastError() == cudaSuccess ? 2 : -1;
 }
 
 }  // namespace hdr

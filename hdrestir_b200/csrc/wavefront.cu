@@ -196,8 +196,9 @@ __device__ __forceinline__ void bind_deep(SplitStack<Entry, kDepth, kThreads> &s
 }
 
 template <bool kWide, bool kShallow, bool kAnyHit, class Put>
-__device__ __forceinline__ void phased_trace(const DeviceScene &s, const float4 *__restrict__ q, int n,
-                                             int *fetch_at, int quorum, Put put, unsigned &e) {
+__device__ __forceinline__ void phased_trace(const DeviceScene &s, const float4 *__restrict__ q,
+                                             const int *__restrict__ order, int n, int *fetch_at, int quorum,
+                                             Put put, unsigned &e) {
     using PW = PhasedTraceWalk<kWide, kAnyHit, kShallow>;
     __shared__ typename PW::Entry col[PW::kShared * kTraceThreads];
     typename PW::Entry deep[kShallow ? 1 : kTraceStack - PW::kShared];
@@ -217,7 +218,8 @@ __device__ __forceinline__ void phased_trace(const DeviceScene &s, const float4 
         const int k = fetch_ray(fetch_at, n, done, drained);
         if (done) {
             if (k >= 0) {
-                const float4 a = q[2 * (size_t)k], b = q[2 * (size_t)k + 1];
+                const size_t r = order ? (size_t)order[k] : (size_t)k;
+                const float4 a = q[2 * r], b = q[2 * r + 1];
                 w.start(s, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, kAnyHit ? b.w : 0.0f);
                 slot = __float_as_int(a.w);
             } else {
@@ -245,13 +247,16 @@ constexpr int phased_min_blocks() {
     return kWide ? 6 : 8;
 }
 
+// Closest hits on the reference's trees for the queue entries order[0..*count)
+// (order nullptr: entries 0..*count), fetch counting the entries handed out.
 template <bool kWide, bool kShallow>
 __global__ void __launch_bounds__(kTraceThreads, phased_min_blocks<kWide>()) trace_closest_phased_kernel(DeviceScene s, const float4 *__restrict__ q,
-                                                                             int *counts, float4 *hits, float *hit_v,
+                                                                             const int *order, const int *count,
+                                                                             int *fetch, float4 *hits, float *hit_v,
                                                                              int quorum, unsigned *err) {
     unsigned e = 0;
     phased_trace<kWide, kShallow, false>(
-        s, q, counts[0], &counts[3], quorum,
+        s, q, order, *count, fetch, quorum,
         [&](int slot, const auto &w) {
             hits[slot] = make_float4(w.hit.t, __int_as_float(w.hit.inst), __int_as_float(w.hit.tri), w.hit.u);
             hit_v[slot] = w.hit.v;
@@ -267,7 +272,7 @@ __global__ void __launch_bounds__(kTraceThreads, phased_min_blocks<kWide>()) tra
                                                                             unsigned *err) {
     unsigned e = 0;
     phased_trace<kWide, kShallow, true>(
-        s, q, *count, fetch, quorum,
+        s, q, nullptr, *count, fetch, quorum,
         [&](int slot, const auto &w) { occ[slot] = w.shadow_answer() ? 1 : 0; }, e);
     if (e) atomicOr(err, e);
 }
@@ -321,8 +326,9 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) trace_shadow4_kerne
     if (e) atomicOr(err, e);
 }
 
-// Closest-hit queue over the 4-wide SAH trees (DeviceScene::sh4_closest, opt-in),
-// scheduled like trace_shadow4_kernel (Closest4Walk).
+// Closest-hit queue over the 4-wide SAH trees (DeviceScene::sh4_closest),
+// scheduled like trace_shadow4_kernel (Closest4Walk). With sh4_closest == 2 the
+// hits are then checked by check_closest_kernel.
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) trace_closest4_kernel(DeviceScene s, const float4 *__restrict__ q,
                                                                                  int *counts, float4 *hits,
@@ -367,6 +373,25 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) trace_closest4_kern
     if (e) atomicOr(err, e);
 }
 
+// The check of the SAH walk's closest hits (sh4_closest == 2), one thread per
+// queue entry: an entry whose hit ref_reaches cannot vouch for is listed in
+// fix[0..*n_fix) for the reference walk. A miss needs no check: the SAH trees'
+// boxes hold every triangle, so the reference walk finds no hit either.
+__global__ void __launch_bounds__(256) check_closest_kernel(DeviceScene s, const float4 *__restrict__ q,
+                                                            const int *count, const float4 *__restrict__ hits,
+                                                            int *fix, int *n_fix) {
+    const int n = *count;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 a = q[2 * (size_t)k];
+        const float4 h = hits[__float_as_int(a.w)];
+        const int inst = __float_as_int(h.y);
+        if (inst < 0) continue;
+        const float4 b = q[2 * (size_t)k + 1];
+        if (!ref_reaches(s.dev, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, inst, __float_as_int(h.z), h.x))
+            fix[atomicAdd(n_fix, 1)] = k;
+    }
+}
+
 // The shadow-ray queue q (count / fetch counters on the device, answers into occ).
 int launch_shadow_queue(const DeviceScene &s, const float4 *q, const int *count, int *fetch, unsigned char *occ,
                         const TraceTuning &tune, unsigned *err, cudaStream_t st) {
@@ -383,7 +408,7 @@ int launch_shadow_queue(const DeviceScene &s, const float4 *q, const int *count,
                                         : trace_shadow_phased_kernel<false, false>);
         shadow<<<tgrid, kTraceThreads, 0, st>>>(s, q, count, fetch, occ, tune.node_quorum, err);
     }
-    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
 template <bool kWide, bool kRefill>
@@ -504,16 +529,27 @@ int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &t
     const bool phased = refill && (tune.mode & kTraceUnphased) == 0;
     const bool shallow = s.shallow && (tune.mode & kTraceSplitStack) == 0;
     if (!mark(ev_begin, 0)) return -1;
+    int launches = 2;
+    auto reference_phased = s.wide    ? trace_closest_phased_kernel<true, false>
+                            : shallow ? trace_closest_phased_kernel<false, true>
+                                      : trace_closest_phased_kernel<false, false>;
     if (s.sh4_closest) {
         auto closest = tune.shadow_shape == 0 ? trace_closest4_kernel<8>
                                               : (tune.shadow_shape == 1 ? trace_closest4_kernel<6>
                                                                         : trace_closest4_kernel<5>);
         closest<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, tune.node_quorum, err);
+        if (s.sh4_closest == 2 && wb.fix) {  // (no fix list: the queue has no entries)
+            // counts[6] entries the check rejected, counts[7] of them handed out
+            if (cudaMemsetAsync(wb.counts + 6, 0, 2 * sizeof(int), st) != cudaSuccess) return -1;
+            check_closest_kernel<<<tune.sm_count * 8, 256, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.fix,
+                                                                      wb.counts + 6);
+            reference_phased<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.fix, wb.counts + 6, wb.counts + 7,
+                                                              wb.hits, wb.hit_v, tune.node_quorum, err);
+            launches += 2;
+        }
     } else if (phased) {
-        auto closest = s.wide      ? trace_closest_phased_kernel<true, false>
-                       : shallow   ? trace_closest_phased_kernel<false, true>
-                                   : trace_closest_phased_kernel<false, false>;
-        closest<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, wb.counts, wb.hits, wb.hit_v, tune.node_quorum, err);
+        reference_phased<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_closest, nullptr, wb.counts, wb.counts + 3, wb.hits,
+                                                          wb.hit_v, tune.node_quorum, err);
     } else {
         auto closest = s.wide ? (refill ? trace_closest_kernel<true, true> : trace_closest_kernel<true, false>)
                               : (refill ? trace_closest_kernel<false, true> : trace_closest_kernel<false, false>);
@@ -528,7 +564,7 @@ int launch_wave_trace(const DeviceScene &s, WaveBuffers wb, const TraceTuning &t
         shadow<<<tgrid, kTraceThreads, 0, st>>>(s, wb.q_shadow, wb.counts, wb.occ, err);
     }
     if (!mark(ev_end, 1)) return -1;
-    return cudaGetLastError() == cudaSuccess ? 2 : -1;
+    return cudaPeekAtLastError() == cudaSuccess ? launches : -1;
 }
 
 namespace {
@@ -559,7 +595,7 @@ int launch_ris_generate(const DeviceScene &s, const CameraD &cam, int frame_inde
     ris_generate_kernel<<<tile_blocks(cam.width, cam.height), 256, 0, st>>>(s, cam, frame_index, path_run(p),
                                                                              ris_run(p), gb, wb, color, trace_level,
                                                                              err);
-    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
 int launch_ris_shade(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
@@ -585,7 +621,7 @@ int launch_ris_shade(const DeviceScene &s, const CameraD &cam, int frame_index, 
             ris_shade_kernel<256, 1><<<blocks, 256, 0, st>>>(s, cam, frame_index, pr, ris, gb, rv, wb, color,
                                                              trace_level, err);
     }
-    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
 // After the queued winner shadow rays: a pixel whose winner turned out occluded
@@ -629,7 +665,7 @@ int launch_winner_visibility(const DeviceScene &s, const CameraD &cam, int frame
         return -1;
     ris_winner_fixup_kernel<<<tune.sm_count * 4, 256, 0, st>>>(s, cam, frame_index, path_run(p), gb, rv, wb.q_winner,
                                                                wb.counts + 4, wb.occ_winner, color);
-    return cudaGetLastError() == cudaSuccess ? 2 : -1;
+    return cudaPeekAtLastError() == cudaSuccess ? 2 : -1;
 }
 
 int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_index, const RisParamsD &p,
@@ -645,11 +681,12 @@ int launch_ris_wavefront(const DeviceScene &s, const CameraD &cam, int frame_ind
     // calls its own launchers, not hdr::'s
     if ((launch_ris_generate)(s, cam, frame_index, p, gb, wb, color, trace_level, err, st) < 0) return -1;
     if (!mark(ev_end, 0)) return -1;
-    if ((launch_wave_trace)(s, wb, tune, err, st, ev_begin ? ev_begin + 1 : nullptr, ev_end ? ev_end + 1 : nullptr) < 0)
-        return -1;
+    const int traced =
+        (launch_wave_trace)(s, wb, tune, err, st, ev_begin ? ev_begin + 1 : nullptr, ev_end ? ev_end + 1 : nullptr);
+    if (traced < 0) return -1;
     if (!mark(ev_begin, 3)) return -1;
     if ((launch_ris_shade)(s, cam, frame_index, p, gb, rv, wb, color, trace_level, err, st, tune) < 0) return -1;
-    int launches = 4;
+    int launches = 2 + traced;
     if (wb.q_winner) {  // the winners' shadow rays, then the pixels they found occluded
         if ((launch_winner_visibility)(s, cam, frame_index, p, gb, rv, wb, color, err, st, tune) < 0) return -1;
         launches += 2;

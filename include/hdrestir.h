@@ -311,12 +311,21 @@ typedef struct hdr_gbuffer_texel {
                                      distance). The answers agree: the same triangle test in the
                                      same instance space, conservative boxes, and closest-hit ties
                                      broken in the reference's walk order. */
-#define HDR_CTX_SAH_CLOSEST 1024u /* closest hits too walk the 4-wide SAH trees (ties broken in
-                                     the reference's walk order). Faster, and the reference's
-                                     answer except where the reference's own rounded box tests cull
-                                     the nearest hit (coplanar surfaces): about 1e-3 of random rays
-                                     in config 1's scene, 5e-6 in config 2's. Off by default:
-                                     closest hits are held to the reference bit for bit. */
+#define HDR_CTX_SAH_CLOSEST 1024u /* closest hits walk the 4-wide SAH trees (ties broken in the
+                                     reference's walk order) WITHOUT the check below: the
+                                     reference's answer except where the reference's own rounded
+                                     box tests cull the nearest hit (coplanar surfaces): about 1e-3
+                                     of random rays in config 1's scene, 5e-6 in config 2's.
+                                     By default closest hits also walk the SAH trees, and each
+                                     hit is checked against the reference walk: every box on the
+                                     way down to it in the reference's own trees must pass the
+                                     reference's slab test no farther than the hit; a ray that
+                                     fails the check walks the reference's trees. The answer is
+                                     then the reference's bit for bit. Scenes whose trees were
+                                     built on the device (HDR_CTX_DEVICE_BUILD) or whose instances
+                                     moved on the device walk the reference trees. */
+#define HDR_CTX_REFERENCE_CLOSEST 2048u /* closest hits walk the reference's trees only (for A/B
+                                     checks; same answers as the default) */
 #define HDR_CTX_RECORD_LIGHTS 256u /* diagnostic, no reference counterpart: the wavefront
                                      hdr_ris_path_trace records the light index each NEE candidate
                                      selected (UniformLightSampler::ProposeCandidate,
