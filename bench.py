@@ -450,7 +450,8 @@ def serving_leg(n_jobs: int, rate: float = 200.0):
                      "latency_p99_ms": 1000.0 * lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))],
                      "steps": steps}
     out["modes"] = ("plain: one job at a time, each frame rendered alone; served_all: every admitted job "
-                    "advances each step; served: least remaining work first, 32 Mpx per step; each mode "
+                    "advances each step; served: least remaining work first less half the work served "
+                    "since the job arrived, 32 Mpx per step; each mode "
                     "timed on its second pass over the job stream (the first warms the server up)")
     return out
 

@@ -100,7 +100,7 @@ class TraceTuning(C.Structure):
 
 class ServerDesc(C.Structure):
     _fields_ = [("device", _i), ("flags", C.c_uint32), ("hbm_budget_bytes", C.c_size_t), ("max_batch", _i),
-                ("step_pixels", C.c_int64)]
+                ("step_pixels", C.c_int64), ("age_weight", C.c_float)]
 
 
 class JobDesc(C.Structure):

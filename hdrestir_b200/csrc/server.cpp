@@ -43,6 +43,7 @@ struct Job {
     int32_t frames_done = 0;
     int32_t state = HDR_JOB_QUEUED;
     size_t bytes = 0;  // admission estimate of its device buffers
+    int64_t rendered_at_submit = 0;  // hdr_server::rendered when the job was submitted
 };
 
 size_t pixels_of(const hdr_job_desc &d) { return (size_t)d.camera.width * (size_t)d.camera.height; }
@@ -71,6 +72,8 @@ struct hdr_server {
     size_t in_use = 0;
     int max_batch = 64;
     int64_t step_pixels = 0;
+    double age_weight = 0.5;
+    int64_t rendered = 0;  // pixels of every frame the server has rendered (its work clock)
     std::vector<hdr_ctx *> scenes;  // one owner ctx per uploaded scene
     std::deque<std::unique_ptr<Job>> queued;
     std::vector<std::unique_ptr<Job>> active;
@@ -185,6 +188,7 @@ hdr_status hdr_server_create(hdr_server **out, const hdr_server_desc *desc) {
     sv->budget = desc->hbm_budget_bytes;
     sv->max_batch = desc->max_batch > 0 ? desc->max_batch : 64;
     sv->step_pixels = desc->step_pixels > 0 ? desc->step_pixels : 0;
+    sv->age_weight = desc->age_weight > 0.0f ? desc->age_weight : (desc->age_weight < 0.0f ? 0.0 : 0.5);
     *out = sv;
     return HDR_OK;
 }
@@ -229,6 +233,7 @@ hdr_status hdr_server_submit(hdr_server *sv, const hdr_job_desc *job, int64_t *j
         return hdr::set_last_error(HDR_EINVAL, "bad frame size %dx%d", job->camera.width, job->camera.height);
     auto j = std::make_unique<Job>();
     j->id = sv->next_id++;
+    j->rendered_at_submit = sv->rendered;
     j->d = *job;
     j->bytes = job_bytes(*job);
     if (sv->budget && j->bytes > sv->budget)
@@ -247,18 +252,26 @@ hdr_status hdr_server_step(hdr_server *sv, int32_t *jobs_finished) {
     if (st != HDR_OK) return st;
     if (sv->active.empty()) return HDR_OK;
     const bool serial = (sv->flags & HDR_SERVER_SERIAL) != 0;
-    // this step's jobs: all admitted ones, or the least remaining work first up to step_pixels
+    // this step's jobs: all admitted ones, or by priority up to step_pixels. Key: remaining work
+    // less a credit for the work served since the job arrived. Least remaining work alone gives
+    // the best median latency, but a large job that arrives early waits behind every later small
+    // one and finishes last, so the tail is worse than one job at a time; the credit, measured on
+    // the server's own work clock (pixels rendered, so an idle server ages nothing), bounds that.
     std::vector<Job *> run;
     for (auto &j : sv->active) run.push_back(j.get());
     if (sv->step_pixels > 0) {
-        auto left = [](const Job *j) { return (int64_t)(j->d.frames - j->frames_done) * (int64_t)pixels_of(j->d); };
-        std::stable_sort(run.begin(), run.end(), [&](const Job *a, const Job *b) { return left(a) < left(b); });
+        auto key = [sv](const Job *j) {
+            return (double)(j->d.frames - j->frames_done) * (double)pixels_of(j->d) -
+                   sv->age_weight * (double)(sv->rendered - j->rendered_at_submit);
+        };
+        std::stable_sort(run.begin(), run.end(), [&](const Job *a, const Job *b) { return key(a) < key(b); });
         int64_t px = 0;
         size_t k = 0;
         while (k < run.size() && (k == 0 || px + (int64_t)pixels_of(run[k]->d) <= sv->step_pixels))
             px += (int64_t)pixels_of(run[k++]->d);
         run.resize(k);
     }
+    for (const Job *j : run) sv->rendered += (int64_t)pixels_of(j->d);
     // 1. primary rays, each job on its own stream
     for (Job *j : run)
         if (hdr_raycast(j->ctx, &j->d.camera, j->frames_done, 0) != HDR_OK) fail_job(sv, *j);

@@ -14,11 +14,11 @@ from .scene import Camera, Scene
 
 class Server:
     def __init__(self, device: int = 0, hbm_budget: int = 0, max_batch: int = 0, serial: bool = False,
-                 step_pixels: int = 0):
+                 step_pixels: int = 0, age_weight: float = 0.0):
         self._lib = abi.lib()
         self._h = C.c_void_p()
         d = abi.ServerDesc(int(device), abi.SERVER_SERIAL if serial else 0, int(hbm_budget), int(max_batch),
-                           int(step_pixels))
+                           int(step_pixels), float(age_weight))
         abi.check(self._lib.hdr_server_create(C.byref(self._h), C.byref(d)))
         self._sizes: dict[int, tuple[int, int]] = {}
 

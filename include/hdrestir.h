@@ -439,7 +439,8 @@ hdr_status hdr_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_camer
  * per Hydra delegate). Scenes are uploaded once and shared; jobs are admitted
  * first-in first-out while the estimate of their frame buffers fits the HBM
  * budget; each hdr_server_step advances admitted jobs by one frame (all of
- * them, or those with the least remaining work up to step_pixels), with the
+ * them, or up to step_pixels of them by priority: least remaining work, less
+ * a credit that grows with the work served since the job arrived), with the
  * RIS jobs of one scene traced in one batched launch and path-traced jobs
  * side by side on their own streams. Accumulation follows GpuAccumulationPass
  * (HDR_ACCUM_SHADER). HDR_SERVER_SERIAL runs one job at a time, each frame
@@ -455,7 +456,10 @@ typedef struct hdr_server_desc {
     size_t hbm_budget_bytes;   /* admission budget for the jobs' frame buffers, 0 = unlimited */
     int32_t max_batch;         /* images per batched RIS launch, 0 = 64 */
     int64_t step_pixels;       /* pixels rendered per step, 0 = every admitted job; the jobs with the
-                                  least remaining work (frames left x pixels) go first */
+                                  lowest key go first: remaining work (frames left x pixels) less
+                                  age_weight x the pixels the server rendered since the job's submission */
+    float age_weight;          /* 0 = 0.5; negative = no credit (least remaining work first). The credit
+                                  keeps early large jobs from waiting behind every later small one */
 } hdr_server_desc;
 
 enum { HDR_JOB_PATH_TRACER = 0, HDR_JOB_RIS = 1 };

@@ -124,3 +124,28 @@ def test_reused_contexts_give_the_images_of_fresh_ones(serial):
             got = sv.take(jid)
             want = _alone(s2, cam, fr, pipe, kw)
             assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.parametrize("age_weight,big_last", [(-1.0, True), (0.0, False)])
+def test_age_credit_bounds_the_wait_of_an_early_large_job(age_weight, big_last):
+    """One job per step (step_pixels below every job's size), a large job submitted first and a
+    small one arriving at every step. Least remaining work alone (age_weight < 0) runs the large
+    job only after the small ones stop arriving; with the default credit (half the pixels served
+    since it arrived) it finishes while they still arrive."""
+    s2, _, _ = _scenes()
+    with Server(device=0, step_pixels=256, age_weight=age_weight) as sv:
+        sid = sv.add_scene(s2)
+        big = sv.submit(sid, configs.orbit_camera(0.0, 32, 32), 4, "ris", **RIS)
+        small = configs.orbit_camera(1.0, 16, 16)
+        order = []
+        for _ in range(60):
+            sv.submit(sid, small, 1, "ris", **RIS)
+            sv.step()
+            order += sv.finished()
+        for _ in range(10):
+            sv.step()
+            order += sv.finished()
+        assert len(order) == 61
+    assert (order[-1] == big) == big_last
+    if not big_last:  # 4096 px of work starts once its credit has passed 3,840 px: after 30 small jobs
+        assert order.index(big) < 40
