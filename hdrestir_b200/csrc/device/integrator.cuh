@@ -296,7 +296,7 @@ __device__ inline Spec mis_direct_li(const DeviceScene &s, const Surface &sf, bo
     const MisNeePart nee = mis_nee_part(s, sf, has_conn, sc, rng);
     Spec total = spec(0.0f);
     if (nee.cast && !occluded(s, nee.o, nee.d, nee.limit, err)) total = total + nee.add;
-    if (s.sky) {  // the physical sky's sun, after the sampler's candidate
+    if (sky_on(s)) {  // the physical sky's sun, after the sampler's candidate
         const MisNeePart sun = mis_sky_part(s, sf, sc);
         if (sun.cast && !occluded(s, sun.o, sun.d, sun.limit, err)) total = total + sun.add;
     }

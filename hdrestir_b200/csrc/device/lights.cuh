@@ -18,7 +18,17 @@
 #include "sky.cuh"
 #include "traverse.cuh"
 
+// HDR_SKY 0 compiles the light code without the physical sky, for kernels whose
+// launchers never take a scene with it (the wavefront forms): they keep the
+// registers they had without it.
+#ifndef HDR_SKY
+#define HDR_SKY 1
+#endif
+
 namespace hdr {
+
+// the scene renders under the physical sky (and this build has its code)
+__device__ __forceinline__ bool sky_on(const DeviceScene &s) { return HDR_SKY && s.sky; }
 
 constexpr int kLightDistant = 0, kLightDome = 1, kLightRect = 2, kLightPoint = 3;
 
@@ -38,7 +48,7 @@ __device__ __forceinline__ bool light_is_delta(const DeviceScene &s, int li) {
 // ---- PhysicalSky as a light (physical_sky.cpp:161-187) ----------------------
 // SampleLight: the sun, the same sample for every point (no random numbers).
 __device__ __forceinline__ bool sky_sun_sample(const DeviceScene &s, LightSampleD &ls) {
-    if (!s.sky || s.sky_sun.w == 0.0f) return false;
+    if (!sky_on(s) || s.sky_sun.w == 0.0f) return false;
     const V3 d{s.sky_sun.x, s.sky_sun.y, s.sky_sun.z};
     ls = LightSampleD{d, V3{s.sky_sun_color.x, s.sky_sun_color.y, s.sky_sun_color.z}, -d, 1e30f, 1.0f, true};
     return true;
@@ -85,12 +95,12 @@ __device__ __forceinline__ float dome_lum_pdf(const DeviceScene &s, V3 texel) {
 }
 // Scene::GetEnvironment (scene.cpp:248-268): the physical sky when enabled, else
 // the first dome light, else none.
-__device__ __forceinline__ bool env_present(const DeviceScene &s) { return s.sky || s.env_light >= 0; }
+__device__ __forceinline__ bool env_present(const DeviceScene &s) { return sky_on(s) || s.env_light >= 0; }
 // The environment's light index in a candidate (the dome's; the sky has none)
-__device__ __forceinline__ int env_light_index(const DeviceScene &s) { return s.sky ? -1 : s.env_light; }
+__device__ __forceinline__ int env_light_index(const DeviceScene &s) { return sky_on(s) ? -1 : s.env_light; }
 // IEnvironment::Sample (miss radiance)
 __device__ __forceinline__ V3 env_radiance(const DeviceScene &s, V3 dir) {
-    if (s.sky) return sky_radiance(V3{s.sky_sun_n.x, s.sky_sun_n.y, s.sky_sun_n.z}, dir);
+    if (sky_on(s)) return sky_radiance(V3{s.sky_sun_n.x, s.sky_sun_n.y, s.sky_sun_n.z}, dir);
     if (s.env_light < 0 || s.dome_width <= 0) return v3s(0.0f);
     int x, y;
     dome_xy(s, dir, x, y);
@@ -100,7 +110,7 @@ __device__ __forceinline__ V3 env_radiance(const DeviceScene &s, V3 dir) {
 // IEnvironment::EvalPdf(dir): the dome's importance-sampling pdf; the sky's is 0
 // (IEnvironment's default, sceneInterface/environment.h:19-24)
 __device__ __forceinline__ float env_pdf(const DeviceScene &s, V3 dir) {
-    if (s.sky || s.env_light < 0 || s.dome_width <= 0 || s.dome_total_lum <= 0.f) return 0.f;
+    if (sky_on(s) || s.env_light < 0 || s.dome_width <= 0 || s.dome_total_lum <= 0.f) return 0.f;
     int x, y;
     dome_xy(s, dir, x, y);
     return dome_lum_pdf(s, dome_pixel(s, x, y));
@@ -239,7 +249,7 @@ __device__ __forceinline__ float light_select_pdf(const DeviceScene &s) {
 // UniformLightSampler::EvalPdf(*environment): the dome is a scene light, the
 // physical sky is not (so it gets a technique of its own)
 __device__ __forceinline__ float env_select_pdf(const DeviceScene &s) {
-    return (s.sky || s.env_light < 0) ? 0.0f : light_select_pdf(s);
+    return (sky_on(s) || s.env_light < 0) ? 0.0f : light_select_pdf(s);
 }
 
 // The RIS technique split (ris_direct_light_integrator.cpp:89-99): light-sampler

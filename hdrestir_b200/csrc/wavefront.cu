@@ -33,6 +33,7 @@
 #ifndef HDR_WAVE_TEXTURED
 #define HDR_TEXTURES 0
 #endif
+#define HDR_SKY 0  // the launchers never take a scene under the physical sky
 
 #include "device/integrator.cuh"
 #include "device/pixel.cuh"
