@@ -70,10 +70,11 @@ struct DeviceScene {
     // which then walks the reference trees for the rare ray whose answer it cannot vouch for
     int sh4_closest;
     // parent links of the reference trees for that check
-    const int *ref_tlas_parent;  // per TLAS node, -1 at the root
-    const int *ref_inst_leaf;    // per instance: its TLAS leaf
-    const int *ref_blas_parent;  // per BLAS node of all meshes: mesh-local parent, -1 at a root
-    const int *ref_tri_leaf;     // per triangle record: its mesh-local leaf
+    // path records, 2 float4 per node: (box min, parent index bits, -1 at a root), (box max, 0)
+    const float4 *ref_tlas_path;  // per TLAS node
+    const int *ref_inst_leaf;     // per instance: its TLAS leaf
+    const float4 *ref_blas_path;  // per BLAS node of all meshes, mesh-local parents
+    const int *ref_tri_leaf;      // per triangle record: its mesh-local leaf
     // This struct's own copy in device memory. Kernels take the scene by value
     // (parameter space); a non-inlined callee gets this pointer instead of the
     // parameter's address, which would make every thread copy the parameter
@@ -788,21 +789,37 @@ namespace hdr {
 // grazes a box the reference's rounding rejects fails the check.
 __device__ __noinline__ static bool ref_reaches(const DeviceScene *s, V3 o, V3 d, int inst, int tri, float t) {
     const SlabRay wr = make_slab_ray<false>(o, d);
-    for (int n = __ldg(&s->ref_inst_leaf[inst]); n >= 0; n = __ldg(&s->ref_tlas_parent[n])) {
-        const float4 *np = s->tlas_nodes + 2 * (size_t)n;
-        float ta;
-        if (!slab_test(wr, __ldg(np), __ldg(np + 1), ta) || ta > t) return false;
-    }
     const float4 *ip = s->instances + 8 * (size_t)inst;
     const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2), m3 = __ldg(ip + 3);
     const float inv[16] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w,
                            m2.x, m2.y, m2.z, m2.w, m3.x, m3.y, m3.z, m3.w};
     const SlabRay br = make_slab_ray<true>(m4f_transform(inv, o), m4f_transform_dir(inv, d));
     const int node_base = fbits(__ldg(&ip[4].w)), tri_base = fbits(__ldg(&ip[5].w));
-    for (int n = __ldg(&s->ref_tri_leaf[tri_base + tri]); n >= 0; n = __ldg(&s->ref_blas_parent[node_base + n])) {
-        const float4 *np = s->blas_nodes + 2 * (size_t)(node_base + n);
+    // The boxes on these paths are reachable ones, so DeviceScene::proper_boxes lets
+    // the walks' regular slab test stand in for the full one, as in the walks.
+    const bool wreg = s->proper_boxes && !wr.any_small, breg = s->proper_boxes && !br.any_small;
+    // Both paths are climbed together, one level of each per iteration: every level
+    // reads one 32-byte record (the box and the link up), and the two records'
+    // loads are issued together so that their latencies overlap. A finished path
+    // re-reads its last record (in bounds) and tests nothing.
+    int nt = __ldg(&s->ref_inst_leaf[inst]), nb = __ldg(&s->ref_tri_leaf[tri_base + tri]);
+    if (nt < 0 || nb < 0) return false;  // in no leaf of the reference's trees: its walk decides
+    int lt = nt, lb = nb;
+    while (nt >= 0 || nb >= 0) {
+        const float4 *tp = s->ref_tlas_path + 2 * (size_t)(nt >= 0 ? nt : lt);
+        const float4 *bp = s->ref_blas_path + 2 * (size_t)(node_base + (nb >= 0 ? nb : lb));
+        const float4 tlo = __ldg(tp), thi = __ldg(tp + 1), blo = __ldg(bp), bhi = __ldg(bp + 1);
         float ta;
-        if (!slab_test(br, __ldg(np), __ldg(np + 1), ta) || ta > t) return false;
+        if (nt >= 0) {
+            if (!(wreg ? slab_test_regular(wr, tlo, thi, ta) : slab_test(wr, tlo, thi, ta)) || ta > t) return false;
+            lt = nt;
+            nt = __float_as_int(tlo.w);
+        }
+        if (nb >= 0) {
+            if (!(breg ? slab_test_regular(br, blo, bhi, ta) : slab_test(br, blo, bhi, ta)) || ta > t) return false;
+            lb = nb;
+            nb = __float_as_int(blo.w);
+        }
     }
     return true;
 }

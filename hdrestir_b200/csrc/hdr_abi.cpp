@@ -635,15 +635,28 @@ namespace {
 // per TLAS node its parent, per instance its TLAS leaf, per BLAS node (all meshes,
 // mesh-local indices) its parent, per triangle record its mesh-local leaf. Only
 // nodes a walk can reach are linked (-1 elsewhere). Needs the host-built trees.
+// The check's path records: per TLAS node and per BLAS node, 8 floats (32 B, one
+// sector): the node's box min, its parent's index bits (-1 at a root), its box max, 0.
 struct RefLinks {
-    std::vector<int> tlas_parent, inst_leaf, blas_parent, tri_leaf;
+    std::vector<float> tlas_path, blas_path;
+    std::vector<int> inst_leaf, tri_leaf;
 };
+void set_path_record(std::vector<float> &path, size_t n, const float *rec, int parent) {
+    float *p = &path[8 * n];
+    p[0] = rec[0];
+    p[1] = rec[1];
+    p[2] = rec[2];
+    std::memcpy(&p[3], &parent, sizeof(int));
+    p[4] = rec[4];
+    p[5] = rec[5];
+    p[6] = rec[6];
+    p[7] = 0.0f;
+}
 bool build_ref_links(const hdr::FlatScene &f, RefLinks &L) {
     if (f.blas_nodes.empty() || f.tlas_nodes.empty() || f.num_instances <= 0) return false;
     const size_t n_tlas = f.tlas_nodes.size() / 8, n_blas = f.blas_nodes.size() / 8, n_tri = f.tri_geo.size() / 12;
-    L.tlas_parent.assign(n_tlas, -1);
+    std::vector<int> tlas_parent(n_tlas, -1), blas_parent(n_blas, -1);
     L.inst_leaf.assign((size_t)f.num_instances, -1);
-    L.blas_parent.assign(n_blas, -1);
     L.tri_leaf.assign(n_tri, -1);
     auto ibits = [](float v) {
         int i;
@@ -659,7 +672,7 @@ bool build_ref_links(const hdr::FlatScene &f, RefLinks &L) {
         if (left >= 0) {
             for (int ch : {left, left + 1}) {
                 if ((size_t)ch >= n_tlas) return false;
-                L.tlas_parent[(size_t)ch] = n;
+                tlas_parent[(size_t)ch] = n;
                 todo.push_back(ch);
             }
         } else {
@@ -688,7 +701,7 @@ bool build_ref_links(const hdr::FlatScene &f, RefLinks &L) {
             if (left >= 0) {
                 for (int ch : {left, left + 1}) {
                     if ((size_t)node_base + (size_t)ch >= n_blas) return false;
-                    L.blas_parent[(size_t)node_base + (size_t)ch] = m;
+                    blas_parent[(size_t)node_base + (size_t)ch] = m;
                     todo.push_back(ch);
                 }
             } else {
@@ -701,6 +714,10 @@ bool build_ref_links(const hdr::FlatScene &f, RefLinks &L) {
             }
         }
     }
+    L.tlas_path.assign(8 * n_tlas, 0.0f);
+    for (size_t n = 0; n < n_tlas; ++n) set_path_record(L.tlas_path, n, &f.tlas_nodes[8 * n], tlas_parent[n]);
+    L.blas_path.assign(8 * n_blas, 0.0f);
+    for (size_t n = 0; n < n_blas; ++n) set_path_record(L.blas_path, n, &f.blas_nodes[8 * n], blas_parent[n]);
     return true;
 }
 
@@ -886,9 +903,9 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
         store->sh4_blas_depth = sb.blas_depth;
         RefLinks links;  // exact closest hits on the SAH trees (closest_mode 2)
         if (build_ref_links(f, links)) {
-            UP(links.tlas_parent, ref_tlas_parent);
+            UP(links.tlas_path, ref_tlas_path);
             UP(links.inst_leaf, ref_inst_leaf);
-            UP(links.blas_parent, ref_blas_parent);
+            UP(links.blas_path, ref_blas_path);
             UP(links.tri_leaf, ref_tri_leaf);
             store->ref_links = true;
         }
