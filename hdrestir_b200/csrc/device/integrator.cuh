@@ -461,8 +461,13 @@ struct RisCtx {
 
 // Candidate j of allCandidates: NEE (sampler), then sky NEE, then BSDF.
 // kFull = false only advances the stream exactly like the full generation.
+// HDR_CANDIDATE_INLINE: how the including kernels take it (a call returns the
+// candidate through local memory, about 20 stores and loads per candidate).
+#ifndef HDR_CANDIDATE_INLINE
+#define HDR_CANDIDATE_INLINE
+#endif
 template <bool kFull, class RP>
-__device__ Cand ris_candidate(const RisCtx<RP> &x, int j, MtStream &rng, unsigned &err) {
+__device__ HDR_CANDIDATE_INLINE Cand ris_candidate(const RisCtx<RP> &x, int j, MtStream &rng, unsigned &err) {
     const DeviceScene &s = *x.s;
     const Surface &sf = *x.sf;
     const SpectralCtx &sc = *x.sc;

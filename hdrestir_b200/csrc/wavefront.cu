@@ -34,6 +34,7 @@
 #define HDR_TEXTURES 0
 #endif
 #define HDR_SKY 0  // the launchers never take a scene under the physical sky
+#define HDR_CANDIDATE_INLINE __forceinline__
 
 #include "device/integrator.cuh"
 #include "device/pixel.cuh"
