@@ -403,8 +403,8 @@ __device__ inline Spec ris_reevaluate(const DeviceScene &s, const Surface &sf, i
     return rgb_to_spectrum(ls.color, sc.up) * rgb_to_spectrum(bval * n_l, sc.up);
 }
 
-// _evaluateBSDFConnection (:693-780)
-__device__ inline RisContrib ris_evaluate_bsdf_connection(const DeviceScene &s, const Surface &sf, const Connection &cn,
+// _evaluateBSDFConnection (:693-780); HDR_BOUNCE_INLINE as sample_bounce
+__device__ HDR_BOUNCE_INLINE RisContrib ris_evaluate_bsdf_connection(const DeviceScene &s, const Surface &sf, const Connection &cn,
                                                    const RisStrategy &strat, const SpectralCtx &sc) {
     const Bounce &b = cn.b;
     RisContrib r{spec(0.0f), b.integrand, 0.0f, b.pdf, false, true};
@@ -713,7 +713,7 @@ __device__ __forceinline__ bool reprojected_history(const ReprojD &rj, V3 p, Res
 // already knows it (the wavefront generate kernel saved it); NULL replays the
 // sampling decisions to find it.
 template <class RP>
-__device__ inline Spec ris_direct_li(const DeviceScene &s, const RP &rp, const Surface &sf, bool has_conn,
+__device__ HDR_BOUNCE_INLINE Spec ris_direct_li(const DeviceScene &s, const RP &rp, const Surface &sf, bool has_conn,
                                      const Connection &cn, const SpectralCtx &sc, MtStream &rng, bool primary,
                                      const RisRun &run, const ReservoirView &rv, size_t pixel,
                                      const MtStream *gen_end_state, unsigned &err) {

@@ -436,8 +436,15 @@ __device__ __forceinline__ Bounce specular_bounce(V3 origin, V3 dir, Spec tmul, 
     return r;
 }
 
+// HDR_BOUNCE_INLINE: how the including kernels take sample_bounce and the RIS
+// pass's direct-light estimate and BSDF-connection evaluation (a call keeps the
+// closure, surface, spectral context and random stream it is given in local
+// memory).
+#ifndef HDR_BOUNCE_INLINE
+#define HDR_BOUNCE_INLINE inline
+#endif
 // IMaterial::SampleBounce dispatch
-__device__ inline Bounce sample_bounce(const Closure &c, V3 sn, bool inside, V3 hit_pos, V3 ray_dir, int max_refl,
+__device__ HDR_BOUNCE_INLINE Bounce sample_bounce(const Closure &c, V3 sn, bool inside, V3 hit_pos, V3 ray_dir, int max_refl,
                                 int max_refr, BounceState &st, const SpectralCtx &sc, MtStream &rng) {
     if (c.is_default) return sample_bounce_default(c, sn, hit_pos, sc, rng);
     // --- coat (preview_surface.cpp:136-196)

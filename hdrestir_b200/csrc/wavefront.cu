@@ -35,6 +35,7 @@
 #endif
 #define HDR_SKY 0  // the launchers never take a scene under the physical sky
 #define HDR_CANDIDATE_INLINE __forceinline__
+#define HDR_BOUNCE_INLINE __forceinline__
 
 #include "device/integrator.cuh"
 #include "device/pixel.cuh"
@@ -56,9 +57,15 @@ __device__ __forceinline__ int queue_append(int *counter, bool want) {
     return base + __popc(mask & ((1u << lane) - 1u));
 }
 
-__global__ void __launch_bounds__(256) ris_generate_kernel(DeviceScene s, CameraD cam, int frame_arg, PathRun pr,
-                                                           RisRun ris, GBufferView gb, WaveBuffers wb, float4 *color,
-                                                           int trace_level, unsigned *err) {
+// Kernel parameters of struct type are __grid_constant__: code that takes their
+// address (a reference kept in a struct, a call) reads the parameter space
+// instead of a per-thread copy in local memory (a few hundred bytes written per
+// thread).
+__global__ void __launch_bounds__(256)
+    ris_generate_kernel(const __grid_constant__ DeviceScene s, const __grid_constant__ CameraD cam, int frame_arg,
+                        const __grid_constant__ PathRun pr, const __grid_constant__ RisRun ris,
+                        const __grid_constant__ GBufferView gb, const __grid_constant__ WaveBuffers wb, float4 *color,
+                        int trace_level, unsigned *err) {
     uint64_t spill[312];
     MtStream rng;
     PixelStart ps;
@@ -498,10 +505,11 @@ __global__ void __launch_bounds__(kTraceThreads) trace_shadow_kernel(DeviceScene
 }
 
 template <int kThreads, int kMinBlocks>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) ris_shade_kernel(DeviceScene s, CameraD cam, int frame_arg,
-                                                                         PathRun pr, RisRun ris, GBufferView gb,
-                                                                         ReservoirView rv, WaveBuffers wb, float4 *color,
-                                                                         int trace_level, unsigned *err) {
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    ris_shade_kernel(const __grid_constant__ DeviceScene s, const __grid_constant__ CameraD cam, int frame_arg,
+                     const __grid_constant__ PathRun pr, const __grid_constant__ RisRun ris,
+                     const __grid_constant__ GBufferView gb, const __grid_constant__ ReservoirView rv,
+                     const __grid_constant__ WaveBuffers wb, float4 *color, int trace_level, unsigned *err) {
     uint64_t spill[312];
     MtStream rng;
     PixelStart ps;
