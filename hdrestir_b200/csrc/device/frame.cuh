@@ -130,7 +130,7 @@ constexpr int kTraceLanePerRay = 1, kTraceUnphased = 2, kTraceSplitStack = 4;
 constexpr int kShadowShapes = 3;
 struct TraceTuning {
     int mode = 0;
-    int node_quorum = 16;
+    int node_quorum = 12;  // best for the SAH-tree walks (16 for the reference-tree ones)
     int blocks_per_sm = 16;
     int sm_count = 148;
     int shade_shape = 3;  // ris_shade launch shape, 0 .. kShadeShapes - 1 (128 x 4: fastest at 1080p)
