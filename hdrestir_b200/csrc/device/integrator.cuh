@@ -291,7 +291,7 @@ __device__ inline Spec mis_conn_part(const DeviceScene &s, Spec total, bool has_
 
 
 // MisDirectLightIntegrator::Li (per-bounce form, :250-269) = _integrateNEE + _integrateBSDFConnection
-__device__ inline Spec mis_direct_li(const DeviceScene &s, const Surface &sf, bool has_conn, const Connection &cn,
+__device__ HDR_BOUNCE_INLINE Spec mis_direct_li(const DeviceScene &s, const Surface &sf, bool has_conn, const Connection &cn,
                                      const SpectralCtx &sc, MtStream &rng, unsigned &err) {
     const MisNeePart nee = mis_nee_part(s, sf, has_conn, sc, rng);
     Spec total = spec(0.0f);

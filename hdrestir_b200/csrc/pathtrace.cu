@@ -19,6 +19,9 @@
 // reaches draw 250 would soon need its full 312-word state, which does not
 // travel between kernels: such a path is finished in the connect kernel's
 // thread, by the one-thread loop (path_li_continue).
+// bounce sampling and the NEE estimate inlined: as calls they keep the surface,
+// closure, spectral context and random stream they are given in local memory
+#define HDR_BOUNCE_INLINE __forceinline__
 #include "device/integrator.cuh"
 
 namespace hdr {
@@ -123,8 +126,8 @@ __device__ __noinline__ Spec pt_finish_in_thread(const DeviceScene *s, Spec tota
 }
 
 template <bool kBatch>
-__global__ void __launch_bounds__(256) pt_start_kernel(DeviceScene s, PtJobD one, const PtJobD *table, int n_jobs,
-                                                       PtBuffers B) {
+__global__ void __launch_bounds__(256) pt_start_kernel(const __grid_constant__ DeviceScene s, const __grid_constant__ PtJobD one, const PtJobD *table,
+                                                       int n_jobs, const __grid_constant__ PtBuffers B) {
     const int jk = kBatch ? job_of_block(table, n_jobs) : 0;
     const PtJobD &job = kBatch ? table[jk] : one;
     const CameraD &cam = job.cam;
@@ -170,7 +173,7 @@ __global__ void __launch_bounds__(256) pt_start_kernel(DeviceScene s, PtJobD one
 }
 
 // vertex v >= 1 of the paths in `list` (their extension hit is in the hit slots)
-__global__ void __launch_bounds__(256) pt_sample_kernel(DeviceScene s, PathRun pr, PtBuffers B, const int *list,
+__global__ void __launch_bounds__(256) pt_sample_kernel(const __grid_constant__ DeviceScene s, const __grid_constant__ PathRun pr, const __grid_constant__ PtBuffers B, const int *list,
                                                         const int *count, unsigned *err) {
     const int n = *count;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -198,8 +201,8 @@ __global__ void __launch_bounds__(256) pt_sample_kernel(DeviceScene s, PathRun p
 // vertex v of the paths in `list`: the vertex's direct light, then the path goes
 // on (appended to `next`) or ends (its colour written)
 template <bool kBatch>
-__global__ void __launch_bounds__(256) pt_connect_kernel(DeviceScene s, PtJobD one, const PtJobD *table, PathRun pr,
-                                                         PtBuffers B, const int *list, const int *count, int *next,
+__global__ void __launch_bounds__(256) pt_connect_kernel(const __grid_constant__ DeviceScene s, const __grid_constant__ PtJobD one, const PtJobD *table,
+                                                         const __grid_constant__ PathRun pr, const __grid_constant__ PtBuffers B, const int *list, const int *count, int *next,
                                                          int *next_count, int vertex, unsigned *err) {
     const int n = *count;
     unsigned e = 0;
