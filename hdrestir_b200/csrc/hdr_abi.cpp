@@ -652,38 +652,54 @@ void set_path_record(std::vector<float> &path, size_t n, const float *rec, int p
     p[6] = rec[6];
     p[7] = 0.0f;
 }
-bool build_ref_links(const hdr::FlatScene &f, RefLinks &L) {
-    if (f.blas_nodes.empty() || f.tlas_nodes.empty() || f.num_instances <= 0) return false;
-    const size_t n_tlas = f.tlas_nodes.size() / 8, n_blas = f.blas_nodes.size() / 8, n_tri = f.tri_geo.size() / 12;
-    std::vector<int> tlas_parent(n_tlas, -1), blas_parent(n_blas, -1);
-    L.inst_leaf.assign((size_t)f.num_instances, -1);
-    L.tri_leaf.assign(n_tri, -1);
-    auto ibits = [](float v) {
-        int i;
-        std::memcpy(&i, &v, sizeof(i));
-        return i;
-    };
+int float_bits(float v) {
+    int i;
+    std::memcpy(&i, &v, sizeof(i));
+    return i;
+}
+// The TLAS half of the links: a path record per node (n_tlas of the 8-float nodes)
+// and each instance's leaf, from a walk of the tree as it is now. False when the
+// tree does not fit the records or names an instance outside the scene.
+bool tlas_links(const float *nodes, size_t n_tlas, const int *tlas_inst, size_t n_tlas_inst, int num_instances,
+                std::vector<float> &path, std::vector<int> &inst_leaf) {
+    std::vector<int> parent(n_tlas, -1);
+    inst_leaf.assign((size_t)num_instances, -1);
     std::vector<int> todo{0};
     while (!todo.empty()) {
         const int n = todo.back();
         todo.pop_back();
-        const float *rec = &f.tlas_nodes[8 * (size_t)n];
-        const int left = ibits(rec[3]), count = ibits(rec[7]);
+        const float *rec = &nodes[8 * (size_t)n];
+        const int left = float_bits(rec[3]), count = float_bits(rec[7]);
         if (left >= 0) {
             for (int ch : {left, left + 1}) {
                 if ((size_t)ch >= n_tlas) return false;
-                tlas_parent[(size_t)ch] = n;
+                parent[(size_t)ch] = n;
                 todo.push_back(ch);
             }
         } else {
             const int first = -left - 1;
             for (int k = 0; k < count; ++k) {
-                const int ii = f.tlas_inst[(size_t)(first + k)];
-                if (ii < 0 || ii >= f.num_instances) return false;
-                L.inst_leaf[(size_t)ii] = n;
+                if (first < 0 || (size_t)(first + k) >= n_tlas_inst) return false;
+                const int ii = tlas_inst[(size_t)(first + k)];
+                if (ii < 0 || ii >= num_instances) return false;
+                inst_leaf[(size_t)ii] = n;
             }
         }
     }
+    path.assign(8 * n_tlas, 0.0f);
+    for (size_t n = 0; n < n_tlas; ++n) set_path_record(path, n, &nodes[8 * n], parent[n]);
+    return true;
+}
+bool build_ref_links(const hdr::FlatScene &f, RefLinks &L) {
+    if (f.blas_nodes.empty() || f.tlas_nodes.empty() || f.num_instances <= 0) return false;
+    const size_t n_tlas = f.tlas_nodes.size() / 8, n_blas = f.blas_nodes.size() / 8, n_tri = f.tri_geo.size() / 12;
+    std::vector<int> blas_parent(n_blas, -1);
+    L.tri_leaf.assign(n_tri, -1);
+    auto ibits = float_bits;
+    if (!tlas_links(f.tlas_nodes.data(), n_tlas, f.tlas_inst.data(), f.tlas_inst.size(), f.num_instances, L.tlas_path,
+                    L.inst_leaf))
+        return false;
+    std::vector<int> todo;
     std::vector<char> done_mesh(n_blas + 1, 0);
     for (int i = 0; i < f.num_instances; ++i) {  // each mesh's tree once, from its instances' bases
         const float *ir = &f.instances[32 * (size_t)i];
@@ -714,8 +730,6 @@ bool build_ref_links(const hdr::FlatScene &f, RefLinks &L) {
             }
         }
     }
-    L.tlas_path.assign(8 * n_tlas, 0.0f);
-    for (size_t n = 0; n < n_tlas; ++n) set_path_record(L.tlas_path, n, &f.tlas_nodes[8 * n], tlas_parent[n]);
     L.blas_path.assign(8 * n_blas, 0.0f);
     for (size_t n = 0; n < n_blas; ++n) set_path_record(L.blas_path, n, &f.blas_nodes[8 * n], blas_parent[n]);
     return true;
@@ -1500,9 +1514,32 @@ hdr_status hdr_scene_set_instance_transforms(hdr_ctx *c, const float *transforms
             store->sh4 = false;  // too deep for the shadow walk's stack: the reference trees serve shadow rays
         }
     }
-    // the reference TLAS changed on the device: its parent links no longer describe it, so
-    // closest hits go back to the reference walk for this scene
-    store->ref_links = false;
+    // the reference TLAS changed on the device: its path records are rebuilt from it (the BLAS
+    // ones still hold); if the new tree does not fit them, closest hits go back to the reference
+    // walk for this scene
+    if (store->ref_links && store->sh4) {
+        const size_t n_rec = store->arrays["ref_tlas_path"].second / 32;
+        const size_t n_nodes = std::min(n_rec, (size_t)store->tlas_capacity);
+        std::vector<float> nodes(8 * n_nodes);
+        std::vector<int> tlas_inst((size_t)num_instances), inst_leaf;
+        std::vector<float> path;
+        HDR_CUDA(cudaMemcpyAsync(nodes.data(), s.tlas_nodes, nodes.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                                 c->stream));
+        HDR_CUDA(cudaMemcpyAsync(tlas_inst.data(), s.tlas_inst, tlas_inst.size() * sizeof(int),
+                                 cudaMemcpyDeviceToHost, c->stream));
+        HDR_CUDA(cudaStreamSynchronize(c->stream));
+        store->ref_links =
+            tlas_links(nodes.data(), n_nodes, tlas_inst.data(), tlas_inst.size(), num_instances, path, inst_leaf);
+        if (store->ref_links) {
+            HDR_CUDA(cudaMemcpyAsync(const_cast<float4 *>(s.ref_tlas_path), path.data(), path.size() * sizeof(float),
+                                     cudaMemcpyHostToDevice, c->stream));
+            HDR_CUDA(cudaMemcpyAsync(const_cast<int *>(s.ref_inst_leaf), inst_leaf.data(),
+                                     inst_leaf.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+            HDR_CUDA(cudaStreamSynchronize(c->stream));  // host buffers
+        }
+    } else {
+        store->ref_links = false;
+    }
     s.sh4 = (store->sh4 && !(c->flags & HDR_CTX_REFERENCE_SHADOWS)) ? 1 : 0;
     s.sh4_closest = closest_mode(c->flags, s.sh4, store->ref_links);
     s.dev = store->desc_dev + desc_index(s);
