@@ -690,9 +690,11 @@ bool tlas_links(const float *nodes, size_t n_tlas, const int *tlas_inst, size_t 
     for (size_t n = 0; n < n_tlas; ++n) set_path_record(path, n, &nodes[8 * n], parent[n]);
     return true;
 }
-bool build_ref_links(const hdr::FlatScene &f, RefLinks &L) {
-    if (f.blas_nodes.empty() || f.tlas_nodes.empty() || f.num_instances <= 0) return false;
-    const size_t n_tlas = f.tlas_nodes.size() / 8, n_blas = f.blas_nodes.size() / 8, n_tri = f.tri_geo.size() / 12;
+// blas_nodes: every mesh's BLAS nodes (8 floats each, the host build's or a copy of the device
+// build's); n_tri: the triangle records.
+bool build_ref_links(const hdr::FlatScene &f, const std::vector<float> &blas_nodes, size_t n_tri, RefLinks &L) {
+    if (blas_nodes.empty() || f.tlas_nodes.empty() || f.num_instances <= 0) return false;
+    const size_t n_tlas = f.tlas_nodes.size() / 8, n_blas = blas_nodes.size() / 8;
     std::vector<int> blas_parent(n_blas, -1);
     L.tri_leaf.assign(n_tri, -1);
     auto ibits = float_bits;
@@ -712,7 +714,7 @@ bool build_ref_links(const hdr::FlatScene &f, RefLinks &L) {
             todo.pop_back();
             const size_t g = (size_t)node_base + (size_t)m;
             if (g >= n_blas) return false;
-            const float *rec = &f.blas_nodes[8 * g];
+            const float *rec = &blas_nodes[8 * g];
             const int left = ibits(rec[3]), count = ibits(rec[7]);
             if (left >= 0) {
                 for (int ch : {left, left + 1}) {
@@ -731,7 +733,7 @@ bool build_ref_links(const hdr::FlatScene &f, RefLinks &L) {
         }
     }
     L.blas_path.assign(8 * n_blas, 0.0f);
-    for (size_t n = 0; n < n_blas; ++n) set_path_record(L.blas_path, n, &f.blas_nodes[8 * n], blas_parent[n]);
+    for (size_t n = 0; n < n_blas; ++n) set_path_record(L.blas_path, n, &blas_nodes[8 * n], blas_parent[n]);
     return true;
 }
 
@@ -916,7 +918,15 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
         store->sh4_tlas_capacity = sb.tlas_capacity;
         store->sh4_blas_depth = sb.blas_depth;
         RefLinks links;  // exact closest hits on the SAH trees (closest_mode 2)
-        if (build_ref_links(f, links)) {
+        std::vector<float> dev_nodes;  // a device build's BLAS nodes, copied back for the links
+        if (device_build && f.num_blas_nodes > 0) {
+            dev_nodes.resize((size_t)f.num_blas_nodes * 8);
+            HDR_CUDA(cudaMemcpyAsync(dev_nodes.data(), s.blas_nodes, dev_nodes.size() * sizeof(float),
+                                     cudaMemcpyDeviceToHost, c->stream));
+            HDR_CUDA(cudaStreamSynchronize(c->stream));
+        }
+        if (build_ref_links(f, device_build ? dev_nodes : f.blas_nodes,
+                            device_build ? (size_t)f.num_triangles : f.tri_geo.size() / 12, links)) {
             UP(links.tlas_path, ref_tlas_path);
             UP(links.inst_leaf, ref_inst_leaf);
             UP(links.blas_path, ref_blas_path);

@@ -321,9 +321,7 @@ typedef struct hdr_gbuffer_texel {
                                      way down to it in the reference's own trees must pass the
                                      reference's slab test no farther than the hit; a ray that
                                      fails the check walks the reference's trees. The answer is
-                                     then the reference's bit for bit. Scenes whose trees were
-                                     built on the device (HDR_CTX_DEVICE_BUILD) walk the reference
-                                     trees. */
+                                     then the reference's bit for bit. */
 #define HDR_CTX_REFERENCE_CLOSEST 2048u /* closest hits walk the reference's trees only (for A/B
                                      checks; same answers as the default) */
 #define HDR_CTX_RECORD_LIGHTS 256u /* diagnostic, no reference counterpart: the wavefront
