@@ -17,6 +17,7 @@ HDR_OK, HDR_EINVAL, HDR_ENOMEM, HDR_ECANCELLED, HDR_ETIMEOUT, HDR_ECUDA, HDR_ENO
 STATUS_NAMES = {0: "HDR_OK", 1: "HDR_EINVAL", 2: "HDR_ENOMEM", 3: "HDR_ECANCELLED", 4: "HDR_ETIMEOUT",
                 5: "HDR_ECUDA", 6: "HDR_ENOSCENE", 7: "HDR_EDEVICE"}
 LIGHT_DISTANT, LIGHT_DOME, LIGHT_RECT, LIGHT_POINT = 0, 1, 2, 3
+LIGHT_TRIANGLE = 4  # extension: an emissive triangle (half of the rect of the same size)
 AOV_DEPTH, AOV_ALBEDO, AOV_NORMAL = 1, 2, 4
 ACCUM_PARITY, ACCUM_SHADER = 0, 1
 CTX_TIMINGS, CTX_WIDE_BVH, CTX_LANE_PER_RAY, CTX_UNPHASED, CTX_PT_ONE_KERNEL = 1, 2, 8, 16, 32

@@ -31,6 +31,7 @@ namespace hdr {
 __device__ __forceinline__ bool sky_on(const DeviceScene &s) { return HDR_SKY && s.sky; }
 
 constexpr int kLightDistant = 0, kLightDome = 1, kLightRect = 2, kLightPoint = 3;
+constexpr int kLightTriangle = 4;  // extension: HDR_LIGHT_TRIANGLE
 
 struct LightSampleD {  // LightSample
     V3 dir, color, normal;
@@ -123,9 +124,15 @@ __device__ inline bool sample_light(const DeviceScene &s, int li, V3 hit_pos, Mt
     const int type = fbits(a.x);
     const V3 color{b.x, b.y, b.z};
     const V3 lnormal{c.x, c.y, c.z};
-    if (type == kLightRect) {
-        const float u = rng.next_float() - 0.5f;
-        const float v = rng.next_float() - 0.5f;
+    if (type == kLightRect || type == kLightTriangle) {
+        float u = rng.next_float();
+        float v = rng.next_float();
+        if (type == kLightTriangle && u + v > 1.0f) {  // the lower-left half of the unit square, folded
+            u = 1.0f - u;
+            v = 1.0f - v;
+        }
+        u -= 0.5f;
+        v -= 0.5f;
         float m[16];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -136,7 +143,7 @@ __device__ inline bool sample_light(const DeviceScene &s, int li, V3 hit_pos, Mt
         const V3 to_light = lpos - hit_pos;
         const float dist = length(to_light);
         const V3 ldir = div_d(to_light, (double)dist);
-        const float area = a.z * a.w;
+        const float area = type == kLightTriangle ? 0.5f * (a.z * a.w) : a.z * a.w;
         if (area <= 0.0f) return false;
         const float cos_l = smaxf(0.0f, dot(lnormal, -ldir));
         if (cos_l <= 0.0f) return false;
@@ -197,7 +204,7 @@ __device__ inline bool sample_light(const DeviceScene &s, int li, V3 hit_pos, Mt
 // Number of random numbers SampleLight consumes (for replaying a stream).
 __device__ __forceinline__ int light_sample_draws(const DeviceScene &s, int li) {
     const int type = light_type(s, li);
-    if (type == kLightRect) return 2;
+    if (type == kLightRect || type == kLightTriangle) return 2;
     if (type == kLightDome) return (s.dome_width > 0 && li == s.env_light) ? 2 : 0;
     return 0;
 }
@@ -206,8 +213,8 @@ __device__ __forceinline__ int light_sample_draws(const DeviceScene &s, int li) 
 __device__ __forceinline__ void light_eval_pdf(const DeviceScene &s, int li, V3 dir, float &value, bool &solid) {
     const float4 a = __ldg(&s.lights[12 * li]);
     const int type = fbits(a.x);
-    if (type == kLightRect) {
-        const float area = a.z * a.w;
+    if (type == kLightRect || type == kLightTriangle) {
+        const float area = type == kLightTriangle ? 0.5f * (a.z * a.w) : a.z * a.w;
         value = area <= 0.f ? 0.f : 1.f / area;
         solid = false;
     } else if (type == kLightDome) {

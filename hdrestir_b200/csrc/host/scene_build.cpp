@@ -404,7 +404,7 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
     out.lights.assign((size_t)desc.num_lights * kLightFloats, 0.0f);
     for (int i = 0; i < desc.num_lights; ++i) {
         const hdr_light_desc &L = desc.lights[i];
-        if (L.type < HDR_LIGHT_DISTANT || L.type > HDR_LIGHT_POINT) {
+        if (L.type < HDR_LIGHT_DISTANT || L.type > HDR_LIGHT_TRIANGLE) {
             err = "light " + std::to_string(i) + ": unknown type";
             return false;
         }
@@ -414,7 +414,7 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
         const float eff = L.intensity * std::exp2(L.exposure);       // LightParams::EffectiveIntensity
         const V3 color = V3{L.color[0], L.color[1], L.color[2]} * eff;
         const V3 lnormal = normalized(m4f_transform_dir(M, V3{0.0f, 0.0f, -1.0f}));
-        const float area = L.width * L.height;
+        const float area = L.type == HDR_LIGHT_TRIANGLE ? 0.5f * (L.width * L.height) : L.width * L.height;
         const float cone_rad = L.shaping_cone_angle * (float)(3.14159265358979323846 / 180.0);
         const float cos_cone = std::cos(cone_rad);
         const float cos_inner = std::cos(cone_rad * (1.0f - L.shaping_cone_softness));

@@ -162,7 +162,12 @@ typedef struct hdr_mtl_textures {  /* asset paths per HDR_TEX_* slot ("" = none)
 } hdr_mtl_textures;
 
 /* LightType order of scene/light_factory.h */
-enum { HDR_LIGHT_DISTANT = 0, HDR_LIGHT_DOME = 1, HDR_LIGHT_RECT = 2, HDR_LIGHT_POINT = 3 };
+/* HDR_LIGHT_TRIANGLE: extension, no reference counterpart (the reference has no emissive-geometry
+ * light): an emissive triangle, the half of the rect of the same width, height and transform
+ * below its diagonal, with local corners (-w/2, -h/2), (w/2, -h/2), (-w/2, h/2); the transform
+ * (affine) places any triangle. One-sided and sampled uniformly over its area like the rect, whose
+ * convention it follows: the area is w * h / 2 in local units. */
+enum { HDR_LIGHT_DISTANT = 0, HDR_LIGHT_DOME = 1, HDR_LIGHT_RECT = 2, HDR_LIGHT_POINT = 3, HDR_LIGHT_TRIANGLE = 4 };
 
 typedef struct hdr_light_desc {
     int32_t type;

@@ -475,14 +475,20 @@ static int sample_light(const orc_scene *s, int li, ov3 hp, orc_rng *r, olsample
     const olight *L = &s->lights[li];
     float m[16];
     light_matrix(L, m);
-    if (L->type == HDR_LIGHT_RECT) {
-        float u = orc_rng_float(r) - 0.5f;
-        float v = orc_rng_float(r) - 0.5f;
+    if (L->type == HDR_LIGHT_RECT || L->type == HDR_LIGHT_TRIANGLE) {
+        float u = orc_rng_float(r);
+        float v = orc_rng_float(r);
+        if (L->type == HDR_LIGHT_TRIANGLE && u + v > 1.0f) { /* extension: the folded half square */
+            u = 1.0f - u;
+            v = 1.0f - v;
+        }
+        u -= 0.5f;
+        v -= 0.5f;
         ov3 lp = m4f_xform(m, V(u * L->width, v * L->height, 0.0f));
         ov3 tl = vsub(lp, hp);
         float dist = vlen(tl);
         ov3 ld = vdivd(tl, (double)dist);
-        float area = L->width * L->height;
+        float area = L->type == HDR_LIGHT_TRIANGLE ? 0.5f * (L->width * L->height) : L->width * L->height;
         if (area <= 0.0f) return 0;
         ov3 ln = vnorm(m4f_xdir(m, V(0, 0, -1)));
         float cl = omax(0.0f, vdot(ln, vneg(ld)));
@@ -572,8 +578,8 @@ static int sample_light(const orc_scene *s, int li, ov3 hp, orc_rng *r, olsample
 /* ILight::EvalPdf(hitPos, dir, dist, lightNormal) */
 static void light_eval_pdf(const orc_scene *s, int li, ov3 d, float *val, int *solid) {
     const olight *L = &s->lights[li];
-    if (L->type == HDR_LIGHT_RECT) {
-        float a = L->width * L->height;
+    if (L->type == HDR_LIGHT_RECT || L->type == HDR_LIGHT_TRIANGLE) {
+        float a = L->type == HDR_LIGHT_TRIANGLE ? 0.5f * (L->width * L->height) : L->width * L->height;
         *val = a <= 0.f ? 0.f : 1.f / a;
         *solid = 0;
     } else if (L->type == HDR_LIGHT_DOME) {
