@@ -62,7 +62,8 @@ class MaterialDesc(C.Structure):
 class LightDesc(C.Structure):
     _fields_ = [("type", _i), ("color", _f * 3), ("intensity", _f), ("exposure", _f),
                 ("transform", C.c_double * 16), ("width", _f), ("height", _f), ("shaping_cone_angle", _f),
-                ("shaping_cone_softness", _f), ("texture", _pf), ("tex_width", _i), ("tex_height", _i)]
+                ("shaping_cone_softness", _f), ("texture", _pf), ("tex_width", _i), ("tex_height", _i),
+                ("temperature", _f)]
 
 
 class SceneDesc(C.Structure):

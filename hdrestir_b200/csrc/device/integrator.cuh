@@ -207,7 +207,7 @@ __device__ inline MisNeePart mis_nee_part(const DeviceScene &s, const Surface &s
     const V3 wo = -sf.ray_d;
     const float bpdf = ggx_pdf_f(sf.g, sf.sn, wo, ls.dir);
     const V3 bval = ggx_eval_f(sf.g, sf.sn, wo, ls.dir);
-    const Spec radiance = rgb_to_spectrum(bval, sc.up) * rgb_to_spectrum(ls.color, sc.up) * (n_l / p_nee);
+    const Spec radiance = rgb_to_spectrum(bval, sc.up) * light_emission(s, li, ls.color, sc) * (n_l / p_nee);
     const bool separate_env = env_present(s) && env_select_pdf(s) <= 0.0f;
     const float w = (delta || !has_conn) ? 1.0f
                     : separate_env       ? power_heuristic3(p_nee, 1, 0.0f, 1, bpdf, 1)
@@ -361,7 +361,7 @@ __device__ inline RisContrib ris_evaluate_light_sample(const DeviceScene &s, con
     if (n_l <= 0.0f || p_nee <= 0.0f || (cos_y <= 0.0f && !delta)) return r;
     r.tmul = rgb_to_spectrum(bval * n_l, sc.up);
     if (skip_vis) {
-        r.emission = rgb_to_spectrum(ls.color, sc.up);
+        r.emission = light_emission(s, li, ls.color, sc);
         r.vis_tested = false;
         return r;
     }
@@ -369,7 +369,7 @@ __device__ inline RisContrib ris_evaluate_light_sample(const DeviceScene &s, con
     const float lim = ls.dist - 1e-3f;
     const bool occ = shadow_slot >= 0 ? rp.shadow(shadow_slot, so, ls.dir, lim, err) : rp.winner_shadow(so, ls.dir, lim, err);
     if (occ) return r;
-    r.emission = rgb_to_spectrum(ls.color, sc.up);
+    r.emission = light_emission(s, li, ls.color, sc);
     return r;
 }
 
@@ -400,7 +400,7 @@ __device__ inline Spec ris_reevaluate(const DeviceScene &s, const Surface &sf, i
     const float p_nee = pdf_to_solid_angle(ls.pdf, ls.pdf_solid_angle, dist2, smaxf(cos_y, 1e-6f));
     if (n_l <= 0.0f || p_nee <= 0.0f || (cos_y <= 0.0f && !light_is_delta(s, li))) return spec(0.0f);
     const V3 bval = ggx_eval_f(sf.g, sf.sn, wo, ls.dir);
-    return rgb_to_spectrum(ls.color, sc.up) * rgb_to_spectrum(bval * n_l, sc.up);
+    return light_emission(s, li, ls.color, sc) * rgb_to_spectrum(bval * n_l, sc.up);
 }
 
 // _evaluateBSDFConnection (:693-780); HDR_BOUNCE_INLINE as sample_bounce

@@ -16,6 +16,7 @@
 
 #include "rng.cuh"
 #include "sky.cuh"
+#include "spectrum.cuh"
 #include "traverse.cuh"
 
 // HDR_SKY 0 compiles the light code without the physical sky, for kernels whose
@@ -41,6 +42,34 @@ struct LightSampleD {  // LightSample
 };
 
 __device__ __forceinline__ int light_type(const DeviceScene &s, int li) { return fbits(__ldg(&s.lights[12 * li].x)); }
+
+// Extension (hdr_light_desc.temperature > 0): blackbody emission. Planck's law
+// B(l, T) = 2hc^2 / l^5 / (exp(c2 / (l T)) - 1), c2 = hc / k, divided by its value at
+// Wien's peak l_max = b / T, where c2 / (l_max T) = c2 / b: (l_max / l)^5 (e^(c2/b) - 1) /
+// (exp(c2 / (l T)) - 1), at the wavelength l in nm.
+__device__ __forceinline__ float blackbody_normalized(float lambda_nm, float kelvin) {
+    const float c2 = 1.4387769e-2f, wien_b = 2.8977721e-3f;  // m K
+    const float l = lambda_nm * 1e-9f, lmax = wien_b / kelvin;
+    const float r = lmax / l;
+    const float peak_den = 142.32490f;  // e^(c2 / b) - 1, c2 / b = 4.9651141
+    return (r * r * r * r * r) * peak_den / expm1f(c2 / (l * kelvin));
+}
+// The spectral emission of scene light li whose sample carries the colour rgb: the
+// colour upsampled as the reference does, or the blackbody spectrum times the light's
+// effective intensity (record float 35) for a light with a temperature (record float 15).
+__device__ __forceinline__ Spec light_emission(const DeviceScene &s, int li, V3 rgb, const SpectralCtx &sc) {
+    if (li >= 0 && li < s.num_lights) {
+        const float kelvin = __ldg(&s.lights[12 * li + 3]).w;
+        if (kelvin > 0.0f) {
+            const float eff = __ldg(&s.lights[12 * li + 8]).w;
+            Spec e;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) e.v[i] = eff * blackbody_normalized(sc.lambda.l[i], kelvin);
+            return e;
+        }
+    }
+    return rgb_to_spectrum(rgb, sc.up);
+}
 // ILight::IsDeltaLight; light index num_lights is the physical sky's sun (a delta light)
 __device__ __forceinline__ bool light_is_delta(const DeviceScene &s, int li) {
     return li >= s.num_lights || fbits(__ldg(&s.lights[12 * li].y)) != 0;

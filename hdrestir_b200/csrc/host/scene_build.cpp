@@ -408,6 +408,10 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
             err = "light " + std::to_string(i) + ": unknown type";
             return false;
         }
+        if (!(L.temperature >= 0.0f) || !std::isfinite(L.temperature)) {
+            err = "light " + std::to_string(i) + ": temperature must be finite and >= 0";
+            return false;
+        }
         float *r = &out.lights[(size_t)i * kLightFloats];
         float M[16];
         for (int k = 0; k < 16; ++k) M[k] = (float)L.transform[k];  // GfMatrix4f(GfMatrix4d)
@@ -422,7 +426,7 @@ bool build_flat_scene(const hdr_scene_desc &desc, FlatScene &out, std::string &e
         const float head[16] = {as_float(L.type), as_float(is_delta), L.width, L.height,
                                 color.x, color.y, color.z, area,
                                 lnormal.x, lnormal.y, lnormal.z, L.shaping_cone_angle,
-                                cos_cone, cos_inner, L.shaping_cone_softness, 0.0f};
+                                cos_cone, cos_inner, L.shaping_cone_softness, L.temperature};
         std::memcpy(r, head, sizeof(head));
         std::memcpy(r + 16, M, sizeof(M));
         // light params color & intensity kept separately for the dome's CompMult

@@ -79,6 +79,7 @@ class Light:  # LightFactoryInput / LightParams (sceneInterface/light_params.h:1
     height: float = 1.0
     shaping_cone_angle: float = 180.0
     shaping_cone_softness: float = 0.0
+    temperature: float = 0.0  # extension: blackbody emission in kelvin (0 = the colour)
     texture: np.ndarray | None = None  # dome: (H, W, 3) f32
 
 
@@ -168,6 +169,7 @@ class Scene:
             d.transform[:] = [float(v) for v in np.asarray(L.transform, np.float64).reshape(-1)]
             d.width, d.height = float(L.width), float(L.height)
             d.shaping_cone_angle, d.shaping_cone_softness = float(L.shaping_cone_angle), float(L.shaping_cone_softness)
+            d.temperature = float(L.temperature)
             if L.texture is not None:
                 tex = np.ascontiguousarray(L.texture, np.float32)
                 keep.append(tex)

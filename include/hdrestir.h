@@ -180,6 +180,10 @@ typedef struct hdr_light_desc {
     float shaping_cone_softness;
     const float *texture;        /* dome: RGB f32, tex_width*tex_height*3 (the decoded TextureFile) */
     int32_t tex_width, tex_height;
+    float temperature;           /* extension, no reference counterpart: > 0 makes a rect, triangle,
+                                    point or distant light emit a blackbody spectrum of this many
+                                    kelvin (Planck's law at the sampled wavelengths, 1 at its peak)
+                                    times intensity * 2^exposure, in place of its colour; 0 = colour */
 } hdr_light_desc;
 
 typedef struct hdr_scene_desc {

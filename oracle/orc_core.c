@@ -448,6 +448,7 @@ orc_scene *orc_scene_create(const hdr_scene_desc *d) {
         L->height = ld->height;
         L->cone_angle = ld->shaping_cone_angle;
         L->cone_softness = ld->shaping_cone_softness;
+        L->temperature = ld->temperature;
         if (L->type == HDR_LIGHT_DOME) {
             if (s->env < 0) {
                 s->env = i;

@@ -135,6 +135,7 @@ typedef struct {
     float color[3], intensity, exposure;
     double xf[16];
     float width, height, cone_angle, cone_softness;
+    float temperature; /* extension: blackbody emission in kelvin, 0 = the colour */
     float *pixels;
     int w, h;
     float *row_cdf, *col_cdf;

@@ -416,6 +416,25 @@ static void light_matrix(const olight *L, float *m) {
 static ov3 light_color(const olight *L) {
     return vmulf(V(L->color[0], L->color[1], L->color[2]), L->intensity * exp2f(L->exposure));
 }
+/* Extension: blackbody emission (hdr_light_desc.temperature > 0), Planck's law divided by its
+ * value at Wien's peak: (lmax / l)^5 (e^(c2/b) - 1) / (exp(c2 / (l T)) - 1); else the colour
+ * upsampled as the reference does. */
+static float blackbody_normalized(float lambda_nm, float kelvin) {
+    const float c2 = 1.4387769e-2f, wien_b = 2.8977721e-3f;
+    const float l = lambda_nm * 1e-9f, lmax = wien_b / kelvin;
+    const float r = lmax / l;
+    return (r * r * r * r * r) * 142.32490f / expm1f(c2 / (l * kelvin));
+}
+static ospec light_emission(const orc_scene *s, int li, ov3 rgb, const olambda *w) {
+    if (li >= 0 && li < s->n_lights && s->lights[li].temperature > 0.0f) {
+        const olight *L = &s->lights[li];
+        const float eff = L->intensity * exp2f(L->exposure);
+        ospec e;
+        for (int i = 0; i < 4; ++i) e.v[i] = eff * blackbody_normalized(w->l[i], L->temperature);
+        return e;
+    }
+    return orc_rgb_to_spectrum(rgb, w);
+}
 static int is_delta(const olight *L) { return L->type == HDR_LIGHT_POINT || L->type == HDR_LIGHT_DISTANT; }
 /* ILight::IsDeltaLight by index: n_lights is the physical sky's sun (a delta light) */
 static int light_delta(const orc_scene *s, int li) { return li >= s->n_lights || is_delta(&s->lights[li]); }
@@ -667,7 +686,7 @@ static int mis_nee(const orc_scene *s, const osurf *sf, int li, const olsample *
     ov3 wo = vneg(sf->rd);
     *bp = ggx_pdf(&sf->c, sf->sn, wo, ls->dir);
     ov3 bv = ggx_eval(&sf->c, sf->sn, wo, ls->dir);
-    *rad = smulf(smul(orc_rgb_to_spectrum(bv, w), orc_rgb_to_spectrum(ls->color, w)), nl / *pn);
+    *rad = smulf(smul(orc_rgb_to_spectrum(bv, w), light_emission(s, li, ls->color, w)), nl / *pn);
     return 1;
 }
 
@@ -770,12 +789,12 @@ static ocontrib eval_light_sample(const orc_scene *s, const osurf *sf, int li, c
     if (nl <= 0.0f || pn <= 0.0f || (cy <= 0.0f && !delta)) return r;
     r.tmul = orc_rgb_to_spectrum(vmulf(bv, nl), w);
     if (skip) {
-        r.emission = orc_rgb_to_spectrum(ls->color, w);
+        r.emission = light_emission(s, li, ls->color, w);
         r.vis_tested = 0;
         return r;
     }
     if (occluded(s, vadd(sf->hit.position, vmulf(sf->sn, 1e-4f)), ls->dir, ls->dist)) return r;
-    r.emission = orc_rgb_to_spectrum(ls->color, w);
+    r.emission = light_emission(s, li, ls->color, w);
     return r;
 }
 
@@ -829,7 +848,7 @@ static ospec reeval(const orc_scene *s, const osurf *sf, int li, const olsample 
     float pn = pdf_sa(ls->pdf, ls->solid, d2, omax(cy, 1e-6f));
     if (nl <= 0.0f || pn <= 0.0f || (cy <= 0.0f && !light_delta(s, li))) return S1(0.0f);
     ov3 bv = ggx_eval(&sf->c, sf->sn, wo, ls->dir);
-    return smul(orc_rgb_to_spectrum(ls->color, w), orc_rgb_to_spectrum(vmulf(bv, nl), w));
+    return smul(light_emission(s, li, ls->color, w), orc_rgb_to_spectrum(vmulf(bv, nl), w));
 }
 
 /* per-pixel RIS trace records for parity tests */
