@@ -25,6 +25,10 @@
 #ifndef HDR_SKY
 #define HDR_SKY 1
 #endif
+// HDR_BLACKBODY 0 likewise leaves out the blackbody emission extension.
+#ifndef HDR_BLACKBODY
+#define HDR_BLACKBODY 1
+#endif
 
 namespace hdr {
 
@@ -58,7 +62,7 @@ __device__ __forceinline__ float blackbody_normalized(float lambda_nm, float kel
 // colour upsampled as the reference does, or the blackbody spectrum times the light's
 // effective intensity (record float 35) for a light with a temperature (record float 15).
 __device__ __forceinline__ Spec light_emission(const DeviceScene &s, int li, V3 rgb, const SpectralCtx &sc) {
-    if (li >= 0 && li < s.num_lights) {
+    if (HDR_BLACKBODY && s.blackbody && li >= 0 && li < s.num_lights) {
         const float kelvin = __ldg(&s.lights[12 * li + 3]).w;
         if (kelvin > 0.0f) {
             const float eff = __ldg(&s.lights[12 * li + 8]).w;

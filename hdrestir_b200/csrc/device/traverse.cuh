@@ -43,6 +43,7 @@ struct DeviceScene {
     // PhysicalSky (sky.cuh): the environment when `sky` is 1. Its sun is light index
     // num_lights for reservoirs and the delta-light test, outside the light sampler.
     int sky;
+    int blackbody;             // extension: some light has a temperature (blackbody emission)
     float4 sky_sun;            // the sun direction; w = 1 when SampleDirect gives a sample
     float4 sky_sun_n;          // the direction normalised again, as Sample() uses it
     float4 sky_sun_color;      // SampleDirect's colour

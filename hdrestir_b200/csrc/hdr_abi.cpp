@@ -966,6 +966,8 @@ hdr_status hdr_scene_upload(hdr_ctx *c, const hdr_scene_desc *desc) {
     s.num_lights = f.num_lights;
     s.env_light = f.env_light;
     s.sky = desc->enable_physical_sky ? 1 : 0;
+    s.blackbody = 0;
+    for (int i = 0; i < desc->num_lights; ++i) s.blackbody |= desc->lights[i].temperature > 0.0f ? 1 : 0;
     if (s.sky) {  // PhysicalSky's sun (scene.cpp:249-254, physical_sky.cpp:161-169), with the host's libm
         const hdr::V3 sun = hdr::sky_sun_direction(desc->physical_sky_time);
         const hdr::V3 sun_n = hdr::normalized(sun);
@@ -1206,10 +1208,11 @@ static hdr_status ris_path_trace_pass(hdr_ctx *c, const hdr_camera *cam, int32_t
     if (p->spatial_neighbors < 0 || p->spatial_neighbors > 64 || !(p->spatial_radius >= 0.0f))
         return fail(HDR_EINVAL, "spatial_neighbors %d / spatial_radius out of range ([0, 64], >= 0)",
                     p->spatial_neighbors);
-    // wavefront form: direct light only (no later bounces), no stochastic opacity, and no
-    // physical sky (its sun technique is served by the one-kernel form only)
-    const bool wave =
-        p->path.max_depth == 1 && c->scene_opaque && !c->scene.sky && !(p->flags & HDR_RIS_ONE_KERNEL);
+    // wavefront form: direct light only (no later bounces), no stochastic opacity, no physical
+    // sky (its sun technique is served by the one-kernel form only) and no blackbody lights
+    // (an extension the wavefront kernels are built without, to keep their registers)
+    const bool wave = p->path.max_depth == 1 && c->scene_opaque && !c->scene.sky && !c->scene.blackbody &&
+                      !(p->flags & HDR_RIS_ONE_KERNEL);
     const bool spatial = p->spatial_neighbors > 0 && p->use_reservoir;
     if (spatial && !wave)
         return fail(HDR_EINVAL, "spatial reuse runs in the wavefront form only (max_depth 1, opaque scene)");
@@ -1658,7 +1661,8 @@ hdr_status hdr_ris_path_trace_batch(hdr_ctx *const *ctxs, int32_t n, const hdr_c
         const hdr_ris_params *p = &params[i];
         together = p->spatial_neighbors == 0 && !(p->flags & HDR_RIS_REPROJECT) && c->device == ctxs[0]->device && c->has_scene && c->scene_store &&
                    c->scene_store == ctxs[0]->scene_store && c->scene.wide == ctxs[0]->scene.wide &&
-                   p->path.max_depth == 1 && c->scene_opaque && !c->scene.sky && !(p->flags & HDR_RIS_ONE_KERNEL);
+                   p->path.max_depth == 1 && c->scene_opaque && !c->scene.sky && !c->scene.blackbody &&
+                   !(p->flags & HDR_RIS_ONE_KERNEL);
     }
     std::vector<hdr_ctx *> order(ctxs, ctxs + n);
     std::sort(order.begin(), order.end());

@@ -33,7 +33,8 @@
 #ifndef HDR_WAVE_TEXTURED
 #define HDR_TEXTURES 0
 #endif
-#define HDR_SKY 0  // the launchers never take a scene under the physical sky
+#define HDR_SKY 0        // the launchers never take a scene under the physical sky
+#define HDR_BLACKBODY 0  // nor one with blackbody lights (extension)
 #define HDR_CANDIDATE_INLINE __forceinline__
 #define HDR_BOUNCE_INLINE __forceinline__
 
