@@ -133,7 +133,7 @@ struct TraceTuning {
     int node_quorum = 12;  // best for the SAH-tree walks (16 for the reference-tree ones)
     int blocks_per_sm = 16;
     int sm_count = 148;
-    int shade_shape = 3;  // ris_shade launch shape, 0 .. kShadeShapes - 1 (128 x 4: fastest at 1080p)
+    int shade_shape = 1;  // ris_shade launch shape, 0 .. kShadeShapes - 1 (256 x 2: fastest at 1080p)
     int shadow_shape = 1; // shadow-BVH walk register budget, 0 .. kShadowShapes - 1: 64 / 80 / 90 registers
 };
 // ris_shade launch shapes: (threads per block, minimum resident blocks per SM)

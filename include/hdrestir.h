@@ -592,8 +592,8 @@ hdr_status hdr_trace_rays(hdr_ctx *ctx, const float *rays, const float *tmax, in
  * warp step nodes (1..32); blocks_per_sm: persistent blocks per SM (1..64).
  * trace_ms: device time of the two trace kernels (autotune output).
  * shade_shape: launch shape of the resampling kernel: 0 = 256 threads with the
- * register file of one block per SM, 1 = 256 threads for two blocks,
- * 2 / 3 (default) = 128 threads for three / four blocks (no effect on results).
+ * register file of one block per SM, 1 (default) = 256 threads for two blocks,
+ * 2 / 3 = 128 threads for three / four blocks (no effect on results).
  * shadow_shape: register budget of the shadow-BVH walk kernel: 0 = 64 registers
  * (8 resident blocks of 128 threads), 1 (default) = 80 (6 blocks), 2 = 90 (5 blocks). */
 typedef struct hdr_trace_tuning {
